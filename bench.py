@@ -1,0 +1,394 @@
+"""Benchmark of the B200 SMAC step (CADMAS-SURF/3D VF_V1CAL + VF_F1CAL).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): the plain FP64 wave flume with a porous breakwater,
+512 x 32 x 96 cells (dx=dy=0.02 m, dz=0.01 m), still-water depth 0.5 m,
+porous block x in [6,7] m, z < 0.6 m, porosity 0.4, CM 1.2, CD 1.0, 2 m
+sponge at the outlet, dt = 2e-3 s, BiCGSTAB relative tolerance 1e-10.
+The wave train H = 0.08 m, T = 1.5 s is the initial state (first-order
+progressive wave over the whole flume) instead of a wave maker at x = 0.
+
+One step = one full SMAC step on the GPU (momentum predictor, Poisson
+assembly, MILU-BiCGSTAB solve, correction, VOF advection and flags).
+value = interior cells x steps / device time (CUDA events on the library's
+stream) over all ranks; with N GPUs every rank runs its own replica of the
+flume (independent instances, no data exchange).  e2e = the same through
+the Fortran-callable entry point vf_step_gpu_ with the state in pinned host
+arrays copied in and out every step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "multiscale-and-multiphysics-integrated-simulator-for-tsunami_b200"
+METRIC = "Mcell-steps/s at 1e-8 rel residual: learned+mixed vs plain FP64 GPU; HBM %"
+UNIT = "Mcell-steps/s"
+
+# Algorithmic bytes per interior cell of each stage (each distinct array
+# read or written once: 8 B per double, 4 B per int).
+STAGE_BYTES = {
+    "flux": 10 * 8 + 5 * 4 + 9 * 8,      # u,v,w,ANU,GL*,GG* + NF,IND*,INDC -> 9 fluxes
+    "predict": 19 * 8 + 4 * 4 + 3 * 8,   # 9 fluxes,u,v,w,p,GGV,GLV,CD0,GG* + NF,IND* -> u,v,w
+    "vpcoef": 10 * 8 + 5 * 4 + 8 * 8,    # u,v,w,p,F,GGV,GLV,GG* + NF,INDC,IND* -> 8 arrays
+    "dcmp": 7 * 8 + 4 + 8,               # 7 coefficients + INDC -> DD
+    "fwd": 7 * 8 + 8 + 8 + 4 + 8,        # 7 coefficients, P, DD, INDC -> T (SpMV fused)
+    "bwd": 5 * 8 + 4 + 8,                # T, AUI, AUJ, AUK, DD, INDC -> X
+}
+
+
+def _load_pkg():
+    import importlib.util
+    if "cadmas_b200" in sys.modules:
+        return sys.modules["cadmas_b200"]
+    spec = importlib.util.spec_from_file_location("cadmas_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["cadmas_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def combine_ranks(t_local: float, units_local: float, device=None):
+    """Max of the per-rank times and sum of the per-rank work units."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return t_local, units_local
+    t = torch.tensor([t_local], dtype=torch.float64, device=device)
+    u = torch.tensor([units_local], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
+def build_case(args):
+    P = _load_pkg()
+    c = P.cases.porous_flume(nx=args.nx, ny=args.ny, nz=args.nz)
+    P.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
+    return c
+
+
+def params_for(args):
+    return dict(cgepsr=1.0e-10, precond_ti=args.ti, precond_tj=args.tj)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = max(mx)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(sm)
+        os.unlink(self.path)
+        return out
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(case, args, max_seconds=25.0, min_steps=1):
+    """The oracle (single-thread CPU restatement, reference summation order)
+    on the same flume: one warm-up step, then timed steps until max_seconds."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    sys.path.pop(0)
+    o = pyoracle.Oracle(case, sum_mode=pyoracle.SUM_REF, **params_for(args))
+    o.init_state(True)
+    o.step(case.dt)
+    n, t0 = 0, time.perf_counter()
+    while n < min_steps or (time.perf_counter() - t0 < max_seconds and n < 50):
+        o.step(case.dt)
+        n += 1
+    dt = time.perf_counter() - t0
+    o.close()
+    return case.interior_cells * n / dt / 1e6, n, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    case = build_case(args)
+    budget = 150.0
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    sys.path.pop(0)
+    o = pyoracle.Oracle(case, sum_mode=pyoracle.SUM_REF, **params_for(args))
+    o.init_state(True)
+    for _ in range(min(args.warmup, 1)):
+        o.step(case.dt)
+    n, t0 = 0, time.perf_counter()
+    while n < args.steps and (n == 0 or time.perf_counter() - t0 < budget):
+        o.step(case.dt)
+        n += 1
+    dt = time.perf_counter() - t0
+    v = case.interior_cells * n / dt / 1e6
+    sample = (f"{n} of {args.steps} steps of the {case.ni-2}x{case.nj-2}x{case.nk-2} flume after "
+              f"{min(args.warmup, 1)} warm-up step(s), {dt:.1f} s")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+            "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / n,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(case, args),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(case, args):
+    return {"workload": f"porous wave flume {case.ni-2}x{case.nj-2}x{case.nk-2} plain FP64 SMAC step "
+                        f"(linear wave initial state, dt={case.dt}, tol 1e-10, block-Jacobi MILU "
+                        f"{args.ti}x{args.tj} columns)",
+            "cells": case.interior_cells, "precond_block": [args.ti, args.tj],
+            "l2": "inputs larger than L2 (about 40 arrays of 13.7 MB resident)"}
+
+
+def pinned_state(P, case, torch):
+    """Host state arrays in pinned memory, Fortran order."""
+    ni, nj, nk, nb = case.ni, case.nj, case.nk, max(case.numb, 1)
+
+    def buf(n, dt):
+        t = torch.empty(n, dtype=dt, pin_memory=True)
+        return t
+
+    keep, arrs = [], {}
+    for n in ("uu", "vv", "ww", "pp", "ff"):
+        t = buf(ni * nj * nk, torch.float64)
+        keep.append(t)
+        arrs[n] = t.numpy().reshape((ni, nj, nk), order="F")
+    for n in ("nf", "indc"):
+        t = buf(ni * nj * nk, torch.int32)
+        keep.append(t)
+        arrs[n] = t.numpy().reshape((ni, nj, nk), order="F")
+    for n in ("bcu", "bcv", "bcw", "bcp", "bcf"):
+        t = buf(nb, torch.float64)
+        keep.append(t)
+        arrs[n] = t.numpy()
+    return keep, arrs
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    P = _load_pkg()
+    sys.path.insert(0, str(PKG_DIR))
+    import build as pbuild
+    sys.path.pop(0)
+    if rank == 0:
+        pbuild.build()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    case = build_case(args)
+    tank = P.Tank(case, **params_for(args))
+    tank.init_state(True)
+    stream = torch.cuda.ExternalStream(tank.stream(), device=dev)
+    for _ in range(args.warmup):
+        tank.step(case.dt)
+    tank.sync()
+    tank.stage_timers(enable=1)
+    l0 = P.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    iters = []
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            tank.step(case.dt)
+            iters.append(tank.stats()["icgitr"])
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    launches = P.kernel_launches() - l0
+    t_ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        dist.barrier()
+    stages = tank.stage_timers(enable=0)
+    clocks = clk.summary()
+    t_max, units = combine_ranks(t_ms / 1e3, case.interior_cells * args.steps, device=dev)
+    value = units / t_max / 1e6
+    # true relative residual of one more solve (diagnostic, outside the timing)
+    relres = None
+    try:
+        tank2 = P.Tank(case, diag_relres=1, **params_for(args))
+        tank2.set_state(tank.get_state())
+        tank2.step(case.dt)
+        relres = tank2.stats()["true_relres"]
+        tank2.close()
+    except Exception:
+        relres = None
+    # ---- end to end through vf_step_gpu_ with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        keep, arrs = pinned_state(P, case, torch)
+        st = tank.get_state()
+        for n in arrs:
+            arrs[n][...] = st[n][: arrs[n].shape[0]] if arrs[n].ndim == 1 else st[n]
+        lib = tank.lib
+        hp = ctypes.c_void_p(tank.h.value)
+        dtc = ctypes.c_double(case.dt)
+        tnow = ctypes.c_double(st["tnow"])
+        nnow = ctypes.c_int(st["nnow"])
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        argv = [ctypes.byref(hp), ctypes.byref(dtc), dp(arrs["uu"]), dp(arrs["vv"]), dp(arrs["ww"]),
+                dp(arrs["pp"]), dp(arrs["ff"]), ip(arrs["nf"]), ip(arrs["indc"]), dp(arrs["bcu"]),
+                dp(arrs["bcv"]), dp(arrs["bcw"]), dp(arrs["bcp"]), dp(arrs["bcf"]), ctypes.byref(tnow),
+                ctypes.byref(nnow)]
+        nsteps_e2e = max(1, min(args.steps, 10))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(nsteps_e2e):
+            rc = lib.vf_step_gpu_(*argv)
+            if rc != 0:
+                raise P.CadmasError(rc, "vf_step_gpu_")
+        e1.record(stream)
+        e1.synchronize()
+        te_max, ue = combine_ranks(e0.elapsed_time(e1) / 1e3, case.interior_cells * nsteps_e2e, device=dev)
+        bytes_io = sum(a.nbytes for a in arrs.values())
+        e2e = {"value": ue / te_max / 1e6, "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+               "d2h_bytes_per_step": bytes_io, "steps": nsteps_e2e,
+               "path": "vf_step_gpu_ (pinned host state in/out every step)"}
+    # ---- roofline of the dominant stage
+    peak, peak_kind = measured_peak_hbm()
+    dom = max((k for k in STAGE_BYTES), key=lambda k: stages[k][0])
+    ms_dom, n_dom = stages[dom]
+    bytes_launch = STAGE_BYTES[dom] * case.interior_cells
+    achieved = bytes_launch / (ms_dom / n_dom / 1e3) / 1e9 if n_dom else 0.0
+    total_ms = sum(v[0] for v in stages.values())
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_launch, "launches": n_dom,
+                "avg_launch_ms": ms_dom / n_dom if n_dom else None,
+                "share_of_step": ms_dom / total_ms if total_ms else None}
+    if rank != 0:
+        tank.close()
+        return
+    cpu = None
+    if not args.no_cpu:
+        v_cpu, n_cpu, t_cpu = cpu_baseline(case, args)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{n_cpu} steps of the same flume after 1 warm-up step, {t_cpu:.1f} s, "
+                         f"single-thread oracle (reference summation order)"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {**workload_config(case, args), "parallelism": f"replicas x{world}",
+                       "mean_bicgstab_iters": float(np.mean(iters)), "true_relres": relres},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks,
+            "stage_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()}}
+    print(json.dumps(line), flush=True)
+    tank.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--ny", type=int, default=32)
+    ap.add_argument("--nz", type=int, default=96)
+    ap.add_argument("--ti", type=int, default=16)
+    ap.add_argument("--tj", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

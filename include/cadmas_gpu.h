@@ -1,0 +1,224 @@
+/*
+ * cadmas_gpu.h -- C ABI of the B200 SMAC time-step library (libcadmas_gpu.so).
+ *
+ * The library replaces the two per-step driver subroutines of CADMAS-SURF/3D:
+ *   VF_V1CAL  (Simulators/CADMAS-SURF-3D/Source code/vf_v1cal.f:1-9)
+ *   VF_F1CAL  (Simulators/CADMAS-SURF-3D/Source code/vf_f1cal.f:1-20)
+ * which the time loop calls at vf_a1main.f:1058-1066 and :1104-1115.
+ *
+ * Data layout follows the Fortran program so that a Fortran or C caller can
+ * pass its own arrays unchanged:
+ *   - cell/face arrays are (NUMI,NUMJ,NUMK) column-major, I fastest, with one
+ *     ghost layer on every side (NUMI = cells in x + 2).  Element (I,J,K),
+ *     1-based, is at offset (I-1) + NUMI*((J-1) + NUMJ*(K-1));
+ *   - face arrays are staggered: UU(I,J,K) is the x-face between cells I-1
+ *     and I (vf_vmodif.f:74);
+ *   - grid metrics XX(6,NUMI), YY(6,NUMJ), ZZ(6,NUMK) hold
+ *     (coordinate, d, c, 1/d, 1/c, 1/(d_i+d_{i-1})) as built by VF_CGRID
+ *     (vf_cgrid.f:44-67);
+ *   - INDB(4,NUMB) is the boundary-face list of VF_CINDB (vf_cindb.f).
+ *
+ * Every entry point returns an int status (CADMAS_OK on success).  The
+ * reference aborts the MPI job through VF_A2ERR instead (vf_a2err.f:46-49);
+ * the codes below map its messages.  State lives on the GPU between calls;
+ * host arrays are read or written only by the calls that name them.  A
+ * handle is bound to the device that was current at cadmas_create and owns
+ * one CUDA stream; calls on one handle must come from one host thread.
+ */
+#ifndef CADMAS_GPU_H
+#define CADMAS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CADMAS_OK            0
+#define CADMAS_EINVAL        1  /* bad argument or size                          */
+#define CADMAS_ECUDA         2  /* CUDA runtime error                            */
+#define CADMAS_ENOTCONV      3  /* 'NOT CONVERGED.'          vf_vpsol.f:71-72    */
+#define CADMAS_EDIVERGE      4  /* 'INSTABILITY.'            vf_vpsol.f:73-74    */
+#define CADMAS_EPIVOT        5  /* 'CAN NOT DECOMPOSITION.'  vf_vpsol.f:75-76    */
+#define CADMAS_EPG           6  /* 'P.G ERROR.' (vf_vpcoef.f:433, vf_fnfprv.f:223)*/
+#define CADMAS_ECAP          7  /* a device-side iteration cap was reached       */
+#define CADMAS_ENOMEM        8  /* device allocation failed                      */
+#define CADMAS_EUNSUPPORTED  9  /* option outside the implemented path           */
+#define CADMAS_ENOSTATIC    10  /* cadmas_upload_static not called yet           */
+
+/* ---- sizes (/VF_ANUMBI/, VF_ANUMBI.h) ----------------------------------- */
+typedef struct cadmas_dims {
+  int numi, numj, numk;  /* NUMI, NUMJ, NUMK: cells + 2 in each direction */
+  int numb;              /* NUMB: number of boundary faces (INDB columns)  */
+} cadmas_dims;
+
+/* ---- parameters read from COMMON blocks by the reference ---------------- */
+typedef struct cadmas_params {
+  double rho0;           /* RHO0   /VF_APHYSR/  (default 1.0e3, vf_a2dflt.f)  */
+  double grz0;           /* GRZ0   /VF_APHYSR/  gravity (default 9.8)          */
+  double vvmax;          /* VVMAX  velocity clamp in VF_VEULER (default 30)     */
+  double cgpara;         /* CGPARA MILU parameter (default 0.95)               */
+  double cgepsa;         /* CGEPSA absolute tolerance (default 1e-15)          */
+  double cgepsr;         /* CGEPSR relative tolerance (default 1e-12)          */
+  double cgdiv;          /* CGDIV  divergence threshold (default 1e30)         */
+  double flower;         /* FLOWER = FEPS (default 1e-6)                       */
+  double fupper;         /* FUPPER = 1-FEPS                                     */
+  double plower;         /* PLOWER porosity floor (default 1e-4)               */
+  double scmvp;          /* SCMVP  upwind weight of momentum fluxes (1 = donor) */
+  double wvlvl;          /* WVLVL  still-water level                           */
+  double wbub;           /* WBUB   TimerDoor bubble rise speed; < 0 disables    */
+  double glxmin, glxmax; /* GLXMIN/GLXMAX domain x extent (sponge distances)   */
+  double glymin, glymax; /* GLYMIN/GLYMAX domain y extent                       */
+  double damp[4][4];     /* DAMP(1..4,JD) as damp[JD-1][m-1]: PARAM-XY,
+                            PARAM-Z, WIDTH, DEPTH of sponge JD = X-,X+,Y-,Y+  */
+  int    idamp[4];       /* IDAMP(JD): sponge degree, < 0 = no sponge           */
+  int    icgtyp;         /* ICGTYP 0 = ILU, otherwise MILU (default 1)         */
+  int    icgmax;         /* ICGMAX iteration cap (default 500)                 */
+  int    ibsuw0;         /* IBSUW0 0 = linear extrapolation of surface velocity */
+  /* Preconditioner decomposition.  The reference run on NPI x NPJ MPI ranks
+     (PARALLEL X/Y, vf_cpara.f) factors and sweeps MILU inside each rank's
+     x-y block only (vf_mzdcmp.f:53-67 over MYIS..MYIE, MYJS..MYJE), i.e. a
+     block-Jacobi MILU.  precond_ti/precond_tj give the interior cells per
+     block in x and y; 0 means one block spanning the whole axis (the serial
+     NPROCS=1 reference).                                                    */
+  int    precond_ti, precond_tj;
+  /* 1: after every solve also measure the true residual ||b-Ax||/||b||
+     (cadmas_stats.true_relres); costs one extra pass over the system. */
+  int    diag_relres;
+  int    reserved[5];
+} cadmas_params;
+
+/* ---- static fields (set once; host pointers) ---------------------------- */
+typedef struct cadmas_static {
+  const double *xx, *yy, *zz;      /* XX(6,NUMI), YY(6,NUMJ), ZZ(6,NUMK)      */
+  const double *ggv, *ggx, *ggy, *ggz;   /* porosity, face permeabilities     */
+  const double *glv, *glx, *gly, *glz;   /* = G + (1-G)*CM (VF_CGLV/CGLXYZ)   */
+  const double *cd0;               /* drag coefficient CD0                     */
+  const double *anu;               /* ANU molecular (+eddy) viscosity          */
+  const int    *indx, *indy, *indz;/* face index (-1 obstacle,0 normal,>0 bnd)*/
+  const int    *indb;              /* INDB(4,NUMB)                             */
+} cadmas_static;
+
+/* ---- dynamic state (host pointers; read by set_state, written by get_state)
+   NULL pointers are skipped.                                                 */
+typedef struct cadmas_state {
+  double *uu, *vv, *ww, *pp, *ff;  /* (NUMI,NUMJ,NUMK)                         */
+  int    *nf, *indc;               /* NF, INDC                                 */
+  double *bcu, *bcv, *bcw, *bcp, *bcf; /* (NUMB) boundary values              */
+  double *tbub;                    /* TBUB(NUMK) TimerDoor timers              */
+  double tnow;                     /* TNOW                                     */
+  int    nnow;                     /* NNOW                                     */
+} cadmas_state;
+
+/* ---- per-step record (the list-file line of vf_a1main.f:954-961) -------- */
+typedef struct cadmas_stats {
+  double fsum, fcut;               /* fluid volume and cut-off volume (FCUT01) */
+  double cgbnrm, cgxnrm;           /* |M^-1 b|, |M^-1 r| of the last solve     */
+  double divnorm;                  /* |VD| from VF_CDIV00                      */
+  double true_relres;              /* ||b-Ax||_2/||b||_2 of the last solve,
+                                      INDC != -1 cells; < 0 when not measured  */
+  int    icgitr;                   /* ICGITR iterations of the last solve      */
+  int    nums;                     /* NUMS surface cells                       */
+  int    last_status;              /* status of the last step                  */
+  int    pad;
+} cadmas_stats;
+
+typedef struct cadmas_handle cadmas_handle;
+
+/* Defaults of vf_a2dflt.f for every field of cadmas_params. */
+void cadmas_default_params(cadmas_params *p);
+
+/* Allocate device state for one grid on the current device.
+   Replaces the ALLOCATE block of vf_a1main.f:415-700 for the step arrays. */
+int cadmas_create(const cadmas_dims *d, const cadmas_params *p,
+                  cadmas_handle **out);
+int cadmas_destroy(cadmas_handle *h);
+
+/* Upload metrics, porosity, face indices and the boundary list
+   (the fields VF_CGRID/VF_CGLV/VF_CGLXYZ/VF_CINDX/VF_CINDB prepare). */
+int cadmas_upload_static(cadmas_handle *h, const cadmas_static *s);
+
+/* Copy host state to the device (NULL members skipped). */
+int cadmas_set_state(cadmas_handle *h, const cadmas_state *s);
+/* Copy device state to the host (NULL members skipped). */
+int cadmas_get_state(cadmas_handle *h, cadmas_state *s);
+
+/* Initial classification and boundary values of VF_CINIT
+   (vf_cinit.f:202-207 and the BC calls after :283): FCUT01, BWFF, FNFINI,
+   FNFPRV, CINDC; then, if hydrostatic != 0, p = RHO0*GRZ0*(WVLVL - z_c) on
+   INDC != -1 cells (vf_cinit.f:283); then BWUWN, BSUWT, BSUWT2, BSUWN3,
+   BSPP, BWUWT, BWPP.  F must be set (cadmas_set_state) before the call. */
+int cadmas_init_state(cadmas_handle *h, int hydrostatic);
+
+/* One SMAC step of vf_a1main.f:1029-1104 with LOOPS=1: NNOW += 1,
+   TNOW += dt, VF_V1CAL, VF_F1CAL. */
+int cadmas_step(cadmas_handle *h, double dt);
+/* The two halves separately (TNOW/DTNOW already advanced by the caller
+   through cadmas_set_time). */
+int cadmas_set_time(cadmas_handle *h, double tnow, double dtnow, int nnow);
+int cadmas_v1cal(cadmas_handle *h);
+int cadmas_f1cal(cadmas_handle *h);
+
+/* VF_CDIV00 (vf_cdiv00.f:38-56) on the current state; also stored in stats. */
+int cadmas_divnorm(cadmas_handle *h, double *val);
+int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st);
+
+/* Synchronise the handle's stream. */
+int cadmas_sync(cadmas_handle *h);
+
+/* ---- Fortran-callable step (drop-in for the two CALLs of the time loop) --
+   Arguments by reference, as gfortran passes them.  The arrays are the
+   caller's host arrays; they are copied in before and out after the step,
+   so a Fortran time loop can call it in place of
+     CALL VF_V1CAL(...) ; CALL VF_F1CAL(...)
+   The handle comes from cadmas_create + cadmas_upload_static.           */
+int vf_step_gpu_(cadmas_handle **h, const double *dtnow,
+                 double *uu, double *vv, double *ww, double *pp, double *ff,
+                 int *nf, int *indc, double *bcu, double *bcv, double *bcw,
+                 double *bcp, double *bcf, double *tnow, int *nnow);
+
+/* ---- Poisson solver alone (VF_M1BCGS, vf_m1bcgs.f:1-5) -----------------
+   Device pointers, (NUMI,NUMJ,NUMK) each.  x0 is the initial guess on
+   entry and the solution on exit when converged (vf_m1bcgs.f:251-261).
+   iter receives ICGITR semantics (>icgmax not converged, -1 factorisation
+   failed, -2 diverged); bnorm/xnorm receive the square roots of
+   |M^-1 b|^2 and |M^-1 r|^2.  Scratch comes from the handle.            */
+int cadmas_m1bcgs_dev(cadmas_handle *h,
+                      const double *ad, const double *ali, const double *alj,
+                      const double *alk, const double *aui, const double *auj,
+                      const double *auk, const double *bb, double *x0,
+                      const int *indc, int *iter, double *bnorm,
+                      double *xnorm);
+
+/* The CUDA stream (cudaStream_t) on which every call of the handle issues
+   its work; callers may record CUDA events on it or wait on it. */
+int cadmas_get_stream(cadmas_handle *h, void **stream);
+
+/* Number of kernels this library has launched in the process so far. */
+long long cadmas_kernel_launches(void);
+
+/* Per-stage GPU time.  While enabled, every launch of a stage is
+   bracketed by two CUDA events on the handle's stream; ms[i] and count[i]
+   receive the accumulated milliseconds and launches of stage i (see
+   CADMAS_STAGE_*), for n <= CADMAS_NSTAGES stages.  enable < 0 only reads;
+   enable 0/1 switches timing off/on and clears the totals. */
+#define CADMAS_STAGE_FLUX      0  /* VF_VFLXDU/DV/DW                          */
+#define CADMAS_STAGE_PREDICT   1  /* VF_VGENE + VF_VEULER                     */
+#define CADMAS_STAGE_VPCOEF    2  /* VF_VPCOEF                                */
+#define CADMAS_STAGE_DCMP      3  /* VF_MZDCMP                                */
+#define CADMAS_STAGE_FWD       4  /* VF_MZAX + VF_MZFRWD (fused)              */
+#define CADMAS_STAGE_BWD       5  /* VF_MZBKWD                                */
+#define CADMAS_STAGE_DOT       6  /* VF_MZIP dot products and scalar updates  */
+#define CADMAS_STAGE_VEC       7  /* BiCGSTAB vector updates                  */
+#define CADMAS_STAGE_MODIF     8  /* VF_VMODIF and the V1CAL boundary rules   */
+#define CADMAS_STAGE_VOF       9  /* FCONV, FEULER, FMOD1, FCUT01             */
+#define CADMAS_STAGE_FLAGS    10  /* FNFINI, FBUBUP, FNFPRV, CINDC            */
+#define CADMAS_STAGE_FBC      11  /* F1CAL boundary rules, BSPPFL             */
+#define CADMAS_NSTAGES        12
+int cadmas_stage_timers(cadmas_handle *h, int enable, double *ms, long long *count, int n);
+
+const char *cadmas_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CADMAS_GPU_H */

@@ -1,0 +1,315 @@
+"""Python host side of libcadmas_gpu.so, the B200 SMAC step of CADMAS-SURF/3D.
+
+This mirrors the per-step driver interface of the reference
+(VF_V1CAL, Simulators/CADMAS-SURF-3D/Source code/vf_v1cal.f:1-9, and
+VF_F1CAL, vf_f1cal.f:1-20, called once per step from the time loop at
+vf_a1main.f:1058 and :1104) over the C ABI declared in
+include/cadmas_gpu.h.  Arrays are numpy arrays of shape (NUMI,NUMJ,NUMK) in
+Fortran order, exactly the Fortran arrays.  The reference aborts through
+VF_A2ERR on an error; here every call raises CadmasError carrying the status
+code and the reference's message.
+
+The CUDA library is required: importing this package does not need a GPU,
+but creating a Tank without libcadmas_gpu.so, or without a CUDA device,
+raises.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+import numpy as np
+
+from . import cases  # noqa: F401  (re-exported)
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libcadmas_gpu.so"
+
+OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC = range(11)
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class Dims(C.Structure):
+    _fields_ = [("numi", C.c_int), ("numj", C.c_int), ("numk", C.c_int), ("numb", C.c_int)]
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "rho0", "grz0", "vvmax", "cgpara", "cgepsa", "cgepsr", "cgdiv", "flower", "fupper",
+        "plower", "scmvp", "wvlvl", "wbub", "glxmin", "glxmax", "glymin", "glymax")] + [
+        ("damp", (C.c_double * 4) * 4),
+        ("idamp", C.c_int * 4),
+        ("icgtyp", C.c_int), ("icgmax", C.c_int), ("ibsuw0", C.c_int),
+        ("precond_ti", C.c_int), ("precond_tj", C.c_int),
+        ("diag_relres", C.c_int), ("reserved", C.c_int * 5)]
+
+
+class Static(C.Structure):
+    _fields_ = [(n, _dp) for n in ("xx", "yy", "zz", "ggv", "ggx", "ggy", "ggz", "glv", "glx",
+                                   "gly", "glz", "cd0", "anu")] + [
+        (n, _ip) for n in ("indx", "indy", "indz", "indb")]
+
+
+class State(C.Structure):
+    _fields_ = [(n, _dp) for n in ("uu", "vv", "ww", "pp", "ff")] + [
+        ("nf", _ip), ("indc", _ip)] + [(n, _dp) for n in ("bcu", "bcv", "bcw", "bcp", "bcf", "tbub")] + [
+        ("tnow", C.c_double), ("nnow", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("fsum", "fcut", "cgbnrm", "cgxnrm", "divnorm", "true_relres")] + [
+        (n, C.c_int) for n in ("icgitr", "nums", "last_status", "pad")]
+
+
+EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_upload_static",
+            "cadmas_set_state", "cadmas_get_state", "cadmas_init_state", "cadmas_step",
+            "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
+            "cadmas_sync", "vf_step_gpu_", "cadmas_m1bcgs_dev", "cadmas_strerror",
+            "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers"]
+
+STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]
+
+
+class CadmasError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: pathlib.Path | None = None):
+    """Load libcadmas_gpu.so (no GPU needed to load it)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise CadmasError(EINVAL, f"{p} not built: run build.py (nvcc, sm_100a)")
+    lib = C.CDLL(str(p))
+    lib.cadmas_default_params.argtypes = [C.POINTER(Params)]
+    lib.cadmas_default_params.restype = None
+    lib.cadmas_create.argtypes = [C.POINTER(Dims), C.POINTER(Params), C.POINTER(C.c_void_p)]
+    lib.cadmas_destroy.argtypes = [C.c_void_p]
+    lib.cadmas_upload_static.argtypes = [C.c_void_p, C.POINTER(Static)]
+    lib.cadmas_set_state.argtypes = [C.c_void_p, C.POINTER(State)]
+    lib.cadmas_get_state.argtypes = [C.c_void_p, C.POINTER(State)]
+    lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
+    lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
+    lib.cadmas_set_time.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+    lib.cadmas_v1cal.argtypes = [C.c_void_p]
+    lib.cadmas_f1cal.argtypes = [C.c_void_p]
+    lib.cadmas_divnorm.argtypes = [C.c_void_p, _dp]
+    lib.cadmas_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    lib.cadmas_sync.argtypes = [C.c_void_p]
+    lib.cadmas_m1bcgs_dev.argtypes = [C.c_void_p] + [C.c_void_p] * 10 + [_ip, _dp, _dp]
+    lib.cadmas_get_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.cadmas_kernel_launches.argtypes = []
+    lib.cadmas_kernel_launches.restype = C.c_longlong
+    lib.cadmas_stage_timers.argtypes = [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_longlong), C.c_int]
+    lib.cadmas_strerror.argtypes = [C.c_int]
+    lib.cadmas_strerror.restype = C.c_char_p
+    vf = lib.vf_step_gpu_
+    vf.argtypes = [C.POINTER(C.c_void_p), _dp] + [_dp] * 5 + [_ip, _ip] + [_dp] * 5 + [_dp, _ip]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, rc):
+    if rc != OK:
+        raise CadmasError(rc, lib.cadmas_strerror(rc).decode())
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def default_params(lib=None) -> Params:
+    lib = lib or load_library()
+    p = Params()
+    lib.cadmas_default_params(C.byref(p))
+    return p
+
+
+def make_params(case, base: Params | None = None, **over) -> Params:
+    """cadmas_params for a case: library defaults (vf_a2dflt.f), then the
+    case's settings, then keyword overrides."""
+    p = base if base is not None else default_params()
+    d = dict(case.params)
+    d.update(over)
+    for k, v in d.items():
+        if k in ("idamp",):
+            for i in range(4):
+                p.idamp[i] = int(v[i])
+        elif k.startswith("damp_"):
+            jd = {"damp_xm": 0, "damp_xp": 1, "damp_ym": 2, "damp_yp": 3}[k]
+            for m in range(4):
+                p.damp[jd][m] = float(v[m])
+        elif k == "anu0":
+            continue
+        elif hasattr(p, k):
+            setattr(p, k, type(getattr(p, k))(v))
+        else:
+            raise KeyError(f"unknown parameter {k}")
+    return p
+
+
+def static_of(case) -> Static:
+    s = Static()
+    for n in ("xx", "yy", "zz", "ggv", "ggx", "ggy", "ggz", "glv", "glx", "gly", "glz", "cd0", "anu"):
+        a = getattr(case, n)
+        assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1)
+        setattr(s, n, _dptr(a))
+    for n in ("indx", "indy", "indz", "indb"):
+        a = getattr(case, n)
+        assert a.dtype == np.int32 and a.flags.f_contiguous
+        setattr(s, n, _iptr(a))
+    return s
+
+
+def new_state_arrays(ni, nj, nk, nb):
+    f3 = lambda dt: np.zeros((ni, nj, nk), dtype=dt, order="F")
+    nbx = max(nb, 1)
+    return dict(uu=f3(np.float64), vv=f3(np.float64), ww=f3(np.float64), pp=f3(np.float64),
+                ff=f3(np.float64), nf=f3(np.int32), indc=f3(np.int32),
+                bcu=np.zeros(nbx), bcv=np.zeros(nbx), bcw=np.zeros(nbx), bcp=np.zeros(nbx),
+                bcf=np.zeros(nbx), tbub=np.zeros(nk), tnow=0.0, nnow=0)
+
+
+def state_struct(arrs) -> State:
+    s = State()
+    for n in ("uu", "vv", "ww", "pp", "ff", "bcu", "bcv", "bcw", "bcp", "bcf", "tbub"):
+        setattr(s, n, _dptr(arrs.get(n)))
+    s.nf = _iptr(arrs.get("nf"))
+    s.indc = _iptr(arrs.get("indc"))
+    s.tnow = float(arrs.get("tnow", 0.0))
+    s.nnow = int(arrs.get("nnow", 0))
+    return s
+
+
+def initial_state(case):
+    """Host arrays of the initial state of a case (F, velocities; NF from
+    the obstacle map, INDC unset) for cadmas_set_state."""
+    st = new_state_arrays(case.ni, case.nj, case.nk, case.numb)
+    st["uu"][...] = case.uu
+    st["vv"][...] = case.vv
+    st["ww"][...] = case.ww
+    st["pp"][...] = case.pp
+    st["ff"][...] = case.ff
+    st["nf"][...] = case.nf
+    st["indc"][...] = -1
+    for n in ("bcu", "bcv", "bcw", "bcp", "bcf"):
+        st[n][...] = getattr(case, n)
+    return st
+
+
+class Tank:
+    """One grid on the GPU: the state of the time loop between two steps."""
+
+    def __init__(self, case, lib=None, **over):
+        self.lib = lib or load_library()
+        self.case = case
+        self.params = make_params(case, default_params(self.lib), **over)
+        d = Dims(case.ni, case.nj, case.nk, case.numb)
+        h = C.c_void_p()
+        _check(self.lib, self.lib.cadmas_create(C.byref(d), C.byref(self.params), C.byref(h)))
+        self.h = h
+        self._static = static_of(case)   # keep the pointers' owners alive
+        _check(self.lib, self.lib.cadmas_upload_static(self.h, C.byref(self._static)))
+        self.set_state(initial_state(case))
+
+    # ------------------------------------------------------------ state
+    def set_state(self, arrs):
+        s = state_struct(arrs)
+        _check(self.lib, self.lib.cadmas_set_state(self.h, C.byref(s)))
+
+    def get_state(self):
+        arrs = new_state_arrays(self.case.ni, self.case.nj, self.case.nk, self.case.numb)
+        s = state_struct(arrs)
+        _check(self.lib, self.lib.cadmas_get_state(self.h, C.byref(s)))
+        arrs["tnow"], arrs["nnow"] = s.tnow, s.nnow
+        return arrs
+
+    def init_state(self, hydrostatic=True):
+        _check(self.lib, self.lib.cadmas_init_state(self.h, int(bool(hydrostatic))))
+
+    # ------------------------------------------------------------ step
+    def step(self, dt=None):
+        _check(self.lib, self.lib.cadmas_step(self.h, float(dt if dt is not None else self.case.dt)))
+
+    def set_time(self, tnow, dtnow, nnow):
+        _check(self.lib, self.lib.cadmas_set_time(self.h, float(tnow), float(dtnow), int(nnow)))
+
+    def v1cal(self):
+        _check(self.lib, self.lib.cadmas_v1cal(self.h))
+
+    def f1cal(self):
+        _check(self.lib, self.lib.cadmas_f1cal(self.h))
+
+    def divnorm(self):
+        v = C.c_double()
+        _check(self.lib, self.lib.cadmas_divnorm(self.h, C.byref(v)))
+        return v.value
+
+    def stats(self):
+        st = Stats()
+        _check(self.lib, self.lib.cadmas_get_stats(self.h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in Stats._fields_ if n != "pad"}
+
+    def sync(self):
+        _check(self.lib, self.lib.cadmas_sync(self.h))
+
+    def stream(self) -> int:
+        """Address of the cudaStream_t all work of this tank runs on."""
+        p = C.c_void_p()
+        _check(self.lib, self.lib.cadmas_get_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def stage_timers(self, enable=-1):
+        """Per-stage GPU milliseconds and launch counts; enable 1/0 also
+        switches timing on/off and clears the totals."""
+        n = len(STAGES)
+        ms = (C.c_double * n)()
+        cnt = (C.c_longlong * n)()
+        _check(self.lib, self.lib.cadmas_stage_timers(self.h, int(enable), ms, cnt, n))
+        return {STAGES[i]: (ms[i], cnt[i]) for i in range(n)}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cadmas_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def kernel_launches(lib=None) -> int:
+    """Kernels launched by libcadmas_gpu.so in this process so far."""
+    return int((lib or load_library()).cadmas_kernel_launches())
+
+
+def m1bcgs_dev(tank: Tank, ad, ali, alj, alk, aui, auj, auk, bb, x0, indc):
+    """VF_M1BCGS on device buffers (integer device addresses, e.g. from
+    torch.Tensor.data_ptr()).  Returns (iter, bnorm, xnorm); x0 is updated
+    in place on convergence."""
+    it, bn, xn = C.c_int(), C.c_double(), C.c_double()
+    args = [C.c_void_p(int(a)) for a in (ad, ali, alj, alk, aui, auj, auk, bb, x0, indc)]
+    _check(tank.lib, tank.lib.cadmas_m1bcgs_dev(tank.h, *args, C.byref(it), C.byref(bn), C.byref(xn)))
+    return it.value, bn.value, xn.value

@@ -1,0 +1,550 @@
+"""Synthetic wave-tank cases: the host-side set-up of CADMAS-SURF/3D in numpy.
+
+The Fortran program prepares the static fields of a run once, before the time
+loop, from its text input.  This module does the same from Python arguments,
+restating the set-up routines (Simulators/CADMAS-SURF-3D/Source code/):
+
+  grid metrics XX/YY/ZZ(6,N)       VF_CGRID   vf_cgrid.f:44-67
+  ghost cells and obstacles NF=-1  VF_CNFDFL  vf_cnfdfl.f:37-50, VF_IIOBST vf_iiobst.f:50
+  porosity GGV/GGX/GGY/GGZ, CM, CD VF_IIPORO  vf_iiporo.f:80-245
+  face indices INDX/INDY/INDZ      VF_CINDX   vf_cindx.f:30-140
+  boundary list INDB(4,NUMB)       VF_CINDB   vf_cindb.f:30-95
+  GLV, GLX/GLY/GLZ                 VF_CGLV    vf_cglv.f:34, VF_CGLXYZ vf_cglxyz.f:65-105
+  ANU                              VF_CNU00   vf_cnu00.f:30-45
+  initial F (still water + F box)  VF_CINIT   vf_cinit.f:150-190
+
+Every 3-D array is a numpy array of shape (NUMI, NUMJ, NUMK) in Fortran
+order, so ``a.ctypes.data`` is the Fortran array the library expects.
+Indices in the arguments below are the Fortran array indices (1-based, ghost
+layer included): interior cells are 2..NUMI-1.
+
+Randomness (obstacle boxes, porosity) comes from numpy's Philox generator
+seeded with the case seed, so the GPU library and the oracle see the same
+bytes.
+"""
+from __future__ import annotations
+
+import dataclasses
+import numpy as np
+
+# Velocity/pressure boundary types INDB(3,L) and F boundary types INDB(4,L)
+# (vf_a1main.f:151-170).
+VP_SLIP, VP_NOSLIP, VP_FIXED, VP_FREE, VP_WAVE = 1, 2, 3, 4, 5
+F_FIXED, F_FREE = 1, 2
+
+
+def grid_metrics(coords: np.ndarray) -> np.ndarray:
+    """VF_CGRID (vf_cgrid.f:44-67) for one axis of a serial run.
+
+    coords: the NUML-1 face coordinates of the interior, XYZ(1,2..NUML).
+    Returns XYZ(6,NUML) in Fortran order, flattened as the library expects.
+    """
+    coords = np.asarray(coords, dtype=np.float64)
+    nl = coords.size + 1
+    x = np.zeros((6, nl), order="F")
+    x[0, 1:] = coords
+    for i in range(1, nl - 1):            # I = 2..NUML-1
+        x[1, i] = x[0, i + 1] - x[0, i]
+        x[3, i] = 1.0 / x[1, i]
+    x[1, 0] = x[1, 1]                     # LG1 == 2
+    x[3, 0] = 1.0 / x[1, 0]
+    x[0, 0] = x[0, 1] - x[1, 0]
+    x[1, nl - 1] = x[1, nl - 2]           # LG2 == NUML0
+    x[3, nl - 1] = 1.0 / x[1, nl - 1]
+    for i in range(1, nl):                # I = 2..NUML
+        x[2, i] = (x[1, i] + x[1, i - 1]) / 2.0
+        x[4, i] = 1.0 / x[2, i]
+        x[5, i] = 1.0 / (x[1, i] + x[1, i - 1])
+    x[2, 0] = x[4, 0] = x[5, 0] = 0.0
+    return x
+
+
+@dataclasses.dataclass
+class Case:
+    """Static fields, initial state and parameters of one run."""
+    name: str
+    ni: int
+    nj: int
+    nk: int
+    xx: np.ndarray
+    yy: np.ndarray
+    zz: np.ndarray
+    nf: np.ndarray
+    ggv: np.ndarray
+    ggx: np.ndarray
+    ggy: np.ndarray
+    ggz: np.ndarray
+    cm0: np.ndarray
+    cd0: np.ndarray
+    glv: np.ndarray = None
+    glx: np.ndarray = None
+    gly: np.ndarray = None
+    glz: np.ndarray = None
+    anu: np.ndarray = None
+    indx: np.ndarray = None
+    indy: np.ndarray = None
+    indz: np.ndarray = None
+    indb: np.ndarray = None
+    numb: int = 0
+    ff: np.ndarray = None
+    uu: np.ndarray = None
+    vv: np.ndarray = None
+    ww: np.ndarray = None
+    pp: np.ndarray = None
+    bcu: np.ndarray = None
+    bcv: np.ndarray = None
+    bcw: np.ndarray = None
+    bcp: np.ndarray = None
+    bcf: np.ndarray = None
+    params: dict = dataclasses.field(default_factory=dict)
+    dt: float = 1e-3
+    hydrostatic: bool = True
+
+    @property
+    def interior_cells(self) -> int:
+        return (self.ni - 2) * (self.nj - 2) * (self.nk - 2)
+
+
+def _z3(ni, nj, nk, val=0.0, dtype=np.float64):
+    return np.full((ni, nj, nk), val, dtype=dtype, order="F")
+
+
+def new_case(name, xs, ys, zs) -> Case:
+    """Grid from face coordinates; all cells fluid-capable, porosity 1
+    (vf_a1main.f:495-510), ghost layer obstacle (VF_CNFDFL)."""
+    xx, yy, zz = grid_metrics(xs), grid_metrics(ys), grid_metrics(zs)
+    ni, nj, nk = xx.shape[1], yy.shape[1], zz.shape[1]
+    nf = np.zeros((ni, nj, nk), dtype=np.int32, order="F")
+    nf[0, :, :] = nf[-1, :, :] = -1
+    nf[:, 0, :] = nf[:, -1, :] = -1
+    nf[:, :, 0] = nf[:, :, -1] = -1
+    return Case(name=name, ni=ni, nj=nj, nk=nk, xx=xx, yy=yy, zz=zz, nf=nf,
+                ggv=_z3(ni, nj, nk, 1.0), ggx=_z3(ni, nj, nk, 1.0),
+                ggy=_z3(ni, nj, nk, 1.0), ggz=_z3(ni, nj, nk, 1.0),
+                cm0=_z3(ni, nj, nk), cd0=_z3(ni, nj, nk))
+
+
+def add_obstacle(c: Case, i1, j1, k1, i2, j2, k2):
+    """OBST box over array cells I1..I2, J1..J2, K1..K2 (vf_iiobst.f:42-53)."""
+    c.nf[i1 - 1:i2, j1 - 1:j2, k1 - 1:k2] = -1
+
+
+def add_porous(c: Case, i1, j1, k1, i2, j2, k2, gamma, cm=0.0, cd=0.0,
+               plower=1.0e-4):
+    """POROUS V/X/Y/Z/CM/CD over array cells I1..I2 x J1..J2 x K1..K2
+    (vf_iiporo.f): cells get GGV; the faces of those cells, both sides
+    included, get GGX/GGY/GGZ; CM/CD on non-obstacle cells."""
+    val = max(gamma, plower)  # VAL=MAX(V2+(1-V2)*V1,PLOWER) with V2=0
+    sl = (slice(i1 - 1, i2), slice(j1 - 1, j2), slice(k1 - 1, k2))
+    obst = c.nf[sl] == -1
+    c.ggv[sl] = np.where(obst, c.ggv[sl], val)
+    c.cm0[sl] = np.where(obst, c.cm0[sl], cm)
+    c.cd0[sl] = np.where(obst, c.cd0[sl], cd)
+    c._porous_faces = getattr(c, "_porous_faces", [])
+    c._porous_faces.append((i1, j1, k1, i2, j2, k2, val))
+
+
+def _apply_porous_faces(c: Case):
+    # Face permeabilities need INDX/INDY/INDZ (set only where not -1).
+    for (i1, j1, k1, i2, j2, k2, val) in getattr(c, "_porous_faces", []):
+        sx = (slice(i1 - 1, i2 + 1), slice(j1 - 1, j2), slice(k1 - 1, k2))
+        sy = (slice(i1 - 1, i2), slice(j1 - 1, j2 + 1), slice(k1 - 1, k2))
+        sz = (slice(i1 - 1, i2), slice(j1 - 1, j2), slice(k1 - 1, k2 + 1))
+        c.ggx[sx] = np.where(c.indx[sx] != -1, val, c.ggx[sx])
+        c.ggy[sy] = np.where(c.indy[sy] != -1, val, c.ggy[sy])
+        c.ggz[sz] = np.where(c.indz[sz] != -1, val, c.ggz[sz])
+
+
+def build_faces(c: Case):
+    """VF_CINDX (vf_cindx.f:30-140): -1 between two obstacles, a boundary
+    number (1-based, numbered x, then y, then z faces, each in K,J,I order)
+    where exactly one side is obstacle, 0 otherwise."""
+    ni, nj, nk, nf = c.ni, c.nj, c.nk, c.nf
+    indx = np.zeros((ni, nj, nk), dtype=np.int32, order="F")
+    indy = np.zeros_like(indx)
+    indz = np.zeros_like(indx)
+    ob = nf == -1
+    indx[0, :, :] = -1
+    indx[1:, :, :] = np.where(ob[:-1, :, :] & ob[1:, :, :], -1, 0)
+    indy[:, 0, :] = -1
+    indy[:, 1:, :] = np.where(ob[:, :-1, :] & ob[:, 1:, :], -1, 0)
+    indz[:, :, 0] = -1
+    indz[:, :, 1:] = np.where(ob[:, :, :-1] & ob[:, :, 1:], -1, 0)
+    numb = 0
+    # x faces: K=2..NK-1, J=2..NJ-1, I=2..NI
+    cand = np.zeros_like(indx, dtype=bool)
+    n1 = ob[:-1, :, :]
+    n2 = ob[1:, :, :]
+    cx = (n1 | n2) & (indx[1:, :, :] != -1)
+    cand[1:, :, :] = cx
+    cand[:, 0, :] = cand[:, -1, :] = False
+    cand[:, :, 0] = cand[:, :, -1] = False
+    # exceptions: I==2 and N2==-1, I==NUMI and N1==-1
+    cand[1, :, :] &= ~ob[1, :, :]
+    cand[ni - 1, :, :] &= ~ob[ni - 2, :, :]
+    idx = np.nonzero(cand.ravel(order="F"))[0]
+    vals = np.arange(numb + 1, numb + 1 + idx.size, dtype=np.int32)
+    flat = indx.reshape(-1, order="F")
+    flat[idx] = vals
+    indx = flat.reshape((ni, nj, nk), order="F")
+    numb += idx.size
+    # y faces: K=2..NK-1, J=2..NJ, I=2..NI-1
+    cand = np.zeros_like(indy, dtype=bool)
+    cy = (ob[:, :-1, :] | ob[:, 1:, :]) & (indy[:, 1:, :] != -1)
+    cand[:, 1:, :] = cy
+    cand[0, :, :] = cand[-1, :, :] = False
+    cand[:, :, 0] = cand[:, :, -1] = False
+    cand[:, 1, :] &= ~ob[:, 1, :]
+    cand[:, nj - 1, :] &= ~ob[:, nj - 2, :]
+    idx = np.nonzero(cand.ravel(order="F"))[0]
+    flat = indy.reshape(-1, order="F")
+    flat[idx] = np.arange(numb + 1, numb + 1 + idx.size, dtype=np.int32)
+    indy = flat.reshape((ni, nj, nk), order="F")
+    numb += idx.size
+    # z faces: K=2..NK, J=2..NJ-1, I=2..NI-1 (no end exceptions)
+    cand = np.zeros_like(indz, dtype=bool)
+    cz = (ob[:, :, :-1] | ob[:, :, 1:]) & (indz[:, :, 1:] != -1)
+    cand[:, :, 1:] = cz
+    cand[0, :, :] = cand[-1, :, :] = False
+    cand[:, 0, :] = cand[:, -1, :] = False
+    idx = np.nonzero(cand.ravel(order="F"))[0]
+    flat = indz.reshape(-1, order="F")
+    flat[idx] = np.arange(numb + 1, numb + 1 + idx.size, dtype=np.int32)
+    indz = flat.reshape((ni, nj, nk), order="F")
+    numb += idx.size
+    c.indx, c.indy, c.indz, c.numb = indx, indy, indz, numb
+
+
+def build_boundary_list(c: Case, vp_type=VP_SLIP, f_type=F_FREE, faces=None):
+    """VF_CINDB (vf_cindb.f:30-95) plus the B.C. types.
+
+    faces: optional callable (axis, i, j, k, side) -> (vp, f) overriding the
+    default types for individual faces (1-based array indices)."""
+    nb = max(c.numb, 1)
+    indb = np.zeros((4, nb), dtype=np.int32, order="F")
+    ni, nj = c.ni, c.nj
+    for axis, ind, ns_lo, ns_hi in ((0, c.indx, 1, 2), (1, c.indy, 3, 4), (2, c.indz, 5, 6)):
+        flat = ind.reshape(-1, order="F")
+        pos = np.nonzero(flat >= 1)[0]
+        for p in pos:
+            nb_ = flat[p]
+            i = p % ni + 1
+            j = (p // ni) % nj + 1
+            k = p // (ni * nj) + 1
+            indb[0, nb_ - 1] = i + ni * (j - 1) + ni * nj * (k - 1)
+            n2 = c.nf[i - 1, j - 1, k - 1]
+            indb[1, nb_ - 1] = ns_lo if n2 != -1 else ns_hi
+            vp, ft = vp_type, f_type
+            if faces is not None:
+                o = faces(axis, i, j, k, indb[1, nb_ - 1])
+                if o is not None:
+                    vp, ft = o
+            indb[2, nb_ - 1] = vp
+            indb[3, nb_ - 1] = ft
+    c.indb = indb
+    zb = np.zeros(nb, dtype=np.float64)
+    c.bcu, c.bcv, c.bcw, c.bcp, c.bcf = (zb.copy() for _ in range(5))
+
+
+def build_inertia(c: Case):
+    """VF_CGLV (vf_cglv.f:34) and VF_CGLXYZ (vf_cglxyz.f:65-105)."""
+    ni, nj, nk = c.ni, c.nj, c.nk
+    c.glv = np.where(c.nf == -1, 1.0, c.ggv + (1.0 - c.ggv) * c.cm0)
+    c.glv = np.asfortranarray(c.glv)
+    glx = _z3(ni, nj, nk, 1.0)
+    gly = _z3(ni, nj, nk, 1.0)
+    glz = _z3(ni, nj, nk, 1.0)
+    x6, x2 = c.xx[5], c.xx[1]
+    y6, y2 = c.yy[5], c.yy[1]
+    z6, z2 = c.zz[5], c.zz[1]
+    cm, nf = c.cm0, c.nf
+    for k in range(nk):
+        for j in range(nj):
+            for i in range(ni):
+                # GLX
+                v = c.indx[i, j, k]
+                if v == -1:
+                    glx[i, j, k] = 1.0
+                elif v == 0:
+                    m = x6[i] * (x2[i] * cm[i, j, k] + x2[i - 1] * cm[i - 1, j, k])
+                    glx[i, j, k] = c.ggx[i, j, k] + (1.0 - c.ggx[i, j, k]) * m
+                elif nf[i, j, k] != -1:
+                    glx[i, j, k] = c.ggx[i, j, k] + (1.0 - c.ggx[i, j, k]) * cm[i, j, k]
+                else:
+                    glx[i, j, k] = c.ggx[i, j, k] + (1.0 - c.ggx[i, j, k]) * cm[i - 1, j, k]
+                v = c.indy[i, j, k]
+                if v == -1:
+                    gly[i, j, k] = 1.0
+                elif v == 0:
+                    m = y6[j] * (y2[j] * cm[i, j, k] + y2[j - 1] * cm[i, j - 1, k])
+                    gly[i, j, k] = c.ggy[i, j, k] + (1.0 - c.ggy[i, j, k]) * m
+                elif nf[i, j, k] != -1:
+                    gly[i, j, k] = c.ggy[i, j, k] + (1.0 - c.ggy[i, j, k]) * cm[i, j, k]
+                else:
+                    gly[i, j, k] = c.ggy[i, j, k] + (1.0 - c.ggy[i, j, k]) * cm[i, j - 1, k]
+                v = c.indz[i, j, k]
+                if v == -1:
+                    glz[i, j, k] = 1.0
+                elif v == 0:
+                    m = z6[k] * (z2[k] * cm[i, j, k] + z2[k - 1] * cm[i, j, k - 1])
+                    glz[i, j, k] = c.ggz[i, j, k] + (1.0 - c.ggz[i, j, k]) * m
+                elif nf[i, j, k] != -1:
+                    glz[i, j, k] = c.ggz[i, j, k] + (1.0 - c.ggz[i, j, k]) * cm[i, j, k]
+                else:
+                    glz[i, j, k] = c.ggz[i, j, k] + (1.0 - c.ggz[i, j, k]) * cm[i, j, k - 1]
+    c.glx, c.gly, c.glz = glx, gly, glz
+
+
+def build_inertia_fast(c: Case):
+    """Vectorised VF_CGLXYZ for large grids; same arithmetic per element."""
+    c.glv = np.asfortranarray(np.where(c.nf == -1, 1.0, c.ggv + (1.0 - c.ggv) * c.cm0))
+    cm, nf = c.cm0, c.nf
+
+    def one(ind, gg, d6, d2, axis):
+        sh = [1, 1, 1]
+        sh[axis] = -1
+        d6b = d6.reshape(sh)
+        d2b = d2.reshape(sh)
+        d2m = np.roll(d2, 1).reshape(sh)
+        cmm = np.roll(cm, 1, axis=axis)
+        m = d6b * (d2b * cm + d2m * cmm)
+        normal = gg + (1.0 - gg) * m
+        own = gg + (1.0 - gg) * cm
+        oth = gg + (1.0 - gg) * cmm
+        out = np.where(ind == -1, 1.0, np.where(ind == 0, normal, np.where(nf != -1, own, oth)))
+        return np.asfortranarray(out)
+
+    c.glx = one(c.indx, c.ggx, c.xx[5], c.xx[1], 0)
+    c.gly = one(c.indy, c.ggy, c.yy[5], c.yy[1], 1)
+    c.glz = one(c.indz, c.ggz, c.zz[5], c.zz[1], 2)
+
+
+def build_viscosity(c: Case, anu0=1.0e-6):
+    """VF_CNU00 without k-epsilon (vf_cnu00.f:30-45)."""
+    anu = _z3(c.ni, c.nj, c.nk)
+    inner = (slice(1, -1), slice(1, -1), slice(1, -1))
+    anu[inner] = np.where(c.nf[inner] != -1, anu0, 0.0)
+    c.anu = anu
+
+
+def init_f_still_water(c: Case, wvlvl: float):
+    """VF_CINIT F from the still-water level (vf_cinit.f:150-160)."""
+    ff = _z3(c.ni, c.nj, c.nk)
+    z1 = c.zz[0]
+    for k in range(1, c.nk - 1):          # K = 2..NK-1
+        if z1[k] > wvlvl:
+            val = 0.0
+        elif z1[k + 1] < wvlvl:
+            val = 1.0
+        else:
+            val = (wvlvl - z1[k]) / (z1[k + 1] - z1[k])
+        sl = c.nf[1:-1, 1:-1, k] != -1
+        ff[1:-1, 1:-1, k] = np.where(sl, val, 0.0)
+    c.ff = ff
+
+
+def f_box(c: Case, i1, j1, k1, i2, j2, k2, val):
+    """DEBUG F-BOX (vf_cinit.f:171-182), array indices."""
+    sl = (slice(i1 - 1, i2), slice(j1 - 1, j2), slice(k1 - 1, k2))
+    c.ff[sl] = np.where(c.nf[sl] != -1, val, c.ff[sl])
+
+
+def finish(c: Case, vp_type=VP_SLIP, f_type=F_FREE, faces=None, fast=None):
+    """Faces, boundary list, porous faces, inertia, viscosity, zero state."""
+    build_faces(c)
+    _apply_porous_faces(c)
+    build_boundary_list(c, vp_type, f_type, faces)
+    if fast is None:
+        fast = c.ni * c.nj * c.nk > 200_000
+    (build_inertia_fast if fast else build_inertia)(c)
+    build_viscosity(c, c.params.get("anu0", 1.0e-6))
+    shape = (c.ni, c.nj, c.nk)
+    c.uu = _z3(*shape)
+    c.vv = _z3(*shape)
+    c.ww = _z3(*shape)
+    c.pp = _z3(*shape)
+    if c.ff is None:
+        c.ff = _z3(*shape)
+    return c
+
+
+# ----------------------------------------------------------------- the cases
+def dam_break(nx=64, ny=8, nz=32, d=0.01, column=(16, 16), dt=1.0e-4):
+    """Plain FP64 dam break in a closed free-slip box.
+
+    64x8x32 cells of 0.01 m; water where x < 0.16 m and z < 0.16 m: still
+    water level 0.16 m plus an F box of F=0 over interior cells
+    i = 17..64, all j, k = 1..16 (DEBUG F-BOX)."""
+    c = new_case("dam_break", np.arange(nx + 1) * d, np.arange(ny + 1) * d,
+                 np.arange(nz + 1) * d)
+    c.params.update(wvlvl=column[1] * d, wbub=-1.0, cgepsr=1.0e-10)
+    init_f_still_water(c, column[1] * d)
+    f_box(c, column[0] + 2, 2, 2, nx + 1, ny + 1, column[1] + 1, 0.0)
+    c.dt = dt
+    return finish(c)
+
+
+def porous_flume(nx=512, ny=32, nz=96, dx=0.02, dy=0.02, dz=0.01, depth=0.5,
+                 block=(6.0, 7.0, 0.6), gamma=0.4, cm=1.2, cd=1.0,
+                 sponge_width=2.0, sponge_degree=2, dt=2.0e-3):
+    """Wave flume with a porous breakwater and an outlet sponge.
+
+    Still-water depth 0.5 m; porous block x in [6,7] m, full width,
+    z < 0.6 m, porosity 0.4, CM 1.2, CD 1.0; 2 m damping zone at x+
+    (MODEL DAMP X+).  Walls are free-slip."""
+    c = new_case("porous_flume", np.arange(nx + 1) * dx, np.arange(ny + 1) * dy,
+                 np.arange(nz + 1) * dz)
+    i1 = int(round(block[0] / dx)) + 2
+    i2 = int(round(block[1] / dx)) + 1
+    k2 = min(int(round(block[2] / dz)) + 1, nz + 1)
+    add_porous(c, i1, 2, 2, i2, ny + 1, k2, gamma, cm, cd)
+    c.params.update(wvlvl=depth, wbub=-1.0, cgepsr=1.0e-10,
+                    glxmin=0.0, glxmax=nx * dx, glymin=0.0, glymax=ny * dy,
+                    idamp=[-1, sponge_degree, -1, -1],
+                    damp_xp=[0.6, 0.6, sponge_width, depth])
+    init_f_still_water(c, depth)
+    c.dt = dt
+    return finish(c)
+
+
+def solitary_beach(nx=1024, ny=128, nz=128, dx=0.02, dy=0.02, dz=0.01,
+                   depth=0.6, x_toe=10.0, slope=1.0 / 20.0, amp=0.15,
+                   x0=5.0, nbox=40, seed=0, dt=1.0e-3):
+    """Solitary wave on a 1:20 beach with 40 seeded porous boxes.
+
+    Beach: staircase obstacle cells below z = (x - x_toe)*slope.  Boxes:
+    sides U(0.1,0.5) m, porosity U(0.3,1.0), resting on the bed.  The first
+    order solitary wave eta = A sech^2(k (x-x0)), k = sqrt(3A/(4h^3)),
+    u = sqrt(g/h) eta, is injected as the initial F and u."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    c = new_case("solitary_beach", np.arange(nx + 1) * dx, np.arange(ny + 1) * dy,
+                 np.arange(nz + 1) * dz)
+    xc = (np.arange(nx) + 0.5) * dx
+    zb = np.clip((xc - x_toe) * slope, 0.0, None)
+    for i in range(nx):
+        kk = int(np.floor(zb[i] / dz + 1e-9))
+        if kk > 0:
+            c.nf[i + 1, 1:-1, 1:kk + 1] = -1
+    for _ in range(nbox):
+        sx, sy, sz = rng.uniform(0.1, 0.5, size=3)
+        g = rng.uniform(0.3, 1.0)
+        bx = rng.uniform(0.0, nx * dx - sx)
+        by = rng.uniform(0.0, ny * dy - sy)
+        i1 = int(bx / dx) + 2
+        i2 = min(int((bx + sx) / dx) + 1, nx + 1)
+        j1 = int(by / dy) + 2
+        j2 = min(int((by + sy) / dy) + 1, ny + 1)
+        ic = min(max((i1 + i2) // 2 - 2, 0), nx - 1)
+        kb = int(np.floor(zb[ic] / dz + 1e-9)) + 2
+        k2 = min(kb + int(sz / dz) - 1, nz + 1)
+        if i2 >= i1 and j2 >= j1 and k2 >= kb:
+            add_porous(c, i1, j1, kb, i2, j2, k2, g)
+    g0 = 9.8
+    k_s = np.sqrt(3.0 * amp / (4.0 * depth ** 3))
+    eta = amp / np.cosh(k_s * (xc - x0)) ** 2
+    c.params.update(wvlvl=depth, wbub=-1.0, cgepsr=1.0e-8)
+    init_f_still_water(c, depth)
+    ff = c.ff
+    z1 = c.zz[0]
+    for i in range(nx):
+        lvl = depth + eta[i]
+        for k in range(1, nz + 1):
+            if z1[k] > lvl:
+                v = 0.0
+            elif z1[k + 1] < lvl:
+                v = 1.0
+            else:
+                v = (lvl - z1[k]) / (z1[k + 1] - z1[k])
+            ff[i + 1, 1:-1, k] = np.where(c.nf[i + 1, 1:-1, k] != -1, v, 0.0)
+    c.dt = dt
+    finish(c)
+    xf = c.xx[0]                                   # XX(1,I): face I position
+    u_face = np.sqrt(g0 / depth) * amp / np.cosh(k_s * (xf - x0)) ** 2
+    nf, ff, uu = c.nf, c.ff, c.uu
+    for i0 in range(2, c.ni - 1):                  # faces I = 3..NUMI-1
+        m = (nf[i0 - 1] != -1) & (nf[i0] != -1) & ((ff[i0 - 1] > 0.0) | (ff[i0] > 0.0))
+        uu[i0] = np.where(m, u_face[i0], 0.0)
+    c.hydrostatic = True
+    return c
+
+
+def random_tank(seed=0, nx=12, ny=6, nz=10, d=0.01, nobst=2, nporous=2,
+                level=0.55, nbox=2, dt=2.0e-4, slip=True):
+    """Small random tank for parity tests: obstacles, porous blocks, a still
+    water level and random F boxes, with random face spacing."""
+    rng = np.random.Generator(np.random.Philox(seed))
+
+    def axis(n):
+        w = rng.uniform(0.8, 1.25, size=n) * d
+        return np.concatenate([[0.0], np.cumsum(w)])
+
+    c = new_case(f"random_tank_{seed}", axis(nx), axis(ny), axis(nz))
+    for _ in range(nobst):
+        i1 = int(rng.integers(3, nx)); j1 = int(rng.integers(2, ny + 1))
+        i2 = min(i1 + int(rng.integers(0, 3)), nx + 1)
+        j2 = min(j1 + int(rng.integers(0, 3)), ny + 1)
+        k2 = int(rng.integers(2, max(3, nz // 3)))
+        add_obstacle(c, i1, j1, 2, i2, j2, k2)
+    for _ in range(nporous):
+        i1 = int(rng.integers(2, nx)); j1 = int(rng.integers(2, ny))
+        k1 = int(rng.integers(2, nz))
+        i2 = min(i1 + int(rng.integers(1, 4)), nx + 1)
+        j2 = min(j1 + int(rng.integers(1, 4)), ny + 1)
+        k2 = min(k1 + int(rng.integers(1, 4)), nz + 1)
+        add_porous(c, i1, j1, k1, i2, j2, k2, float(rng.uniform(0.3, 0.9)),
+                   float(rng.uniform(0.0, 1.5)), float(rng.uniform(0.0, 2.0)))
+    ztop = c.zz[0, -1]
+    wv = level * ztop
+    c.params.update(wvlvl=wv, wbub=-1.0, cgepsr=1.0e-12)
+    init_f_still_water(c, wv)
+    for _ in range(nbox):
+        i1 = int(rng.integers(2, nx + 1)); i2 = min(i1 + int(rng.integers(1, 5)), nx + 1)
+        j1 = int(rng.integers(2, ny + 1)); j2 = min(j1 + int(rng.integers(1, 4)), ny + 1)
+        k1 = int(rng.integers(2, nz + 1)); k2 = min(k1 + int(rng.integers(1, 4)), nz + 1)
+        f_box(c, i1, j1, k1, i2, j2, k2, float(rng.choice([0.0, 1.0, rng.uniform()])))
+    c.dt = dt
+    finish(c, vp_type=VP_SLIP if slip else VP_NOSLIP)
+    return c
+
+
+def linear_wave_initial(c: Case, H: float, T: float, depth: float, g0: float = 9.8):
+    """Fill the tank with a first-order (Airy) progressive wave train,
+    eta = H/2 cos(kx), u = H/2 w cosh(kz)/sinh(kh) cos(kx),
+    w = H/2 w sinh(kz)/sinh(kh) sin(kx) (z from the bed), with
+    w^2 = g k tanh(k h).  Used as the initial state of the flume workload
+    in place of a wave maker at the inflow boundary."""
+    om = 2.0 * np.pi / T
+    k = om * om / g0
+    for _ in range(60):  # Newton on f(k) = g k tanh(kh) - w^2
+        th = np.tanh(k * depth)
+        fk = g0 * k * th - om * om
+        dk = g0 * th + g0 * k * depth * (1.0 - th * th)
+        k -= fk / dk
+    a = 0.5 * H
+    x1, z1 = c.xx[0], c.zz[0]
+    xc = 0.5 * (x1[1:-1] + x1[2:])                    # cell centres I = 2..NI-1
+    level = depth + a * np.cos(k * xc)
+    for i in range(1, c.ni - 1):
+        lv = level[i - 1]
+        for kk in range(1, c.nk - 1):
+            if z1[kk] > lv:
+                v = 0.0
+            elif z1[kk + 1] < lv:
+                v = 1.0
+            else:
+                v = (lv - z1[kk]) / (z1[kk + 1] - z1[kk])
+            c.ff[i, 1:-1, kk] = np.where(c.nf[i, 1:-1, kk] != -1, v, 0.0)
+    zc = 0.5 * (z1[1:-1] + z1[2:])                    # cell-centre heights K = 2..NK-1
+    sk = np.sinh(k * depth)
+    wet = c.ff > 0.0
+    for i0 in range(2, c.ni - 1):                     # x faces between interior cells
+        prof = a * om * np.cosh(k * zc) / sk * np.cos(k * x1[i0])
+        m = (c.nf[i0 - 1, 1:-1, 1:-1] != -1) & (c.nf[i0, 1:-1, 1:-1] != -1) & \
+            (wet[i0 - 1, 1:-1, 1:-1] | wet[i0, 1:-1, 1:-1])
+        c.uu[i0, 1:-1, 1:-1] = np.where(m, prof[None, :], 0.0)
+    for kk in range(2, c.nk - 1):                     # z faces between interior cells
+        prof = a * om * np.sinh(k * z1[kk]) / sk * np.sin(k * xc)
+        m = (c.nf[1:-1, 1:-1, kk - 1] != -1) & (c.nf[1:-1, 1:-1, kk] != -1) & \
+            (wet[1:-1, 1:-1, kk - 1] | wet[1:-1, 1:-1, kk])
+        c.ww[1:-1, 1:-1, kk] = np.where(m, prof[:, None], 0.0)
+    return k

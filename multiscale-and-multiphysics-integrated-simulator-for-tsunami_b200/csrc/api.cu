@@ -1,0 +1,823 @@
+// api.cu -- handle, device memory and the step driver behind the C ABI of
+// include/cadmas_gpu.h.
+//
+// The driver issues the kernels in the call order of VF_V1CAL
+// (vf_v1cal.f:118-297) and VF_F1CAL (vf_f1cal.f:121-243) on one stream.
+// Host synchronisation happens only where the reference itself takes a
+// data-dependent branch on a global value: the BiCGSTAB convergence test
+// (batched, see solve()), the NF fixed-point loop of VF_FNFINI, and the
+// error flags at the end of a step.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cadmas_dev.cuh"
+#include "kernels.h"
+
+using namespace cadmas;
+
+std::atomic<long long> cadmas::g_kernel_launches{0};
+
+namespace {
+thread_local std::string g_last_error;
+
+#define CK(call)                                                              \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);      \
+      return CADMAS_ECUDA;                                                    \
+    }                                                                         \
+  } while (0)
+
+template <class T> int dalloc(T **p, size_t n) {
+  cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); *p = nullptr; return CADMAS_ENOMEM; }
+  e = cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); return CADMAS_ECUDA; }
+  return CADMAS_OK;
+}
+}  // namespace
+
+// Optional per-stage GPU timing with CUDA event pairs on the handle stream.
+struct StageTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  struct Pend { int stage; cudaEvent_t a, b; };
+  std::vector<Pend> pend;
+  cudaEvent_t open_a = nullptr;
+  int open_stage = -1;
+  double ms[CADMAS_NSTAGES] = {0};
+  long long cnt[CADMAS_NSTAGES] = {0};
+  cudaEvent_t get() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  void begin(cudaStream_t s, int stage) {
+    if (!on) return;
+    open_a = get();
+    cudaEventRecord(open_a, s);
+    open_stage = stage;
+  }
+  void end(cudaStream_t s) {
+    if (!on || open_stage < 0) return;
+    cudaEvent_t b = get();
+    cudaEventRecord(b, s);
+    pend.push_back({open_stage, open_a, b});
+    open_stage = -1;
+  }
+  void resolve() {
+    for (Pend &q : pend) {
+      float t = 0.0f;
+      cudaEventSynchronize(q.b);
+      cudaEventElapsedTime(&t, q.a, q.b);
+      ms[q.stage] += t;
+      cnt[q.stage] += 1;
+      pool.push_back(q.a);
+      pool.push_back(q.b);
+    }
+    pend.clear();
+  }
+  void clear() {
+    resolve();
+    for (int i = 0; i < CADMAS_NSTAGES; ++i) { ms[i] = 0.0; cnt[i] = 0; }
+  }
+  ~StageTimer() {
+    resolve();
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+};
+
+struct cadmas_handle {
+  int device = 0;
+  cudaStream_t s = nullptr;
+  cadmas_params P;
+  Geo g;
+  Prm p;
+  Fld f;
+  size_t N = 0, NB = 0;
+  int TI = 0, TJ = 0;
+  bool have_static = false;
+  // static
+  double *xx = nullptr, *yy = nullptr, *zz = nullptr;
+  double *ggv = nullptr, *ggx = nullptr, *ggy = nullptr, *ggz = nullptr;
+  double *glv = nullptr, *glx = nullptr, *gly = nullptr, *glz = nullptr, *cd0 = nullptr, *anu = nullptr;
+  int *indx = nullptr, *indy = nullptr, *indz = nullptr, *indb = nullptr;
+  // state (velocities and pressure double-buffered)
+  double *vel[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int cur = 0;
+  double *pbuf[2] = {nullptr, nullptr};
+  int pcur = 0;
+  double *ff = nullptr;
+  int *nf = nullptr, *indc = nullptr, *nf0 = nullptr, *nlim = nullptr;
+  double *bcu = nullptr, *bcv = nullptr, *bcw = nullptr, *bcp = nullptr, *bcf = nullptr;
+  // work: 9 flux arrays, reused as the Poisson system (0..7) and PT (8)
+  double *wk[9] = {nullptr};
+  // solver scratch
+  double *dd = nullptr, *xw = nullptr, *y2 = nullptr, *r0 = nullptr, *rr = nullptr, *pv = nullptr,
+         *ap = nullptr, *ae = nullptr, *tt = nullptr;
+  double *rb0 = nullptr, *rb1 = nullptr, *dres = nullptr;
+  SolveState *st = nullptr;
+  int *dint = nullptr;            // [0] err [1] nch [2] done [3] iter [4] nums
+  unsigned char *active = nullptr;
+  // pinned host mirrors
+  SolveState *h_st = nullptr;
+  int *h_int = nullptr;
+  double *h_res = nullptr;
+  // host-side scalars
+  std::vector<double> tbub;
+  std::vector<double> zz2;  // ZZ(2,K) on the host, K = 1..NK
+  std::vector<unsigned char> h_active;
+  double tnow = 0.0, dtnow = 0.0;
+  int nnow = 0;
+  cadmas_stats stats;
+  int last_iter = 8;   // iterations of the previous solve: size of the first batch
+  StageTimer tm;
+};
+
+#define TB(stage) h->tm.begin(h->s, (stage))
+#define TE() h->tm.end(h->s)
+
+static void refresh_fld(cadmas_handle *h) {
+  Fld &f = h->f;
+  f.ggv = h->ggv; f.ggx = h->ggx; f.ggy = h->ggy; f.ggz = h->ggz;
+  f.glv = h->glv; f.glx = h->glx; f.gly = h->gly; f.glz = h->glz;
+  f.cd0 = h->cd0; f.anu = h->anu;
+  f.indx = h->indx; f.indy = h->indy; f.indz = h->indz; f.indb = h->indb;
+  f.uu = h->vel[h->cur][0]; f.vv = h->vel[h->cur][1]; f.ww = h->vel[h->cur][2];
+  f.pp = h->pbuf[h->pcur];
+  f.ff = h->ff; f.nf = h->nf; f.indc = h->indc; f.nf0 = h->nf0;
+  f.bcu = h->bcu; f.bcv = h->bcv; f.bcw = h->bcw; f.bcp = h->bcp; f.bcf = h->bcf;
+}
+
+static void refresh_prm(cadmas_handle *h) {
+  const cadmas_params &P = h->P;
+  Prm &p = h->p;
+  p.rho0 = P.rho0; p.grz0 = P.grz0; p.vvmax = P.vvmax; p.cgpara = P.cgpara; p.cgepsa = P.cgepsa;
+  p.cgepsr = P.cgepsr; p.cgdiv = P.cgdiv; p.flower = P.flower; p.fupper = P.fupper;
+  p.plower = P.plower; p.scmvp = P.scmvp; p.wvlvl = P.wvlvl; p.wbub = P.wbub;
+  p.glxmin = P.glxmin; p.glxmax = P.glxmax; p.glymin = P.glymin; p.glymax = P.glymax;
+  p.dtnow = h->dtnow; p.tnow = h->tnow;
+  p.icgtyp = P.icgtyp; p.icgmax = P.icgmax; p.ibsuw0 = P.ibsuw0;
+  // sponge parameters of vf_veuler.f:77-113
+  p.ipa = 0;
+  for (int d = 0; d < 4; ++d) {
+    p.ip[d] = P.idamp[d];
+    p.sw[d] = p.spx[d] = p.spz[d] = 0.0;
+    if (p.ip[d] >= 0) {
+      p.ipa = p.ipa + 1;
+      double D = std::sqrt(P.grz0 / P.damp[d][3]);
+      p.sw[d] = P.damp[d][2];
+      p.spx[d] = (double)(p.ip[d] + 1) * P.damp[d][0] * D;
+      p.spz[d] = (double)(p.ip[d] + 1) * P.damp[d][1] * D;
+    }
+  }
+}
+
+static long long nrows(const cadmas_handle *h) { return (long long)h->g.NJ * h->g.NK; }
+
+// ------------------------------------------------------------ solver
+// VF_M1BCGS on the system a with initial guess/result x0.  The BiCGSTAB
+// scalars stay on the device; iterations are issued in batches and every
+// kernel returns at once after convergence, so results do not depend on
+// the batch size.  The host reads the scalars once per batch.
+static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc, int &iter,
+                 double &bnorm, double &xnorm) {
+  cudaStream_t s = h->s;
+  const Geo &g = h->g;
+  const size_t bytes = h->N * sizeof(double);
+  const double epsa2 = h->P.cgepsa * h->P.cgepsa, epsr2 = h->P.cgepsr * h->P.cgepsr,
+               div2 = h->P.cgdiv * h->P.cgdiv;
+  const int icgmax = h->P.icgmax;
+  const long long nr = nrows(h);
+  SolveState *st = h->st;
+  // vf_m1bcgs.f:79-95
+  CK(cudaMemcpyAsync(h->xw, x0, bytes, cudaMemcpyDeviceToDevice, s));
+  double *zero_list[] = {h->dd, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->tt};
+  for (double *z : zero_list) CK(cudaMemsetAsync(z, 0, bytes, s));
+  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
+  TB(CADMAS_STAGE_DCMP);
+  launch_dcmp(s, g, h->TI, h->TJ, U, a, indc, h->dd, &st->pivot_bad);
+  launch_pivot_check(s, st);
+  TE();
+  // YY = MINV*BB, BNORM = (YY,YY)
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, a.bb, nullptr, h->tt, st); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->y2, st); TE();
+  TB(CADMAS_STAGE_DOT);
+  launch_dot(s, g, indc, h->y2, h->y2, nullptr, nullptr, h->rb0, nullptr, st);
+  launch_fin(s, FIN_BNORM, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+  TE();
+  // YY = A*XW; YY = BB - YY; R0 = MINV*YY; S = (R0,R0)
+  TB(CADMAS_STAGE_VEC);
+  launch_spmv(s, g, a, indc, h->xw, h->y2, st);
+  launch_bmy(s, g, indc, a.bb, h->y2, st);
+  TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->y2, nullptr, h->tt, st); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->r0, st); TE();
+  TB(CADMAS_STAGE_DOT);
+  launch_dot(s, g, indc, h->r0, h->r0, nullptr, nullptr, h->rb0, nullptr, st);
+  launch_fin(s, FIN_START, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+  TE();
+  TB(CADMAS_STAGE_VEC); launch_copy2(s, g, indc, h->r0, h->rr, h->pv, st); TE();
+  // First batch as long as the previous solve; after that batches of 4.
+  int batch = std::max(2, std::min(h->last_iter, 64));
+  for (int guard = 0; guard < 100000; ++guard) {
+    for (int b = 0; b < batch; ++b) {
+      // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, nullptr, h->pv, h->tt, st); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->ap, st); TE();
+      TB(CADMAS_STAGE_DOT);
+      launch_dot(s, g, indc, h->r0, h->ap, nullptr, nullptr, h->rb0, nullptr, st);
+      launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      TE();
+      TB(CADMAS_STAGE_VEC); launch_axpy_rr(s, g, indc, h->ap, h->rr, st); TE();
+      // AE = MINV*(A*RR); OMEGA = (RR,AE)/(AE,AE)
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, nullptr, h->rr, h->tt, st); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->ae, st); TE();
+      TB(CADMAS_STAGE_DOT);
+      launch_dot(s, g, indc, h->rr, h->ae, h->ae, h->ae, h->rb0, h->rb1, st);
+      launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      TE();
+      // XW += ALPHA*PP + OMEGA*RR; RR -= OMEGA*AE; convergence; BETA
+      TB(CADMAS_STAGE_VEC);
+      launch_upd_xr(s, g, indc, h->pv, h->ae, h->r0, h->xw, h->rr, h->rb0, h->rb1, st);
+      launch_fin(s, FIN_CONV, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      launch_upd_p(s, g, indc, h->rr, h->ap, h->pv, st);
+      TE();
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_st, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_st->done) break;
+    batch = 4;
+  }
+  launch_x0(s, g, indc, h->xw, x0, st);
+  CK(cudaGetLastError());
+  const SolveState &hs = *h->h_st;
+  iter = hs.iter;
+  if (iter > 0) h->last_iter = iter;
+  if (iter == -1) { bnorm = 0.0; xnorm = 0.0; }
+  else { bnorm = std::sqrt(hs.bnorm); xnorm = std::sqrt(hs.xnorm); }
+  return CADMAS_OK;
+}
+
+static int map_iter(int iter, int icgmax) {
+  if (iter > icgmax) return CADMAS_ENOTCONV;
+  if (iter == -2) return CADMAS_EDIVERGE;
+  if (iter == -1) return CADMAS_EPIVOT;
+  return CADMAS_OK;
+}
+
+static int read_err(cadmas_handle *h, int &errbits) {
+  CK(cudaMemcpyAsync(h->h_int, h->dint, 5 * sizeof(int), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  errbits = h->h_int[0];
+  return CADMAS_OK;
+}
+static int map_err(int bits) {
+  if (bits & ERR_PG) return CADMAS_EPG;
+  if (bits & ERR_UNSUP) return CADMAS_EUNSUPPORTED;
+  if (bits & ERR_CAP) return CADMAS_ECAP;
+  return CADMAS_OK;
+}
+
+// VF_FNFINI: init pass then sweeps until no surface cell changes.
+static int fnfini(cadmas_handle *h) {
+  cudaStream_t s = h->s;
+  launch_fnf_init(s, h->g, h->f, h->p);
+  CK(cudaMemsetAsync(h->dint + 1, 0, 3 * sizeof(int), s));  // nch, done, iter
+  const int cap = 100000;
+  int batch = 2;
+  for (int guard = 0; guard < cap; guard += batch) {
+    for (int b = 0; b < batch; ++b)
+      launch_fnf_sweep(s, h->g, h->nf, h->dint + 1, h->dint + 2, h->dint + 3, cap, h->dint);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_int, h->dint, 5 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_int[2]) return CADMAS_OK;
+    batch = std::min(batch * 2, 16);
+  }
+  return CADMAS_ECAP;
+}
+
+static int bc_tail_v1(cadmas_handle *h) {
+  cudaStream_t s = h->s;
+  launch_bsuwt(s, h->g, h->f, h->p);
+  launch_bsuwt2(s, h->g, h->f);
+  launch_bsuwn(s, h->g, h->f);
+  launch_bwuwt(s, h->g, h->f);
+  launch_bwpp(s, h->g, h->f);
+  return CADMAS_OK;
+}
+
+static int do_v1cal(cadmas_handle *h) {
+  cudaStream_t s = h->s;
+  refresh_prm(h);
+  refresh_fld(h);
+  CK(cudaMemsetAsync(h->dint, 0, sizeof(int), s));
+  // fluxes, sources, provisional velocity (vf_v1cal.f:153-230)
+  TB(CADMAS_STAGE_FLUX); launch_flux(s, h->g, h->f, h->p, h->wk); TE();
+  const int nxt = h->cur ^ 1;
+  TB(CADMAS_STAGE_PREDICT);
+  launch_predict(s, h->g, h->f, h->p, h->wk, h->vel[nxt][0], h->vel[nxt][1], h->vel[nxt][2]);
+  TE();
+  h->cur = nxt;
+  refresh_fld(h);
+  // normal boundary velocities (vf_v1cal.f:251-254)
+  TB(CADMAS_STAGE_MODIF); launch_bwuwn(s, h->g, h->f, h->dint); TE();
+  // Poisson system (vf_v1cal.f:259-271)
+  SysPtr a{h->wk[0], h->wk[1], h->wk[2], h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[7]};
+  TB(CADMAS_STAGE_VPCOEF); launch_vpcoef(s, h->g, h->f, h->p, a, h->dint); TE();
+  // VF_VPSOL: PT = 0, solve (vf_vpsol.f:52-76)
+  double *PT = h->wk[8];
+  CK(cudaMemsetAsync(PT, 0, h->N * sizeof(double), s));
+  int iter;
+  double bn, xn;
+  int rc = solve(h, a, PT, h->indc, iter, bn, xn);
+  if (rc) return rc;
+  h->stats.icgitr = iter;
+  h->stats.cgbnrm = bn;
+  h->stats.cgxnrm = xn;
+  rc = map_iter(iter, h->P.icgmax);
+  if (rc) return rc;
+  if (h->P.diag_relres) {
+    launch_relres(s, h->g, a, h->indc, PT, h->rb0, h->rb1);
+    launch_fin(s, FIN_STORE, h->rb0, h->rb1, nrows(h), h->st, h->dres + 2, 0, 0, 0, 0);
+    CK(cudaMemcpyAsync(h->h_res, h->dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    h->stats.true_relres = h->h_res[3] > 0.0 ? std::sqrt(h->h_res[2]) / std::sqrt(h->h_res[3]) : 0.0;
+  }
+  // correction and boundary values (vf_v1cal.f:286-297)
+  TB(CADMAS_STAGE_MODIF);
+  launch_vmodif(s, h->g, h->f, h->p, PT);
+  bc_tail_v1(h);
+  TE();
+  CK(cudaGetLastError());
+  return CADMAS_OK;
+}
+
+static int do_f1cal(cadmas_handle *h) {
+  cudaStream_t s = h->s;
+  refresh_prm(h);
+  refresh_fld(h);
+  const Geo &g = h->g;
+  // fluxes and Euler update (vf_f1cal.f:124-163)
+  TB(CADMAS_STAGE_VOF);
+  launch_fconv(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
+  launch_feuler(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
+  // surface redistribution, cut-off and volume (vf_f1cal.f:185-188)
+  launch_fmod1(s, g, h->f, h->nlim);
+  launch_fcut(s, g, h->f, h->p, h->rb0, h->rb1);
+  launch_fin(s, FIN_STORE, h->rb0, h->rb1, nrows(h), h->st, h->dres, 0, 0, 0, 0);
+  TE();
+  // boundary values (vf_f1cal.f:192-194)
+  TB(CADMAS_STAGE_FBC);
+  launch_bwff(s, g, h->f, h->dint);
+  launch_bsuwn3(s, g, h->f, h->p);
+  launch_bsuwem(s, g, h->f, h->nlim);
+  TE();
+  // NF before the update (vf_f1cal.f:197-203)
+  CK(cudaMemcpyAsync(h->nf0, h->nf, h->N * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  // NF and INDC (vf_f1cal.f:207-219)
+  TB(CADMAS_STAGE_FLAGS);
+  int rc = fnfini(h);
+  if (rc) return rc;
+  if (h->P.wbub >= 1.0e-20) {
+    // VF_FBUBUP level timers (vf_fbubup.f:35-38, 49) on the host
+    bool any = false;
+    for (int K = h->g.NK - 2; K >= 2; --K) {
+      double DTBUB = h->zz2[K] / h->P.wbub;
+      h->h_active[K] = 0;
+      if (h->tnow - h->tbub[K - 1] > DTBUB) {
+        h->h_active[K] = 1;
+        any = true;
+        h->tbub[K - 1] = h->tbub[K - 1] + DTBUB;
+      }
+    }
+    if (any) {
+      CK(cudaMemcpyAsync(h->active, h->h_active.data(), h->h_active.size(), cudaMemcpyHostToDevice, s));
+      launch_fbubup(s, g, h->f, h->p, h->active);
+    }
+    rc = fnfini(h);
+    if (rc) return rc;
+  }
+  launch_fnfprv(s, g, h->f, h->dint);
+  CK(cudaMemsetAsync(h->dint + 4, 0, sizeof(int), s));
+  launch_cindc(s, g, h->f, h->dint + 4);
+  TE();
+  // gas-to-fluid pressure (vf_f1cal.f:230)
+  TB(CADMAS_STAGE_FBC);
+  const int pn = h->pcur ^ 1;
+  launch_bsppfl(s, g, h->f, h->pbuf[h->pcur], h->pbuf[pn]);
+  h->pcur = pn;
+  refresh_fld(h);
+  // boundary values (vf_f1cal.f:234-239)
+  launch_bsuwt(s, g, h->f, h->p);
+  launch_bsuwt2(s, g, h->f);
+  launch_bsuwn3(s, g, h->f, h->p);
+  launch_bspp(s, g, h->f);
+  launch_bwuwt(s, g, h->f);
+  launch_bwpp(s, g, h->f);
+  TE();
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_res, h->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  int bits;
+  rc = read_err(h, bits);
+  if (rc) return rc;
+  h->tm.resolve();
+  h->stats.fsum = h->h_res[0];
+  h->stats.fcut = h->h_res[1];
+  h->stats.nums = h->h_int[4];
+  return map_err(bits);
+}
+
+// ============================================================== C ABI
+extern "C" {
+
+const char *cadmas_strerror(int status) {
+  switch (status) {
+    case CADMAS_OK: return "ok";
+    case CADMAS_EINVAL: return "invalid argument";
+    case CADMAS_ECUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
+    case CADMAS_ENOTCONV: return "NOT CONVERGED. (Poisson solve reached ICGMAX)";
+    case CADMAS_EDIVERGE: return "INSTABILITY. (Poisson solve diverged)";
+    case CADMAS_EPIVOT: return "CAN NOT DECOMPOSITION. (non-positive MILU pivot)";
+    case CADMAS_EPG: return "P.G ERROR. (inconsistent cell flags)";
+    case CADMAS_ECAP: return "device iteration cap reached";
+    case CADMAS_ENOMEM: return "device allocation failed";
+    case CADMAS_EUNSUPPORTED: return "option outside the implemented path";
+    case CADMAS_ENOSTATIC: return "static fields not uploaded";
+    default: return "unknown status";
+  }
+}
+
+void cadmas_default_params(cadmas_params *p) {
+  std::memset(p, 0, sizeof(*p));
+  p->rho0 = 1.0e3; p->grz0 = 9.8; p->vvmax = 30.0;
+  p->cgpara = 0.95; p->cgepsa = 1.0e-15; p->cgepsr = 1.0e-12; p->cgdiv = 1.0e30;
+  p->flower = 1.0e-6; p->fupper = 1.0 - 1.0e-6; p->plower = 1.0e-4; p->scmvp = 1.0;
+  p->wvlvl = 0.0; p->wbub = 0.2;
+  for (int d = 0; d < 4; ++d) {
+    p->idamp[d] = -1;
+    p->damp[d][0] = 0.6; p->damp[d][1] = 0.6; p->damp[d][2] = 0.0; p->damp[d][3] = 0.0;
+  }
+  p->icgtyp = 1; p->icgmax = 500; p->ibsuw0 = 0;
+  p->precond_ti = 0; p->precond_tj = 0;
+}
+
+int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **out) {
+  if (!d || !p || !out) return CADMAS_EINVAL;
+  if (d->numi < 5 || d->numj < 3 || d->numk < 5 || d->numb < 0) return CADMAS_EINVAL;
+  const long long N = (long long)d->numi * d->numj * d->numk;
+  if (N > (1LL << 34)) return CADMAS_EINVAL;
+  int TI = p->precond_ti > 0 ? p->precond_ti : d->numi - 2;
+  int TJ = p->precond_tj > 0 ? p->precond_tj : d->numj - 2;
+  TI = std::min(TI, d->numi - 2);
+  TJ = std::min(TJ, d->numj - 2);
+  if (TI * TJ > 1024) {
+    g_last_error = "preconditioner block of more than 1024 columns; set precond_ti/precond_tj";
+    return CADMAS_EUNSUPPORTED;
+  }
+  cadmas_handle *h = new cadmas_handle();
+  h->P = *p;
+  h->TI = TI; h->TJ = TJ;
+  if (cudaGetDevice(&h->device) != cudaSuccess) { delete h; return CADMAS_ECUDA; }
+  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) { delete h; return CADMAS_ECUDA; }
+  h->N = (size_t)N;
+  h->NB = (size_t)std::max(d->numb, 1);
+  h->g.NI = d->numi; h->g.NJ = d->numj; h->g.NK = d->numk; h->g.NB = d->numb; h->g.N = N;
+  int rc = CADMAS_OK;
+#define AL(ptr, n) if (!rc) rc = dalloc(&(ptr), (n))
+  AL(h->xx, 6 * (size_t)d->numi); AL(h->yy, 6 * (size_t)d->numj); AL(h->zz, 6 * (size_t)d->numk);
+  AL(h->ggv, h->N); AL(h->ggx, h->N); AL(h->ggy, h->N); AL(h->ggz, h->N);
+  AL(h->glv, h->N); AL(h->glx, h->N); AL(h->gly, h->N); AL(h->glz, h->N);
+  AL(h->cd0, h->N); AL(h->anu, h->N);
+  AL(h->indx, h->N); AL(h->indy, h->N); AL(h->indz, h->N); AL(h->indb, 4 * h->NB);
+  for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) AL(h->vel[b][c], h->N);
+  AL(h->pbuf[0], h->N); AL(h->pbuf[1], h->N);
+  AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
+  AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
+  for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
+  AL(h->dd, h->N); AL(h->xw, h->N); AL(h->y2, h->N); AL(h->r0, h->N); AL(h->rr, h->N);
+  AL(h->pv, h->N); AL(h->ap, h->N); AL(h->ae, h->N); AL(h->tt, h->N);
+  AL(h->rb0, (size_t)nrows(h)); AL(h->rb1, (size_t)nrows(h)); AL(h->dres, 8);
+  AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
+#undef AL
+  if (!rc && cudaMallocHost((void **)&h->h_st, sizeof(SolveState)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMallocHost((void **)&h->h_int, 8 * sizeof(int)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMallocHost((void **)&h->h_res, 8 * sizeof(double)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (rc) { cadmas_destroy(h); return rc; }
+  // NF starts as all obstacle until set_state; INDC as non-computed.
+  cudaMemset(h->nf, 0xff, h->N * sizeof(int));
+  cudaMemset(h->indc, 0xff, h->N * sizeof(int));
+  h->tbub.assign(d->numk, 0.0);
+  h->h_active.assign(d->numk + 1, 0);
+  std::memset(&h->stats, 0, sizeof(h->stats));
+  h->stats.true_relres = -1.0;
+  h->g.XX = h->xx; h->g.YY = h->yy; h->g.ZZ = h->zz;
+  refresh_prm(h);
+  refresh_fld(h);
+  *out = h;
+  return CADMAS_OK;
+}
+
+int cadmas_destroy(cadmas_handle *h) {
+  if (!h) return CADMAS_OK;
+  cudaStreamSynchronize(h->s);
+  double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
+                  h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
+                  h->dd, h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->tt, h->rb0, h->rb1, h->dres};
+  for (double *q : dl) if (q) cudaFree(q);
+  for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) if (h->vel[b][c]) cudaFree(h->vel[b][c]);
+  for (double *q : h->wk) if (q) cudaFree(q);
+  int *il[] = {h->indx, h->indy, h->indz, h->indb, h->nf, h->indc, h->nf0, h->nlim, h->dint};
+  for (int *q : il) if (q) cudaFree(q);
+  if (h->st) cudaFree(h->st);
+  if (h->active) cudaFree(h->active);
+  if (h->h_st) cudaFreeHost(h->h_st);
+  if (h->h_int) cudaFreeHost(h->h_int);
+  if (h->h_res) cudaFreeHost(h->h_res);
+  if (h->s) cudaStreamDestroy(h->s);
+  delete h;
+  return CADMAS_OK;
+}
+
+int cadmas_upload_static(cadmas_handle *h, const cadmas_static *st) {
+  if (!h || !st) return CADMAS_EINVAL;
+  const double *req[] = {st->xx, st->yy, st->zz, st->ggv, st->ggx, st->ggy, st->ggz, st->glv,
+                         st->glx, st->gly, st->glz, st->cd0, st->anu};
+  for (const double *q : req) if (!q) return CADMAS_EINVAL;
+  if (!st->indx || !st->indy || !st->indz || (h->g.NB > 0 && !st->indb)) return CADMAS_EINVAL;
+  cudaStream_t s = h->s;
+  const size_t b8 = h->N * sizeof(double), b4 = h->N * sizeof(int);
+  CK(cudaMemcpyAsync(h->xx, st->xx, 6 * h->g.NI * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->yy, st->yy, 6 * h->g.NJ * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->zz, st->zz, 6 * h->g.NK * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->ggv, st->ggv, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->ggx, st->ggx, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->ggy, st->ggy, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->ggz, st->ggz, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->glv, st->glv, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->glx, st->glx, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->gly, st->gly, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->glz, st->glz, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->cd0, st->cd0, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->anu, st->anu, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->indx, st->indx, b4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->indy, st->indy, b4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->indz, st->indz, b4, cudaMemcpyHostToDevice, s));
+  if (h->g.NB > 0) CK(cudaMemcpyAsync(h->indb, st->indb, 4 * h->g.NB * sizeof(int), cudaMemcpyHostToDevice, s));
+  // host copy of ZZ(2,K) for the bubble timers
+  h->zz2.assign(h->g.NK + 1, 0.0);
+  std::vector<double> zz(6 * h->g.NK);
+  std::memcpy(zz.data(), st->zz, zz.size() * sizeof(double));
+  for (int k = 1; k <= h->g.NK; ++k) h->zz2[k] = zz[1 + 6 * (k - 1)];
+  CK(cudaStreamSynchronize(s));
+  h->have_static = true;
+  return CADMAS_OK;
+}
+
+int cadmas_set_state(cadmas_handle *h, const cadmas_state *st) {
+  if (!h || !st) return CADMAS_EINVAL;
+  cudaStream_t s = h->s;
+  const size_t b8 = h->N * sizeof(double), b4 = h->N * sizeof(int), bb = (size_t)h->g.NB * sizeof(double);
+  refresh_fld(h);
+  if (st->uu) CK(cudaMemcpyAsync(h->f.uu, st->uu, b8, cudaMemcpyHostToDevice, s));
+  if (st->vv) CK(cudaMemcpyAsync(h->f.vv, st->vv, b8, cudaMemcpyHostToDevice, s));
+  if (st->ww) CK(cudaMemcpyAsync(h->f.ww, st->ww, b8, cudaMemcpyHostToDevice, s));
+  if (st->pp) CK(cudaMemcpyAsync(h->f.pp, st->pp, b8, cudaMemcpyHostToDevice, s));
+  if (st->ff) CK(cudaMemcpyAsync(h->ff, st->ff, b8, cudaMemcpyHostToDevice, s));
+  if (st->nf) CK(cudaMemcpyAsync(h->nf, st->nf, b4, cudaMemcpyHostToDevice, s));
+  if (st->indc) CK(cudaMemcpyAsync(h->indc, st->indc, b4, cudaMemcpyHostToDevice, s));
+  if (bb) {
+    if (st->bcu) CK(cudaMemcpyAsync(h->bcu, st->bcu, bb, cudaMemcpyHostToDevice, s));
+    if (st->bcv) CK(cudaMemcpyAsync(h->bcv, st->bcv, bb, cudaMemcpyHostToDevice, s));
+    if (st->bcw) CK(cudaMemcpyAsync(h->bcw, st->bcw, bb, cudaMemcpyHostToDevice, s));
+    if (st->bcp) CK(cudaMemcpyAsync(h->bcp, st->bcp, bb, cudaMemcpyHostToDevice, s));
+    if (st->bcf) CK(cudaMemcpyAsync(h->bcf, st->bcf, bb, cudaMemcpyHostToDevice, s));
+  }
+  if (st->tbub) std::memcpy(h->tbub.data(), st->tbub, h->g.NK * sizeof(double));
+  h->tnow = st->tnow;
+  h->nnow = st->nnow;
+  CK(cudaStreamSynchronize(s));
+  return CADMAS_OK;
+}
+
+int cadmas_get_state(cadmas_handle *h, cadmas_state *st) {
+  if (!h || !st) return CADMAS_EINVAL;
+  cudaStream_t s = h->s;
+  const size_t b8 = h->N * sizeof(double), b4 = h->N * sizeof(int), bb = (size_t)h->g.NB * sizeof(double);
+  refresh_fld(h);
+  if (st->uu) CK(cudaMemcpyAsync(st->uu, h->f.uu, b8, cudaMemcpyDeviceToHost, s));
+  if (st->vv) CK(cudaMemcpyAsync(st->vv, h->f.vv, b8, cudaMemcpyDeviceToHost, s));
+  if (st->ww) CK(cudaMemcpyAsync(st->ww, h->f.ww, b8, cudaMemcpyDeviceToHost, s));
+  if (st->pp) CK(cudaMemcpyAsync(st->pp, h->f.pp, b8, cudaMemcpyDeviceToHost, s));
+  if (st->ff) CK(cudaMemcpyAsync(st->ff, h->ff, b8, cudaMemcpyDeviceToHost, s));
+  if (st->nf) CK(cudaMemcpyAsync(st->nf, h->nf, b4, cudaMemcpyDeviceToHost, s));
+  if (st->indc) CK(cudaMemcpyAsync(st->indc, h->indc, b4, cudaMemcpyDeviceToHost, s));
+  if (bb) {
+    if (st->bcu) CK(cudaMemcpyAsync(st->bcu, h->bcu, bb, cudaMemcpyDeviceToHost, s));
+    if (st->bcv) CK(cudaMemcpyAsync(st->bcv, h->bcv, bb, cudaMemcpyDeviceToHost, s));
+    if (st->bcw) CK(cudaMemcpyAsync(st->bcw, h->bcw, bb, cudaMemcpyDeviceToHost, s));
+    if (st->bcp) CK(cudaMemcpyAsync(st->bcp, h->bcp, bb, cudaMemcpyDeviceToHost, s));
+    if (st->bcf) CK(cudaMemcpyAsync(st->bcf, h->bcf, bb, cudaMemcpyDeviceToHost, s));
+  }
+  if (st->tbub) std::memcpy(st->tbub, h->tbub.data(), h->g.NK * sizeof(double));
+  st->tnow = h->tnow;
+  st->nnow = h->nnow;
+  CK(cudaStreamSynchronize(s));
+  return CADMAS_OK;
+}
+
+int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
+  if (!h) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  cudaStream_t s = h->s;
+  refresh_prm(h);
+  refresh_fld(h);
+  CK(cudaMemsetAsync(h->dint, 0, 8 * sizeof(int), s));
+  // vf_cinit.f:202-207
+  launch_fcut(s, h->g, h->f, h->p, h->rb0, h->rb1);
+  launch_fin(s, FIN_STORE, h->rb0, h->rb1, nrows(h), h->st, h->dres, 0, 0, 0, 0);
+  launch_bwff(s, h->g, h->f, h->dint);
+  int rc = fnfini(h);
+  if (rc) return rc;
+  launch_fnfprv(s, h->g, h->f, h->dint);
+  CK(cudaMemsetAsync(h->indc, 0xff, h->N * sizeof(int), s));
+  CK(cudaMemsetAsync(h->dint + 4, 0, sizeof(int), s));
+  launch_cindc(s, h->g, h->f, h->dint + 4);
+  if (hydrostatic) {
+    // p = RHO0*GRZ0*(WVLVL - z_c) on INDC != -1 (vf_cinit.f:273-285)
+    std::vector<double> pp(h->N, 0.0);
+    std::vector<int> indc(h->N);
+    std::vector<double> zz(6 * h->g.NK);
+    CK(cudaMemcpyAsync(indc.data(), h->indc, h->N * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(zz.data(), h->zz, zz.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int NI = h->g.NI, NJ = h->g.NJ, NK = h->g.NK;
+    for (int K = 2; K <= NK - 1; ++K) {
+      double VAL = h->P.rho0 * h->P.grz0 * (h->P.wvlvl - (zz[6 * (K - 1)] + zz[6 * K]) * 0.5);
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = (size_t)(I - 1) + (size_t)NI * ((size_t)(J - 1) + (size_t)NJ * (K - 1));
+          if (indc[c] != -1) pp[c] = VAL;
+        }
+    }
+    CK(cudaMemcpyAsync(h->f.pp, pp.data(), h->N * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  // vf_cinit.f:388-394
+  launch_bwuwn(s, h->g, h->f, h->dint);
+  launch_bsuwt(s, h->g, h->f, h->p);
+  launch_bsuwt2(s, h->g, h->f);
+  launch_bsuwn3(s, h->g, h->f, h->p);
+  launch_bspp(s, h->g, h->f);
+  launch_bwuwt(s, h->g, h->f);
+  launch_bwpp(s, h->g, h->f);
+  std::fill(h->tbub.begin(), h->tbub.end(), 0.0);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_res, h->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  int bits;
+  rc = read_err(h, bits);
+  if (rc) return rc;
+  h->stats.fsum = h->h_res[0];
+  h->stats.fcut = h->h_res[1];
+  h->stats.nums = h->h_int[4];
+  return map_err(bits);
+}
+
+int cadmas_set_time(cadmas_handle *h, double tnow, double dtnow, int nnow) {
+  if (!h) return CADMAS_EINVAL;
+  h->tnow = tnow; h->dtnow = dtnow; h->nnow = nnow;
+  return CADMAS_OK;
+}
+
+int cadmas_v1cal(cadmas_handle *h) {
+  if (!h) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  int rc = do_v1cal(h);
+  if (rc == CADMAS_OK) {
+    int bits;
+    rc = read_err(h, bits);
+    if (rc == CADMAS_OK) rc = map_err(bits);
+  }
+  h->stats.last_status = rc;
+  return rc;
+}
+
+int cadmas_f1cal(cadmas_handle *h) {
+  if (!h) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  int rc = do_f1cal(h);
+  h->stats.last_status = rc;
+  return rc;
+}
+
+int cadmas_step(cadmas_handle *h, double dt) {
+  if (!h) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  if (!(dt > 0.0)) return CADMAS_EINVAL;
+  // vf_a1main.f:1029-1047 with LOOPS = 1
+  h->dtnow = dt;
+  h->nnow = h->nnow + 1;
+  h->tnow = h->tnow + h->dtnow;
+  int rc = cadmas_v1cal(h);
+  if (rc == CADMAS_OK) rc = cadmas_f1cal(h);
+  h->stats.last_status = rc;
+  return rc;
+}
+
+int cadmas_divnorm(cadmas_handle *h, double *val) {
+  if (!h || !val) return CADMAS_EINVAL;
+  refresh_fld(h);
+  launch_cdiv(h->s, h->g, h->f, h->rb0);
+  launch_fin(h->s, FIN_STORE, h->rb0, h->rb0, nrows(h), h->st, h->dres + 4, 0, 0, 0, 0);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_res, h->dres, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  *val = std::sqrt(h->h_res[4]);
+  h->stats.divnorm = *val;
+  return CADMAS_OK;
+}
+
+int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st) {
+  if (!h || !st) return CADMAS_EINVAL;
+  *st = h->stats;
+  return CADMAS_OK;
+}
+
+int cadmas_get_stream(cadmas_handle *h, void **stream) {
+  if (!h || !stream) return CADMAS_EINVAL;
+  *stream = (void *)h->s;
+  return CADMAS_OK;
+}
+
+long long cadmas_kernel_launches(void) { return g_kernel_launches.load(); }
+
+int cadmas_stage_timers(cadmas_handle *h, int enable, double *ms, long long *count, int n) {
+  if (!h || n < 0 || n > CADMAS_NSTAGES) return CADMAS_EINVAL;
+  CK(cudaStreamSynchronize(h->s));
+  h->tm.resolve();
+  for (int i = 0; i < n; ++i) {
+    if (ms) ms[i] = h->tm.ms[i];
+    if (count) count[i] = h->tm.cnt[i];
+  }
+  if (enable >= 0) {
+    h->tm.clear();
+    h->tm.on = (enable != 0);
+  }
+  return CADMAS_OK;
+}
+
+int cadmas_sync(cadmas_handle *h) {
+  if (!h) return CADMAS_EINVAL;
+  CK(cudaStreamSynchronize(h->s));
+  return CADMAS_OK;
+}
+
+int vf_step_gpu_(cadmas_handle **hp, const double *dtnow, double *uu, double *vv, double *ww,
+                 double *pp, double *ff, int *nf, int *indc, double *bcu, double *bcv, double *bcw,
+                 double *bcp, double *bcf, double *tnow, int *nnow) {
+  if (!hp || !*hp || !dtnow || !tnow || !nnow) return CADMAS_EINVAL;
+  cadmas_handle *h = *hp;
+  cadmas_state s{uu, vv, ww, pp, ff, nf, indc, bcu, bcv, bcw, bcp, bcf, nullptr, *tnow, *nnow};
+  int rc = cadmas_set_state(h, &s);
+  if (rc) return rc;
+  rc = cadmas_step(h, *dtnow);
+  int rc2 = cadmas_get_state(h, &s);
+  *tnow = s.tnow;
+  *nnow = s.nnow;
+  return rc ? rc : rc2;
+}
+
+int cadmas_m1bcgs_dev(cadmas_handle *h, const double *ad, const double *ali, const double *alj,
+                      const double *alk, const double *aui, const double *auj, const double *auk,
+                      const double *bb, double *x0, const int *indc, int *iter, double *bnorm,
+                      double *xnorm) {
+  if (!h || !ad || !ali || !alj || !alk || !aui || !auj || !auk || !bb || !x0 || !indc || !iter ||
+      !bnorm || !xnorm)
+    return CADMAS_EINVAL;
+  SysPtr a{const_cast<double *>(ad), const_cast<double *>(ali), const_cast<double *>(alj),
+           const_cast<double *>(alk), const_cast<double *>(aui), const_cast<double *>(auj),
+           const_cast<double *>(auk), const_cast<double *>(bb)};
+  int it;
+  double bn, xn;
+  int rc = solve(h, a, x0, indc, it, bn, xn);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->s));
+  *iter = it; *bnorm = bn; *xnorm = xn;
+  return CADMAS_OK;
+}
+
+}  // extern "C"

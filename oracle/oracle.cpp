@@ -1,0 +1,2168 @@
+// oracle.cpp -- CPU restatement of the CADMAS-SURF/3D SMAC step.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle.h).  Every routine restates the
+// Fortran routine it is named after, loop for loop and in the Fortran
+// evaluation order (left to right, parentheses kept), from
+//   Simulators/CADMAS-SURF-3D/Source code/<file>.f
+// Built with -O2 -ffp-contract=off so that no fused multiply-add changes a
+// rounding.  Loops run on the serial (NPROCS=1) index ranges: MYIS=2,
+// MYIE=NUMI-1, MYJS=2, MYJE=NUMJ-1, MYMIS=MYMIE=MYMJS=MYMJE=1
+// (vf_cpara.f:80-98).  Options outside the configurations exercised here
+// (k-epsilon, temperature, scalars, wave-source terms ISCTYP, time-dependent
+// porosity IPRNT>1, air-pressure model PVCP0, matrix wave data MTBTYP=3,
+// log-law walls, droplet fall IDROP) are not restated and are rejected.
+#include "oracle.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+namespace {
+
+typedef std::vector<double> vd;
+typedef std::vector<int> vi;
+
+struct Timer {
+  std::chrono::steady_clock::time_point t0;
+  void start() { t0 = std::chrono::steady_clock::now(); }
+  double stop() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+// gfortran's integer power (libgfortran pow_r8_i4: square and multiply).
+static double ipow(double x, int n) {
+  double pow = 1.0;
+  if (n != 0) {
+    unsigned u;
+    if (n < 0) { u = (unsigned)(-n); x = pow / x; } else { u = (unsigned)n; }
+    for (;;) {
+      if (u & 1u) pow *= x;
+      u >>= 1;
+      if (u) x *= x; else break;
+    }
+  }
+  return pow;
+}
+
+// MAX/MIN with the comparison the GPU kernels use (first operand on ties).
+static inline double dmax(double a, double b) { return (a < b) ? b : a; }
+static inline double dmin(double a, double b) { return (b < a) ? b : a; }
+
+// Warp tree of the GPU reduction: lane 0 after shfl_down by 16,8,4,2,1.
+static double warp_tree(double *s) {
+  for (int off = 16; off >= 1; off >>= 1)
+    for (int l = 0; l < off; ++l) s[l] = s[l] + s[l + off];
+  return s[0];
+}
+
+}  // namespace
+
+struct orc_handle {
+  int NI, NJ, NK, NB;
+  cadmas_params P;
+  int sum_mode;
+  // static
+  vd XX, YY, ZZ, GGV, GGX, GGY, GGZ, GLV, GLX, GLY, GLZ, CD0, ANU;
+  vi INDX, INDY, INDZ, INDB;
+  bool have_static = false;
+  // state
+  vd UU, VV, WW, PP, FF, BCU, BCV, BCW, BCP, BCF, TBUB;
+  vi NF, INDC, INDS, NLIM;
+  int NUMS = 0;
+  double TNOW = 0, DTNOW = 0;
+  int NNOW = 0;
+  // work arrays WK01..WK17
+  vd WK[18];
+  // solver scratch
+  vd DD, XW, Y2, R0, RR, PPv, AP, AE;
+  cadmas_stats st;
+  double tmr[5];
+
+  // ---------------------------------------------------------------- helpers
+  inline size_t id(int i, int j, int k) const {
+    return (size_t)(i - 1) + (size_t)NI * ((size_t)(j - 1) + (size_t)NJ * (size_t)(k - 1));
+  }
+  inline double X_(int m, int i) const { return XX[(m - 1) + 6 * (i - 1)]; }
+  inline double Y_(int m, int j) const { return YY[(m - 1) + 6 * (j - 1)]; }
+  inline double Z_(int m, int k) const { return ZZ[(m - 1) + 6 * (k - 1)]; }
+  inline int IB_(int m, int l) const { return INDB[(m - 1) + 4 * (l - 1)]; }
+  void decode(int ijk, int &i, int &j, int &k) const {
+    k = (ijk - 1) / (NI * NJ) + 1;
+    ijk = ijk - NI * NJ * (k - 1);
+    j = (ijk - 1) / NI + 1;
+    i = ijk - NI * (j - 1);
+  }
+
+  // Global sum over cells of a masked contribution.  f(i,j,k,&c) returns
+  // true when the cell contributes c.  The reference order loops K=2..NK-1,
+  // J=2..NJ-1, I=2..NI-1 (e.g. vf_mzip.f:36-43); the GPU order is the row
+  // tree described in oracle.h.  Cells outside the interior never
+  // contribute in either order (their masks are false).
+  template <class F> double gsum(F f) const {
+    if (sum_mode == ORC_SUM_REF) {
+      double s = 0.0, c;
+      for (int k = 2; k <= NK - 1; ++k)
+        for (int j = 2; j <= NJ - 1; ++j)
+          for (int i = 2; i <= NI - 1; ++i)
+            if (f(i, j, k, c)) s = s + c;
+      return s;
+    }
+    const int NR = NJ * NK;
+    std::vector<double> R(NR);
+    double lane[32];
+    for (int r = 0; r < NR; ++r) {
+      int j = r % NJ + 1, k = r / NJ + 1;
+      for (int l = 0; l < 32; ++l) {
+        double s = 0.0, c;
+        for (int i0 = l; i0 < NI; i0 += 32)
+          if (f(i0 + 1, j, k, c)) s = s + c;
+        lane[l] = s;
+      }
+      R[r] = warp_tree(lane);
+    }
+    double u[1024];
+    for (int t = 0; t < 1024; ++t) {
+      double s = 0.0;
+      for (int r = t; r < NR; r += 1024) s = s + R[r];
+      u[t] = s;
+    }
+    double w[32];
+    for (int q = 0; q < 32; ++q) w[q] = warp_tree(u + 32 * q);
+    return warp_tree(w);
+  }
+
+  // interior mask helper used by gsum callers
+  inline bool interior(int i, int j, int k) const {
+    return i >= 2 && i <= NI - 1 && j >= 2 && j <= NJ - 1 && k >= 2 && k <= NK - 1;
+  }
+
+  // ======================================================================
+  // Momentum fluxes  VF_VFLXDU  vf_vflxdu.f:62-347
+  void vflxdu(vd &FLUU, vd &FLUV, vd &FLUW) {
+    const double SU = P.scmvp, SC = 1.0 - P.scmvp;
+    const int LA = 3, LB = NI - 1;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = LA - 1; I <= LB; ++I) {
+          if (INDC[id(I, J, K)] == -1) continue;
+          double WIN = (GLX[id(I, J, K)] * UU[id(I, J, K)] + GLX[id(I + 1, J, K)] * UU[id(I + 1, J, K)]) * 0.5;
+          double FG = WIN * (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5;
+          double &F = FLUU[id(I, J, K)];
+          F = F - SU * (dmax(WIN, 0.0) * UU[id(I, J, K)] - dmax(-WIN, 0.0) * UU[id(I + 1, J, K)]) - SC * FG;
+          F = F + (GGX[id(I, J, K)] + GGX[id(I + 1, J, K)]) * ANU[id(I, J, K)] * X_(4, I) *
+                      (UU[id(I + 1, J, K)] - UU[id(I, J, K)]);
+        }
+    // (Gy*v)*u  :93-213
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = LA; I <= LB; ++I) {
+          int IC = NF[id(I - 1, J - 1, K)] * NF[id(I, J - 1, K)] * NF[id(I - 1, J, K)] * NF[id(I, J, K)];
+          int IT = INDX[id(I, J, K)], IBt = INDX[id(I, J - 1, K)];
+          double &F = FLUV[id(I, J, K)];
+          if (IC != 0 || (IT != 0 && IBt != 0)) {
+          } else if (IT == 0 && IBt == 0) {
+            double WIN = X_(6, I) * (X_(2, I - 1) * GLY[id(I, J, K)] * VV[id(I, J, K)] +
+                                     X_(2, I) * GLY[id(I - 1, J, K)] * VV[id(I - 1, J, K)]);
+            double FG = WIN * Y_(6, J) * (Y_(2, J - 1) * UU[id(I, J, K)] + Y_(2, J) * UU[id(I, J - 1, K)]);
+            F = F - SU * (dmax(WIN, 0.0) * UU[id(I, J - 1, K)] - dmax(-WIN, 0.0) * UU[id(I, J, K)]) - SC * FG;
+            double GG = X_(6, I) * (X_(2, I - 1) * GGY[id(I, J, K)] + X_(2, I) * GGY[id(I - 1, J, K)]);
+            double ANR = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I, J, K)] + Y_(2, J) * ANU[id(I, J - 1, K)]);
+            double ANL = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I - 1, J, K)] + Y_(2, J) * ANU[id(I - 1, J - 1, K)]);
+            double AN = X_(6, I) * (X_(2, I - 1) * ANR + X_(2, I) * ANL);
+            double D1 = Y_(5, J) * (UU[id(I, J, K)] - UU[id(I, J - 1, K)]);
+            double D2 = X_(5, I) * (VV[id(I, J, K)] - VV[id(I - 1, J, K)]);
+            F = F + GG * AN * (D1 + D2);
+          } else {
+            double BR, BL;
+            int IS = INDY[id(I, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BR = (IB_(2, IS) == 3) ? UU[id(I, J, K)] : UU[id(I, J - 1, K)];
+              else BR = BCU[IS - 1];
+            } else {
+              BR = Y_(6, J) * (Y_(2, J - 1) * (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) +
+                               Y_(2, J) * (UU[id(I, J - 1, K)] + UU[id(I + 1, J - 1, K)])) * 0.5;
+            }
+            IS = INDY[id(I - 1, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BL = (IB_(2, IS) == 3) ? UU[id(I, J, K)] : UU[id(I, J - 1, K)];
+              else BL = BCU[IS - 1];
+            } else {
+              BL = Y_(6, J) * (Y_(2, J - 1) * (UU[id(I, J, K)] + UU[id(I - 1, J, K)]) +
+                               Y_(2, J) * (UU[id(I, J - 1, K)] + UU[id(I - 1, J - 1, K)])) * 0.5;
+            }
+            double WIN = X_(6, I) * (X_(2, I - 1) * GLY[id(I, J, K)] * VV[id(I, J, K)] +
+                                     X_(2, I) * GLY[id(I - 1, J, K)] * VV[id(I - 1, J, K)]);
+            double FG = X_(6, I) * (X_(2, I) * GLY[id(I, J, K)] * VV[id(I, J, K)] * BR +
+                                    X_(2, I - 1) * GLY[id(I - 1, J, K)] * VV[id(I - 1, J, K)] * BL);
+            if (IT == 0 && WIN < 0.0) F = F - SU * WIN * UU[id(I, J, K)] - SC * FG;
+            else if (IBt == 0 && WIN > 0.0) F = F - SU * WIN * UU[id(I, J - 1, K)] - SC * FG;
+            else F = F - FG;
+            double GG = X_(6, I) * (X_(2, I - 1) * GGY[id(I, J, K)] + X_(2, I) * GGY[id(I - 1, J, K)]);
+            FG = X_(6, I) * (X_(2, I) * BR + X_(2, I - 1) * BL);
+            double ANR, ANL;
+            if (NF[id(I, J, K)] == -1) ANR = ANU[id(I, J - 1, K)];
+            else if (NF[id(I, J - 1, K)] == -1) ANR = ANU[id(I, J, K)];
+            else ANR = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I, J, K)] + Y_(2, J) * ANU[id(I, J - 1, K)]);
+            if (NF[id(I - 1, J, K)] == -1) ANL = ANU[id(I - 1, J - 1, K)];
+            else if (NF[id(I - 1, J - 1, K)] == -1) ANL = ANU[id(I - 1, J, K)];
+            else ANL = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I - 1, J, K)] + Y_(2, J) * ANU[id(I - 1, J - 1, K)]);
+            double AN = X_(6, I) * (X_(2, I - 1) * ANR + X_(2, I) * ANL);
+            double D1 = (IT == 0) ? Y_(4, J) * (UU[id(I, J, K)] - FG) * 2.0
+                                  : Y_(4, J - 1) * (FG - UU[id(I, J - 1, K)]) * 2.0;
+            double D2 = X_(5, I) * (VV[id(I, J, K)] - VV[id(I - 1, J, K)]);
+            F = F + GG * AN * (D1 + D2);
+          }
+        }
+    // (Gz*w)*u  :215-345
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = LA; I <= LB; ++I) {
+          int IC = NF[id(I - 1, J, K - 1)] * NF[id(I, J, K - 1)] * NF[id(I - 1, J, K)] * NF[id(I, J, K)];
+          int IT = INDX[id(I, J, K)], IBt = INDX[id(I, J, K - 1)];
+          double &F = FLUW[id(I, J, K)];
+          if (IC != 0 || (IT != 0 && IBt != 0)) {
+          } else if (IT == 0 && IBt == 0) {
+            double WIN = X_(6, I) * (X_(2, I - 1) * GLZ[id(I, J, K)] * WW[id(I, J, K)] +
+                                     X_(2, I) * GLZ[id(I - 1, J, K)] * WW[id(I - 1, J, K)]);
+            double FG = WIN * Z_(6, K) * (Z_(2, K - 1) * UU[id(I, J, K)] + Z_(2, K) * UU[id(I, J, K - 1)]);
+            F = F - SU * (dmax(WIN, 0.0) * UU[id(I, J, K - 1)] - dmax(-WIN, 0.0) * UU[id(I, J, K)]) - SC * FG;
+            double GG = X_(6, I) * (X_(2, I - 1) * GGZ[id(I, J, K)] + X_(2, I) * GGZ[id(I - 1, J, K)]);
+            double ANR = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I, J, K)] + Z_(2, K) * ANU[id(I, J, K - 1)]);
+            double ANL = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I - 1, J, K)] + Z_(2, K) * ANU[id(I - 1, J, K - 1)]);
+            double AN = X_(6, I) * (X_(2, I - 1) * ANR + X_(2, I) * ANL);
+            double D1 = Z_(5, K) * (UU[id(I, J, K)] - UU[id(I, J, K - 1)]);
+            double D2 = X_(5, I) * (WW[id(I, J, K)] - WW[id(I - 1, J, K)]);
+            F = F + GG * AN * (D1 + D2);
+          } else {
+            double BR, BL;
+            int IS = INDZ[id(I, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BR = (IB_(2, IS) == 5) ? UU[id(I, J, K)] : UU[id(I, J, K - 1)];
+              else BR = BCU[IS - 1];
+            } else {
+              BR = Z_(6, K) * (Z_(2, K - 1) * (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) +
+                               Z_(2, K) * (UU[id(I, J, K - 1)] + UU[id(I + 1, J, K - 1)])) * 0.5;
+            }
+            IS = INDZ[id(I - 1, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BL = (IB_(2, IS) == 5) ? UU[id(I, J, K)] : UU[id(I, J, K - 1)];
+              else BL = BCU[IS - 1];
+            } else {
+              BL = Z_(6, K) * (Z_(2, K - 1) * (UU[id(I, J, K)] + UU[id(I - 1, J, K)]) +
+                               Z_(2, K) * (UU[id(I, J, K - 1)] + UU[id(I - 1, J, K - 1)])) * 0.5;
+            }
+            double WIN = X_(6, I) * (X_(2, I - 1) * GLZ[id(I, J, K)] * WW[id(I, J, K)] +
+                                     X_(2, I) * GLZ[id(I - 1, J, K)] * WW[id(I - 1, J, K)]);
+            double FG = X_(6, I) * (X_(2, I) * GLZ[id(I, J, K)] * WW[id(I, J, K)] * BR +
+                                    X_(2, I - 1) * GLZ[id(I - 1, J, K)] * WW[id(I - 1, J, K)] * BL);
+            if (IT == 0 && WIN < 0.0) F = F - SU * WIN * UU[id(I, J, K)] - SC * FG;
+            else if (IBt == 0 && WIN > 0.0) F = F - SU * WIN * UU[id(I, J, K - 1)] - SC * FG;
+            else F = F - FG;
+            double GG = X_(6, I) * (X_(2, I - 1) * GGZ[id(I, J, K)] + X_(2, I) * GGZ[id(I - 1, J, K)]);
+            FG = X_(6, I) * (X_(2, I) * BR + X_(2, I - 1) * BL);
+            double ANR, ANL;
+            if (NF[id(I, J, K)] == -1) ANR = ANU[id(I, J, K - 1)];
+            else if (NF[id(I, J, K - 1)] == -1) ANR = ANU[id(I, J, K)];
+            else ANR = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I, J, K)] + Z_(2, K) * ANU[id(I, J, K - 1)]);
+            if (NF[id(I - 1, J, K)] == -1) ANL = ANU[id(I - 1, J, K - 1)];
+            else if (NF[id(I - 1, J, K - 1)] == -1) ANL = ANU[id(I - 1, J, K)];
+            else ANL = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I - 1, J, K)] + Z_(2, K) * ANU[id(I - 1, J, K - 1)]);
+            double AN = X_(6, I) * (X_(2, I - 1) * ANR + X_(2, I) * ANL);
+            double D1 = (IT == 0) ? Z_(4, K) * (UU[id(I, J, K)] - FG) * 2.0
+                                  : Z_(4, K - 1) * (FG - UU[id(I, J, K - 1)]) * 2.0;
+            double D2 = X_(5, I) * (WW[id(I, J, K)] - WW[id(I - 1, J, K)]);
+            F = F + GG * AN * (D1 + D2);
+          }
+        }
+  }
+
+  // VF_VFLXDV  vf_vflxdv.f:62-347
+  void vflxdv(vd &FLVU, vd &FLVV, vd &FLVW) {
+    const double SU = P.scmvp, SC = 1.0 - P.scmvp;
+    const int LA = 3, LB = NJ - 1;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = LA - 1; J <= LB; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (INDC[id(I, J, K)] == -1) continue;
+          double WIN = (GLY[id(I, J, K)] * VV[id(I, J, K)] + GLY[id(I, J + 1, K)] * VV[id(I, J + 1, K)]) * 0.5;
+          double FG = WIN * (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5;
+          double &F = FLVV[id(I, J, K)];
+          F = F - SU * (dmax(WIN, 0.0) * VV[id(I, J, K)] - dmax(-WIN, 0.0) * VV[id(I, J + 1, K)]) - SC * FG;
+          F = F + (GGY[id(I, J, K)] + GGY[id(I, J + 1, K)]) * ANU[id(I, J, K)] * Y_(4, J) *
+                      (VV[id(I, J + 1, K)] - VV[id(I, J, K)]);
+        }
+    // (Gx*u)*v
+    for (int K = 2; K <= NK; ++K)
+      for (int J = LA; J <= LB; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          int IC = NF[id(I - 1, J - 1, K)] * NF[id(I - 1, J, K)] * NF[id(I, J - 1, K)] * NF[id(I, J, K)];
+          int IT = INDY[id(I, J, K)], IBt = INDY[id(I - 1, J, K)];
+          double &F = FLVU[id(I, J, K)];
+          if (IC != 0 || (IT != 0 && IBt != 0)) {
+          } else if (IT == 0 && IBt == 0) {
+            double WIN = Y_(6, J) * (Y_(2, J - 1) * GLX[id(I, J, K)] * UU[id(I, J, K)] +
+                                     Y_(2, J) * GLX[id(I, J - 1, K)] * UU[id(I, J - 1, K)]);
+            double FG = WIN * X_(6, I) * (X_(2, I - 1) * VV[id(I, J, K)] + X_(2, I) * VV[id(I - 1, J, K)]);
+            F = F - SU * (dmax(WIN, 0.0) * VV[id(I - 1, J, K)] - dmax(-WIN, 0.0) * VV[id(I, J, K)]) - SC * FG;
+            double GG = Y_(6, J) * (Y_(2, J - 1) * GGX[id(I, J, K)] + Y_(2, J) * GGX[id(I, J - 1, K)]);
+            double ANR = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J, K)] + X_(2, I) * ANU[id(I - 1, J, K)]);
+            double ANL = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J - 1, K)] + X_(2, I) * ANU[id(I - 1, J - 1, K)]);
+            double AN = Y_(6, J) * (Y_(2, J - 1) * ANR + Y_(2, J) * ANL);
+            double D1 = X_(5, I) * (VV[id(I, J, K)] - VV[id(I - 1, J, K)]);
+            double D2 = Y_(5, J) * (UU[id(I, J, K)] - UU[id(I, J - 1, K)]);
+            F = F + GG * AN * (D1 + D2);
+          } else {
+            double BR, BL;
+            int IS = INDX[id(I, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BR = (IB_(2, IS) == 1) ? VV[id(I, J, K)] : VV[id(I - 1, J, K)];
+              else BR = BCV[IS - 1];
+            } else {
+              BR = X_(6, I) * (X_(2, I - 1) * (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) +
+                               X_(2, I) * (VV[id(I - 1, J, K)] + VV[id(I - 1, J + 1, K)])) * 0.5;
+            }
+            IS = INDX[id(I, J - 1, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BL = (IB_(2, IS) == 1) ? VV[id(I, J, K)] : VV[id(I - 1, J, K)];
+              else BL = BCV[IS - 1];
+            } else {
+              BL = X_(6, I) * (X_(2, I - 1) * (VV[id(I, J, K)] + VV[id(I, J - 1, K)]) +
+                               X_(2, I) * (VV[id(I - 1, J, K)] + VV[id(I - 1, J - 1, K)])) * 0.5;
+            }
+            double WIN = Y_(6, J) * (Y_(2, J - 1) * GLX[id(I, J, K)] * UU[id(I, J, K)] +
+                                     Y_(2, J) * GLX[id(I, J - 1, K)] * UU[id(I, J - 1, K)]);
+            double FG = Y_(6, J) * (Y_(2, J) * GLX[id(I, J, K)] * UU[id(I, J, K)] * BR +
+                                    Y_(2, J - 1) * GLX[id(I, J - 1, K)] * UU[id(I, J - 1, K)] * BL);
+            if (IT == 0 && WIN < 0.0) F = F - SU * WIN * VV[id(I, J, K)] - SC * FG;
+            else if (IBt == 0 && WIN > 0.0) F = F - SU * WIN * VV[id(I - 1, J, K)] - SC * FG;
+            else F = F - FG;
+            double GG = Y_(6, J) * (Y_(2, J - 1) * GGX[id(I, J, K)] + Y_(2, J) * GGX[id(I, J - 1, K)]);
+            FG = Y_(6, J) * (Y_(2, J) * BR + Y_(2, J - 1) * BL);
+            double ANR, ANL;
+            if (NF[id(I, J, K)] == -1) ANR = ANU[id(I - 1, J, K)];
+            else if (NF[id(I - 1, J, K)] == -1) ANR = ANU[id(I, J, K)];
+            else ANR = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J, K)] + X_(2, I) * ANU[id(I - 1, J, K)]);
+            if (NF[id(I, J - 1, K)] == -1) ANL = ANU[id(I - 1, J - 1, K)];
+            else if (NF[id(I - 1, J - 1, K)] == -1) ANL = ANU[id(I, J - 1, K)];
+            else ANL = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J - 1, K)] + X_(2, I) * ANU[id(I - 1, J - 1, K)]);
+            double AN = Y_(6, J) * (Y_(2, J - 1) * ANR + Y_(2, J) * ANL);
+            double D1 = (IT == 0) ? X_(4, I) * (VV[id(I, J, K)] - FG) * 2.0
+                                  : X_(4, I - 1) * (FG - VV[id(I - 1, J, K)]) * 2.0;
+            double D2 = Y_(5, J) * (UU[id(I, J, K)] - UU[id(I, J - 1, K)]);
+            F = F + GG * AN * (D1 + D2);
+          }
+        }
+    // (Gz*w)*v
+    for (int K = 2; K <= NK; ++K)
+      for (int J = LA; J <= LB; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          int IC = NF[id(I, J - 1, K - 1)] * NF[id(I, J, K - 1)] * NF[id(I, J - 1, K)] * NF[id(I, J, K)];
+          int IT = INDY[id(I, J, K)], IBt = INDY[id(I, J, K - 1)];
+          double &F = FLVW[id(I, J, K)];
+          if (IC != 0 || (IT != 0 && IBt != 0)) {
+          } else if (IT == 0 && IBt == 0) {
+            double WIN = Y_(6, J) * (Y_(2, J - 1) * GLZ[id(I, J, K)] * WW[id(I, J, K)] +
+                                     Y_(2, J) * GLZ[id(I, J - 1, K)] * WW[id(I, J - 1, K)]);
+            double FG = WIN * Z_(6, K) * (Z_(2, K - 1) * VV[id(I, J, K)] + Z_(2, K) * VV[id(I, J, K - 1)]);
+            F = F - SU * (dmax(WIN, 0.0) * VV[id(I, J, K - 1)] - dmax(-WIN, 0.0) * VV[id(I, J, K)]) - SC * FG;
+            double GG = Y_(6, J) * (Y_(2, J - 1) * GGZ[id(I, J, K)] + Y_(2, J) * GGZ[id(I, J - 1, K)]);
+            double ANR = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I, J, K)] + Z_(2, K) * ANU[id(I, J, K - 1)]);
+            double ANL = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I, J - 1, K)] + Z_(2, K) * ANU[id(I, J - 1, K - 1)]);
+            double AN = Y_(6, J) * (Y_(2, J - 1) * ANR + Y_(2, J) * ANL);
+            double D1 = Z_(5, K) * (VV[id(I, J, K)] - VV[id(I, J, K - 1)]);
+            double D2 = Y_(5, J) * (WW[id(I, J, K)] - WW[id(I, J - 1, K)]);
+            F = F + GG * AN * (D1 + D2);
+          } else {
+            double BR, BL;
+            int IS = INDZ[id(I, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BR = (IB_(2, IS) == 5) ? VV[id(I, J, K)] : VV[id(I, J, K - 1)];
+              else BR = BCV[IS - 1];
+            } else {
+              BR = Z_(6, K) * (Z_(2, K - 1) * (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) +
+                               Z_(2, K) * (VV[id(I, J, K - 1)] + VV[id(I, J + 1, K - 1)])) * 0.5;
+            }
+            IS = INDZ[id(I, J - 1, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BL = (IB_(2, IS) == 5) ? VV[id(I, J, K)] : VV[id(I, J, K - 1)];
+              else BL = BCV[IS - 1];
+            } else {
+              BL = Z_(6, K) * (Z_(2, K - 1) * (VV[id(I, J, K)] + VV[id(I, J - 1, K)]) +
+                               Z_(2, K) * (VV[id(I, J, K - 1)] + VV[id(I, J - 1, K - 1)])) * 0.5;
+            }
+            double WIN = Y_(6, J) * (Y_(2, J - 1) * GLZ[id(I, J, K)] * WW[id(I, J, K)] +
+                                     Y_(2, J) * GLZ[id(I, J - 1, K)] * WW[id(I, J - 1, K)]);
+            double FG = Y_(6, J) * (Y_(2, J) * GLZ[id(I, J, K)] * WW[id(I, J, K)] * BR +
+                                    Y_(2, J - 1) * GLZ[id(I, J - 1, K)] * WW[id(I, J - 1, K)] * BL);
+            if (IT == 0 && WIN < 0.0) F = F - SU * WIN * VV[id(I, J, K)] - SC * FG;
+            else if (IBt == 0 && WIN > 0.0) F = F - SU * WIN * VV[id(I, J, K - 1)] - SC * FG;
+            else F = F - FG;
+            double GG = Y_(6, J) * (Y_(2, J - 1) * GGZ[id(I, J, K)] + Y_(2, J) * GGZ[id(I, J - 1, K)]);
+            FG = Y_(6, J) * (Y_(2, J) * BR + Y_(2, J - 1) * BL);
+            double ANR, ANL;
+            if (NF[id(I, J, K)] == -1) ANR = ANU[id(I, J, K - 1)];
+            else if (NF[id(I, J, K - 1)] == -1) ANR = ANU[id(I, J, K)];
+            else ANR = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I, J, K)] + Z_(2, K) * ANU[id(I, J, K - 1)]);
+            if (NF[id(I, J - 1, K)] == -1) ANL = ANU[id(I, J - 1, K - 1)];
+            else if (NF[id(I, J - 1, K - 1)] == -1) ANL = ANU[id(I, J - 1, K)];
+            else ANL = Z_(6, K) * (Z_(2, K - 1) * ANU[id(I, J - 1, K)] + Z_(2, K) * ANU[id(I, J - 1, K - 1)]);
+            double AN = Y_(6, J) * (Y_(2, J - 1) * ANR + Y_(2, J) * ANL);
+            double D1 = (IT == 0) ? Z_(4, K) * (VV[id(I, J, K)] - FG) * 2.0
+                                  : Z_(4, K - 1) * (FG - VV[id(I, J, K - 1)]) * 2.0;
+            double D2 = Y_(5, J) * (WW[id(I, J, K)] - WW[id(I, J - 1, K)]);
+            F = F + GG * AN * (D1 + D2);
+          }
+        }
+  }
+
+  // VF_VFLXDW  vf_vflxdw.f:58-342
+  void vflxdw(vd &FLWU, vd &FLWV, vd &FLWW) {
+    const double SU = P.scmvp, SC = 1.0 - P.scmvp;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (INDC[id(I, J, K)] == -1) continue;
+          double WIN = (GLZ[id(I, J, K)] * WW[id(I, J, K)] + GLZ[id(I, J, K + 1)] * WW[id(I, J, K + 1)]) * 0.5;
+          double FG = WIN * (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5;
+          double &F = FLWW[id(I, J, K)];
+          F = F - SU * (dmax(WIN, 0.0) * WW[id(I, J, K)] - dmax(-WIN, 0.0) * WW[id(I, J, K + 1)]) - SC * FG;
+          F = F + (GGZ[id(I, J, K)] + GGZ[id(I, J, K + 1)]) * ANU[id(I, J, K)] * Z_(4, K) *
+                      (WW[id(I, J, K + 1)] - WW[id(I, J, K)]);
+        }
+    // (Gx*u)*w
+    for (int K = 3; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          int IC = NF[id(I - 1, J, K - 1)] * NF[id(I - 1, J, K)] * NF[id(I, J, K - 1)] * NF[id(I, J, K)];
+          int IT = INDZ[id(I, J, K)], IBt = INDZ[id(I - 1, J, K)];
+          double &F = FLWU[id(I, J, K)];
+          if (IC != 0 || (IT != 0 && IBt != 0)) {
+          } else if (IT == 0 && IBt == 0) {
+            double WIN = Z_(6, K) * (Z_(2, K - 1) * GLX[id(I, J, K)] * UU[id(I, J, K)] +
+                                     Z_(2, K) * GLX[id(I, J, K - 1)] * UU[id(I, J, K - 1)]);
+            double FG = WIN * X_(6, I) * (X_(2, I - 1) * WW[id(I, J, K)] + X_(2, I) * WW[id(I - 1, J, K)]);
+            F = F - SU * (dmax(WIN, 0.0) * WW[id(I - 1, J, K)] - dmax(-WIN, 0.0) * WW[id(I, J, K)]) - SC * FG;
+            double GG = Z_(6, K) * (Z_(2, K - 1) * GGX[id(I, J, K)] + Z_(2, K) * GGX[id(I, J, K - 1)]);
+            double ANR = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J, K)] + X_(2, I) * ANU[id(I - 1, J, K)]);
+            double ANL = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J, K - 1)] + X_(2, I) * ANU[id(I - 1, J, K - 1)]);
+            double AN = Z_(6, K) * (Z_(2, K - 1) * ANR + Z_(2, K) * ANL);
+            double D1 = X_(5, I) * (WW[id(I, J, K)] - WW[id(I - 1, J, K)]);
+            double D2 = Z_(5, K) * (UU[id(I, J, K)] - UU[id(I, J, K - 1)]);
+            F = F + GG * AN * (D1 + D2);
+          } else {
+            double BR, BL;
+            int IS = INDX[id(I, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BR = (IB_(2, IS) == 1) ? WW[id(I, J, K)] : WW[id(I - 1, J, K)];
+              else BR = BCW[IS - 1];
+            } else {
+              BR = X_(6, I) * (X_(2, I - 1) * (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) +
+                               X_(2, I) * (WW[id(I - 1, J, K)] + WW[id(I - 1, J, K + 1)])) * 0.5;
+            }
+            IS = INDX[id(I, J, K - 1)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BL = (IB_(2, IS) == 1) ? WW[id(I, J, K)] : WW[id(I - 1, J, K)];
+              else BL = BCW[IS - 1];
+            } else {
+              BL = X_(6, I) * (X_(2, I - 1) * (WW[id(I, J, K)] + WW[id(I, J, K - 1)]) +
+                               X_(2, I) * (WW[id(I - 1, J, K)] + WW[id(I - 1, J, K - 1)])) * 0.5;
+            }
+            double WIN = Z_(6, K) * (Z_(2, K - 1) * GLX[id(I, J, K)] * UU[id(I, J, K)] +
+                                     Z_(2, K) * GLX[id(I, J, K - 1)] * UU[id(I, J, K - 1)]);
+            double FG = Z_(6, K) * (Z_(2, K) * GLX[id(I, J, K)] * UU[id(I, J, K)] * BR +
+                                    Z_(2, K - 1) * GLX[id(I, J, K - 1)] * UU[id(I, J, K - 1)] * BL);
+            if (IT == 0 && WIN < 0.0) F = F - SU * WIN * WW[id(I, J, K)] - SC * FG;
+            else if (IBt == 0 && WIN > 0.0) F = F - SU * WIN * WW[id(I - 1, J, K)] - SC * FG;
+            else F = F - FG;
+            double GG = Z_(6, K) * (Z_(2, K - 1) * GGX[id(I, J, K)] + Z_(2, K) * GGX[id(I, J, K - 1)]);
+            FG = Z_(6, K) * (Z_(2, K) * BR + Z_(2, K - 1) * BL);
+            double ANR, ANL;
+            if (NF[id(I, J, K)] == -1) ANR = ANU[id(I - 1, J, K)];
+            else if (NF[id(I - 1, J, K)] == -1) ANR = ANU[id(I, J, K)];
+            else ANR = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J, K)] + X_(2, I) * ANU[id(I - 1, J, K)]);
+            if (NF[id(I, J, K - 1)] == -1) ANL = ANU[id(I - 1, J, K - 1)];
+            else if (NF[id(I - 1, J, K - 1)] == -1) ANL = ANU[id(I, J, K - 1)];
+            else ANL = X_(6, I) * (X_(2, I - 1) * ANU[id(I, J, K - 1)] + X_(2, I) * ANU[id(I - 1, J, K - 1)]);
+            double AN = Z_(6, K) * (Z_(2, K - 1) * ANR + Z_(2, K) * ANL);
+            double D1 = (IT == 0) ? X_(4, I) * (WW[id(I, J, K)] - FG) * 2.0
+                                  : X_(4, I - 1) * (FG - WW[id(I - 1, J, K)]) * 2.0;
+            double D2 = Z_(5, K) * (UU[id(I, J, K)] - UU[id(I, J, K - 1)]);
+            F = F + GG * AN * (D1 + D2);
+          }
+        }
+    // (Gy*v)*w
+    for (int K = 3; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          int IC = NF[id(I, J - 1, K - 1)] * NF[id(I, J - 1, K)] * NF[id(I, J, K - 1)] * NF[id(I, J, K)];
+          int IT = INDZ[id(I, J, K)], IBt = INDZ[id(I, J - 1, K)];
+          double &F = FLWV[id(I, J, K)];
+          if (IC != 0 || (IT != 0 && IBt != 0)) {
+          } else if (IT == 0 && IBt == 0) {
+            double WIN = Z_(6, K) * (Z_(2, K - 1) * GLY[id(I, J, K)] * VV[id(I, J, K)] +
+                                     Z_(2, K) * GLY[id(I, J, K - 1)] * VV[id(I, J, K - 1)]);
+            double FG = WIN * Y_(6, J) * (Y_(2, J - 1) * WW[id(I, J, K)] + Y_(2, J) * WW[id(I, J - 1, K)]);
+            F = F - SU * (dmax(WIN, 0.0) * WW[id(I, J - 1, K)] - dmax(-WIN, 0.0) * WW[id(I, J, K)]) - SC * FG;
+            double GG = Z_(6, K) * (Z_(2, K - 1) * GGY[id(I, J, K)] + Z_(2, K) * GGY[id(I, J, K - 1)]);
+            double ANR = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I, J, K)] + Y_(2, J) * ANU[id(I, J - 1, K)]);
+            double ANL = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I, J, K - 1)] + Y_(2, J) * ANU[id(I, J - 1, K - 1)]);
+            double AN = Z_(6, K) * (Z_(2, K - 1) * ANR + Z_(2, K) * ANL);
+            double D1 = Y_(5, J) * (WW[id(I, J, K)] - WW[id(I, J - 1, K)]);
+            double D2 = Z_(5, K) * (VV[id(I, J, K)] - VV[id(I, J, K - 1)]);
+            F = F + GG * AN * (D1 + D2);
+          } else {
+            double BR, BL;
+            int IS = INDY[id(I, J, K)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BR = (IB_(2, IS) == 3) ? WW[id(I, J, K)] : WW[id(I, J - 1, K)];
+              else BR = BCW[IS - 1];
+            } else {
+              BR = Y_(6, J) * (Y_(2, J - 1) * (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) +
+                               Y_(2, J) * (WW[id(I, J - 1, K)] + WW[id(I, J - 1, K + 1)])) * 0.5;
+            }
+            IS = INDY[id(I, J, K - 1)];
+            if (IS >= 1) {
+              if (IB_(3, IS) == 1 || IB_(3, IS) == 4) BL = (IB_(2, IS) == 3) ? WW[id(I, J, K)] : WW[id(I, J - 1, K)];
+              else BL = BCW[IS - 1];
+            } else {
+              BL = Y_(6, J) * (Y_(2, J - 1) * (WW[id(I, J, K)] + WW[id(I, J, K - 1)]) +
+                               Y_(2, J) * (WW[id(I, J - 1, K)] + WW[id(I, J - 1, K - 1)])) * 0.5;
+            }
+            double WIN = Z_(6, K) * (Z_(2, K - 1) * GLY[id(I, J, K)] * VV[id(I, J, K)] +
+                                     Z_(2, K) * GLY[id(I, J, K - 1)] * VV[id(I, J, K - 1)]);
+            double FG = Z_(6, K) * (Z_(2, K) * GLY[id(I, J, K)] * VV[id(I, J, K)] * BR +
+                                    Z_(2, K - 1) * GLY[id(I, J, K - 1)] * VV[id(I, J, K - 1)] * BL);
+            if (IT == 0 && WIN < 0.0) F = F - SU * WIN * WW[id(I, J, K)] - SC * FG;
+            else if (IBt == 0 && WIN > 0.0) F = F - SU * WIN * WW[id(I, J - 1, K)] - SC * FG;
+            else F = F - FG;
+            double GG = Z_(6, K) * (Z_(2, K - 1) * GGY[id(I, J, K)] + Z_(2, K) * GGY[id(I, J, K - 1)]);
+            FG = Z_(6, K) * (Z_(2, K) * BR + Z_(2, K - 1) * BL);
+            double ANR, ANL;
+            if (NF[id(I, J, K)] == -1) ANR = ANU[id(I, J - 1, K)];
+            else if (NF[id(I, J - 1, K)] == -1) ANR = ANU[id(I, J, K)];
+            else ANR = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I, J, K)] + Y_(2, J) * ANU[id(I, J - 1, K)]);
+            if (NF[id(I, J, K - 1)] == -1) ANL = ANU[id(I, J - 1, K - 1)];
+            else if (NF[id(I, J - 1, K - 1)] == -1) ANL = ANU[id(I, J, K - 1)];
+            else ANL = Y_(6, J) * (Y_(2, J - 1) * ANU[id(I, J, K - 1)] + Y_(2, J) * ANU[id(I, J - 1, K - 1)]);
+            double AN = Z_(6, K) * (Z_(2, K - 1) * ANR + Z_(2, K) * ANL);
+            double D1 = (IT == 0) ? Y_(4, J) * (WW[id(I, J, K)] - FG) * 2.0
+                                  : Y_(4, J - 1) * (FG - WW[id(I, J - 1, K)]) * 2.0;
+            double D2 = Z_(5, K) * (VV[id(I, J, K)] - VV[id(I, J, K - 1)]);
+            F = F + GG * AN * (D1 + D2);
+          }
+        }
+  }
+
+  // VF_VGENE  vf_vgene.f:84-332 (IDRGN<=0 drag, no k-eps/T/C/wave source)
+  void vgene(vd &QU, vd &QV, vd &QW) {
+    const double RI = 1.0 / P.rho0;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 3; I <= NI - 1; ++I) {
+          int I1 = I - 1;
+          if (!(INDX[id(I, J, K)] == 0 && NF[id(I1, J, K)] * NF[id(I, J, K)] == 0)) continue;
+          double GV = X_(6, I) * (X_(2, I) * GGV[id(I, J, K)] + X_(2, I1) * GGV[id(I1, J, K)]);
+          double CD = X_(6, I) * (X_(2, I) * CD0[id(I, J, K)] + X_(2, I1) * CD0[id(I1, J, K)]);
+          double &Q = QU[id(I, J, K)];
+          Q = Q + GV * RI * X_(5, I) * (PP[id(I1, J, K)] - PP[id(I, J, K)]);
+          double U = UU[id(I, J, K)];
+          double V = X_(6, I) * (X_(2, I1) * (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) +
+                                 X_(2, I) * (VV[id(I1, J, K)] + VV[id(I1, J + 1, K)])) * 0.5;
+          double W = X_(6, I) * (X_(2, I1) * (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) +
+                                 X_(2, I) * (WW[id(I1, J, K)] + WW[id(I1, J, K + 1)])) * 0.5;
+          double UVW = std::sqrt(U * U + V * V + W * W);
+          Q = Q - 0.5 * CD * X_(5, I) * (1.0 - GGX[id(I, J, K)]) * U * UVW;
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 3; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          int J1 = J - 1;
+          if (!(INDY[id(I, J, K)] == 0 && NF[id(I, J1, K)] * NF[id(I, J, K)] == 0)) continue;
+          double GV = Y_(6, J) * (Y_(2, J) * GGV[id(I, J, K)] + Y_(2, J1) * GGV[id(I, J1, K)]);
+          double CD = Y_(6, J) * (Y_(2, J) * CD0[id(I, J, K)] + Y_(2, J1) * CD0[id(I, J1, K)]);
+          double &Q = QV[id(I, J, K)];
+          Q = Q + GV * RI * Y_(5, J) * (PP[id(I, J1, K)] - PP[id(I, J, K)]);
+          double U = Y_(6, J) * (Y_(2, J1) * (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) +
+                                 Y_(2, J) * (UU[id(I, J1, K)] + UU[id(I + 1, J1, K)])) * 0.5;
+          double V = VV[id(I, J, K)];
+          double W = Y_(6, J) * (Y_(2, J1) * (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) +
+                                 Y_(2, J) * (WW[id(I, J1, K)] + WW[id(I, J1, K + 1)])) * 0.5;
+          double UVW = std::sqrt(U * U + V * V + W * W);
+          Q = Q - 0.5 * CD * Y_(5, J) * (1.0 - GGY[id(I, J, K)]) * V * UVW;
+        }
+    for (int K = 3; K <= NK - 1; ++K) {
+      int K1 = K - 1;
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (!(INDZ[id(I, J, K)] == 0 && NF[id(I, J, K1)] * NF[id(I, J, K)] == 0)) continue;
+          double GV = Z_(6, K) * (Z_(2, K) * GGV[id(I, J, K)] + Z_(2, K1) * GGV[id(I, J, K1)]);
+          double CD = Z_(6, K) * (Z_(2, K) * CD0[id(I, J, K)] + Z_(2, K1) * CD0[id(I, J, K1)]);
+          double &Q = QW[id(I, J, K)];
+          Q = Q + GV * RI * Z_(5, K) * (PP[id(I, J, K1)] - PP[id(I, J, K)]);
+          double U = Z_(6, K) * (Z_(2, K1) * (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) +
+                                 Z_(2, K) * (UU[id(I, J, K1)] + UU[id(I + 1, J, K1)])) * 0.5;
+          double V = Z_(6, K) * (Z_(2, K1) * (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) +
+                                 Z_(2, K) * (VV[id(I, J, K1)] + VV[id(I, J + 1, K1)])) * 0.5;
+          double W = WW[id(I, J, K)];
+          double UVW = std::sqrt(U * U + V * V + W * W);
+          Q = Q - 0.5 * CD * Z_(5, K) * (1.0 - GGZ[id(I, J, K)]) * W * UVW;
+          Q = Q - GV * P.grz0;
+          double DR = 0.0;  // no temperature / concentration (vf_vgene.f:318-327)
+          Q = Q - GV * P.grz0 * DR / P.rho0;
+        }
+    }
+  }
+
+  // Sponge of VF_VEULER (vf_veuler.f:77-113 parameters, :131-166 profile)
+  struct Sponge {
+    int IPA = 0, IP[4];
+    double W[4], PX[4], PZ[4];
+  };
+  Sponge sponge() const {
+    Sponge s;
+    for (int d = 0; d < 4; ++d) {
+      s.IP[d] = P.idamp[d];
+      s.W[d] = s.PX[d] = s.PZ[d] = 0.0;
+      if (s.IP[d] >= 0) {
+        s.IPA = s.IPA + 1;
+        double D = std::sqrt(P.grz0 / P.damp[d][3]);
+        s.W[d] = P.damp[d][2];
+        s.PX[d] = (double)(s.IP[d] + 1) * P.damp[d][0] * D;
+        s.PZ[d] = (double)(s.IP[d] + 1) * P.damp[d][1] * D;
+      }
+    }
+    return s;
+  }
+  double sponge_dmax(const Sponge &s, double X, double Y, bool z) const {
+    double DMAX = 0.0, D;
+    const double *PP_ = z ? s.PZ : s.PX;
+    if (s.IP[0] >= 0) { D = X - P.glxmin; if (D <= s.W[0]) { D = PP_[0] * ipow(1.0 - D / s.W[0], s.IP[0]); if (D > DMAX) DMAX = D; } }
+    if (s.IP[1] >= 0) { D = P.glxmax - X; if (D <= s.W[1]) { D = PP_[1] * ipow(1.0 - D / s.W[1], s.IP[1]); if (D > DMAX) DMAX = D; } }
+    if (s.IP[2] >= 0) { D = Y - P.glymin; if (D <= s.W[2]) { D = PP_[2] * ipow(1.0 - D / s.W[2], s.IP[2]); if (D > DMAX) DMAX = D; } }
+    if (s.IP[3] >= 0) { D = P.glymax - Y; if (D <= s.W[3]) { D = PP_[3] * ipow(1.0 - D / s.W[3], s.IP[3]); if (D > DMAX) DMAX = D; } }
+    return DMAX;
+  }
+
+  // VF_VEULER  vf_veuler.f:115-284  (GLV0 = GLV, GGV0 = GGV for IPRNT<=1)
+  void veuler(const vd &FLUU, const vd &FLUV, const vd &FLUW, const vd &QU,
+              const vd &FLVU, const vd &FLVV, const vd &FLVW, const vd &QV,
+              const vd &FLWU, const vd &FLWV, const vd &FLWW, const vd &QW) {
+    Sponge s = sponge();
+    const double DT = DTNOW, VM = P.vvmax;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 3; I <= NI - 1; ++I) {
+          if (!(INDX[id(I, J, K)] == 0 && NF[id(I - 1, J, K)] * NF[id(I, J, K)] == 0)) continue;
+          double GV = X_(6, I) * (X_(2, I) * GLV[id(I, J, K)] + X_(2, I - 1) * GLV[id(I - 1, J, K)]);
+          double GV0 = X_(6, I) * (X_(2, I) * GLV[id(I, J, K)] + X_(2, I - 1) * GLV[id(I - 1, J, K)]);
+          double DU = (X_(5, I) * (FLUU[id(I, J, K)] - FLUU[id(I - 1, J, K)]) +
+                       Y_(4, J) * (FLUV[id(I, J + 1, K)] - FLUV[id(I, J, K)]) +
+                       Z_(4, K) * (FLUW[id(I, J, K + 1)] - FLUW[id(I, J, K)]) + QU[id(I, J, K)]);
+          double &U = UU[id(I, J, K)];
+          U = (GV * U + DT * DU) / GV0;
+          if (U > VM) U = VM;
+          if (U < -VM) U = -VM;
+          if (s.IPA != 0) {
+            double X = X_(1, I), Y = (Y_(1, J) + Y_(1, J + 1)) * 0.5;
+            double DMAX = sponge_dmax(s, X, Y, false);
+            double G = X_(6, I) * (X_(2, I) * GGV[id(I, J, K)] + X_(2, I - 1) * GGV[id(I - 1, J, K)]);
+            double D = GV0 / (GV0 + DT * G * DMAX);
+            U = U * D;
+          }
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 3; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (!(INDY[id(I, J, K)] == 0 && NF[id(I, J - 1, K)] * NF[id(I, J, K)] == 0)) continue;
+          double GV = Y_(6, J) * (Y_(2, J) * GLV[id(I, J, K)] + Y_(2, J - 1) * GLV[id(I, J - 1, K)]);
+          double GV0 = Y_(6, J) * (Y_(2, J) * GLV[id(I, J, K)] + Y_(2, J - 1) * GLV[id(I, J - 1, K)]);
+          double DV = (X_(4, I) * (FLVU[id(I + 1, J, K)] - FLVU[id(I, J, K)]) +
+                       Y_(5, J) * (FLVV[id(I, J, K)] - FLVV[id(I, J - 1, K)]) +
+                       Z_(4, K) * (FLVW[id(I, J, K + 1)] - FLVW[id(I, J, K)]) + QV[id(I, J, K)]);
+          double &V = VV[id(I, J, K)];
+          V = (GV * V + DT * DV) / GV0;
+          if (V > VM) V = VM;
+          if (V < -VM) V = -VM;
+          if (s.IPA != 0) {
+            double X = (X_(1, I) + X_(1, I + 1)) * 0.5, Y = Y_(1, J);
+            double DMAX = sponge_dmax(s, X, Y, false);
+            double G = Y_(6, J) * (Y_(2, J) * GGV[id(I, J, K)] + Y_(2, J - 1) * GGV[id(I, J - 1, K)]);
+            double D = GV0 / (GV0 + DT * G * DMAX);
+            V = V * D;
+          }
+        }
+    for (int K = 3; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (!(INDZ[id(I, J, K)] == 0 && NF[id(I, J, K - 1)] * NF[id(I, J, K)] == 0)) continue;
+          double GV = Z_(6, K) * (Z_(2, K) * GLV[id(I, J, K)] + Z_(2, K - 1) * GLV[id(I, J, K - 1)]);
+          double GV0 = Z_(6, K) * (Z_(2, K) * GLV[id(I, J, K)] + Z_(2, K - 1) * GLV[id(I, J, K - 1)]);
+          double DW = (X_(4, I) * (FLWU[id(I + 1, J, K)] - FLWU[id(I, J, K)]) +
+                       Y_(4, J) * (FLWV[id(I, J + 1, K)] - FLWV[id(I, J, K)]) +
+                       Z_(5, K) * (FLWW[id(I, J, K)] - FLWW[id(I, J, K - 1)]) + QW[id(I, J, K)]);
+          double &W = WW[id(I, J, K)];
+          W = (GV * W + DT * DW) / GV0;
+          if (W > VM) W = VM;
+          if (W < -VM) W = -VM;
+          if (s.IPA != 0) {
+            double X = (X_(1, I) + X_(1, I + 1)) * 0.5, Y = (Y_(1, J) + Y_(1, J + 1)) * 0.5;
+            double DMAX = sponge_dmax(s, X, Y, true);
+            double G = Z_(6, K) * (Z_(2, K) * GGV[id(I, J, K)] + Z_(2, K - 1) * GGV[id(I, J, K - 1)]);
+            double D = GV0 / (GV0 + DT * G * DMAX);
+            W = W * D;
+          }
+        }
+  }
+
+  // VF_BWUWN  vf_bwuwn.f:93-160 (slip, no-slip, fixed, free; wave/open
+  // faces (IB=5,7) keep the values the caller set in BCU/BCV/BCW)
+  int bwuwn() {
+    for (int L = 1; L <= NB; ++L) {
+      int I, J, K;
+      decode(IB_(1, L), I, J, K);
+      int NS = IB_(2, L), IB = IB_(3, L);
+      if (IB == 1 || IB == 6 || IB == 8) {
+        if (NS == 1 || NS == 2) { BCU[L - 1] = 0.0; UU[id(I, J, K)] = 0.0; }
+        else if (NS == 3 || NS == 4) { BCV[L - 1] = 0.0; VV[id(I, J, K)] = 0.0; }
+        else { BCW[L - 1] = 0.0; WW[id(I, J, K)] = 0.0; }
+        if (IB != 1) return CADMAS_EUNSUPPORTED;
+      } else if (IB == 2) {
+        BCU[L - 1] = 0.0; BCV[L - 1] = 0.0; BCW[L - 1] = 0.0;
+        if (NS == 1 || NS == 2) UU[id(I, J, K)] = BCU[L - 1];
+        else if (NS == 3 || NS == 4) VV[id(I, J, K)] = BCV[L - 1];
+        else WW[id(I, J, K)] = BCW[L - 1];
+      } else if (IB == 3) {
+        if (NS == 1 || NS == 2) UU[id(I, J, K)] = BCU[L - 1];
+        else if (NS == 3 || NS == 4) VV[id(I, J, K)] = BCV[L - 1];
+        else WW[id(I, J, K)] = BCW[L - 1];
+      } else if (IB == 4) {
+        double VAL;
+        if (NS == 1) { VAL = UU[id(I + 1, J, K)]; BCU[L - 1] = VAL; UU[id(I, J, K)] = VAL; }
+        else if (NS == 2) { VAL = UU[id(I - 1, J, K)]; BCU[L - 1] = VAL; UU[id(I, J, K)] = VAL; }
+        else if (NS == 3) { VAL = VV[id(I, J + 1, K)]; BCV[L - 1] = VAL; VV[id(I, J, K)] = VAL; }
+        else if (NS == 4) { VAL = VV[id(I, J - 1, K)]; BCV[L - 1] = VAL; VV[id(I, J, K)] = VAL; }
+        else if (NS == 5) { VAL = WW[id(I, J, K + 1)]; BCW[L - 1] = VAL; WW[id(I, J, K)] = VAL; }
+        else if (NS == 6) { VAL = WW[id(I, J, K - 1)]; BCW[L - 1] = VAL; WW[id(I, J, K)] = VAL; }
+      } else if (IB == 5 || IB == 7) {
+        return CADMAS_EUNSUPPORTED;
+      } else {
+        return CADMAS_EPG;
+      }
+    }
+    return CADMAS_OK;
+  }
+
+  // VF_VPCOEF  vf_vpcoef.f:117-437 (IPRNT<=1: GGV0=GGV; PVCP0<0: PPS=0)
+  int vpcoef(vd &AD, vd &ALI, vd &ALJ, vd &ALK, vd &AUI, vd &AUJ, vd &AUK, vd &BB) {
+    std::fill(AD.begin(), AD.end(), 0.0);
+    std::fill(ALI.begin(), ALI.end(), 0.0); std::fill(ALJ.begin(), ALJ.end(), 0.0);
+    std::fill(ALK.begin(), ALK.end(), 0.0); std::fill(AUI.begin(), AUI.end(), 0.0);
+    std::fill(AUJ.begin(), AUJ.end(), 0.0); std::fill(AUK.begin(), AUK.end(), 0.0);
+    std::fill(BB.begin(), BB.end(), 0.0);
+    const double DTI = 1.0 / DTNOW, TR = DTNOW / P.rho0, PPS = 0.0;
+    for (int K = 1; K <= NK; ++K)
+      for (int J = 1; J <= NJ; ++J)
+        for (int I = 1; I <= NI; ++I) {
+          size_t c = id(I, J, K);
+          int N = NF[c];
+          if (INDC[c] == -1) {
+            AD[c] = 1.0; ALI[c] = 0.0; ALJ[c] = 0.0; ALK[c] = 0.0;
+            AUI[c] = 0.0; AUJ[c] = 0.0; AUK[c] = 0.0; BB[c] = 0.0;
+          } else if (N == 0) {
+            int IM = I - 1, IP = I + 1, JM = J - 1, JP = J + 1, KM = K - 1, KP = K + 1;
+            double AXY = X_(2, I) * Y_(2, J), AXZ = X_(2, I) * Z_(2, K), AYZ = Y_(2, J) * Z_(2, K);
+            double AVL = X_(2, I) * Y_(2, J) * Z_(2, K);
+            double AIM, AIP, AJM, AJP, AKM, AKP, GV;
+            int IS = INDX[c];
+            if (IS == 0) {
+              GV = X_(6, I) * (X_(2, I) * GGV[c] / GLV[c] + X_(2, IM) * GGV[id(IM, J, K)] / GLV[id(IM, J, K)]);
+              AIM = AYZ * X_(5, I) * GGX[c] * GV; ALI[c] = -AIM;
+            } else if (IS >= 1) {
+              if (IB_(3, IS) == 4) { AIM = 2.0 * AYZ * X_(4, I) * GGX[c] * GGV[c] / GLV[c]; ALI[c] = 0.0; }
+              else { AIM = 0.0; ALI[c] = 0.0; }
+            } else return CADMAS_EPG;
+            IS = INDX[id(IP, J, K)];
+            if (IS == 0) {
+              GV = X_(6, IP) * (X_(2, IP) * GGV[id(IP, J, K)] / GLV[id(IP, J, K)] + X_(2, I) * GGV[c] / GLV[c]);
+              AIP = AYZ * X_(5, IP) * GGX[id(IP, J, K)] * GV; AUI[c] = -AIP;
+            } else if (IS >= 1) {
+              if (IB_(3, IS) == 4) { AIP = 2.0 * AYZ * X_(4, I) * GGX[id(IP, J, K)] * GGV[c] / GLV[c]; AUI[c] = 0.0; }
+              else { AIP = 0.0; AUI[c] = 0.0; }
+            } else return CADMAS_EPG;
+            IS = INDY[c];
+            if (IS == 0) {
+              GV = Y_(6, J) * (Y_(2, J) * GGV[c] / GLV[c] + Y_(2, JM) * GGV[id(I, JM, K)] / GLV[id(I, JM, K)]);
+              AJM = AXZ * Y_(5, J) * GGY[c] * GV; ALJ[c] = -AJM;
+            } else if (IS >= 1) {
+              if (IB_(3, IS) == 4) { AJM = 2.0 * AXZ * Y_(4, J) * GGY[c] * GGV[c] / GLV[c]; ALJ[c] = 0.0; }
+              else { AJM = 0.0; ALJ[c] = 0.0; }
+            } else return CADMAS_EPG;
+            IS = INDY[id(I, JP, K)];
+            if (IS == 0) {
+              GV = Y_(6, JP) * (Y_(2, JP) * GGV[id(I, JP, K)] / GLV[id(I, JP, K)] + Y_(2, J) * GGV[c] / GLV[c]);
+              AJP = AXZ * Y_(5, JP) * GGY[id(I, JP, K)] * GV; AUJ[c] = -AJP;
+            } else if (IS >= 1) {
+              if (IB_(3, IS) == 4) { AJP = 2.0 * AXZ * Y_(4, J) * GGY[id(I, JP, K)] * GGV[c] / GLV[c]; AUJ[c] = 0.0; }
+              else { AJP = 0.0; AUJ[c] = 0.0; }
+            } else return CADMAS_EPG;
+            IS = INDZ[c];
+            if (IS == 0) {
+              GV = Z_(6, K) * (Z_(2, K) * GGV[c] / GLV[c] + Z_(2, KM) * GGV[id(I, J, KM)] / GLV[id(I, J, KM)]);
+              AKM = AXY * Z_(5, K) * GGZ[c] * GV; ALK[c] = -AKM;
+            } else if (IS >= 1) {
+              if (IB_(3, IS) != 4) { AKM = 0.0; ALK[c] = 0.0; }
+              else { AKM = 2.0 * AXY * Z_(4, K) * GGZ[c] * GGV[c] / GLV[c]; ALK[c] = 0.0; }
+            } else return CADMAS_EPG;
+            IS = INDZ[id(I, J, KP)];
+            if (IS == 0) {
+              GV = Z_(6, KP) * (Z_(2, KP) * GGV[id(I, J, KP)] / GLV[id(I, J, KP)] + Z_(2, K) * GGV[c] / GLV[c]);
+              AKP = AXY * Z_(5, KP) * GGZ[id(I, J, KP)] * GV; AUK[c] = -AKP;
+            } else if (IS >= 1) {
+              if (IB_(3, IS) != 4) { AKP = 0.0; AUK[c] = 0.0; }
+              else { AKP = 2.0 * AXY * Z_(4, K) * GGZ[id(I, J, KP)] * GGV[c] / GLV[c]; AUK[c] = 0.0; }
+            } else return CADMAS_EPG;
+            AD[c] = AKM + AJM + AIM + AIP + AJP + AKP;
+            double VD = AYZ * (GGX[id(IP, J, K)] * UU[id(IP, J, K)] - GGX[c] * UU[c]) +
+                        AXZ * (GGY[id(I, JP, K)] * VV[id(I, JP, K)] - GGY[c] * VV[c]) +
+                        AXY * (GGZ[id(I, J, KP)] * WW[id(I, J, KP)] - GGZ[c] * WW[c]);
+            double VQ = -(GGV[c] - GGV[c]) * DTI * AVL;
+            BB[c] = VD - VQ;
+          } else if (N == 5) {
+            double PSI = Z_(3, K) / (0.5 * Z_(2, K - 1) + FF[c] * Z_(2, K));
+            AD[c] = 1.0; ALI[c] = 0.0; ALJ[c] = 0.0; ALK[c] = PSI - 1.0; AUI[c] = 0.0; AUJ[c] = 0.0; AUK[c] = 0.0;
+            BB[c] = -TR * ((1.0 - PSI) * PP[id(I, J, K - 1)] + PSI * PPS - PP[c]);
+          } else if (N == 6) {
+            double PSI = Z_(3, K + 1) / (0.5 * Z_(2, K + 1) + FF[c] * Z_(2, K));
+            AD[c] = 1.0; ALI[c] = 0.0; ALJ[c] = 0.0; ALK[c] = 0.0; AUI[c] = 0.0; AUJ[c] = 0.0; AUK[c] = PSI - 1.0;
+            BB[c] = -TR * ((1.0 - PSI) * PP[id(I, J, K + 1)] + PSI * PPS - PP[c]);
+          } else if (N == 3) {
+            double PSI = Y_(3, J) / (0.5 * Y_(2, J - 1) + FF[c] * Y_(2, J));
+            AD[c] = 1.0; ALI[c] = 0.0; ALJ[c] = PSI - 1.0; ALK[c] = 0.0; AUI[c] = 0.0; AUJ[c] = 0.0; AUK[c] = 0.0;
+            BB[c] = -TR * ((1.0 - PSI) * PP[id(I, J - 1, K)] + PSI * PPS - PP[c]);
+          } else if (N == 4) {
+            double PSI = Y_(3, J + 1) / (0.5 * Y_(2, J + 1) + FF[c] * Y_(2, J));
+            AD[c] = 1.0; ALI[c] = 0.0; ALJ[c] = 0.0; ALK[c] = 0.0; AUI[c] = 0.0; AUJ[c] = PSI - 1.0; AUK[c] = 0.0;
+            BB[c] = -TR * ((1.0 - PSI) * PP[id(I, J + 1, K)] + PSI * PPS - PP[c]);
+          } else if (N == 1) {
+            double PSI = X_(3, I) / (0.5 * X_(2, I - 1) + FF[c] * X_(2, I));
+            AD[c] = 1.0; ALI[c] = PSI - 1.0; ALJ[c] = 0.0; ALK[c] = 0.0; AUI[c] = 0.0; AUJ[c] = 0.0; AUK[c] = 0.0;
+            BB[c] = -TR * ((1.0 - PSI) * PP[id(I - 1, J, K)] + PSI * PPS - PP[c]);
+          } else if (N == 2) {
+            double PSI = X_(3, I + 1) / (0.5 * X_(2, I + 1) + FF[c] * X_(2, I));
+            AD[c] = 1.0; ALI[c] = 0.0; ALJ[c] = 0.0; ALK[c] = 0.0; AUI[c] = PSI - 1.0; AUJ[c] = 0.0; AUK[c] = 0.0;
+            BB[c] = -TR * ((1.0 - PSI) * PP[id(I + 1, J, K)] + PSI * PPS - PP[c]);
+          } else {
+            return CADMAS_EPG;
+          }
+        }
+    return CADMAS_OK;
+  }
+
+  // ----------------------------------------------------------- solver
+  // Block decomposition of the interior for the preconditioner
+  // (emulated PARALLEL X/Y ranks; tile = one rank's MYIS..MYIE x MYJS..MYJE).
+  struct Tile { int is, ie, js, je; };
+  std::vector<Tile> tiles() const {
+    int ti = P.precond_ti > 0 ? P.precond_ti : (NI - 2);
+    int tj = P.precond_tj > 0 ? P.precond_tj : (NJ - 2);
+    std::vector<Tile> t;
+    for (int js = 2; js <= NJ - 1; js += tj)
+      for (int is = 2; is <= NI - 1; is += ti)
+        t.push_back({is, std::min(NI - 1, is + ti - 1), js, std::min(NJ - 1, js + tj - 1)});
+    return t;
+  }
+
+  // VF_MZDCMP  vf_mzdcmp.f:53-67, per tile.  A neighbour outside the tile
+  // is a halo cell of the rank: DD=0 there and its coefficients are 0
+  // (VF_VPCOEF zeroes the arrays and the halo exchanges are disabled), so
+  // its term is coef*0*0.
+  bool mzdcmp(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
+              const vd &AUJ, const vd &AUK, vd &DDo, const int *IC) {
+    const double U = (P.icgtyp != 0) ? P.cgpara : 0.0;
+    bool npos = true;
+    for (const Tile &t : tiles())
+      for (int K = 2; K <= NK - 1; ++K)
+        for (int J = t.js; J <= t.je; ++J)
+          for (int I = t.is; I <= t.ie; ++I) {
+            size_t c = id(I, J, K);
+            if (IC[c] == -1) continue;
+            double d1 = 0.0, a1 = 0.0, d2 = 0.0, a2 = 0.0, d3 = 0.0, a3 = 0.0;
+            if (I > t.is) { size_t n = id(I - 1, J, K); d1 = DDo[n]; a1 = AUI[n] + U * (AUJ[n] + AUK[n]); }
+            else { a1 = 0.0 + U * (0.0 + 0.0); }
+            if (J > t.js) { size_t n = id(I, J - 1, K); d2 = DDo[n]; a2 = AUJ[n] + U * (AUI[n] + AUK[n]); }
+            else { a2 = 0.0 + U * (0.0 + 0.0); }
+            { size_t n = id(I, J, K - 1); d3 = DDo[n]; a3 = AUK[n] + U * (AUI[n] + AUJ[n]); }
+            DDo[c] = 1.0 / (AD[c] - ALI[c] * d1 * a1 - ALJ[c] * d2 * a2 - ALK[c] * d3 * a3);
+            if (DDo[c] <= 0.0) npos = false;
+          }
+    return npos;
+  }
+  // VF_MZFRWD vf_mzfrwd.f:37-48 then VF_MZBKWD vf_mzbkwd.f:37-47, per tile.
+  void mzminv(const vd &DDv, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
+              const vd &AUJ, const vd &AUK, vd &X, const vd &Yv, const int *IC) {
+    for (const Tile &t : tiles()) {
+      for (int K = 2; K <= NK - 1; ++K)
+        for (int J = t.js; J <= t.je; ++J)
+          for (int I = t.is; I <= t.ie; ++I) {
+            size_t c = id(I, J, K);
+            if (IC[c] == -1) continue;
+            double d1 = 0.0, x1 = 0.0, d2 = 0.0, x2 = 0.0;
+            if (I > t.is) { d1 = DDv[id(I - 1, J, K)]; x1 = X[id(I - 1, J, K)]; }
+            if (J > t.js) { d2 = DDv[id(I, J - 1, K)]; x2 = X[id(I, J - 1, K)]; }
+            double d3 = DDv[id(I, J, K - 1)], x3 = X[id(I, J, K - 1)];
+            X[c] = Yv[c] - ALI[c] * d1 * x1 - ALJ[c] * d2 * x2 - ALK[c] * d3 * x3;
+          }
+      for (int K = NK - 1; K >= 2; --K)
+        for (int J = t.je; J >= t.js; --J)
+          for (int I = t.ie; I >= t.is; --I) {
+            size_t c = id(I, J, K);
+            if (IC[c] == -1) continue;
+            double x1 = (I < t.ie) ? X[id(I + 1, J, K)] : 0.0;
+            double x2 = (J < t.je) ? X[id(I, J + 1, K)] : 0.0;
+            double x3 = X[id(I, J, K + 1)];
+            X[c] = (X[c] - AUI[c] * x1 - AUJ[c] * x2 - AUK[c] * x3) * DDv[c];
+          }
+    }
+  }
+  // VF_MZAX  vf_mzax.f:42-56
+  void mzax(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
+            const vd &AUJ, const vd &AUK, const vd &X, vd &Yv, const int *IC) {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (IC[c] == -1) continue;
+          Yv[c] = AD[c] * X[c] + ALI[c] * X[id(I - 1, J, K)] + ALJ[c] * X[id(I, J - 1, K)] +
+                  ALK[c] * X[id(I, J, K - 1)] + AUI[c] * X[id(I + 1, J, K)] + AUJ[c] * X[id(I, J + 1, K)] +
+                  AUK[c] * X[id(I, J, K + 1)];
+        }
+  }
+  // VF_MZIP  vf_mzip.f:32-43 (+ VF_P1SUMD): per-rank partial sums in ref
+  // order, the row tree in GPU order.
+  double mzip(const vd &X, const vd &Yv, const int *IC) {
+    if (sum_mode == ORC_SUM_REF) {
+      double S = 0.0;
+      for (const Tile &t : tiles()) {
+        double s = 0.0;
+        for (int K = 2; K <= NK - 1; ++K)
+          for (int J = t.js; J <= t.je; ++J)
+            for (int I = t.is; I <= t.ie; ++I) {
+              size_t c = id(I, J, K);
+              if (IC[c] != -1) s = s + X[c] * Yv[c];
+            }
+        S = S + s;
+      }
+      return S;
+    }
+    return gsum([&](int i, int j, int k, double &c) {
+      size_t q = id(i, j, k);
+      if (IC[q] == -1) return false;
+      c = X[q] * Yv[q];
+      return true;
+    });
+  }
+
+  // VF_M1BCGS  vf_m1bcgs.f:76-266
+  void m1bcgs(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
+              const vd &AUJ, const vd &AUK, const vd &BB, vd &X0, const int *IC,
+              double &BNORM, double &XNORM, int &ITER) {
+    size_t N = X0.size();
+    XW = X0;
+    DD.assign(N, 0.0); Y2.assign(N, 0.0); R0.assign(N, 0.0); RR.assign(N, 0.0);
+    PPv.assign(N, 0.0); AP.assign(N, 0.0); AE.assign(N, 0.0);
+    ITER = -1; BNORM = 0.0; XNORM = 0.0;
+    if (!mzdcmp(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, DD, IC)) return;
+    const double EPSA2 = P.cgepsa * P.cgepsa, EPSR2 = P.cgepsr * P.cgepsr, DIV2 = P.cgdiv * P.cgdiv;
+    mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, Y2, BB, IC);
+    BNORM = mzip(Y2, Y2, IC);
+    ITER = 0;
+    mzax(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, XW, Y2, IC);
+    for (size_t c = 0; c < N; ++c) if (IC[c] != -1) Y2[c] = BB[c] - Y2[c];
+    mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, R0, Y2, IC);
+    double S = mzip(R0, R0, IC);
+    XNORM = S;
+    if (!(XNORM <= BNORM * EPSR2 + EPSA2)) {
+      for (size_t c = 0; c < N; ++c) if (IC[c] != -1) { RR[c] = R0[c]; PPv[c] = R0[c]; }
+      for (;;) {
+        ITER = ITER + 1;
+        if (ITER > P.icgmax) break;
+        mzax(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, PPv, Y2, IC);
+        mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, AP, Y2, IC);
+        double W1 = mzip(R0, AP, IC);
+        double ALPHA = S / W1;
+        for (size_t c = 0; c < N; ++c) if (IC[c] != -1) RR[c] = RR[c] - ALPHA * AP[c];
+        mzax(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, RR, Y2, IC);
+        mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, AE, Y2, IC);
+        W1 = mzip(RR, AE, IC);
+        double W2 = mzip(AE, AE, IC);
+        double OMEGA = W1 / W2;
+        for (size_t c = 0; c < N; ++c)
+          if (IC[c] != -1) {
+            XW[c] = XW[c] + (ALPHA * PPv[c] + OMEGA * RR[c]);
+            RR[c] = RR[c] - OMEGA * AE[c];
+          }
+        XNORM = mzip(RR, RR, IC);
+        if (XNORM <= BNORM * EPSR2 + EPSA2) break;
+        if (XNORM > DIV2) { ITER = -2; break; }
+        W1 = mzip(R0, RR, IC);
+        double BETA = W1 * ALPHA / (S * OMEGA);
+        for (size_t c = 0; c < N; ++c)
+          if (IC[c] != -1) PPv[c] = RR[c] + BETA * (PPv[c] - OMEGA * AP[c]);
+        S = W1;
+      }
+    }
+    BNORM = std::sqrt(BNORM);
+    XNORM = std::sqrt(XNORM);
+    if (ITER >= 0)
+      for (size_t c = 0; c < N; ++c) if (IC[c] != -1) X0[c] = XW[c];
+  }
+  inline bool interior_c(size_t c) const {
+    int i = (int)(c % NI) + 1, j = (int)((c / NI) % NJ) + 1, k = (int)(c / ((size_t)NI * NJ)) + 1;
+    return interior(i, j, k);
+  }
+
+  // ||b - A x||_2 / ||b||_2 over INDC != -1 (diagnostic of the metric)
+  double true_relres(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
+                     const vd &AUJ, const vd &AUK, const vd &BB, const vd &X, const int *IC) {
+    double rn = gsum([&](int I, int J, int K, double &c) {
+      if (!interior(I, J, K)) return false;
+      size_t q = id(I, J, K);
+      if (IC[q] == -1) return false;
+      double ax = AD[q] * X[q] + ALI[q] * X[id(I - 1, J, K)] + ALJ[q] * X[id(I, J - 1, K)] +
+                  ALK[q] * X[id(I, J, K - 1)] + AUI[q] * X[id(I + 1, J, K)] + AUJ[q] * X[id(I, J + 1, K)] +
+                  AUK[q] * X[id(I, J, K + 1)];
+      double r = BB[q] - ax;
+      c = r * r;
+      return true;
+    });
+    double bn = gsum([&](int I, int J, int K, double &c) {
+      size_t q = id(I, J, K);
+      if (!interior(I, J, K) || IC[q] == -1) return false;
+      c = BB[q] * BB[q];
+      return true;
+    });
+    return bn > 0.0 ? std::sqrt(rn) / std::sqrt(bn) : 0.0;
+  }
+
+  // VF_VMODIF  vf_vmodif.f:58-215 (wave faces with matrix data not restated)
+  void vmodif(const vd &PT) {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          if (NF[id(I - 1, J, K)] * NF[id(I, J, K)] != 0) continue;
+          int IS = INDX[id(I, J, K)];
+          if (IS == 0) {
+            double GV = X_(6, I) * (X_(2, I) * GGV[id(I, J, K)] / GLV[id(I, J, K)] +
+                                    X_(2, I - 1) * GGV[id(I - 1, J, K)] / GLV[id(I - 1, J, K)]);
+            UU[id(I, J, K)] = UU[id(I, J, K)] + X_(5, I) * GV * (PT[id(I, J, K)] - PT[id(I - 1, J, K)]);
+          } else if (IS > 0 && IB_(3, IS) == 4) {
+            if (IB_(2, IS) == 1)
+              UU[id(I, J, K)] = UU[id(I, J, K)] + 2.0 * X_(4, I) * GGV[id(I, J, K)] / GLV[id(I, J, K)] * PT[id(I, J, K)];
+            else
+              UU[id(I, J, K)] = UU[id(I, J, K)] - 2.0 * X_(4, I - 1) * GGV[id(I - 1, J, K)] / GLV[id(I - 1, J, K)] * PT[id(I - 1, J, K)];
+            BCU[IS - 1] = UU[id(I, J, K)];
+          }
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (NF[id(I, J - 1, K)] * NF[id(I, J, K)] != 0) continue;
+          int IS = INDY[id(I, J, K)];
+          if (IS == 0) {
+            double GV = Y_(6, J) * (Y_(2, J) * GGV[id(I, J, K)] / GLV[id(I, J, K)] +
+                                    Y_(2, J - 1) * GGV[id(I, J - 1, K)] / GLV[id(I, J - 1, K)]);
+            VV[id(I, J, K)] = VV[id(I, J, K)] + Y_(5, J) * GV * (PT[id(I, J, K)] - PT[id(I, J - 1, K)]);
+          } else if (IS > 0 && IB_(3, IS) == 4) {
+            if (IB_(2, IS) == 3)
+              VV[id(I, J, K)] = VV[id(I, J, K)] + 2.0 * Y_(4, J) * GGV[id(I, J, K)] / GLV[id(I, J, K)] * PT[id(I, J, K)];
+            else
+              VV[id(I, J, K)] = VV[id(I, J, K)] - 2.0 * Y_(4, J - 1) * GGV[id(I, J - 1, K)] / GLV[id(I, J - 1, K)] * PT[id(I, J - 1, K)];
+            BCV[IS - 1] = VV[id(I, J, K)];
+          }
+        }
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (NF[id(I, J, K - 1)] * NF[id(I, J, K)] != 0) continue;
+          int IS = INDZ[id(I, J, K)];
+          if (IS == 0) {
+            double GV = Z_(6, K) * (Z_(2, K) * GGV[id(I, J, K)] / GLV[id(I, J, K)] +
+                                    Z_(2, K - 1) * GGV[id(I, J, K - 1)] / GLV[id(I, J, K - 1)]);
+            WW[id(I, J, K)] = WW[id(I, J, K)] + Z_(5, K) * GV * (PT[id(I, J, K)] - PT[id(I, J, K - 1)]);
+          } else if (IS > 0 && IB_(3, IS) == 4) {
+            if (IB_(2, IS) == 5)
+              WW[id(I, J, K)] = WW[id(I, J, K)] + 2.0 * Z_(4, K) * GGV[id(I, J, K)] / GLV[id(I, J, K)] * PT[id(I, J, K)];
+            else
+              WW[id(I, J, K)] = WW[id(I, J, K)] - 2.0 * Z_(4, K - 1) * GGV[id(I, J, K - 1)] / GLV[id(I, J, K - 1)] * PT[id(I, J, K - 1)];
+            BCW[IS - 1] = WW[id(I, J, K)];
+          }
+        }
+    const double RT = P.rho0 / DTNOW;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I)
+          if (INDC[id(I, J, K)] != -1) PP[id(I, J, K)] = PP[id(I, J, K)] - RT * PT[id(I, J, K)];
+  }
+
+  // VF_BSUWT  vf_bsuwt.f:41-470 (one axis; 'a' is the face array, the
+  // surface directions checked are the other two axes).
+  // Written out per axis below to keep the Fortran operand order.
+  void bsuwt() {
+    const int S0 = (P.ibsuw0 == 0);
+    // x faces
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 3; I <= NI - 1; ++I) {
+          if (INDX[id(I, J, K)] != 0) continue;
+          int I1 = I - 1, NL = NF[id(I1, J, K)], NR = NF[id(I, J, K)];
+          if (NL == 8 && NR == 8) { UU[id(I, J, K)] = 0.0; continue; }
+          if (!(NL != 0 && NR != 0)) continue;
+          double DL = 0, VL = 0, DR = 0, VR = 0, V0;
+          if (NL == 3 || NR == 3) {
+            V0 = UU[id(I, J - 1, K)];
+            if (S0) { int L1 = J - 1, L2 = J - 2;
+              if (NF[id(I1, L1, K)] != -1 && NF[id(I, L1, K)] != -1)
+                if (NF[id(I1, L2, K)] != -1 && NF[id(I, L2, K)] != -1)
+                  if (NF[id(I1, L2, K)] == 0 || NF[id(I, L2, K)] == 0)
+                    V0 = V0 + (V0 - UU[id(I, L2, K)]) * Y_(3, J) / Y_(3, L1); }
+            if (NL == 3) { DL = Y_(3, J); VL = V0; }
+            if (NR == 3) { DR = Y_(3, J); VR = V0; }
+          }
+          if (NL == 4 || NR == 4) {
+            V0 = UU[id(I, J + 1, K)];
+            if (S0) { int L1 = J + 1, L2 = J + 2;
+              if (NF[id(I1, L1, K)] != -1 && NF[id(I, L1, K)] != -1)
+                if (NF[id(I1, L2, K)] != -1 && NF[id(I, L2, K)] != -1)
+                  if (NF[id(I1, L2, K)] == 0 || NF[id(I, L2, K)] == 0)
+                    V0 = V0 + (V0 - UU[id(I, L2, K)]) * Y_(3, L1) / Y_(3, L2); }
+            if (NL == 4) { DL = Y_(3, J + 1); VL = V0; }
+            if (NR == 4) { DR = Y_(3, J + 1); VR = V0; }
+          }
+          if (NL == 5 || NR == 5) {
+            V0 = UU[id(I, J, K - 1)];
+            if (S0) { int L1 = K - 1, L2 = K - 2;
+              if (NF[id(I1, J, L1)] != -1 && NF[id(I, J, L1)] != -1)
+                if (NF[id(I1, J, L2)] != -1 && NF[id(I, J, L2)] != -1)
+                  if (NF[id(I1, J, L2)] == 0 || NF[id(I, J, L2)] == 0)
+                    V0 = V0 + (V0 - UU[id(I, J, L2)]) * Z_(3, K) / Z_(3, L1); }
+            if (NL == 5) { DL = Z_(3, K); VL = V0; }
+            if (NR == 5) { DR = Z_(3, K); VR = V0; }
+          }
+          if (NL == 6 || NR == 6) {
+            V0 = UU[id(I, J, K + 1)];
+            if (S0) { int L1 = K + 1, L2 = K + 2;
+              if (NF[id(I1, J, L1)] != -1 && NF[id(I, J, L1)] != -1)
+                if (NF[id(I1, J, L2)] != -1 && NF[id(I, J, L2)] != -1)
+                  if (NF[id(I1, J, L2)] == 0 || NF[id(I, J, L2)] == 0)
+                    V0 = V0 + (V0 - UU[id(I, J, L2)]) * Z_(3, L1) / Z_(3, L2); }
+            if (NL == 6) { DL = Z_(3, K + 1); VL = V0; }
+            if (NR == 6) { DR = Z_(3, K + 1); VR = V0; }
+          }
+          if (NL == 8) UU[id(I, J, K)] = VR;
+          else if (NR == 8) UU[id(I, J, K)] = VL;
+          else UU[id(I, J, K)] = (DR * VL + DL * VR) / (DR + DL);
+        }
+    // y faces
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 3; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (INDY[id(I, J, K)] != 0) continue;
+          int J1 = J - 1, NL = NF[id(I, J1, K)], NR = NF[id(I, J, K)];
+          if (NL == 8 && NR == 8) { VV[id(I, J, K)] = 0.0; continue; }
+          if (!(NL != 0 && NR != 0)) continue;
+          double DL = 0, VL = 0, DR = 0, VR = 0, V0;
+          if (NL == 1 || NR == 1) {
+            V0 = VV[id(I - 1, J, K)];
+            if (S0) { int L1 = I - 1, L2 = I - 2;
+              if (NF[id(L1, J1, K)] != -1 && NF[id(L1, J, K)] != -1)
+                if (NF[id(L2, J1, K)] != -1 && NF[id(L2, J, K)] != -1)
+                  if (NF[id(L2, J1, K)] == 0 || NF[id(L2, J, K)] == 0)
+                    V0 = V0 + (V0 - VV[id(L2, J, K)]) * X_(3, I) / X_(3, L1); }
+            if (NL == 1) { DL = X_(3, I); VL = V0; }
+            if (NR == 1) { DR = X_(3, I); VR = V0; }
+          }
+          if (NL == 2 || NR == 2) {
+            V0 = VV[id(I + 1, J, K)];
+            if (S0) { int L1 = I + 1, L2 = I + 2;
+              if (NF[id(L1, J1, K)] != -1 && NF[id(L1, J, K)] != -1)
+                if (NF[id(L2, J1, K)] != -1 && NF[id(L2, J, K)] != -1)
+                  if (NF[id(L2, J1, K)] == 0 || NF[id(L2, J, K)] == 0)
+                    V0 = V0 + (V0 - VV[id(L2, J, K)]) * X_(3, L1) / X_(3, L2); }
+            if (NL == 2) { DL = X_(3, I + 1); VL = V0; }
+            if (NR == 2) { DR = X_(3, I + 1); VR = V0; }
+          }
+          if (NL == 5 || NR == 5) {
+            V0 = VV[id(I, J, K - 1)];
+            if (S0) { int L1 = K - 1, L2 = K - 2;
+              if (NF[id(I, J1, L1)] != -1 && NF[id(I, J, L1)] != -1)
+                if (NF[id(I, J1, L2)] != -1 && NF[id(I, J, L2)] != -1)
+                  if (NF[id(I, J1, L2)] == 0 || NF[id(I, J, L2)] == 0)
+                    V0 = V0 + (V0 - VV[id(I, J, L2)]) * Z_(3, K) / Z_(3, L1); }
+            if (NL == 5) { DL = Z_(3, K); VL = V0; }
+            if (NR == 5) { DR = Z_(3, K); VR = V0; }
+          }
+          if (NL == 6 || NR == 6) {
+            V0 = VV[id(I, J, K + 1)];
+            if (S0) { int L1 = K + 1, L2 = K + 2;
+              if (NF[id(I, J1, L1)] != -1 && NF[id(I, J, L1)] != -1)
+                if (NF[id(I, J1, L2)] != -1 && NF[id(I, J, L2)] != -1)
+                  if (NF[id(I, J1, L2)] == 0 || NF[id(I, J, L2)] == 0)
+                    V0 = V0 + (V0 - VV[id(I, J, L2)]) * Z_(3, L1) / Z_(3, L2); }
+            if (NL == 6) { DL = Z_(3, K + 1); VL = V0; }
+            if (NR == 6) { DR = Z_(3, K + 1); VR = V0; }
+          }
+          if (NL == 8) VV[id(I, J, K)] = VR;
+          else if (NR == 8) VV[id(I, J, K)] = VL;
+          else VV[id(I, J, K)] = (DR * VL + DL * VR) / (DR + DL);
+        }
+    // z faces
+    for (int K = 3; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (INDZ[id(I, J, K)] != 0) continue;
+          int K1 = K - 1, NL = NF[id(I, J, K1)], NR = NF[id(I, J, K)];
+          if (NL == 8 && NR == 8) { WW[id(I, J, K)] = 0.0; continue; }
+          if (!(NL != 0 && NR != 0)) continue;
+          double DL = 0, VL = 0, DR = 0, VR = 0, V0;
+          if (NL == 1 || NR == 1) {
+            V0 = WW[id(I - 1, J, K)];
+            if (S0) { int L1 = I - 1, L2 = I - 2;
+              if (NF[id(L1, J, K1)] != -1 && NF[id(L1, J, K)] != -1)
+                if (NF[id(L2, J, K1)] != -1 && NF[id(L2, J, K)] != -1)
+                  if (NF[id(L2, J, K1)] == 0 || NF[id(L2, J, K)] == 0)
+                    V0 = V0 + (V0 - WW[id(L2, J, K)]) * X_(3, I) / X_(3, L1); }
+            if (NL == 1) { DL = X_(3, I); VL = V0; }
+            if (NR == 1) { DR = X_(3, I); VR = V0; }
+          }
+          if (NL == 2 || NR == 2) {
+            V0 = WW[id(I + 1, J, K)];
+            if (S0) { int L1 = I + 1, L2 = I + 2;
+              if (NF[id(L1, J, K1)] != -1 && NF[id(L1, J, K)] != -1)
+                if (NF[id(L2, J, K1)] != -1 && NF[id(L2, J, K)] != -1)
+                  if (NF[id(L2, J, K1)] == 0 || NF[id(L2, J, K)] == 0)
+                    V0 = V0 + (V0 - WW[id(L2, J, K)]) * X_(3, L1) / X_(3, L2); }
+            if (NL == 2) { DL = X_(3, I + 1); VL = V0; }
+            if (NR == 2) { DR = X_(3, I + 1); VR = V0; }
+          }
+          if (NL == 3 || NR == 3) {
+            V0 = WW[id(I, J - 1, K)];
+            if (S0) { int L1 = J - 1, L2 = J - 2;
+              if (NF[id(I, L1, K1)] != -1 && NF[id(I, L1, K)] != -1)
+                if (NF[id(I, L2, K1)] != -1 && NF[id(I, L2, K)] != -1)
+                  if (NF[id(I, L2, K1)] == 0 || NF[id(I, L2, K)] == 0)
+                    V0 = V0 + (V0 - WW[id(I, L2, K)]) * Y_(3, J) / Y_(3, L1); }
+            if (NL == 3) { DL = Y_(3, J); VL = V0; }
+            if (NR == 3) { DR = Y_(3, J); VR = V0; }
+          }
+          if (NL == 4 || NR == 4) {
+            V0 = WW[id(I, J + 1, K)];
+            if (S0) { int L1 = J + 1, L2 = J + 2;
+              if (NF[id(I, L1, K1)] != -1 && NF[id(I, L1, K)] != -1)
+                if (NF[id(I, L2, K1)] != -1 && NF[id(I, L2, K)] != -1)
+                  if (NF[id(I, L2, K1)] == 0 || NF[id(I, L2, K)] == 0)
+                    V0 = V0 + (V0 - WW[id(I, L2, K)]) * Y_(3, L1) / Y_(3, L2); }
+            if (NL == 4) { DL = Y_(3, J + 1); VL = V0; }
+            if (NR == 4) { DR = Y_(3, J + 1); VR = V0; }
+          }
+          if (NL == 8) WW[id(I, J, K)] = VR;
+          else if (NR == 8) WW[id(I, J, K)] = VL;
+          else WW[id(I, J, K)] = (DR * VL + DL * VR) / (DR + DL);
+        }
+  }
+
+  // VF_BSUWT2  vf_bsuwt2.f:36-107
+  void bsuwt2() {
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K;
+      decode(INDS[L], I, J, K);
+      int NF0 = NF[id(I, J, K)];
+      int L1, L2, LB;
+      if (NF0 == 5 || NF0 == 6) {
+        LB = (NF0 == 5) ? K - 1 : K + 1;
+        L1 = I; L2 = I;
+        if (NF[id(I - 1, J, K)] == 8 && INDX[id(I, J, LB)] != 0) L2 = L2 + 1;
+        if (NF[id(I + 1, J, K)] == 8 && INDX[id(I + 1, J, LB)] != 0) L1 = L1 + 1;
+        UU[id(L1, J, K)] = UU[id(L2, J, K)];
+        L1 = J; L2 = J;
+        if (NF[id(I, J - 1, K)] == 8 && INDY[id(I, J, LB)] != 0) L2 = L2 + 1;
+        if (NF[id(I, J + 1, K)] == 8 && INDY[id(I, J + 1, LB)] != 0) L1 = L1 + 1;
+        VV[id(I, L1, K)] = VV[id(I, L2, K)];
+      } else if (NF0 == 3 || NF0 == 4) {
+        LB = (NF0 == 3) ? J - 1 : J + 1;
+        L1 = I; L2 = I;
+        if (NF[id(I - 1, J, K)] == 8 && INDX[id(I, LB, K)] != 0) L2 = L2 + 1;
+        if (NF[id(I + 1, J, K)] == 8 && INDX[id(I + 1, LB, K)] != 0) L1 = L1 + 1;
+        UU[id(L1, J, K)] = UU[id(L2, J, K)];
+        L1 = K; L2 = K;
+        if (NF[id(I, J, K - 1)] == 8 && INDZ[id(I, LB, K)] != 0) L2 = L2 + 1;
+        if (NF[id(I, J, K + 1)] == 8 && INDZ[id(I, LB, K + 1)] != 0) L1 = L1 + 1;
+        WW[id(I, J, L1)] = WW[id(I, J, L2)];
+      } else if (NF0 == 1 || NF0 == 2) {
+        LB = (NF0 == 1) ? I - 1 : I + 1;
+        L1 = J; L2 = J;
+        if (NF[id(I, J - 1, K)] == 8 && INDY[id(LB, J, K)] != 0) L2 = L2 + 1;
+        if (NF[id(I, J + 1, K)] == 8 && INDY[id(LB, J + 1, K)] != 0) L1 = L1 + 1;
+        VV[id(I, L1, K)] = VV[id(I, L2, K)];
+        L1 = K; L2 = K;
+        if (NF[id(I, J, K - 1)] == 8 && INDZ[id(LB, J, K)] != 0) L2 = L2 + 1;
+        if (NF[id(I, J, K + 1)] == 8 && INDZ[id(LB, J, K + 1)] != 0) L1 = L1 + 1;
+        WW[id(I, J, L1)] = WW[id(I, J, L2)];
+      }
+    }
+  }
+
+  // VF_BSUWN  vf_bsuwn.f:57-86 (no wave source)
+  void bsuwn() {
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K;
+      decode(INDS[L], I, J, K);
+      int NF0 = NF[id(I, J, K)];
+      int I1 = I + 1, J1 = J + 1, K1 = K + 1;
+      double FXP = GGX[id(I1, J, K)] * UU[id(I1, J, K)], FXM = GGX[id(I, J, K)] * UU[id(I, J, K)];
+      double FYP = GGY[id(I, J1, K)] * VV[id(I, J1, K)], FYM = GGY[id(I, J, K)] * VV[id(I, J, K)];
+      double FZP = GGZ[id(I, J, K1)] * WW[id(I, J, K1)], FZM = GGZ[id(I, J, K)] * WW[id(I, J, K)];
+      if (NF0 == 5) WW[id(I, J, K1)] = (FZM - Z_(2, K) * (X_(4, I) * (FXP - FXM) + Y_(4, J) * (FYP - FYM))) / GGZ[id(I, J, K1)];
+      else if (NF0 == 6) WW[id(I, J, K)] = (FZP + Z_(2, K) * (X_(4, I) * (FXP - FXM) + Y_(4, J) * (FYP - FYM))) / GGZ[id(I, J, K)];
+      else if (NF0 == 3) VV[id(I, J1, K)] = (FYM - Y_(2, J) * (X_(4, I) * (FXP - FXM) + Z_(4, K) * (FZP - FZM))) / GGY[id(I, J1, K)];
+      else if (NF0 == 4) VV[id(I, J, K)] = (FYP + Y_(2, J) * (X_(4, I) * (FXP - FXM) + Z_(4, K) * (FZP - FZM))) / GGY[id(I, J, K)];
+      else if (NF0 == 1) UU[id(I1, J, K)] = (FXM - X_(2, I) * (Y_(4, J) * (FYP - FYM) + Z_(4, K) * (FZP - FZM))) / GGX[id(I1, J, K)];
+      else if (NF0 == 2) UU[id(I, J, K)] = (FXP + X_(2, I) * (Y_(4, J) * (FYP - FYM) + Z_(4, K) * (FZP - FZM))) / GGX[id(I, J, K)];
+    }
+  }
+
+  // VF_BSUWN3  vf_bsuwn3.f:37-340; written for the z case and mapped by
+  // a small accessor per axis so that every operand keeps its position.
+  void bsuwn3() {
+    const int S0 = (P.ibsuw0 == 0);
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K;
+      decode(INDS[L], I, J, K);
+      int NF0 = NF[id(I, J, K)];
+      int IS1 = 0, IS2 = 0, IS3 = 0, IS4 = 0;
+      double D0, V0, D1 = 0, V1 = 0, D2 = 0, V2 = 0, D3 = 0, V3 = 0, D4 = 0, V4 = 0;
+      auto lat = [&](int &isx, double &dx, double &vx, size_t a, size_t b, double d, double v) {
+        if (NF[a] == 0 || NF[b] == 0)
+          if (NF[a] != -1 && NF[b] != -1) { isx = 1; dx = d; vx = v; }
+      };
+      if (NF0 == 5) {
+        D0 = Z_(2, K); V0 = WW[id(I, J, K)]; int L1 = K + 1;
+        lat(IS1, D1, V1, id(I - 1, J, K), id(I - 1, J, L1), X_(3, I), WW[id(I - 1, J, L1)]);
+        lat(IS2, D2, V2, id(I + 1, J, K), id(I + 1, J, L1), X_(3, I + 1), WW[id(I + 1, J, L1)]);
+        lat(IS3, D3, V3, id(I, J - 1, K), id(I, J - 1, L1), Y_(3, J), WW[id(I, J - 1, L1)]);
+        lat(IS4, D4, V4, id(I, J + 1, K), id(I, J + 1, L1), Y_(3, J + 1), WW[id(I, J + 1, L1)]);
+        int ISS = IS1 + IS2 + IS3 + IS4;
+        if (ISS <= 0) {
+          if (S0 && NF[id(I, J, K - 2)] == 0) V0 = V0 + (V0 - WW[id(I, J, K - 1)]) * Z_(2, K) / Z_(2, K - 1);
+          WW[id(I, J, K + 1)] = V0;
+        } else {
+          double DS = D0 + D1 + D2 + D3 + D4;
+          WW[id(I, J, K + 1)] = ((DS - D0) * V0 + (DS - D1) * V1 + (DS - D2) * V2 + (DS - D3) * V3 + (DS - D4) * V4) / DS / (double)ISS;
+        }
+      } else if (NF0 == 6) {
+        D0 = Z_(2, K); V0 = WW[id(I, J, K + 1)]; int L1 = K - 1;
+        lat(IS1, D1, V1, id(I - 1, J, K), id(I - 1, J, L1), X_(3, I), WW[id(I - 1, J, K)]);
+        lat(IS2, D2, V2, id(I + 1, J, K), id(I + 1, J, L1), X_(3, I + 1), WW[id(I + 1, J, K)]);
+        lat(IS3, D3, V3, id(I, J - 1, K), id(I, J - 1, L1), Y_(3, J), WW[id(I, J - 1, K)]);
+        lat(IS4, D4, V4, id(I, J + 1, K), id(I, J + 1, L1), Y_(3, J + 1), WW[id(I, J + 1, K)]);
+        int ISS = IS1 + IS2 + IS3 + IS4;
+        if (ISS <= 0) {
+          if (S0 && NF[id(I, J, K + 2)] == 0) V0 = V0 + (V0 - WW[id(I, J, K + 2)]) * Z_(2, K) / Z_(2, K + 1);
+          WW[id(I, J, K)] = V0;
+        } else {
+          double DS = D0 + D1 + D2 + D3 + D4;
+          WW[id(I, J, K)] = ((DS - D0) * V0 + (DS - D1) * V1 + (DS - D2) * V2 + (DS - D3) * V3 + (DS - D4) * V4) / DS / (double)ISS;
+        }
+      } else if (NF0 == 3) {
+        D0 = Y_(2, J); V0 = VV[id(I, J, K)]; int L1 = J + 1;
+        lat(IS1, D1, V1, id(I - 1, J, K), id(I - 1, L1, K), X_(3, I), VV[id(I - 1, L1, K)]);
+        lat(IS2, D2, V2, id(I + 1, J, K), id(I + 1, L1, K), X_(3, I + 1), VV[id(I + 1, L1, K)]);
+        lat(IS3, D3, V3, id(I, J, K - 1), id(I, L1, K - 1), Z_(3, K), VV[id(I, L1, K - 1)]);
+        lat(IS4, D4, V4, id(I, J, K + 1), id(I, L1, K + 1), Z_(3, K + 1), VV[id(I, L1, K + 1)]);
+        int ISS = IS1 + IS2 + IS3 + IS4;
+        if (ISS <= 0) {
+          if (S0 && NF[id(I, J - 2, K)] == 0) V0 = V0 + (V0 - VV[id(I, J - 1, K)]) * Y_(2, J) / Y_(2, J - 1);
+          VV[id(I, J + 1, K)] = V0;
+        } else {
+          double DS = D0 + D1 + D2 + D3 + D4;
+          VV[id(I, J + 1, K)] = ((DS - D0) * V0 + (DS - D1) * V1 + (DS - D2) * V2 + (DS - D3) * V3 + (DS - D4) * V4) / DS / (double)ISS;
+        }
+      } else if (NF0 == 4) {
+        D0 = Y_(2, J); V0 = VV[id(I, J + 1, K)]; int L1 = J - 1;
+        lat(IS1, D1, V1, id(I - 1, J, K), id(I - 1, L1, K), X_(3, I), VV[id(I - 1, J, K)]);
+        lat(IS2, D2, V2, id(I + 1, J, K), id(I + 1, L1, K), X_(3, I + 1), VV[id(I + 1, J, K)]);
+        lat(IS3, D3, V3, id(I, J, K - 1), id(I, L1, K - 1), Z_(3, K), VV[id(I, J, K - 1)]);
+        lat(IS4, D4, V4, id(I, J, K + 1), id(I, L1, K + 1), Z_(3, K + 1), VV[id(I, J, K + 1)]);
+        int ISS = IS1 + IS2 + IS3 + IS4;
+        if (ISS <= 0) {
+          if (S0 && NF[id(I, J + 2, K)] == 0) V0 = V0 + (V0 - VV[id(I, J + 2, K)]) * Y_(2, J) / Y_(2, J + 1);
+          VV[id(I, J, K)] = V0;
+        } else {
+          double DS = D0 + D1 + D2 + D3 + D4;
+          VV[id(I, J, K)] = ((DS - D0) * V0 + (DS - D1) * V1 + (DS - D2) * V2 + (DS - D3) * V3 + (DS - D4) * V4) / DS / (double)ISS;
+        }
+      } else if (NF0 == 1) {
+        D0 = X_(2, I); V0 = UU[id(I, J, K)]; int L1 = I + 1;
+        lat(IS1, D1, V1, id(I, J - 1, K), id(L1, J - 1, K), Y_(3, J), UU[id(L1, J - 1, K)]);
+        lat(IS2, D2, V2, id(I, J + 1, K), id(L1, J + 1, K), Y_(3, J + 1), UU[id(L1, J + 1, K)]);
+        lat(IS3, D3, V3, id(I, J, K - 1), id(L1, J, K - 1), Z_(3, K), UU[id(L1, J, K - 1)]);
+        lat(IS4, D4, V4, id(I, J, K + 1), id(L1, J, K + 1), Z_(3, K + 1), UU[id(L1, J, K + 1)]);
+        int ISS = IS1 + IS2 + IS3 + IS4;
+        if (ISS <= 0) {
+          if (S0 && NF[id(I - 2, J, K)] == 0) V0 = V0 + (V0 - UU[id(I - 1, J, K)]) * X_(2, I) / X_(2, I - 1);
+          UU[id(I + 1, J, K)] = V0;
+        } else {
+          double DS = D0 + D1 + D2 + D3 + D4;
+          UU[id(I + 1, J, K)] = ((DS - D0) * V0 + (DS - D1) * V1 + (DS - D2) * V2 + (DS - D3) * V3 + (DS - D4) * V4) / DS / (double)ISS;
+        }
+      } else if (NF0 == 2) {
+        D0 = X_(2, I); V0 = UU[id(I + 1, J, K)]; int L1 = I - 1;
+        lat(IS1, D1, V1, id(I, J - 1, K), id(L1, J - 1, K), Y_(3, J), UU[id(I, J - 1, K)]);
+        lat(IS2, D2, V2, id(I, J + 1, K), id(L1, J + 1, K), Y_(3, J + 1), UU[id(I, J + 1, K)]);
+        lat(IS3, D3, V3, id(I, J, K - 1), id(L1, J, K - 1), Z_(3, K), UU[id(I, J, K - 1)]);
+        lat(IS4, D4, V4, id(I, J, K + 1), id(L1, J, K + 1), Z_(3, K + 1), UU[id(I, J, K + 1)]);
+        int ISS = IS1 + IS2 + IS3 + IS4;
+        if (ISS <= 0) {
+          if (S0 && NF[id(I + 2, J, K)] == 0) V0 = V0 + (V0 - UU[id(I + 2, J, K)]) * X_(2, I) / X_(2, I + 1);
+          UU[id(I, J, K)] = V0;
+        } else {
+          double DS = D0 + D1 + D2 + D3 + D4;
+          UU[id(I, J, K)] = ((DS - D0) * V0 + (DS - D1) * V1 + (DS - D2) * V2 + (DS - D3) * V3 + (DS - D4) * V4) / DS / (double)ISS;
+        }
+      }
+    }
+  }
+
+  // VF_BWUWT  vf_bwuwt.f:41-118 (slip/free, no-slip, fixed; wave faces
+  // without matrix data and radiation faces untouched)
+  void bwuwt() {
+    for (int L = 1; L <= NB; ++L) {
+      int I, J, K;
+      decode(IB_(1, L), I, J, K);
+      int NS = IB_(2, L), IB = IB_(3, L);
+      if (IB == 1 || IB == 4) {
+        if (NS == 1) { BCV[L - 1] = (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5; }
+        else if (NS == 2) { BCV[L - 1] = (VV[id(I - 1, J, K)] + VV[id(I - 1, J + 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I - 1, J, K)] + WW[id(I - 1, J, K + 1)]) * 0.5; }
+        else if (NS == 3) { BCU[L - 1] = (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5; }
+        else if (NS == 4) { BCU[L - 1] = (UU[id(I, J - 1, K)] + UU[id(I + 1, J - 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J - 1, K)] + WW[id(I, J - 1, K + 1)]) * 0.5; }
+        else if (NS == 5) { BCU[L - 1] = (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5; BCV[L - 1] = (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5; }
+        else if (NS == 6) { BCU[L - 1] = (UU[id(I, J, K - 1)] + UU[id(I + 1, J, K - 1)]) * 0.5; BCV[L - 1] = (VV[id(I, J, K - 1)] + VV[id(I, J + 1, K - 1)]) * 0.5; }
+      }
+    }
+  }
+  // VF_BWPP  vf_bwpp.f:28-51
+  void bwpp() {
+    for (int L = 1; L <= NB; ++L) {
+      int I, J, K;
+      decode(IB_(1, L), I, J, K);
+      int NS = IB_(2, L);
+      if (NS == 1) BCP[L - 1] = PP[id(I, J, K)];
+      else if (NS == 2) BCP[L - 1] = PP[id(I - 1, J, K)];
+      else if (NS == 3) BCP[L - 1] = PP[id(I, J, K)];
+      else if (NS == 4) BCP[L - 1] = PP[id(I, J - 1, K)];
+      else if (NS == 5) BCP[L - 1] = PP[id(I, J, K)];
+      else if (NS == 6) BCP[L - 1] = PP[id(I, J, K - 1)];
+    }
+  }
+
+  // ---------------------------------------------------------------- VOF
+  // VF_FCONV  vf_fconv.f:56-206
+  void fconv(vd &FLFU, vd &FLFV, vd &FLFW) {
+    const double DT = DTNOW, FL = P.flower;
+    auto face = [&](double C, int N, double FDa, int ndm, double FDMa, double Vd, double Vo, double bcf,
+                    int na, double FAa, int dirA, int dirB, int dirC, int dirD, double &FL_, int &lim) {
+      (void)dirA;
+      double AC = std::fabs(C), FD, FDMW, V, FA;
+      if (N != -1) { FD = FDa; FDMW = 1.0; if (ndm != -1) FDMW = FDMa; V = Vd; }
+      else { FD = bcf; FDMW = 1.0; V = Vo; }
+      FA = (na != -1) ? FAa : FD;
+      double FAD = FA;
+      if (N == -1 || N == dirA || N == dirB || N == dirC || N == dirD)
+        if (FDMW != 0.0 && FA != 0.0) FAD = FD;
+      double FDM = dmax(FDMW, FD);
+      if (FDMW < FL && FA < FL) FDM = dmax(FDM, 0.1);
+      double CFX = dmax((FDM - FAD) * AC - (FDM - FD) * V, 0.0);
+      double FVX = FAD * AC + CFX;
+      double FVM = FD * V;
+      FL_ = dmin(FVX, FVM);
+      lim = (FVX > FVM);
+    };
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          if (INDX[id(I, J, K)] == -1) continue;
+          double C = DT * GGX[id(I, J, K)] * UU[id(I, J, K)];
+          int LSN, LA, LD, LDM;
+          if (C >= 0.0) { LSN = 1; LA = I; LD = I - 1; LDM = I - 2; } else { LSN = -1; LA = I - 1; LD = I; LDM = I + 1; }
+          int N = NF[id(LD, J, K)];
+          int ndm = (N != -1) ? NF[id(LDM, J, K)] : -1;
+          double fdm = (N != -1 && ndm != -1) ? FF[id(LDM, J, K)] : 0.0;
+          double vd_ = (N != -1) ? X_(2, LD) * GGV[id(LD, J, K)] : 0.0;
+          double bcf = (N == -1) ? BCF[INDX[id(I, J, K)] - 1] : 0.0;
+          int na = NF[id(LA, J, K)];
+          double fl; int lim;
+          face(C, N, (N != -1) ? FF[id(LD, J, K)] : 0.0, ndm, fdm, vd_, X_(2, LD), bcf, na,
+               (na != -1) ? FF[id(LA, J, K)] : 0.0, 3, 4, 5, 6, fl, lim);
+          FLFU[id(I, J, K)] = FLFU[id(I, J, K)] - (double)LSN * fl;
+          if (lim) NLIM[id(LD, J, K)] = 1;
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (INDY[id(I, J, K)] == -1) continue;
+          double C = DT * GGY[id(I, J, K)] * VV[id(I, J, K)];
+          int LSN, LA, LD, LDM;
+          if (C >= 0.0) { LSN = 1; LA = J; LD = J - 1; LDM = J - 2; } else { LSN = -1; LA = J - 1; LD = J; LDM = J + 1; }
+          int N = NF[id(I, LD, K)];
+          int ndm = (N != -1) ? NF[id(I, LDM, K)] : -1;
+          double fdm = (N != -1 && ndm != -1) ? FF[id(I, LDM, K)] : 0.0;
+          double vd_ = (N != -1) ? Y_(2, LD) * GGV[id(I, LD, K)] : 0.0;
+          double bcf = (N == -1) ? BCF[INDY[id(I, J, K)] - 1] : 0.0;
+          int na = NF[id(I, LA, K)];
+          double fl; int lim;
+          face(C, N, (N != -1) ? FF[id(I, LD, K)] : 0.0, ndm, fdm, vd_, Y_(2, LD), bcf, na,
+               (na != -1) ? FF[id(I, LA, K)] : 0.0, 1, 2, 5, 6, fl, lim);
+          FLFV[id(I, J, K)] = FLFV[id(I, J, K)] - (double)LSN * fl;
+          if (lim) NLIM[id(I, LD, K)] = 1;
+        }
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (INDZ[id(I, J, K)] == -1) continue;
+          double C = DT * GGZ[id(I, J, K)] * WW[id(I, J, K)];
+          int LSN, LA, LD, LDM;
+          if (C >= 0.0) { LSN = 1; LA = K; LD = K - 1; LDM = K - 2; } else { LSN = -1; LA = K - 1; LD = K; LDM = K + 1; }
+          int N = NF[id(I, J, LD)];
+          int ndm = (N != -1) ? NF[id(I, J, LDM)] : -1;
+          double fdm = (N != -1 && ndm != -1) ? FF[id(I, J, LDM)] : 0.0;
+          double vd_ = (N != -1) ? Z_(2, LD) * GGV[id(I, J, LD)] : 0.0;
+          double bcf = (N == -1) ? BCF[INDZ[id(I, J, K)] - 1] : 0.0;
+          int na = NF[id(I, J, LA)];
+          double fl; int lim;
+          face(C, N, (N != -1) ? FF[id(I, J, LD)] : 0.0, ndm, fdm, vd_, Z_(2, LD), bcf, na,
+               (na != -1) ? FF[id(I, J, LA)] : 0.0, 1, 2, 3, 4, fl, lim);
+          FLFW[id(I, J, K)] = FLFW[id(I, J, K)] - (double)LSN * fl;
+          if (lim) NLIM[id(I, J, LD)] = 1;
+        }
+  }
+
+  // VF_FEULER  vf_feuler.f:43-56 (QF = 0, GGV0 = GGV, LOOPS = 1)
+  void feuler(const vd &FLFU, const vd &FLFV, const vd &FLFW) {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] == -1) continue;
+          double G0 = GGV[c] - (GGV[c] - GGV[c]) * 1.0;
+          double DF = (X_(4, I) * (FLFU[id(I + 1, J, K)] - FLFU[c]) + Y_(4, J) * (FLFV[id(I, J + 1, K)] - FLFV[c]) +
+                       Z_(4, K) * (FLFW[id(I, J, K + 1)] - FLFW[c]) + DTNOW * 0.0);
+          FF[c] = (G0 * FF[c] + DF) / GGV[c];
+        }
+  }
+
+  // VF_FMOD1  vf_fmod1.f:37-200
+  void fmod1() {
+    std::fill(NLIM.begin(), NLIM.end(), 0);
+    auto ends = [&](int I, int J, int K, int N, int &IE, int &JE, int &KE, int &IF, int &JF, int &KF) {
+      IE = I; JE = J; KE = K; IF = I; JF = J; KF = K;
+      if (N == 5) { KE = K + 1; KF = K - 1; }
+      else if (N == 6) { KE = K - 1; KF = K + 1; }
+      else if (N == 3) { JE = J + 1; JF = J - 1; }
+      else if (N == 4) { JE = J - 1; JF = J + 1; }
+      else if (N == 1) { IE = I + 1; IF = I - 1; }
+      else if (N == 2) { IE = I - 1; IF = I + 1; }
+    };
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K, IE, JE, KE, IF, JF, KF;
+      decode(INDS[L], I, J, K);
+      ends(I, J, K, NF[id(I, J, K)], IE, JE, KE, IF, JF, KF);
+      NLIM[id(IE, JE, KE)] += 1;
+      NLIM[id(IF, JF, KF)] += 1;
+    }
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K, IE, JE, KE, IF, JF, KF;
+      decode(INDS[L], I, J, K);
+      ends(I, J, K, NF[id(I, J, K)], IE, JE, KE, IF, JF, KF);
+      size_t e = id(IE, JE, KE), s = id(I, J, K), f = id(IF, JF, KF);
+      double VE = X_(2, IE) * Y_(2, JE) * Z_(2, KE) * GGV[e];
+      double VS = X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[s];
+      double VF = X_(2, IF) * Y_(2, JF) * Z_(2, KF) * GGV[f];
+      double SS = VS * FF[s];
+      if (NLIM[e] == 1) SS = SS + VE * FF[e];
+      if (NLIM[f] == 1) SS = SS + VF * FF[f];
+      double DS;
+      if (NLIM[f] == 1) { DS = dmin(VF, SS); SS = SS - DS; FF[f] = DS / VF; }
+      DS = dmin(VS, SS); SS = SS - DS; FF[s] = DS / VS;
+      if (NLIM[e] == 1) { DS = dmin(VE, SS); SS = SS - DS; FF[e] = DS / VE; }
+      if (SS > 0.0) {
+        if (NLIM[e] == 1) FF[e] = FF[e] + SS / VE;
+        else FF[s] = FF[s] + SS / VS;
+      }
+    }
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K, IE, JE, KE, IF, JF, KF;
+      decode(INDS[L], I, J, K);
+      ends(I, J, K, NF[id(I, J, K)], IE, JE, KE, IF, JF, KF);
+      size_t e = id(IE, JE, KE), s = id(I, J, K), f = id(IF, JF, KF);
+      double VE = X_(2, IE) * Y_(2, JE) * Z_(2, KE) * GGV[e];
+      double VS = X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[s];
+      double VF = X_(2, IF) * Y_(2, JF) * Z_(2, KF) * GGV[f];
+      if (FF[s] > 1.0) { FF[e] = FF[e] + VS * (FF[s] - 1.0) / VE; FF[s] = 1.0; }
+      if (FF[s] < 0.0) { FF[f] = FF[f] + VS * FF[s] / VF; FF[s] = 0.0; }
+    }
+  }
+
+  // VF_FCUT01  vf_fcut01.f:34-56; in GPU order the cut-off of each cell is
+  // applied first and both sums use the row tree.
+  void fcut01(double &FSUM, double &FCUT) {
+    if (sum_mode == ORC_SUM_REF) {
+      FSUM = 0.0; FCUT = 0.0;
+      for (int K = 2; K <= NK - 1; ++K)
+        for (int J = 2; J <= NJ - 1; ++J)
+          for (int I = 2; I <= NI - 1; ++I) {
+            size_t c = id(I, J, K);
+            if (NF[c] == -1) continue;
+            double V = X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[c];
+            if (FF[c] > P.fupper) { FCUT = FCUT + (FF[c] - 1.0) * V; FF[c] = 1.0; }
+            else if (FF[c] < P.flower) { FCUT = FCUT + (FF[c] - 0.0) * V; FF[c] = 0.0; }
+            FSUM = FSUM + FF[c] * V;
+          }
+      return;
+    }
+    vd cut(FF.size(), 0.0);
+    std::vector<char> hc(FF.size(), 0);
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] == -1) continue;
+          double V = X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[c];
+          if (FF[c] > P.fupper) { cut[c] = (FF[c] - 1.0) * V; hc[c] = 1; FF[c] = 1.0; }
+          else if (FF[c] < P.flower) { cut[c] = (FF[c] - 0.0) * V; hc[c] = 1; FF[c] = 0.0; }
+        }
+    FCUT = gsum([&](int I, int J, int K, double &c) {
+      size_t q = id(I, J, K);
+      if (!interior(I, J, K) || NF[q] == -1 || !hc[q]) return false;
+      c = cut[q]; return true;
+    });
+    FSUM = gsum([&](int I, int J, int K, double &c) {
+      size_t q = id(I, J, K);
+      if (!interior(I, J, K) || NF[q] == -1) return false;
+      double V = X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[q];
+      c = FF[q] * V; return true;
+    });
+  }
+
+  // VF_BWFF  vf_bwff.f:31-89
+  int bwff() {
+    for (int L = 1; L <= NB; ++L) {
+      int I, J, K;
+      decode(IB_(1, L), I, J, K);
+      int NS = IB_(2, L), IB = IB_(4, L);
+      if (IB == 1) {
+      } else if (IB == 2 || IB == 5 || IB == 7) {
+        if (NS == 1) BCF[L - 1] = FF[id(I, J, K)];
+        else if (NS == 2) BCF[L - 1] = FF[id(I - 1, J, K)];
+        else if (NS == 3) BCF[L - 1] = FF[id(I, J, K)];
+        else if (NS == 4) BCF[L - 1] = FF[id(I, J - 1, K)];
+        else if (IB == 2 && NS == 5) BCF[L - 1] = FF[id(I, J, K)];
+        else if (IB == 2 && NS == 6) BCF[L - 1] = FF[id(I, J, K - 1)];
+        else return CADMAS_EPG;
+      } else return CADMAS_EPG;
+    }
+    return CADMAS_OK;
+  }
+
+  // VF_BSUWEM  vf_bsuwem.f:37-103
+  void bsuwem() {
+    std::fill(NLIM.begin(), NLIM.end(), 0);
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K;
+      decode(INDS[L], I, J, K);
+      int N = NF[id(I, J, K)];
+      if (N == 5 || N == 6) { NLIM[id(I + 1, J, K)]++; NLIM[id(I - 1, J, K)]++; NLIM[id(I, J + 1, K)]++; NLIM[id(I, J - 1, K)]++; }
+      else if (N == 3 || N == 4) { NLIM[id(I + 1, J, K)]++; NLIM[id(I - 1, J, K)]++; NLIM[id(I, J, K + 1)]++; NLIM[id(I, J, K - 1)]++; }
+      else { NLIM[id(I, J + 1, K)]++; NLIM[id(I, J - 1, K)]++; NLIM[id(I, J, K + 1)]++; NLIM[id(I, J, K - 1)]++; }
+    }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (!(NLIM[id(I, J, K)] >= 2 && NF[id(I, J, K)] == 8)) continue;
+          if (NF[id(I - 1, J, K)] == 8 && NLIM[id(I - 1, J, K)] < 2)
+            if (NF[id(I + 1, J, K)] != 8) UU[id(I, J, K)] = UU[id(I + 1, J, K)];
+          if (NF[id(I + 1, J, K)] == 8 && NLIM[id(I + 1, J, K)] < 2)
+            if (NF[id(I - 1, J, K)] != 8) UU[id(I + 1, J, K)] = UU[id(I, J, K)];
+          if (NF[id(I, J - 1, K)] == 8 && NLIM[id(I, J - 1, K)] < 2)
+            if (NF[id(I, J + 1, K)] != 8) VV[id(I, J, K)] = VV[id(I, J + 1, K)];
+          if (NF[id(I, J + 1, K)] == 8 && NLIM[id(I, J + 1, K)] < 2)
+            if (NF[id(I, J - 1, K)] != 8) VV[id(I, J + 1, K)] = VV[id(I, J, K)];
+          if (NF[id(I, J, K - 1)] == 8 && NLIM[id(I, J, K - 1)] < 2)
+            if (NF[id(I, J, K + 1)] != 8) WW[id(I, J, K)] = WW[id(I, J, K + 1)];
+          if (NF[id(I, J, K + 1)] == 8 && NLIM[id(I, J, K + 1)] < 2)
+            if (NF[id(I, J, K - 1)] != 8) WW[id(I, J, K + 1)] = WW[id(I, J, K)];
+        }
+  }
+
+  // VF_FNFINI  vf_fnfini.f:36-197
+  int fnfini() {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 1; J <= NJ; ++J)
+        for (int I = 1; I <= NI; ++I)
+          if (NF[id(I, J, K)] != -1) NF[id(I, J, K)] = 0;
+    const double FU = P.fupper;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] == -1 || !(FF[c] < P.flower)) continue;
+          int IX1 = INDX[c], IX2 = INDX[id(I + 1, J, K)], IY1 = INDY[c], IY2 = INDY[id(I, J + 1, K)];
+          int IZ1 = INDZ[c], IZ2 = INDZ[id(I, J, K + 1)];
+          double FX1 = IX1 >= 1 ? BCF[IX1 - 1] : FF[id(I - 1, J, K)];
+          double FX2 = IX2 >= 1 ? BCF[IX2 - 1] : FF[id(I + 1, J, K)];
+          double FY1 = IY1 >= 1 ? BCF[IY1 - 1] : FF[id(I, J - 1, K)];
+          double FY2 = IY2 >= 1 ? BCF[IY2 - 1] : FF[id(I, J + 1, K)];
+          double FZ1 = IZ1 >= 1 ? BCF[IZ1 - 1] : FF[id(I, J, K - 1)];
+          double FZ2 = IZ2 >= 1 ? BCF[IZ2 - 1] : FF[id(I, J, K + 1)];
+          if (!(FZ1 > FU && IZ1 == 0) && !(FY1 > FU && IY1 == 0) && !(FY2 > FU && IY2 == 0) &&
+              !(FX1 > FU && IX1 == 0) && !(FX2 > FU && IX2 == 0) && !(FZ2 > FU && IZ2 == 0))
+            NF[c] = 8;
+        }
+    const int ICAP = 100000;
+    for (int ITER = 1;; ++ITER) {
+      if (ITER > ICAP) return CADMAS_ECAP;
+      int NS = 0;
+      INDS.clear();
+      for (int K = 2; K <= NK - 1; ++K)
+        for (int J = 2; J <= NJ - 1; ++J)
+          for (int I = 2; I <= NI - 1; ++I) {
+            size_t c = id(I, J, K);
+            if (NF[c] == -1 || NF[c] == 8) continue;
+            if (NF[id(I, J, K + 1)] == 8 || NF[id(I, J + 1, K)] == 8 || NF[id(I, J - 1, K)] == 8 ||
+                NF[id(I + 1, J, K)] == 8 || NF[id(I - 1, J, K)] == 8 || NF[id(I, J, K - 1)] == 8) {
+              NS++;
+              INDS.push_back(I + NI * (J - 1) + NI * NJ * (K - 1));
+              NF[c] = 7;
+            }
+          }
+      std::vector<int> keep;
+      for (int L = 0; L < NS; ++L) {
+        int I, J, K;
+        decode(INDS[L], I, J, K);
+        if (NF[id(I, J, K + 1)] != 0 && NF[id(I, J + 1, K)] != 0 && NF[id(I, J - 1, K)] != 0 &&
+            NF[id(I + 1, J, K)] != 0 && NF[id(I - 1, J, K)] != 0 && NF[id(I, J, K - 1)] != 0)
+          NF[id(I, J, K)] = 8;
+        else keep.push_back(INDS[L]);
+      }
+      INDS = keep;
+      NUMS = (int)INDS.size();
+      int NCH = 0;
+      for (int L = 0; L < NUMS; ++L) {
+        int I, J, K;
+        decode(INDS[L], I, J, K);
+        auto nf = [&](int a, int b, int c) { return NF[id(a, b, c)]; };
+        if (nf(I, J, K - 1) != 0 || nf(I, J, K + 1) != 8)
+          if (nf(I - 1, J, K) != 0 || nf(I + 1, J, K) != 8)
+            if (nf(I + 1, J, K) != 0 || nf(I - 1, J, K) != 8)
+              if (nf(I, J - 1, K) != 0 || nf(I, J + 1, K) != 8)
+                if (nf(I, J + 1, K) != 0 || nf(I, J - 1, K) != 8)
+                  if (nf(I, J, K + 1) != 0 || nf(I, J, K - 1) != 8) { NF[id(I, J, K)] = -7; NCH++; }
+      }
+      if (NCH <= 0) break;
+      for (int L = 0; L < NUMS; ++L) {
+        int I, J, K;
+        decode(INDS[L], I, J, K);
+        if (NF[id(I, J, K)] == -7) NF[id(I, J, K)] = 8;
+      }
+    }
+    return CADMAS_OK;
+  }
+
+  // VF_FBUBUP  vf_fbubup.f:35-51
+  void fbubup() {
+    for (int K = NK - 2; K >= 2; --K) {
+      double DTBUB = Z_(2, K) / P.wbub;
+      if (!(TNOW - TBUB[K - 1] > DTBUB)) continue;
+      int K1 = K + 1;
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K), u = id(I, J, K1);
+          if (FF[c] < P.fupper && NF[c] == 0 && NF[u] != -1) {
+            double V0 = Z_(2, K) * GGV[c], V1 = Z_(2, K1) * GGV[u];
+            double FMOVE = dmin((1.0 - FF[c]) * V0, FF[u] * V1);
+            FF[u] = FF[u] - FMOVE / V1;
+            FF[c] = FF[c] + FMOVE / V0;
+          }
+        }
+      TBUB[K - 1] = TBUB[K - 1] + DTBUB;
+    }
+  }
+
+  // VF_FNFPRV  vf_fnfprv.f:34-225
+  int fnfprv() {
+    for (int L = 0; L < NUMS; ++L) {
+      int I, J, K;
+      decode(INDS[L], I, J, K);
+      size_t c = id(I, J, K);
+      double FM = -1.0, FS;
+      auto bf = [&](int ind, double f) { return ind >= 1 ? BCF[ind - 1] : f; };
+      int KB = K - 1;
+      if (NF[id(I, J, KB)] == 0 && NF[id(I, J, K + 1)] == 8) {
+        FS = 2.0 * FF[id(I, J, KB)];
+        FS = FS + bf(INDX[id(I, J, KB)], FF[id(I - 1, J, KB)]);
+        FS = FS + bf(INDX[id(I + 1, J, KB)], FF[id(I + 1, J, KB)]);
+        FS = FS + bf(INDY[id(I, J, KB)], FF[id(I, J - 1, KB)]);
+        FS = FS + bf(INDY[id(I, J + 1, KB)], FF[id(I, J + 1, KB)]);
+        if (FS > FM) { NF[c] = 5; FM = FS; }
+      }
+      KB = K + 1;
+      if (NF[id(I, J, KB)] == 0 && NF[id(I, J, K - 1)] == 8) {
+        FS = 2.0 * FF[id(I, J, KB)];
+        FS = FS + bf(INDX[id(I, J, KB)], FF[id(I - 1, J, KB)]);
+        FS = FS + bf(INDX[id(I + 1, J, KB)], FF[id(I + 1, J, KB)]);
+        FS = FS + bf(INDY[id(I, J, KB)], FF[id(I, J - 1, KB)]);
+        FS = FS + bf(INDY[id(I, J + 1, KB)], FF[id(I, J + 1, KB)]);
+        if (FS > FM) { NF[c] = 6; FM = FS; }
+      }
+      int JB = J - 1;
+      if (NF[id(I, JB, K)] == 0 && NF[id(I, J + 1, K)] == 8) {
+        FS = 2.0 * FF[id(I, JB, K)];
+        FS = FS + bf(INDX[id(I, JB, K)], FF[id(I - 1, JB, K)]);
+        FS = FS + bf(INDX[id(I + 1, JB, K)], FF[id(I + 1, JB, K)]);
+        FS = FS + bf(INDZ[id(I, JB, K)], FF[id(I, JB, K - 1)]);
+        FS = FS + bf(INDZ[id(I, JB, K + 1)], FF[id(I, JB, K + 1)]);
+        if (FS > FM) { NF[c] = 3; FM = FS; }
+      }
+      JB = J + 1;
+      if (NF[id(I, JB, K)] == 0 && NF[id(I, J - 1, K)] == 8) {
+        FS = 2.0 * FF[id(I, JB, K)];
+        FS = FS + bf(INDX[id(I, JB, K)], FF[id(I - 1, JB, K)]);
+        FS = FS + bf(INDX[id(I + 1, JB, K)], FF[id(I + 1, JB, K)]);
+        FS = FS + bf(INDZ[id(I, JB, K)], FF[id(I, JB, K - 1)]);
+        FS = FS + bf(INDZ[id(I, JB, K + 1)], FF[id(I, JB, K + 1)]);
+        if (FS > FM) { NF[c] = 4; FM = FS; }
+      }
+      int IB = I - 1;
+      if (NF[id(IB, J, K)] == 0 && NF[id(I + 1, J, K)] == 8) {
+        FS = 2.0 * FF[id(IB, J, K)];
+        FS = FS + bf(INDY[id(IB, J, K)], FF[id(IB, J - 1, K)]);
+        FS = FS + bf(INDY[id(IB, J + 1, K)], FF[id(IB, J + 1, K)]);
+        FS = FS + bf(INDZ[id(IB, J, K)], FF[id(IB, J, K - 1)]);
+        FS = FS + bf(INDZ[id(IB, J, K + 1)], FF[id(IB, J, K + 1)]);
+        if (FS > FM) { NF[c] = 1; FM = FS; }
+      }
+      IB = I + 1;
+      if (NF[id(IB, J, K)] == 0 && NF[id(I - 1, J, K)] == 8) {
+        FS = 2.0 * FF[id(IB, J, K)];
+        FS = FS + bf(INDY[id(IB, J, K)], FF[id(IB, J - 1, K)]);
+        FS = FS + bf(INDY[id(IB, J + 1, K)], FF[id(IB, J + 1, K)]);
+        FS = FS + bf(INDZ[id(IB, J, K)], FF[id(IB, J, K - 1)]);
+        FS = FS + bf(INDZ[id(IB, J, K + 1)], FF[id(IB, J, K + 1)]);
+        if (FS > FM) { NF[c] = 2; FM = FS; }
+      }
+      if (NF[c] == 7) return CADMAS_EPG;
+    }
+    return CADMAS_OK;
+  }
+
+  // VF_CINDC  vf_cindc.f:35-53
+  void cindc() {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          int n = NF[id(I, J, K)];
+          INDC[id(I, J, K)] = (n == 8 || n == -1) ? -1 : 0;
+        }
+  }
+
+  // VF_BSPPFL  vf_bsppfl.f:40-67 (NF0 = NF before FNFINI, kept in NLIM)
+  void bsppfl() {
+    vd PP0 = PP;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (!(NF[id(I, J, K)] == 0 && NLIM[id(I, J, K)] == 8)) continue;
+          double SUMF = 0.0, SUMP = 0.0;
+          for (int KP = -1; KP <= 1; ++KP)
+            for (int JP = -1; JP <= 1; ++JP)
+              for (int IP = -1; IP <= 1; ++IP) {
+                size_t q = id(I + IP, J + JP, K + KP);
+                if (NF[q] == 0) { double F = FF[q]; SUMF = SUMF + F; SUMP = SUMP + F * PP0[q]; }
+              }
+          PP[id(I, J, K)] = (SUMF < 1.0e-20) ? 0.0 : SUMP / SUMF;
+        }
+  }
+
+  // VF_BSPP  vf_bspp.f:33-61 (PVCP0 < 0)
+  void bspp() {
+    const double PPS = 0.0;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          int n = NF[c];
+          double PSI;
+          if (n == 8) PP[c] = 0.0;
+          else if (n == 5) { PSI = Z_(3, K) / (0.5 * Z_(2, K - 1) + FF[c] * Z_(2, K)); PP[c] = (1.0 - PSI) * PP[id(I, J, K - 1)] + PSI * PPS; }
+          else if (n == 6) { PSI = Z_(3, K + 1) / (0.5 * Z_(2, K + 1) + FF[c] * Z_(2, K)); PP[c] = (1.0 - PSI) * PP[id(I, J, K + 1)] + PSI * PPS; }
+          else if (n == 3) { PSI = Y_(3, J) / (0.5 * Y_(2, J - 1) + FF[c] * Y_(2, J)); PP[c] = (1.0 - PSI) * PP[id(I, J - 1, K)] + PSI * PPS; }
+          else if (n == 4) { PSI = Y_(3, J + 1) / (0.5 * Y_(2, J + 1) + FF[c] * Y_(2, J)); PP[c] = (1.0 - PSI) * PP[id(I, J + 1, K)] + PSI * PPS; }
+          else if (n == 1) { PSI = X_(3, I) / (0.5 * X_(2, I - 1) + FF[c] * X_(2, I)); PP[c] = (1.0 - PSI) * PP[id(I - 1, J, K)] + PSI * PPS; }
+          else if (n == 2) { PSI = X_(3, I + 1) / (0.5 * X_(2, I + 1) + FF[c] * X_(2, I)); PP[c] = (1.0 - PSI) * PP[id(I + 1, J, K)] + PSI * PPS; }
+        }
+  }
+
+  // VF_CDIV00  vf_cdiv00.f:38-56
+  double cdiv00() {
+    double v = gsum([&](int I, int J, int K, double &c) {
+      if (!interior(I, J, K)) return false;
+      size_t q = id(I, J, K);
+      if (INDC[q] == -1) return false;
+      double VD = Y_(2, J) * Z_(2, K) * (GGX[id(I + 1, J, K)] * UU[id(I + 1, J, K)] - GGX[q] * UU[q]) +
+                  X_(2, I) * Z_(2, K) * (GGY[id(I, J + 1, K)] * VV[id(I, J + 1, K)] - GGY[q] * VV[q]) +
+                  X_(2, I) * Y_(2, J) * (GGZ[id(I, J, K + 1)] * WW[id(I, J, K + 1)] - GGZ[q] * WW[q]);
+      c = VD * VD;
+      return true;
+    });
+    return std::sqrt(v);
+  }
+
+  // ---------------------------------------------------------------- drivers
+  // VF_V1CAL  vf_v1cal.f:118-297 (ILOOP = 1)
+  int v1cal() {
+    Timer T;
+    size_t N = UU.size();
+    T.start();
+    for (int w = 1; w <= 12; ++w) WK[w].assign(N, 0.0);
+    WK[13] = UU; WK[14] = VV; WK[15] = WW;
+    vflxdu(WK[1], WK[2], WK[3]);
+    vflxdv(WK[5], WK[6], WK[7]);
+    vflxdw(WK[9], WK[10], WK[11]);
+    vgene(WK[4], WK[8], WK[12]);
+    veuler(WK[1], WK[2], WK[3], WK[4], WK[5], WK[6], WK[7], WK[8], WK[9], WK[10], WK[11], WK[12]);
+    int rc = bwuwn();
+    if (rc) return rc;
+    tmr[0] += T.stop();
+    T.start();
+    rc = vpcoef(WK[1], WK[2], WK[3], WK[4], WK[5], WK[6], WK[7], WK[8]);
+    if (rc) return rc;
+    tmr[1] += T.stop();
+    T.start();
+    // VF_VPSOL vf_vpsol.f:52-76
+    WK[9].assign(N, 0.0);
+    double bn, xn; int it;
+    m1bcgs(WK[1], WK[2], WK[3], WK[4], WK[5], WK[6], WK[7], WK[8], WK[9], INDC.data(), bn, xn, it);
+    st.cgbnrm = bn; st.cgxnrm = xn; st.icgitr = it;
+    tmr[2] += T.stop();
+    if (it > P.icgmax) return CADMAS_ENOTCONV;
+    if (it == -2) return CADMAS_EDIVERGE;
+    if (it == -1) return CADMAS_EPIVOT;
+    if (P.diag_relres) st.true_relres = true_relres(WK[1], WK[2], WK[3], WK[4], WK[5], WK[6], WK[7], WK[8], WK[9], INDC.data());
+    T.start();
+    vmodif(WK[9]);
+    bsuwt(); bsuwt2(); bsuwn(); bwuwt(); bwpp();
+    tmr[3] += T.stop();
+    return CADMAS_OK;
+  }
+
+  // VF_F1CAL  vf_f1cal.f:121-243
+  int f1cal() {
+    Timer T;
+    T.start();
+    size_t N = UU.size();
+    vd FLFU(N, 0.0), FLFV(N, 0.0), FLFW(N, 0.0);
+    std::fill(NLIM.begin(), NLIM.end(), 0);
+    fconv(FLFU, FLFV, FLFW);
+    feuler(FLFU, FLFV, FLFW);
+    fmod1();
+    double fs, fc;
+    fcut01(fs, fc);
+    st.fsum = fs; st.fcut = fc;
+    int rc = bwff();
+    if (rc) return rc;
+    bsuwn3();
+    bsuwem();
+    NLIM = NF;
+    rc = fnfini();
+    if (rc) return rc;
+    if (P.wbub >= 1.0e-20) {
+      fbubup();
+      rc = fnfini();
+      if (rc) return rc;
+    }
+    rc = fnfprv();
+    if (rc) return rc;
+    cindc();
+    bsppfl();
+    bsuwt(); bsuwt2(); bsuwn3(); bspp(); bwuwt(); bwpp();
+    st.nums = NUMS;
+    tmr[4] += T.stop();
+    return CADMAS_OK;
+  }
+};
+
+// ============================================================================
+extern "C" {
+
+orc_handle *orc_create(const cadmas_dims *d, const cadmas_params *p, int sum_mode) {
+  if (!d || !p || d->numi < 5 || d->numj < 3 || d->numk < 5 || d->numb < 0) return nullptr;
+  orc_handle *h = new orc_handle();
+  h->NI = d->numi; h->NJ = d->numj; h->NK = d->numk; h->NB = d->numb;
+  h->P = *p;
+  h->sum_mode = sum_mode;
+  size_t N = (size_t)h->NI * h->NJ * h->NK;
+  h->UU.assign(N, 0); h->VV.assign(N, 0); h->WW.assign(N, 0); h->PP.assign(N, 0); h->FF.assign(N, 0);
+  h->NF.assign(N, -1); h->INDC.assign(N, -1); h->NLIM.assign(N, 0);
+  size_t B = (size_t)std::max(h->NB, 1);
+  h->BCU.assign(B, 0); h->BCV.assign(B, 0); h->BCW.assign(B, 0); h->BCP.assign(B, 0); h->BCF.assign(B, 0);
+  h->TBUB.assign(h->NK, 0.0);
+  std::memset(&h->st, 0, sizeof(h->st));
+  h->st.true_relres = -1.0;
+  return h;
+}
+
+void orc_destroy(orc_handle *h) { delete h; }
+
+int orc_upload_static(orc_handle *h, const cadmas_static *s) {
+  size_t N = (size_t)h->NI * h->NJ * h->NK;
+  h->XX.assign(s->xx, s->xx + 6 * h->NI);
+  h->YY.assign(s->yy, s->yy + 6 * h->NJ);
+  h->ZZ.assign(s->zz, s->zz + 6 * h->NK);
+  h->GGV.assign(s->ggv, s->ggv + N); h->GGX.assign(s->ggx, s->ggx + N);
+  h->GGY.assign(s->ggy, s->ggy + N); h->GGZ.assign(s->ggz, s->ggz + N);
+  h->GLV.assign(s->glv, s->glv + N); h->GLX.assign(s->glx, s->glx + N);
+  h->GLY.assign(s->gly, s->gly + N); h->GLZ.assign(s->glz, s->glz + N);
+  h->CD0.assign(s->cd0, s->cd0 + N); h->ANU.assign(s->anu, s->anu + N);
+  h->INDX.assign(s->indx, s->indx + N); h->INDY.assign(s->indy, s->indy + N);
+  h->INDZ.assign(s->indz, s->indz + N);
+  h->INDB.assign(s->indb, s->indb + 4 * (size_t)h->NB);
+  if (h->NB == 0) h->INDB.assign(4, 0);
+  h->have_static = true;
+  return CADMAS_OK;
+}
+
+int orc_set_state(orc_handle *h, const cadmas_state *s) {
+  size_t N = (size_t)h->NI * h->NJ * h->NK, B = (size_t)h->NB;
+  if (s->uu) h->UU.assign(s->uu, s->uu + N);
+  if (s->vv) h->VV.assign(s->vv, s->vv + N);
+  if (s->ww) h->WW.assign(s->ww, s->ww + N);
+  if (s->pp) h->PP.assign(s->pp, s->pp + N);
+  if (s->ff) h->FF.assign(s->ff, s->ff + N);
+  if (s->nf) h->NF.assign(s->nf, s->nf + N);
+  if (s->indc) h->INDC.assign(s->indc, s->indc + N);
+  if (s->bcu) std::copy(s->bcu, s->bcu + B, h->BCU.begin());
+  if (s->bcv) std::copy(s->bcv, s->bcv + B, h->BCV.begin());
+  if (s->bcw) std::copy(s->bcw, s->bcw + B, h->BCW.begin());
+  if (s->bcp) std::copy(s->bcp, s->bcp + B, h->BCP.begin());
+  if (s->bcf) std::copy(s->bcf, s->bcf + B, h->BCF.begin());
+  if (s->tbub) h->TBUB.assign(s->tbub, s->tbub + h->NK);
+  h->TNOW = s->tnow; h->NNOW = s->nnow;
+  // rebuild INDS in the order FNFINI produces (ascending linear index)
+  h->INDS.clear();
+  for (int K = 2; K <= h->NK - 1; ++K)
+    for (int J = 2; J <= h->NJ - 1; ++J)
+      for (int I = 2; I <= h->NI - 1; ++I) {
+        int n = h->NF[h->id(I, J, K)];
+        if (n >= 1 && n <= 7) h->INDS.push_back(I + h->NI * (J - 1) + h->NI * h->NJ * (K - 1));
+      }
+  h->NUMS = (int)h->INDS.size();
+  return CADMAS_OK;
+}
+
+int orc_get_state(orc_handle *h, cadmas_state *s) {
+  size_t B = (size_t)h->NB;
+  if (s->uu) std::copy(h->UU.begin(), h->UU.end(), s->uu);
+  if (s->vv) std::copy(h->VV.begin(), h->VV.end(), s->vv);
+  if (s->ww) std::copy(h->WW.begin(), h->WW.end(), s->ww);
+  if (s->pp) std::copy(h->PP.begin(), h->PP.end(), s->pp);
+  if (s->ff) std::copy(h->FF.begin(), h->FF.end(), s->ff);
+  if (s->nf) std::copy(h->NF.begin(), h->NF.end(), s->nf);
+  if (s->indc) std::copy(h->INDC.begin(), h->INDC.end(), s->indc);
+  if (s->bcu) std::copy(h->BCU.begin(), h->BCU.begin() + B, s->bcu);
+  if (s->bcv) std::copy(h->BCV.begin(), h->BCV.begin() + B, s->bcv);
+  if (s->bcw) std::copy(h->BCW.begin(), h->BCW.begin() + B, s->bcw);
+  if (s->bcp) std::copy(h->BCP.begin(), h->BCP.begin() + B, s->bcp);
+  if (s->bcf) std::copy(h->BCF.begin(), h->BCF.begin() + B, s->bcf);
+  if (s->tbub) std::copy(h->TBUB.begin(), h->TBUB.end(), s->tbub);
+  s->tnow = h->TNOW; s->nnow = h->NNOW;
+  return CADMAS_OK;
+}
+
+// VF_CINIT vf_cinit.f:202-283 and the BC calls that follow it.
+int orc_init_state(orc_handle *h, int hydrostatic) {
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  double fs, fc;
+  h->fcut01(fs, fc);
+  h->st.fsum = fs; h->st.fcut = fc;
+  int rc = h->bwff();
+  if (rc) return rc;
+  rc = h->fnfini();
+  if (rc) return rc;
+  rc = h->fnfprv();
+  if (rc) return rc;
+  std::fill(h->INDC.begin(), h->INDC.end(), -1);
+  h->cindc();
+  if (hydrostatic) {
+    std::fill(h->PP.begin(), h->PP.end(), 0.0);
+    for (int K = 2; K <= h->NK - 1; ++K) {
+      double VAL = h->P.rho0 * h->P.grz0 * (h->P.wvlvl - (h->Z_(1, K) + h->Z_(1, K + 1)) * 0.5);
+      for (int J = 2; J <= h->NJ - 1; ++J)
+        for (int I = 2; I <= h->NI - 1; ++I)
+          if (h->INDC[h->id(I, J, K)] != -1) h->PP[h->id(I, J, K)] = VAL;
+    }
+  }
+  rc = h->bwuwn();
+  if (rc) return rc;
+  h->bsuwt(); h->bsuwt2(); h->bsuwn3(); h->bspp(); h->bwuwt(); h->bwpp();
+  std::fill(h->TBUB.begin(), h->TBUB.end(), 0.0);
+  h->st.nums = h->NUMS;
+  return CADMAS_OK;
+}
+
+int orc_step(orc_handle *h, double dt) {
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  for (double &t : h->tmr) t = 0.0;
+  h->DTNOW = dt;
+  h->NNOW = h->NNOW + 1;
+  h->TNOW = h->TNOW + h->DTNOW;
+  int rc = h->v1cal();
+  if (rc == CADMAS_OK) rc = h->f1cal();
+  h->st.last_status = rc;
+  return rc;
+}
+
+int orc_get_stats(orc_handle *h, cadmas_stats *st) { *st = h->st; return CADMAS_OK; }
+
+int orc_divnorm(orc_handle *h, double *val) {
+  *val = h->cdiv00();
+  h->st.divnorm = *val;
+  return CADMAS_OK;
+}
+
+int orc_m1bcgs(orc_handle *h, const double *ad, const double *ali, const double *alj,
+               const double *alk, const double *aui, const double *auj, const double *auk,
+               const double *bb, double *x0, const int *indc, int *iter, double *bnorm,
+               double *xnorm) {
+  size_t N = (size_t)h->NI * h->NJ * h->NK;
+  vd AD(ad, ad + N), ALI(ali, ali + N), ALJ(alj, alj + N), ALK(alk, alk + N), AUI(aui, aui + N),
+      AUJ(auj, auj + N), AUK(auk, auk + N), BB(bb, bb + N), X(x0, x0 + N);
+  h->m1bcgs(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, BB, X, indc, *bnorm, *xnorm, *iter);
+  std::copy(X.begin(), X.end(), x0);
+  return CADMAS_OK;
+}
+
+int orc_get_poisson(orc_handle *h, int which, double *out) {
+  if (which < 0 || which > 8) return CADMAS_EINVAL;
+  const vd &a = h->WK[which + 1];
+  if (a.empty()) return CADMAS_EINVAL;
+  std::copy(a.begin(), a.end(), out);
+  return CADMAS_OK;
+}
+
+int orc_get_timers(orc_handle *h, double *t5) {
+  for (int i = 0; i < 5; ++i) t5[i] = h->tmr[i];
+  return CADMAS_OK;
+}
+
+}  // extern "C"

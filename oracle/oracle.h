@@ -1,0 +1,62 @@
+/*
+ * oracle.h -- CPU restatement of the CADMAS-SURF/3D SMAC step (test infrastructure).
+ *
+ * THIS IS TEST INFRASTRUCTURE.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference arm of bench.py may load it, and only to check or
+ * time the GPU library.  Nothing in the product links or calls it.
+ *
+ * The reference (Fortran 77 + MPI) cannot be compiled in this environment
+ * (no Fortran compiler), so each routine below is restated loop by loop from
+ * Simulators/CADMAS-SURF-3D/Source code/ (file:line cited at each function in
+ * oracle.cpp).  The reference ships no tests or golden outputs, so parity of
+ * this restatement with the Fortran program itself is UNPINNED; it is pinned
+ * only by the invariants checked in tests/ (hydrostatic rest, volume balance,
+ * ILU = MILU at CGPARA 0, BiCGSTAB vs a dense solve).
+ *
+ * Two summation orders are offered for every global sum (dot products of
+ * VF_MZIP, FSUM/FCUT of VF_FCUT01, |VD| of VF_CDIV00):
+ *   ORC_SUM_REF : the reference order, K,J,I sequential, per emulated rank,
+ *                 ranks combined in rank order;
+ *   ORC_SUM_GPU : the fixed tree order of the GPU library's reductions
+ *                 (per x-row warp tree, then a 1024-thread tree over rows),
+ *                 so that GPU results can be compared bit for bit.
+ */
+#ifndef CADMAS_ORACLE_H
+#define CADMAS_ORACLE_H
+#include "../include/cadmas_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_SUM_REF 0
+#define ORC_SUM_GPU 1
+
+typedef struct orc_handle orc_handle;
+
+orc_handle *orc_create(const cadmas_dims *d, const cadmas_params *p, int sum_mode);
+void orc_destroy(orc_handle *h);
+int orc_upload_static(orc_handle *h, const cadmas_static *s);
+int orc_set_state(orc_handle *h, const cadmas_state *s);
+int orc_get_state(orc_handle *h, cadmas_state *s);
+int orc_init_state(orc_handle *h, int hydrostatic);
+int orc_step(orc_handle *h, double dt);
+int orc_get_stats(orc_handle *h, cadmas_stats *st);
+int orc_divnorm(orc_handle *h, double *val);
+/* VF_M1BCGS on host arrays with the handle's decomposition and sum order. */
+int orc_m1bcgs(orc_handle *h, const double *ad, const double *ali,
+               const double *alj, const double *alk, const double *aui,
+               const double *auj, const double *auk, const double *bb,
+               double *x0, const int *indc, int *iter, double *bnorm,
+               double *xnorm);
+/* Read back the last Poisson system (WK01..WK08) and PT (WK09) of a step:
+   which: 0 AD,1 ALI,2 ALJ,3 ALK,4 AUI,5 AUJ,6 AUK,7 BB,8 PT.               */
+int orc_get_poisson(orc_handle *h, int which, double *out);
+/* Seconds spent in the last orc_step by stage: [0] momentum predictor,
+   [1] assembly, [2] solve, [3] correction+BC, [4] VOF+flags.              */
+int orc_get_timers(orc_handle *h, double *t5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,160 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Loaded by tests/, __graft_entry__.smoke() and the CPU arms of bench.py to
+check or time the GPU library; never by the library itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import sys
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+SUM_REF, SUM_GPU = 0, 1
+
+
+def _pkg():
+    mod = sys.modules.get("cadmas_b200")
+    if mod is None:
+        import importlib.util
+        d = HERE.parent / "multiscale-and-multiphysics-integrated-simulator-for-tsunami_b200"
+        spec = importlib.util.spec_from_file_location("cadmas_b200", d / "__init__.py",
+                                                      submodule_search_locations=[str(d)])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["cadmas_b200"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        from . import build as _b  # noqa: F401
+    return _lib
+
+
+def _load_lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    sys.path.insert(0, str(HERE))
+    import build as obuild  # oracle/build.py
+    sys.path.pop(0)
+    obuild.build()
+    P = _pkg()
+    lib = C.CDLL(str(HERE / "liboracle.so"))
+    lib.orc_create.argtypes = [C.POINTER(P.Dims), C.POINTER(P.Params), C.c_int]
+    lib.orc_create.restype = C.c_void_p
+    lib.orc_destroy.argtypes = [C.c_void_p]
+    lib.orc_destroy.restype = None
+    lib.orc_upload_static.argtypes = [C.c_void_p, C.POINTER(P.Static)]
+    lib.orc_set_state.argtypes = [C.c_void_p, C.POINTER(P.State)]
+    lib.orc_get_state.argtypes = [C.c_void_p, C.POINTER(P.State)]
+    lib.orc_init_state.argtypes = [C.c_void_p, C.c_int]
+    lib.orc_step.argtypes = [C.c_void_p, C.c_double]
+    lib.orc_get_stats.argtypes = [C.c_void_p, C.POINTER(P.Stats)]
+    lib.orc_divnorm.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    dp = C.POINTER(C.c_double)
+    lib.orc_m1bcgs.argtypes = [C.c_void_p] + [dp] * 9 + [C.POINTER(C.c_int), C.POINTER(C.c_int), dp, dp]
+    lib.orc_get_poisson.argtypes = [C.c_void_p, C.c_int, dp]
+    lib.orc_get_timers.argtypes = [C.c_void_p, dp]
+    _lib = lib
+    return lib
+
+
+class Oracle:
+    """CPU restatement of the SMAC step on the same inputs as cadmas_b200.Tank."""
+
+    def __init__(self, case, sum_mode=SUM_GPU, **over):
+        self.lib = _load_lib()
+        P = _pkg()
+        self.P = P
+        self.case = case
+        # defaults of the library header restated (vf_a2dflt.f)
+        base = P.Params()
+        base.rho0, base.grz0, base.vvmax = 1.0e3, 9.8, 30.0
+        base.cgpara, base.cgepsa, base.cgepsr, base.cgdiv = 0.95, 1.0e-15, 1.0e-12, 1.0e30
+        base.flower, base.fupper, base.plower, base.scmvp = 1.0e-6, 1.0 - 1.0e-6, 1.0e-4, 1.0
+        base.wvlvl, base.wbub = 0.0, 0.2
+        for d in range(4):
+            base.idamp[d] = -1
+            base.damp[d][0], base.damp[d][1], base.damp[d][2], base.damp[d][3] = 0.6, 0.6, 0.0, 0.0
+        base.icgtyp, base.icgmax, base.ibsuw0 = 1, 500, 0
+        self.params = P.make_params(case, base, **over)
+        d = P.Dims(case.ni, case.nj, case.nk, case.numb)
+        self.h = self.lib.orc_create(C.byref(d), C.byref(self.params), int(sum_mode))
+        if not self.h:
+            raise RuntimeError("orc_create failed")
+        self._static = P.static_of(case)
+        self._rc(self.lib.orc_upload_static(self.h, C.byref(self._static)))
+        self.set_state(P.initial_state(case))
+
+    def _rc(self, rc):
+        if rc != 0:
+            raise self.P.CadmasError(rc, f"oracle status {rc}")
+
+    def set_state(self, arrs):
+        s = self.P.state_struct(arrs)
+        self._rc(self.lib.orc_set_state(self.h, C.byref(s)))
+
+    def get_state(self):
+        c = self.case
+        arrs = self.P.new_state_arrays(c.ni, c.nj, c.nk, c.numb)
+        s = self.P.state_struct(arrs)
+        self._rc(self.lib.orc_get_state(self.h, C.byref(s)))
+        arrs["tnow"], arrs["nnow"] = s.tnow, s.nnow
+        return arrs
+
+    def init_state(self, hydrostatic=True):
+        self._rc(self.lib.orc_init_state(self.h, int(bool(hydrostatic))))
+
+    def step(self, dt=None):
+        self._rc(self.lib.orc_step(self.h, float(dt if dt is not None else self.case.dt)))
+
+    def stats(self):
+        st = self.P.Stats()
+        self._rc(self.lib.orc_get_stats(self.h, C.byref(st)))
+        return {n: getattr(st, n) for n, _ in self.P.Stats._fields_ if n != "pad"}
+
+    def divnorm(self):
+        v = C.c_double()
+        self._rc(self.lib.orc_divnorm(self.h, C.byref(v)))
+        return v.value
+
+    def timers(self):
+        t = (C.c_double * 5)()
+        self.lib.orc_get_timers(self.h, t)
+        return list(t)
+
+    def poisson(self, which):
+        c = self.case
+        out = np.zeros((c.ni, c.nj, c.nk), order="F")
+        self._rc(self.lib.orc_get_poisson(self.h, which, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def m1bcgs(self, ad, ali, alj, alk, aui, auj, auk, bb, x0, indc):
+        dp = C.POINTER(C.c_double)
+        it, bn, xn = C.c_int(), C.c_double(), C.c_double()
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (ad, ali, alj, alk, aui, auj, auk, bb)]
+        x = np.array(x0, dtype=np.float64, order="F")
+        ic = np.asfortranarray(indc, dtype=np.int32)
+        self._rc(self.lib.orc_m1bcgs(self.h, *[a.ctypes.data_as(dp) for a in arrs], x.ctypes.data_as(dp),
+                                     ic.ctypes.data_as(C.POINTER(C.c_int)), C.byref(it), C.byref(bn),
+                                     C.byref(xn)))
+        return x, it.value, bn.value, xn.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

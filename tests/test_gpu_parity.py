@@ -1,0 +1,163 @@
+"""GPU library against the oracle, through the C ABI.
+
+The oracle runs in the GPU's summation order (the only order-dependent
+values are global sums), the library is compiled with --fmad=false, and
+every per-cell expression keeps the Fortran operand order, so the state
+after every step must be bit-identical: tolerance 0 on every field, on
+NF/INDC and on the step statistics.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("uu", "vv", "ww", "pp", "ff", "nf", "indc", "bcu", "bcv", "bcw", "bcp", "bcf")
+
+
+def assert_same(ga, oa, where):
+    for n in FIELDS:
+        a, b = ga[n], oa[n]
+        if not np.array_equal(a.view(np.uint8), b.view(np.uint8)):
+            bad = np.argwhere(a != b)
+            d = np.abs(a.astype(np.float64) - b.astype(np.float64)).max()
+            raise AssertionError(f"{where}: {n} differs at {bad.shape[0]} places, first {bad[:3].tolist()}, max |d| {d}")
+
+
+def run_pair(pkg, orc, case, steps, check_every=1, **over):
+    t = pkg.Tank(case, **over)
+    o = orc.Oracle(case, sum_mode=orc.SUM_GPU, **over)
+    t.init_state(case.hydrostatic)
+    o.init_state(case.hydrostatic)
+    assert_same(t.get_state(), o.get_state(), "init")
+    for n in range(1, steps + 1):
+        t.step(case.dt)
+        o.step(case.dt)
+        if n % check_every == 0 or n == steps:
+            assert_same(t.get_state(), o.get_state(), f"step {n}")
+            sg, so = t.stats(), o.stats()
+            for k in ("fsum", "fcut", "cgbnrm", "cgxnrm", "icgitr", "nums"):
+                assert sg[k] == so[k], (n, k, sg[k], so[k])
+    return t, o
+
+
+def test_dam_break_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.dam_break()
+    t, o = run_pair(pkg, orc, c, 30, check_every=5)
+    assert t.divnorm() == o.divnorm()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 5, 8])
+def test_random_tanks_bitwise(gpu_lib, pkg, orc, seed):
+    c = pkg.cases.random_tank(seed)
+    run_pair(pkg, orc, c, 8)
+
+
+def test_block_jacobi_preconditioner_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.dam_break()
+    run_pair(pkg, orc, c, 10, check_every=5, precond_ti=16, precond_tj=4)
+
+
+def test_porous_flume_with_sponge_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.porous_flume(nx=64, ny=6, nz=30, dx=0.05, dz=0.025, depth=0.4,
+                               block=(1.2, 1.8, 0.5), sponge_width=0.6, dt=2e-3)
+    run_pair(pkg, orc, c, 10, check_every=5)
+
+
+def test_bubble_rise_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.random_tank(9)
+    run_pair(pkg, orc, c, 6, wbub=0.2)
+
+
+def test_ilu_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.random_tank(4)
+    run_pair(pkg, orc, c, 4, icgtyp=0)
+
+
+def test_solver_alone_through_c_abi(gpu_lib, pkg, orc):
+    """cadmas_m1bcgs_dev on device buffers equals VF_M1BCGS of the oracle."""
+    import torch
+    c = pkg.cases.random_tank(4)
+    o = orc.Oracle(c, sum_mode=orc.SUM_GPU)
+    o.init_state(True)
+    o.step(c.dt)
+    indc = o.get_state()["indc"]      # flags the next system is assembled with
+    o.step(c.dt)
+    sysa = [o.poisson(w) for w in range(8)]
+    xo, ito, bno, xno = o.m1bcgs(*sysa, np.zeros_like(sysa[0]), indc)
+    t = pkg.Tank(c)
+    dev = [torch.from_numpy(a.reshape(-1, order="F").copy()).cuda() for a in sysa]
+    x = torch.zeros_like(dev[0])
+    ic = torch.from_numpy(indc.reshape(-1, order="F").copy()).cuda()
+    it, bn, xn = pkg.m1bcgs_dev(t, *[d.data_ptr() for d in dev], x.data_ptr(), ic.data_ptr())
+    assert (it, bn, xn) == (ito, bno, xno)
+    assert np.array_equal(x.cpu().numpy(), xo.reshape(-1, order="F"))
+
+
+def test_not_converged_status(gpu_lib, pkg):
+    c = pkg.cases.dam_break()
+    t = pkg.Tank(c, icgmax=1)
+    t.init_state(True)
+    with pytest.raises(pkg.CadmasError) as e:
+        t.step(c.dt)
+    assert e.value.status == pkg.ENOTCONV
+
+
+def test_pivot_failure_status(gpu_lib, pkg):
+    """A non-positive MILU pivot gives ITER=-1 ('CAN NOT DECOMPOSITION.')."""
+    import torch
+    c = pkg.cases.random_tank(1)
+    t = pkg.Tank(c)
+    t.init_state(True)
+    n = c.ni * c.nj * c.nk
+    indc = torch.from_numpy(t.get_state()["indc"].reshape(-1, order="F").copy()).cuda()
+    ad = torch.full((n,), -1.0, dtype=torch.float64, device="cuda")
+    z = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(7)]
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    it, bn, xn = pkg.m1bcgs_dev(t, ad.data_ptr(), *[q.data_ptr() for q in z[:6]], z[6].data_ptr(),
+                                x.data_ptr(), indc.data_ptr())
+    assert it == -1 and bn == 0.0 and xn == 0.0
+
+
+def test_fortran_entry_point(gpu_lib, pkg, orc):
+    """vf_step_gpu_ (host arrays in, host arrays out) equals cadmas_step."""
+    c = pkg.cases.random_tank(3)
+    t = pkg.Tank(c)
+    t.init_state(True)
+    st = t.get_state()
+    t2 = pkg.Tank(c)
+    t2.set_state(st)
+    t2.step(c.dt)
+    ref = t2.get_state()
+    lib = gpu_lib
+    hp = ctypes.c_void_p(t.h.value)
+    dt = ctypes.c_double(c.dt)
+    tnow = ctypes.c_double(st["tnow"])
+    nnow = ctypes.c_int(st["nnow"])
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    rc = lib.vf_step_gpu_(ctypes.byref(hp), ctypes.byref(dt), dp(st["uu"]), dp(st["vv"]), dp(st["ww"]),
+                          dp(st["pp"]), dp(st["ff"]), ip(st["nf"]), ip(st["indc"]), dp(st["bcu"]),
+                          dp(st["bcv"]), dp(st["bcw"]), dp(st["bcp"]), dp(st["bcf"]), ctypes.byref(tnow),
+                          ctypes.byref(nnow))
+    assert rc == 0
+    assert nnow.value == ref["nnow"] and tnow.value == ref["tnow"]
+    assert_same(st, ref, "vf_step_gpu_")
+
+
+def test_flume_full_size_properties(gpu_lib, pkg):
+    """512x32x96 porous flume (block-Jacobi tiles): a few steps keep the
+    fluid volume (closed box) and a divergence-free correction."""
+    c = pkg.cases.porous_flume()
+    t = pkg.Tank(c, precond_ti=32, precond_tj=8, diag_relres=1)
+    t.init_state(True)
+    v0 = t.stats()["fsum"]
+    cut = 0.0
+    for _ in range(3):
+        t.step(c.dt)
+        s = t.stats()
+        cut += s["fcut"]
+        assert s["true_relres"] < 1e-8
+    assert abs(s["fsum"] + cut - v0) / v0 < 1e-10
+    assert np.isfinite(t.divnorm())
