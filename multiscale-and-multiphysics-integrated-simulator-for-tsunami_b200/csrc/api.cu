@@ -124,9 +124,14 @@ struct cadmas_handle {
   // work: 9 flux arrays, reused as the Poisson system (0..7) and PT (8)
   double *wk[9] = {nullptr};
   // solver scratch
-  double *dd = nullptr, *xw = nullptr, *y2 = nullptr, *r0 = nullptr, *rr = nullptr, *pv = nullptr,
-         *ap = nullptr, *ae = nullptr, *tt = nullptr;
+  double *xw = nullptr, *y2 = nullptr, *r0 = nullptr, *rr = nullptr, *pv = nullptr,
+         *ap = nullptr, *ae = nullptr;
   double *rb0 = nullptr, *rb1 = nullptr, *dres = nullptr;
+  // skewed-layout copies of the system for the MILU kernels, and the
+  // forward-sweep result
+  SkewGeo q;
+  SkewSys S;
+  double *tt_sl = nullptr;
   SolveState *st = nullptr;
   int *dint = nullptr;            // [0] err [1] nch [2] done [3] iter [4] nums
   unsigned char *active = nullptr;
@@ -203,17 +208,20 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   SolveState *st = h->st;
   // vf_m1bcgs.f:79-95
   CK(cudaMemcpyAsync(h->xw, x0, bytes, cudaMemcpyDeviceToDevice, s));
-  double *zero_list[] = {h->dd, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->tt};
+  double *zero_list[] = {h->y2, h->r0, h->rr, h->pv, h->ap, h->ae};
   for (double *z : zero_list) CK(cudaMemsetAsync(z, 0, bytes, s));
   CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
   const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
+  const SkewGeo &q = h->q;
+  const SkewSys &S = h->S;
   TB(CADMAS_STAGE_DCMP);
-  launch_dcmp(s, g, h->TI, h->TJ, U, a, indc, h->dd, &st->pivot_bad);
+  launch_to_skew(s, g, q, a, indc, S);
+  launch_dcmp(s, g, q, U, S, &st->pivot_bad);
   launch_pivot_check(s, st);
   TE();
   // YY = MINV*BB, BNORM = (YY,YY)
-  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, a.bb, nullptr, h->tt, st); TE();
-  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->y2, st); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, a.bb, nullptr, h->tt_sl, st, h->y2); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->y2, st); TE();
   TB(CADMAS_STAGE_DOT);
   launch_dot(s, g, indc, h->y2, h->y2, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_BNORM, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -223,8 +231,8 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   launch_spmv(s, g, a, indc, h->xw, h->y2, st);
   launch_bmy(s, g, indc, a.bb, h->y2, st);
   TE();
-  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->y2, nullptr, h->tt, st); TE();
-  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->r0, st); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, h->y2, nullptr, h->tt_sl, st, h->y2); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->r0, st); TE();
   TB(CADMAS_STAGE_DOT);
   launch_dot(s, g, indc, h->r0, h->r0, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_START, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -235,16 +243,16 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   for (int guard = 0; guard < 100000; ++guard) {
     for (int b = 0; b < batch; ++b) {
       // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP
-      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, nullptr, h->pv, h->tt, st); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->ap, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, nullptr, h->pv, h->tt_sl, st, h->y2); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->ap, st); TE();
       TB(CADMAS_STAGE_DOT);
       launch_dot(s, g, indc, h->r0, h->ap, nullptr, nullptr, h->rb0, nullptr, st);
       launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
       TB(CADMAS_STAGE_VEC); launch_axpy_rr(s, g, indc, h->ap, h->rr, st); TE();
       // AE = MINV*(A*RR); OMEGA = (RR,AE)/(AE,AE)
-      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, h->TI, h->TJ, a, indc, h->dd, nullptr, h->rr, h->tt, st); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, h->TI, h->TJ, a, indc, h->dd, h->tt, h->ae, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, nullptr, h->rr, h->tt_sl, st, h->y2); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->ae, st); TE();
       TB(CADMAS_STAGE_DOT);
       launch_dot(s, g, indc, h->rr, h->ae, h->ae, h->ae, h->rb0, h->rb1, st);
       launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -509,8 +517,18 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
   AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
   for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
-  AL(h->dd, h->N); AL(h->xw, h->N); AL(h->y2, h->N); AL(h->r0, h->N); AL(h->rr, h->N);
-  AL(h->pv, h->N); AL(h->ap, h->N); AL(h->ae, h->N); AL(h->tt, h->N);
+  AL(h->xw, h->N); AL(h->y2, h->N); AL(h->r0, h->N); AL(h->rr, h->N);
+  AL(h->pv, h->N); AL(h->ap, h->N); AL(h->ae, h->N);
+  h->q.TI = TI; h->q.TJ = TJ; h->q.T = TI * TJ;
+  h->q.W = (d->numk - 2) + (TI - 1) + (TJ - 1);
+  h->q.ntx = (d->numi - 2 + TI - 1) / TI;
+  h->q.nb = h->q.ntx * ((d->numj - 2 + TJ - 1) / TJ);
+  {
+    const size_t nsl = (size_t)h->q.nb * h->q.W * h->q.T;
+    AL(h->S.ad, nsl); AL(h->S.ali, nsl); AL(h->S.alj, nsl); AL(h->S.alk, nsl);
+    AL(h->S.aui, nsl); AL(h->S.auj, nsl); AL(h->S.auk, nsl); AL(h->S.dd, nsl);
+    AL(h->S.indc, nsl); AL(h->tt_sl, nsl);
+  }
   AL(h->rb0, (size_t)nrows(h)); AL(h->rb1, (size_t)nrows(h)); AL(h->dres, 8);
   AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
 #undef AL
@@ -537,11 +555,12 @@ int cadmas_destroy(cadmas_handle *h) {
   cudaStreamSynchronize(h->s);
   double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
                   h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
-                  h->dd, h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->tt, h->rb0, h->rb1, h->dres};
+                  h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->rb0, h->rb1, h->dres,
+                  h->S.ad, h->S.ali, h->S.alj, h->S.alk, h->S.aui, h->S.auj, h->S.auk, h->S.dd, h->tt_sl};
   for (double *q : dl) if (q) cudaFree(q);
   for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) if (h->vel[b][c]) cudaFree(h->vel[b][c]);
   for (double *q : h->wk) if (q) cudaFree(q);
-  int *il[] = {h->indx, h->indy, h->indz, h->indb, h->nf, h->indc, h->nf0, h->nlim, h->dint};
+  int *il[] = {h->indx, h->indy, h->indz, h->indb, h->nf, h->indc, h->nf0, h->nlim, h->dint, h->S.indc};
   for (int *q : il) if (q) cudaFree(q);
   if (h->st) cudaFree(h->st);
   if (h->active) cudaFree(h->active);

@@ -22,6 +22,7 @@
 // halo DD and coefficients are zero).
 #include "cadmas_dev.cuh"
 #include "kernels.h"
+#include <algorithm>
 
 namespace cadmas {
 
@@ -149,126 +150,284 @@ __device__ __forceinline__ TileGeo tile_geo(const Geo &g, int TI, int TJ) {
   return t;
 }
 
-// VF_MZDCMP over one tile.  Shared: DD of the previous step.
-__global__ void k_dcmp(Geo g, int TI, int TJ, double U, SysPtr A_, const int *INDC, double *DD,
-                       int *pivot_bad) {
+// ---------------------------------------------------------------------------
+// Column prefetch.  Each thread streams its own column through a ring of R
+// shared-memory slots with cp.async, D wavefront steps ahead of use, so a
+// step only waits for shared memory and one barrier.  Values of the
+// neighbouring columns at the same plane are read from the neighbours' ring
+// slots: the left/lower neighbour handled plane k one step earlier (slot
+// s-1), the right/upper one handles it one step later (slot s+1, prefetched
+// long before).  R = D+3: at step s a thread refills slot s+D before the
+// step's barrier, while a slower neighbour may still read slot s-2.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Ring layout in dynamic shared memory: double r[R][NV][T], int ri[R][T],
+// then the exchange buffers double xb[2][T].
+template <int NV> struct Ring {
+  double *r;
+  int *ri;
+  double *xb;
+  int T, R;
+  __device__ __forceinline__ double &v(int slot, int q, int t) const { return r[((slot * NV) + q) * T + t]; }
+  __device__ __forceinline__ int &ind(int slot, int t) const { return ri[slot * T + t]; }
+};
+template <int NV> __device__ __forceinline__ Ring<NV> ring_setup(int T, int R) {
   extern __shared__ double sm[];
-  const int T = TI * TJ;
-  double *ds = sm;  // [2][T]
-  TileGeo t = tile_geo(g, TI, TJ);
-  const int I = t.is + t.ti, J = t.js + t.tj;
+  Ring<NV> g;
+  g.T = T; g.R = R;
+  g.r = sm;
+  g.xb = sm + (size_t)R * NV * T;
+  g.ri = (int *)(g.xb + 2 * T);
+  return g;
+}
+inline size_t ring_bytes(int NV, int T, int R) {
+  return (size_t)R * NV * T * sizeof(double) + 2 * (size_t)T * sizeof(double) + (size_t)R * T * sizeof(int);
+}
+
+// ----------------------------------------------------- tile-skewed layout
+// The MILU kernels visit, at wavefront step s, cell (is+ti, js+tj,
+// k = 2+s-ti-tj) with thread t = ti + TI*tj.  The arrays that stay constant
+// through a solve (7 coefficients, DD, INDC) and the forward-sweep result
+// are stored tile by tile in that visiting order,
+//     sl(b, w, t) = (b*W + w)*T + t,   w = (k-2) + ti + tj,
+// b = tile index, W = (NK-2) + (TI-1) + (TJ-1), so the T values a block
+// needs at one step are contiguous and every load of the sweep coalesces.
+__device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, int t) {
+  return ((long long)b * q.W + w) * q.T + t;
+}
+
+// Copy the Poisson system (7 coefficients) and INDC into the skewed layout.
+// Entries outside the tile or the interior get 0 (INDC -1).
+__global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S) {
+  const long long n = (long long)q.nb * q.W * q.T;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(e % q.T);
+    const long long bw = e / q.T;
+    const int w = (int)(bw % q.W), b = (int)(bw / q.W);
+    const int ti = t % q.TI, tj = t / q.TI;
+    const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    int ic = -1;
+    if (I <= g.NI - 1 && J <= g.NJ - 1 && k >= 2 && k <= g.NK - 1) {
+      const long long c = cid(g, I, J, k);
+      v[0] = A_.ad[c]; v[1] = A_.ali[c]; v[2] = A_.alj[c]; v[3] = A_.alk[c];
+      v[4] = A_.aui[c]; v[5] = A_.auj[c]; v[6] = A_.auk[c];
+      ic = INDC[c];
+    }
+    S.ad[e] = v[0]; S.ali[e] = v[1]; S.alj[e] = v[2]; S.alk[e] = v[3];
+    S.aui[e] = v[4]; S.auj[e] = v[5]; S.auk[e] = v[6]; S.indc[e] = ic;
+  }
+}
+
+// ------------------------------------------------------------ VF_MZDCMP
+// ring values: 0 AD, 1 ALI, 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK; DD is
+// written in the skewed layout.
+template <int D>
+__global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
+  constexpr int NV = 7, R = D + 3;
+  const int TI = q.TI, T = q.T;
+  Ring<NV> rg = ring_setup<NV>(T, R);
+  TileGeo t = tile_geo(g, TI, q.TJ);
+  const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
-  double dk1 = 0.0, au3 = 0.0;  // DD(i,j,k-1) and its AU3; k-1 = 1 is the zero ghost layer
+  auto prefetch = [&](int s) {
+    const int k = 2 + s - t.ti - t.tj;
+    if (t.valid && k >= 2 && k <= g.NK - 1) {
+      const long long e = sl_index(q, b, s, tid);
+      const int sl = s % R;
+      cp_async8(&rg.v(sl, 0, tid), S.ad + e);  cp_async8(&rg.v(sl, 1, tid), S.ali + e);
+      cp_async8(&rg.v(sl, 2, tid), S.alj + e); cp_async8(&rg.v(sl, 3, tid), S.alk + e);
+      cp_async8(&rg.v(sl, 4, tid), S.aui + e); cp_async8(&rg.v(sl, 5, tid), S.auj + e);
+      cp_async8(&rg.v(sl, 6, tid), S.auk + e); cp_async4(&rg.ind(sl, tid), S.indc + e);
+    }
+    cp_commit();
+  };
+#pragma unroll 1
+  for (int s = 0; s < D; ++s) prefetch(s);
+  double dk1 = 0.0, au3 = 0.0;  // DD(i,j,k-1) and AU3 of (i,j,k-1); k-1 = 1 is the zero ghost layer
   bool bad = false;
   for (int s = 0; s < nsteps; ++s) {
+    prefetch(s + D);
+    cp_wait<D - 1>();
+    __syncthreads();
     const int k = 2 + s - t.ti - t.tj;
-    const int cur = s & 1, prv = cur ^ 1;
+    const int sl = s % R, slp = (s + R - 1) % R, cur = s & 1, prv = cur ^ 1;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long c = cid(g, I, J, k);
       double dd = 0.0;
-      if (INDC[c] != -1) {
+      if (rg.ind(sl, tid) != -1) {
         double d1 = 0.0, a1, d2 = 0.0, a2;
         if (t.ti > 0) {
-          const long long n = c - 1;
-          d1 = ds[prv * T + threadIdx.x - 1];
-          a1 = A_.aui[n] + U * (A_.auj[n] + A_.auk[n]);
+          d1 = rg.xb[prv * T + tid - 1];
+          a1 = rg.v(slp, 4, tid - 1) + U * (rg.v(slp, 5, tid - 1) + rg.v(slp, 6, tid - 1));
         } else {
           a1 = 0.0 + U * (0.0 + 0.0);
         }
         if (t.tj > 0) {
-          const long long n = c - g.NI;
-          d2 = ds[prv * T + threadIdx.x - TI];
-          a2 = A_.auj[n] + U * (A_.aui[n] + A_.auk[n]);
+          d2 = rg.xb[prv * T + tid - TI];
+          a2 = rg.v(slp, 5, tid - TI) + U * (rg.v(slp, 4, tid - TI) + rg.v(slp, 6, tid - TI));
         } else {
           a2 = 0.0 + U * (0.0 + 0.0);
         }
-        dd = 1.0 / (A_.ad[c] - A_.ali[c] * d1 * a1 - A_.alj[c] * d2 * a2 - A_.alk[c] * dk1 * au3);
+        dd = 1.0 / (rg.v(sl, 0, tid) - rg.v(sl, 1, tid) * d1 * a1 - rg.v(sl, 2, tid) * d2 * a2 -
+                    rg.v(sl, 3, tid) * dk1 * au3);
         if (dd <= 0.0) bad = true;
       }
-      DD[c] = dd;
-      ds[cur * T + threadIdx.x] = dd;
+      S.dd[sl_index(q, b, s, tid)] = dd;
+      rg.xb[cur * T + tid] = dd;
       dk1 = dd;
-      au3 = A_.auk[c] + U * (A_.aui[c] + A_.auj[c]);
+      au3 = rg.v(sl, 6, tid) + U * (rg.v(sl, 4, tid) + rg.v(sl, 5, tid));
     }
-    __syncthreads();
   }
+  cp_wait<0>();
   if (bad) atomicOr(pivot_bad, 1);
 }
 
-// Forward sweep (L D^-1 + I) X = Y.  When spmv_x is non-null the input is
-// Y = A * spmv_x computed on the fly (VF_MZAX then VF_MZFRWD); otherwise
-// Y is read from y.  Either way X is written for every column cell (0 on
-// INDC=-1 cells, where the reference leaves its zero-initialised value).
-__global__ void k_fwd(Geo g, int TI, int TJ, SysPtr A_, const int *INDC, const double *DD,
-                      const double *y, const double *spmv_x, double *X, const SolveState *st) {
+// ------------------------------------------------------- VF_MZFRWD (+MZAX)
+// FUSED: the input is Y = A*P computed on the fly (VF_MZAX then VF_MZFRWD).
+// Ring values, fused:  0 AD, 1 ALI, 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK, 7 DD
+//                      (skewed), 8 P, 9 P(i-1), 10 P(i+1), 11 P(j-1),
+//                      12 P(j+1) (P in the standard layout; 9..12 only on
+//                      tile-edge threads)
+// Ring values, plain:  0 Y (standard layout), 1 ALI, 2 ALJ, 3 ALK, 4 DD
+// The result is written in the skewed layout for k_bwd.
+template <int D, bool FUSED>
+__global__ void k_fwd(Geo g, SkewGeo q, SkewSys S, const double *y, const double *P, double *Tout,
+                      const SolveState *st) {
   if (st && st->done) return;
-  extern __shared__ double sm[];
-  const int T = TI * TJ;
-  double *xs = sm, *ds = sm + 2 * T;
-  TileGeo t = tile_geo(g, TI, TJ);
-  const int I = t.is + t.ti, J = t.js + t.tj;
+  constexpr int NV = FUSED ? 13 : 5, R = D + 3;
+  constexpr int QDD = FUSED ? 7 : 4;
+  const int TI = q.TI, T = q.T;
+  Ring<NV> rg = ring_setup<NV>(T, R);
+  TileGeo t = tile_geo(g, TI, q.TJ);
+  const int I = t.is + t.ti, J = t.js + t.tj, tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
+  const long long NIJ = (long long)g.NI * g.NJ;
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
-  double xk1 = 0.0, dk1 = 0.0;
-  for (int s = 0; s < nsteps; ++s) {
+  const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
+  auto prefetch = [&](int s) {
     const int k = 2 + s - t.ti - t.tj;
-    const int cur = s & 1, prv = cur ^ 1;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long c = cid(g, I, J, k);
-      double x = 0.0, d = DD[c];
-      if (INDC[c] != -1) {
+      const long long c = cid(g, I, J, k), e = sl_index(q, b, s, tid);
+      const int sl = s % R;
+      if (FUSED) {
+        cp_async8(&rg.v(sl, 0, tid), S.ad + e);  cp_async8(&rg.v(sl, 1, tid), S.ali + e);
+        cp_async8(&rg.v(sl, 2, tid), S.alj + e); cp_async8(&rg.v(sl, 3, tid), S.alk + e);
+        cp_async8(&rg.v(sl, 4, tid), S.aui + e); cp_async8(&rg.v(sl, 5, tid), S.auj + e);
+        cp_async8(&rg.v(sl, 6, tid), S.auk + e); cp_async8(&rg.v(sl, 7, tid), S.dd + e);
+        cp_async8(&rg.v(sl, 8, tid), P + c);
+        if (ex0) cp_async8(&rg.v(sl, 9, tid), P + c - 1);
+        if (ex1) cp_async8(&rg.v(sl, 10, tid), P + c + 1);
+        if (ey0) cp_async8(&rg.v(sl, 11, tid), P + c - g.NI);
+        if (ey1) cp_async8(&rg.v(sl, 12, tid), P + c + g.NI);
+      } else {
+        cp_async8(&rg.v(sl, 0, tid), y + c);      cp_async8(&rg.v(sl, 1, tid), S.ali + e);
+        cp_async8(&rg.v(sl, 2, tid), S.alj + e);  cp_async8(&rg.v(sl, 3, tid), S.alk + e);
+        cp_async8(&rg.v(sl, 4, tid), S.dd + e);
+      }
+      cp_async4(&rg.ind(sl, tid), S.indc + e);
+    }
+    cp_commit();
+  };
+#pragma unroll 1
+  for (int s = 0; s < D; ++s) prefetch(s);
+  double xk1 = 0.0, dk1 = 0.0;  // X and DD at (i,j,k-1); k-1 = 1 is the zero ghost layer
+  for (int s = 0; s < nsteps; ++s) {
+    prefetch(s + D);
+    cp_wait<D - 1>();
+    __syncthreads();
+    const int k = 2 + s - t.ti - t.tj;
+    const int sl = s % R, slp = (s + R - 1) % R, sln = (s + 1) % R, cur = s & 1, prv = cur ^ 1;
+    if (t.valid && k >= 2 && k <= g.NK - 1) {
+      double x = 0.0;
+      const double d = rg.v(sl, QDD, tid);
+      if (rg.ind(sl, tid) != -1) {
         double yv;
-        if (spmv_x) {
-          const double *P = spmv_x;
-          yv = A_.ad[c] * P[c] + A_.ali[c] * P[c - 1] + A_.alj[c] * P[c - g.NI] +
-               A_.alk[c] * P[c - (long long)g.NI * g.NJ] + A_.aui[c] * P[c + 1] +
-               A_.auj[c] * P[c + g.NI] + A_.auk[c] * P[c + (long long)g.NI * g.NJ];
+        if (FUSED) {
+          const long long c = cid(g, I, J, k);
+          const double pc = rg.v(sl, 8, tid);
+          const double pxm = ex0 ? rg.v(sl, 9, tid) : rg.v(slp, 8, tid - 1);
+          const double pym = ey0 ? rg.v(sl, 11, tid) : rg.v(slp, 8, tid - TI);
+          const double pzm = (k > 2) ? rg.v(slp, 8, tid) : P[c - NIJ];
+          const double pxp = ex1 ? rg.v(sl, 10, tid) : rg.v(sln, 8, tid + 1);
+          const double pyp = ey1 ? rg.v(sl, 12, tid) : rg.v(sln, 8, tid + TI);
+          const double pzp = (k < g.NK - 1) ? rg.v(sln, 8, tid) : P[c + NIJ];
+          yv = rg.v(sl, 0, tid) * pc + rg.v(sl, 1, tid) * pxm + rg.v(sl, 2, tid) * pym +
+               rg.v(sl, 3, tid) * pzm + rg.v(sl, 4, tid) * pxp + rg.v(sl, 5, tid) * pyp +
+               rg.v(sl, 6, tid) * pzp;
         } else {
-          yv = y[c];
+          yv = rg.v(sl, 0, tid);
         }
         double d1 = 0.0, x1 = 0.0, d2 = 0.0, x2 = 0.0;
-        if (t.ti > 0) { d1 = ds[prv * T + threadIdx.x - 1]; x1 = xs[prv * T + threadIdx.x - 1]; }
-        if (t.tj > 0) { d2 = ds[prv * T + threadIdx.x - TI]; x2 = xs[prv * T + threadIdx.x - TI]; }
-        x = yv - A_.ali[c] * d1 * x1 - A_.alj[c] * d2 * x2 - A_.alk[c] * dk1 * xk1;
+        if (t.ti > 0) { d1 = rg.v(slp, QDD, tid - 1); x1 = rg.xb[prv * T + tid - 1]; }
+        if (t.tj > 0) { d2 = rg.v(slp, QDD, tid - TI); x2 = rg.xb[prv * T + tid - TI]; }
+        x = yv - rg.v(sl, 1, tid) * d1 * x1 - rg.v(sl, 2, tid) * d2 * x2 - rg.v(sl, 3, tid) * dk1 * xk1;
       }
-      X[c] = x;
-      xs[cur * T + threadIdx.x] = x;
-      ds[cur * T + threadIdx.x] = d;
+      Tout[sl_index(q, b, s, tid)] = x;
+      rg.xb[cur * T + tid] = x;
       xk1 = x;
       dk1 = d;
     }
-    __syncthreads();
   }
+  cp_wait<0>();
 }
 
-// Backward sweep (D + U) X = Tin, reversed loop order.
-__global__ void k_bwd(Geo g, int TI, int TJ, SysPtr A_, const int *INDC, const double *DD,
-                      const double *Tin, double *X, const SolveState *st) {
+// ------------------------------------------------------------ VF_MZBKWD
+// ring values: 0 T, 1 AUI, 2 AUJ, 3 AUK, 4 DD (all skewed); reversed loop
+// order; X written in the standard layout.
+template <int D>
+__global__ void k_bwd(Geo g, SkewGeo q, SkewSys S, const double *Tin, double *X, const SolveState *st) {
   if (st && st->done) return;
-  extern __shared__ double sm[];
-  const int T = TI * TJ;
-  double *xs = sm;
-  TileGeo t = tile_geo(g, TI, TJ);
-  const int I = t.is + t.ti, J = t.js + t.tj;
+  constexpr int NV = 5, R = D + 3;
+  const int TI = q.TI, T = q.T;
+  Ring<NV> rg = ring_setup<NV>(T, R);
+  TileGeo t = tile_geo(g, TI, q.TJ);
+  const int I = t.is + t.ti, J = t.js + t.tj, tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
   const int ri = t.wi - 1 - t.ti, rj = t.wj - 1 - t.tj;  // distance from the far corner
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
+  auto prefetch = [&](int s) {
+    const int k = (g.NK - 1) - (s - ri - rj);
+    if (t.valid && k >= 2 && k <= g.NK - 1) {
+      const long long e = sl_index(q, b, (k - 2) + t.ti + t.tj, tid);
+      const int sl = s % R;
+      cp_async8(&rg.v(sl, 0, tid), Tin + e);      cp_async8(&rg.v(sl, 1, tid), S.aui + e);
+      cp_async8(&rg.v(sl, 2, tid), S.auj + e);    cp_async8(&rg.v(sl, 3, tid), S.auk + e);
+      cp_async8(&rg.v(sl, 4, tid), S.dd + e);     cp_async4(&rg.ind(sl, tid), S.indc + e);
+    }
+    cp_commit();
+  };
+#pragma unroll 1
+  for (int s = 0; s < D; ++s) prefetch(s);
   double xk1 = 0.0;  // X(i,j,k+1); k+1 = NK is the zero ghost layer
   for (int s = 0; s < nsteps; ++s) {
+    prefetch(s + D);
+    cp_wait<D - 1>();
+    __syncthreads();
     const int k = (g.NK - 1) - (s - ri - rj);
-    const int cur = s & 1, prv = cur ^ 1;
+    const int sl = s % R, cur = s & 1, prv = cur ^ 1;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long c = cid(g, I, J, k);
       double x = 0.0;
-      if (INDC[c] != -1) {
-        double x1 = (ri > 0) ? xs[prv * T + threadIdx.x + 1] : 0.0;
-        double x2 = (rj > 0) ? xs[prv * T + threadIdx.x + TI] : 0.0;
-        x = (Tin[c] - A_.aui[c] * x1 - A_.auj[c] * x2 - A_.auk[c] * xk1) * DD[c];
+      if (rg.ind(sl, tid) != -1) {
+        const double x1 = (ri > 0) ? rg.xb[prv * T + tid + 1] : 0.0;
+        const double x2 = (rj > 0) ? rg.xb[prv * T + tid + TI] : 0.0;
+        x = (rg.v(sl, 0, tid) - rg.v(sl, 1, tid) * x1 - rg.v(sl, 2, tid) * x2 - rg.v(sl, 3, tid) * xk1) *
+            rg.v(sl, 4, tid);
       }
-      X[c] = x;
-      xs[cur * T + threadIdx.x] = x;
+      X[cid(g, I, J, k)] = x;
+      rg.xb[cur * T + tid] = x;
       xk1 = x;
     }
-    __syncthreads();
   }
+  cp_wait<0>();
 }
 
 // ------------------------------------------------------------ row kernels
@@ -518,23 +677,68 @@ void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
   k_vpcoef<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, f, p, a, err);
   count_launch();
 }
-static inline dim3 tile_grid(const Geo &g, int TI, int TJ) {
-  return dim3((unsigned)((g.NI - 2 + TI - 1) / TI), (unsigned)((g.NJ - 2 + TJ - 1) / TJ));
+// Prefetch depth: the largest of 8, 4, 2, 1 whose ring fits the shared
+// memory a block may use (200 KB here).
+static int ring_depth(int NV, int T) {
+  const size_t cap = 200 * 1024;
+  for (int d : {8, 4, 2, 1})
+    if (ring_bytes(NV, T, d + 3) <= cap) return d;
+  return 0;
 }
-void launch_dcmp(cudaStream_t s, const Geo &g, int TI, int TJ, double U, const SysPtr &a,
-                 const int *indc, double *dd, int *pivot_bad) {
-  k_dcmp<<<tile_grid(g, TI, TJ), TI * TJ, 2 * TI * TJ * sizeof(double), s>>>(g, TI, TJ, U, a, indc, dd, pivot_bad);
+template <class K> static void set_smem(K kern, size_t bytes) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+static inline dim3 skew_grid(const SkewGeo &q) { return dim3((unsigned)q.ntx, (unsigned)(q.nb / q.ntx)); }
+#define RING_LAUNCH2(KER, NV, ...)                                                             \
+  do {                                                                                        \
+    const int T_ = q.T, d_ = ring_depth(NV, T_);                                              \
+    const size_t b_ = ring_bytes(NV, T_, d_ + 3);                                             \
+    switch (d_) {                                                                             \
+      case 8: set_smem(KER<8 RING_EXTRA>, b_); KER<8 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
+      case 4: set_smem(KER<4 RING_EXTRA>, b_); KER<4 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
+      case 2: set_smem(KER<2 RING_EXTRA>, b_); KER<2 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
+      default: set_smem(KER<1 RING_EXTRA>, b_); KER<1 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
+    }                                                                                         \
+    count_launch();                                                                           \
+  } while (0)
+
+void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
+                    const SkewSys &S) {
+  const long long n = (long long)q.nb * q.W * q.T;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  k_to_skew<<<blocks, 256, 0, s>>>(g, q, a, indc, S);
   count_launch();
 }
-void launch_fwd(cudaStream_t s, const Geo &g, int TI, int TJ, const SysPtr &a, const int *indc,
-                const double *dd, const double *y, const double *spmv_x, double *x, const SolveState *st) {
-  k_fwd<<<tile_grid(g, TI, TJ), TI * TJ, 4 * TI * TJ * sizeof(double), s>>>(g, TI, TJ, a, indc, dd, y, spmv_x, x, st);
-  count_launch();
+void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad) {
+#define RING_EXTRA
+  RING_LAUNCH2(k_dcmp, 7, g, q, U, S, pivot_bad);
+#undef RING_EXTRA
 }
-void launch_bwd(cudaStream_t s, const Geo &g, int TI, int TJ, const SysPtr &a, const int *indc,
-                const double *dd, const double *t, double *x, const SolveState *st) {
-  k_bwd<<<tile_grid(g, TI, TJ), TI * TJ, 2 * TI * TJ * sizeof(double), s>>>(g, TI, TJ, a, indc, dd, t, x, st);
-  count_launch();
+void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const SkewSys &S,
+                const int *indc, const double *y, const double *spmv_x, double *tout, const SolveState *st,
+                double *ybuf) {
+  if (spmv_x && ring_depth(13, q.T) == 0) {
+    // Ring of the fused kernel too large for this tile: SpMV first.
+    launch_spmv(s, g, a, indc, spmv_x, ybuf, st);
+    y = ybuf;
+    spmv_x = nullptr;
+  }
+  if (spmv_x) {
+#define RING_EXTRA , true
+    RING_LAUNCH2(k_fwd, 13, g, q, S, y, spmv_x, tout, st);
+#undef RING_EXTRA
+  } else {
+#define RING_EXTRA , false
+    RING_LAUNCH2(k_fwd, 5, g, q, S, y, spmv_x, tout, st);
+#undef RING_EXTRA
+  }
+}
+void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
+                double *x, const SolveState *st) {
+#define RING_EXTRA
+  RING_LAUNCH2(k_bwd, 5, g, q, S, tin, x, st);
+#undef RING_EXTRA
 }
 void launch_spmv(cudaStream_t s, const Geo &g, const SysPtr &a, const int *indc, const double *x, double *y,
                  const SolveState *st) {

@@ -15,6 +15,18 @@ struct SysPtr {
   double *ad, *ali, *alj, *alk, *aui, *auj, *auk, *bb;
 };
 
+// The constant part of a solve in the tile-skewed layout of the MILU
+// kernels (k_poisson.cu): 7 coefficients, DD and INDC.
+struct SkewSys {
+  double *ad, *ali, *alj, *alk, *aui, *auj, *auk, *dd;
+  int *indc;
+};
+// Tile geometry of the skewed layout: TI x TJ columns per tile (T threads),
+// W wavefront slabs per tile, ntx tiles along x, nb tiles in all.
+struct SkewGeo {
+  int TI, TJ, T, W, ntx, nb;
+};
+
 enum FinMode { FIN_BNORM = 0, FIN_START = 1, FIN_STORE = 2, FIN_RELRES = 3,
                FIN_ALPHA = 10, FIN_OMEGA = 11, FIN_CONV = 12 };
 
@@ -26,12 +38,14 @@ void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, int *err);
 
 // k_poisson.cu
 void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const SysPtr &a, int *err);
-void launch_dcmp(cudaStream_t s, const Geo &g, int TI, int TJ, double U, const SysPtr &a,
-                 const int *indc, double *dd, int *pivot_bad);
-void launch_fwd(cudaStream_t s, const Geo &g, int TI, int TJ, const SysPtr &a, const int *indc,
-                const double *dd, const double *y, const double *spmv_x, double *x, const SolveState *st);
-void launch_bwd(cudaStream_t s, const Geo &g, int TI, int TJ, const SysPtr &a, const int *indc,
-                const double *dd, const double *t, double *x, const SolveState *st);
+void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
+                    const SkewSys &S);
+void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad);
+void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const SkewSys &S,
+                const int *indc, const double *y, const double *spmv_x, double *tout, const SolveState *st,
+                double *ybuf);
+void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
+                double *x, const SolveState *st);
 void launch_spmv(cudaStream_t s, const Geo &g, const SysPtr &a, const int *indc, const double *x,
                  double *y, const SolveState *st);
 void launch_bmy(cudaStream_t s, const Geo &g, const int *indc, const double *b, double *y,
