@@ -131,7 +131,9 @@ struct cadmas_handle {
   // forward-sweep result
   SkewGeo q;
   SkewSys S;
-  double *tt_sl = nullptr;
+  double *tt_sl = nullptr, *bb_sl = nullptr;
+  size_t nsl = 0;        // entries of a skewed vector
+  long long nslab = 0;   // slabs (dot-product rows) of a skewed vector
   SolveState *st = nullptr;
   int *dint = nullptr;            // [0] err [1] nch [2] done [3] iter [4] nums
   unsigned char *active = nullptr;
@@ -200,68 +202,68 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
                  double &bnorm, double &xnorm) {
   cudaStream_t s = h->s;
   const Geo &g = h->g;
-  const size_t bytes = h->N * sizeof(double);
+  const size_t vbytes = h->nsl * sizeof(double);
   const double epsa2 = h->P.cgepsa * h->P.cgepsa, epsr2 = h->P.cgepsr * h->P.cgepsr,
                div2 = h->P.cgdiv * h->P.cgdiv;
   const int icgmax = h->P.icgmax;
-  const long long nr = nrows(h);
+  const long long nr = h->nslab;
   SolveState *st = h->st;
-  // vf_m1bcgs.f:79-95
-  CK(cudaMemcpyAsync(h->xw, x0, bytes, cudaMemcpyDeviceToDevice, s));
-  double *zero_list[] = {h->y2, h->r0, h->rr, h->pv, h->ap, h->ae};
-  for (double *z : zero_list) CK(cudaMemsetAsync(z, 0, bytes, s));
-  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
-  const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
   const SkewGeo &q = h->q;
   const SkewSys &S = h->S;
+  const int *ic = S.indc;  // INDC in the skewed layout (-1 on padding)
+  // vf_m1bcgs.f:79-95: XW = X0, work vectors zero
+  double *zero_list[] = {h->y2, h->r0, h->rr, h->pv, h->ap, h->ae};
+  for (double *z : zero_list) CK(cudaMemsetAsync(z, 0, vbytes, s));
+  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
   TB(CADMAS_STAGE_DCMP);
-  launch_to_skew(s, g, q, a, indc, S);
+  launch_to_skew(s, g, q, a, indc, S, x0, h->bb_sl, h->xw);
   launch_dcmp(s, g, q, U, S, &st->pivot_bad);
   launch_pivot_check(s, st);
   TE();
   // YY = MINV*BB, BNORM = (YY,YY)
-  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, a.bb, nullptr, h->tt_sl, st, h->y2); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, h->bb_sl, nullptr, h->tt_sl, st, h->y2); TE();
   TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->y2, st); TE();
   TB(CADMAS_STAGE_DOT);
-  launch_dot(s, g, indc, h->y2, h->y2, nullptr, nullptr, h->rb0, nullptr, st);
+  launch_dot(s, q, ic, h->y2, h->y2, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_BNORM, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
   TE();
   // YY = A*XW; YY = BB - YY; R0 = MINV*YY; S = (R0,R0)
   TB(CADMAS_STAGE_VEC);
-  launch_spmv(s, g, a, indc, h->xw, h->y2, st);
-  launch_bmy(s, g, indc, a.bb, h->y2, st);
+  launch_spmv(s, g, q, S, h->xw, h->y2, st);
+  launch_bmy(s, q, ic, h->bb_sl, h->y2, st);
   TE();
-  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, h->y2, nullptr, h->tt_sl, st, h->y2); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, h->y2, nullptr, h->tt_sl, st, h->y2); TE();
   TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->r0, st); TE();
   TB(CADMAS_STAGE_DOT);
-  launch_dot(s, g, indc, h->r0, h->r0, nullptr, nullptr, h->rb0, nullptr, st);
+  launch_dot(s, q, ic, h->r0, h->r0, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_START, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
   TE();
-  TB(CADMAS_STAGE_VEC); launch_copy2(s, g, indc, h->r0, h->rr, h->pv, st); TE();
+  TB(CADMAS_STAGE_VEC); launch_copy2(s, q, ic, h->r0, h->rr, h->pv, st); TE();
   // First batch as long as the previous solve; after that batches of 4.
   int batch = std::max(2, std::min(h->last_iter, 64));
   for (int guard = 0; guard < 100000; ++guard) {
     for (int b = 0; b < batch; ++b) {
       // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP
-      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, nullptr, h->pv, h->tt_sl, st, h->y2); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, nullptr, h->pv, h->tt_sl, st, h->y2); TE();
       TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->ap, st); TE();
       TB(CADMAS_STAGE_DOT);
-      launch_dot(s, g, indc, h->r0, h->ap, nullptr, nullptr, h->rb0, nullptr, st);
+      launch_dot(s, q, ic, h->r0, h->ap, nullptr, nullptr, h->rb0, nullptr, st);
       launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
-      TB(CADMAS_STAGE_VEC); launch_axpy_rr(s, g, indc, h->ap, h->rr, st); TE();
+      TB(CADMAS_STAGE_VEC); launch_axpy_rr(s, q, ic, h->ap, h->rr, st); TE();
       // AE = MINV*(A*RR); OMEGA = (RR,AE)/(AE,AE)
-      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, a, S, indc, nullptr, h->rr, h->tt_sl, st, h->y2); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, nullptr, h->rr, h->tt_sl, st, h->y2); TE();
       TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->ae, st); TE();
       TB(CADMAS_STAGE_DOT);
-      launch_dot(s, g, indc, h->rr, h->ae, h->ae, h->ae, h->rb0, h->rb1, st);
+      launch_dot(s, q, ic, h->rr, h->ae, h->ae, h->ae, h->rb0, h->rb1, st);
       launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
       // XW += ALPHA*PP + OMEGA*RR; RR -= OMEGA*AE; convergence; BETA
       TB(CADMAS_STAGE_VEC);
-      launch_upd_xr(s, g, indc, h->pv, h->ae, h->r0, h->xw, h->rr, h->rb0, h->rb1, st);
+      launch_upd_xr(s, q, ic, h->pv, h->ae, h->r0, h->xw, h->rr, h->rb0, h->rb1, st);
       launch_fin(s, FIN_CONV, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
-      launch_upd_p(s, g, indc, h->rr, h->ap, h->pv, st);
+      launch_upd_p(s, q, ic, h->rr, h->ap, h->pv, st);
       TE();
     }
     CK(cudaGetLastError());
@@ -270,7 +272,7 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
     if (h->h_st->done) break;
     batch = 4;
   }
-  launch_x0(s, g, indc, h->xw, x0, st);
+  launch_x0(s, g, q, ic, h->xw, x0, st);
   CK(cudaGetLastError());
   const SolveState &hs = *h->h_st;
   iter = hs.iter;
@@ -360,8 +362,8 @@ static int do_v1cal(cadmas_handle *h) {
   rc = map_iter(iter, h->P.icgmax);
   if (rc) return rc;
   if (h->P.diag_relres) {
-    launch_relres(s, h->g, a, h->indc, PT, h->rb0, h->rb1);
-    launch_fin(s, FIN_STORE, h->rb0, h->rb1, nrows(h), h->st, h->dres + 2, 0, 0, 0, 0);
+    launch_relres(s, h->g, h->q, h->S, h->bb_sl, h->xw, h->rb0, h->rb1);
+    launch_fin(s, FIN_STORE, h->rb0, h->rb1, h->nslab, h->st, h->dres + 2, 0, 0, 0, 0);
     CK(cudaMemcpyAsync(h->h_res, h->dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     h->stats.true_relres = h->h_res[3] > 0.0 ? std::sqrt(h->h_res[2]) / std::sqrt(h->h_res[3]) : 0.0;
@@ -517,19 +519,21 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
   AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
   for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
-  AL(h->xw, h->N); AL(h->y2, h->N); AL(h->r0, h->N); AL(h->rr, h->N);
-  AL(h->pv, h->N); AL(h->ap, h->N); AL(h->ae, h->N);
   h->q.TI = TI; h->q.TJ = TJ; h->q.T = TI * TJ;
   h->q.W = (d->numk - 2) + (TI - 1) + (TJ - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJ - 1) / TJ);
+  h->nsl = (size_t)h->q.nb * h->q.W * h->q.T;
+  h->nslab = (long long)h->q.nb * h->q.W;
   {
-    const size_t nsl = (size_t)h->q.nb * h->q.W * h->q.T;
+    const size_t nsl = h->nsl;
     AL(h->S.ad, nsl); AL(h->S.ali, nsl); AL(h->S.alj, nsl); AL(h->S.alk, nsl);
     AL(h->S.aui, nsl); AL(h->S.auj, nsl); AL(h->S.auk, nsl); AL(h->S.dd, nsl);
-    AL(h->S.indc, nsl); AL(h->tt_sl, nsl);
+    AL(h->S.indc, nsl); AL(h->tt_sl, nsl); AL(h->bb_sl, nsl);
+    AL(h->xw, nsl); AL(h->y2, nsl); AL(h->r0, nsl); AL(h->rr, nsl);
+    AL(h->pv, nsl); AL(h->ap, nsl); AL(h->ae, nsl);
   }
-  AL(h->rb0, (size_t)nrows(h)); AL(h->rb1, (size_t)nrows(h)); AL(h->dres, 8);
+  AL(h->rb0, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->rb1, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->dres, 8);
   AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
 #undef AL
   if (!rc && cudaMallocHost((void **)&h->h_st, sizeof(SolveState)) != cudaSuccess) rc = CADMAS_ENOMEM;
@@ -556,7 +560,7 @@ int cadmas_destroy(cadmas_handle *h) {
   double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
                   h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
                   h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->rb0, h->rb1, h->dres,
-                  h->S.ad, h->S.ali, h->S.alj, h->S.alk, h->S.aui, h->S.auj, h->S.auk, h->S.dd, h->tt_sl};
+                  h->S.ad, h->S.ali, h->S.alj, h->S.alk, h->S.aui, h->S.auj, h->S.auk, h->S.dd, h->tt_sl, h->bb_sl};
   for (double *q : dl) if (q) cudaFree(q);
   for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) if (h->vel[b][c]) cudaFree(h->vel[b][c]);
   for (double *q : h->wk) if (q) cudaFree(q);

@@ -209,7 +209,8 @@ __device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, in
 
 // Copy the Poisson system (7 coefficients) and INDC into the skewed layout.
 // Entries outside the tile or the interior get 0 (INDC -1).
-__global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S) {
+__global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
+                          double *bsl, double *xsl) {
   const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int t = (int)(e % q.T);
@@ -217,17 +218,45 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
     const int w = (int)(bw % q.W), b = (int)(bw / q.W);
     const int ti = t % q.TI, tj = t / q.TI;
     const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
-    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    double v[7] = {0, 0, 0, 0, 0, 0, 0}, bv = 0.0, xv = 0.0;
     int ic = -1;
     if (I <= g.NI - 1 && J <= g.NJ - 1 && k >= 2 && k <= g.NK - 1) {
       const long long c = cid(g, I, J, k);
       v[0] = A_.ad[c]; v[1] = A_.ali[c]; v[2] = A_.alj[c]; v[3] = A_.alk[c];
       v[4] = A_.aui[c]; v[5] = A_.auj[c]; v[6] = A_.auk[c];
       ic = INDC[c];
+      bv = A_.bb[c];
+      xv = X0[c];
     }
     S.ad[e] = v[0]; S.ali[e] = v[1]; S.alj[e] = v[2]; S.alk[e] = v[3];
     S.aui[e] = v[4]; S.auj[e] = v[5]; S.auk[e] = v[6]; S.indc[e] = ic;
+    bsl[e] = bv;
+    xsl[e] = xv;
   }
+}
+
+// Value of a skewed vector at the cell (ti,tj,k) of tile (bx,by), where ti
+// and tj may step one past the tile into the neighbouring tile; cells
+// outside the interior are the zero ghost layer of the reference vectors.
+__device__ __forceinline__ long long skew_nb(const Geo &g, const SkewGeo &q, int bx, int by, int ti, int tj,
+                                             int k) {
+  if (ti < 0) { bx -= 1; ti += q.TI; } else if (ti >= q.TI) { bx += 1; ti -= q.TI; }
+  if (tj < 0) { by -= 1; tj += q.TJ; } else if (tj >= q.TJ) { by += 1; tj -= q.TJ; }
+  const int I = 2 + bx * q.TI + ti, J = 2 + by * q.TJ + tj;
+  if (bx < 0 || by < 0 || I > g.NI - 1 || J > g.NJ - 1 || k < 2 || k > g.NK - 1) return -1;
+  return sl_index(q, bx + q.ntx * by, (k - 2) + ti + tj, ti + q.TI * tj);
+}
+__device__ __forceinline__ double skew_at(const Geo &g, const SkewGeo &q, const double *X, int bx, int by,
+                                          int ti, int tj, int k) {
+  const long long e = skew_nb(g, q, bx, by, ti, tj, k);
+  return e < 0 ? 0.0 : X[e];
+}
+// Asynchronous copy of a neighbour value into shared memory (0 for ghosts).
+__device__ __forceinline__ void skew_fetch(double *dst, const Geo &g, const SkewGeo &q, const double *X, int bx,
+                                           int by, int ti, int tj, int k) {
+  const long long e = skew_nb(g, q, bx, by, ti, tj, k);
+  if (e < 0) *dst = 0.0;
+  else cp_async8(dst, X + e);
 }
 
 // ------------------------------------------------------------ VF_MZDCMP
@@ -310,27 +339,28 @@ __global__ void k_fwd(Geo g, SkewGeo q, SkewSys S, const double *y, const double
   const int TI = q.TI, T = q.T;
   Ring<NV> rg = ring_setup<NV>(T, R);
   TileGeo t = tile_geo(g, TI, q.TJ);
-  const int I = t.is + t.ti, J = t.js + t.tj, tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
-  const long long NIJ = (long long)g.NI * g.NJ;
+  const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
+  const int bx = blockIdx.x, by = blockIdx.y;
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
   const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
   auto prefetch = [&](int s) {
     const int k = 2 + s - t.ti - t.tj;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long c = cid(g, I, J, k), e = sl_index(q, b, s, tid);
+      const long long e = sl_index(q, b, s, tid);
       const int sl = s % R;
       if (FUSED) {
         cp_async8(&rg.v(sl, 0, tid), S.ad + e);  cp_async8(&rg.v(sl, 1, tid), S.ali + e);
         cp_async8(&rg.v(sl, 2, tid), S.alj + e); cp_async8(&rg.v(sl, 3, tid), S.alk + e);
         cp_async8(&rg.v(sl, 4, tid), S.aui + e); cp_async8(&rg.v(sl, 5, tid), S.auj + e);
         cp_async8(&rg.v(sl, 6, tid), S.auk + e); cp_async8(&rg.v(sl, 7, tid), S.dd + e);
-        cp_async8(&rg.v(sl, 8, tid), P + c);
-        if (ex0) cp_async8(&rg.v(sl, 9, tid), P + c - 1);
-        if (ex1) cp_async8(&rg.v(sl, 10, tid), P + c + 1);
-        if (ey0) cp_async8(&rg.v(sl, 11, tid), P + c - g.NI);
-        if (ey1) cp_async8(&rg.v(sl, 12, tid), P + c + g.NI);
+        cp_async8(&rg.v(sl, 8, tid), P + e);
+        // values of the neighbouring tiles (or the zero ghost layer)
+        if (ex0) skew_fetch(&rg.v(sl, 9, tid), g, q, P, bx, by, t.ti - 1, t.tj, k);
+        if (ex1) skew_fetch(&rg.v(sl, 10, tid), g, q, P, bx, by, t.ti + 1, t.tj, k);
+        if (ey0) skew_fetch(&rg.v(sl, 11, tid), g, q, P, bx, by, t.ti, t.tj - 1, k);
+        if (ey1) skew_fetch(&rg.v(sl, 12, tid), g, q, P, bx, by, t.ti, t.tj + 1, k);
       } else {
-        cp_async8(&rg.v(sl, 0, tid), y + c);      cp_async8(&rg.v(sl, 1, tid), S.ali + e);
+        cp_async8(&rg.v(sl, 0, tid), y + e);      cp_async8(&rg.v(sl, 1, tid), S.ali + e);
         cp_async8(&rg.v(sl, 2, tid), S.alj + e);  cp_async8(&rg.v(sl, 3, tid), S.alk + e);
         cp_async8(&rg.v(sl, 4, tid), S.dd + e);
       }
@@ -353,14 +383,13 @@ __global__ void k_fwd(Geo g, SkewGeo q, SkewSys S, const double *y, const double
       if (rg.ind(sl, tid) != -1) {
         double yv;
         if (FUSED) {
-          const long long c = cid(g, I, J, k);
           const double pc = rg.v(sl, 8, tid);
           const double pxm = ex0 ? rg.v(sl, 9, tid) : rg.v(slp, 8, tid - 1);
           const double pym = ey0 ? rg.v(sl, 11, tid) : rg.v(slp, 8, tid - TI);
-          const double pzm = (k > 2) ? rg.v(slp, 8, tid) : P[c - NIJ];
+          const double pzm = (k > 2) ? rg.v(slp, 8, tid) : 0.0;
           const double pxp = ex1 ? rg.v(sl, 10, tid) : rg.v(sln, 8, tid + 1);
           const double pyp = ey1 ? rg.v(sl, 12, tid) : rg.v(sln, 8, tid + TI);
-          const double pzp = (k < g.NK - 1) ? rg.v(sln, 8, tid) : P[c + NIJ];
+          const double pzp = (k < g.NK - 1) ? rg.v(sln, 8, tid) : 0.0;
           yv = rg.v(sl, 0, tid) * pc + rg.v(sl, 1, tid) * pxm + rg.v(sl, 2, tid) * pym +
                rg.v(sl, 3, tid) * pzm + rg.v(sl, 4, tid) * pxp + rg.v(sl, 5, tid) * pyp +
                rg.v(sl, 6, tid) * pzp;
@@ -422,142 +451,158 @@ __global__ void k_bwd(Geo g, SkewGeo q, SkewSys S, const double *Tin, double *X,
         x = (rg.v(sl, 0, tid) - rg.v(sl, 1, tid) * x1 - rg.v(sl, 2, tid) * x2 - rg.v(sl, 3, tid) * xk1) *
             rg.v(sl, 4, tid);
       }
-      X[cid(g, I, J, k)] = x;
+      X[sl_index(q, b, (k - 2) + t.ti + t.tj, tid)] = x;
       rg.xb[cur * T + tid] = x;
       xk1 = x;
     }
   }
   cp_wait<0>();
+  (void)I; (void)J;
 }
 
-// ------------------------------------------------------------ row kernels
+// ------------------------------------------------------------ slab kernels
+// The BiCGSTAB vectors live in the skewed layout; a vector kernel maps one
+// warp to one slab (b,w) of T entries and lets lane l visit t = l, l+32, ...
+// The dot products (VF_MZIP) sum in that order: lane partials, warp tree
+// per slab, then the 1024-thread tree over the slab partials (block_final).
+// Padding entries carry INDC = -1 and are skipped like non-computed cells.
+#define SLAB_LOOP_BEGIN(q)                                                          \
+  const int lane_ = threadIdx.x & 31;                                               \
+  const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
+  if (slab_ < (long long)(q).nb * (q).W) {                                          \
+    for (int t_ = lane_; t_ < (q).T; t_ += 32) {                                    \
+      const long long e = slab_ * (q).T + t_;
+#define SLAB_LOOP_END \
+    }                 \
+  }
+#define SLAB_ROW ((long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5))
+
 __device__ __forceinline__ bool interior(const Geo &g, int I, int J, int K) {
   return I >= 2 && I <= g.NI - 1 && J >= 2 && J <= g.NJ - 1 && K >= 2 && K <= g.NK - 1;
 }
 
+// A*X at skewed entry e (VF_MZAX expression, vf_mzax.f:46-53).
+__device__ __forceinline__ double skew_ax(const Geo &g, const SkewGeo &q, const SkewSys &S, const double *X,
+                                          long long e) {
+  const int t = (int)(e % q.T);
+  const long long bw = e / q.T;
+  const int w = (int)(bw % q.W), b = (int)(bw / q.W);
+  const int ti = t % q.TI, tj = t / q.TI, bx = b % q.ntx, by = b / q.ntx, k = 2 + w - ti - tj;
+  return S.ad[e] * X[e] + S.ali[e] * skew_at(g, q, X, bx, by, ti - 1, tj, k) +
+         S.alj[e] * skew_at(g, q, X, bx, by, ti, tj - 1, k) + S.alk[e] * skew_at(g, q, X, bx, by, ti, tj, k - 1) +
+         S.aui[e] * skew_at(g, q, X, bx, by, ti + 1, tj, k) + S.auj[e] * skew_at(g, q, X, bx, by, ti, tj + 1, k) +
+         S.auk[e] * skew_at(g, q, X, bx, by, ti, tj, k + 1);
+}
+
 // Y = A X on INDC != -1 (VF_MZAX); Y untouched elsewhere.
-__global__ void k_spmv(Geo g, SysPtr A_, const int *INDC, const double *X, double *Y,
-                       const SolveState *st) {
+__global__ void k_spmv(Geo g, SkewGeo q, SkewSys S, const double *X, double *Y, const SolveState *st) {
   if (st && st->done) return;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) {
-    Y[c] = A_.ad[c] * X[c] + A_.ali[c] * X[c - 1] + A_.alj[c] * X[c - g.NI] +
-           A_.alk[c] * X[c - (long long)g.NI * g.NJ] + A_.aui[c] * X[c + 1] +
-           A_.auj[c] * X[c + g.NI] + A_.auk[c] * X[c + (long long)g.NI * g.NJ];
-  }
-  ROW_LOOP_END
+  SLAB_LOOP_BEGIN(q)
+  if (S.indc[e] != -1) Y[e] = skew_ax(g, q, S, X, e);
+  SLAB_LOOP_END
 }
 
 // Y = B - Y on INDC != -1 (vf_m1bcgs.f:124-132)
-__global__ void k_bmy(Geo g, const int *INDC, const double *B, double *Y, const SolveState *st) {
+__global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, const SolveState *st) {
   if (st->done) return;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) Y[c] = B[c] - Y[c];
-  ROW_LOOP_END
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) Y[e] = B[e] - Y[e];
+  SLAB_LOOP_END
 }
 
-// Row partials of up to two dot products (VF_MZIP).
-__global__ void k_dot(Geo g, const int *INDC, const double *x0, const double *y0, const double *x1,
+// Slab partials of up to two dot products (VF_MZIP).
+__global__ void k_dot(SkewGeo q, const int *INDC, const double *x0, const double *y0, const double *x1,
                       const double *y1, double *rb0, double *rb1, const SolveState *st) {
   if (st && st->done) return;
   double s0 = 0.0, s1 = 0.0;
-  const long long nrows = (long long)g.NJ * g.NK;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) {
-    s0 = s0 + x0[c] * y0[c];
-    if (x1) s1 = s1 + x1[c] * y1[c];
+  const long long nslab = (long long)q.nb * q.W;
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) {
+    s0 = s0 + x0[e] * y0[e];
+    if (x1) s1 = s1 + x1[e] * y1[e];
   }
-  ROW_LOOP_END
-  const long long row = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5);
-  row_store(s0, rb0, row, nrows);
-  if (x1) row_store(s1, rb1, row, nrows);
+  SLAB_LOOP_END
+  row_store(s0, rb0, SLAB_ROW, nslab);
+  if (x1) row_store(s1, rb1, SLAB_ROW, nslab);
 }
 
 // RR = R0, PP = R0
-__global__ void k_copy2(Geo g, const int *INDC, const double *R0, double *RR, double *PP,
+__global__ void k_copy2(SkewGeo q, const int *INDC, const double *R0, double *RR, double *PP,
                         const SolveState *st) {
   if (st->done) return;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) { RR[c] = R0[c]; PP[c] = R0[c]; }
-  ROW_LOOP_END
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) { RR[e] = R0[e]; PP[e] = R0[e]; }
+  SLAB_LOOP_END
 }
 
 // RR = RR - ALPHA*AP (vf_m1bcgs.f:181-189)
-__global__ void k_axpy_rr(Geo g, const int *INDC, const double *AP, double *RR, const SolveState *st) {
+__global__ void k_axpy_rr(SkewGeo q, const int *INDC, const double *AP, double *RR, const SolveState *st) {
   if (st->done) return;
   const double alpha = st->alpha;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) RR[c] = RR[c] - alpha * AP[c];
-  ROW_LOOP_END
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) RR[e] = RR[e] - alpha * AP[e];
+  SLAB_LOOP_END
 }
 
-// XW = XW + (ALPHA*PP + OMEGA*RR); RR = RR - OMEGA*AE; row partials of
+// XW = XW + (ALPHA*PP + OMEGA*RR); RR = RR - OMEGA*AE; slab partials of
 // (RR,RR) and (R0,RR) on the updated RR (vf_m1bcgs.f:206-225).
-__global__ void k_upd_xr(Geo g, const int *INDC, const double *PP, const double *AE, const double *R0,
+__global__ void k_upd_xr(SkewGeo q, const int *INDC, const double *PP, const double *AE, const double *R0,
                          double *XW, double *RR, double *rb0, double *rb1, const SolveState *st) {
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
   double s0 = 0.0, s1 = 0.0;
-  const long long nrows = (long long)g.NJ * g.NK;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) {
-    XW[c] = XW[c] + (alpha * PP[c] + omega * RR[c]);
-    double r = RR[c] - omega * AE[c];
-    RR[c] = r;
+  const long long nslab = (long long)q.nb * q.W;
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) {
+    XW[e] = XW[e] + (alpha * PP[e] + omega * RR[e]);
+    double r = RR[e] - omega * AE[e];
+    RR[e] = r;
     s0 = s0 + r * r;
-    s1 = s1 + R0[c] * r;
+    s1 = s1 + R0[e] * r;
   }
-  ROW_LOOP_END
-  const long long row = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5);
-  row_store(s0, rb0, row, nrows);
-  row_store(s1, rb1, row, nrows);
+  SLAB_LOOP_END
+  row_store(s0, rb0, SLAB_ROW, nslab);
+  row_store(s1, rb1, SLAB_ROW, nslab);
 }
 
 // PP = RR + BETA*(PP - OMEGA*AP) (vf_m1bcgs.f:229-238)
-__global__ void k_upd_p(Geo g, const int *INDC, const double *RR, const double *AP, double *PP,
+__global__ void k_upd_p(SkewGeo q, const int *INDC, const double *RR, const double *AP, double *PP,
                         const SolveState *st) {
   if (st->done) return;
   const double beta = st->beta, omega = st->omega;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) PP[c] = RR[c] + beta * (PP[c] - omega * AP[c]);
-  ROW_LOOP_END
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) PP[e] = RR[e] + beta * (PP[e] - omega * AP[e]);
+  SLAB_LOOP_END
 }
 
-// X0 = XW on INDC != -1 when ITER >= 0 (vf_m1bcgs.f:251-261)
-__global__ void k_x0(Geo g, const int *INDC, const double *XW, double *X0, const SolveState *st) {
+// X0 = XW on INDC != -1 when ITER >= 0 (vf_m1bcgs.f:251-261), back to the
+// standard layout.
+__global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double *X0, const SolveState *st) {
   if (st->iter < 0) return;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (INDC[c] != -1) X0[c] = XW[c];
-  ROW_LOOP_END
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) {
+    const int ti = t_ % q.TI, tj = t_ / q.TI;
+    const int w = (int)(slab_ % q.W), b = (int)(slab_ / q.W);
+    const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
+    X0[cid(g, I, J, k)] = XW[e];
+  }
+  SLAB_LOOP_END
 }
 
-// ||b-Ax||^2 and ||b||^2 row partials (diagnostic of the metric)
-__global__ void k_relres(Geo g, SysPtr A_, const int *INDC, const double *X, double *rb0,
+// ||b-Ax||^2 and ||b||^2 slab partials (diagnostic of the metric)
+__global__ void k_relres(Geo g, SkewGeo q, SkewSys S, const double *B, const double *X, double *rb0,
                          double *rb1) {
   double s0 = 0.0, s1 = 0.0;
-  const long long nrows = (long long)g.NJ * g.NK;
-  ROW_LOOP_BEGIN(g)
-  const long long c = cid(g, I, J, K);
-  if (interior(g, I, J, K) && INDC[c] != -1) {
-    double ax = A_.ad[c] * X[c] + A_.ali[c] * X[c - 1] + A_.alj[c] * X[c - g.NI] +
-                A_.alk[c] * X[c - (long long)g.NI * g.NJ] + A_.aui[c] * X[c + 1] +
-                A_.auj[c] * X[c + g.NI] + A_.auk[c] * X[c + (long long)g.NI * g.NJ];
-    double r = A_.bb[c] - ax;
+  const long long nslab = (long long)q.nb * q.W;
+  SLAB_LOOP_BEGIN(q)
+  if (S.indc[e] != -1) {
+    double r = B[e] - skew_ax(g, q, S, X, e);
     s0 = s0 + r * r;
-    s1 = s1 + A_.bb[c] * A_.bb[c];
+    s1 = s1 + B[e] * B[e];
   }
-  ROW_LOOP_END
-  const long long row = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5);
-  row_store(s0, rb0, row, nrows);
-  row_store(s1, rb1, row, nrows);
+  SLAB_LOOP_END
+  row_store(s0, rb0, SLAB_ROW, nslab);
+  row_store(s1, rb1, SLAB_ROW, nslab);
 }
 
 // ------------------------------------------------------------- finalisers
@@ -704,10 +749,10 @@ static inline dim3 skew_grid(const SkewGeo &q) { return dim3((unsigned)q.ntx, (u
   } while (0)
 
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
-                    const SkewSys &S) {
+                    const SkewSys &S, const double *x0, double *bsl, double *xsl) {
   const long long n = (long long)q.nb * q.W * q.T;
   const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-  k_to_skew<<<blocks, 256, 0, s>>>(g, q, a, indc, S);
+  k_to_skew<<<blocks, 256, 0, s>>>(g, q, a, indc, S, x0, bsl, xsl);
   count_launch();
 }
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad) {
@@ -715,12 +760,11 @@ void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const
   RING_LAUNCH2(k_dcmp, 7, g, q, U, S, pivot_bad);
 #undef RING_EXTRA
 }
-void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const SkewSys &S,
-                const int *indc, const double *y, const double *spmv_x, double *tout, const SolveState *st,
-                double *ybuf) {
+void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
+                const double *spmv_x, double *tout, const SolveState *st, double *ybuf) {
   if (spmv_x && ring_depth(13, q.T) == 0) {
     // Ring of the fused kernel too large for this tile: SpMV first.
-    launch_spmv(s, g, a, indc, spmv_x, ybuf, st);
+    launch_spmv(s, g, q, S, spmv_x, ybuf, st);
     y = ybuf;
     spmv_x = nullptr;
   }
@@ -740,51 +784,33 @@ void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S
   RING_LAUNCH2(k_bwd, 5, g, q, S, tin, x, st);
 #undef RING_EXTRA
 }
-void launch_spmv(cudaStream_t s, const Geo &g, const SysPtr &a, const int *indc, const double *x, double *y,
-                 const SolveState *st) {
-  k_spmv<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, a, indc, x, y, st);
-  count_launch();
+static inline unsigned slab_blocks(const SkewGeo &q) {
+  return (unsigned)(((long long)q.nb * q.W + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK);
 }
-void launch_bmy(cudaStream_t s, const Geo &g, const int *indc, const double *b, double *y,
-                const SolveState *st) {
-  k_bmy<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, b, y, st);
-  count_launch();
-}
-void launch_dot(cudaStream_t s, const Geo &g, const int *indc, const double *x0, const double *y0,
+#define SL(kern, ...) (kern<<<slab_blocks(q), ROW_THREADS, 0, s>>>(__VA_ARGS__), count_launch())
+void launch_spmv(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *x, double *y,
+                 const SolveState *st) { SL(k_spmv, g, q, S, x, y, st); }
+void launch_bmy(cudaStream_t s, const SkewGeo &q, const int *indc, const double *b, double *y,
+                const SolveState *st) { SL(k_bmy, q, indc, b, y, st); }
+void launch_dot(cudaStream_t s, const SkewGeo &q, const int *indc, const double *x0, const double *y0,
                 const double *x1, const double *y1, double *rb0, double *rb1, const SolveState *st) {
-  k_dot<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, x0, y0, x1, y1, rb0, rb1, st);
-  count_launch();
+  SL(k_dot, q, indc, x0, y0, x1, y1, rb0, rb1, st);
 }
-void launch_copy2(cudaStream_t s, const Geo &g, const int *indc, const double *r0, double *rr,
-                  double *pp, const SolveState *st) {
-  k_copy2<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, r0, rr, pp, st);
-  count_launch();
-}
-void launch_axpy_rr(cudaStream_t s, const Geo &g, const int *indc, const double *ap, double *rr,
-                    const SolveState *st) {
-  k_axpy_rr<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, ap, rr, st);
-  count_launch();
-}
-void launch_upd_xr(cudaStream_t s, const Geo &g, const int *indc, const double *pp, const double *ae,
+void launch_copy2(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r0, double *rr, double *pp,
+                  const SolveState *st) { SL(k_copy2, q, indc, r0, rr, pp, st); }
+void launch_axpy_rr(cudaStream_t s, const SkewGeo &q, const int *indc, const double *ap, double *rr,
+                    const SolveState *st) { SL(k_axpy_rr, q, indc, ap, rr, st); }
+void launch_upd_xr(cudaStream_t s, const SkewGeo &q, const int *indc, const double *pp, const double *ae,
                    const double *r0, double *xw, double *rr, double *rb0, double *rb1, const SolveState *st) {
-  k_upd_xr<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, pp, ae, r0, xw, rr, rb0, rb1, st);
-  count_launch();
+  SL(k_upd_xr, q, indc, pp, ae, r0, xw, rr, rb0, rb1, st);
 }
-void launch_upd_p(cudaStream_t s, const Geo &g, const int *indc, const double *rr, const double *ap,
-                  double *pp, const SolveState *st) {
-  k_upd_p<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, rr, ap, pp, st);
-  count_launch();
-}
-void launch_x0(cudaStream_t s, const Geo &g, const int *indc, const double *xw, double *x0,
-               const SolveState *st) {
-  k_x0<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, indc, xw, x0, st);
-  count_launch();
-}
-void launch_relres(cudaStream_t s, const Geo &g, const SysPtr &a, const int *indc, const double *x,
-                   double *rb0, double *rb1) {
-  k_relres<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, a, indc, x, rb0, rb1);
-  count_launch();
-}
+void launch_upd_p(cudaStream_t s, const SkewGeo &q, const int *indc, const double *rr, const double *ap,
+                  double *pp, const SolveState *st) { SL(k_upd_p, q, indc, rr, ap, pp, st); }
+void launch_x0(cudaStream_t s, const Geo &g, const SkewGeo &q, const int *indc, const double *xw, double *x0,
+               const SolveState *st) { SL(k_x0, g, q, indc, xw, x0, st); }
+void launch_relres(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *b,
+                   const double *x, double *rb0, double *rb1) { SL(k_relres, g, q, S, b, x, rb0, rb1); }
+#undef SL
 void launch_fin(cudaStream_t s, int mode, const double *rb0, const double *rb1, long long nrows,
                 SolveState *st, double *out, double epsa2, double epsr2, double div2, int icgmax) {
   k_fin<<<1, 1024, 0, s>>>(mode, rb0, rb1, nrows, st, out, epsa2, epsr2, div2, icgmax);

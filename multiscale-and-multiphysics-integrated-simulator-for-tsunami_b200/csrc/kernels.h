@@ -39,32 +39,30 @@ void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, int *err);
 // k_poisson.cu
 void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const SysPtr &a, int *err);
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
-                    const SkewSys &S);
+                    const SkewSys &S, const double *x0, double *bsl, double *xsl);
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad);
-void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const SkewSys &S,
-                const int *indc, const double *y, const double *spmv_x, double *tout, const SolveState *st,
-                double *ybuf);
+void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
+                const double *spmv_x, double *tout, const SolveState *st, double *ybuf);
 void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
                 double *x, const SolveState *st);
-void launch_spmv(cudaStream_t s, const Geo &g, const SysPtr &a, const int *indc, const double *x,
-                 double *y, const SolveState *st);
-void launch_bmy(cudaStream_t s, const Geo &g, const int *indc, const double *b, double *y,
+void launch_spmv(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *x, double *y,
+                 const SolveState *st);
+void launch_bmy(cudaStream_t s, const SkewGeo &q, const int *indc, const double *b, double *y,
                 const SolveState *st);
-void launch_dot(cudaStream_t s, const Geo &g, const int *indc, const double *x0, const double *y0,
+void launch_dot(cudaStream_t s, const SkewGeo &q, const int *indc, const double *x0, const double *y0,
                 const double *x1, const double *y1, double *rb0, double *rb1, const SolveState *st);
-void launch_copy2(cudaStream_t s, const Geo &g, const int *indc, const double *r0, double *rr,
-                  double *pp, const SolveState *st);
-void launch_axpy_rr(cudaStream_t s, const Geo &g, const int *indc, const double *ap, double *rr,
+void launch_copy2(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r0, double *rr, double *pp,
+                  const SolveState *st);
+void launch_axpy_rr(cudaStream_t s, const SkewGeo &q, const int *indc, const double *ap, double *rr,
                     const SolveState *st);
-void launch_upd_xr(cudaStream_t s, const Geo &g, const int *indc, const double *pp, const double *ae,
-                   const double *r0, double *xw, double *rr, double *rb0, double *rb1,
-                   const SolveState *st);
-void launch_upd_p(cudaStream_t s, const Geo &g, const int *indc, const double *rr, const double *ap,
+void launch_upd_xr(cudaStream_t s, const SkewGeo &q, const int *indc, const double *pp, const double *ae,
+                   const double *r0, double *xw, double *rr, double *rb0, double *rb1, const SolveState *st);
+void launch_upd_p(cudaStream_t s, const SkewGeo &q, const int *indc, const double *rr, const double *ap,
                   double *pp, const SolveState *st);
-void launch_x0(cudaStream_t s, const Geo &g, const int *indc, const double *xw, double *x0,
+void launch_x0(cudaStream_t s, const Geo &g, const SkewGeo &q, const int *indc, const double *xw, double *x0,
                const SolveState *st);
-void launch_relres(cudaStream_t s, const Geo &g, const SysPtr &a, const int *indc, const double *x,
-                   double *rb0, double *rb1);
+void launch_relres(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *b,
+                   const double *x, double *rb0, double *rb1);
 void launch_fin(cudaStream_t s, int mode, const double *rb0, const double *rb1, long long nrows,
                 SolveState *st, double *out, double epsa2, double epsr2, double div2, int icgmax);
 void launch_pivot_check(cudaStream_t s, SolveState *st);

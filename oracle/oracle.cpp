@@ -134,6 +134,48 @@ struct orc_handle {
     return warp_tree(w);
   }
 
+  // The same tree over the slabs of the GPU solver's tile-skewed layout:
+  // tile b (x fastest), wavefront slab w = (k-2)+ti+tj, slab entry
+  // t = ti + TI*tj; lane l of a slab sums t = l, l+32, ... in order, warp
+  // tree per slab, then the 1024-thread tree over the slabs.  This is the
+  // order of the dot products of VF_M1BCGS in the GPU library.
+  template <class F> double gsum_skew(F f) const {
+    const int TI = std::min(P.precond_ti > 0 ? P.precond_ti : NI - 2, NI - 2);
+    const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2);
+    const int T = TI * TJ, W = (NK - 2) + (TI - 1) + (TJ - 1);
+    const int ntx = (NI - 2 + TI - 1) / TI, nb = ntx * ((NJ - 2 + TJ - 1) / TJ);
+    const long long NS = (long long)nb * W;
+    std::vector<double> R(NS);
+    double lane[32];
+    for (long long sl = 0; sl < NS; ++sl) {
+      const int b = (int)(sl / W), w = (int)(sl % W), bx = b % ntx, by = b / ntx;
+      for (int l = 0; l < 32; ++l) {
+        double s = 0.0, c;
+        for (int t = l; t < T; t += 32) {
+          const int ti = t % TI, tj = t / TI;
+          const int I = 2 + bx * TI + ti, J = 2 + by * TJ + tj, k = 2 + w - ti - tj;
+          if (I > NI - 1 || J > NJ - 1 || k < 2 || k > NK - 1) continue;
+          if (f(I, J, k, c)) s = s + c;
+        }
+        lane[l] = s;
+      }
+      R[sl] = warp_tree(lane);
+    }
+    double u[1024];
+    for (int t = 0; t < 1024; ++t) {
+      double s = 0.0;
+      for (long long r = t; r < NS; r += 1024) s = s + R[r];
+      u[t] = s;
+    }
+    double wv[32];
+    for (int q = 0; q < 32; ++q) wv[q] = warp_tree(u + 32 * q);
+    return warp_tree(wv);
+  }
+
+  template <class F> double solver_sum(F f) const {
+    return sum_mode == ORC_SUM_GPU ? gsum_skew(f) : gsum(f);
+  }
+
   // interior mask helper used by gsum callers
   inline bool interior(int i, int j, int k) const {
     return i >= 2 && i <= NI - 1 && j >= 2 && j <= NJ - 1 && k >= 2 && k <= NK - 1;
@@ -957,7 +999,7 @@ struct orc_handle {
       }
       return S;
     }
-    return gsum([&](int i, int j, int k, double &c) {
+    return gsum_skew([&](int i, int j, int k, double &c) {
       size_t q = id(i, j, k);
       if (IC[q] == -1) return false;
       c = X[q] * Yv[q];
@@ -1027,7 +1069,7 @@ struct orc_handle {
   // ||b - A x||_2 / ||b||_2 over INDC != -1 (diagnostic of the metric)
   double true_relres(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
                      const vd &AUJ, const vd &AUK, const vd &BB, const vd &X, const int *IC) {
-    double rn = gsum([&](int I, int J, int K, double &c) {
+    double rn = solver_sum([&](int I, int J, int K, double &c) {
       if (!interior(I, J, K)) return false;
       size_t q = id(I, J, K);
       if (IC[q] == -1) return false;
@@ -1038,7 +1080,7 @@ struct orc_handle {
       c = r * r;
       return true;
     });
-    double bn = gsum([&](int I, int J, int K, double &c) {
+    double bn = solver_sum([&](int I, int J, int K, double &c) {
       size_t q = id(I, J, K);
       if (!interior(I, J, K) || IC[q] == -1) return false;
       c = BB[q] * BB[q];
