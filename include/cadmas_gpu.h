@@ -44,6 +44,7 @@ extern "C" {
 #define CADMAS_ENOMEM        8  /* device allocation failed                      */
 #define CADMAS_EUNSUPPORTED  9  /* option outside the implemented path           */
 #define CADMAS_ENOSTATIC    10  /* cadmas_upload_static not called yet           */
+#define CADMAS_ETIMEOUT     11  /* a device-side wait ran out of time (2 s)      */
 
 /* ---- sizes (/VF_ANUMBI/, VF_ANUMBI.h) ----------------------------------- */
 typedef struct cadmas_dims {

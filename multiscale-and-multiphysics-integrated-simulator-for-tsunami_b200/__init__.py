@@ -25,7 +25,7 @@ from . import cases  # noqa: F401  (re-exported)
 HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = HERE / "libcadmas_gpu.so"
 
-OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC = range(11)
+OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC, ETIMEOUT = range(12)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

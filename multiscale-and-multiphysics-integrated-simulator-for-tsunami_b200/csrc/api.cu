@@ -269,6 +269,10 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h->h_st, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (h->h_st->timeout) {
+      g_last_error = "a bulk-copy wait of the MILU sweep ran out of time";
+      return CADMAS_ETIMEOUT;
+    }
     if (h->h_st->done) break;
     batch = 4;
   }
@@ -468,6 +472,7 @@ const char *cadmas_strerror(int status) {
     case CADMAS_ENOMEM: return "device allocation failed";
     case CADMAS_EUNSUPPORTED: return "option outside the implemented path";
     case CADMAS_ENOSTATIC: return "static fields not uploaded";
+    case CADMAS_ETIMEOUT: return "a device-side wait ran out of time";
     default: return "unknown status";
   }
 }
@@ -519,16 +524,19 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
   AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
   for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
-  h->q.TI = TI; h->q.TJ = TJ; h->q.T = TI * TJ;
+  h->q.TI = TI; h->q.TJ = TJ; h->q.TIp = TI + (TI & 1); h->q.T = h->q.TIp * TJ;
   h->q.W = (d->numk - 2) + (TI - 1) + (TJ - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJ - 1) / TJ);
+  if (!sweep_supported(h->q)) {
+    g_last_error = "preconditioner block too large for the MILU sweeps; set precond_ti/precond_tj";
+    rc = CADMAS_EUNSUPPORTED;
+  }
   h->nsl = (size_t)h->q.nb * h->q.W * h->q.T;
   h->nslab = (long long)h->q.nb * h->q.W;
   {
     const size_t nsl = h->nsl;
-    AL(h->S.ad, nsl); AL(h->S.ali, nsl); AL(h->S.alj, nsl); AL(h->S.alk, nsl);
-    AL(h->S.aui, nsl); AL(h->S.auj, nsl); AL(h->S.auk, nsl); AL(h->S.dd, nsl);
+    AL(h->S.sys, (size_t)SYS_N * nsl);
     AL(h->S.indc, nsl); AL(h->tt_sl, nsl); AL(h->bb_sl, nsl);
     AL(h->xw, nsl); AL(h->y2, nsl); AL(h->r0, nsl); AL(h->rr, nsl);
     AL(h->pv, nsl); AL(h->ap, nsl); AL(h->ae, nsl);
@@ -560,7 +568,7 @@ int cadmas_destroy(cadmas_handle *h) {
   double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
                   h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
                   h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->rb0, h->rb1, h->dres,
-                  h->S.ad, h->S.ali, h->S.alj, h->S.alk, h->S.aui, h->S.auj, h->S.auk, h->S.dd, h->tt_sl, h->bb_sl};
+                  h->S.sys, h->tt_sl, h->bb_sl};
   for (double *q : dl) if (q) cudaFree(q);
   for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) if (h->vel[b][c]) cudaFree(h->vel[b][c]);
   for (double *q : h->wk) if (q) cudaFree(q);

@@ -136,6 +136,7 @@ __device__ __forceinline__ double block_final(const double *rowbuf, long long nr
 struct SolveState {
   double S, alpha, omega, beta, bnorm, xnorm, w1, w2, rn, bn;
   int iter, done, status, pivot_bad;
+  int timeout, pad_;  // a bulk-copy wait of a sweep ran out of time
 };
 
 // Error flags raised by kernels (bitmask in a device int).

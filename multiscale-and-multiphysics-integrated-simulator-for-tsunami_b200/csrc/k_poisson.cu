@@ -138,15 +138,15 @@ struct TileGeo {
   int ti, tj;          // thread coordinates
   bool valid;
 };
-__device__ __forceinline__ TileGeo tile_geo(const Geo &g, int TI, int TJ) {
+__device__ __forceinline__ TileGeo tile_geo(const Geo &g, const SkewGeo &q) {
   TileGeo t;
-  t.is = 2 + blockIdx.x * TI;
-  t.js = 2 + blockIdx.y * TJ;
-  t.wi = min(TI, g.NI - t.is);  // interior cells is..NI-1
-  t.wj = min(TJ, g.NJ - t.js);
-  t.ti = threadIdx.x % TI;
-  t.tj = threadIdx.x / TI;
-  t.valid = (t.ti < t.wi) && (t.tj < t.wj);
+  t.is = 2 + blockIdx.x * q.TI;
+  t.js = 2 + blockIdx.y * q.TJ;
+  t.wi = min(q.TI, g.NI - t.is);  // interior cells is..NI-1
+  t.wj = min(q.TJ, g.NJ - t.js);
+  t.ti = threadIdx.x % q.TIp;
+  t.tj = threadIdx.x / q.TIp;
+  t.valid = (t.ti < t.wi) && (t.tj < t.wj);  // also false on the padding column ti = TI
   return t;
 }
 
@@ -197,9 +197,9 @@ inline size_t ring_bytes(int NV, int T, int R) {
 
 // ----------------------------------------------------- tile-skewed layout
 // The MILU kernels visit, at wavefront step s, cell (is+ti, js+tj,
-// k = 2+s-ti-tj) with thread t = ti + TI*tj.  The arrays that stay constant
-// through a solve (7 coefficients, DD, INDC) and the forward-sweep result
-// are stored tile by tile in that visiting order,
+// k = 2+s-ti-tj) with thread t = ti + TIp*tj.  The arrays that stay constant
+// through a solve (7 coefficients, DD, INDC), the right-hand side and the
+// BiCGSTAB vectors are stored tile by tile in that visiting order,
 //     sl(b, w, t) = (b*W + w)*T + t,   w = (k-2) + ti + tj,
 // b = tile index, W = (NK-2) + (TI-1) + (TJ-1), so the T values a block
 // needs at one step are contiguous and every load of the sweep coalesces.
@@ -207,8 +207,9 @@ __device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, in
   return ((long long)b * q.W + w) * q.T + t;
 }
 
-// Copy the Poisson system (7 coefficients) and INDC into the skewed layout.
-// Entries outside the tile or the interior get 0 (INDC -1).
+// Copy the Poisson system (7 coefficients, interleaved per slab; DD set to
+// 0 for MZDCMP to fill), INDC, BB and X0 into the skewed layout.  Entries
+// outside the tile or the interior get 0 (INDC -1).
 __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
                           double *bsl, double *xsl) {
   const long long n = (long long)q.nb * q.W * q.T;
@@ -216,11 +217,11 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
     const int t = (int)(e % q.T);
     const long long bw = e / q.T;
     const int w = (int)(bw % q.W), b = (int)(bw / q.W);
-    const int ti = t % q.TI, tj = t / q.TI;
+    const int ti = t % q.TIp, tj = t / q.TIp;
     const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
     double v[7] = {0, 0, 0, 0, 0, 0, 0}, bv = 0.0, xv = 0.0;
     int ic = -1;
-    if (I <= g.NI - 1 && J <= g.NJ - 1 && k >= 2 && k <= g.NK - 1) {
+    if (ti < q.TI && I <= g.NI - 1 && J <= g.NJ - 1 && k >= 2 && k <= g.NK - 1) {
       const long long c = cid(g, I, J, k);
       v[0] = A_.ad[c]; v[1] = A_.ali[c]; v[2] = A_.alj[c]; v[3] = A_.alk[c];
       v[4] = A_.aui[c]; v[5] = A_.auj[c]; v[6] = A_.auk[c];
@@ -228,8 +229,9 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
       bv = A_.bb[c];
       xv = X0[c];
     }
-    S.ad[e] = v[0]; S.ali[e] = v[1]; S.alj[e] = v[2]; S.alk[e] = v[3];
-    S.aui[e] = v[4]; S.auj[e] = v[5]; S.auk[e] = v[6]; S.indc[e] = ic;
+    for (int c = 0; c < 7; ++c) S.sys[sys_at(bw, c, q.T, t)] = v[c];
+    S.sys[sys_at(bw, SYS_DD, q.T, t)] = 0.0;
+    S.indc[e] = ic;
     bsl[e] = bv;
     xsl[e] = xv;
   }
@@ -244,7 +246,7 @@ __device__ __forceinline__ long long skew_nb(const Geo &g, const SkewGeo &q, int
   if (tj < 0) { by -= 1; tj += q.TJ; } else if (tj >= q.TJ) { by += 1; tj -= q.TJ; }
   const int I = 2 + bx * q.TI + ti, J = 2 + by * q.TJ + tj;
   if (bx < 0 || by < 0 || I > g.NI - 1 || J > g.NJ - 1 || k < 2 || k > g.NK - 1) return -1;
-  return sl_index(q, bx + q.ntx * by, (k - 2) + ti + tj, ti + q.TI * tj);
+  return sl_index(q, bx + q.ntx * by, (k - 2) + ti + tj, ti + q.TIp * tj);
 }
 __device__ __forceinline__ double skew_at(const Geo &g, const SkewGeo &q, const double *X, int bx, int by,
                                           int ti, int tj, int k) {
@@ -265,20 +267,20 @@ __device__ __forceinline__ void skew_fetch(double *dst, const Geo &g, const Skew
 template <int D>
 __global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
   constexpr int NV = 7, R = D + 3;
-  const int TI = q.TI, T = q.T;
+  const int TIp = q.TIp, T = q.T;
   Ring<NV> rg = ring_setup<NV>(T, R);
-  TileGeo t = tile_geo(g, TI, q.TJ);
+  TileGeo t = tile_geo(g, q);
   const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
   auto prefetch = [&](int s) {
     const int k = 2 + s - t.ti - t.tj;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long e = sl_index(q, b, s, tid);
+      const long long slab = (long long)b * q.W + s, e = slab * T + tid;
+      const double *sy = S.sys + sys_at(slab, 0, T, tid);
       const int sl = s % R;
-      cp_async8(&rg.v(sl, 0, tid), S.ad + e);  cp_async8(&rg.v(sl, 1, tid), S.ali + e);
-      cp_async8(&rg.v(sl, 2, tid), S.alj + e); cp_async8(&rg.v(sl, 3, tid), S.alk + e);
-      cp_async8(&rg.v(sl, 4, tid), S.aui + e); cp_async8(&rg.v(sl, 5, tid), S.auj + e);
-      cp_async8(&rg.v(sl, 6, tid), S.auk + e); cp_async4(&rg.ind(sl, tid), S.indc + e);
+#pragma unroll
+      for (int c = 0; c < 7; ++c) cp_async8(&rg.v(sl, c, tid), sy + (long long)c * T);
+      cp_async4(&rg.ind(sl, tid), S.indc + e);
     }
     cp_commit();
   };
@@ -303,8 +305,8 @@ __global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
           a1 = 0.0 + U * (0.0 + 0.0);
         }
         if (t.tj > 0) {
-          d2 = rg.xb[prv * T + tid - TI];
-          a2 = rg.v(slp, 5, tid - TI) + U * (rg.v(slp, 4, tid - TI) + rg.v(slp, 6, tid - TI));
+          d2 = rg.xb[prv * T + tid - TIp];
+          a2 = rg.v(slp, 5, tid - TIp) + U * (rg.v(slp, 4, tid - TIp) + rg.v(slp, 6, tid - TIp));
         } else {
           a2 = 0.0 + U * (0.0 + 0.0);
         }
@@ -312,7 +314,7 @@ __global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
                     rg.v(sl, 3, tid) * dk1 * au3);
         if (dd <= 0.0) bad = true;
       }
-      S.dd[sl_index(q, b, s, tid)] = dd;
+      S.sys[sys_at((long long)b * q.W + s, SYS_DD, T, tid)] = dd;
       rg.xb[cur * T + tid] = dd;
       dk1 = dd;
       au3 = rg.v(sl, 6, tid) + U * (rg.v(sl, 4, tid) + rg.v(sl, 5, tid));
@@ -322,142 +324,249 @@ __global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
   if (bad) atomicOr(pivot_bad, 1);
 }
 
-// ------------------------------------------------------- VF_MZFRWD (+MZAX)
-// FUSED: the input is Y = A*P computed on the fly (VF_MZAX then VF_MZFRWD).
-// Ring values, fused:  0 AD, 1 ALI, 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK, 7 DD
-//                      (skewed), 8 P, 9 P(i-1), 10 P(i+1), 11 P(j-1),
-//                      12 P(j+1) (P in the standard layout; 9..12 only on
-//                      tile-edge threads)
-// Ring values, plain:  0 Y (standard layout), 1 ALI, 2 ALJ, 3 ALK, 4 DD
-// The result is written in the skewed layout for k_bwd.
-template <int D, bool FUSED>
-__global__ void k_fwd(Geo g, SkewGeo q, SkewSys S, const double *y, const double *P, double *Tout,
-                      const SolveState *st) {
-  if (st && st->done) return;
-  constexpr int NV = FUSED ? 13 : 5, R = D + 3;
-  constexpr int QDD = FUSED ? 7 : 4;
-  const int TI = q.TI, T = q.T;
-  Ring<NV> rg = ring_setup<NV>(T, R);
-  TileGeo t = tile_geo(g, TI, q.TJ);
-  const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
-  const int bx = blockIdx.x, by = blockIdx.y;
-  const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
-  const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
-  auto prefetch = [&](int s) {
-    const int k = 2 + s - t.ti - t.tj;
-    if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long e = sl_index(q, b, s, tid);
-      const int sl = s % R;
-      if (FUSED) {
-        cp_async8(&rg.v(sl, 0, tid), S.ad + e);  cp_async8(&rg.v(sl, 1, tid), S.ali + e);
-        cp_async8(&rg.v(sl, 2, tid), S.alj + e); cp_async8(&rg.v(sl, 3, tid), S.alk + e);
-        cp_async8(&rg.v(sl, 4, tid), S.aui + e); cp_async8(&rg.v(sl, 5, tid), S.auj + e);
-        cp_async8(&rg.v(sl, 6, tid), S.auk + e); cp_async8(&rg.v(sl, 7, tid), S.dd + e);
-        cp_async8(&rg.v(sl, 8, tid), P + e);
-        // values of the neighbouring tiles (or the zero ghost layer)
-        if (ex0) skew_fetch(&rg.v(sl, 9, tid), g, q, P, bx, by, t.ti - 1, t.tj, k);
-        if (ex1) skew_fetch(&rg.v(sl, 10, tid), g, q, P, bx, by, t.ti + 1, t.tj, k);
-        if (ey0) skew_fetch(&rg.v(sl, 11, tid), g, q, P, bx, by, t.ti, t.tj - 1, k);
-        if (ey1) skew_fetch(&rg.v(sl, 12, tid), g, q, P, bx, by, t.ti, t.tj + 1, k);
-      } else {
-        cp_async8(&rg.v(sl, 0, tid), y + e);      cp_async8(&rg.v(sl, 1, tid), S.ali + e);
-        cp_async8(&rg.v(sl, 2, tid), S.alj + e);  cp_async8(&rg.v(sl, 3, tid), S.alk + e);
-        cp_async8(&rg.v(sl, 4, tid), S.dd + e);
-      }
-      cp_async4(&rg.ind(sl, tid), S.indc + e);
-    }
-    cp_commit();
-  };
-#pragma unroll 1
-  for (int s = 0; s < D; ++s) prefetch(s);
-  double xk1 = 0.0, dk1 = 0.0;  // X and DD at (i,j,k-1); k-1 = 1 is the zero ghost layer
-  for (int s = 0; s < nsteps; ++s) {
-    prefetch(s + D);
-    cp_wait<D - 1>();
-    __syncthreads();
-    const int k = 2 + s - t.ti - t.tj;
-    const int sl = s % R, slp = (s + R - 1) % R, sln = (s + 1) % R, cur = s & 1, prv = cur ^ 1;
-    if (t.valid && k >= 2 && k <= g.NK - 1) {
-      double x = 0.0;
-      const double d = rg.v(sl, QDD, tid);
-      if (rg.ind(sl, tid) != -1) {
-        double yv;
-        if (FUSED) {
-          const double pc = rg.v(sl, 8, tid);
-          const double pxm = ex0 ? rg.v(sl, 9, tid) : rg.v(slp, 8, tid - 1);
-          const double pym = ey0 ? rg.v(sl, 11, tid) : rg.v(slp, 8, tid - TI);
-          const double pzm = (k > 2) ? rg.v(slp, 8, tid) : 0.0;
-          const double pxp = ex1 ? rg.v(sl, 10, tid) : rg.v(sln, 8, tid + 1);
-          const double pyp = ey1 ? rg.v(sl, 12, tid) : rg.v(sln, 8, tid + TI);
-          const double pzp = (k < g.NK - 1) ? rg.v(sln, 8, tid) : 0.0;
-          yv = rg.v(sl, 0, tid) * pc + rg.v(sl, 1, tid) * pxm + rg.v(sl, 2, tid) * pym +
-               rg.v(sl, 3, tid) * pzm + rg.v(sl, 4, tid) * pxp + rg.v(sl, 5, tid) * pyp +
-               rg.v(sl, 6, tid) * pzp;
-        } else {
-          yv = rg.v(sl, 0, tid);
-        }
-        double d1 = 0.0, x1 = 0.0, d2 = 0.0, x2 = 0.0;
-        if (t.ti > 0) { d1 = rg.v(slp, QDD, tid - 1); x1 = rg.xb[prv * T + tid - 1]; }
-        if (t.tj > 0) { d2 = rg.v(slp, QDD, tid - TI); x2 = rg.xb[prv * T + tid - TI]; }
-        x = yv - rg.v(sl, 1, tid) * d1 * x1 - rg.v(sl, 2, tid) * d2 * x2 - rg.v(sl, 3, tid) * dk1 * xk1;
-      }
-      Tout[sl_index(q, b, s, tid)] = x;
-      rg.xb[cur * T + tid] = x;
-      xk1 = x;
-      dk1 = d;
-    }
+// ------------------------------------------------ bulk-copy slab pipeline
+// The sweeps read, at every wavefront step, one contiguous slab of T
+// values from each of 5 or 9 skewed arrays.  A producer warp moves those
+// slabs into a ring of R = D+2 shared-memory slots with cp.async.bulk, D
+// steps ahead, each slot completing on its own mbarrier (transaction
+// count); the T consumer threads wait on the mbarrier of the step they
+// need and then work purely from shared memory.  One block barrier per
+// step orders the exchange of the sweep values between neighbouring
+// columns and frees the slot of step s-2 for the producer.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Wait for the phase `parity` of an mbarrier, giving up after limit_ns.
+__device__ __noinline__ bool mbar_wait_slow(unsigned bar, unsigned parity, unsigned long long limit_ns) {
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    for (int i = 0; i < 64; ++i)
+      if (mbar_try(bar, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
   }
-  cp_wait<0>();
+}
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, 2000000000ull);
 }
 
-// ------------------------------------------------------------ VF_MZBKWD
-// ring values: 0 T, 1 AUI, 2 AUJ, 3 AUK, 4 DD (all skewed); reversed loop
-// order; X written in the standard layout.
-template <int D>
-__global__ void k_bwd(Geo g, SkewGeo q, SkewSys S, const double *Tin, double *X, const SolveState *st) {
-  if (st && st->done) return;
-  constexpr int NV = 5, R = D + 3;
-  const int TI = q.TI, T = q.T;
-  Ring<NV> rg = ring_setup<NV>(T, R);
-  TileGeo t = tile_geo(g, TI, q.TJ);
-  const int I = t.is + t.ti, J = t.js + t.tj, tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
-  const int ri = t.wi - 1 - t.ti, rj = t.wj - 1 - t.tj;  // distance from the far corner
+// ------------------------------------ VF_MZFRWD (+VF_MZAX) and VF_MZBKWD
+// One block per tile: T consumer threads (thread t = ti + TIp*tj owns
+// column (ti,tj)) and one producer warp.  MODE (SweepMode):
+//   SWEEP_FWD     T = MINV_L * Y, Y given (skewed);  vf_mzfrwd.f
+//   SWEEP_FWD_AX  T = MINV_L * (A*P), A*P formed on the fly (VF_MZAX
+//                 then VF_MZFRWD: vf_mzax.f:46-53, vf_mzfrwd.f)
+//   SWEEP_BWD     X = MINV_U * T;  vf_mzbkwd.f
+// Results are written in the skewed layout.  Forward step s visits
+// k = 2+s-ti-tj, backward step s visits k = NK-1-(s-ri-rj) (ri, rj the
+// distances from the far corner), so step s of every thread is one slab.
+// A cell is computed where DD != 0: MZDCMP gives DD = 0 exactly on
+// INDC = -1 and a positive (or NaN) DD elsewhere, and a zero or negative
+// pivot ends the solve before any sweep runs.
+//
+// Only the recurrence sits between two block barriers: the neighbours'
+// results of step s-1 are read, combined in five dependent operations and
+// published.  Everything that does not depend on step s-1 -- the ring
+// loads, the 7-term product A*P and the products ALI*DD(i-1) etc. of the
+// recurrence -- is prepared for step s+1 after the result of step s is
+// published, while the other warps reach the barrier.  The expressions
+// and their evaluation order are those of the reference loops, so the
+// results do not change.  The step loop is unrolled by the ring length so
+// slot addresses and mbarrier phases are constants.
+template <int D, int MODE, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+    k_sweep(Geo g, SkewGeo q, SkewSys S, const double *vin, double *vout, SolveState *st) {
+  if (st->done) return;
+  constexpr int R = D + 2;
+  constexpr int AHEAD = (MODE == SWEEP_FWD_AX) ? 2 : 1;  // preparing step s+1 reads the slot of step s+AHEAD
+  extern __shared__ __align__(16) double sm[];
+  const int T = q.T, TIp = q.TIp;
+  const int Tc = (T + 31) & ~31;
+  const int SS = sweep_slot(q, MODE);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm);
+  double *ring = sm + ((R + 1) & ~1);
+  double *xb = ring + (size_t)R * SS;
+  const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
+  TileGeo t = tile_geo(g, q);
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
-  auto prefetch = [&](int s) {
-    const int k = (g.NK - 1) - (s - ri - rj);
-    if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long e = sl_index(q, b, (k - 2) + t.ti + t.tj, tid);
-      const int sl = s % R;
-      cp_async8(&rg.v(sl, 0, tid), Tin + e);      cp_async8(&rg.v(sl, 1, tid), S.aui + e);
-      cp_async8(&rg.v(sl, 2, tid), S.auj + e);    cp_async8(&rg.v(sl, 3, tid), S.auk + e);
-      cp_async8(&rg.v(sl, 4, tid), S.dd + e);     cp_async4(&rg.ind(sl, tid), S.indc + e);
-    }
-    cp_commit();
+  const bool producer = tid >= Tc;
+  const int lane = tid & 31;
+
+  if (tid == 0)
+    for (int r = 0; r < R; ++r) mbar_init(smem_u32(bar + r), 1);
+  if (MODE == SWEEP_FWD_AX) {  // halo values of absent neighbours stay 0 (ghost layer)
+    const int nh = 2 * halo_span(q) + 2 * TIp;
+    for (int r = 0; r < R; ++r)
+      for (int i = tid; i < nh; i += blockDim.x) ring[(size_t)r * SS + halo_left(q) + i] = 0.0;
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  __syncthreads();
+
+  // Producer: lane l issues copy l of every step (at most 6); its fixed
+  // part is worked out once here.
+  const double *src0 = nullptr;
+  SweepLane l0;
+  l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; l0.dst = 0; l0.wstride = 0;  // empty range: no copy
+  if (producer && lane < sweep_ncopy(q, MODE) && sweep_lane(q, MODE, b, lane, l0))
+    src0 = (l0.arr == 0 ? S.sys : vin) + l0.base;
+  else { l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; }
+  const unsigned bar0 = smem_u32(bar), ring0 = smem_u32(ring);
+  auto issue = [&](int u, int slot) {
+    if (u >= nsteps) return;
+    const int w = (MODE == SWEEP_BWD) ? nsteps - 1 - u : u;
+    const unsigned bslot = bar0 + 8u * slot;
+    const unsigned dslot = ring0 + 8u * (unsigned)(slot * SS);
+    const bool v0 = (w >= l0.dlo && w <= l0.dhi);
+    const unsigned bytes = __reduce_add_sync(0xffffffffu, v0 ? l0.bytes : 0);
+    if (lane == 0) mbar_expect_tx(bslot, bytes);
+    __syncwarp();
+    if (v0) bulk_load(dslot + 8u * l0.dst, src0 + (long long)w * l0.wstride, l0.bytes, bslot);
   };
+  // data of step u sits in slot u % R, phase (u / R) & 1
+  auto wait_data = [&](int u, int slot, unsigned parity) -> bool {
+    return u >= nsteps || mbar_wait(bar0 + 8u * slot, parity);
+  };
+
+  if (producer) {
 #pragma unroll 1
-  for (int s = 0; s < D; ++s) prefetch(s);
-  double xk1 = 0.0;  // X(i,j,k+1); k+1 = NK is the zero ghost layer
-  for (int s = 0; s < nsteps; ++s) {
-    prefetch(s + D);
-    cp_wait<D - 1>();
-    __syncthreads();
-    const int k = (g.NK - 1) - (s - ri - rj);
-    const int sl = s % R, cur = s & 1, prv = cur ^ 1;
-    if (t.valid && k >= 2 && k <= g.NK - 1) {
-      double x = 0.0;
-      if (rg.ind(sl, tid) != -1) {
-        const double x1 = (ri > 0) ? rg.xb[prv * T + tid + 1] : 0.0;
-        const double x2 = (rj > 0) ? rg.xb[prv * T + tid + TI] : 0.0;
-        x = (rg.v(sl, 0, tid) - rg.v(sl, 1, tid) * x1 - rg.v(sl, 2, tid) * x2 - rg.v(sl, 3, tid) * xk1) *
-            rg.v(sl, 4, tid);
+    for (int u = 0; u < D; ++u) issue(u, u % R);
+  }
+
+  // Column geometry: active steps slo..shi (k inside 2..NK-1).
+  const int ri = t.wi - 1 - t.ti, rj = t.wj - 1 - t.tj;
+  const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
+  const int slo = (MODE == SWEEP_BWD) ? ri + rj : t.ti + t.tj, shi = slo + g.NK - 3;
+  const bool col = t.valid && !producer;
+  const int lofs = (q.TI - 1) & 1;  // left halo: position of column TI-1 in its pair
+  const int hl = halo_left(q) + TIp * t.tj + lofs, hr = halo_right(q) + TIp * t.tj, hd = halo_down(q) + t.ti,
+            hu = halo_up(q) + t.ti;
+  double *vp = vout + ((long long)b * q.W + (MODE == SWEEP_BWD ? nsteps - 1 : 0)) * T + tid;
+  const long long vstep = (MODE == SWEEP_BWD) ? -(long long)T : (long long)T;
+
+  // Prepared values of the next step.
+  bool act = false;             // the column has a cell at this step
+  double dd = 0.0;              // DD of the cell (0: not computed)
+  double y0 = 0.0;              // FWD: Y or A*P;  BWD: T
+  double c1 = 0.0, c2 = 0.0, c3 = 0.0;  // FWD: ALI*DD(i-1), ALJ*DD(j-1), ALK*DD(k-1); BWD: AUI, AUJ, AUK
+  double dk1 = 0.0, pk1 = 0.0;  // DD and P of this column at the previous step (FWD)
+  double xk1 = 0.0;             // result of this column at the previous step
+  // Prepare step s: cs = slot of s, ps = slot of s-1, ns = slot of s+1.
+  auto prepare = [&](int s, const double *cs, const double *ps, const double *ns) {
+    act = col && s >= slo && s <= shi;
+    if (!act) return;
+    if (MODE == SWEEP_FWD_AX) {
+      const int k = 2 + s - t.ti - t.tj;
+      const double d = cs[7 * T + tid], pc = cs[8 * T + tid];
+      if (d != 0.0) {
+        const double pxm = ex0 ? cs[hl] : ps[8 * T + tid - 1];
+        const double pym = ey0 ? cs[hd] : ps[8 * T + tid - TIp];
+        const double pzm = (k > 2) ? pk1 : 0.0;
+        const double pxp = ex1 ? cs[hr] : ns[8 * T + tid + 1];
+        const double pyp = ey1 ? cs[hu] : ns[8 * T + tid + TIp];
+        const double pzp = (k < g.NK - 1) ? ns[8 * T + tid] : 0.0;
+        y0 = cs[tid] * pc + cs[T + tid] * pxm + cs[2 * T + tid] * pym + cs[3 * T + tid] * pzm +
+             cs[4 * T + tid] * pxp + cs[5 * T + tid] * pyp + cs[6 * T + tid] * pzp;
+        const double d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : 0.0;
+        const double d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : 0.0;
+        c1 = cs[T + tid] * d1;
+        c2 = cs[2 * T + tid] * d2;
+        c3 = cs[3 * T + tid] * dk1;
       }
-      X[sl_index(q, b, (k - 2) + t.ti + t.tj, tid)] = x;
-      rg.xb[cur * T + tid] = x;
-      xk1 = x;
+      dd = d; dk1 = d; pk1 = pc;
+    } else if (MODE == SWEEP_FWD) {
+      const double d = cs[7 * T + tid];
+      if (d != 0.0) {
+        const double d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : 0.0;
+        const double d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : 0.0;
+        y0 = cs[tid];
+        c1 = cs[T + tid] * d1;
+        c2 = cs[2 * T + tid] * d2;
+        c3 = cs[3 * T + tid] * dk1;
+      }
+      dd = d; dk1 = d;
+    } else {
+      dd = cs[4 * T + tid];
+      if (dd != 0.0) { y0 = cs[tid]; c1 = cs[T + tid]; c2 = cs[2 * T + tid]; c3 = cs[3 * T + tid]; }
+    }
+  };
+  auto slot_ptr = [&](int r) -> const double * { return ring + (size_t)r * SS; };
+
+  bool ok = true;
+  if (!producer) {
+    for (int u = 0; u < AHEAD; ++u) if (ok) ok = wait_data(u, u % R, (unsigned)((u / R) & 1));
+    if (ok) prepare(0, slot_ptr(0), slot_ptr(R - 1), slot_ptr(1 % R));
+  }
+  bool aborted = false;
+  int issued = min(D, nsteps) - 1;  // last step whose copies were issued (producer)
+  unsigned ph = 0;                  // (s0 / R) & 1
+#pragma unroll 1
+  for (int s0 = 0; s0 < nsteps && !aborted; s0 += R, ph ^= 1u) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int s = s0 + r;
+      if (s >= nsteps) break;
+      if (producer) {
+        issue(s + D, (r + D) % R);
+        if (s + D < nsteps) issued = s + D;
+      } else {
+        // the recurrence of step s
+        if (act) {
+          const int cur = (s & 1) * T, prv = T - cur;
+          double x = 0.0;
+          if (dd != 0.0) {
+            if (MODE == SWEEP_BWD) {
+              const double x1 = (ri > 0) ? xb[prv + tid + 1] : 0.0;
+              const double x2 = (rj > 0) ? xb[prv + tid + TIp] : 0.0;
+              x = (y0 - c1 * x1 - c2 * x2 - c3 * xk1) * dd;
+            } else {
+              const double x1 = (t.ti > 0) ? xb[prv + tid - 1] : 0.0;
+              const double x2 = (t.tj > 0) ? xb[prv + tid - TIp] : 0.0;
+              x = y0 - c1 * x1 - c2 * x2 - c3 * xk1;
+            }
+          }
+          xb[cur + tid] = x;
+          *vp = x;
+          xk1 = x;
+        }
+        vp += vstep;
+        // prepare step s+1
+        const int u = s + 1 + AHEAD - 1;  // newest data that preparing s+1 reads
+        if (ok) ok = wait_data(u, (r + AHEAD) % R, ph ^ (unsigned)((r + AHEAD) / R));
+        if (ok && s + 1 < nsteps) prepare(s + 1, slot_ptr((r + 1) % R), slot_ptr(r), slot_ptr((r + 2) % R));
+      }
+      if (__syncthreads_or(!ok)) { aborted = true; break; }
     }
   }
-  cp_wait<0>();
-  (void)I; (void)J;
+  if (aborted && producer) {
+    // Let the copies already issued land (bounded) before the block exits.
+    if (lane == 0)
+      for (int u = max(0, issued - R + 1); u <= issued; ++u)
+        mbar_wait_slow(bar0 + 8u * (u % R), (unsigned)((u / R) & 1), 100000000ull);
+    if (lane == 0) { st->timeout = 1; st->done = 1; }
+  }
 }
 
 // ------------------------------------------------------------ slab kernels
@@ -487,11 +596,15 @@ __device__ __forceinline__ double skew_ax(const Geo &g, const SkewGeo &q, const 
   const int t = (int)(e % q.T);
   const long long bw = e / q.T;
   const int w = (int)(bw % q.W), b = (int)(bw / q.W);
-  const int ti = t % q.TI, tj = t / q.TI, bx = b % q.ntx, by = b / q.ntx, k = 2 + w - ti - tj;
-  return S.ad[e] * X[e] + S.ali[e] * skew_at(g, q, X, bx, by, ti - 1, tj, k) +
-         S.alj[e] * skew_at(g, q, X, bx, by, ti, tj - 1, k) + S.alk[e] * skew_at(g, q, X, bx, by, ti, tj, k - 1) +
-         S.aui[e] * skew_at(g, q, X, bx, by, ti + 1, tj, k) + S.auj[e] * skew_at(g, q, X, bx, by, ti, tj + 1, k) +
-         S.auk[e] * skew_at(g, q, X, bx, by, ti, tj, k + 1);
+  const int ti = t % q.TIp, tj = t / q.TIp, bx = b % q.ntx, by = b / q.ntx, k = 2 + w - ti - tj;
+  const double *a = S.sys + sys_at(bw, 0, q.T, t);
+  const long long T = q.T;
+  return a[SYS_AD * T] * X[e] + a[SYS_ALI * T] * skew_at(g, q, X, bx, by, ti - 1, tj, k) +
+         a[SYS_ALJ * T] * skew_at(g, q, X, bx, by, ti, tj - 1, k) +
+         a[SYS_ALK * T] * skew_at(g, q, X, bx, by, ti, tj, k - 1) +
+         a[SYS_AUI * T] * skew_at(g, q, X, bx, by, ti + 1, tj, k) +
+         a[SYS_AUJ * T] * skew_at(g, q, X, bx, by, ti, tj + 1, k) +
+         a[SYS_AUK * T] * skew_at(g, q, X, bx, by, ti, tj, k + 1);
 }
 
 // Y = A X on INDC != -1 (VF_MZAX); Y untouched elsewhere.
@@ -581,7 +694,7 @@ __global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double
   if (st->iter < 0) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) {
-    const int ti = t_ % q.TI, tj = t_ / q.TI;
+    const int ti = t_ % q.TIp, tj = t_ / q.TIp;
     const int w = (int)(slab_ % q.W), b = (int)(slab_ / q.W);
     const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
     X0[cid(g, I, J, k)] = XW[e];
@@ -760,29 +873,57 @@ void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const
   RING_LAUNCH2(k_dcmp, 7, g, q, U, S, pivot_bad);
 #undef RING_EXTRA
 }
+// Sweeps: prefetch depth D in {8, 4, 2}, the largest whose ring (R = D+2
+// slots, mbarriers, exchange buffers) fits 200 KB.
+static size_t sweep_bytes(const SkewGeo &q, int mode, int D) {
+  const int R = D + 2;
+  return (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode) * 8 + 2 * (size_t)q.T * 8;
+}
+static int sweep_depth(const SkewGeo &q, int mode) {
+  if (sweep_threads(q.T) > 1024) return 0;
+  for (int d : {8, 4, 2})
+    if (sweep_bytes(q, mode, d) <= 200 * 1024) return d;
+  return 0;
+}
+template <int MODE>
+static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *vin,
+                         double *vout, SolveState *st) {
+  const int d = sweep_depth(q, MODE);
+  const size_t bytes = sweep_bytes(q, MODE, d);
+  const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
+  // Blocks of up to 256 threads get the registers to keep a prepared step
+  // in flight; larger tiles run the same code within 64 registers.
+  const bool small = sweep_threads(q.T) <= 256;
+  switch (d * 2 + (small ? 1 : 0)) {
+#define SWEEP_CASE(DD, MT)                                                              \
+  case DD * 2 + (MT == 256 ? 1 : 0):                                                    \
+    set_smem(k_sweep<DD, MODE, MT>, bytes);                                             \
+    k_sweep<DD, MODE, MT><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);           \
+    break;
+    SWEEP_CASE(8, 256) SWEEP_CASE(4, 256) SWEEP_CASE(2, 256)
+    SWEEP_CASE(8, 1024) SWEEP_CASE(4, 1024) SWEEP_CASE(2, 1024)
+#undef SWEEP_CASE
+    default: return;  // rejected by cadmas_create (sweep_supported)
+  }
+  count_launch();
+}
+bool sweep_supported(const SkewGeo &q) {
+  return sweep_depth(q, SWEEP_FWD) > 0 && sweep_depth(q, SWEEP_BWD) > 0;
+}
 void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
-                const double *spmv_x, double *tout, const SolveState *st, double *ybuf) {
-  if (spmv_x && ring_depth(13, q.T) == 0) {
-    // Ring of the fused kernel too large for this tile: SpMV first.
+                const double *spmv_x, double *tout, SolveState *st, double *ybuf) {
+  if (spmv_x && sweep_depth(q, SWEEP_FWD_AX) == 0) {
+    // Ring of the fused sweep too large for this tile: SpMV first.
     launch_spmv(s, g, q, S, spmv_x, ybuf, st);
     y = ybuf;
     spmv_x = nullptr;
   }
-  if (spmv_x) {
-#define RING_EXTRA , true
-    RING_LAUNCH2(k_fwd, 13, g, q, S, y, spmv_x, tout, st);
-#undef RING_EXTRA
-  } else {
-#define RING_EXTRA , false
-    RING_LAUNCH2(k_fwd, 5, g, q, S, y, spmv_x, tout, st);
-#undef RING_EXTRA
-  }
+  if (spmv_x) launch_sweep<SWEEP_FWD_AX>(s, g, q, S, spmv_x, tout, st);
+  else launch_sweep<SWEEP_FWD>(s, g, q, S, y, tout, st);
 }
 void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
-                double *x, const SolveState *st) {
-#define RING_EXTRA
-  RING_LAUNCH2(k_bwd, 5, g, q, S, tin, x, st);
-#undef RING_EXTRA
+                double *x, SolveState *st) {
+  launch_sweep<SWEEP_BWD>(s, g, q, S, tin, x, st);
 }
 static inline unsigned slab_blocks(const SkewGeo &q) {
   return (unsigned)(((long long)q.nb * q.W + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK);

@@ -16,16 +16,134 @@ struct SysPtr {
 };
 
 // The constant part of a solve in the tile-skewed layout of the MILU
-// kernels (k_poisson.cu): 7 coefficients, DD and INDC.
+// kernels (k_poisson.cu).  The 7 coefficients and DD are interleaved slab
+// by slab, sys[(slab*SYS_N + c)*T + t], so the values one wavefront step
+// needs are one contiguous block; INDC is a plain skewed array.
+enum SysArray { SYS_AD = 0, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK, SYS_DD, SYS_N };
 struct SkewSys {
-  double *ad, *ali, *alj, *alk, *aui, *auj, *auk, *dd;
+  double *sys;
   int *indc;
 };
-// Tile geometry of the skewed layout: TI x TJ columns per tile (T threads),
-// W wavefront slabs per tile, ntx tiles along x, nb tiles in all.
+// Tile geometry of the skewed layout: TI x TJ columns per tile, W
+// wavefront slabs per tile, ntx tiles along x, nb tiles in all.  Slab
+// entry t = ti + TIp*tj with the row stride TIp = TI rounded up to even
+// (T = TIp*TJ entries per slab), so every slab, slab row and pair of
+// columns starts on a 16-byte boundary and moves with one bulk copy.
 struct SkewGeo {
-  int TI, TJ, T, W, ntx, nb;
+  int TI, TJ, TIp, T, W, ntx, nb;
 };
+
+__host__ __device__ inline long long sys_at(long long slab, int c, int T, int t) {
+  return (slab * SYS_N + c) * T + t;
+}
+
+// Bulk copies of one wavefront step of the MILU sweeps (k_sweep).  A ring
+// slot holds NV slabs of T values (slab c at c*T):
+// MODE 0: forward sweep of a given vector: {Y, ALI, ALJ, ALK, AUI, AUJ,
+//         AUK, DD} (AUI..AUK unused), copies: Y, system slabs 1..7;
+// MODE 1: forward sweep fused with Y = A*P: {AD, ALI, ALJ, ALK, AUI, AUJ,
+//         AUK, DD, P} plus the P values of the four neighbouring tiles at
+//         the step's cells (down/up: one row of TIp; left/right: the span
+//         of the neighbour's slab from its last/first column of row 0 to
+//         that of row TJ-1), copies: system slabs 0..7, P, down, up, left,
+//         right;
+// MODE 2: backward sweep: {T, AUI, AUJ, AUK, DD}, copies: T, system
+//         slabs 4..7.
+// Offsets are in doubles; `arr` 0 is the interleaved system, 1 the vector.
+enum SweepMode { SWEEP_FWD = 0, SWEEP_FWD_AX = 1, SWEEP_BWD = 2 };
+struct SweepCopy {
+  long long src;
+  int dst, bytes, arr;
+};
+__host__ __device__ inline int sweep_nv(int mode) {
+  return mode == SWEEP_FWD_AX ? 9 : (mode == SWEEP_FWD ? 8 : 5);
+}
+__host__ __device__ inline int sweep_ncopy(const SkewGeo &, int mode) { return mode == SWEEP_FWD_AX ? 6 : 2; }
+// Doubles of a left/right halo span: TIp*(TJ-1)+2 (even).
+__host__ __device__ inline int halo_span(const SkewGeo &q) { return q.TIp * (q.TJ - 1) + 2; }
+// doubles per ring slot (even, so slots stay 16-byte aligned)
+__host__ __device__ inline int sweep_slot(const SkewGeo &q, int mode) {
+  return sweep_nv(mode) * q.T + (mode == SWEEP_FWD_AX ? 2 * halo_span(q) + 2 * q.TIp : 0);
+}
+// Offsets of the halo values inside a slot (MODE 1): the value of row tj
+// is at halo_left + TIp*tj + ((TI-1)&1), halo_right + TIp*tj,
+// halo_down + ti and halo_up + ti.
+__host__ __device__ inline int halo_left(const SkewGeo &q) { return 9 * q.T; }
+__host__ __device__ inline int halo_right(const SkewGeo &q) { return 9 * q.T + halo_span(q); }
+__host__ __device__ inline int halo_down(const SkewGeo &q) { return 9 * q.T + 2 * halo_span(q); }
+__host__ __device__ inline int halo_up(const SkewGeo &q) { return 9 * q.T + 2 * halo_span(q) + q.TIp; }
+// Copy c of tile b, the part that does not change from step to step: the
+// slab of step u is w = u (forward) or nsteps-1-u (backward), and the copy
+// reads array `arr` at offset base + w*wstride when dlo <= w <= dhi (false
+// when the copy does not exist: no neighbouring tile).  The range excludes
+// the steps where the neighbour's slab lies outside 0..W-1; no cell of
+// such a step uses the value (its edge cells are above or below the
+// interior).
+struct SweepLane {
+  long long base;
+  int wstride, dst, bytes, arr, dlo, dhi;
+};
+__host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, int c, SweepLane &l) {
+  const long long slab0 = (long long)b * q.W;
+  l.dlo = 0; l.dhi = q.W - 1;
+  const int sys_c = (mode == SWEEP_FWD_AX) ? 0 : 1;  // copy index of the system block
+  const int vec_c = 1 - sys_c;
+  if (c == sys_c) {
+    const int first = (mode == SWEEP_FWD_AX) ? SYS_AD : (mode == SWEEP_FWD ? SYS_ALI : SYS_AUI);
+    l.base = sys_at(slab0, first, q.T, 0);
+    l.wstride = SYS_N * q.T;
+    l.dst = (mode == SWEEP_FWD_AX) ? 0 : q.T;
+    l.bytes = (SYS_N - first) * q.T * 8;
+    l.arr = 0;
+    return true;
+  }
+  l.wstride = q.T;
+  l.arr = 1;
+  if (c == vec_c) {
+    l.base = slab0 * q.T;
+    l.dst = (mode == SWEEP_FWD_AX) ? 8 * q.T : 0;
+    l.bytes = q.T * 8;
+    return true;
+  }
+  if (mode != SWEEP_FWD_AX) return false;
+  const int bx = b % q.ntx, by = b / q.ntx, nty = q.nb / q.ntx;
+  int nb_tile, dw, toff;
+  if (c == 2) {  // down: row tj = TJ-1 of tile b-ntx
+    if (by == 0) return false;
+    nb_tile = b - q.ntx; dw = q.TJ - 1; toff = q.TIp * (q.TJ - 1);
+    l.dst = halo_down(q); l.bytes = q.TIp * 8;
+  } else if (c == 3) {  // up: row tj = 0 of tile b+ntx
+    if (by == nty - 1) return false;
+    nb_tile = b + q.ntx; dw = -(q.TJ - 1); toff = 0;
+    l.dst = halo_up(q); l.bytes = q.TIp * 8;
+  } else if (c == 4) {  // left: tile b-1 from column (TI-1)&~1 of row 0 to column TI-1 of row TJ-1
+    if (bx == 0) return false;
+    nb_tile = b - 1; dw = q.TI - 1; toff = (q.TI - 1) & ~1;
+    l.dst = halo_left(q); l.bytes = halo_span(q) * 8;
+  } else if (c == 5) {  // right: tile b+1 from column 0 of row 0 to column 1 of row TJ-1
+    if (bx == q.ntx - 1) return false;
+    nb_tile = b + 1; dw = -(q.TI - 1); toff = 0;
+    l.dst = halo_right(q); l.bytes = halo_span(q) * 8;
+  } else {
+    return false;
+  }
+  l.base = ((long long)nb_tile * q.W + dw) * q.T + toff;
+  l.dlo = dw < 0 ? -dw : 0;                 // 0 <= w + dw
+  l.dhi = dw > 0 ? q.W - 1 - dw : q.W - 1;  // w + dw <= W-1
+  return true;
+}
+// Copy c for wavefront step u of tile b (nsteps steps); false when it is
+// not issued.
+__host__ __device__ inline bool sweep_copy(const SkewGeo &q, int mode, int b, int nsteps, int u, int c,
+                                           SweepCopy &cp) {
+  SweepLane l;
+  if (!sweep_lane(q, mode, b, c, l)) return false;
+  const int w = (mode == SWEEP_BWD) ? nsteps - 1 - u : u;
+  if (w < l.dlo || w > l.dhi) return false;
+  cp.src = l.base + (long long)w * l.wstride;
+  cp.dst = l.dst; cp.bytes = l.bytes; cp.arr = l.arr;
+  return true;
+}
 
 enum FinMode { FIN_BNORM = 0, FIN_START = 1, FIN_STORE = 2, FIN_RELRES = 3,
                FIN_ALPHA = 10, FIN_OMEGA = 11, FIN_CONV = 12 };
@@ -42,9 +160,14 @@ void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr
                     const SkewSys &S, const double *x0, double *bsl, double *xsl);
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad);
 void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
-                const double *spmv_x, double *tout, const SolveState *st, double *ybuf);
+                const double *spmv_x, double *tout, SolveState *st, double *ybuf);
 void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
-                double *x, const SolveState *st);
+                double *x, SolveState *st);
+// Thread block of the sweeps for a tile of T slab entries (T consumer
+// threads rounded up to whole warps, plus the producer warp).
+inline int sweep_threads(int T) { return ((T + 31) & ~31) + 32; }
+// Whether the sweeps can run this tile geometry (block size, shared memory).
+bool sweep_supported(const SkewGeo &q);
 void launch_spmv(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *x, double *y,
                  const SolveState *st);
 void launch_bmy(cudaStream_t s, const SkewGeo &q, const int *indc, const double *b, double *y,

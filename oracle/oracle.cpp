@@ -136,13 +136,15 @@ struct orc_handle {
 
   // The same tree over the slabs of the GPU solver's tile-skewed layout:
   // tile b (x fastest), wavefront slab w = (k-2)+ti+tj, slab entry
-  // t = ti + TI*tj; lane l of a slab sums t = l, l+32, ... in order, warp
-  // tree per slab, then the 1024-thread tree over the slabs.  This is the
-  // order of the dot products of VF_M1BCGS in the GPU library.
+  // t = ti + TIp*tj (TIp = TI rounded up to even; the column ti = TI of an
+  // odd TI is padding); lane l of a slab sums t = l, l+32, ... in order,
+  // warp tree per slab, then the 1024-thread tree over the slabs.  This is
+  // the order of the dot products of VF_M1BCGS in the GPU library.
   template <class F> double gsum_skew(F f) const {
     const int TI = std::min(P.precond_ti > 0 ? P.precond_ti : NI - 2, NI - 2);
     const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2);
-    const int T = TI * TJ, W = (NK - 2) + (TI - 1) + (TJ - 1);
+    const int TIp = TI + (TI & 1);
+    const int T = TIp * TJ, W = (NK - 2) + (TI - 1) + (TJ - 1);
     const int ntx = (NI - 2 + TI - 1) / TI, nb = ntx * ((NJ - 2 + TJ - 1) / TJ);
     const long long NS = (long long)nb * W;
     std::vector<double> R(NS);
@@ -152,9 +154,9 @@ struct orc_handle {
       for (int l = 0; l < 32; ++l) {
         double s = 0.0, c;
         for (int t = l; t < T; t += 32) {
-          const int ti = t % TI, tj = t / TI;
+          const int ti = t % TIp, tj = t / TIp;
           const int I = 2 + bx * TI + ti, J = 2 + by * TJ + tj, k = 2 + w - ti - tj;
-          if (I > NI - 1 || J > NJ - 1 || k < 2 || k > NK - 1) continue;
+          if (ti >= TI || I > NI - 1 || J > NJ - 1 || k < 2 || k > NK - 1) continue;
           if (f(I, J, k, c)) s = s + c;
         }
         lane[l] = s;
