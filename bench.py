@@ -44,8 +44,8 @@ STAGE_BYTES = {
     "predict": 19 * 8 + 4 * 4 + 3 * 8,   # 9 fluxes,u,v,w,p,GGV,GLV,CD0,GG* + NF,IND* -> u,v,w
     "vpcoef": 10 * 8 + 5 * 4 + 8 * 8,    # u,v,w,p,F,GGV,GLV,GG* + NF,INDC,IND* -> 8 arrays
     "dcmp": 7 * 8 + 4 + 8,               # 7 coefficients + INDC -> DD
-    "fwd": 7 * 8 + 8 + 8 + 4 + 8,        # 7 coefficients, P, DD, INDC -> T (SpMV fused)
-    "bwd": 5 * 8 + 4 + 8,                # T, AUI, AUJ, AUK, DD, INDC -> X
+    "fwd": 7 * 8 + 8 + 8 + 8,            # 7 coefficients, DD, P -> T (SpMV fused; DD != 0 marks INDC != -1)
+    "bwd": 5 * 8 + 8,                    # T, AUI, AUJ, AUK, DD -> X
 }
 
 

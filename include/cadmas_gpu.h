@@ -177,6 +177,22 @@ int vf_step_gpu_(cadmas_handle **h, const double *dtnow,
                  int *nf, int *indc, double *bcu, double *bcv, double *bcw,
                  double *bcp, double *bcf, double *tnow, int *nnow);
 
+/* ---- Fortran-callable V1CAL / F1CAL, one call each -----------------------
+   Same arrays as vf_step_gpu_, copied in before and out after the call.
+   TNOW, DTNOW and NNOW are taken as the time loop has already advanced
+   them (vf_a1main.f:1029-1047) and are not changed, as the COMMON block
+   /VF_ATIMER/ is read, not written, by VF_V1CAL and VF_F1CAL.
+     vf_v1cal_gpu_  replaces  CALL VF_V1CAL(...)  (vf_a1main.f:1058-1066)
+     vf_f1cal_gpu_  replaces  CALL VF_F1CAL(...)  (vf_a1main.f:1104-1115) */
+int vf_v1cal_gpu_(cadmas_handle **h, const double *tnow, const double *dtnow, const int *nnow,
+                  double *uu, double *vv, double *ww, double *pp, double *ff,
+                  int *nf, int *indc, double *bcu, double *bcv, double *bcw,
+                  double *bcp, double *bcf);
+int vf_f1cal_gpu_(cadmas_handle **h, const double *tnow, const double *dtnow, const int *nnow,
+                  double *uu, double *vv, double *ww, double *pp, double *ff,
+                  int *nf, int *indc, double *bcu, double *bcv, double *bcw,
+                  double *bcp, double *bcf);
+
 /* ---- Poisson solver alone (VF_M1BCGS, vf_m1bcgs.f:1-5) -----------------
    Device pointers, (NUMI,NUMJ,NUMK) each.  x0 is the initial guess on
    entry and the solution on exit when converged (vf_m1bcgs.f:251-261).

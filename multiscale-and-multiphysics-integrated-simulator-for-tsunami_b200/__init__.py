@@ -66,7 +66,8 @@ class Stats(C.Structure):
 EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_upload_static",
             "cadmas_set_state", "cadmas_get_state", "cadmas_init_state", "cadmas_step",
             "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
-            "cadmas_sync", "vf_step_gpu_", "cadmas_m1bcgs_dev", "cadmas_strerror",
+            "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
+            "cadmas_strerror",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers"]
 
 STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]

@@ -832,6 +832,36 @@ int vf_step_gpu_(cadmas_handle **hp, const double *dtnow, double *uu, double *vv
   return rc ? rc : rc2;
 }
 
+// One of V1CAL/F1CAL through host arrays: state in, call, state out.
+static int fortran_call(cadmas_handle **hp, const double *tnow, const double *dtnow, const int *nnow,
+                        double *uu, double *vv, double *ww, double *pp, double *ff, int *nf, int *indc,
+                        double *bcu, double *bcv, double *bcw, double *bcp, double *bcf,
+                        int (*call)(cadmas_handle *)) {
+  if (!hp || !*hp || !tnow || !dtnow || !nnow) return CADMAS_EINVAL;
+  if (!(*dtnow > 0.0)) return CADMAS_EINVAL;
+  cadmas_handle *h = *hp;
+  cadmas_state s{uu, vv, ww, pp, ff, nf, indc, bcu, bcv, bcw, bcp, bcf, nullptr, *tnow, *nnow};
+  int rc = cadmas_set_state(h, &s);
+  if (rc) return rc;
+  rc = cadmas_set_time(h, *tnow, *dtnow, *nnow);
+  if (rc) return rc;
+  rc = call(h);
+  const int rc2 = cadmas_get_state(h, &s);
+  return rc ? rc : rc2;
+}
+
+int vf_v1cal_gpu_(cadmas_handle **h, const double *tnow, const double *dtnow, const int *nnow, double *uu,
+                  double *vv, double *ww, double *pp, double *ff, int *nf, int *indc, double *bcu, double *bcv,
+                  double *bcw, double *bcp, double *bcf) {
+  return fortran_call(h, tnow, dtnow, nnow, uu, vv, ww, pp, ff, nf, indc, bcu, bcv, bcw, bcp, bcf, cadmas_v1cal);
+}
+
+int vf_f1cal_gpu_(cadmas_handle **h, const double *tnow, const double *dtnow, const int *nnow, double *uu,
+                  double *vv, double *ww, double *pp, double *ff, int *nf, int *indc, double *bcu, double *bcv,
+                  double *bcw, double *bcp, double *bcf) {
+  return fortran_call(h, tnow, dtnow, nnow, uu, vv, ww, pp, ff, nf, indc, bcu, bcv, bcw, bcp, bcf, cadmas_f1cal);
+}
+
 int cadmas_m1bcgs_dev(cadmas_handle *h, const double *ad, const double *ali, const double *alj,
                       const double *alk, const double *aui, const double *auj, const double *auk,
                       const double *bb, double *x0, const int *indc, int *iter, double *bnorm,

@@ -146,6 +146,33 @@ def test_fortran_entry_point(gpu_lib, pkg, orc):
     assert_same(st, ref, "vf_step_gpu_")
 
 
+def test_fortran_v1cal_f1cal_entry_points(gpu_lib, pkg):
+    """vf_v1cal_gpu_ then vf_f1cal_gpu_, with the time advanced by the
+    caller as the reference loop does, equal cadmas_step."""
+    c = pkg.cases.random_tank(5)
+    t = pkg.Tank(c)
+    t.init_state(True)
+    st = t.get_state()
+    t2 = pkg.Tank(c)
+    t2.set_state(st)
+    t2.step(c.dt)
+    ref = t2.get_state()
+    lib = gpu_lib
+    hp = ctypes.c_void_p(t.h.value)
+    dt = ctypes.c_double(c.dt)
+    tnow = ctypes.c_double(st["tnow"] + c.dt)
+    nnow = ctypes.c_int(st["nnow"] + 1)
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    for fn in (lib.vf_v1cal_gpu_, lib.vf_f1cal_gpu_):
+        rc = fn(ctypes.byref(hp), ctypes.byref(tnow), ctypes.byref(dt), ctypes.byref(nnow), dp(st["uu"]),
+                dp(st["vv"]), dp(st["ww"]), dp(st["pp"]), dp(st["ff"]), ip(st["nf"]), ip(st["indc"]),
+                dp(st["bcu"]), dp(st["bcv"]), dp(st["bcw"]), dp(st["bcp"]), dp(st["bcf"]))
+        assert rc == 0
+    assert nnow.value == ref["nnow"] and tnow.value == ref["tnow"]
+    assert_same(st, ref, "vf_v1cal_gpu_/vf_f1cal_gpu_")
+
+
 def test_flume_full_size_properties(gpu_lib, pkg):
     """512x32x96 porous flume (block-Jacobi tiles): a few steps keep the
     fluid volume (closed box) and a divergence-free correction."""
