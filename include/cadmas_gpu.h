@@ -45,6 +45,8 @@ extern "C" {
 #define CADMAS_EUNSUPPORTED  9  /* option outside the implemented path           */
 #define CADMAS_ENOSTATIC    10  /* cadmas_upload_static not called yet           */
 #define CADMAS_ETIMEOUT     11  /* a device-side wait ran out of time (2 s)      */
+#define CADMAS_ESCRATCH     12  /* grid larger than the static scratch of
+                                   cadmas_divnorm_noalloc                       */
 
 /* ---- sizes (/VF_ANUMBI/, VF_ANUMBI.h) ----------------------------------- */
 typedef struct cadmas_dims {
@@ -205,6 +207,29 @@ int cadmas_m1bcgs_dev(cadmas_handle *h,
                       const double *auk, const double *bb, double *x0,
                       const int *indc, int *iter, double *bnorm,
                       double *xnorm);
+
+/* ---- Allocation-free divergence norm (no counterpart in the reference) --
+   |VD| of VF_CDIV00 (vf_cdiv00.f:38-56), the value cadmas_divnorm returns
+   for a handle's state, computed on arrays the caller holds on the device
+   (device pointers, reference layout) without a handle and without
+   allocating any memory: the row partials go to a static device array of
+   CADMAS_NOALLOC_MAX_ROWS doubles (512 KB).  Runs on `stream`
+   (cudaStream_t; NULL = the default stream), waits for it, writes the
+   norm to *val (host).
+     - NUMJ*NUMK above CADMAS_NOALLOC_MAX_ROWS: CADMAS_ESCRATCH, nothing runs.
+     - Nothing in the scratch needs to start at zero (every partial is
+       written before it is read).
+     - The scratch is one array per device: calls that overlap in time on
+       one device (any streams or threads) race; issue them one after
+       another.
+     - The first call on a device looks the scratch up
+       (cudaGetSymbolAddress) and may load the module; make it before any
+       phase that must not see such set-up work.                          */
+#define CADMAS_NOALLOC_MAX_ROWS 65536
+int cadmas_divnorm_noalloc(const cadmas_dims *d, const double *xx, const double *yy,
+                           const double *zz, const double *ggx, const double *ggy,
+                           const double *ggz, const double *uu, const double *vv,
+                           const double *ww, const int *indc, void *stream, double *val);
 
 /* The CUDA stream (cudaStream_t) on which every call of the handle issues
    its work; callers may record CUDA events on it or wait on it. */

@@ -25,7 +25,7 @@ from . import cases  # noqa: F401  (re-exported)
 HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = HERE / "libcadmas_gpu.so"
 
-OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC, ETIMEOUT = range(12)
+OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC, ETIMEOUT, ESCRATCH = range(13)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -67,7 +67,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_set_state", "cadmas_get_state", "cadmas_init_state", "cadmas_step",
             "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
             "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
-            "cadmas_strerror",
+            "cadmas_strerror", "cadmas_divnorm_noalloc",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers"]
 
 STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]
@@ -115,6 +115,7 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_strerror.restype = C.c_char_p
     vf = lib.vf_step_gpu_
     vf.argtypes = [C.POINTER(C.c_void_p), _dp] + [_dp] * 5 + [_ip, _ip] + [_dp] * 5 + [_dp, _ip]
+    lib.cadmas_divnorm_noalloc.argtypes = [C.POINTER(Dims)] + [C.c_void_p] * 11 + [_dp]
     if path is None:
         _lib = lib
     return lib
@@ -314,3 +315,15 @@ def m1bcgs_dev(tank: Tank, ad, ali, alj, alk, aui, auj, auk, bb, x0, indc):
     args = [C.c_void_p(int(a)) for a in (ad, ali, alj, alk, aui, auj, auk, bb, x0, indc)]
     _check(tank.lib, tank.lib.cadmas_m1bcgs_dev(tank.h, *args, C.byref(it), C.byref(bn), C.byref(xn)))
     return it.value, bn.value, xn.value
+
+
+def divnorm_noalloc(dims, xx, yy, zz, ggx, ggy, ggz, uu, vv, ww, indc, stream=0, lib=None):
+    """|VD| of VF_CDIV00 on device arrays (integer device addresses, e.g.
+    torch.Tensor.data_ptr(); reference layout) without a handle and without
+    allocating: cadmas_divnorm_noalloc.  dims = (NUMI, NUMJ, NUMK)."""
+    lib = lib or load_library()
+    d = Dims(int(dims[0]), int(dims[1]), int(dims[2]), 0)
+    v = C.c_double()
+    args = [C.c_void_p(int(a)) for a in (xx, yy, zz, ggx, ggy, ggz, uu, vv, ww, indc)]
+    _check(lib, lib.cadmas_divnorm_noalloc(C.byref(d), *args, C.c_void_p(int(stream)), C.byref(v)))
+    return v.value

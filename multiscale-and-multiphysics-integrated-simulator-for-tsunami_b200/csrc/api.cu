@@ -473,6 +473,7 @@ const char *cadmas_strerror(int status) {
     case CADMAS_EUNSUPPORTED: return "option outside the implemented path";
     case CADMAS_ENOSTATIC: return "static fields not uploaded";
     case CADMAS_ETIMEOUT: return "a device-side wait ran out of time";
+    case CADMAS_ESCRATCH: return "grid has more than CADMAS_NOALLOC_MAX_ROWS (65536) rows NUMJ*NUMK";
     default: return "unknown status";
   }
 }
