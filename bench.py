@@ -364,7 +364,7 @@ def main():
     ap.add_argument("--ny", type=int, default=32)
     ap.add_argument("--nz", type=int, default=96)
     ap.add_argument("--ti", type=int, default=16)
-    ap.add_argument("--tj", type=int, default=8)
+    ap.add_argument("--tj", type=int, default=16)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

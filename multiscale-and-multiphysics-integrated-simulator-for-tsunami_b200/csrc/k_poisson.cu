@@ -368,6 +368,17 @@ __device__ __noinline__ bool mbar_wait_slow(unsigned bar, unsigned parity, unsig
     if (global_ns() - t0 > limit_ns) return false;
   }
 }
+// Non-blocking test of a phase: its latency overlaps the instructions that
+// follow until the predicate is used.
+__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
   return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, 2000000000ull);
 }
@@ -414,8 +425,14 @@ __global__ void __launch_bounds__(MAXT, 1)
   const bool producer = tid >= Tc;
   const int lane = tid & 31;
 
-  if (tid == 0)
+  // s_abort[c & 1]: a wait of some thread ran out of time during ring
+  // cycle c.  Written during a cycle, read after its last barrier; the two
+  // entries keep those reads apart from the writes of the next cycle.
+  __shared__ int s_abort[2];
+  if (tid == 0) {
     for (int r = 0; r < R; ++r) mbar_init(smem_u32(bar + r), 1);
+    s_abort[0] = s_abort[1] = 0;
+  }
   if (MODE == SWEEP_FWD_AX) {  // halo values of absent neighbours stay 0 (ghost layer)
     const int nh = 2 * halo_span(q) + 2 * TIp;
     for (int r = 0; r < R; ++r)
@@ -518,10 +535,11 @@ __global__ void __launch_bounds__(MAXT, 1)
   if (!producer) {
     for (int u = 0; u < AHEAD; ++u) if (ok) ok = wait_data(u, u % R, (unsigned)((u / R) & 1));
     if (ok) prepare(0, slot_ptr(0), slot_ptr(R - 1), slot_ptr(1 % R));
+    else s_abort[0] = 1;
   }
   bool aborted = false;
   int issued = min(D, nsteps) - 1;  // last step whose copies were issued (producer)
-  unsigned ph = 0;                  // (s0 / R) & 1
+  unsigned ph = 0;                  // (s0 / R) & 1, also the ring cycle's s_abort entry
 #pragma unroll 1
   for (int s0 = 0; s0 < nsteps && !aborted; s0 += R, ph ^= 1u) {
 #pragma unroll
@@ -532,8 +550,13 @@ __global__ void __launch_bounds__(MAXT, 1)
         issue(s + D, (r + D) % R);
         if (s + D < nsteps) issued = s + D;
       } else {
+        // Test the data of the step to prepare next now, so the test's
+        // latency overlaps the recurrence; wait only if it is not there.
+        const int u = s + AHEAD;  // newest data that preparing s+1 reads
+        const unsigned ubar = bar0 + 8u * ((r + AHEAD) % R), upar = ph ^ (unsigned)((r + AHEAD) / R);
+        const bool ready = !ok || u >= nsteps || mbar_test(ubar, upar);
         // the recurrence of step s
-        if (act) {
+        if (act && ok) {
           const int cur = (s & 1) * T, prv = T - cur;
           double x = 0.0;
           if (dd != 0.0) {
@@ -553,12 +576,17 @@ __global__ void __launch_bounds__(MAXT, 1)
         }
         vp += vstep;
         // prepare step s+1
-        const int u = s + 1 + AHEAD - 1;  // newest data that preparing s+1 reads
-        if (ok) ok = wait_data(u, (r + AHEAD) % R, ph ^ (unsigned)((r + AHEAD) / R));
+        if (!ready) {
+          ok = mbar_wait_slow(ubar, upar, 2000000000ull);
+          if (!ok) s_abort[ph] = 1;
+        }
         if (ok && s + 1 < nsteps) prepare(s + 1, slot_ptr((r + 1) % R), slot_ptr(r), slot_ptr((r + 2) % R));
       }
-      if (__syncthreads_or(!ok)) { aborted = true; break; }
+      __syncthreads();
     }
+    // A timed-out wait stops the sweep at the end of this ring cycle; the
+    // threads that gave up skip their remaining waits and work meanwhile.
+    if (s_abort[ph]) aborted = true;
   }
   if (aborted && producer) {
     // Let the copies already issued land (bounded) before the block exits.
@@ -873,16 +901,17 @@ void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const
   RING_LAUNCH2(k_dcmp, 7, g, q, U, S, pivot_bad);
 #undef RING_EXTRA
 }
-// Sweeps: prefetch depth D in {8, 4, 2}, the largest whose ring (R = D+2
-// slots, mbarriers, exchange buffers) fits 200 KB.
+// Sweeps: prefetch depth D in {8, 6, 4, 3, 2}, the largest whose ring
+// (R = D+2 slots, mbarriers, exchange buffers) fits the 227 KB of shared
+// memory a block may use.
 static size_t sweep_bytes(const SkewGeo &q, int mode, int D) {
   const int R = D + 2;
   return (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode) * 8 + 2 * (size_t)q.T * 8;
 }
 static int sweep_depth(const SkewGeo &q, int mode) {
   if (sweep_threads(q.T) > 1024) return 0;
-  for (int d : {8, 4, 2})
-    if (sweep_bytes(q, mode, d) <= 200 * 1024) return d;
+  for (int d : {8, 6, 4, 3, 2})
+    if (sweep_bytes(q, mode, d) <= 227 * 1024) return d;
   return 0;
 }
 template <int MODE>
@@ -891,17 +920,19 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   const int d = sweep_depth(q, MODE);
   const size_t bytes = sweep_bytes(q, MODE, d);
   const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
-  // Blocks of up to 256 threads get the registers to keep a prepared step
-  // in flight; larger tiles run the same code within 64 registers.
-  const bool small = sweep_threads(q.T) <= 256;
-  switch (d * 2 + (small ? 1 : 0)) {
+  // The register budget follows the block size (255, 128 or 64 registers
+  // for blocks of up to 256, 512 or 1024 threads).
+  const int nt = sweep_threads(q.T);
+  const int mt = nt <= 256 ? 256 : (nt <= 512 ? 512 : 1024);
+  switch (d * 4096 + mt) {
 #define SWEEP_CASE(DD, MT)                                                              \
-  case DD * 2 + (MT == 256 ? 1 : 0):                                                    \
+  case DD * 4096 + MT:                                                                  \
     set_smem(k_sweep<DD, MODE, MT>, bytes);                                             \
     k_sweep<DD, MODE, MT><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);           \
     break;
-    SWEEP_CASE(8, 256) SWEEP_CASE(4, 256) SWEEP_CASE(2, 256)
-    SWEEP_CASE(8, 1024) SWEEP_CASE(4, 1024) SWEEP_CASE(2, 1024)
+    SWEEP_CASE(8, 256) SWEEP_CASE(6, 256) SWEEP_CASE(4, 256) SWEEP_CASE(3, 256) SWEEP_CASE(2, 256)
+    SWEEP_CASE(8, 512) SWEEP_CASE(6, 512) SWEEP_CASE(4, 512) SWEEP_CASE(3, 512) SWEEP_CASE(2, 512)
+    SWEEP_CASE(8, 1024) SWEEP_CASE(6, 1024) SWEEP_CASE(4, 1024) SWEEP_CASE(3, 1024) SWEEP_CASE(2, 1024)
 #undef SWEEP_CASE
     default: return;  // rejected by cadmas_create (sweep_supported)
   }
