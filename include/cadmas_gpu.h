@@ -125,6 +125,36 @@ typedef struct cadmas_stats {
   int    pad;
 } cadmas_stats;
 
+/* ---- wave-maker boundary, matrix-table form (WAVE-BC ... FUNC MATRIX) ----
+   The inflow of a side JD is interpolated from a table in time phase and
+   height, as VF_CWMTB1/VF_CWMTB2 do (vf_cwmtb1.f, vf_cwmtb2.f), scaled to
+   the current water column and faded in as VF_BWUWN does
+   (vf_bwuwn.f:259-470).  Tables are column-major like the Fortran
+   DMTBUN(MTBZZ,MTBTT).                                                     */
+typedef struct cadmas_wave_table {
+  int ntt, nzz;          /* MTBTT, MTBZZ                                     */
+  int mtbtyp;            /* MTBTYP: 1 level and velocities (scaled to the
+                            column's water level), 2 velocities only        */
+  int pad;
+  double phase0;         /* DMTBT0: phase at TNOW = 0                        */
+  const double *tt;      /* DMTBTT(MTBTT) phase, ascending in [0,1]         */
+  const double *hh;      /* DMTBHH(MTBTT) water level above WVLVL            */
+  const double *zz;      /* DMTBZZ(MTBZZ) height above WVLVL, ascending      */
+  const double *un;      /* DMTBUN(MTBZZ,MTBTT) velocity normal to the side  */
+  const double *ut;      /* DMTBUT(MTBZZ,MTBTT) vertical velocity            */
+} cadmas_wave_table;
+
+typedef struct cadmas_wave_bc {
+  int side;              /* JD: 1 X-, 2 X+, 3 Y-, 4 Y+                      */
+  int first, last;       /* IBCTYP(3..4,JD): J (X sides) or I (Y sides) of
+                            the generated faces, 1-based with ghosts       */
+  int pad;
+  double depth;          /* BCTYP(1,JD) still-water depth D                  */
+  double period;         /* BCTYP(3,JD) period T                             */
+  double ramp;           /* BCTYP(8,JD) AMPL: periods of the sine fade-in;
+                            0 = none                                        */
+} cadmas_wave_bc;
+
 typedef struct cadmas_handle cadmas_handle;
 
 /* Defaults of vf_a2dflt.f for every field of cadmas_params. */
@@ -167,6 +197,12 @@ int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st);
 
 /* Synchronise the handle's stream. */
 int cadmas_sync(cadmas_handle *h);
+
+/* Declare side w->side a wave-maker boundary driven by `tab` (copied).  Its
+   boundary faces are those of INDB with INDB(3,L) = 5 on that side.  One
+   table serves every wave side, as the reference's matrix data does.
+   Sides and tables persist until cadmas_destroy. */
+int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *tab);
 
 /* ---- Fortran-callable step (drop-in for the two CALLs of the time loop) --
    Arguments by reference, as gfortran passes them.  The arrays are the

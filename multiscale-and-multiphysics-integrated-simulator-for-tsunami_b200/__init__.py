@@ -35,6 +35,30 @@ class Dims(C.Structure):
     _fields_ = [("numi", C.c_int), ("numj", C.c_int), ("numk", C.c_int), ("numb", C.c_int)]
 
 
+class WaveTable(C.Structure):
+    _fields_ = [("ntt", C.c_int), ("nzz", C.c_int), ("mtbtyp", C.c_int), ("pad", C.c_int),
+                ("phase0", C.c_double), ("tt", _dp), ("hh", _dp), ("zz", _dp), ("un", _dp), ("ut", _dp)]
+
+
+class WaveBC(C.Structure):
+    _fields_ = [("side", C.c_int), ("first", C.c_int), ("last", C.c_int), ("pad", C.c_int),
+                ("depth", C.c_double), ("period", C.c_double), ("ramp", C.c_double)]
+
+
+def wave_structs(wave):
+    """(WaveBC, WaveTable, keep-alive arrays) of a case's wave-maker dict
+    (cases.wave_maker)."""
+    t = wave["table"]
+    arrs = {n: np.ascontiguousarray(t[n], dtype=np.float64) for n in ("tt", "hh", "zz")}
+    for n in ("un", "ut"):
+        arrs[n] = np.asfortranarray(t[n], dtype=np.float64)  # (MTBZZ, MTBTT)
+    tab = WaveTable(len(arrs["tt"]), len(arrs["zz"]), int(t.get("mtbtyp", 1)), 0, float(t.get("phase0", 0.0)),
+                    *(arrs[n].ctypes.data_as(_dp) for n in ("tt", "hh", "zz", "un", "ut")))
+    bc = WaveBC(int(wave["side"]), int(wave["first"]), int(wave["last"]), 0, float(wave["depth"]),
+                float(wave["period"]), float(wave.get("ramp", 0.0)))
+    return bc, tab, arrs
+
+
 class Params(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "rho0", "grz0", "vvmax", "cgpara", "cgepsa", "cgepsr", "cgdiv", "flower", "fupper",
@@ -67,7 +91,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_set_state", "cadmas_get_state", "cadmas_init_state", "cadmas_step",
             "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
             "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
-            "cadmas_strerror", "cadmas_divnorm_noalloc",
+            "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers"]
 
 STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]
@@ -116,6 +140,7 @@ def load_library(path: pathlib.Path | None = None):
     vf = lib.vf_step_gpu_
     vf.argtypes = [C.POINTER(C.c_void_p), _dp] + [_dp] * 5 + [_ip, _ip] + [_dp] * 5 + [_dp, _ip]
     lib.cadmas_divnorm_noalloc.argtypes = [C.POINTER(Dims)] + [C.c_void_p] * 11 + [_dp]
+    lib.cadmas_set_wave.argtypes = [C.c_void_p, C.POINTER(WaveBC), C.POINTER(WaveTable)]
     if path is None:
         _lib = lib
     return lib
@@ -226,7 +251,14 @@ class Tank:
         self.h = h
         self._static = static_of(case)   # keep the pointers' owners alive
         _check(self.lib, self.lib.cadmas_upload_static(self.h, C.byref(self._static)))
+        if getattr(case, "wave", None):
+            self.set_wave(case.wave)
         self.set_state(initial_state(case))
+
+    def set_wave(self, wave):
+        """Wave-maker side from a dict made by cases.wave_maker (cadmas_set_wave)."""
+        bc, tab, keep = wave_structs(wave)
+        _check(self.lib, self.lib.cadmas_set_wave(self.h, C.byref(bc), C.byref(tab)))
 
     # ------------------------------------------------------------ state
     def set_state(self, arrs):

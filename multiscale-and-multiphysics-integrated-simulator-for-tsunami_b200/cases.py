@@ -30,7 +30,7 @@ import numpy as np
 # Velocity/pressure boundary types INDB(3,L) and F boundary types INDB(4,L)
 # (vf_a1main.f:151-170).
 VP_SLIP, VP_NOSLIP, VP_FIXED, VP_FREE, VP_WAVE = 1, 2, 3, 4, 5
-F_FIXED, F_FREE = 1, 2
+F_FIXED, F_FREE, F_WAVE = 1, 2, 5
 
 
 def grid_metrics(coords: np.ndarray) -> np.ndarray:
@@ -97,6 +97,7 @@ class Case:
     bcp: np.ndarray = None
     bcf: np.ndarray = None
     params: dict = dataclasses.field(default_factory=dict)
+    wave: dict = None          # wave-maker side (wave_maker), or None
     dt: float = 1e-3
     hydrostatic: bool = True
 
@@ -548,3 +549,61 @@ def linear_wave_initial(c: Case, H: float, T: float, depth: float, g0: float = 9
             (wet[1:-1, 1:-1, kk - 1] | wet[1:-1, 1:-1, kk])
         c.ww[1:-1, 1:-1, kk] = np.where(m, prof[:, None], 0.0)
     return k
+
+
+def _wavenumber(T: float, depth: float, g0: float = 9.8) -> float:
+    """k of w^2 = g k tanh(k h) by Newton from the deep-water value."""
+    om = 2.0 * np.pi / T
+    k = om * om / g0
+    for _ in range(60):
+        th = np.tanh(k * depth)
+        fk = g0 * k * th - om * om
+        dk = g0 * th + g0 * k * depth * (1.0 - th * th)
+        k -= fk / dk
+    return k
+
+
+def first_order_wave_table(H: float, T: float, depth: float, g0: float = 9.8, ntt: int = 121,
+                           nzz: int = 81, ztop: float | None = None) -> dict:
+    """Matrix table (the input of WAVE-BC ... FUNC MATRIX) of a first-order
+    progressive wave at the boundary, eta = H/2 cos(2 pi p),
+    u = H/2 w cosh(k(z+h))/sinh(kh) cos(2 pi p),
+    w = H/2 w sinh(k(z+h))/sinh(kh) sin(2 pi p), at phases p = 0..1 and
+    heights z = -h..ztop above the still water level; the reference's
+    phase at time t is p = frac(p0 - t/T), so p0 = 0 puts a crest at
+    the boundary at t = 0."""
+    k = _wavenumber(T, depth, g0)
+    om = 2.0 * np.pi / T
+    a = 0.5 * H
+    tt = np.linspace(0.0, 1.0, ntt)
+    zt = ztop if ztop is not None else 1.5 * a
+    zz = np.linspace(-depth, zt, nzz)
+    sk = np.sinh(k * depth)
+    ph = 2.0 * np.pi * tt
+    un = a * om * np.cosh(k * (zz[:, None] + depth)) / sk * np.cos(ph)[None, :]
+    ut = a * om * np.sinh(k * (zz[:, None] + depth)) / sk * np.sin(ph)[None, :]
+    return dict(tt=tt, hh=a * np.cos(ph), zz=zz, un=np.asfortranarray(un), ut=np.asfortranarray(ut),
+                phase0=0.0, mtbtyp=1, wavenumber=k)
+
+
+def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: float = 0.0,
+               table: dict | None = None) -> Case:
+    """Make side `side` (1 X-, 2 X+, 3 Y-, 4 Y+) a wave-maker boundary:
+    its domain-boundary faces get B.C. type 5 for velocity and F
+    (WAVE-BC, INDB(3,L) = INDB(4,L) = 5) over the whole side, driven by a
+    first-order wave table unless `table` is given."""
+    ns = {1: 1, 2: 2, 3: 3, 4: 4}[side]
+    for L in range(c.indb.shape[1]):
+        ijk, NS = int(c.indb[0, L]), int(c.indb[1, L])
+        if NS != ns:
+            continue
+        i = (ijk - 1) % c.ni + 1
+        j = ((ijk - 1) // c.ni) % c.nj + 1
+        if (side == 1 and i == 2) or (side == 2 and i == c.ni) or (side == 3 and j == 2) or \
+                (side == 4 and j == c.nj):
+            c.indb[2, L] = VP_WAVE
+            c.indb[3, L] = F_WAVE
+    first, last = 2, (c.nj - 1 if side <= 2 else c.ni - 1)
+    c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp,
+                  table=table if table is not None else first_order_wave_table(H, T, depth))
+    return c

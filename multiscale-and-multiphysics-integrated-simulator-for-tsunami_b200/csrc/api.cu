@@ -150,6 +150,18 @@ struct cadmas_handle {
   cadmas_stats stats;
   int last_iter = 8;   // iterations of the previous solve: size of the first batch
   StageTimer tm;
+  // wave maker (matrix table): sides JD = 1..4, one table for all of them
+  struct WaveSide {
+    bool on = false;
+    int first = 0, last = 0;
+    double d = 0.0, t = 0.0, a = 0.0;
+  } wave[4];
+  int mtbtyp = 0, mtbnow = 0;  // MTBTYP, MTBNOW (persists between calls, vf_a2dflt.f:114)
+  double dmtbt0 = 0.0;
+  std::vector<double> wtt, whh;  // DMTBTT, DMTBHH (host)
+  int nzz = 0;
+  double *wzz = nullptr, *wun = nullptr, *wut = nullptr;  // DMTBZZ, DMTBUN, DMTBUT (device)
+  double wave_level[4] = {0, 0, 0, 0};  // BCTYP(7,JD) = WVZ*AW of the last call
 };
 
 #define TB(stage) h->tm.begin(h->s, (stage))
@@ -192,6 +204,69 @@ static void refresh_prm(cadmas_handle *h) {
 }
 
 static long long nrows(const cadmas_handle *h) { return (long long)h->g.NJ * h->g.NK; }
+
+// VF_CWMTB1 (vf_cwmtb1.f:26-69): weights of the table rows around phase
+// WVT and the interpolated level; the search starts at MTBNOW.
+static bool cwmtb1(cadmas_handle *h, double WVT, double &W1, double &W2, double &WVZ) {
+  const std::vector<double> &TT = h->wtt;
+  const int MTBTT = (int)TT.size();
+  int &MTBNOW = h->mtbnow;
+  if (MTBNOW <= 0) MTBNOW = MTBTT - 1;
+  if (WVT <= TT[0]) {
+    MTBNOW = 1; W1 = 1.0; W2 = 0.0;
+  } else if (WVT >= TT[MTBTT - 1]) {
+    MTBNOW = MTBTT - 1; W1 = 0.0; W2 = 1.0;
+  } else {
+    int IP = 0;
+    W1 = W2 = 0.0;
+    for (int I = MTBNOW; I >= 1; --I)
+      if (TT[I - 1] <= WVT && WVT <= TT[I]) {
+        IP = I; W2 = 1.0 / (TT[I] - TT[I - 1]); W1 = (TT[I] - WVT) * W2; W2 = (WVT - TT[I - 1]) * W2;
+        break;
+      }
+    if (IP == 0)
+      for (int I = MTBTT - 1; I >= MTBNOW + 1; --I)
+        if (TT[I - 1] <= WVT && WVT <= TT[I]) {
+          IP = I; W2 = 1.0 / (TT[I] - TT[I - 1]); W1 = (TT[I] - WVT) * W2; W2 = (WVT - TT[I - 1]) * W2;
+          break;
+        }
+    if (IP == 0) return false;  // 'P.G ERROR.'
+    MTBNOW = IP;
+  }
+  WVZ = (h->mtbtyp != 2) ? W1 * h->whh[MTBNOW - 1] + W2 * h->whh[MTBNOW] : 0.0;
+  return true;
+}
+
+// Wave-maker part of VF_BWUWN (vf_bwuwn.f:259-470) for the matrix-table
+// inflow: the time part here, the faces on the device (k_wave).
+static int wave_bc(cadmas_handle *h) {
+  const double PI = 3.141592653589794, ZERO = 1.0e-20;  // VF_A0PRM.h
+  for (int jd = 0; jd < 4; ++jd) {
+    const cadmas_handle::WaveSide &ws = h->wave[jd];
+    if (!ws.on) continue;
+    const double T = ws.t, T0 = h->dmtbt0;
+    float R4TN = (float)(T0 - h->tnow / T);
+    R4TN = R4TN - (float)(int)R4TN;
+    if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
+    double AW = 1.0, A = ws.a;
+    if (A >= ZERO) {
+      A = h->tnow / T / A;
+      if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
+    }
+    const double WVT = (double)R4TN;
+    WaveDev w;
+    if (!cwmtb1(h, WVT, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
+    h->wave_level[jd] = w.wvz * AW;
+    w.side = jd + 1; w.first = ws.first; w.last = ws.last;
+    w.mtbtyp = h->mtbtyp; w.nzz = h->nzz; w.mtbnow = h->mtbnow;
+    w.d = ws.d; w.aw = AW; w.wvlvl = h->P.wvlvl;
+    w.sa = (jd == 0) ? 1.0 : (jd == 1 ? -1.0 : 0.0);  // normal incidence (vf_bwuwn.f:298-310)
+    w.sb = (jd == 2) ? 1.0 : (jd == 3 ? -1.0 : 0.0);
+    w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
+    launch_wave(h->s, h->g, h->f, w, h->dint);
+  }
+  return CADMAS_OK;
+}
 
 // ------------------------------------------------------------ solver
 // VF_M1BCGS on the system a with initial guess/result x0.  The BiCGSTAB
@@ -349,7 +424,10 @@ static int do_v1cal(cadmas_handle *h) {
   h->cur = nxt;
   refresh_fld(h);
   // normal boundary velocities (vf_v1cal.f:251-254)
-  TB(CADMAS_STAGE_MODIF); launch_bwuwn(s, h->g, h->f, h->dint); TE();
+  TB(CADMAS_STAGE_MODIF);
+  launch_bwuwn(s, h->g, h->f, h->dint);
+  { const int rw = wave_bc(h); if (rw) return rw; }
+  TE();
   // Poisson system (vf_v1cal.f:259-271)
   SysPtr a{h->wk[0], h->wk[1], h->wk[2], h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[7]};
   TB(CADMAS_STAGE_VPCOEF); launch_vpcoef(s, h->g, h->f, h->p, a, h->dint); TE();
@@ -580,8 +658,44 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_st) cudaFreeHost(h->h_st);
   if (h->h_int) cudaFreeHost(h->h_int);
   if (h->h_res) cudaFreeHost(h->h_res);
+  for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
+  return CADMAS_OK;
+}
+
+int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
+  if (!h || !w || !t || !t->tt || !t->hh || !t->zz || !t->un || !t->ut) return CADMAS_EINVAL;
+  if (w->side < 1 || w->side > 4 || t->ntt < 2 || t->nzz < 2) return CADMAS_EINVAL;
+  if (t->mtbtyp != 1 && t->mtbtyp != 2) {
+    g_last_error = "wave table type MTBTYP 3 (fixed water level) is not implemented";
+    return CADMAS_EUNSUPPORTED;
+  }
+  if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
+  const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;  // vf_iimdl.f:101-106
+  if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
+  for (int i = 1; i < t->ntt; ++i) if (!(t->tt[i] >= t->tt[i - 1])) return CADMAS_EINVAL;
+  for (int k = 1; k < t->nzz; ++k) if (!(t->zz[k] > t->zz[k - 1])) return CADMAS_EINVAL;
+  const size_t nzt = (size_t)t->nzz * t->ntt;
+  if (h->nzz != 0 && (h->nzz != t->nzz || (int)h->wtt.size() != t->ntt)) return CADMAS_EINVAL;
+  if (!h->wzz) {
+    int rc = CADMAS_OK;
+    if (!rc) rc = dalloc(&h->wzz, (size_t)t->nzz);
+    if (!rc) rc = dalloc(&h->wun, nzt);
+    if (!rc) rc = dalloc(&h->wut, nzt);
+    if (rc) return rc;
+  }
+  CK(cudaMemcpy(h->wzz, t->zz, (size_t)t->nzz * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->wun, t->un, nzt * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->wut, t->ut, nzt * sizeof(double), cudaMemcpyHostToDevice));
+  h->wtt.assign(t->tt, t->tt + t->ntt);
+  h->whh.assign(t->hh, t->hh + t->ntt);
+  h->nzz = t->nzz;
+  h->mtbtyp = t->mtbtyp;
+  h->dmtbt0 = t->phase0;
+  cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
+  ws.on = true; ws.first = w->first; ws.last = w->last;
+  ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
   return CADMAS_OK;
 }
 
@@ -711,6 +825,7 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   }
   // vf_cinit.f:388-394
   launch_bwuwn(s, h->g, h->f, h->dint);
+  { const int rw = wave_bc(h); if (rw) return rw; }
   launch_bsuwt(s, h->g, h->f, h->p);
   launch_bsuwt2(s, h->g, h->f);
   launch_bsuwn3(s, h->g, h->f, h->p);

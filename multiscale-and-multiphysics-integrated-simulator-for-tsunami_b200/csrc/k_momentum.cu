@@ -578,14 +578,111 @@ __global__ void k_bwuwn(Geo g, Fld f, int *err) {
     else if (NS == 3 || NS == 4) { f.bcv[L - 1] = 0.0; VV[cid(g, I, J, K)] = 0.0; }
     else { f.bcw[L - 1] = 0.0; WW[cid(g, I, J, K)] = 0.0; }
     atomicOr(err, ERR_UNSUP);
-  } else if (IB == 5 || IB == 7) {
+  } else if (IB == 5) {
+    // wave-maker faces: set by k_wave after this pass (vf_bwuwn.f:259-470);
+    // the per-face rule of vf_bwuwn.f:161-216 applies to MTBTYP 3 only,
+    // which cadmas_set_wave does not accept
+  } else if (IB == 7) {
     atomicOr(err, ERR_UNSUP);
   } else {
     atomicOr(err, ERR_PG);
   }
 }
 
+// ------------------------------------------------- VF_BWUWN, wave maker
+// Wave-maker faces of one side for the matrix-table inflow
+// (vf_bwuwn.f:330-470 with VF_CWMTB2, vf_cwmtb2.f), one thread per
+// boundary line (J on the X sides, I on the Y sides).  The host has done
+// the time part: phase, fade-in AW and VF_CWMTB1's weights and row MTBNOW.
+__global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
+  const int n = w.first + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (n > w.last) return;
+  const int NI = g.NI, NJ = g.NJ, NK = g.NK;
+  const bool xs = (w.side <= 2);
+  int I, J, IC, JC;
+  if (xs) {
+    J = n; JC = n;
+    if (J < 2 || J > NJ - 1) return;
+    I = (w.side == 1) ? 2 : NI;
+    IC = (w.side == 1) ? 2 : NI - 1;
+  } else {
+    I = n; IC = n;
+    if (I < 2 || I > NI - 1) return;
+    J = (w.side == 3) ? 2 : NJ;
+    JC = (w.side == 3) ? 2 : NJ - 1;
+  }
+  // current water level of the column next to the boundary, scaling
+  double VWS;
+  if (w.mtbtyp != 1) {
+    VWS = 1.0;
+  } else {
+    double VAL = 0.0;
+    for (int K = 2; K <= NK - 1; ++K) {
+      const int NW = f.nf[cid(g, IC, JC, K)];
+      if (NW == -1) {
+        VAL = VAL + gz(g, 2, K) * 1.0;
+      } else if (NW == 0) {
+        VAL = VAL + gz(g, 2, K) * f.ff[cid(g, IC, JC, K)];
+      } else if (NW != 8) {
+        VAL = VAL + gz(g, 2, K) * f.ff[cid(g, IC, JC, K)];
+        break;
+      }
+    }
+    VAL = VAL - (w.wvlvl - gz(g, 1, 2));
+    VWS = (w.wvz + w.d) / (VAL + w.d);
+  }
+  // boundary values face by face; the height search starts where the face
+  // below found its interval
+  int KM = 1;
+  const int nz = w.nzz;
+  for (int K = 2; K <= NK - 1; ++K) {
+    const long long c = cid(g, I, J, K);
+    const int L = xs ? f.indx[c] : f.indy[c];
+    if (L < 1) continue;
+    double ZC = (gz(g, 1, K) + gz(g, 1, K + 1)) * 0.5 - w.wvlvl;
+    ZC = VWS * (ZC + w.d) - w.d;
+    double W1, W2;
+    if (ZC <= w.zz[0]) {
+      KM = 1; W1 = 1.0; W2 = 0.0;
+    } else if (ZC >= w.zz[nz - 1]) {
+      KM = nz - 1; W1 = 0.0; W2 = 1.0;
+    } else {
+      int KP = 0;
+      W1 = 0.0; W2 = 0.0;
+      for (int k = KM; k <= nz - 1; ++k) {
+        if (w.zz[k - 1] <= ZC && ZC <= w.zz[k]) {
+          KP = k;
+          W2 = 1.0 / (w.zz[k] - w.zz[k - 1]);
+          W1 = (w.zz[k] - ZC) * W2;
+          W2 = (ZC - w.zz[k - 1]) * W2;
+          break;
+        }
+      }
+      if (KP == 0) { atomicOr(err, ERR_PG); return; }
+      KM = KP;
+    }
+    const long long i0 = (long long)nz * (w.mtbnow - 1), i1 = i0 + nz;  // columns MTBNOW, MTBNOW+1
+    double P1 = W1 * w.un[i0 + KM - 1] + W2 * w.un[i0 + KM];
+    double P2 = W1 * w.un[i1 + KM - 1] + W2 * w.un[i1 + KM];
+    const double UN = w.wt1 * P1 + w.wt2 * P2;
+    P1 = W1 * w.ut[i0 + KM - 1] + W2 * w.ut[i0 + KM];
+    P2 = W1 * w.ut[i1 + KM - 1] + W2 * w.ut[i1 + KM];
+    const double UT = w.wt1 * P1 + w.wt2 * P2;
+    f.bcu[L - 1] = UN * VWS * w.aw * w.sa;
+    f.bcv[L - 1] = UN * VWS * w.aw * w.sb;
+    f.bcw[L - 1] = UT * VWS * w.aw;
+    if (xs) f.uu[c] = f.bcu[L - 1];
+    else f.vv[c] = f.bcv[L - 1];
+  }
+}
+
 // ------------------------------------------------------------ launchers
+void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, int *err) {
+  const int n = w.last - w.first + 1;
+  if (n <= 0) return;
+  k_wave<<<(n + 127) / 128, 128, 0, s>>>(g, f, w, err);
+  count_launch();
+}
 void launch_flux(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl) {
   k_flux<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, f, p, fl[0], fl[1], fl[2], fl[3], fl[4], fl[5],
                                                 fl[6], fl[7], fl[8]);

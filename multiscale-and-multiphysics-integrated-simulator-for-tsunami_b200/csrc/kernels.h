@@ -148,11 +148,20 @@ __host__ __device__ inline bool sweep_copy(const SkewGeo &q, int mode, int b, in
 enum FinMode { FIN_BNORM = 0, FIN_START = 1, FIN_STORE = 2, FIN_RELRES = 3,
                FIN_ALPHA = 10, FIN_OMEGA = 11, FIN_CONV = 12 };
 
+// Time-dependent part of one wave-maker side (host side of VF_BWUWN).
+struct WaveDev {
+  int side, first, last;  // JD and the range of boundary lines
+  int mtbtyp, nzz, mtbnow;  // table type, MTBZZ, row MTBNOW (1-based)
+  double d, wvz, wt1, wt2, aw, sa, sb, wvlvl;
+  const double *zz, *un, *ut;  // device copies of DMTBZZ, DMTBUN, DMTBUT
+};
+
 // k_momentum.cu
 void launch_flux(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl);
 void launch_predict(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl,
                     double *un, double *vn, double *wn);
 void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, int *err);
+void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, int *err);
 
 // k_poisson.cu
 void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const SysPtr &a, int *err);

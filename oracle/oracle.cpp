@@ -73,6 +73,12 @@ struct orc_handle {
   vi NF, INDC, INDS, NLIM;
   int NUMS = 0;
   double TNOW = 0, DTNOW = 0;
+  // wave maker, matrix table (WAVE-BC ... FUNC MATRIX): IBCTYP/BCTYP of
+  // the four sides and the table of /VF_AFILEI/ (vf_iimdl.f:49-106)
+  struct Wave { int on = 0, l1 = 0, l2 = 0; double d = 0, t = 0, a = 0; } WV[4];
+  int MTBTYP = 0, MTBNOW = 0;
+  double DMTBT0 = 0;
+  vd DMTBTT, DMTBHH, DMTBZZ, DMTBUN, DMTBUT;
   int NNOW = 0;
   // work arrays WK01..WK17
   vd WK[18];
@@ -790,10 +796,146 @@ struct orc_handle {
         else if (NS == 4) { VAL = VV[id(I, J - 1, K)]; BCV[L - 1] = VAL; VV[id(I, J, K)] = VAL; }
         else if (NS == 5) { VAL = WW[id(I, J, K + 1)]; BCW[L - 1] = VAL; WW[id(I, J, K)] = VAL; }
         else if (NS == 6) { VAL = WW[id(I, J, K - 1)]; BCW[L - 1] = VAL; WW[id(I, J, K)] = VAL; }
-      } else if (IB == 5 || IB == 7) {
+      } else if (IB == 5) {
+        // vf_bwuwn.f:161-216 acts for MTBTYP 3 only (not accepted here)
+      } else if (IB == 7) {
         return CADMAS_EUNSUPPORTED;
       } else {
         return CADMAS_EPG;
+      }
+    }
+    return bwuwn_wave();
+  }
+
+  // VF_CWMTB1  vf_cwmtb1.f:26-69
+  bool cwmtb1(double WVT, double &W1, double &W2, double &WVZ) {
+    const int MTBTT = (int)DMTBTT.size();
+    auto TT = [&](int i) { return DMTBTT[i - 1]; };
+    if (MTBNOW <= 0) MTBNOW = MTBTT - 1;
+    if (WVT <= TT(1)) {
+      MTBNOW = 1; W1 = 1.0; W2 = 0.0;
+    } else if (WVT >= TT(MTBTT)) {
+      MTBNOW = MTBTT - 1; W1 = 0.0; W2 = 1.0;
+    } else {
+      int IP = 0;
+      W1 = W2 = 0.0;
+      for (int I = MTBNOW; I >= 1 && IP == 0; --I) {
+        if (TT(I) <= WVT && WVT <= TT(I + 1)) {
+          IP = I;
+          W2 = 1.0 / (TT(I + 1) - TT(I));
+          W1 = (TT(I + 1) - WVT) * W2;
+          W2 = (WVT - TT(I)) * W2;
+        }
+      }
+      for (int I = MTBTT - 1; I >= MTBNOW + 1 && IP == 0; --I) {
+        if (TT(I) <= WVT && WVT <= TT(I + 1)) {
+          IP = I;
+          W2 = 1.0 / (TT(I + 1) - TT(I));
+          W1 = (TT(I + 1) - WVT) * W2;
+          W2 = (WVT - TT(I)) * W2;
+        }
+      }
+      if (IP == 0) return false;
+      MTBNOW = IP;
+    }
+    WVZ = (MTBTYP != 2) ? W1 * DMTBHH[MTBNOW - 1] + W2 * DMTBHH[MTBNOW] : 0.0;
+    return true;
+  }
+
+  // VF_CWMTB2  vf_cwmtb2.f:26-66
+  bool cwmtb2(int &KM, double WT1, double WT2, double ZC, double &UN, double &UT) const {
+    const int MTBZZ = (int)DMTBZZ.size();
+    auto ZT = [&](int k) { return DMTBZZ[k - 1]; };
+    auto TUN = [&](int k, int i) { return DMTBUN[(k - 1) + (size_t)MTBZZ * (i - 1)]; };
+    auto TUT = [&](int k, int i) { return DMTBUT[(k - 1) + (size_t)MTBZZ * (i - 1)]; };
+    double W1, W2;
+    if (ZC <= ZT(1)) {
+      KM = 1; W1 = 1.0; W2 = 0.0;
+    } else if (ZC >= ZT(MTBZZ)) {
+      KM = MTBZZ - 1; W1 = 0.0; W2 = 1.0;
+    } else {
+      int KP = 0;
+      W1 = W2 = 0.0;
+      for (int K = KM; K <= MTBZZ - 1 && KP == 0; ++K) {
+        if (ZT(K) <= ZC && ZC <= ZT(K + 1)) {
+          KP = K;
+          W2 = 1.0 / (ZT(K + 1) - ZT(K));
+          W1 = (ZT(K + 1) - ZC) * W2;
+          W2 = (ZC - ZT(K)) * W2;
+        }
+      }
+      if (KP == 0) return false;
+      KM = KP;
+    }
+    const int KM1 = KM + 1, IM = MTBNOW, IM1 = MTBNOW + 1;
+    double P1 = W1 * TUN(KM, IM) + W2 * TUN(KM1, IM);
+    double P2 = W1 * TUN(KM, IM1) + W2 * TUN(KM1, IM1);
+    UN = WT1 * P1 + WT2 * P2;
+    P1 = W1 * TUT(KM, IM) + W2 * TUT(KM1, IM);
+    P2 = W1 * TUT(KM, IM1) + W2 * TUT(KM1, IM1);
+    UT = WT1 * P1 + WT2 * P2;
+    return true;
+  }
+
+  // VF_BWUWN wave-maker part  vf_bwuwn.f:259-470, matrix-table inflow
+  // (IBCTYP(2,JD) = -3, MTBTYP 1 or 2; normal incidence, one rank).
+  int bwuwn_wave() {
+    const double PI = 3.141592653589794, ZERO = 1.0e-20;
+    for (int JD = 1; JD <= 4; ++JD) {
+      const Wave &w = WV[JD - 1];
+      if (!w.on) continue;
+      const double D = w.d, T = w.t, T0 = DMTBT0;
+      double A = w.a;
+      float R4TN = (float)(T0 - TNOW / T);
+      R4TN = R4TN - (float)(int)R4TN;
+      if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
+      double AW = 1.0;
+      if (A >= ZERO) {
+        A = TNOW / T / A;
+        if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
+      }
+      const double WVT = (double)R4TN;
+      double WMT1, WMT2, WVZ;
+      if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
+      double SA, SB;
+      if (JD == 1) { SA = 1.0; SB = 0.0; }
+      else if (JD == 2) { SA = -1.0; SB = 0.0; }
+      else if (JD == 3) { SA = 0.0; SB = 1.0; }
+      else { SA = 0.0; SB = -1.0; }
+      const bool xs = (JD == 1 || JD == 2);
+      const int I0 = (JD == 1) ? 2 : NI, IC0 = (JD == 1) ? 2 : NI - 1;
+      const int J0 = (JD == 3) ? 2 : NJ, JC0 = (JD == 3) ? 2 : NJ - 1;
+      for (int n = w.l1; n <= w.l2; ++n) {
+        const int I = xs ? I0 : n, J = xs ? n : J0, IC = xs ? IC0 : n, JC = xs ? n : JC0;
+        if (xs ? (J < 2 || J > NJ - 1) : (I < 2 || I > NI - 1)) continue;
+        double VWS;
+        if (MTBTYP != 1) {
+          VWS = 1.0;
+        } else {
+          double VAL = 0.0;
+          for (int K = 2; K <= NK - 1; ++K) {
+            const int NW = NF[id(IC, JC, K)];
+            if (NW == -1) VAL = VAL + Z_(2, K) * 1.0;
+            else if (NW == 0) VAL = VAL + Z_(2, K) * FF[id(IC, JC, K)];
+            else if (NW != 8) { VAL = VAL + Z_(2, K) * FF[id(IC, JC, K)]; break; }
+          }
+          VAL = VAL - (P.wvlvl - Z_(1, 2));
+          VWS = (WVZ + D) / (VAL + D);
+        }
+        int KMT = 1;
+        for (int K = 2; K <= NK - 1; ++K) {
+          const int L = xs ? INDX[id(I, J, K)] : INDY[id(I, J, K)];
+          if (L < 1) continue;
+          double ZC = (Z_(1, K) + Z_(1, K + 1)) * 0.5 - P.wvlvl;
+          ZC = VWS * (ZC + D) - D;
+          double UN, UT;
+          if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
+          BCU[L - 1] = UN * VWS * AW * SA;
+          BCV[L - 1] = UN * VWS * AW * SB;
+          BCW[L - 1] = UT * VWS * AW;
+          if (xs) UU[id(I, J, K)] = BCU[L - 1];
+          else VV[id(I, J, K)] = BCV[L - 1];
+        }
       }
     }
     return CADMAS_OK;
@@ -2201,6 +2343,21 @@ int orc_get_poisson(orc_handle *h, int which, double *out) {
   const vd &a = h->WK[which + 1];
   if (a.empty()) return CADMAS_EINVAL;
   std::copy(a.begin(), a.end(), out);
+  return CADMAS_OK;
+}
+
+int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
+  if (!h || !w || !t || w->side < 1 || w->side > 4 || t->ntt < 2 || t->nzz < 2) return CADMAS_EINVAL;
+  if (t->mtbtyp != 1 && t->mtbtyp != 2) return CADMAS_EUNSUPPORTED;
+  h->DMTBTT.assign(t->tt, t->tt + t->ntt);
+  h->DMTBHH.assign(t->hh, t->hh + t->ntt);
+  h->DMTBZZ.assign(t->zz, t->zz + t->nzz);
+  h->DMTBUN.assign(t->un, t->un + (size_t)t->nzz * t->ntt);
+  h->DMTBUT.assign(t->ut, t->ut + (size_t)t->nzz * t->ntt);
+  h->MTBTYP = t->mtbtyp;
+  h->DMTBT0 = t->phase0;
+  orc_handle::Wave &v = h->WV[w->side - 1];
+  v.on = 1; v.l1 = w->first; v.l2 = w->last; v.d = w->depth; v.t = w->period; v.a = w->ramp;
   return CADMAS_OK;
 }
 

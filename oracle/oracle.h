@@ -52,6 +52,8 @@ int orc_m1bcgs(orc_handle *h, const double *ad, const double *ali,
 /* Read back the last Poisson system (WK01..WK08) and PT (WK09) of a step:
    which: 0 AD,1 ALI,2 ALJ,3 ALK,4 AUI,5 AUJ,6 AUK,7 BB,8 PT.               */
 int orc_get_poisson(orc_handle *h, int which, double *out);
+/* Wave-maker side with its matrix table (as cadmas_set_wave). */
+int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t);
 /* Seconds spent in the last orc_step by stage: [0] momentum predictor,
    [1] assembly, [2] solve, [3] correction+BC, [4] VOF+flags.              */
 int orc_get_timers(orc_handle *h, double *t5);

@@ -92,6 +92,10 @@ class Oracle:
             raise RuntimeError("orc_create failed")
         self._static = P.static_of(case)
         self._rc(self.lib.orc_upload_static(self.h, C.byref(self._static)))
+        if getattr(case, "wave", None):
+            bc, tab, keep = P.wave_structs(case.wave)
+            self.lib.orc_set_wave.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.WaveTable)]
+            self._rc(self.lib.orc_set_wave(self.h, C.byref(bc), C.byref(tab)))
         self.set_state(P.initial_state(case))
 
     def _rc(self, rc):

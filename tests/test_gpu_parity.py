@@ -120,6 +120,23 @@ def test_pivot_failure_status(gpu_lib, pkg):
     assert it == -1 and bn == 0.0 and xn == 0.0
 
 
+def test_wave_maker_flume_bitwise(gpu_lib, pkg, orc):
+    """Wave-maker inflow (matrix table, X- side, fade-in over one period)
+    into the porous flume: VF_BWUWN's wave part on the GPU, bit for bit."""
+    c = pkg.cases.porous_flume(nx=96, ny=4, nz=64, block=(1.2, 1.4, 0.6), sponge_width=0.4)
+    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5, ramp=1.0)
+    run_pair(pkg, orc, c, 24, check_every=8)
+
+
+def test_wave_maker_flume_tiles_bitwise(gpu_lib, pkg, orc):
+    """The same with a wave train already in the flume, no fade-in and
+    16x2 preconditioner blocks."""
+    c = pkg.cases.porous_flume(nx=96, ny=4, nz=64, block=(1.2, 1.4, 0.6), sponge_width=0.4)
+    pkg.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
+    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5)
+    run_pair(pkg, orc, c, 16, check_every=8, precond_ti=16, precond_tj=2)
+
+
 def test_fortran_entry_point(gpu_lib, pkg, orc):
     """vf_step_gpu_ (host arrays in, host arrays out) equals cadmas_step."""
     c = pkg.cases.random_tank(3)

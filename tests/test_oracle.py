@@ -137,3 +137,31 @@ def test_error_status_not_converged(pkg, orc):
     with pytest.raises(pkg.CadmasError) as e:
         o.step(c.dt)
     assert e.value.status == pkg.ENOTCONV
+
+
+def test_wave_maker_injects_the_table_wave(pkg, orc):
+    """Matrix-table wave maker on the X- side: the boundary faces carry the
+    table's velocity profile scaled by the fade-in, the inflow-side water
+    level rises during the crest phase, and the solver still converges."""
+    c = pkg.cases.porous_flume(nx=48, ny=2, nz=64, block=(0.6, 0.7, 0.6), sponge_width=0.2)
+    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5)          # no fade-in: full amplitude at once
+    o = orc.Oracle(c, sum_mode=orc.SUM_REF)
+    o.init_state(True)
+    v0 = o.stats()["fsum"]
+    o.step(c.dt)
+    st = o.get_state()
+    wave = c.indb[2] == 5
+    assert wave.sum() == (c.nj - 2) * (c.nk - 2)
+    bcu = st["bcu"][wave]
+    # crest at the boundary at t = dt: inflow everywhere below the surface,
+    # growing towards the surface (cosh profile)
+    tab = c.wave["table"]
+    assert np.all(bcu > 0.0)
+    assert bcu.max() <= tab["un"].max() * 1.2
+    col = st["uu"][1, 1, 1:-1]
+    wet = st["ff"][1, 1, 1:-1] > 0
+    assert np.all(np.diff(col[wet][: int(wet.sum()) - 1]) >= 0.0)
+    for _ in range(40):
+        o.step(c.dt)
+    assert o.stats()["fsum"] > v0
+    assert o.stats()["icgitr"] < 500
