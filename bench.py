@@ -92,7 +92,9 @@ def build_case(args):
 
 
 def params_for(args):
-    return dict(cgepsr=1.0e-10, precond_ti=args.ti, precond_tj=args.tj)
+    return dict(cgepsr=1.0e-10, precond_ti=args.ti, precond_tj=args.tj,
+                solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
+                warm_start=1 if getattr(args, "guess", "zero") == "previous" else 0)
 
 
 class ClockSampler:
@@ -210,7 +212,11 @@ def run_reference(args, rank, world):
 
 
 def workload_config(case, args):
-    return {"workload": f"porous wave flume {case.ni-2}x{case.nj-2}x{case.nk-2} plain FP64 SMAC step "
+    solver = ("mixed FP32-inner/FP64-refinement" if getattr(args, "solver", "fp64") == "mixed"
+              else "plain FP64")
+    if getattr(args, "guess", "zero") == "previous":
+        solver += ", previous-step initial guess,"
+    return {"workload": f"porous wave flume {case.ni-2}x{case.nj-2}x{case.nk-2} {solver} SMAC step "
                         f"(wave maker H=0.08 T=1.5 at x=0 on a developed first-order wave train, "
                         f"dt={case.dt}, tol 1e-10, block-Jacobi MILU "
                         f"{args.ti}x{args.tj} columns)",
@@ -379,6 +385,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--solver", choices=["fp64", "mixed"], default="fp64",
+                    help="pressure solver: the reference's FP64 MILU-BiCGSTAB, or FP32 inner solves "
+                         "under FP64 refinement")
+    ap.add_argument("--guess", choices=["zero", "previous"], default="zero",
+                    help="initial guess of each pressure solve: 0 as the reference, or the previous "
+                         "step's solution")
     ap.add_argument("--nx", type=int, default=512)
     ap.add_argument("--ny", type=int, default=32)
     ap.add_argument("--nz", type=int, default=96)

@@ -25,7 +25,7 @@ module cadmas_gpu
   integer(c_int), parameter :: CADMAS_OK = 0, CADMAS_EINVAL = 1, CADMAS_ECUDA = 2, &
        CADMAS_ENOTCONV = 3, CADMAS_EDIVERGE = 4, CADMAS_EPIVOT = 5, CADMAS_EPG = 6, &
        CADMAS_ECAP = 7, CADMAS_ENOMEM = 8, CADMAS_EUNSUPPORTED = 9, CADMAS_ENOSTATIC = 10, &
-       CADMAS_ETIMEOUT = 11
+       CADMAS_ETIMEOUT = 11, CADMAS_ESCRATCH = 12
 
   type, bind(C) :: cadmas_dims
      integer(c_int) :: numi, numj, numk, numb
@@ -40,7 +40,9 @@ module cadmas_gpu
      integer(c_int) :: icgtyp, icgmax, ibsuw0
      integer(c_int) :: precond_ti, precond_tj
      integer(c_int) :: diag_relres
-     integer(c_int) :: reserved(5)
+     integer(c_int) :: solver
+     integer(c_int) :: warm_start
+     integer(c_int) :: reserved(3)
   end type cadmas_params
 
   ! c_loc() of the static arrays (XX(6,NUMI) ... INDB(4,NUMB))
@@ -54,7 +56,7 @@ module cadmas_gpu
 
   type, bind(C) :: cadmas_stats
      real(c_double) :: fsum, fcut, cgbnrm, cgxnrm, divnorm, true_relres
-     integer(c_int) :: icgitr, nums, last_status, pad
+     integer(c_int) :: icgitr, nums, last_status, fallbacks
   end type cadmas_stats
 
   interface

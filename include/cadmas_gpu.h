@@ -87,7 +87,23 @@ typedef struct cadmas_params {
   /* 1: after every solve also measure the true residual ||b-Ax||/||b||
      (cadmas_stats.true_relres); costs one extra pass over the system. */
   int    diag_relres;
-  int    reserved[5];
+  /* Pressure solver (no counterpart in the reference, which has only the
+     first):
+       0  VF_M1BCGS in FP64, converged as the reference does on
+          |M^-1 r| <= CGEPSR |M^-1 b| (+ CGEPSA);
+       1  mixed precision: FP32 MILU factor and FP32 BiCGSTAB inner solves
+          under FP64 iterative refinement, converged on the true residual
+          ||b - Ax||_2 <= CGEPSR ||b||_2 computed in FP64.  Falls back to
+          solver 0 for a solve whose FP32 factor or inner solve fails.    */
+  int    solver;
+  /* Initial guess of the pressure solve (no counterpart in the reference,
+     which always starts from PT = 0, vf_vpsol.f:52-58):
+       0  PT = 0;
+       1  the previous step's solution (0 on cells with INDC = -1 now).
+     The stopping test is unchanged (|M^-1 r| against |M^-1 b| for
+     solver 0), so the result meets the same tolerance.                  */
+  int    warm_start;
+  int    reserved[3];
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */
@@ -122,7 +138,8 @@ typedef struct cadmas_stats {
   int    icgitr;                   /* ICGITR iterations of the last solve      */
   int    nums;                     /* NUMS surface cells                       */
   int    last_status;              /* status of the last step                  */
-  int    pad;
+  int    fallbacks;                /* solver 1: solves handed to the FP64
+                                      solver so far (0 for solver 0)          */
 } cadmas_stats;
 
 /* ---- wave-maker boundary, matrix-table form (WAVE-BC ... FUNC MATRIX) ----

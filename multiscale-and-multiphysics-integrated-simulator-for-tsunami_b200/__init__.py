@@ -67,7 +67,7 @@ class Params(C.Structure):
         ("idamp", C.c_int * 4),
         ("icgtyp", C.c_int), ("icgmax", C.c_int), ("ibsuw0", C.c_int),
         ("precond_ti", C.c_int), ("precond_tj", C.c_int),
-        ("diag_relres", C.c_int), ("reserved", C.c_int * 5)]
+        ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class Static(C.Structure):
@@ -84,7 +84,7 @@ class State(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("fsum", "fcut", "cgbnrm", "cgxnrm", "divnorm", "true_relres")] + [
-        (n, C.c_int) for n in ("icgitr", "nums", "last_status", "pad")]
+        (n, C.c_int) for n in ("icgitr", "nums", "last_status", "fallbacks")]
 
 
 EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_upload_static",
@@ -296,7 +296,7 @@ class Tank:
     def stats(self):
         st = Stats()
         _check(self.lib, self.lib.cadmas_get_stats(self.h, C.byref(st)))
-        return {n: getattr(st, n) for n, _ in Stats._fields_ if n != "pad"}
+        return {n: getattr(st, n) for n, _ in Stats._fields_}
 
     def sync(self):
         _check(self.lib, self.lib.cadmas_sync(self.h))

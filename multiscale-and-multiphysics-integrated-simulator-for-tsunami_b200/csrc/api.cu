@@ -132,6 +132,13 @@ struct cadmas_handle {
   SkewGeo q;
   SkewSys S;
   double *tt_sl = nullptr, *bb_sl = nullptr;
+  // FP32 system and inner-solve vectors of the mixed solver (solver 1)
+  SkewSysF Sf{nullptr, nullptr};
+  float *bf = nullptr, *xf = nullptr, *r0f = nullptr, *rrf = nullptr, *pvf = nullptr, *apf = nullptr,
+        *aef = nullptr, *ttf = nullptr, *y2f = nullptr;
+  long long mixed_outer = 0, mixed_fallback = 0;  // refinement passes and FP64 fallbacks so far
+  int warm_now = 0;  // the next solve starts from the previous solution (warm_start 1)
+  bool have_prev = false;  // xw holds a converged solution of an earlier step
   size_t nsl = 0;        // entries of a skewed vector
   long long nslab = 0;   // slabs (dot-product rows) of a skewed vector
   SolveState *st = nullptr;
@@ -292,7 +299,7 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
   const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
   TB(CADMAS_STAGE_DCMP);
-  launch_to_skew(s, g, q, a, indc, S, x0, h->bb_sl, h->xw);
+  launch_to_skew(s, g, q, a, indc, S, x0, h->bb_sl, h->xw, h->warm_now);
   launch_dcmp(s, g, q, U, S, &st->pivot_bad);
   launch_pivot_check(s, st);
   TE();
@@ -358,6 +365,145 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   if (iter > 0) h->last_iter = iter;
   if (iter == -1) { bnorm = 0.0; xnorm = 0.0; }
   else { bnorm = std::sqrt(hs.bnorm); xnorm = std::sqrt(hs.xnorm); }
+  return CADMAS_OK;
+}
+
+// ------------------------------------------------ mixed-precision solver
+// One FP32 MILU-BiCGSTAB solve of A d = bf from d = 0 (the iteration of
+// VF_M1BCGS, vf_m1bcgs.f:76-266, on the FP32 copy of the system), to the
+// reference's criterion |M^-1 r| <= eps |M^-1 bf|.  Returns the
+// iteration count in `iter` with VF_M1BCGS's meaning (-1 factor failed,
+// -2 diverged, > icgmax not converged).
+static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
+  cudaStream_t s = h->s;
+  const Geo &g = h->g;
+  const SkewGeo &q = h->q;
+  const SkewSysF &S = h->Sf;
+  const int *ic = S.indc;
+  const long long nr = h->nslab;
+  SolveState *st = h->st;
+  const double epsa2 = h->P.cgepsa * h->P.cgepsa, epsr2 = eps * eps, div2 = h->P.cgdiv * h->P.cgdiv;
+  const int icgmax = h->P.icgmax;
+  const size_t vb = h->nsl * sizeof(float);
+  float *zl[] = {h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef};
+  for (float *z : zl) CK(cudaMemsetAsync(z, 0, vb, s));
+  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  // YY = MINV*BB, BNORM = (YY,YY); with XW = 0, R0 = YY and S = BNORM
+  TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, h->bf, nullptr, h->ttf, st, h->y2f); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->ttf, h->r0f, st); TE();
+  TB(CADMAS_STAGE_DOT);
+  launch_dot_t<float>(s, q, ic, h->r0f, h->r0f, nullptr, nullptr, h->rb0, nullptr, st);
+  launch_fin(s, FIN_BNORM, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+  launch_fin(s, FIN_START, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+  TE();
+  TB(CADMAS_STAGE_VEC); launch_copy2_t<float>(s, q, ic, h->r0f, h->rrf, h->pvf, st); TE();
+  int batch = std::max(2, std::min(h->last_iter, 64));
+  for (int guard = 0; guard < 100000; ++guard) {
+    for (int b = 0; b < batch; ++b) {
+      TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->pvf, h->ttf, st, h->y2f); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->ttf, h->apf, st); TE();
+      TB(CADMAS_STAGE_DOT);
+      launch_dot_t<float>(s, q, ic, h->r0f, h->apf, nullptr, nullptr, h->rb0, nullptr, st);
+      launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      TE();
+      TB(CADMAS_STAGE_VEC); launch_axpy_rr_t<float>(s, q, ic, h->apf, h->rrf, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->rrf, h->ttf, st, h->y2f); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->ttf, h->aef, st); TE();
+      TB(CADMAS_STAGE_DOT);
+      launch_dot_t<float>(s, q, ic, h->rrf, h->aef, h->aef, h->aef, h->rb0, h->rb1, st);
+      launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      TE();
+      TB(CADMAS_STAGE_VEC);
+      launch_upd_xr_t<float>(s, q, ic, h->pvf, h->aef, h->r0f, h->xf, h->rrf, h->rb0, h->rb1, st);
+      launch_fin(s, FIN_CONV, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      launch_upd_p_t<float>(s, q, ic, h->rrf, h->apf, h->pvf, st);
+      TE();
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_st, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_st->timeout) {
+      g_last_error = "a bulk-copy wait of the MILU sweep ran out of time";
+      return CADMAS_ETIMEOUT;
+    }
+    if (h->h_st->done) break;
+    batch = 4;
+  }
+  iter = h->h_st->iter;
+  return CADMAS_OK;
+}
+
+// Mixed-precision solve of A x = b (solver 1): FP32 MILU factor and FP32
+// inner BiCGSTAB solves of A d = r / |r| under FP64 iterative refinement,
+// x += |r| d, with r = b - A x and its norm in FP64, until
+// |b - A x| <= CGEPSR |b|.  A failed FP32 factor or inner solve hands the
+// system to the FP64 solve.  iter = inner iterations of all passes.
+static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc, int &iter,
+                 double &bnorm, double &xnorm);
+static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc, int &iter,
+                       double &bnorm, double &xnorm) {
+  cudaStream_t s = h->s;
+  const Geo &g = h->g;
+  const SkewGeo &q = h->q;
+  const int *ic = h->S.indc;
+  const long long nr = h->nslab;
+  SolveState *st = h->st;
+  h->Sf.indc = h->S.indc;
+  const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
+  TB(CADMAS_STAGE_DCMP);
+  launch_to_skew(s, g, q, a, indc, h->S, x0, h->bb_sl, h->xw, h->warm_now);
+  launch_sys_to_f(s, q, h->S.sys, h->Sf.sys);
+  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  launch_dcmp_f(s, g, q, U, h->Sf, &st->pivot_bad);
+  TE();
+  CK(cudaMemcpyAsync(h->h_st, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (h->h_st->pivot_bad) { h->mixed_fallback++; return solve(h, a, x0, indc, iter, bnorm, xnorm); }
+  const double tol2 = h->P.cgepsr * h->P.cgepsr;
+  int total = 0;
+  bool converged = false;
+  double b2 = 0.0, r2 = 0.0;
+  for (int outer = 0; outer < 40; ++outer) {
+    // r = b - A x and the two norms in FP64
+    CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+    TB(CADMAS_STAGE_VEC);
+    launch_spmv(s, g, q, h->S, h->xw, h->y2, st);
+    launch_bmy(s, q, ic, h->bb_sl, h->y2, st);
+    TE();
+    TB(CADMAS_STAGE_DOT);
+    launch_dot(s, q, ic, h->bb_sl, h->bb_sl, h->y2, h->y2, h->rb0, h->rb1, st);
+    launch_fin(s, FIN_STORE, h->rb0, h->rb1, nr, st, h->dres + 6, 0, 0, 0, 0);
+    TE();
+    CK(cudaMemcpyAsync(h->h_res + 6, h->dres + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    b2 = h->h_res[6];
+    r2 = h->h_res[7];
+    h->mixed_outer++;
+    if (r2 <= tol2 * b2) { converged = true; break; }
+    const double rn = std::sqrt(r2);
+    launch_scale_to_f(s, q, ic, h->y2, 1.0 / rn, h->bf);
+    // each pass reduces the residual by about the inner tolerance
+    int it = 0;
+    int rc = solve_inner_f(h, 1.0e-5, it);
+    if (rc) return rc;
+    if (it < 0 || it > h->P.icgmax) {  // factor, divergence or cap: FP64 takes over
+      h->mixed_fallback++;
+      return solve(h, a, x0, indc, iter, bnorm, xnorm);
+    }
+    total += it;
+    launch_add_f(s, q, ic, h->xf, rn, h->xw);
+  }
+  if (!converged) {
+    h->mixed_fallback++;
+    return solve(h, a, x0, indc, iter, bnorm, xnorm);
+  }
+  // X0 = XW on INDC != -1 (k_x0 requires ITER >= 0: the state is clear)
+  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  launch_x0(s, g, q, ic, h->xw, x0, st);
+  CK(cudaGetLastError());
+  iter = total;
+  bnorm = std::sqrt(b2);
+  xnorm = std::sqrt(r2);
   return CADMAS_OK;
 }
 
@@ -436,12 +582,16 @@ static int do_v1cal(cadmas_handle *h) {
   CK(cudaMemsetAsync(PT, 0, h->N * sizeof(double), s));
   int iter;
   double bn, xn;
-  int rc = solve(h, a, PT, h->indc, iter, bn, xn);
+  const bool mixed = (h->P.solver == 1);
+  h->warm_now = (h->P.warm_start == 1 && h->have_prev) ? 1 : 0;
+  int rc = mixed ? solve_mixed(h, a, PT, h->indc, iter, bn, xn) : solve(h, a, PT, h->indc, iter, bn, xn);
+  h->warm_now = 0;
   if (rc) return rc;
+  h->have_prev = (iter >= 0);
   h->stats.icgitr = iter;
   h->stats.cgbnrm = bn;
   h->stats.cgxnrm = xn;
-  rc = map_iter(iter, h->P.icgmax);
+  rc = mixed ? (iter < 0 ? map_iter(iter, h->P.icgmax) : CADMAS_OK) : map_iter(iter, h->P.icgmax);
   if (rc) return rc;
   if (h->P.diag_relres) {
     launch_relres(s, h->g, h->q, h->S, h->bb_sl, h->xw, h->rb0, h->rb1);
@@ -603,7 +753,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
   AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
   for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
-  h->q.TI = TI; h->q.TJ = TJ; h->q.TIp = TI + (TI & 1); h->q.T = h->q.TIp * TJ;
+  h->q.TI = TI; h->q.TJ = TJ; h->q.TIp = (TI + 3) & ~3; h->q.T = h->q.TIp * TJ;
   h->q.W = (d->numk - 2) + (TI - 1) + (TJ - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJ - 1) / TJ);
@@ -619,6 +769,17 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
     AL(h->S.indc, nsl); AL(h->tt_sl, nsl); AL(h->bb_sl, nsl);
     AL(h->xw, nsl); AL(h->y2, nsl); AL(h->r0, nsl); AL(h->rr, nsl);
     AL(h->pv, nsl); AL(h->ap, nsl); AL(h->ae, nsl);
+    if (p->solver == 1) {
+      if (!sweep_supported_f(h->q)) {
+        g_last_error = "preconditioner block too large for the FP32 sweeps; set precond_ti/precond_tj";
+        rc = rc ? rc : CADMAS_EUNSUPPORTED;
+      }
+      AL(h->Sf.sys, (size_t)SYS_N * nsl);
+      AL(h->bf, nsl); AL(h->xf, nsl); AL(h->r0f, nsl); AL(h->rrf, nsl); AL(h->pvf, nsl);
+      AL(h->apf, nsl); AL(h->aef, nsl); AL(h->ttf, nsl); AL(h->y2f, nsl);
+    } else if (p->solver != 0) {
+      rc = rc ? rc : CADMAS_EINVAL;
+    }
   }
   AL(h->rb0, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->rb1, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->dres, 8);
   AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
@@ -659,6 +820,8 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_int) cudaFreeHost(h->h_int);
   if (h->h_res) cudaFreeHost(h->h_res);
   for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
+  for (float *q : {h->Sf.sys, h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->ttf, h->y2f})
+    if (q) cudaFree(q);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
   return CADMAS_OK;
@@ -900,6 +1063,7 @@ int cadmas_divnorm(cadmas_handle *h, double *val) {
 
 int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st) {
   if (!h || !st) return CADMAS_EINVAL;
+  h->stats.fallbacks = (int)h->mixed_fallback;
   *st = h->stats;
   return CADMAS_OK;
 }

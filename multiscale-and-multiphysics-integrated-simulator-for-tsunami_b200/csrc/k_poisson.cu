@@ -172,27 +172,32 @@ template <int N> __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Ring layout in dynamic shared memory: double r[R][NV][T], int ri[R][T],
-// then the exchange buffers double xb[2][T].
-template <int NV> struct Ring {
-  double *r;
+template <typename V> __device__ __forceinline__ void cp_async_v(V *smem, const V *gmem) {
+  if (sizeof(V) == 8) cp_async8(smem, gmem);
+  else cp_async4(smem, gmem);
+}
+
+// Ring layout in dynamic shared memory: V r[R][NV][T], then the exchange
+// buffers V xb[2][T], then int ri[R][T].
+template <int NV, typename V> struct Ring {
+  V *r;
   int *ri;
-  double *xb;
+  V *xb;
   int T, R;
-  __device__ __forceinline__ double &v(int slot, int q, int t) const { return r[((slot * NV) + q) * T + t]; }
+  __device__ __forceinline__ V &v(int slot, int q, int t) const { return r[((slot * NV) + q) * T + t]; }
   __device__ __forceinline__ int &ind(int slot, int t) const { return ri[slot * T + t]; }
 };
-template <int NV> __device__ __forceinline__ Ring<NV> ring_setup(int T, int R) {
-  extern __shared__ double sm[];
-  Ring<NV> g;
+template <int NV, typename V> __device__ __forceinline__ Ring<NV, V> ring_setup(int T, int R) {
+  extern __shared__ __align__(16) double sm[];
+  Ring<NV, V> g;
   g.T = T; g.R = R;
-  g.r = sm;
-  g.xb = sm + (size_t)R * NV * T;
+  g.r = reinterpret_cast<V *>(sm);
+  g.xb = g.r + (size_t)R * NV * T;
   g.ri = (int *)(g.xb + 2 * T);
   return g;
 }
-inline size_t ring_bytes(int NV, int T, int R) {
-  return (size_t)R * NV * T * sizeof(double) + 2 * (size_t)T * sizeof(double) + (size_t)R * T * sizeof(int);
+inline size_t ring_bytes(int NV, int T, int R, size_t es = sizeof(double)) {
+  return (size_t)R * NV * T * es + 2 * (size_t)T * es + (size_t)R * T * sizeof(int);
 }
 
 // ----------------------------------------------------- tile-skewed layout
@@ -209,9 +214,11 @@ __device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, in
 
 // Copy the Poisson system (7 coefficients, interleaved per slab; DD set to
 // 0 for MZDCMP to fill), INDC, BB and X0 into the skewed layout.  Entries
-// outside the tile or the interior get 0 (INDC -1).
+// outside the tile or the interior get 0 (INDC -1).  warm: keep the
+// previous solution already in xsl as the initial guess (0 where INDC is
+// now -1) instead of X0.
 __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
-                          double *bsl, double *xsl) {
+                          double *bsl, double *xsl, int warm) {
   const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int t = (int)(e % q.T);
@@ -227,7 +234,7 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
       v[4] = A_.aui[c]; v[5] = A_.auj[c]; v[6] = A_.auk[c];
       ic = INDC[c];
       bv = A_.bb[c];
-      xv = X0[c];
+      xv = warm ? (ic != -1 ? xsl[e] : 0.0) : X0[c];
     }
     for (int c = 0; c < 7; ++c) S.sys[sys_at(bw, c, q.T, t)] = v[c];
     S.sys[sys_at(bw, SYS_DD, q.T, t)] = 0.0;
@@ -264,11 +271,11 @@ __device__ __forceinline__ void skew_fetch(double *dst, const Geo &g, const Skew
 // ------------------------------------------------------------ VF_MZDCMP
 // ring values: 0 AD, 1 ALI, 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK; DD is
 // written in the skewed layout.
-template <int D>
-__global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
+template <int D, typename V>
+__global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
   constexpr int NV = 7, R = D + 3;
   const int TIp = q.TIp, T = q.T;
-  Ring<NV> rg = ring_setup<NV>(T, R);
+  Ring<NV, V> rg = ring_setup<NV, V>(T, R);
   TileGeo t = tile_geo(g, q);
   const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
@@ -276,17 +283,18 @@ __global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
     const int k = 2 + s - t.ti - t.tj;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
       const long long slab = (long long)b * q.W + s, e = slab * T + tid;
-      const double *sy = S.sys + sys_at(slab, 0, T, tid);
+      const V *sy = S.sys + sys_at(slab, 0, T, tid);
       const int sl = s % R;
 #pragma unroll
-      for (int c = 0; c < 7; ++c) cp_async8(&rg.v(sl, c, tid), sy + (long long)c * T);
+      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)c * T);
       cp_async4(&rg.ind(sl, tid), S.indc + e);
     }
     cp_commit();
   };
 #pragma unroll 1
   for (int s = 0; s < D; ++s) prefetch(s);
-  double dk1 = 0.0, au3 = 0.0;  // DD(i,j,k-1) and AU3 of (i,j,k-1); k-1 = 1 is the zero ghost layer
+  V dk1 = V(0), au3 = V(0);  // DD(i,j,k-1) and AU3 of (i,j,k-1); k-1 = 1 is the zero ghost layer
+  const V z = V(0), one = V(1);
   bool bad = false;
   for (int s = 0; s < nsteps; ++s) {
     prefetch(s + D);
@@ -295,24 +303,24 @@ __global__ void k_dcmp(Geo g, SkewGeo q, double U, SkewSys S, int *pivot_bad) {
     const int k = 2 + s - t.ti - t.tj;
     const int sl = s % R, slp = (s + R - 1) % R, cur = s & 1, prv = cur ^ 1;
     if (t.valid && k >= 2 && k <= g.NK - 1) {
-      double dd = 0.0;
+      V dd = z;
       if (rg.ind(sl, tid) != -1) {
-        double d1 = 0.0, a1, d2 = 0.0, a2;
+        V d1 = z, a1, d2 = z, a2;
         if (t.ti > 0) {
           d1 = rg.xb[prv * T + tid - 1];
           a1 = rg.v(slp, 4, tid - 1) + U * (rg.v(slp, 5, tid - 1) + rg.v(slp, 6, tid - 1));
         } else {
-          a1 = 0.0 + U * (0.0 + 0.0);
+          a1 = z + U * (z + z);
         }
         if (t.tj > 0) {
           d2 = rg.xb[prv * T + tid - TIp];
           a2 = rg.v(slp, 5, tid - TIp) + U * (rg.v(slp, 4, tid - TIp) + rg.v(slp, 6, tid - TIp));
         } else {
-          a2 = 0.0 + U * (0.0 + 0.0);
+          a2 = z + U * (z + z);
         }
-        dd = 1.0 / (rg.v(sl, 0, tid) - rg.v(sl, 1, tid) * d1 * a1 - rg.v(sl, 2, tid) * d2 * a2 -
+        dd = one / (rg.v(sl, 0, tid) - rg.v(sl, 1, tid) * d1 * a1 - rg.v(sl, 2, tid) * d2 * a2 -
                     rg.v(sl, 3, tid) * dk1 * au3);
-        if (dd <= 0.0) bad = true;
+        if (dd <= z) bad = true;
       }
       S.sys[sys_at((long long)b * q.W + s, SYS_DD, T, tid)] = dd;
       rg.xb[cur * T + tid] = dd;
@@ -406,19 +414,20 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
 // and their evaluation order are those of the reference loops, so the
 // results do not change.  The step loop is unrolled by the ring length so
 // slot addresses and mbarrier phases are constants.
-template <int D, int MODE, int MAXT>
+template <int D, int MODE, int MAXT, typename V>
 __global__ void __launch_bounds__(MAXT, 1)
-    k_sweep(Geo g, SkewGeo q, SkewSys S, const double *vin, double *vout, SolveState *st) {
+    k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st) {
   if (st->done) return;
   constexpr int R = D + 2;
   constexpr int AHEAD = (MODE == SWEEP_FWD_AX) ? 2 : 1;  // preparing step s+1 reads the slot of step s+AHEAD
   extern __shared__ __align__(16) double sm[];
   const int T = q.T, TIp = q.TIp;
   const int Tc = (T + 31) & ~31;
-  const int SS = sweep_slot(q, MODE);
+  constexpr int ES = (int)sizeof(V);
+  const int SS = sweep_slot(q, MODE, ES);
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm);
-  double *ring = sm + ((R + 1) & ~1);
-  double *xb = ring + (size_t)R * SS;
+  V *ring = reinterpret_cast<V *>(sm + ((R + 1) & ~1));
+  V *xb = ring + (size_t)R * SS;
   const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
   TileGeo t = tile_geo(g, q);
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
@@ -434,9 +443,9 @@ __global__ void __launch_bounds__(MAXT, 1)
     s_abort[0] = s_abort[1] = 0;
   }
   if (MODE == SWEEP_FWD_AX) {  // halo values of absent neighbours stay 0 (ghost layer)
-    const int nh = 2 * halo_span(q) + 2 * TIp;
+    const int nh = 2 * halo_span(q, ES) + 2 * TIp;
     for (int r = 0; r < R; ++r)
-      for (int i = tid; i < nh; i += blockDim.x) ring[(size_t)r * SS + halo_left(q) + i] = 0.0;
+      for (int i = tid; i < nh; i += blockDim.x) ring[(size_t)r * SS + halo_left(q, ES) + i] = V(0);
   }
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -444,10 +453,10 @@ __global__ void __launch_bounds__(MAXT, 1)
 
   // Producer: lane l issues copy l of every step (at most 6); its fixed
   // part is worked out once here.
-  const double *src0 = nullptr;
+  const V *src0 = nullptr;
   SweepLane l0;
   l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; l0.dst = 0; l0.wstride = 0;  // empty range: no copy
-  if (producer && lane < sweep_ncopy(q, MODE) && sweep_lane(q, MODE, b, lane, l0))
+  if (producer && lane < sweep_ncopy(q, MODE) && sweep_lane(q, MODE, b, lane, l0, ES))
     src0 = (l0.arr == 0 ? S.sys : vin) + l0.base;
   else { l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; }
   const unsigned bar0 = smem_u32(bar), ring0 = smem_u32(ring);
@@ -455,12 +464,12 @@ __global__ void __launch_bounds__(MAXT, 1)
     if (u >= nsteps) return;
     const int w = (MODE == SWEEP_BWD) ? nsteps - 1 - u : u;
     const unsigned bslot = bar0 + 8u * slot;
-    const unsigned dslot = ring0 + 8u * (unsigned)(slot * SS);
+    const unsigned dslot = ring0 + (unsigned)ES * (unsigned)(slot * SS);
     const bool v0 = (w >= l0.dlo && w <= l0.dhi);
     const unsigned bytes = __reduce_add_sync(0xffffffffu, v0 ? l0.bytes : 0);
     if (lane == 0) mbar_expect_tx(bslot, bytes);
     __syncwarp();
-    if (v0) bulk_load(dslot + 8u * l0.dst, src0 + (long long)w * l0.wstride, l0.bytes, bslot);
+    if (v0) bulk_load(dslot + (unsigned)ES * l0.dst, src0 + (long long)w * l0.wstride, l0.bytes, bslot);
   };
   // data of step u sits in slot u % R, phase (u / R) & 1
   auto wait_data = [&](int u, int slot, unsigned parity) -> bool {
@@ -477,47 +486,46 @@ __global__ void __launch_bounds__(MAXT, 1)
   const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
   const int slo = (MODE == SWEEP_BWD) ? ri + rj : t.ti + t.tj, shi = slo + g.NK - 3;
   const bool col = t.valid && !producer;
-  const int lofs = (q.TI - 1) & 1;  // left halo: position of column TI-1 in its pair
-  const int hl = halo_left(q) + TIp * t.tj + lofs, hr = halo_right(q) + TIp * t.tj, hd = halo_down(q) + t.ti,
-            hu = halo_up(q) + t.ti;
-  double *vp = vout + ((long long)b * q.W + (MODE == SWEEP_BWD ? nsteps - 1 : 0)) * T + tid;
+  const int hl = halo_left(q, ES) + TIp * t.tj + halo_lofs(q, ES), hr = halo_right(q, ES) + TIp * t.tj,
+            hd = halo_down(q, ES) + t.ti, hu = halo_up(q, ES) + t.ti;
+  V *vp = vout + ((long long)b * q.W + (MODE == SWEEP_BWD ? nsteps - 1 : 0)) * T + tid;
   const long long vstep = (MODE == SWEEP_BWD) ? -(long long)T : (long long)T;
 
   // Prepared values of the next step.
   bool act = false;             // the column has a cell at this step
-  double dd = 0.0;              // DD of the cell (0: not computed)
-  double y0 = 0.0;              // FWD: Y or A*P;  BWD: T
-  double c1 = 0.0, c2 = 0.0, c3 = 0.0;  // FWD: ALI*DD(i-1), ALJ*DD(j-1), ALK*DD(k-1); BWD: AUI, AUJ, AUK
-  double dk1 = 0.0, pk1 = 0.0;  // DD and P of this column at the previous step (FWD)
-  double xk1 = 0.0;             // result of this column at the previous step
+  V dd = V(0);              // DD of the cell (0: not computed)
+  V y0 = V(0);              // FWD: Y or A*P;  BWD: T
+  V c1 = V(0), c2 = V(0), c3 = V(0);  // FWD: ALI*DD(i-1), ALJ*DD(j-1), ALK*DD(k-1); BWD: AUI, AUJ, AUK
+  V dk1 = V(0), pk1 = V(0);  // DD and P of this column at the previous step (FWD)
+  V xk1 = V(0);             // result of this column at the previous step
   // Prepare step s: cs = slot of s, ps = slot of s-1, ns = slot of s+1.
-  auto prepare = [&](int s, const double *cs, const double *ps, const double *ns) {
+  auto prepare = [&](int s, const V *cs, const V *ps, const V *ns) {
     act = col && s >= slo && s <= shi;
     if (!act) return;
     if (MODE == SWEEP_FWD_AX) {
       const int k = 2 + s - t.ti - t.tj;
-      const double d = cs[7 * T + tid], pc = cs[8 * T + tid];
-      if (d != 0.0) {
-        const double pxm = ex0 ? cs[hl] : ps[8 * T + tid - 1];
-        const double pym = ey0 ? cs[hd] : ps[8 * T + tid - TIp];
-        const double pzm = (k > 2) ? pk1 : 0.0;
-        const double pxp = ex1 ? cs[hr] : ns[8 * T + tid + 1];
-        const double pyp = ey1 ? cs[hu] : ns[8 * T + tid + TIp];
-        const double pzp = (k < g.NK - 1) ? ns[8 * T + tid] : 0.0;
+      const V d = cs[7 * T + tid], pc = cs[8 * T + tid];
+      if (d != V(0)) {
+        const V pxm = ex0 ? cs[hl] : ps[8 * T + tid - 1];
+        const V pym = ey0 ? cs[hd] : ps[8 * T + tid - TIp];
+        const V pzm = (k > 2) ? pk1 : V(0);
+        const V pxp = ex1 ? cs[hr] : ns[8 * T + tid + 1];
+        const V pyp = ey1 ? cs[hu] : ns[8 * T + tid + TIp];
+        const V pzp = (k < g.NK - 1) ? ns[8 * T + tid] : V(0);
         y0 = cs[tid] * pc + cs[T + tid] * pxm + cs[2 * T + tid] * pym + cs[3 * T + tid] * pzm +
              cs[4 * T + tid] * pxp + cs[5 * T + tid] * pyp + cs[6 * T + tid] * pzp;
-        const double d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : 0.0;
-        const double d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : 0.0;
+        const V d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : V(0);
+        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : V(0);
         c1 = cs[T + tid] * d1;
         c2 = cs[2 * T + tid] * d2;
         c3 = cs[3 * T + tid] * dk1;
       }
       dd = d; dk1 = d; pk1 = pc;
     } else if (MODE == SWEEP_FWD) {
-      const double d = cs[7 * T + tid];
-      if (d != 0.0) {
-        const double d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : 0.0;
-        const double d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : 0.0;
+      const V d = cs[7 * T + tid];
+      if (d != V(0)) {
+        const V d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : V(0);
+        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : V(0);
         y0 = cs[tid];
         c1 = cs[T + tid] * d1;
         c2 = cs[2 * T + tid] * d2;
@@ -526,10 +534,10 @@ __global__ void __launch_bounds__(MAXT, 1)
       dd = d; dk1 = d;
     } else {
       dd = cs[4 * T + tid];
-      if (dd != 0.0) { y0 = cs[tid]; c1 = cs[T + tid]; c2 = cs[2 * T + tid]; c3 = cs[3 * T + tid]; }
+      if (dd != V(0)) { y0 = cs[tid]; c1 = cs[T + tid]; c2 = cs[2 * T + tid]; c3 = cs[3 * T + tid]; }
     }
   };
-  auto slot_ptr = [&](int r) -> const double * { return ring + (size_t)r * SS; };
+  auto slot_ptr = [&](int r) -> const V * { return ring + (size_t)r * SS; };
 
   bool ok = true;
   if (!producer) {
@@ -558,15 +566,15 @@ __global__ void __launch_bounds__(MAXT, 1)
         // the recurrence of step s
         if (act && ok) {
           const int cur = (s & 1) * T, prv = T - cur;
-          double x = 0.0;
-          if (dd != 0.0) {
+          V x = V(0);
+          if (dd != V(0)) {
             if (MODE == SWEEP_BWD) {
-              const double x1 = (ri > 0) ? xb[prv + tid + 1] : 0.0;
-              const double x2 = (rj > 0) ? xb[prv + tid + TIp] : 0.0;
+              const V x1 = (ri > 0) ? xb[prv + tid + 1] : V(0);
+              const V x2 = (rj > 0) ? xb[prv + tid + TIp] : V(0);
               x = (y0 - c1 * x1 - c2 * x2 - c3 * xk1) * dd;
             } else {
-              const double x1 = (t.ti > 0) ? xb[prv + tid - 1] : 0.0;
-              const double x2 = (t.tj > 0) ? xb[prv + tid - TIp] : 0.0;
+              const V x1 = (t.ti > 0) ? xb[prv + tid - 1] : V(0);
+              const V x2 = (t.tj > 0) ? xb[prv + tid - TIp] : V(0);
               x = y0 - c1 * x1 - c2 * x2 - c3 * xk1;
             }
           }
@@ -619,24 +627,27 @@ __device__ __forceinline__ bool interior(const Geo &g, int I, int J, int K) {
 }
 
 // A*X at skewed entry e (VF_MZAX expression, vf_mzax.f:46-53).
-__device__ __forceinline__ double skew_ax(const Geo &g, const SkewGeo &q, const SkewSys &S, const double *X,
-                                          long long e) {
+template <typename V>
+__device__ __forceinline__ V skew_ax(const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *X,
+                                     long long e) {
   const int t = (int)(e % q.T);
   const long long bw = e / q.T;
   const int w = (int)(bw % q.W), b = (int)(bw / q.W);
   const int ti = t % q.TIp, tj = t / q.TIp, bx = b % q.ntx, by = b / q.ntx, k = 2 + w - ti - tj;
-  const double *a = S.sys + sys_at(bw, 0, q.T, t);
+  const V *a = S.sys + sys_at(bw, 0, q.T, t);
   const long long T = q.T;
-  return a[SYS_AD * T] * X[e] + a[SYS_ALI * T] * skew_at(g, q, X, bx, by, ti - 1, tj, k) +
-         a[SYS_ALJ * T] * skew_at(g, q, X, bx, by, ti, tj - 1, k) +
-         a[SYS_ALK * T] * skew_at(g, q, X, bx, by, ti, tj, k - 1) +
-         a[SYS_AUI * T] * skew_at(g, q, X, bx, by, ti + 1, tj, k) +
-         a[SYS_AUJ * T] * skew_at(g, q, X, bx, by, ti, tj + 1, k) +
-         a[SYS_AUK * T] * skew_at(g, q, X, bx, by, ti, tj, k + 1);
+  auto at = [&](int di, int dj, int dk) -> V {
+    const long long n = skew_nb(g, q, bx, by, ti + di, tj + dj, k + dk);
+    return n < 0 ? V(0) : X[n];
+  };
+  return a[SYS_AD * T] * X[e] + a[SYS_ALI * T] * at(-1, 0, 0) + a[SYS_ALJ * T] * at(0, -1, 0) +
+         a[SYS_ALK * T] * at(0, 0, -1) + a[SYS_AUI * T] * at(1, 0, 0) + a[SYS_AUJ * T] * at(0, 1, 0) +
+         a[SYS_AUK * T] * at(0, 0, 1);
 }
 
 // Y = A X on INDC != -1 (VF_MZAX); Y untouched elsewhere.
-__global__ void k_spmv(Geo g, SkewGeo q, SkewSys S, const double *X, double *Y, const SolveState *st) {
+template <typename V>
+__global__ void k_spmv(Geo g, SkewGeo q, SkewSysT<V> S, const V *X, V *Y, const SolveState *st) {
   if (st && st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (S.indc[e] != -1) Y[e] = skew_ax(g, q, S, X, e);
@@ -645,22 +656,28 @@ __global__ void k_spmv(Geo g, SkewGeo q, SkewSys S, const double *X, double *Y, 
 
 // Y = B - Y on INDC != -1 (vf_m1bcgs.f:124-132)
 __global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, const SolveState *st) {
-  if (st->done) return;
+  if (st && st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) Y[e] = B[e] - Y[e];
   SLAB_LOOP_END
 }
 
+// The BiCGSTAB vector kernels below serve the FP64 solve (V = double) and
+// the FP32 inner solves of the mixed solver (V = float).  With float
+// vectors the arithmetic runs in double (the scalars are double) and is
+// rounded once on the store; dot products always accumulate in double.
+
 // Slab partials of up to two dot products (VF_MZIP).
-__global__ void k_dot(SkewGeo q, const int *INDC, const double *x0, const double *y0, const double *x1,
-                      const double *y1, double *rb0, double *rb1, const SolveState *st) {
+template <typename V>
+__global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, const V *x1, const V *y1,
+                      double *rb0, double *rb1, const SolveState *st) {
   if (st && st->done) return;
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) {
-    s0 = s0 + x0[e] * y0[e];
-    if (x1) s1 = s1 + x1[e] * y1[e];
+    s0 = s0 + (double)x0[e] * (double)y0[e];
+    if (x1) s1 = s1 + (double)x1[e] * (double)y1[e];
   }
   SLAB_LOOP_END
   row_store(s0, rb0, SLAB_ROW, nslab);
@@ -668,8 +685,8 @@ __global__ void k_dot(SkewGeo q, const int *INDC, const double *x0, const double
 }
 
 // RR = R0, PP = R0
-__global__ void k_copy2(SkewGeo q, const int *INDC, const double *R0, double *RR, double *PP,
-                        const SolveState *st) {
+template <typename V>
+__global__ void k_copy2(SkewGeo q, const int *INDC, const V *R0, V *RR, V *PP, const SolveState *st) {
   if (st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) { RR[e] = R0[e]; PP[e] = R0[e]; }
@@ -677,29 +694,31 @@ __global__ void k_copy2(SkewGeo q, const int *INDC, const double *R0, double *RR
 }
 
 // RR = RR - ALPHA*AP (vf_m1bcgs.f:181-189)
-__global__ void k_axpy_rr(SkewGeo q, const int *INDC, const double *AP, double *RR, const SolveState *st) {
+template <typename V>
+__global__ void k_axpy_rr(SkewGeo q, const int *INDC, const V *AP, V *RR, const SolveState *st) {
   if (st->done) return;
   const double alpha = st->alpha;
   SLAB_LOOP_BEGIN(q)
-  if (INDC[e] != -1) RR[e] = RR[e] - alpha * AP[e];
+  if (INDC[e] != -1) RR[e] = (V)(RR[e] - alpha * AP[e]);
   SLAB_LOOP_END
 }
 
 // XW = XW + (ALPHA*PP + OMEGA*RR); RR = RR - OMEGA*AE; slab partials of
 // (RR,RR) and (R0,RR) on the updated RR (vf_m1bcgs.f:206-225).
-__global__ void k_upd_xr(SkewGeo q, const int *INDC, const double *PP, const double *AE, const double *R0,
-                         double *XW, double *RR, double *rb0, double *rb1, const SolveState *st) {
+template <typename V>
+__global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, const V *R0, V *XW, V *RR,
+                         double *rb0, double *rb1, const SolveState *st) {
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) {
-    XW[e] = XW[e] + (alpha * PP[e] + omega * RR[e]);
-    double r = RR[e] - omega * AE[e];
+    XW[e] = (V)(XW[e] + (alpha * PP[e] + omega * RR[e]));
+    const V r = (V)(RR[e] - omega * AE[e]);
     RR[e] = r;
-    s0 = s0 + r * r;
-    s1 = s1 + R0[e] * r;
+    s0 = s0 + (double)r * (double)r;
+    s1 = s1 + (double)R0[e] * (double)r;
   }
   SLAB_LOOP_END
   row_store(s0, rb0, SLAB_ROW, nslab);
@@ -707,12 +726,36 @@ __global__ void k_upd_xr(SkewGeo q, const int *INDC, const double *PP, const dou
 }
 
 // PP = RR + BETA*(PP - OMEGA*AP) (vf_m1bcgs.f:229-238)
-__global__ void k_upd_p(SkewGeo q, const int *INDC, const double *RR, const double *AP, double *PP,
-                        const SolveState *st) {
+template <typename V>
+__global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V *PP, const SolveState *st) {
   if (st->done) return;
   const double beta = st->beta, omega = st->omega;
   SLAB_LOOP_BEGIN(q)
-  if (INDC[e] != -1) PP[e] = RR[e] + beta * (PP[e] - omega * AP[e]);
+  if (INDC[e] != -1) PP[e] = (V)(RR[e] + beta * (PP[e] - omega * AP[e]));
+  SLAB_LOOP_END
+}
+
+// ------------------------------------------- mixed-precision conversions
+// FP32 copy of the 7 coefficients (DD comes from the FP32 factorisation).
+__global__ void k_sys_to_f(SkewGeo q, const double *sys, float *sysf) {
+  const long long n = (long long)q.nb * q.W * q.T;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long slab = e / q.T;
+    const int t = (int)(e - slab * q.T);
+#pragma unroll
+    for (int c = 0; c < SYS_DD; ++c) sysf[sys_at(slab, c, q.T, t)] = (float)sys[sys_at(slab, c, q.T, t)];
+  }
+}
+// RF = R * scale on INDC != -1 (the right-hand side of an inner solve)
+__global__ void k_scale_to_f(SkewGeo q, const int *INDC, const double *R, double scale, float *RF) {
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) RF[e] = (float)(R[e] * scale);
+  SLAB_LOOP_END
+}
+// X = X + D * inv_scale on INDC != -1 (the correction of an inner solve)
+__global__ void k_add_f(SkewGeo q, const int *INDC, const float *D, double inv_scale, double *X) {
+  SLAB_LOOP_BEGIN(q)
+  if (INDC[e] != -1) X[e] = X[e] + (double)D[e] * inv_scale;
   SLAB_LOOP_END
 }
 
@@ -865,10 +908,10 @@ void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
 }
 // Prefetch depth: the largest of 8, 4, 2, 1 whose ring fits the shared
 // memory a block may use (200 KB here).
-static int ring_depth(int NV, int T) {
+static int ring_depth(int NV, int T, size_t es) {
   const size_t cap = 200 * 1024;
   for (int d : {8, 4, 2, 1})
-    if (ring_bytes(NV, T, d + 3) <= cap) return d;
+    if (ring_bytes(NV, T, d + 3, es) <= cap) return d;
   return 0;
 }
 template <class K> static void set_smem(K kern, size_t bytes) {
@@ -876,49 +919,55 @@ template <class K> static void set_smem(K kern, size_t bytes) {
 }
 
 static inline dim3 skew_grid(const SkewGeo &q) { return dim3((unsigned)q.ntx, (unsigned)(q.nb / q.ntx)); }
-#define RING_LAUNCH2(KER, NV, ...)                                                             \
-  do {                                                                                        \
-    const int T_ = q.T, d_ = ring_depth(NV, T_);                                              \
-    const size_t b_ = ring_bytes(NV, T_, d_ + 3);                                             \
-    switch (d_) {                                                                             \
-      case 8: set_smem(KER<8 RING_EXTRA>, b_); KER<8 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
-      case 4: set_smem(KER<4 RING_EXTRA>, b_); KER<4 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
-      case 2: set_smem(KER<2 RING_EXTRA>, b_); KER<2 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
-      default: set_smem(KER<1 RING_EXTRA>, b_); KER<1 RING_EXTRA><<<skew_grid(q), T_, b_, s>>>(__VA_ARGS__); break; \
-    }                                                                                         \
-    count_launch();                                                                           \
-  } while (0)
 
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
-                    const SkewSys &S, const double *x0, double *bsl, double *xsl) {
+                    const SkewSys &S, const double *x0, double *bsl, double *xsl, int warm) {
   const long long n = (long long)q.nb * q.W * q.T;
   const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-  k_to_skew<<<blocks, 256, 0, s>>>(g, q, a, indc, S, x0, bsl, xsl);
+  k_to_skew<<<blocks, 256, 0, s>>>(g, q, a, indc, S, x0, bsl, xsl, warm);
+  count_launch();
+}
+template <typename V>
+static void launch_dcmp_t(cudaStream_t s, const Geo &g, const SkewGeo &q, V U, const SkewSysT<V> &S, int *pivot_bad) {
+  const int T = q.T, d = ring_depth(7, T, sizeof(V));
+  const size_t bytes = ring_bytes(7, T, d + 3, sizeof(V));
+  switch (d) {
+#define DCMP_CASE(DD)                                                                    \
+  case DD:                                                                               \
+    set_smem(k_dcmp<DD, V>, bytes);                                                      \
+    k_dcmp<DD, V><<<skew_grid(q), T, bytes, s>>>(g, q, U, S, pivot_bad);                 \
+    break;
+    DCMP_CASE(8) DCMP_CASE(4) DCMP_CASE(2)
+    default: DCMP_CASE(1)
+#undef DCMP_CASE
+  }
   count_launch();
 }
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad) {
-#define RING_EXTRA
-  RING_LAUNCH2(k_dcmp, 7, g, q, U, S, pivot_bad);
-#undef RING_EXTRA
+  launch_dcmp_t<double>(s, g, q, U, S, pivot_bad);
+}
+void launch_dcmp_f(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSysF &S, int *pivot_bad) {
+  launch_dcmp_t<float>(s, g, q, (float)U, S, pivot_bad);
 }
 // Sweeps: prefetch depth D in {8, 6, 4, 3, 2}, the largest whose ring
 // (R = D+2 slots, mbarriers, exchange buffers) fits the 227 KB of shared
 // memory a block may use.
-static size_t sweep_bytes(const SkewGeo &q, int mode, int D) {
+static size_t sweep_bytes(const SkewGeo &q, int mode, int D, int es) {
   const int R = D + 2;
-  return (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode) * 8 + 2 * (size_t)q.T * 8;
+  return (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode, es) * es + 2 * (size_t)q.T * es;
 }
-static int sweep_depth(const SkewGeo &q, int mode) {
+static int sweep_depth(const SkewGeo &q, int mode, int es) {
   if (sweep_threads(q.T) > 1024) return 0;
   for (int d : {8, 6, 4, 3, 2})
-    if (sweep_bytes(q, mode, d) <= 227 * 1024) return d;
+    if (sweep_bytes(q, mode, d, es) <= 227 * 1024) return d;
   return 0;
 }
-template <int MODE>
-static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *vin,
-                         double *vout, SolveState *st) {
-  const int d = sweep_depth(q, MODE);
-  const size_t bytes = sweep_bytes(q, MODE, d);
+template <int MODE, typename V>
+static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *vin,
+                         V *vout, SolveState *st) {
+  constexpr int ES = (int)sizeof(V);
+  const int d = sweep_depth(q, MODE, ES);
+  const size_t bytes = sweep_bytes(q, MODE, d, ES);
   const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
   // The register budget follows the block size (255, 128 or 64 registers
   // for blocks of up to 256, 512 or 1024 threads).
@@ -927,8 +976,8 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   switch (d * 4096 + mt) {
 #define SWEEP_CASE(DD, MT)                                                              \
   case DD * 4096 + MT:                                                                  \
-    set_smem(k_sweep<DD, MODE, MT>, bytes);                                             \
-    k_sweep<DD, MODE, MT><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);           \
+    set_smem(k_sweep<DD, MODE, MT, V>, bytes);                                          \
+    k_sweep<DD, MODE, MT, V><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);        \
     break;
     SWEEP_CASE(8, 256) SWEEP_CASE(6, 256) SWEEP_CASE(4, 256) SWEEP_CASE(3, 256) SWEEP_CASE(2, 256)
     SWEEP_CASE(8, 512) SWEEP_CASE(6, 512) SWEEP_CASE(4, 512) SWEEP_CASE(3, 512) SWEEP_CASE(2, 512)
@@ -939,49 +988,120 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   count_launch();
 }
 bool sweep_supported(const SkewGeo &q) {
-  return sweep_depth(q, SWEEP_FWD) > 0 && sweep_depth(q, SWEEP_BWD) > 0;
+  return sweep_depth(q, SWEEP_FWD, 8) > 0 && sweep_depth(q, SWEEP_BWD, 8) > 0;
 }
-void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
-                const double *spmv_x, double *tout, SolveState *st, double *ybuf) {
-  if (spmv_x && sweep_depth(q, SWEEP_FWD_AX) == 0) {
+bool sweep_supported_f(const SkewGeo &q) {
+  return sweep_depth(q, SWEEP_FWD, 4) > 0 && sweep_depth(q, SWEEP_BWD, 4) > 0 && ring_depth(7, q.T, 4) > 0;
+}
+template <typename V>
+static void launch_fwd_t(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *y,
+                         const V *spmv_x, V *tout, SolveState *st, V *ybuf) {
+  if (spmv_x && sweep_depth(q, SWEEP_FWD_AX, (int)sizeof(V)) == 0) {
     // Ring of the fused sweep too large for this tile: SpMV first.
-    launch_spmv(s, g, q, S, spmv_x, ybuf, st);
+    launch_spmv_t<V>(s, g, q, S, spmv_x, ybuf, st);
     y = ybuf;
     spmv_x = nullptr;
   }
-  if (spmv_x) launch_sweep<SWEEP_FWD_AX>(s, g, q, S, spmv_x, tout, st);
-  else launch_sweep<SWEEP_FWD>(s, g, q, S, y, tout, st);
+  if (spmv_x) launch_sweep<SWEEP_FWD_AX, V>(s, g, q, S, spmv_x, tout, st);
+  else launch_sweep<SWEEP_FWD, V>(s, g, q, S, y, tout, st);
+}
+void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
+                const double *spmv_x, double *tout, SolveState *st, double *ybuf) {
+  launch_fwd_t<double>(s, g, q, S, y, spmv_x, tout, st, ybuf);
+}
+void launch_fwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *y,
+                  const float *spmv_x, float *tout, SolveState *st, float *ybuf) {
+  launch_fwd_t<float>(s, g, q, S, y, spmv_x, tout, st, ybuf);
 }
 void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
                 double *x, SolveState *st) {
-  launch_sweep<SWEEP_BWD>(s, g, q, S, tin, x, st);
+  launch_sweep<SWEEP_BWD, double>(s, g, q, S, tin, x, st);
+}
+void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *tin,
+                  float *x, SolveState *st) {
+  launch_sweep<SWEEP_BWD, float>(s, g, q, S, tin, x, st);
 }
 static inline unsigned slab_blocks(const SkewGeo &q) {
   return (unsigned)(((long long)q.nb * q.W + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK);
 }
 #define SL(kern, ...) (kern<<<slab_blocks(q), ROW_THREADS, 0, s>>>(__VA_ARGS__), count_launch())
+template <typename V>
+void launch_spmv_t(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *x, V *y,
+                   const SolveState *st) { SL(k_spmv<V>, g, q, S, x, y, st); }
 void launch_spmv(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *x, double *y,
-                 const SolveState *st) { SL(k_spmv, g, q, S, x, y, st); }
+                 const SolveState *st) { launch_spmv_t<double>(s, g, q, S, x, y, st); }
 void launch_bmy(cudaStream_t s, const SkewGeo &q, const int *indc, const double *b, double *y,
                 const SolveState *st) { SL(k_bmy, q, indc, b, y, st); }
+template <typename V>
+void launch_dot_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *x0, const V *y0, const V *x1,
+                  const V *y1, double *rb0, double *rb1, const SolveState *st) {
+  SL(k_dot<V>, q, indc, x0, y0, x1, y1, rb0, rb1, st);
+}
+template <typename V>
+void launch_copy2_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *r0, V *rr, V *pp,
+                    const SolveState *st) { SL(k_copy2<V>, q, indc, r0, rr, pp, st); }
+template <typename V>
+void launch_axpy_rr_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *ap, V *rr,
+                      const SolveState *st) { SL(k_axpy_rr<V>, q, indc, ap, rr, st); }
+template <typename V>
+void launch_upd_xr_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *pp, const V *ae, const V *r0,
+                     V *xw, V *rr, double *rb0, double *rb1, const SolveState *st) {
+  SL(k_upd_xr<V>, q, indc, pp, ae, r0, xw, rr, rb0, rb1, st);
+}
+template <typename V>
+void launch_upd_p_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *rr, const V *ap, V *pp,
+                    const SolveState *st) { SL(k_upd_p<V>, q, indc, rr, ap, pp, st); }
+template void launch_spmv_t<double>(cudaStream_t, const Geo &, const SkewGeo &, const SkewSysT<double> &,
+                                    const double *, double *, const SolveState *);
+template void launch_spmv_t<float>(cudaStream_t, const Geo &, const SkewGeo &, const SkewSysT<float> &,
+                                   const float *, float *, const SolveState *);
+template void launch_dot_t<double>(cudaStream_t, const SkewGeo &, const int *, const double *, const double *,
+                                   const double *, const double *, double *, double *, const SolveState *);
+template void launch_dot_t<float>(cudaStream_t, const SkewGeo &, const int *, const float *, const float *,
+                                  const float *, const float *, double *, double *, const SolveState *);
+template void launch_copy2_t<double>(cudaStream_t, const SkewGeo &, const int *, const double *, double *,
+                                     double *, const SolveState *);
+template void launch_copy2_t<float>(cudaStream_t, const SkewGeo &, const int *, const float *, float *, float *,
+                                    const SolveState *);
+template void launch_axpy_rr_t<double>(cudaStream_t, const SkewGeo &, const int *, const double *, double *,
+                                       const SolveState *);
+template void launch_axpy_rr_t<float>(cudaStream_t, const SkewGeo &, const int *, const float *, float *,
+                                      const SolveState *);
+template void launch_upd_xr_t<double>(cudaStream_t, const SkewGeo &, const int *, const double *, const double *,
+                                      const double *, double *, double *, double *, double *, const SolveState *);
+template void launch_upd_xr_t<float>(cudaStream_t, const SkewGeo &, const int *, const float *, const float *,
+                                     const float *, float *, float *, double *, double *, const SolveState *);
+template void launch_upd_p_t<double>(cudaStream_t, const SkewGeo &, const int *, const double *, const double *,
+                                     double *, const SolveState *);
+template void launch_upd_p_t<float>(cudaStream_t, const SkewGeo &, const int *, const float *, const float *,
+                                    float *, const SolveState *);
 void launch_dot(cudaStream_t s, const SkewGeo &q, const int *indc, const double *x0, const double *y0,
                 const double *x1, const double *y1, double *rb0, double *rb1, const SolveState *st) {
-  SL(k_dot, q, indc, x0, y0, x1, y1, rb0, rb1, st);
+  launch_dot_t<double>(s, q, indc, x0, y0, x1, y1, rb0, rb1, st);
 }
 void launch_copy2(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r0, double *rr, double *pp,
-                  const SolveState *st) { SL(k_copy2, q, indc, r0, rr, pp, st); }
+                  const SolveState *st) { launch_copy2_t<double>(s, q, indc, r0, rr, pp, st); }
 void launch_axpy_rr(cudaStream_t s, const SkewGeo &q, const int *indc, const double *ap, double *rr,
-                    const SolveState *st) { SL(k_axpy_rr, q, indc, ap, rr, st); }
+                    const SolveState *st) { launch_axpy_rr_t<double>(s, q, indc, ap, rr, st); }
 void launch_upd_xr(cudaStream_t s, const SkewGeo &q, const int *indc, const double *pp, const double *ae,
                    const double *r0, double *xw, double *rr, double *rb0, double *rb1, const SolveState *st) {
-  SL(k_upd_xr, q, indc, pp, ae, r0, xw, rr, rb0, rb1, st);
+  launch_upd_xr_t<double>(s, q, indc, pp, ae, r0, xw, rr, rb0, rb1, st);
 }
 void launch_upd_p(cudaStream_t s, const SkewGeo &q, const int *indc, const double *rr, const double *ap,
-                  double *pp, const SolveState *st) { SL(k_upd_p, q, indc, rr, ap, pp, st); }
+                  double *pp, const SolveState *st) { launch_upd_p_t<double>(s, q, indc, rr, ap, pp, st); }
 void launch_x0(cudaStream_t s, const Geo &g, const SkewGeo &q, const int *indc, const double *xw, double *x0,
                const SolveState *st) { SL(k_x0, g, q, indc, xw, x0, st); }
 void launch_relres(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *b,
                    const double *x, double *rb0, double *rb1) { SL(k_relres, g, q, S, b, x, rb0, rb1); }
+void launch_sys_to_f(cudaStream_t s, const SkewGeo &q, const double *sys, float *sysf) {
+  const long long n = (long long)q.nb * q.W * q.T;
+  k_sys_to_f<<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, s>>>(q, sys, sysf);
+  count_launch();
+}
+void launch_scale_to_f(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r, double scale,
+                       float *rf) { SL(k_scale_to_f, q, indc, r, scale, rf); }
+void launch_add_f(cudaStream_t s, const SkewGeo &q, const int *indc, const float *d, double inv_scale,
+                  double *x) { SL(k_add_f, q, indc, d, inv_scale, x); }
 #undef SL
 void launch_fin(cudaStream_t s, int mode, const double *rb0, const double *rb1, long long nrows,
                 SolveState *st, double *out, double epsa2, double epsr2, double div2, int icgmax) {

@@ -20,15 +20,18 @@ struct SysPtr {
 // by slab, sys[(slab*SYS_N + c)*T + t], so the values one wavefront step
 // needs are one contiguous block; INDC is a plain skewed array.
 enum SysArray { SYS_AD = 0, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK, SYS_DD, SYS_N };
-struct SkewSys {
-  double *sys;
+template <typename V> struct SkewSysT {
+  V *sys;
   int *indc;
 };
+using SkewSys = SkewSysT<double>;   // the FP64 system of VF_M1BCGS
+using SkewSysF = SkewSysT<float>;   // its FP32 copy for the inner solves of the mixed solver
 // Tile geometry of the skewed layout: TI x TJ columns per tile, W
 // wavefront slabs per tile, ntx tiles along x, nb tiles in all.  Slab
-// entry t = ti + TIp*tj with the row stride TIp = TI rounded up to even
-// (T = TIp*TJ entries per slab), so every slab, slab row and pair of
-// columns starts on a 16-byte boundary and moves with one bulk copy.
+// entry t = ti + TIp*tj with the row stride TIp = TI rounded up to a
+// multiple of 4 (T = TIp*TJ entries per slab), so every slab, slab row and
+// group of 16 bytes of columns starts on a 16-byte boundary in double and
+// in float arrays and moves with one bulk copy.
 struct SkewGeo {
   int TI, TJ, TIp, T, W, ntx, nb;
 };
@@ -49,7 +52,8 @@ __host__ __device__ inline long long sys_at(long long slab, int c, int T, int t)
 //         right;
 // MODE 2: backward sweep: {T, AUI, AUJ, AUK, DD}, copies: T, system
 //         slabs 4..7.
-// Offsets are in doubles; `arr` 0 is the interleaved system, 1 the vector.
+// Offsets are in elements of the sweep's type (es bytes: 8 for double, 4
+// for float); `arr` 0 is the interleaved system, 1 the vector.
 enum SweepMode { SWEEP_FWD = 0, SWEEP_FWD_AX = 1, SWEEP_BWD = 2 };
 struct SweepCopy {
   long long src;
@@ -59,19 +63,24 @@ __host__ __device__ inline int sweep_nv(int mode) {
   return mode == SWEEP_FWD_AX ? 9 : (mode == SWEEP_FWD ? 8 : 5);
 }
 __host__ __device__ inline int sweep_ncopy(const SkewGeo &, int mode) { return mode == SWEEP_FWD_AX ? 6 : 2; }
-// Doubles of a left/right halo span: TIp*(TJ-1)+2 (even).
-__host__ __device__ inline int halo_span(const SkewGeo &q) { return q.TIp * (q.TJ - 1) + 2; }
-// doubles per ring slot (even, so slots stay 16-byte aligned)
-__host__ __device__ inline int sweep_slot(const SkewGeo &q, int mode) {
-  return sweep_nv(mode) * q.T + (mode == SWEEP_FWD_AX ? 2 * halo_span(q) + 2 * q.TIp : 0);
+// Elements per 16 bytes.
+__host__ __device__ inline int sweep_g(int es) { return 16 / es; }
+// Elements of a left/right halo span: TIp*(TJ-1) + 16 bytes.
+__host__ __device__ inline int halo_span(const SkewGeo &q, int es) { return q.TIp * (q.TJ - 1) + sweep_g(es); }
+// elements per ring slot (a multiple of 16 bytes, so slots stay aligned)
+__host__ __device__ inline int sweep_slot(const SkewGeo &q, int mode, int es) {
+  return sweep_nv(mode) * q.T + (mode == SWEEP_FWD_AX ? 2 * halo_span(q, es) + 2 * q.TIp : 0);
 }
 // Offsets of the halo values inside a slot (MODE 1): the value of row tj
-// is at halo_left + TIp*tj + ((TI-1)&1), halo_right + TIp*tj,
+// is at halo_left + TIp*tj + halo_lofs, halo_right + TIp*tj,
 // halo_down + ti and halo_up + ti.
-__host__ __device__ inline int halo_left(const SkewGeo &q) { return 9 * q.T; }
-__host__ __device__ inline int halo_right(const SkewGeo &q) { return 9 * q.T + halo_span(q); }
-__host__ __device__ inline int halo_down(const SkewGeo &q) { return 9 * q.T + 2 * halo_span(q); }
-__host__ __device__ inline int halo_up(const SkewGeo &q) { return 9 * q.T + 2 * halo_span(q) + q.TIp; }
+__host__ __device__ inline int halo_lofs(const SkewGeo &q, int es) { return (q.TI - 1) & (sweep_g(es) - 1); }
+__host__ __device__ inline int halo_left(const SkewGeo &q, int) { return 9 * q.T; }
+__host__ __device__ inline int halo_right(const SkewGeo &q, int es) { return 9 * q.T + halo_span(q, es); }
+__host__ __device__ inline int halo_down(const SkewGeo &q, int es) { return 9 * q.T + 2 * halo_span(q, es); }
+__host__ __device__ inline int halo_up(const SkewGeo &q, int es) {
+  return 9 * q.T + 2 * halo_span(q, es) + q.TIp;
+}
 // Copy c of tile b, the part that does not change from step to step: the
 // slab of step u is w = u (forward) or nsteps-1-u (backward), and the copy
 // reads array `arr` at offset base + w*wstride when dlo <= w <= dhi (false
@@ -83,7 +92,7 @@ struct SweepLane {
   long long base;
   int wstride, dst, bytes, arr, dlo, dhi;
 };
-__host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, int c, SweepLane &l) {
+__host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, int c, SweepLane &l, int es) {
   const long long slab0 = (long long)b * q.W;
   l.dlo = 0; l.dhi = q.W - 1;
   const int sys_c = (mode == SWEEP_FWD_AX) ? 0 : 1;  // copy index of the system block
@@ -93,7 +102,7 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
     l.base = sys_at(slab0, first, q.T, 0);
     l.wstride = SYS_N * q.T;
     l.dst = (mode == SWEEP_FWD_AX) ? 0 : q.T;
-    l.bytes = (SYS_N - first) * q.T * 8;
+    l.bytes = (SYS_N - first) * q.T * es;
     l.arr = 0;
     return true;
   }
@@ -102,7 +111,7 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
   if (c == vec_c) {
     l.base = slab0 * q.T;
     l.dst = (mode == SWEEP_FWD_AX) ? 8 * q.T : 0;
-    l.bytes = q.T * 8;
+    l.bytes = q.T * es;
     return true;
   }
   if (mode != SWEEP_FWD_AX) return false;
@@ -111,19 +120,19 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
   if (c == 2) {  // down: row tj = TJ-1 of tile b-ntx
     if (by == 0) return false;
     nb_tile = b - q.ntx; dw = q.TJ - 1; toff = q.TIp * (q.TJ - 1);
-    l.dst = halo_down(q); l.bytes = q.TIp * 8;
+    l.dst = halo_down(q, es); l.bytes = q.TIp * es;
   } else if (c == 3) {  // up: row tj = 0 of tile b+ntx
     if (by == nty - 1) return false;
     nb_tile = b + q.ntx; dw = -(q.TJ - 1); toff = 0;
-    l.dst = halo_up(q); l.bytes = q.TIp * 8;
-  } else if (c == 4) {  // left: tile b-1 from column (TI-1)&~1 of row 0 to column TI-1 of row TJ-1
+    l.dst = halo_up(q, es); l.bytes = q.TIp * es;
+  } else if (c == 4) {  // left: tile b-1, from the 16 bytes holding column TI-1 of row 0 to those of row TJ-1
     if (bx == 0) return false;
-    nb_tile = b - 1; dw = q.TI - 1; toff = (q.TI - 1) & ~1;
-    l.dst = halo_left(q); l.bytes = halo_span(q) * 8;
-  } else if (c == 5) {  // right: tile b+1 from column 0 of row 0 to column 1 of row TJ-1
+    nb_tile = b - 1; dw = q.TI - 1; toff = (q.TI - 1) & ~(sweep_g(es) - 1);
+    l.dst = halo_left(q, es); l.bytes = halo_span(q, es) * es;
+  } else if (c == 5) {  // right: tile b+1, from column 0 of row 0 to the 16 bytes of row TJ-1
     if (bx == q.ntx - 1) return false;
     nb_tile = b + 1; dw = -(q.TI - 1); toff = 0;
-    l.dst = halo_right(q); l.bytes = halo_span(q) * 8;
+    l.dst = halo_right(q, es); l.bytes = halo_span(q, es) * es;
   } else {
     return false;
   }
@@ -135,9 +144,9 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
 // Copy c for wavefront step u of tile b (nsteps steps); false when it is
 // not issued.
 __host__ __device__ inline bool sweep_copy(const SkewGeo &q, int mode, int b, int nsteps, int u, int c,
-                                           SweepCopy &cp) {
+                                           SweepCopy &cp, int es) {
   SweepLane l;
-  if (!sweep_lane(q, mode, b, c, l)) return false;
+  if (!sweep_lane(q, mode, b, c, l, es)) return false;
   const int w = (mode == SWEEP_BWD) ? nsteps - 1 - u : u;
   if (w < l.dlo || w > l.dhi) return false;
   cp.src = l.base + (long long)w * l.wstride;
@@ -166,12 +175,42 @@ void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, i
 // k_poisson.cu
 void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const SysPtr &a, int *err);
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
-                    const SkewSys &S, const double *x0, double *bsl, double *xsl);
+                    const SkewSys &S, const double *x0, double *bsl, double *xsl, int warm);
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad);
 void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
                 const double *spmv_x, double *tout, SolveState *st, double *ybuf);
 void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
                 double *x, SolveState *st);
+// FP32 forms for the inner solves of the mixed-precision solver.
+void launch_fwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *y,
+                  const float *spmv_x, float *tout, SolveState *st, float *ybuf);
+void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *tin,
+                  float *x, SolveState *st);
+void launch_dcmp_f(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSysF &S, int *pivot_bad);
+bool sweep_supported_f(const SkewGeo &q);
+// Vector kernels for both precisions (explicitly instantiated for double
+// and float in k_poisson.cu).
+template <typename V>
+void launch_spmv_t(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *x, V *y,
+                   const SolveState *st);
+template <typename V>
+void launch_dot_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *x0, const V *y0, const V *x1,
+                  const V *y1, double *rb0, double *rb1, const SolveState *st);
+template <typename V>
+void launch_copy2_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *r0, V *rr, V *pp,
+                    const SolveState *st);
+template <typename V>
+void launch_axpy_rr_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *ap, V *rr, const SolveState *st);
+template <typename V>
+void launch_upd_xr_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *pp, const V *ae, const V *r0,
+                     V *xw, V *rr, double *rb0, double *rb1, const SolveState *st);
+template <typename V>
+void launch_upd_p_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *rr, const V *ap, V *pp,
+                    const SolveState *st);
+void launch_sys_to_f(cudaStream_t s, const SkewGeo &q, const double *sys, float *sysf);
+void launch_scale_to_f(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r, double scale,
+                       float *rf);
+void launch_add_f(cudaStream_t s, const SkewGeo &q, const int *indc, const float *d, double inv_scale, double *x);
 // Thread block of the sweeps for a tile of T slab entries (T consumer
 // threads rounded up to whole warps, plus the producer warp).
 inline int sweep_threads(int T) { return ((T + 31) & ~31) + 32; }

@@ -142,14 +142,14 @@ struct orc_handle {
 
   // The same tree over the slabs of the GPU solver's tile-skewed layout:
   // tile b (x fastest), wavefront slab w = (k-2)+ti+tj, slab entry
-  // t = ti + TIp*tj (TIp = TI rounded up to even; the column ti = TI of an
-  // odd TI is padding); lane l of a slab sums t = l, l+32, ... in order,
+  // t = ti + TIp*tj (TIp = TI rounded up to a multiple of 4; columns
+  // ti >= TI are padding); lane l of a slab sums t = l, l+32, ... in order,
   // warp tree per slab, then the 1024-thread tree over the slabs.  This is
   // the order of the dot products of VF_M1BCGS in the GPU library.
   template <class F> double gsum_skew(F f) const {
     const int TI = std::min(P.precond_ti > 0 ? P.precond_ti : NI - 2, NI - 2);
     const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2);
-    const int TIp = TI + (TI & 1);
+    const int TIp = (TI + 3) & ~3;
     const int T = TIp * TJ, W = (NK - 2) + (TI - 1) + (TJ - 1);
     const int ntx = (NI - 2 + TI - 1) / TI, nb = ntx * ((NJ - 2 + TJ - 1) / TJ);
     const long long NS = (long long)nb * W;
