@@ -85,6 +85,8 @@ def combine_ranks(t_local: float, units_local: float, device=None):
 
 def build_case(args):
     P = _load_pkg()
+    if getattr(args, "case", "flume") == "beach":
+        return P.cases.solitary_beach()
     c = P.cases.porous_flume(nx=args.nx, ny=args.ny, nz=args.nz)
     P.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
     P.cases.wave_maker(c, 0.08, 1.5, 0.5)
@@ -92,7 +94,8 @@ def build_case(args):
 
 
 def params_for(args):
-    return dict(cgepsr=1.0e-10, precond_ti=args.ti, precond_tj=args.tj,
+    return dict(cgepsr=1.0e-8 if getattr(args, "case", "flume") == "beach" else 1.0e-10,
+                precond_ti=args.ti, precond_tj=args.tj,
                 solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
                 warm_start=1 if getattr(args, "guess", "zero") == "previous" else 0)
 
@@ -214,6 +217,12 @@ def run_reference(args, rank, world):
 def workload_config(case, args):
     solver = ("mixed FP32-inner/FP64-refinement" if getattr(args, "solver", "fp64") == "mixed"
               else "plain FP64")
+    if getattr(args, "case", "flume") == "beach":
+        return {"workload": f"solitary wave on a 1:20 beach with 40 porous boxes "
+                            f"{case.ni-2}x{case.nj-2}x{case.nk-2} {solver} SMAC step (dt={case.dt}, "
+                            f"tol 1e-8, block-Jacobi MILU {args.ti}x{args.tj} columns)",
+                "cells": case.interior_cells, "precond_block": [args.ti, args.tj],
+                "l2": "inputs larger than L2"}
     if getattr(args, "guess", "zero") == "previous":
         solver += ", previous-step initial guess,"
     return {"workload": f"porous wave flume {case.ni-2}x{case.nj-2}x{case.nk-2} {solver} SMAC step "
@@ -379,6 +388,70 @@ def run_ours(args, rank, world, local_rank):
     tank.close()
 
 
+def run_ensemble(args, rank, world, local_rank):
+    """Ensemble of independent flumes of uneven size stepped side by side
+    (cadmas_step_ensemble: one host thread and one stream per flume).
+    value = all flumes' interior cells x steps / device time of the steps;
+    the same members stepped one after another give `sequential_value`."""
+    import torch
+    P = _load_pkg()
+    sys.path.insert(0, str(PKG_DIR))
+    import build as pbuild
+    sys.path.pop(0)
+    if rank == 0:
+        pbuild.build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cases = P.cases.ensemble_flumes(args.members, seed=1000 * rank, scale=args.scale)
+    tanks = [P.Tank(c, **params_for(args)) for c in cases]
+    for t in tanks:
+        t.init_state(True)
+    cells = sum(c.interior_cells for c in cases)
+    streams = [torch.cuda.ExternalStream(t.stream(), device=dev) for t in tanks]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        fn()
+        ends = []
+        for st in streams:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(st)
+            ends.append(e)
+        torch.cuda.synchronize()
+        return max(e0.elapsed_time(e) for e in ends)
+
+    for _ in range(args.warmup):
+        P.step_ensemble(tanks)
+    l0 = P.kernel_launches()
+    with ClockSampler(local_rank) as clk:
+        t_par = timed(lambda: [P.step_ensemble(tanks) for _ in range(args.steps)])
+    launches = P.kernel_launches() - l0
+    t_seq = timed(lambda: [t.step() for _ in range(args.steps) for t in tanks])
+    t_max, units = combine_ranks(t_par / 1e3, cells * args.steps, device=dev)
+    iters = [t.stats()["icgitr"] for t in tanks]
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": units / t_max / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_par / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"ensemble of {args.members} independent porous wave flumes of uneven "
+                                   f"size (nx U{{256..1024}}x{args.scale:g}, ny U{{16..64}}, nz U{{64..128}}, "
+                                   f"wave makers, {'mixed' if args.solver == 'mixed' else 'plain FP64'} "
+                                   f"SMAC step, block-Jacobi MILU {args.ti}x{args.tj})",
+                       "cells": cells, "members": args.members,
+                       "sizes": [[c.ni - 2, c.nj - 2, c.nk - 2] for c in cases],
+                       "sequential_value": cells * args.steps / (t_seq / 1e3) / 1e6,
+                       "mean_bicgstab_iters": statistics.mean(iters),
+                       "parallelism": f"{args.members} streams side by side x{world} replicas"},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    for t in tanks:
+        t.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,6 +461,11 @@ def main():
     ap.add_argument("--solver", choices=["fp64", "mixed"], default="fp64",
                     help="pressure solver: the reference's FP64 MILU-BiCGSTAB, or FP32 inner solves "
                          "under FP64 refinement")
+    ap.add_argument("--members", type=int, default=8, help="ensemble members (--case ensemble)")
+    ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
+    ap.add_argument("--case", choices=["flume", "beach", "ensemble"], default="flume",
+                    help="flume: 512x32x96 porous wave flume (default); beach: 1024x128x128 solitary "
+                         "wave on a 1:20 beach with 40 porous boxes")
     ap.add_argument("--guess", choices=["zero", "previous"], default="zero",
                     help="initial guess of each pressure solve: 0 as the reference, or the previous "
                          "step's solution")
@@ -413,6 +491,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.case == "ensemble":
+            run_ensemble(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -215,6 +215,13 @@ int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st);
 /* Synchronise the handle's stream. */
 int cadmas_sync(cadmas_handle *h);
 
+/* ---- ensemble of independent grids (no counterpart in the reference) ----
+   One SMAC step of each of the n handles (one host thread per handle, each
+   handle on its own stream, so the GPU runs the grids' kernels side by
+   side).  dt[i] is handle i's time step; status[i] receives its
+   cadmas_step status.  Returns the first non-zero status, or CADMAS_OK. */
+int cadmas_step_ensemble(cadmas_handle **h, int n, const double *dt, int *status);
+
 /* Declare side w->side a wave-maker boundary driven by `tab` (copied).  Its
    boundary faces are those of INDB with INDB(3,L) = 5 on that side.  One
    table serves every wave side, as the reference's matrix data does.

@@ -91,7 +91,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_set_state", "cadmas_get_state", "cadmas_init_state", "cadmas_step",
             "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
             "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
-            "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave",
+            "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers"]
 
 STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]
@@ -141,6 +141,7 @@ def load_library(path: pathlib.Path | None = None):
     vf.argtypes = [C.POINTER(C.c_void_p), _dp] + [_dp] * 5 + [_ip, _ip] + [_dp] * 5 + [_dp, _ip]
     lib.cadmas_divnorm_noalloc.argtypes = [C.POINTER(Dims)] + [C.c_void_p] * 11 + [_dp]
     lib.cadmas_set_wave.argtypes = [C.c_void_p, C.POINTER(WaveBC), C.POINTER(WaveTable)]
+    lib.cadmas_step_ensemble.argtypes = [C.POINTER(C.c_void_p), C.c_int, _dp, _ip]
     if path is None:
         _lib = lib
     return lib
@@ -359,3 +360,17 @@ def divnorm_noalloc(dims, xx, yy, zz, ggx, ggy, ggz, uu, vv, ww, indc, stream=0,
     args = [C.c_void_p(int(a)) for a in (xx, yy, zz, ggx, ggy, ggz, uu, vv, ww, indc)]
     _check(lib, lib.cadmas_divnorm_noalloc(C.byref(d), *args, C.c_void_p(int(stream)), C.byref(v)))
     return v.value
+
+
+def step_ensemble(tanks, dts=None, lib=None):
+    """One SMAC step of every tank, the tanks running side by side on the
+    GPU (cadmas_step_ensemble).  Returns the per-tank statuses."""
+    lib = lib or load_library()
+    n = len(tanks)
+    hs = (C.c_void_p * n)(*[t.h.value for t in tanks])
+    dt = (C.c_double * n)(*[float(d) for d in (dts if dts is not None else [t.case.dt for t in tanks])])
+    st = (C.c_int * n)()
+    rc = lib.cadmas_step_ensemble(hs, n, dt, st)
+    if rc != OK:
+        raise CadmasError(rc, lib.cadmas_strerror(rc).decode())
+    return list(st)

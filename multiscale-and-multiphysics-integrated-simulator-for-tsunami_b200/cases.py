@@ -607,3 +607,31 @@ def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: f
     c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp,
                   table=table if table is not None else first_order_wave_table(H, T, depth))
     return c
+
+
+def ensemble_flumes(members: int = 64, seed: int = 0, dx: float = 0.02, dz: float = 0.01,
+                    scale: float = 1.0) -> list:
+    """Independent wave flumes of uneven size: nx in U{256..1024},
+    ny in U{16..64}, nz in U{64..128} (times `scale` in x), depth U(0.4,0.8)
+    m (kept below 0.75 of the flume height), regular waves H U(0.05,0.2) m,
+    T U(1,3) s from a wave maker on a developed wave train, one porous block
+    of porosity U(0.3,0.6) per flume (seeded, Philox)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for m in range(members):
+        nx = int(rng.integers(256, 1025) * scale) // 16 * 16
+        ny = int(rng.integers(16, 65)) // 16 * 16
+        nz = int(rng.integers(64, 129))
+        depth = min(float(rng.uniform(0.4, 0.8)), 0.75 * nz * dz)
+        H = min(float(rng.uniform(0.05, 0.2)), 0.3 * depth)
+        T = float(rng.uniform(1.0, 3.0))
+        gam = float(rng.uniform(0.3, 0.6))
+        x0 = float(rng.uniform(0.3, 0.6)) * nx * dx
+        c = porous_flume(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, depth=depth,
+                         block=(x0, x0 + 1.0, depth + H), gamma=gam,
+                         sponge_width=min(2.0, 0.2 * nx * dx))
+        linear_wave_initial(c, H, T, depth)
+        wave_maker(c, H, T, depth)
+        c.name = f"ensemble_{m}"
+        out.append(c)
+    return out

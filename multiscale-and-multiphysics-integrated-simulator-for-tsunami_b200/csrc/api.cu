@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "cadmas_dev.cuh"
@@ -1046,6 +1047,24 @@ int cadmas_step(cadmas_handle *h, double dt) {
   if (rc == CADMAS_OK) rc = cadmas_f1cal(h);
   h->stats.last_status = rc;
   return rc;
+}
+
+int cadmas_step_ensemble(cadmas_handle **hs, int n, const double *dt, int *status) {
+  if (!hs || !dt || !status || n < 0) return CADMAS_EINVAL;
+  for (int i = 0; i < n; ++i)
+    if (!hs[i]) return CADMAS_EINVAL;
+  if (n == 1) return status[0] = cadmas_step(hs[0], dt[0]);
+  std::vector<std::thread> pool;
+  pool.reserve((size_t)n);
+  for (int i = 0; i < n; ++i)
+    pool.emplace_back([=]() {
+      cudaSetDevice(hs[i]->device);
+      status[i] = cadmas_step(hs[i], dt[i]);
+    });
+  for (std::thread &t : pool) t.join();
+  for (int i = 0; i < n; ++i)
+    if (status[i]) return status[i];
+  return CADMAS_OK;
 }
 
 int cadmas_divnorm(cadmas_handle *h, double *val) {
