@@ -261,11 +261,8 @@ def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     P = _load_pkg()
-    sys.path.insert(0, str(PKG_DIR))
-    import build as pbuild
-    sys.path.pop(0)
     if rank == 0:
-        pbuild.build()
+        P.build_library()
     if world > 1:
         dist.barrier()
     torch.cuda.set_device(local_rank)
@@ -395,11 +392,8 @@ def run_ensemble(args, rank, world, local_rank):
     the same members stepped one after another give `sequential_value`."""
     import torch
     P = _load_pkg()
-    sys.path.insert(0, str(PKG_DIR))
-    import build as pbuild
-    sys.path.pop(0)
     if rank == 0:
-        pbuild.build()
+        P.build_library()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     cases = P.cases.ensemble_flumes(args.members, seed=1000 * rank, scale=args.scale)

@@ -42,7 +42,8 @@ module cadmas_gpu
      integer(c_int) :: diag_relres
      integer(c_int) :: solver
      integer(c_int) :: warm_start
-     integer(c_int) :: reserved(3)
+     integer(c_int) :: precond_split
+     integer(c_int) :: reserved(2)
   end type cadmas_params
 
   ! c_loc() of the static arrays (XX(6,NUMI) ... INDB(4,NUMB))

@@ -103,7 +103,13 @@ typedef struct cadmas_params {
      The stopping test is unchanged (|M^-1 r| against |M^-1 b| for
      solver 0), so the result meets the same tolerance.                  */
   int    warm_start;
-  int    reserved[3];
+  /* 0 or 1: one thread block per preconditioner block; 2: two blocks of
+     a thread-block cluster, each sweeping precond_tj/2 rows and passing
+     its boundary row to the other through distributed shared memory.  The
+     preconditioner (and the result) is the same; precond_tj must be even.
+     The BiCGSTAB dot products then sum over half-height slabs.           */
+  int    precond_split;
+  int    reserved[2];
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */

@@ -67,7 +67,8 @@ class Params(C.Structure):
         ("idamp", C.c_int * 4),
         ("icgtyp", C.c_int), ("icgmax", C.c_int), ("ibsuw0", C.c_int),
         ("precond_ti", C.c_int), ("precond_tj", C.c_int),
-        ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("reserved", C.c_int * 3)]
+        ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("precond_split", C.c_int),
+        ("reserved", C.c_int * 2)]
 
 
 class Static(C.Structure):
@@ -104,6 +105,15 @@ class CadmasError(RuntimeError):
 
 
 _lib = None
+
+
+def build_library(force: bool = False, verbose: bool = False) -> pathlib.Path:
+    """Compile libcadmas_gpu.so for sm_100a if its sources changed (nvcc)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("cadmas_b200_build", pathlib.Path(__file__).parent / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(force=force, verbose=verbose)
 
 
 def load_library(path: pathlib.Path | None = None):

@@ -754,10 +754,16 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
   AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
   for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
-  h->q.TI = TI; h->q.TJ = TJ; h->q.TIp = (TI + 3) & ~3; h->q.T = h->q.TIp * TJ;
-  h->q.W = (d->numk - 2) + (TI - 1) + (TJ - 1);
+  // layout tiles: TI x TJ, or TI x TJ/2 when each preconditioner block is
+  // split over a cluster of two thread blocks
+  const int split = (p->precond_split == 2) ? 2 : 1;
+  if (p->precond_split < 0 || p->precond_split > 2 || TJ % split != 0) rc = CADMAS_EINVAL;
+  const int TJl = TJ / split;
+  h->q.split = split;
+  h->q.TI = TI; h->q.TJ = TJl; h->q.TIp = (TI + 3) & ~3; h->q.T = h->q.TIp * TJl;
+  h->q.W = (d->numk - 2) + (TI - 1) + (TJl - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
-  h->q.nb = h->q.ntx * ((d->numj - 2 + TJ - 1) / TJ);
+  h->q.nb = h->q.ntx * ((d->numj - 2 + TJl - 1) / TJl);
   if (!sweep_supported(h->q)) {
     g_last_error = "preconditioner block too large for the MILU sweeps; set precond_ti/precond_tj";
     rc = CADMAS_EUNSUPPORTED;

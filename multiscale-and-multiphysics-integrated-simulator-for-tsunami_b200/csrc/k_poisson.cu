@@ -269,24 +269,35 @@ __device__ __forceinline__ void skew_fetch(double *dst, const Geo &g, const Skew
 }
 
 // ------------------------------------------------------------ VF_MZDCMP
-// ring values: 0 AD, 1 ALI, 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK; DD is
-// written in the skewed layout.
+// One thread block per preconditioner block (TI x TJ*split columns; with
+// split = 2 the block's columns live in two layout tiles), one thread per
+// column, wavefront step s at k = 2+s-ti-tj.  Ring values: 0 AD, 1 ALI,
+// 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK; DD is written in the skewed layout.
 template <int D, typename V>
 __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
   constexpr int NV = 7, R = D + 3;
-  const int TIp = q.TIp, T = q.T;
-  Ring<NV, V> rg = ring_setup<NV, V>(T, R);
-  TileGeo t = tile_geo(g, q);
-  const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
-  const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
+  const int TIp = q.TIp, TJl = q.TJ, Tl = q.T;      // layout tile
+  const int TJb = TJl * q.split, Tb = TIp * TJb;    // preconditioner block
+  Ring<NV, V> rg = ring_setup<NV, V>(Tb, R);
+  const int tid = threadIdx.x;
+  const int ti = tid % TIp, tj = tid / TIp;
+  const int is = 2 + blockIdx.x * q.TI, js = 2 + blockIdx.y * TJb;
+  const int wi = min(q.TI, g.NI - is), wj = min(TJb, g.NJ - js);
+  const bool valid = ti < wi && tj < wj;
+  const int r = tj / TJl, tjl = tj % TJl;
+  const long long bl = blockIdx.x + (long long)q.ntx * (blockIdx.y * q.split + r);  // layout tile
+  // slab of step s: w = (k-2) + ti + tjl = s - r*TJl
+  const long long slab0 = bl * q.W - (long long)r * TJl;
+  const int tl = ti + TIp * tjl;
+  const int nsteps = (g.NK - 2) + (wi - 1) + (wj - 1);
   auto prefetch = [&](int s) {
-    const int k = 2 + s - t.ti - t.tj;
-    if (t.valid && k >= 2 && k <= g.NK - 1) {
-      const long long slab = (long long)b * q.W + s, e = slab * T + tid;
-      const V *sy = S.sys + sys_at(slab, 0, T, tid);
+    const int k = 2 + s - ti - tj;
+    if (valid && k >= 2 && k <= g.NK - 1) {
+      const long long slab = slab0 + s, e = slab * Tl + tl;
+      const V *sy = S.sys + sys_at(slab, 0, Tl, tl);
       const int sl = s % R;
 #pragma unroll
-      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)c * T);
+      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)c * Tl);
       cp_async4(&rg.ind(sl, tid), S.indc + e);
     }
     cp_commit();
@@ -296,23 +307,24 @@ __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
   V dk1 = V(0), au3 = V(0);  // DD(i,j,k-1) and AU3 of (i,j,k-1); k-1 = 1 is the zero ghost layer
   const V z = V(0), one = V(1);
   bool bad = false;
+  const int T = Tb;
   for (int s = 0; s < nsteps; ++s) {
     prefetch(s + D);
     cp_wait<D - 1>();
     __syncthreads();
-    const int k = 2 + s - t.ti - t.tj;
+    const int k = 2 + s - ti - tj;
     const int sl = s % R, slp = (s + R - 1) % R, cur = s & 1, prv = cur ^ 1;
-    if (t.valid && k >= 2 && k <= g.NK - 1) {
+    if (valid && k >= 2 && k <= g.NK - 1) {
       V dd = z;
       if (rg.ind(sl, tid) != -1) {
         V d1 = z, a1, d2 = z, a2;
-        if (t.ti > 0) {
+        if (ti > 0) {
           d1 = rg.xb[prv * T + tid - 1];
           a1 = rg.v(slp, 4, tid - 1) + U * (rg.v(slp, 5, tid - 1) + rg.v(slp, 6, tid - 1));
         } else {
           a1 = z + U * (z + z);
         }
-        if (t.tj > 0) {
+        if (tj > 0) {
           d2 = rg.xb[prv * T + tid - TIp];
           a2 = rg.v(slp, 5, tid - TIp) + U * (rg.v(slp, 4, tid - TIp) + rg.v(slp, 6, tid - TIp));
         } else {
@@ -322,7 +334,7 @@ __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
                     rg.v(sl, 3, tid) * dk1 * au3);
         if (dd <= z) bad = true;
       }
-      S.sys[sys_at((long long)b * q.W + s, SYS_DD, T, tid)] = dd;
+      S.sys[sys_at(slab0 + s, SYS_DD, Tl, tl)] = dd;
       rg.xb[cur * T + tid] = dd;
       dk1 = dd;
       au3 = rg.v(sl, 6, tid) + U * (rg.v(sl, 4, tid) + rg.v(sl, 5, tid));
@@ -391,6 +403,55 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
   return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, 2000000000ull);
 }
 
+// ------------------------------------- cluster exchange (precond_split 2)
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ unsigned mapa(unsigned addr, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;\n" ::"r"(addr), "f"(v) : "memory");
+}
+// Arrive on an mbarrier of another CTA of the cluster, releasing this
+// thread's earlier stores to the cluster.
+__device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(addr) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_cluster(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait (2 s) acquiring what other CTAs of the cluster released.
+__device__ __noinline__ bool mbar_wait_cluster_slow(unsigned bar, unsigned parity) {
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    for (int i = 0; i < 64; ++i)
+      if (mbar_try_cluster(bar, parity)) return true;
+    if (global_ns() - t0 > 2000000000ull) return false;
+  }
+}
+__device__ __forceinline__ bool mbar_wait_cluster(unsigned bar, unsigned parity) {
+  return mbar_try_cluster(bar, parity) || mbar_wait_cluster_slow(bar, parity);
+}
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release;\nbarrier.cluster.wait.acquire;\n" ::: "memory");
+}
+
 // ------------------------------------ VF_MZFRWD (+VF_MZAX) and VF_MZBKWD
 // One block per tile: T consumer threads (thread t = ti + TIp*tj owns
 // column (ti,tj)) and one producer warp.  MODE (SweepMode):
@@ -414,10 +475,19 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
 // and their evaluation order are those of the reference loops, so the
 // results do not change.  The step loop is unrolled by the ring length so
 // slot addresses and mbarrier phases are constants.
-template <int D, int MODE, int MAXT, typename V>
+template <int D, int MODE, int MAXT, typename V, int CS>
 __global__ void __launch_bounds__(MAXT, 1)
     k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st) {
-  if (st->done) return;
+  // CS = 2: the thread blocks of a cluster are the two layout tiles of one
+  // preconditioner block; every block of a cluster runs through the two
+  // cluster barriers below, so none returns early.
+  const bool skip = st->done || (CS == 2 && (int)blockIdx.y >= q.nb / q.ntx);
+  if (CS == 1 && skip) return;
+  if (CS == 2 && skip) {
+    cluster_barrier();
+    cluster_barrier();
+    return;
+  }
   constexpr int R = D + 2;
   constexpr int AHEAD = (MODE == SWEEP_FWD_AX) ? 2 : 1;  // preparing step s+1 reads the slot of step s+AHEAD
   extern __shared__ __align__(16) double sm[];
@@ -434,6 +504,34 @@ __global__ void __launch_bounds__(MAXT, 1)
   const bool producer = tid >= Tc;
   const int lane = tid & 31;
 
+  // Cluster exchange (CS = 2).  The forward sweeps need, on row 0 of the
+  // upper tile, the result and DD of row TJ-1 of the lower tile at the
+  // same k; the backward sweep needs the reverse.  The sending row writes
+  // its values of step u into slot u of the receiver's xin/din and
+  // arrives on the receiver's xfull[u] (one arrival per column of the row,
+  // every step); a slot is written once per sweep.
+  const int NX = q.W;                                   // slots: steps of a tile at most
+  unsigned long long *xfull = reinterpret_cast<unsigned long long *>(xb + 2 * T);
+  V *xin = reinterpret_cast<V *>(xfull + NX);
+  V *din = xin + (size_t)NX * TIp;
+  const int crank = (CS == 2) ? (int)(blockIdx.y & 1) : 0;
+  const int nty = q.nb / q.ntx;
+  const bool has_up = CS == 2 && crank == 0 && (int)blockIdx.y + 1 < nty;
+  const bool has_lo = CS == 2 && crank == 1;
+  const bool recv = (MODE == SWEEP_BWD) ? has_up : has_lo;
+  const bool send = (MODE == SWEEP_BWD) ? has_lo : has_up;
+  const bool srow = send && ((MODE == SWEEP_BWD) ? t.tj == 0 : t.tj == q.TJ - 1) && !producer;
+  const bool rrow = recv && ((MODE == SWEEP_BWD) ? t.tj == t.wj - 1 : t.tj == 0) && !producer;
+  // receiver's step lag: rows of the sending tile minus one
+  const int lag = (MODE == SWEEP_BWD) ? min(q.TJ, g.NJ - (2 + ((int)blockIdx.y + 1) * q.TJ)) - 1 : q.TJ - 1;
+  unsigned r_xin = 0, r_din = 0, r_full = 0;            // the partner's xin, din, xfull
+  if (CS == 2 && send) {
+    const unsigned peer = cluster_rank() ^ 1u;
+    r_xin = mapa(smem_u32(xin), peer);
+    r_din = mapa(smem_u32(din), peer);
+    r_full = mapa(smem_u32(xfull), peer);
+  }
+
   // s_abort[c & 1]: a wait of some thread ran out of time during ring
   // cycle c.  Written during a cycle, read after its last barrier; the two
   // entries keep those reads apart from the writes of the next cycle.
@@ -442,6 +540,8 @@ __global__ void __launch_bounds__(MAXT, 1)
     for (int r = 0; r < R; ++r) mbar_init(smem_u32(bar + r), 1);
     s_abort[0] = s_abort[1] = 0;
   }
+  if (CS == 2 && recv)
+    for (int u = tid; u < NX; u += blockDim.x) mbar_init(smem_u32(xfull + u), (unsigned)TIp);
   if (MODE == SWEEP_FWD_AX) {  // halo values of absent neighbours stay 0 (ghost layer)
     const int nh = 2 * halo_span(q, ES) + 2 * TIp;
     for (int r = 0; r < R; ++r)
@@ -449,7 +549,8 @@ __global__ void __launch_bounds__(MAXT, 1)
   }
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  __syncthreads();
+  if (CS == 2) cluster_barrier();  // partner's barriers initialised before any remote arrival
+  else __syncthreads();
 
   // Producer: lane l issues copy l of every step (at most 6); its fixed
   // part is worked out once here.
@@ -515,7 +616,7 @@ __global__ void __launch_bounds__(MAXT, 1)
         y0 = cs[tid] * pc + cs[T + tid] * pxm + cs[2 * T + tid] * pym + cs[3 * T + tid] * pzm +
              cs[4 * T + tid] * pxp + cs[5 * T + tid] * pyp + cs[6 * T + tid] * pzp;
         const V d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : V(0);
-        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : V(0);
+        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
         c1 = cs[T + tid] * d1;
         c2 = cs[2 * T + tid] * d2;
         c3 = cs[3 * T + tid] * dk1;
@@ -525,7 +626,7 @@ __global__ void __launch_bounds__(MAXT, 1)
       const V d = cs[7 * T + tid];
       if (d != V(0)) {
         const V d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : V(0);
-        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : V(0);
+        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
         y0 = cs[tid];
         c1 = cs[T + tid] * d1;
         c2 = cs[2 * T + tid] * d2;
@@ -542,6 +643,7 @@ __global__ void __launch_bounds__(MAXT, 1)
   bool ok = true;
   if (!producer) {
     for (int u = 0; u < AHEAD; ++u) if (ok) ok = wait_data(u, u % R, (unsigned)((u / R) & 1));
+    if (CS == 2 && ok && rrow && col && 0 >= slo && 0 <= shi) ok = mbar_wait_cluster(smem_u32(xfull + lag), 0u);
     if (ok) prepare(0, slot_ptr(0), slot_ptr(R - 1), slot_ptr(1 % R));
     else s_abort[0] = 1;
   }
@@ -564,28 +666,40 @@ __global__ void __launch_bounds__(MAXT, 1)
         const unsigned ubar = bar0 + 8u * ((r + AHEAD) % R), upar = ph ^ (unsigned)((r + AHEAD) / R);
         const bool ready = !ok || u >= nsteps || mbar_test(ubar, upar);
         // the recurrence of step s
+        V xcur = V(0);
         if (act && ok) {
           const int cur = (s & 1) * T, prv = T - cur;
           V x = V(0);
           if (dd != V(0)) {
+            const V xr = rrow ? xin[(size_t)(s + lag) * TIp + t.ti] : V(0);  // partner tile's row
             if (MODE == SWEEP_BWD) {
               const V x1 = (ri > 0) ? xb[prv + tid + 1] : V(0);
-              const V x2 = (rj > 0) ? xb[prv + tid + TIp] : V(0);
+              const V x2 = (rj > 0) ? xb[prv + tid + TIp] : xr;
               x = (y0 - c1 * x1 - c2 * x2 - c3 * xk1) * dd;
             } else {
               const V x1 = (t.ti > 0) ? xb[prv + tid - 1] : V(0);
-              const V x2 = (t.tj > 0) ? xb[prv + tid - TIp] : V(0);
+              const V x2 = (t.tj > 0) ? xb[prv + tid - TIp] : xr;
               x = y0 - c1 * x1 - c2 * x2 - c3 * xk1;
             }
           }
           xb[cur + tid] = x;
           *vp = x;
           xk1 = x;
+          xcur = x;
         }
         vp += vstep;
+        if (CS == 2 && srow) {  // this step's boundary-row values to the partner tile
+          st_cluster(r_xin + (unsigned)(((size_t)s * TIp + t.ti) * ES), xcur);
+          if (MODE != SWEEP_BWD) st_cluster(r_din + (unsigned)(((size_t)s * TIp + t.ti) * ES), act ? dd : V(0));
+          mbar_arrive_remote(r_full + 8u * (unsigned)s);
+        }
         // prepare step s+1
         if (!ready) {
           ok = mbar_wait_slow(ubar, upar, 2000000000ull);
+          if (!ok) s_abort[ph] = 1;
+        }
+        if (CS == 2 && ok && rrow && col && s + 1 >= slo && s + 1 <= shi) {
+          ok = mbar_wait_cluster(smem_u32(xfull + (s + 1 + lag)), 0u);
           if (!ok) s_abort[ph] = 1;
         }
         if (ok && s + 1 < nsteps) prepare(s + 1, slot_ptr((r + 1) % R), slot_ptr(r), slot_ptr((r + 2) % R));
@@ -603,6 +717,7 @@ __global__ void __launch_bounds__(MAXT, 1)
         mbar_wait_slow(bar0 + 8u * (u % R), (unsigned)((u / R) & 1), 100000000ull);
     if (lane == 0) { st->timeout = 1; st->done = 1; }
   }
+  if (CS == 2) cluster_barrier();  // the partner may still write into this block's shared memory
 }
 
 // ------------------------------------------------------------ slab kernels
@@ -929,13 +1044,15 @@ void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr
 }
 template <typename V>
 static void launch_dcmp_t(cudaStream_t s, const Geo &g, const SkewGeo &q, V U, const SkewSysT<V> &S, int *pivot_bad) {
-  const int T = q.T, d = ring_depth(7, T, sizeof(V));
+  const int T = q.T * q.split, d = ring_depth(7, T, sizeof(V));  // one thread per block column
   const size_t bytes = ring_bytes(7, T, d + 3, sizeof(V));
+  const int TJb = q.TJ * q.split, nby = (g.NJ - 2 + TJb - 1) / TJb;
+  const dim3 grid((unsigned)q.ntx, (unsigned)nby);
   switch (d) {
 #define DCMP_CASE(DD)                                                                    \
   case DD:                                                                               \
     set_smem(k_dcmp<DD, V>, bytes);                                                      \
-    k_dcmp<DD, V><<<skew_grid(q), T, bytes, s>>>(g, q, U, S, pivot_bad);                 \
+    k_dcmp<DD, V><<<grid, T, bytes, s>>>(g, q, U, S, pivot_bad);                         \
     break;
     DCMP_CASE(8) DCMP_CASE(4) DCMP_CASE(2)
     default: DCMP_CASE(1)
@@ -954,12 +1071,17 @@ void launch_dcmp_f(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, con
 // memory a block may use.
 static size_t sweep_bytes(const SkewGeo &q, int mode, int D, int es) {
   const int R = D + 2;
-  return (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode, es) * es + 2 * (size_t)q.T * es;
+  size_t b = (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode, es) * es + 2 * (size_t)q.T * es;
+  if (q.split == 2)  // cluster exchange: xfull[W] barriers, xin (and din) [W][TIp]
+    b += (size_t)q.W * 8 + (size_t)q.W * q.TIp * es * (mode == SWEEP_BWD ? 1 : 2);
+  return b;
 }
 static int sweep_depth(const SkewGeo &q, int mode, int es) {
-  if (sweep_threads(q.T) > 1024) return 0;
-  for (int d : {8, 6, 4, 3, 2})
+  if (sweep_threads(q.T) > (q.split == 2 ? 512 : 1024)) return 0;
+  for (int d : {8, 6, 4, 3, 2}) {
+    if (q.split == 2 && (d == 6 || d == 3)) continue;  // depths built for the cluster form
     if (sweep_bytes(q, mode, d, es) <= 227 * 1024) return d;
+  }
   return 0;
 }
 template <int MODE, typename V>
@@ -968,16 +1090,41 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   constexpr int ES = (int)sizeof(V);
   const int d = sweep_depth(q, MODE, ES);
   const size_t bytes = sweep_bytes(q, MODE, d, ES);
-  const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
+  const int nty = q.nb / q.ntx;
+  const dim3 block((unsigned)sweep_threads(q.T));
   // The register budget follows the block size (255, 128 or 64 registers
   // for blocks of up to 256, 512 or 1024 threads).
   const int nt = sweep_threads(q.T);
   const int mt = nt <= 256 ? 256 : (nt <= 512 ? 512 : 1024);
+  if (q.split == 2) {
+    // one cluster of two thread blocks per preconditioner block
+    const dim3 grid((unsigned)q.ntx, (unsigned)((nty + 1) & ~1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = bytes; cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 1; at[0].val.clusterDim.y = 2; at[0].val.clusterDim.z = 1;
+    cfg.attrs = at; cfg.numAttrs = 1;
+    switch (d * 4096 + mt) {
+#define SWEEP_CASE2(DD, MT)                                                             \
+  case DD * 4096 + MT:                                                                  \
+    set_smem(k_sweep<DD, MODE, MT, V, 2>, bytes);                                       \
+    cudaLaunchKernelEx(&cfg, k_sweep<DD, MODE, MT, V, 2>, g, q, S, vin, vout, st);      \
+    break;
+      SWEEP_CASE2(8, 256) SWEEP_CASE2(4, 256) SWEEP_CASE2(2, 256)
+      SWEEP_CASE2(8, 512) SWEEP_CASE2(4, 512) SWEEP_CASE2(2, 512)
+#undef SWEEP_CASE2
+      default: return;  // rejected by cadmas_create (sweep_supported)
+    }
+    count_launch();
+    return;
+  }
+  const dim3 grid = skew_grid(q);
   switch (d * 4096 + mt) {
 #define SWEEP_CASE(DD, MT)                                                              \
   case DD * 4096 + MT:                                                                  \
-    set_smem(k_sweep<DD, MODE, MT, V>, bytes);                                          \
-    k_sweep<DD, MODE, MT, V><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);        \
+    set_smem(k_sweep<DD, MODE, MT, V, 1>, bytes);                                       \
+    k_sweep<DD, MODE, MT, V, 1><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);     \
     break;
     SWEEP_CASE(8, 256) SWEEP_CASE(6, 256) SWEEP_CASE(4, 256) SWEEP_CASE(3, 256) SWEEP_CASE(2, 256)
     SWEEP_CASE(8, 512) SWEEP_CASE(6, 512) SWEEP_CASE(4, 512) SWEEP_CASE(3, 512) SWEEP_CASE(2, 512)
@@ -988,10 +1135,14 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   count_launch();
 }
 bool sweep_supported(const SkewGeo &q) {
-  return sweep_depth(q, SWEEP_FWD, 8) > 0 && sweep_depth(q, SWEEP_BWD, 8) > 0;
+  const int tb = q.T * q.split;  // threads of the factorisation kernel
+  return sweep_depth(q, SWEEP_FWD, 8) > 0 && sweep_depth(q, SWEEP_BWD, 8) > 0 &&
+         (q.split == 1 || sweep_depth(q, SWEEP_FWD_AX, 8) > 0) && tb <= 1024 && ring_depth(7, tb, 8) > 0;
 }
 bool sweep_supported_f(const SkewGeo &q) {
-  return sweep_depth(q, SWEEP_FWD, 4) > 0 && sweep_depth(q, SWEEP_BWD, 4) > 0 && ring_depth(7, q.T, 4) > 0;
+  const int tb = q.T * q.split;
+  return sweep_depth(q, SWEEP_FWD, 4) > 0 && sweep_depth(q, SWEEP_BWD, 4) > 0 &&
+         (q.split == 1 || sweep_depth(q, SWEEP_FWD_AX, 4) > 0) && tb <= 1024 && ring_depth(7, tb, 4) > 0;
 }
 template <typename V>
 static void launch_fwd_t(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *y,

@@ -32,8 +32,12 @@ using SkewSysF = SkewSysT<float>;   // its FP32 copy for the inner solves of the
 // multiple of 4 (T = TIp*TJ entries per slab), so every slab, slab row and
 // group of 16 bytes of columns starts on a 16-byte boundary in double and
 // in float arrays and moves with one bulk copy.
+// With split = 2 a preconditioner block of TI x 2TJ columns is two layout
+// tiles (rows 2m and 2m+1 of tiles), swept by the two thread blocks of a
+// cluster.
 struct SkewGeo {
   int TI, TJ, TIp, T, W, ntx, nb;
+  int split;  // layout tiles per preconditioner block along y (1 or 2)
 };
 
 __host__ __device__ inline long long sys_at(long long slab, int c, int T, int t) {

@@ -140,7 +140,8 @@ struct orc_handle {
     return warp_tree(w);
   }
 
-  // The same tree over the slabs of the GPU solver's tile-skewed layout:
+  // The same tree over the slabs of the GPU solver's tile-skewed layout
+  // (layout tiles of TI x TJ columns, TJ halved with precond_split = 2):
   // tile b (x fastest), wavefront slab w = (k-2)+ti+tj, slab entry
   // t = ti + TIp*tj (TIp = TI rounded up to a multiple of 4; columns
   // ti >= TI are padding); lane l of a slab sums t = l, l+32, ... in order,
@@ -148,7 +149,8 @@ struct orc_handle {
   // the order of the dot products of VF_M1BCGS in the GPU library.
   template <class F> double gsum_skew(F f) const {
     const int TI = std::min(P.precond_ti > 0 ? P.precond_ti : NI - 2, NI - 2);
-    const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2);
+    const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2) /
+                   (P.precond_split == 2 ? 2 : 1);  // rows of a layout tile
     const int TIp = (TI + 3) & ~3;
     const int T = TIp * TJ, W = (NK - 2) + (TI - 1) + (TJ - 1);
     const int ntx = (NI - 2 + TI - 1) / TI, nb = ntx * ((NJ - 2 + TJ - 1) / TJ);

@@ -31,20 +31,16 @@ def _pkg():
 _lib = None
 
 
-def load():
-    global _lib
-    if _lib is None:
-        from . import build as _b  # noqa: F401
-    return _lib
-
-
 def _load_lib():
     global _lib
     if _lib is not None:
         return _lib
-    sys.path.insert(0, str(HERE))
-    import build as obuild  # oracle/build.py
-    sys.path.pop(0)
+    # oracle/build.py under its own module name: the package has a build.py
+    # too, and whichever is imported first as `build` would shadow the other
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("cadmas_oracle_build", HERE / "build.py")
+    obuild = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(obuild)
     obuild.build()
     P = _pkg()
     lib = C.CDLL(str(HERE / "liboracle.so"))

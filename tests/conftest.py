@@ -49,11 +49,5 @@ def gpu_lib(pkg):
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    import importlib
-    sys.path.insert(0, str(PKG_DIR))
-    try:
-        import build as pbuild
-    finally:
-        sys.path.pop(0)
-    pbuild.build()
+    pkg.build_library()
     return pkg.load_library()

@@ -20,12 +20,7 @@ def test_header_lists_entry_points():
 
 
 def test_library_exports_all(pkg):
-    import sys
-    sys.path.insert(0, str(ROOT / "multiscale-and-multiphysics-integrated-simulator-for-tsunami_b200"))
-    import build as pbuild
-    sys.path.pop(0)
-    pbuild.build()
-    lib = ctypes.CDLL(str(pbuild.LIB))
+    lib = ctypes.CDLL(str(pkg.build_library()))
     missing = [n for n in header_functions() if not hasattr(lib, n)]
     assert not missing, missing
     assert set(pkg.EXPORTED) <= set(header_functions())

@@ -137,6 +137,37 @@ def test_wave_maker_flume_tiles_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 16, check_every=8, precond_ti=16, precond_tj=2)
 
 
+@pytest.mark.parametrize("case,over", [
+    ("flume", dict(precond_ti=16, precond_tj=4, precond_split=2)),
+    ("flume10", dict(precond_ti=24, precond_tj=8, precond_split=2)),
+    ("dam", dict(precond_split=2)),
+    ("tank", dict(precond_ti=6, precond_tj=4, precond_split=2)),
+])
+def test_split_preconditioner_blocks_bitwise(gpu_lib, pkg, orc, case, over):
+    """Each preconditioner block swept by a cluster of two thread blocks
+    that pass their boundary row through distributed shared memory: the
+    same MILU as one block per preconditioner block, bit for bit (the dot
+    products sum over the half-height slabs, as the oracle does).
+    flume10: 10 rows in y with 8-row blocks, so the top block has one
+    4-row-or-less layout tile and its cluster partner has no tile."""
+    if case == "flume":
+        c = pkg.cases.porous_flume(nx=96, ny=4, nz=64, block=(1.2, 1.4, 0.6), sponge_width=0.4)
+        pkg.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
+        pkg.cases.wave_maker(c, 0.08, 1.5, 0.5)
+        steps = 12
+    elif case == "flume10":
+        c = pkg.cases.porous_flume(nx=72, ny=10, nz=64, block=(0.8, 1.0, 0.6), sponge_width=0.3)
+        pkg.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
+        steps = 8
+    elif case == "dam":
+        c = pkg.cases.dam_break()
+        steps = 10
+    else:
+        c = pkg.cases.random_tank(4, ny=10)
+        steps = 10
+    run_pair(pkg, orc, c, steps, check_every=steps // 2, **over)
+
+
 def test_fortran_entry_point(gpu_lib, pkg, orc):
     """vf_step_gpu_ (host arrays in, host arrays out) equals cadmas_step."""
     c = pkg.cases.random_tank(3)
