@@ -95,7 +95,7 @@ def build_case(args):
 
 def params_for(args):
     return dict(cgepsr=1.0e-8 if getattr(args, "case", "flume") == "beach" else 1.0e-10,
-                precond_ti=args.ti, precond_tj=args.tj,
+                precond_ti=args.ti, precond_tj=args.tj, precond_split=getattr(args, "split", 1),
                 solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
                 warm_start=1 if getattr(args, "guess", "zero") == "previous" else 0)
 
@@ -455,6 +455,8 @@ def main():
     ap.add_argument("--solver", choices=["fp64", "mixed"], default="fp64",
                     help="pressure solver: the reference's FP64 MILU-BiCGSTAB, or FP32 inner solves "
                          "under FP64 refinement")
+    ap.add_argument("--split", type=int, choices=[1, 2], default=1,
+                    help="2: each preconditioner block swept by a cluster of two thread blocks")
     ap.add_argument("--members", type=int, default=8, help="ensemble members (--case ensemble)")
     ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
     ap.add_argument("--case", choices=["flume", "beach", "ensemble"], default="flume",

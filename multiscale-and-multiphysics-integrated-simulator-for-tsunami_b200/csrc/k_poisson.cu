@@ -415,16 +415,17 @@ __device__ __forceinline__ unsigned mapa(unsigned addr, unsigned rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(addr), "r"(rank));
   return r;
 }
-__device__ __forceinline__ void st_cluster(unsigned addr, double v) {
-  asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+// Store into another CTA of the cluster and credit the stored bytes to an
+// mbarrier there (transaction count); no release of earlier stores.
+__device__ __forceinline__ void st_async(unsigned addr, double v, unsigned mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];\n" ::"r"(addr), "d"(v),
+               "r"(mbar)
+               : "memory");
 }
-__device__ __forceinline__ void st_cluster(unsigned addr, float v) {
-  asm volatile("st.shared::cluster.f32 [%0], %1;\n" ::"r"(addr), "f"(v) : "memory");
-}
-// Arrive on an mbarrier of another CTA of the cluster, releasing this
-// thread's earlier stores to the cluster.
-__device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(addr) : "memory");
+__device__ __forceinline__ void st_async(unsigned addr, float v, unsigned mbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];\n" ::"r"(addr), "f"(v),
+               "r"(mbar)
+               : "memory");
 }
 __device__ __forceinline__ bool mbar_try_cluster(unsigned bar, unsigned parity) {
   unsigned ok;
@@ -506,10 +507,11 @@ __global__ void __launch_bounds__(MAXT, 1)
 
   // Cluster exchange (CS = 2).  The forward sweeps need, on row 0 of the
   // upper tile, the result and DD of row TJ-1 of the lower tile at the
-  // same k; the backward sweep needs the reverse.  The sending row writes
-  // its values of step u into slot u of the receiver's xin/din and
-  // arrives on the receiver's xfull[u] (one arrival per column of the row,
-  // every step); a slot is written once per sweep.
+  // same k; the backward sweep needs the reverse.  The sending row stores
+  // its values of step u into slot u of the receiver's xin/din with
+  // st.async, each store crediting its bytes to the receiver's xfull[u],
+  // which the receiver armed at start-up for one full row (TIp values of x,
+  // and of DD for the forward sweeps); a slot is written once per sweep.
   const int NX = q.W;                                   // slots: steps of a tile at most
   unsigned long long *xfull = reinterpret_cast<unsigned long long *>(xb + 2 * T);
   V *xin = reinterpret_cast<V *>(xfull + NX);
@@ -540,8 +542,13 @@ __global__ void __launch_bounds__(MAXT, 1)
     for (int r = 0; r < R; ++r) mbar_init(smem_u32(bar + r), 1);
     s_abort[0] = s_abort[1] = 0;
   }
-  if (CS == 2 && recv)
-    for (int u = tid; u < NX; u += blockDim.x) mbar_init(smem_u32(xfull + u), (unsigned)TIp);
+  if (CS == 2 && recv) {
+    const unsigned row_bytes = (unsigned)(TIp * ES * (MODE == SWEEP_BWD ? 1 : 2));
+    for (int u = tid; u < NX; u += blockDim.x) {
+      mbar_init(smem_u32(xfull + u), 1u);
+      mbar_expect_tx(smem_u32(xfull + u), row_bytes);
+    }
+  }
   if (MODE == SWEEP_FWD_AX) {  // halo values of absent neighbours stay 0 (ghost layer)
     const int nh = 2 * halo_span(q, ES) + 2 * TIp;
     for (int r = 0; r < R; ++r)
@@ -689,9 +696,9 @@ __global__ void __launch_bounds__(MAXT, 1)
         }
         vp += vstep;
         if (CS == 2 && srow) {  // this step's boundary-row values to the partner tile
-          st_cluster(r_xin + (unsigned)(((size_t)s * TIp + t.ti) * ES), xcur);
-          if (MODE != SWEEP_BWD) st_cluster(r_din + (unsigned)(((size_t)s * TIp + t.ti) * ES), act ? dd : V(0));
-          mbar_arrive_remote(r_full + 8u * (unsigned)s);
+          const unsigned off = (unsigned)(((size_t)s * TIp + t.ti) * ES), fb = r_full + 8u * (unsigned)s;
+          st_async(r_xin + off, xcur, fb);
+          if (MODE != SWEEP_BWD) st_async(r_din + off, act ? dd : V(0), fb);
         }
         // prepare step s+1
         if (!ready) {
