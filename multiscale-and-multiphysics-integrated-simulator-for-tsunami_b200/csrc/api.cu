@@ -132,11 +132,11 @@ struct cadmas_handle {
   // forward-sweep result
   SkewGeo q;
   SkewSys S;
-  double *tt_sl = nullptr, *bb_sl = nullptr;
+  double *bb_sl = nullptr;
   // FP32 system and inner-solve vectors of the mixed solver (solver 1)
   SkewSysF Sf{nullptr, nullptr};
   float *bf = nullptr, *xf = nullptr, *r0f = nullptr, *rrf = nullptr, *pvf = nullptr, *apf = nullptr,
-        *aef = nullptr, *ttf = nullptr, *y2f = nullptr;
+        *aef = nullptr, *y2f = nullptr;
   long long mixed_outer = 0, mixed_fallback = 0;  // refinement passes and FP64 fallbacks so far
   int warm_now = 0;  // the next solve starts from the previous solution (warm_start 1)
   bool have_prev = false;  // xw holds a converged solution of an earlier step
@@ -305,8 +305,8 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   launch_pivot_check(s, st);
   TE();
   // YY = MINV*BB, BNORM = (YY,YY)
-  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, h->bb_sl, nullptr, h->tt_sl, st, h->y2); TE();
-  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->y2, st); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, h->bb_sl, nullptr, st, h->y2); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->y2, st); TE();
   TB(CADMAS_STAGE_DOT);
   launch_dot(s, q, ic, h->y2, h->y2, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_BNORM, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -316,8 +316,8 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   launch_spmv(s, g, q, S, h->xw, h->y2, st);
   launch_bmy(s, q, ic, h->bb_sl, h->y2, st);
   TE();
-  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, h->y2, nullptr, h->tt_sl, st, h->y2); TE();
-  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->r0, st); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, h->y2, nullptr, st, h->y2); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->r0, st); TE();
   TB(CADMAS_STAGE_DOT);
   launch_dot(s, q, ic, h->r0, h->r0, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_START, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -328,16 +328,16 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   for (int guard = 0; guard < 100000; ++guard) {
     for (int b = 0; b < batch; ++b) {
       // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP
-      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, nullptr, h->pv, h->tt_sl, st, h->y2); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->ap, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, nullptr, h->pv, st, h->y2); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->ap, st); TE();
       TB(CADMAS_STAGE_DOT);
       launch_dot(s, q, ic, h->r0, h->ap, nullptr, nullptr, h->rb0, nullptr, st);
       launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
       TB(CADMAS_STAGE_VEC); launch_axpy_rr(s, q, ic, h->ap, h->rr, st); TE();
       // AE = MINV*(A*RR); OMEGA = (RR,AE)/(AE,AE)
-      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, nullptr, h->rr, h->tt_sl, st, h->y2); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->tt_sl, h->ae, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd(s, g, q, S, nullptr, h->rr, st, h->y2); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd(s, g, q, S, h->ae, st); TE();
       TB(CADMAS_STAGE_DOT);
       launch_dot(s, q, ic, h->rr, h->ae, h->ae, h->ae, h->rb0, h->rb1, st);
       launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -390,8 +390,8 @@ static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
   for (float *z : zl) CK(cudaMemsetAsync(z, 0, vb, s));
   CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
   // YY = MINV*BB, BNORM = (YY,YY); with XW = 0, R0 = YY and S = BNORM
-  TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, h->bf, nullptr, h->ttf, st, h->y2f); TE();
-  TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->ttf, h->r0f, st); TE();
+  TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, h->bf, nullptr, st, h->y2f); TE();
+  TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->r0f, st); TE();
   TB(CADMAS_STAGE_DOT);
   launch_dot_t<float>(s, q, ic, h->r0f, h->r0f, nullptr, nullptr, h->rb0, nullptr, st);
   launch_fin(s, FIN_BNORM, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -401,15 +401,15 @@ static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
   int batch = std::max(2, std::min(h->last_iter, 64));
   for (int guard = 0; guard < 100000; ++guard) {
     for (int b = 0; b < batch; ++b) {
-      TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->pvf, h->ttf, st, h->y2f); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->ttf, h->apf, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->pvf, st, h->y2f); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->apf, st); TE();
       TB(CADMAS_STAGE_DOT);
       launch_dot_t<float>(s, q, ic, h->r0f, h->apf, nullptr, nullptr, h->rb0, nullptr, st);
       launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
       TB(CADMAS_STAGE_VEC); launch_axpy_rr_t<float>(s, q, ic, h->apf, h->rrf, st); TE();
-      TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->rrf, h->ttf, st, h->y2f); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->ttf, h->aef, st); TE();
+      TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->rrf, st, h->y2f); TE();
+      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->aef, st); TE();
       TB(CADMAS_STAGE_DOT);
       launch_dot_t<float>(s, q, ic, h->rrf, h->aef, h->aef, h->aef, h->rb0, h->rb1, st);
       launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
@@ -773,7 +773,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   {
     const size_t nsl = h->nsl;
     AL(h->S.sys, (size_t)SYS_N * nsl);
-    AL(h->S.indc, nsl); AL(h->tt_sl, nsl); AL(h->bb_sl, nsl);
+    AL(h->S.indc, nsl); AL(h->bb_sl, nsl);
     AL(h->xw, nsl); AL(h->y2, nsl); AL(h->r0, nsl); AL(h->rr, nsl);
     AL(h->pv, nsl); AL(h->ap, nsl); AL(h->ae, nsl);
     if (p->solver == 1) {
@@ -783,7 +783,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
       }
       AL(h->Sf.sys, (size_t)SYS_N * nsl);
       AL(h->bf, nsl); AL(h->xf, nsl); AL(h->r0f, nsl); AL(h->rrf, nsl); AL(h->pvf, nsl);
-      AL(h->apf, nsl); AL(h->aef, nsl); AL(h->ttf, nsl); AL(h->y2f, nsl);
+      AL(h->apf, nsl); AL(h->aef, nsl); AL(h->y2f, nsl);
     } else if (p->solver != 0) {
       rc = rc ? rc : CADMAS_EINVAL;
     }
@@ -815,7 +815,7 @@ int cadmas_destroy(cadmas_handle *h) {
   double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
                   h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
                   h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->rb0, h->rb1, h->dres,
-                  h->S.sys, h->tt_sl, h->bb_sl};
+                  h->S.sys, h->bb_sl};
   for (double *q : dl) if (q) cudaFree(q);
   for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) if (h->vel[b][c]) cudaFree(h->vel[b][c]);
   for (double *q : h->wk) if (q) cudaFree(q);
@@ -827,7 +827,7 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_int) cudaFreeHost(h->h_int);
   if (h->h_res) cudaFreeHost(h->h_res);
   for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
-  for (float *q : {h->Sf.sys, h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->ttf, h->y2f})
+  for (float *q : {h->Sf.sys, h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->y2f})
     if (q) cudaFree(q);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;

@@ -102,6 +102,17 @@ inline unsigned row_blocks(const Geo &g) {
     }                \
   }
 
+// Programmatic dependent launch.  The solver's kernels are launched with
+// programmatic stream serialisation (launch_pdl), so a kernel may be
+// scheduled while the previous kernel of the stream still runs.  Each of
+// them starts here: wait until the previous kernel has completed and its
+// writes are visible, then let the next kernel be scheduled.  Without a
+// programmatic dependency the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // Warp tree: lane 0 ends with ((s0+s16)+(s8+s24))+... via shfl_down.
 __device__ __forceinline__ double warp_tree(double s) {
   for (int off = 16; off >= 1; off >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, off);

@@ -219,6 +219,7 @@ __device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, in
 // now -1) instead of X0.
 __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
                           double *bsl, double *xsl, int warm) {
+  pdl_enter();
   const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int t = (int)(e % q.T);
@@ -236,8 +237,11 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
       bv = A_.bb[c];
       xv = warm ? (ic != -1 ? xsl[e] : 0.0) : X0[c];
     }
-    for (int c = 0; c < 7; ++c) S.sys[sys_at(bw, c, q.T, t)] = v[c];
+    constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
+#pragma unroll
+    for (int c = 0; c < 7; ++c) S.sys[sys_at(bw, cs[c], q.T, t)] = v[c];
     S.sys[sys_at(bw, SYS_DD, q.T, t)] = 0.0;
+    S.sys[sys_at(bw, SYS_T, q.T, t)] = 0.0;
     S.indc[e] = ic;
     bsl[e] = bv;
     xsl[e] = xv;
@@ -275,6 +279,7 @@ __device__ __forceinline__ void skew_fetch(double *dst, const Geo &g, const Skew
 // 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK; DD is written in the skewed layout.
 template <int D, typename V>
 __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
+  pdl_enter();
   constexpr int NV = 7, R = D + 3;
   const int TIp = q.TIp, TJl = q.TJ, Tl = q.T;      // layout tile
   const int TJb = TJl * q.split, Tb = TIp * TJb;    // preconditioner block
@@ -296,8 +301,9 @@ __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
       const long long slab = slab0 + s, e = slab * Tl + tl;
       const V *sy = S.sys + sys_at(slab, 0, Tl, tl);
       const int sl = s % R;
+      constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
 #pragma unroll
-      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)c * Tl);
+      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)cs[c] * Tl);
       cp_async4(&rg.ind(sl, tid), S.indc + e);
     }
     cp_commit();
@@ -460,7 +466,9 @@ __device__ __forceinline__ void cluster_barrier() {
 //   SWEEP_FWD_AX  T = MINV_L * (A*P), A*P formed on the fly (VF_MZAX
 //                 then VF_MZFRWD: vf_mzax.f:46-53, vf_mzfrwd.f)
 //   SWEEP_BWD     X = MINV_U * T;  vf_mzbkwd.f
-// Results are written in the skewed layout.  Forward step s visits
+// The forward sweeps write T into the system block (SYS_T), where the
+// backward sweep's one bulk copy per step finds it with AUI..DD; the
+// backward sweep writes X in the skewed layout.  Forward step s visits
 // k = 2+s-ti-tj, backward step s visits k = NK-1-(s-ri-rj) (ri, rj the
 // distances from the far corner), so step s of every thread is one slab.
 // A cell is computed where DD != 0: MZDCMP gives DD = 0 exactly on
@@ -479,6 +487,7 @@ __device__ __forceinline__ void cluster_barrier() {
 template <int D, int MODE, int MAXT, typename V, int CS>
 __global__ void __launch_bounds__(MAXT, 1)
     k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st) {
+  pdl_enter();
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
   // preconditioner block; every block of a cluster runs through the two
   // cluster barriers below, so none returns early.
@@ -496,6 +505,11 @@ __global__ void __launch_bounds__(MAXT, 1)
   const int Tc = (T + 31) & ~31;
   constexpr int ES = (int)sizeof(V);
   const int SS = sweep_slot(q, MODE, ES);
+  // slot offsets of the system arrays
+  constexpr int SF = sweep_sys_first(MODE) - sweep_sys_dst(MODE);
+  const int oDD = (SYS_DD - SF) * T, oAD = (SYS_AD - SF) * T, oALI = (SYS_ALI - SF) * T,
+            oALJ = (SYS_ALJ - SF) * T, oALK = (SYS_ALK - SF) * T, oAUI = (SYS_AUI - SF) * T,
+            oAUJ = (SYS_AUJ - SF) * T, oAUK = (SYS_AUK - SF) * T;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm);
   V *ring = reinterpret_cast<V *>(sm + ((R + 1) & ~1));
   V *xb = ring + (size_t)R * SS;
@@ -596,8 +610,10 @@ __global__ void __launch_bounds__(MAXT, 1)
   const bool col = t.valid && !producer;
   const int hl = halo_left(q, ES) + TIp * t.tj + halo_lofs(q, ES), hr = halo_right(q, ES) + TIp * t.tj,
             hd = halo_down(q, ES) + t.ti, hu = halo_up(q, ES) + t.ti;
-  V *vp = vout + ((long long)b * q.W + (MODE == SWEEP_BWD ? nsteps - 1 : 0)) * T + tid;
-  const long long vstep = (MODE == SWEEP_BWD) ? -(long long)T : (long long)T;
+  // forward: T into the system block; backward: X
+  V *vp = (MODE == SWEEP_BWD) ? vout + ((long long)b * q.W + nsteps - 1) * T + tid
+                              : S.sys + sys_at((long long)b * q.W, SYS_T, T, tid);
+  const long long vstep = (MODE == SWEEP_BWD) ? -(long long)T : (long long)SYS_N * T;
 
   // Prepared values of the next step.
   bool act = false;             // the column has a cell at this step
@@ -612,7 +628,7 @@ __global__ void __launch_bounds__(MAXT, 1)
     if (!act) return;
     if (MODE == SWEEP_FWD_AX) {
       const int k = 2 + s - t.ti - t.tj;
-      const V d = cs[7 * T + tid], pc = cs[8 * T + tid];
+      const V d = cs[oDD + tid], pc = cs[8 * T + tid];
       if (d != V(0)) {
         const V pxm = ex0 ? cs[hl] : ps[8 * T + tid - 1];
         const V pym = ey0 ? cs[hd] : ps[8 * T + tid - TIp];
@@ -620,29 +636,29 @@ __global__ void __launch_bounds__(MAXT, 1)
         const V pxp = ex1 ? cs[hr] : ns[8 * T + tid + 1];
         const V pyp = ey1 ? cs[hu] : ns[8 * T + tid + TIp];
         const V pzp = (k < g.NK - 1) ? ns[8 * T + tid] : V(0);
-        y0 = cs[tid] * pc + cs[T + tid] * pxm + cs[2 * T + tid] * pym + cs[3 * T + tid] * pzm +
-             cs[4 * T + tid] * pxp + cs[5 * T + tid] * pyp + cs[6 * T + tid] * pzp;
-        const V d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : V(0);
-        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
-        c1 = cs[T + tid] * d1;
-        c2 = cs[2 * T + tid] * d2;
-        c3 = cs[3 * T + tid] * dk1;
+        y0 = cs[oAD + tid] * pc + cs[oALI + tid] * pxm + cs[oALJ + tid] * pym + cs[oALK + tid] * pzm +
+             cs[oAUI + tid] * pxp + cs[oAUJ + tid] * pyp + cs[oAUK + tid] * pzp;
+        const V d1 = (t.ti > 0) ? ps[oDD + tid - 1] : V(0);
+        const V d2 = (t.tj > 0) ? ps[oDD + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
+        c1 = cs[oALI + tid] * d1;
+        c2 = cs[oALJ + tid] * d2;
+        c3 = cs[oALK + tid] * dk1;
       }
       dd = d; dk1 = d; pk1 = pc;
     } else if (MODE == SWEEP_FWD) {
-      const V d = cs[7 * T + tid];
+      const V d = cs[oDD + tid];
       if (d != V(0)) {
-        const V d1 = (t.ti > 0) ? ps[7 * T + tid - 1] : V(0);
-        const V d2 = (t.tj > 0) ? ps[7 * T + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
+        const V d1 = (t.ti > 0) ? ps[oDD + tid - 1] : V(0);
+        const V d2 = (t.tj > 0) ? ps[oDD + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
         y0 = cs[tid];
-        c1 = cs[T + tid] * d1;
-        c2 = cs[2 * T + tid] * d2;
-        c3 = cs[3 * T + tid] * dk1;
+        c1 = cs[oALI + tid] * d1;
+        c2 = cs[oALJ + tid] * d2;
+        c3 = cs[oALK + tid] * dk1;
       }
       dd = d; dk1 = d;
     } else {
-      dd = cs[4 * T + tid];
-      if (dd != V(0)) { y0 = cs[tid]; c1 = cs[T + tid]; c2 = cs[2 * T + tid]; c3 = cs[3 * T + tid]; }
+      dd = cs[oDD + tid];
+      if (dd != V(0)) { y0 = cs[tid]; c1 = cs[oAUI + tid]; c2 = cs[oAUJ + tid]; c3 = cs[oAUK + tid]; }
     }
   };
   auto slot_ptr = [&](int r) -> const V * { return ring + (size_t)r * SS; };
@@ -770,6 +786,7 @@ __device__ __forceinline__ V skew_ax(const Geo &g, const SkewGeo &q, const SkewS
 // Y = A X on INDC != -1 (VF_MZAX); Y untouched elsewhere.
 template <typename V>
 __global__ void k_spmv(Geo g, SkewGeo q, SkewSysT<V> S, const V *X, V *Y, const SolveState *st) {
+  pdl_enter();
   if (st && st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (S.indc[e] != -1) Y[e] = skew_ax(g, q, S, X, e);
@@ -778,6 +795,7 @@ __global__ void k_spmv(Geo g, SkewGeo q, SkewSysT<V> S, const V *X, V *Y, const 
 
 // Y = B - Y on INDC != -1 (vf_m1bcgs.f:124-132)
 __global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, const SolveState *st) {
+  pdl_enter();
   if (st && st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) Y[e] = B[e] - Y[e];
@@ -793,6 +811,7 @@ __global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, co
 template <typename V>
 __global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, const V *x1, const V *y1,
                       double *rb0, double *rb1, const SolveState *st) {
+  pdl_enter();
   if (st && st->done) return;
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
@@ -809,6 +828,7 @@ __global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, cons
 // RR = R0, PP = R0
 template <typename V>
 __global__ void k_copy2(SkewGeo q, const int *INDC, const V *R0, V *RR, V *PP, const SolveState *st) {
+  pdl_enter();
   if (st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) { RR[e] = R0[e]; PP[e] = R0[e]; }
@@ -818,6 +838,7 @@ __global__ void k_copy2(SkewGeo q, const int *INDC, const V *R0, V *RR, V *PP, c
 // RR = RR - ALPHA*AP (vf_m1bcgs.f:181-189)
 template <typename V>
 __global__ void k_axpy_rr(SkewGeo q, const int *INDC, const V *AP, V *RR, const SolveState *st) {
+  pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha;
   SLAB_LOOP_BEGIN(q)
@@ -830,6 +851,7 @@ __global__ void k_axpy_rr(SkewGeo q, const int *INDC, const V *AP, V *RR, const 
 template <typename V>
 __global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, const V *R0, V *XW, V *RR,
                          double *rb0, double *rb1, const SolveState *st) {
+  pdl_enter();
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
   double s0 = 0.0, s1 = 0.0;
@@ -850,6 +872,7 @@ __global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, c
 // PP = RR + BETA*(PP - OMEGA*AP) (vf_m1bcgs.f:229-238)
 template <typename V>
 __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V *PP, const SolveState *st) {
+  pdl_enter();
   if (st->done) return;
   const double beta = st->beta, omega = st->omega;
   SLAB_LOOP_BEGIN(q)
@@ -858,24 +881,29 @@ __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V 
 }
 
 // ------------------------------------------- mixed-precision conversions
-// FP32 copy of the 7 coefficients (DD comes from the FP32 factorisation).
+// FP32 copy of the 7 coefficients (DD comes from the FP32 factorisation,
+// T from the FP32 forward sweeps).
 __global__ void k_sys_to_f(SkewGeo q, const double *sys, float *sysf) {
+  pdl_enter();
   const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const long long slab = e / q.T;
     const int t = (int)(e - slab * q.T);
+    constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
 #pragma unroll
-    for (int c = 0; c < SYS_DD; ++c) sysf[sys_at(slab, c, q.T, t)] = (float)sys[sys_at(slab, c, q.T, t)];
+    for (int c = 0; c < 7; ++c) sysf[sys_at(slab, cs[c], q.T, t)] = (float)sys[sys_at(slab, cs[c], q.T, t)];
   }
 }
 // RF = R * scale on INDC != -1 (the right-hand side of an inner solve)
 __global__ void k_scale_to_f(SkewGeo q, const int *INDC, const double *R, double scale, float *RF) {
+  pdl_enter();
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) RF[e] = (float)(R[e] * scale);
   SLAB_LOOP_END
 }
 // X = X + D * inv_scale on INDC != -1 (the correction of an inner solve)
 __global__ void k_add_f(SkewGeo q, const int *INDC, const float *D, double inv_scale, double *X) {
+  pdl_enter();
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) X[e] = X[e] + (double)D[e] * inv_scale;
   SLAB_LOOP_END
@@ -884,6 +912,7 @@ __global__ void k_add_f(SkewGeo q, const int *INDC, const float *D, double inv_s
 // X0 = XW on INDC != -1 when ITER >= 0 (vf_m1bcgs.f:251-261), back to the
 // standard layout.
 __global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double *X0, const SolveState *st) {
+  pdl_enter();
   if (st->iter < 0) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) {
@@ -898,6 +927,7 @@ __global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double
 // ||b-Ax||^2 and ||b||^2 slab partials (diagnostic of the metric)
 __global__ void k_relres(Geo g, SkewGeo q, SkewSys S, const double *B, const double *X, double *rb0,
                          double *rb1) {
+  pdl_enter();
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
   SLAB_LOOP_BEGIN(q)
@@ -917,6 +947,7 @@ __global__ void k_relres(Geo g, SkewGeo q, SkewSys S, const double *B, const dou
 __global__ void k_fin(int mode, const double *rb0, const double *rb1, long long nrows,
                       SolveState *st, double *out, double epsa2, double epsr2, double div2,
                       int icgmax) {
+  pdl_enter();
   if (mode < FIN_ALPHA && mode != FIN_STORE && mode != FIN_RELRES && st->done) return;
   if (mode >= FIN_ALPHA && st->done) return;
   double a = block_final(rb0, nrows);
@@ -970,6 +1001,7 @@ __global__ void k_fin(int mode, const double *rb0, const double *rb1, long long 
 
 // Factorisation failure ends the solve with ITER = -1 (vf_m1bcgs.f:101-102).
 __global__ void k_pivot_check(SolveState *st) {
+  pdl_enter();
   if (st->pivot_bad) { st->iter = -1; st->done = 1; }
 }
 
@@ -1036,6 +1068,26 @@ static int ring_depth(int NV, int T, size_t es) {
     if (ring_bytes(NV, T, d + 3, es) <= cap) return d;
   return 0;
 }
+// Launch a kernel that starts with pdl_enter() with programmatic stream
+// serialisation (cluster dimensions optional).
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, int cluster_y,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  int na = 1;
+  if (cluster_y > 1) {
+    at[1].id = cudaLaunchAttributeClusterDimension;
+    at[1].val.clusterDim.x = 1; at[1].val.clusterDim.y = (unsigned)cluster_y; at[1].val.clusterDim.z = 1;
+    na = 2;
+  }
+  cfg.attrs = at; cfg.numAttrs = na;
+  cudaLaunchKernelEx(&cfg, kern, ((KArgs)args)...);
+  count_launch();
+}
 template <class K> static void set_smem(K kern, size_t bytes) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
@@ -1046,8 +1098,7 @@ void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr
                     const SkewSys &S, const double *x0, double *bsl, double *xsl, int warm) {
   const long long n = (long long)q.nb * q.W * q.T;
   const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-  k_to_skew<<<blocks, 256, 0, s>>>(g, q, a, indc, S, x0, bsl, xsl, warm);
-  count_launch();
+  launch_pdl(k_to_skew, dim3(blocks), dim3(256), 0, s, 1, g, q, a, indc, S, x0, bsl, xsl, warm);
 }
 template <typename V>
 static void launch_dcmp_t(cudaStream_t s, const Geo &g, const SkewGeo &q, V U, const SkewSysT<V> &S, int *pivot_bad) {
@@ -1059,13 +1110,12 @@ static void launch_dcmp_t(cudaStream_t s, const Geo &g, const SkewGeo &q, V U, c
 #define DCMP_CASE(DD)                                                                    \
   case DD:                                                                               \
     set_smem(k_dcmp<DD, V>, bytes);                                                      \
-    k_dcmp<DD, V><<<grid, T, bytes, s>>>(g, q, U, S, pivot_bad);                         \
+    launch_pdl(k_dcmp<DD, V>, grid, dim3(T), bytes, s, 1, g, q, U, S, pivot_bad);              \
     break;
     DCMP_CASE(8) DCMP_CASE(4) DCMP_CASE(2)
     default: DCMP_CASE(1)
 #undef DCMP_CASE
   }
-  count_launch();
 }
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad) {
   launch_dcmp_t<double>(s, g, q, U, S, pivot_bad);
@@ -1106,24 +1156,17 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   if (q.split == 2) {
     // one cluster of two thread blocks per preconditioner block
     const dim3 grid((unsigned)q.ntx, (unsigned)((nty + 1) & ~1));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = bytes; cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = 1; at[0].val.clusterDim.y = 2; at[0].val.clusterDim.z = 1;
-    cfg.attrs = at; cfg.numAttrs = 1;
     switch (d * 4096 + mt) {
 #define SWEEP_CASE2(DD, MT)                                                             \
   case DD * 4096 + MT:                                                                  \
     set_smem(k_sweep<DD, MODE, MT, V, 2>, bytes);                                       \
-    cudaLaunchKernelEx(&cfg, k_sweep<DD, MODE, MT, V, 2>, g, q, S, vin, vout, st);      \
+    launch_pdl(k_sweep<DD, MODE, MT, V, 2>, grid, block, bytes, s, 2, g, q, S, vin, vout, st); \
     break;
       SWEEP_CASE2(8, 256) SWEEP_CASE2(4, 256) SWEEP_CASE2(2, 256)
       SWEEP_CASE2(8, 512) SWEEP_CASE2(4, 512) SWEEP_CASE2(2, 512)
 #undef SWEEP_CASE2
       default: return;  // rejected by cadmas_create (sweep_supported)
     }
-    count_launch();
     return;
   }
   const dim3 grid = skew_grid(q);
@@ -1131,7 +1174,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
 #define SWEEP_CASE(DD, MT)                                                              \
   case DD * 4096 + MT:                                                                  \
     set_smem(k_sweep<DD, MODE, MT, V, 1>, bytes);                                       \
-    k_sweep<DD, MODE, MT, V, 1><<<grid, block, bytes, s>>>(g, q, S, vin, vout, st);     \
+    launch_pdl(k_sweep<DD, MODE, MT, V, 1>, grid, block, bytes, s, 1, g, q, S, vin, vout, st); \
     break;
     SWEEP_CASE(8, 256) SWEEP_CASE(6, 256) SWEEP_CASE(4, 256) SWEEP_CASE(3, 256) SWEEP_CASE(2, 256)
     SWEEP_CASE(8, 512) SWEEP_CASE(6, 512) SWEEP_CASE(4, 512) SWEEP_CASE(3, 512) SWEEP_CASE(2, 512)
@@ -1139,7 +1182,6 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
 #undef SWEEP_CASE
     default: return;  // rejected by cadmas_create (sweep_supported)
   }
-  count_launch();
 }
 bool sweep_supported(const SkewGeo &q) {
   const int tb = q.T * q.split;  // threads of the factorisation kernel
@@ -1153,36 +1195,34 @@ bool sweep_supported_f(const SkewGeo &q) {
 }
 template <typename V>
 static void launch_fwd_t(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *y,
-                         const V *spmv_x, V *tout, SolveState *st, V *ybuf) {
+                         const V *spmv_x, SolveState *st, V *ybuf) {
   if (spmv_x && sweep_depth(q, SWEEP_FWD_AX, (int)sizeof(V)) == 0) {
     // Ring of the fused sweep too large for this tile: SpMV first.
     launch_spmv_t<V>(s, g, q, S, spmv_x, ybuf, st);
     y = ybuf;
     spmv_x = nullptr;
   }
-  if (spmv_x) launch_sweep<SWEEP_FWD_AX, V>(s, g, q, S, spmv_x, tout, st);
-  else launch_sweep<SWEEP_FWD, V>(s, g, q, S, y, tout, st);
+  if (spmv_x) launch_sweep<SWEEP_FWD_AX, V>(s, g, q, S, spmv_x, nullptr, st);
+  else launch_sweep<SWEEP_FWD, V>(s, g, q, S, y, nullptr, st);
 }
 void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
-                const double *spmv_x, double *tout, SolveState *st, double *ybuf) {
-  launch_fwd_t<double>(s, g, q, S, y, spmv_x, tout, st, ybuf);
+                const double *spmv_x, SolveState *st, double *ybuf) {
+  launch_fwd_t<double>(s, g, q, S, y, spmv_x, st, ybuf);
 }
 void launch_fwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *y,
-                  const float *spmv_x, float *tout, SolveState *st, float *ybuf) {
-  launch_fwd_t<float>(s, g, q, S, y, spmv_x, tout, st, ybuf);
+                  const float *spmv_x, SolveState *st, float *ybuf) {
+  launch_fwd_t<float>(s, g, q, S, y, spmv_x, st, ybuf);
 }
-void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
-                double *x, SolveState *st) {
-  launch_sweep<SWEEP_BWD, double>(s, g, q, S, tin, x, st);
+void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, double *x, SolveState *st) {
+  launch_sweep<SWEEP_BWD, double>(s, g, q, S, nullptr, x, st);
 }
-void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *tin,
-                  float *x, SolveState *st) {
-  launch_sweep<SWEEP_BWD, float>(s, g, q, S, tin, x, st);
+void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, float *x, SolveState *st) {
+  launch_sweep<SWEEP_BWD, float>(s, g, q, S, nullptr, x, st);
 }
 static inline unsigned slab_blocks(const SkewGeo &q) {
   return (unsigned)(((long long)q.nb * q.W + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK);
 }
-#define SL(kern, ...) (kern<<<slab_blocks(q), ROW_THREADS, 0, s>>>(__VA_ARGS__), count_launch())
+#define SL(kern, ...) launch_pdl(kern, dim3(slab_blocks(q)), dim3(ROW_THREADS), 0, s, 1, __VA_ARGS__)
 template <typename V>
 void launch_spmv_t(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *x, V *y,
                    const SolveState *st) { SL(k_spmv<V>, g, q, S, x, y, st); }
@@ -1253,8 +1293,8 @@ void launch_relres(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys
                    const double *x, double *rb0, double *rb1) { SL(k_relres, g, q, S, b, x, rb0, rb1); }
 void launch_sys_to_f(cudaStream_t s, const SkewGeo &q, const double *sys, float *sysf) {
   const long long n = (long long)q.nb * q.W * q.T;
-  k_sys_to_f<<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, s>>>(q, sys, sysf);
-  count_launch();
+  launch_pdl(k_sys_to_f, dim3((unsigned)std::min<long long>((n + 255) / 256, 148LL * 16)), dim3(256), 0, s, 1, q, sys,
+             sysf);
 }
 void launch_scale_to_f(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r, double scale,
                        float *rf) { SL(k_scale_to_f, q, indc, r, scale, rf); }
@@ -1263,12 +1303,10 @@ void launch_add_f(cudaStream_t s, const SkewGeo &q, const int *indc, const float
 #undef SL
 void launch_fin(cudaStream_t s, int mode, const double *rb0, const double *rb1, long long nrows,
                 SolveState *st, double *out, double epsa2, double epsr2, double div2, int icgmax) {
-  k_fin<<<1, 1024, 0, s>>>(mode, rb0, rb1, nrows, st, out, epsa2, epsr2, div2, icgmax);
-  count_launch();
+  launch_pdl(k_fin, dim3(1), dim3(1024), 0, s, 1, mode, rb0, rb1, nrows, st, out, epsa2, epsr2, div2, icgmax);
 }
 void launch_pivot_check(cudaStream_t s, SolveState *st) {
-  k_pivot_check<<<1, 1, 0, s>>>(st);
-  count_launch();
+  launch_pdl(k_pivot_check, dim3(1), dim3(1), 0, s, 1, st);
 }
 void launch_vmodif(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const double *pt) {
   k_vmodif<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, f, p, pt);

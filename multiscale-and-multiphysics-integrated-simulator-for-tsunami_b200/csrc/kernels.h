@@ -16,27 +16,23 @@ struct SysPtr {
 };
 
 // The constant part of a solve in the tile-skewed layout of the MILU
-// kernels (k_poisson.cu).  The 7 coefficients and DD are interleaved slab
-// by slab, sys[(slab*SYS_N + c)*T + t], so the values one wavefront step
-// needs are one contiguous block; INDC is a plain skewed array.
-enum SysArray { SYS_AD = 0, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK, SYS_DD, SYS_N };
+// kernels (k_poisson.cu).  Nine arrays are interleaved slab by slab,
+// sys[(slab*SYS_N + c)*T + t], so the values one wavefront step of a sweep
+// needs are one contiguous run: the backward sweep's {T, AUI, AUJ, AUK,
+// DD}, the fused forward sweep's {AUI .. ALK} and the plain forward
+// sweep's {DD, AD, ALI, ALJ, ALK}.  SYS_T is the forward sweep's result
+// T = MINV_L*Y, written by the forward sweep for the backward sweep that
+// follows it.  INDC is a plain skewed array.
+enum SysArray { SYS_T = 0, SYS_AUI, SYS_AUJ, SYS_AUK, SYS_DD, SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_N };
 template <typename V> struct SkewSysT {
   V *sys;
   int *indc;
 };
-using SkewSys = SkewSysT<double>;   // the FP64 system of VF_M1BCGS
-using SkewSysF = SkewSysT<float>;   // its FP32 copy for the inner solves of the mixed solver
-// Tile geometry of the skewed layout: TI x TJ columns per tile, W
-// wavefront slabs per tile, ntx tiles along x, nb tiles in all.  Slab
-// entry t = ti + TIp*tj with the row stride TIp = TI rounded up to a
-// multiple of 4 (T = TIp*TJ entries per slab), so every slab, slab row and
-// group of 16 bytes of columns starts on a 16-byte boundary in double and
-// in float arrays and moves with one bulk copy.
-// With split = 2 a preconditioner block of TI x 2TJ columns is two layout
-// tiles (rows 2m and 2m+1 of tiles), swept by the two thread blocks of a
-// cluster.
+using SkewSys = SkewSysT<double>;
+using SkewSysF = SkewSysT<float>;
 struct SkewGeo {
-  int TI, TJ, TIp, T, W, ntx, nb;
+  int TI, TJ, TIp, T, W;  // layout tile TI x TJ columns (T = TIp*TJ slots), W slabs per tile
+  int ntx, nb;            // layout tiles along x, tiles in total
   int split;  // layout tiles per preconditioner block along y (1 or 2)
 };
 
@@ -46,16 +42,16 @@ __host__ __device__ inline long long sys_at(long long slab, int c, int T, int t)
 
 // Bulk copies of one wavefront step of the MILU sweeps (k_sweep).  A ring
 // slot holds NV slabs of T values (slab c at c*T):
-// MODE 0: forward sweep of a given vector: {Y, ALI, ALJ, ALK, AUI, AUJ,
-//         AUK, DD} (AUI..AUK unused), copies: Y, system slabs 1..7;
-// MODE 1: forward sweep fused with Y = A*P: {AD, ALI, ALJ, ALK, AUI, AUJ,
-//         AUK, DD, P} plus the P values of the four neighbouring tiles at
+// MODE 0: forward sweep of a given vector: {Y, DD, AD, ALI, ALJ, ALK}
+//         (AD unused), copies: Y, system arrays DD..ALK;
+// MODE 1: forward sweep fused with Y = A*P: {AUI, AUJ, AUK, DD, AD, ALI,
+//         ALJ, ALK, P} plus the P values of the four neighbouring tiles at
 //         the step's cells (down/up: one row of TIp; left/right: the span
 //         of the neighbour's slab from its last/first column of row 0 to
-//         that of row TJ-1), copies: system slabs 0..7, P, down, up, left,
-//         right;
-// MODE 2: backward sweep: {T, AUI, AUJ, AUK, DD}, copies: T, system
-//         slabs 4..7.
+//         that of row TJ-1), copies: system arrays AUI..ALK, P, down, up,
+//         left, right;
+// MODE 2: backward sweep: {T, AUI, AUJ, AUK, DD}, copy: system arrays
+//         T..DD.
 // Offsets are in elements of the sweep's type (es bytes: 8 for double, 4
 // for float); `arr` 0 is the interleaved system, 1 the vector.
 enum SweepMode { SWEEP_FWD = 0, SWEEP_FWD_AX = 1, SWEEP_BWD = 2 };
@@ -64,9 +60,16 @@ struct SweepCopy {
   int dst, bytes, arr;
 };
 __host__ __device__ inline int sweep_nv(int mode) {
-  return mode == SWEEP_FWD_AX ? 9 : (mode == SWEEP_FWD ? 8 : 5);
+  return mode == SWEEP_FWD_AX ? 9 : (mode == SWEEP_FWD ? 6 : 5);
 }
-__host__ __device__ inline int sweep_ncopy(const SkewGeo &, int mode) { return mode == SWEEP_FWD_AX ? 6 : 2; }
+__host__ __device__ inline int sweep_ncopy(const SkewGeo &, int mode) {
+  return mode == SWEEP_FWD_AX ? 6 : (mode == SWEEP_FWD ? 2 : 1);
+}
+// First system array of a mode's slot and its position there.
+__host__ __device__ constexpr int sweep_sys_first(int mode) {
+  return mode == SWEEP_FWD_AX ? SYS_AUI : (mode == SWEEP_FWD ? SYS_DD : SYS_T);
+}
+__host__ __device__ constexpr int sweep_sys_dst(int mode) { return mode == SWEEP_FWD ? 1 : 0; }
 // Elements per 16 bytes.
 __host__ __device__ inline int sweep_g(int es) { return 16 / es; }
 // Elements of a left/right halo span: TIp*(TJ-1) + 16 bytes.
@@ -99,20 +102,19 @@ struct SweepLane {
 __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, int c, SweepLane &l, int es) {
   const long long slab0 = (long long)b * q.W;
   l.dlo = 0; l.dhi = q.W - 1;
-  const int sys_c = (mode == SWEEP_FWD_AX) ? 0 : 1;  // copy index of the system block
-  const int vec_c = 1 - sys_c;
+  const int sys_c = (mode == SWEEP_FWD) ? 1 : 0;  // copy index of the system block
   if (c == sys_c) {
-    const int first = (mode == SWEEP_FWD_AX) ? SYS_AD : (mode == SWEEP_FWD ? SYS_ALI : SYS_AUI);
-    l.base = sys_at(slab0, first, q.T, 0);
+    l.base = sys_at(slab0, sweep_sys_first(mode), q.T, 0);
     l.wstride = SYS_N * q.T;
-    l.dst = (mode == SWEEP_FWD_AX) ? 0 : q.T;
-    l.bytes = (SYS_N - first) * q.T * es;
+    l.dst = sweep_sys_dst(mode) * q.T;
+    l.bytes = (mode == SWEEP_FWD_AX ? 8 : 5) * q.T * es;
     l.arr = 0;
     return true;
   }
+  if (mode == SWEEP_BWD) return false;
   l.wstride = q.T;
   l.arr = 1;
-  if (c == vec_c) {
+  if (c == 1 - sys_c) {  // the vector: Y (MODE 0) or P (MODE 1)
     l.base = slab0 * q.T;
     l.dst = (mode == SWEEP_FWD_AX) ? 8 * q.T : 0;
     l.bytes = q.T * es;
@@ -181,15 +183,15 @@ void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
                     const SkewSys &S, const double *x0, double *bsl, double *xsl, int warm);
 void launch_dcmp(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSys &S, int *pivot_bad);
+// T = MINV_L*Y (Y given, or Y = A*spmv_x formed in the sweep) into the
+// system block's SYS_T arrays; X = MINV_U*T from there.
 void launch_fwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *y,
-                const double *spmv_x, double *tout, SolveState *st, double *ybuf);
-void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *tin,
-                double *x, SolveState *st);
+                const double *spmv_x, SolveState *st, double *ybuf);
+void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, double *x, SolveState *st);
 // FP32 forms for the inner solves of the mixed-precision solver.
 void launch_fwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *y,
-                  const float *spmv_x, float *tout, SolveState *st, float *ybuf);
-void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *tin,
-                  float *x, SolveState *st);
+                  const float *spmv_x, SolveState *st, float *ybuf);
+void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, float *x, SolveState *st);
 void launch_dcmp_f(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSysF &S, int *pivot_bad);
 bool sweep_supported_f(const SkewGeo &q);
 // Vector kernels for both precisions (explicitly instantiated for double
