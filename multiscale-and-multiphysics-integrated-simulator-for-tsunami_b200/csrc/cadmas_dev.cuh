@@ -129,8 +129,17 @@ __device__ __forceinline__ void row_store(double s, double *rowbuf, long long ro
 // Second stage: one block of 1024 threads sums the row partials.
 __device__ __forceinline__ double block_final(const double *rowbuf, long long nrows) {
   __shared__ double w[32];
+  // thread t sums rows t, t+1024, t+2048, ... in that order; the loads of
+  // eight of them are issued before their additions
   double s = 0.0;
-  for (long long r = threadIdx.x; r < nrows; r += 1024) s = s + rowbuf[r];
+  for (long long r0 = threadIdx.x; r0 < nrows; r0 += 8 * 1024) {
+    double v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = (r0 + j * 1024 < nrows) ? rowbuf[r0 + j * 1024] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (r0 + j * 1024 < nrows) s = s + v[j];
+  }
   s = warp_tree(s);
   if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
   __syncthreads();

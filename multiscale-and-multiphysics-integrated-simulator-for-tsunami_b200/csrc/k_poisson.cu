@@ -749,10 +749,14 @@ __global__ void __launch_bounds__(MAXT, 1)
 // The dot products (VF_MZIP) sum in that order: lane partials, warp tree
 // per slab, then the 1024-thread tree over the slab partials (block_final).
 // Padding entries carry INDC = -1 and are skipped like non-computed cells.
+// The hot kernels load every operand of an entry before testing its INDC
+// (all entries of the layout are allocated), so the unrolled loop keeps
+// several entries' loads in flight.
 #define SLAB_LOOP_BEGIN(q)                                                          \
   const int lane_ = threadIdx.x & 31;                                               \
   const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
   if (slab_ < (long long)(q).nb * (q).W) {                                          \
+    _Pragma("unroll 4")                                                             \
     for (int t_ = lane_; t_ < (q).T; t_ += 32) {                                    \
       const long long e = slab_ * (q).T + t_;
 #define SLAB_LOOP_END \
@@ -816,9 +820,12 @@ __global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, cons
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
   SLAB_LOOP_BEGIN(q)
-  if (INDC[e] != -1) {
-    s0 = s0 + (double)x0[e] * (double)y0[e];
-    if (x1) s1 = s1 + (double)x1[e] * (double)y1[e];
+  const int ic = INDC[e];
+  const double a0 = (double)x0[e] * (double)y0[e];
+  const double a1 = x1 ? (double)x1[e] * (double)y1[e] : 0.0;
+  if (ic != -1) {
+    s0 = s0 + a0;
+    if (x1) s1 = s1 + a1;
   }
   SLAB_LOOP_END
   row_store(s0, rb0, SLAB_ROW, nslab);
@@ -842,7 +849,9 @@ __global__ void k_axpy_rr(SkewGeo q, const int *INDC, const V *AP, V *RR, const 
   if (st->done) return;
   const double alpha = st->alpha;
   SLAB_LOOP_BEGIN(q)
-  if (INDC[e] != -1) RR[e] = (V)(RR[e] - alpha * AP[e]);
+  const int ic = INDC[e];
+  const V r = RR[e], a = AP[e];
+  if (ic != -1) RR[e] = (V)(r - alpha * a);
   SLAB_LOOP_END
 }
 
@@ -857,12 +866,14 @@ __global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, c
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
   SLAB_LOOP_BEGIN(q)
-  if (INDC[e] != -1) {
-    XW[e] = (V)(XW[e] + (alpha * PP[e] + omega * RR[e]));
-    const V r = (V)(RR[e] - omega * AE[e]);
+  const int ic = INDC[e];
+  const V xw = XW[e], pp = PP[e], rr = RR[e], ae = AE[e], r0 = R0[e];
+  if (ic != -1) {
+    XW[e] = (V)(xw + (alpha * pp + omega * rr));
+    const V r = (V)(rr - omega * ae);
     RR[e] = r;
     s0 = s0 + (double)r * (double)r;
-    s1 = s1 + (double)R0[e] * (double)r;
+    s1 = s1 + (double)r0 * (double)r;
   }
   SLAB_LOOP_END
   row_store(s0, rb0, SLAB_ROW, nslab);
@@ -876,7 +887,9 @@ __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V 
   if (st->done) return;
   const double beta = st->beta, omega = st->omega;
   SLAB_LOOP_BEGIN(q)
-  if (INDC[e] != -1) PP[e] = (V)(RR[e] + beta * (PP[e] - omega * AP[e]));
+  const int ic = INDC[e];
+  const V rr = RR[e], pp = PP[e], ap = AP[e];
+  if (ic != -1) PP[e] = (V)(rr + beta * (pp - omega * ap));
   SLAB_LOOP_END
 }
 
