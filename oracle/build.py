@@ -2,7 +2,9 @@
 
 g++ -O2 -ffp-contract=off: no fused multiply-add, so every expression
 rounds as its sequential left-to-right evaluation, like the GPU library
-built with --fmad=false.
+built with --fmad=false.  -fopenmp: the solver runs one emulated rank
+(preconditioner block) per thread and its cell loops in parallel, with
+results identical to one thread (OMP_NUM_THREADS sets the count).
 """
 from __future__ import annotations
 
@@ -27,7 +29,7 @@ def build(force: bool = False) -> pathlib.Path:
     if not force and not needs_build():
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+    cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
            "-Wall", "-o", str(tmp), str(SRC)]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)

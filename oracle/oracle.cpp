@@ -11,6 +11,9 @@
 // (k-epsilon, temperature, scalars, wave-source terms ISCTYP, time-dependent
 // porosity IPRNT>1, air-pressure model PVCP0, matrix wave data MTBTYP=3,
 // log-law walls, droplet fall IDROP) are not restated and are rejected.
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include "oracle.h"
 
 #include <chrono>
@@ -62,6 +65,8 @@ static double warp_tree(double *s) {
 
 struct orc_handle {
   int NI, NJ, NK, NB;
+  // parallel loops only where a grid is large enough to pay for the threads
+  bool par() const { return (long long)NI * NJ * NK >= 200000; }
   cadmas_params P;
   int sum_mode;
   // static
@@ -1070,8 +1075,12 @@ struct orc_handle {
   bool mzdcmp(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
               const vd &AUJ, const vd &AUK, vd &DDo, const int *IC) {
     const double U = (P.icgtyp != 0) ? P.cgpara : 0.0;
-    bool npos = true;
-    for (const Tile &t : tiles())
+    int npos = 1;
+    const std::vector<Tile> tl = tiles();
+    // tiles are independent (block-Jacobi): one thread per tile
+#pragma omp parallel for schedule(dynamic) reduction(&& : npos) if (par())
+    for (size_t n = 0; n < tl.size(); ++n) {
+      const Tile &t = tl[n];
       for (int K = 2; K <= NK - 1; ++K)
         for (int J = t.js; J <= t.je; ++J)
           for (int I = t.is; I <= t.ie; ++I) {
@@ -1084,14 +1093,18 @@ struct orc_handle {
             else { a2 = 0.0 + U * (0.0 + 0.0); }
             { size_t n = id(I, J, K - 1); d3 = DDo[n]; a3 = AUK[n] + U * (AUI[n] + AUJ[n]); }
             DDo[c] = 1.0 / (AD[c] - ALI[c] * d1 * a1 - ALJ[c] * d2 * a2 - ALK[c] * d3 * a3);
-            if (DDo[c] <= 0.0) npos = false;
+            if (DDo[c] <= 0.0) npos = 0;
           }
-    return npos;
+    }
+    return npos != 0;
   }
   // VF_MZFRWD vf_mzfrwd.f:37-48 then VF_MZBKWD vf_mzbkwd.f:37-47, per tile.
   void mzminv(const vd &DDv, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
               const vd &AUJ, const vd &AUK, vd &X, const vd &Yv, const int *IC) {
-    for (const Tile &t : tiles()) {
+    const std::vector<Tile> tl = tiles();
+#pragma omp parallel for schedule(dynamic) if (par())
+    for (size_t n = 0; n < tl.size(); ++n) {
+      const Tile &t = tl[n];
       for (int K = 2; K <= NK - 1; ++K)
         for (int J = t.js; J <= t.je; ++J)
           for (int I = t.is; I <= t.ie; ++I) {
@@ -1118,6 +1131,7 @@ struct orc_handle {
   // VF_MZAX  vf_mzax.f:42-56
   void mzax(const vd &AD, const vd &ALI, const vd &ALJ, const vd &ALK, const vd &AUI,
             const vd &AUJ, const vd &AUK, const vd &X, vd &Yv, const int *IC) {
+#pragma omp parallel for schedule(static) if (par())
     for (int K = 2; K <= NK - 1; ++K)
       for (int J = 2; J <= NJ - 1; ++J)
         for (int I = 2; I <= NI - 1; ++I) {
@@ -1132,8 +1146,12 @@ struct orc_handle {
   // order, the row tree in GPU order.
   double mzip(const vd &X, const vd &Yv, const int *IC) {
     if (sum_mode == ORC_SUM_REF) {
-      double S = 0.0;
-      for (const Tile &t : tiles()) {
+      // each emulated rank's partial in parallel, then the ranks in order
+      const std::vector<Tile> tl = tiles();
+      std::vector<double> part(tl.size());
+#pragma omp parallel for schedule(dynamic) if (par())
+      for (size_t n = 0; n < tl.size(); ++n) {
+        const Tile &t = tl[n];
         double s = 0.0;
         for (int K = 2; K <= NK - 1; ++K)
           for (int J = t.js; J <= t.je; ++J)
@@ -1141,8 +1159,10 @@ struct orc_handle {
               size_t c = id(I, J, K);
               if (IC[c] != -1) s = s + X[c] * Yv[c];
             }
-        S = S + s;
+        part[n] = s;
       }
+      double S = 0.0;
+      for (double s : part) S = S + s;
       return S;
     }
     return gsum_skew([&](int i, int j, int k, double &c) {
@@ -1168,11 +1188,13 @@ struct orc_handle {
     BNORM = mzip(Y2, Y2, IC);
     ITER = 0;
     mzax(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, XW, Y2, IC);
+#pragma omp parallel for schedule(static) if (par())
     for (size_t c = 0; c < N; ++c) if (IC[c] != -1) Y2[c] = BB[c] - Y2[c];
     mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, R0, Y2, IC);
     double S = mzip(R0, R0, IC);
     XNORM = S;
     if (!(XNORM <= BNORM * EPSR2 + EPSA2)) {
+#pragma omp parallel for schedule(static) if (par())
       for (size_t c = 0; c < N; ++c) if (IC[c] != -1) { RR[c] = R0[c]; PPv[c] = R0[c]; }
       for (;;) {
         ITER = ITER + 1;
@@ -1181,12 +1203,14 @@ struct orc_handle {
         mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, AP, Y2, IC);
         double W1 = mzip(R0, AP, IC);
         double ALPHA = S / W1;
+#pragma omp parallel for schedule(static) if (par())
         for (size_t c = 0; c < N; ++c) if (IC[c] != -1) RR[c] = RR[c] - ALPHA * AP[c];
         mzax(AD, ALI, ALJ, ALK, AUI, AUJ, AUK, RR, Y2, IC);
         mzminv(DD, ALI, ALJ, ALK, AUI, AUJ, AUK, AE, Y2, IC);
         W1 = mzip(RR, AE, IC);
         double W2 = mzip(AE, AE, IC);
         double OMEGA = W1 / W2;
+#pragma omp parallel for schedule(static) if (par())
         for (size_t c = 0; c < N; ++c)
           if (IC[c] != -1) {
             XW[c] = XW[c] + (ALPHA * PPv[c] + OMEGA * RR[c]);
@@ -1197,6 +1221,7 @@ struct orc_handle {
         if (XNORM > DIV2) { ITER = -2; break; }
         W1 = mzip(R0, RR, IC);
         double BETA = W1 * ALPHA / (S * OMEGA);
+#pragma omp parallel for schedule(static) if (par())
         for (size_t c = 0; c < N; ++c)
           if (IC[c] != -1) PPv[c] = RR[c] + BETA * (PPv[c] - OMEGA * AP[c]);
         S = W1;
@@ -2366,6 +2391,14 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
 int orc_get_timers(orc_handle *h, double *t5) {
   for (int i = 0; i < 5; ++i) t5[i] = h->tmr[i];
   return CADMAS_OK;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
 }
 
 }  // extern "C"

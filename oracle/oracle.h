@@ -57,6 +57,8 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
 /* Seconds spent in the last orc_step by stage: [0] momentum predictor,
    [1] assembly, [2] solve, [3] correction+BC, [4] VOF+flags.              */
 int orc_get_timers(orc_handle *h, double *t5);
+/* Threads the oracle's parallel loops use (OpenMP). */
+int orc_num_threads(void);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,8 @@ def _load_lib():
     lib.orc_m1bcgs.argtypes = [C.c_void_p] + [dp] * 9 + [C.POINTER(C.c_int), C.POINTER(C.c_int), dp, dp]
     lib.orc_get_poisson.argtypes = [C.c_void_p, C.c_int, dp]
     lib.orc_get_timers.argtypes = [C.c_void_p, dp]
+    lib.orc_num_threads.argtypes = []
+    lib.orc_num_threads.restype = C.c_int
     _lib = lib
     return lib
 
@@ -158,3 +160,8 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def num_threads() -> int:
+    """Threads of the oracle's parallel loops (OpenMP; OMP_NUM_THREADS)."""
+    return int(_load_lib().orc_num_threads())
