@@ -109,7 +109,11 @@ typedef struct cadmas_params {
      preconditioner (and the result) is the same; precond_tj must be even.
      The BiCGSTAB dot products then sum over half-height slabs.           */
   int    precond_split;
-  int    reserved[2];
+  /* IDROP /VF_APHYSI/: 1 = the TimerDoor droplet model VF_FDROPF after the
+     flag update of every step (vf_f1cal.f:212-217), the reference's
+     default (vf_a2dflt.f:151); 0 = off (DROP OFF).                       */
+  int    idrop;
+  int    reserved[1];
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */
@@ -197,6 +201,17 @@ int cadmas_upload_static(cadmas_handle *h, const cadmas_static *s);
 int cadmas_set_state(cadmas_handle *h, const cadmas_state *s);
 /* Copy device state to the host (NULL members skipped). */
 int cadmas_get_state(cadmas_handle *h, cadmas_state *s);
+
+/* The droplet model's arrays DROPTX, DROPTY, DROPTZ, DROPUU, DROPVV,
+   DROPWW, (NUMI,NUMJ,NUMK) column-major host arrays (NULL skipped): the
+   arguments of the same names of VF_F1CAL (vf_f1cal.f:3) and of the
+   restart file (vf_ir1inp.f:3).  They stay on the device between steps;
+   cadmas_create and cadmas_init_state set them to -1e10, 0, 0, 0, 0, 0
+   as VF_CINIT does (vf_cinit.f:416-427).                                */
+int cadmas_get_drop(cadmas_handle *h, double *droptx, double *dropty, double *droptz, double *dropuu,
+                    double *dropvv, double *dropww);
+int cadmas_set_drop(cadmas_handle *h, const double *droptx, const double *dropty, const double *droptz,
+                    const double *dropuu, const double *dropvv, const double *dropww);
 
 /* Initial classification and boundary values of VF_CINIT
    (vf_cinit.f:202-207 and the BC calls after :283): FCUT01, BWFF, FNFINI,

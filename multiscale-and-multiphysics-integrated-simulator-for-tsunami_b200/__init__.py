@@ -68,7 +68,7 @@ class Params(C.Structure):
         ("icgtyp", C.c_int), ("icgmax", C.c_int), ("ibsuw0", C.c_int),
         ("precond_ti", C.c_int), ("precond_tj", C.c_int),
         ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("precond_split", C.c_int),
-        ("reserved", C.c_int * 2)]
+        ("idrop", C.c_int), ("reserved", C.c_int * 1)]
 
 
 class Static(C.Structure):
@@ -93,7 +93,10 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
             "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
             "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
-            "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers"]
+            "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers", "cadmas_get_drop",
+            "cadmas_set_drop"]
+
+DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 
 STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]
 
@@ -132,6 +135,8 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_upload_static.argtypes = [C.c_void_p, C.POINTER(Static)]
     lib.cadmas_set_state.argtypes = [C.c_void_p, C.POINTER(State)]
     lib.cadmas_get_state.argtypes = [C.c_void_p, C.POINTER(State)]
+    lib.cadmas_get_drop.argtypes = [C.c_void_p] + [_dp] * 6
+    lib.cadmas_set_drop.argtypes = [C.c_void_p] + [_dp] * 6
     lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
     lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
     lib.cadmas_set_time.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
@@ -285,6 +290,16 @@ class Tank:
 
     def init_state(self, hydrostatic=True):
         _check(self.lib, self.lib.cadmas_init_state(self.h, int(bool(hydrostatic))))
+
+    def get_drop(self):
+        """The droplet model's arrays {droptx, dropty, droptz, dropuu, dropvv, dropww}."""
+        arrs = {n: np.zeros(self.case.ni * self.case.nj * self.case.nk) for n in DROP_ARRAYS}
+        _check(self.lib, self.lib.cadmas_get_drop(self.h, *(_dptr(arrs[n]) for n in DROP_ARRAYS)))
+        return arrs
+
+    def set_drop(self, arrs):
+        keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64) for n in DROP_ARRAYS}
+        _check(self.lib, self.lib.cadmas_set_drop(self.h, *(_dptr(keep[n]) for n in DROP_ARRAYS)))
 
     # ------------------------------------------------------------ step
     def step(self, dt=None):

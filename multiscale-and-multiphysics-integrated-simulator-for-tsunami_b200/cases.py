@@ -378,7 +378,7 @@ def dam_break(nx=64, ny=8, nz=32, d=0.01, column=(16, 16), dt=1.0e-4):
     i = 17..64, all j, k = 1..16 (DEBUG F-BOX)."""
     c = new_case("dam_break", np.arange(nx + 1) * d, np.arange(ny + 1) * d,
                  np.arange(nz + 1) * d)
-    c.params.update(wvlvl=column[1] * d, wbub=-1.0, cgepsr=1.0e-10)
+    c.params.update(wvlvl=column[1] * d, wbub=-1.0, idrop=0, cgepsr=1.0e-10)  # BUB OFF, DROP OFF
     init_f_still_water(c, column[1] * d)
     f_box(c, column[0] + 2, 2, 2, nx + 1, ny + 1, column[1] + 1, 0.0)
     c.dt = dt
@@ -505,6 +505,56 @@ def random_tank(seed=0, nx=12, ny=6, nz=10, d=0.01, nobst=2, nporous=2,
         f_box(c, i1, j1, k1, i2, j2, k2, float(rng.choice([0.0, 1.0, rng.uniform()])))
     c.dt = dt
     finish(c, vp_type=VP_SLIP if slip else VP_NOSLIP)
+    return c
+
+
+def droplet_tank(seed=0, nx=24, ny=6, nz=20, d=0.01, ndrop=8, level=0.3, dt=2.0e-3, speed=1.0):
+    """Droplets over a pool (the TimerDoor droplet model VF_FDROPF): single
+    water cells (F in 0.3..1) in the air, each isolated, so the flag update
+    turns them into gas cells that hold water.  An obstacle step and a
+    porous block stand in the pool; droplets above the step land on it.
+    c.drop_state holds droplet arrays (DROPTX..DROPWW, flat, column-major)
+    that make the droplets old ones (time 0) already moving with random
+    velocities (|u|, |w| up to `speed`, |v| up to speed/2), for
+    cadmas_set_drop: they then fly sideways, rise and fall from the first
+    steps."""
+    rng = np.random.Generator(np.random.Philox(seed))
+
+    def axis(n):
+        w = rng.uniform(0.85, 1.2, size=n) * d
+        return np.concatenate([[0.0], np.cumsum(w)])
+
+    c = new_case(f"droplet_tank_{seed}", axis(nx), axis(ny), axis(nz))
+    kw = max(3, int(level * nz))          # last water layer
+    ks = kw + 3                           # top of the obstacle step
+    i1s = nx // 2 + 2
+    add_obstacle(c, i1s, 2, 2, nx + 1, ny + 1, ks)
+    add_porous(c, 3, 2, 2, 5, ny + 1, kw, 0.5, 0.8, 1.0)
+    wv = c.zz[0, kw]
+    c.params.update(wvlvl=wv, wbub=-1.0, cgepsr=1.0e-12, idrop=1)
+    init_f_still_water(c, wv)
+    placed = []
+    tries = 0
+    while len(placed) < ndrop and tries < 1000:
+        tries += 1
+        i = int(rng.integers(3, nx + 1)); j = int(rng.integers(2, ny + 2))
+        k = int(rng.integers(ks + 2, nz))
+        if c.nf[i - 1, j - 1, k - 1] == -1 or any(abs(i - a) + abs(j - b) + abs(k - e) < 4 for a, b, e in placed):
+            continue
+        placed.append((i, j, k))
+        c.ff[i - 1, j - 1, k - 1] = float(rng.uniform(0.3, 1.0))
+    c.dt = dt
+    finish(c)
+    shape = (c.ni, c.nj, c.nk)
+    ds = {"droptx": _z3(*shape, -1.0e10)}
+    for nm in ("dropty", "droptz", "dropuu", "dropvv", "dropww"):
+        ds[nm] = _z3(*shape)
+    for i, j, k in placed:
+        u, v, w = (float(rng.uniform(-speed, speed)) for _ in range(3))
+        c0 = (i - 1, j - 1, k - 1)
+        ds["droptx"][c0] = ds["dropty"][c0] = ds["droptz"][c0] = 0.0
+        ds["dropuu"][c0], ds["dropvv"][c0], ds["dropww"][c0] = u, 0.5 * v, w
+    c.drop_state = {nm: a.reshape(-1, order="F") for nm, a in ds.items()}
     return c
 
 

@@ -151,6 +151,7 @@ struct cadmas_handle {
   double *h_res = nullptr;
   // host-side scalars
   std::vector<double> tbub;
+  DropArrays drop{};  // DROPTX..DROPWW (the droplet model's state)
   std::vector<double> zz2;  // ZZ(2,K) on the host, K = 1..NK
   std::vector<unsigned char> h_active;
   double tnow = 0.0, dtnow = 0.0;
@@ -655,6 +656,11 @@ static int do_f1cal(cadmas_handle *h) {
     rc = fnfini(h);
     if (rc) return rc;
   }
+  if (h->P.idrop >= 1) {  // droplets fall, then the flags again (vf_f1cal.f:212-217)
+    launch_fdropf(s, g, h->f, h->p, h->drop);
+    rc = fnfini(h);
+    if (rc) return rc;
+  }
   launch_fnfprv(s, g, h->f, h->dint);
   CK(cudaMemsetAsync(h->dint + 4, 0, sizeof(int), s));
   launch_cindc(s, g, h->f, h->dint + 4);
@@ -719,6 +725,7 @@ void cadmas_default_params(cadmas_params *p) {
   }
   p->icgtyp = 1; p->icgmax = 500; p->ibsuw0 = 0;
   p->precond_ti = 0; p->precond_tj = 0;
+  p->idrop = 1;
 }
 
 int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **out) {
@@ -790,6 +797,12 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   }
   AL(h->rb0, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->rb1, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->dres, 8);
   AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
+  AL(h->drop.tx, h->N); AL(h->drop.ty, h->N); AL(h->drop.tz, h->N);
+  AL(h->drop.uu, h->N); AL(h->drop.vv, h->N); AL(h->drop.ww, h->N);
+  if (p->idrop >= 1 && !drop_supported(h->g)) {
+    g_last_error = "x lines too long for the droplet model's shared-memory walk";
+    rc = rc ? rc : CADMAS_EUNSUPPORTED;
+  }
 #undef AL
   if (!rc && cudaMallocHost((void **)&h->h_st, sizeof(SolveState)) != cudaSuccess) rc = CADMAS_ENOMEM;
   if (!rc && cudaMallocHost((void **)&h->h_int, 8 * sizeof(int)) != cudaSuccess) rc = CADMAS_ENOMEM;
@@ -798,6 +811,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   // NF starts as all obstacle until set_state; INDC as non-computed.
   cudaMemset(h->nf, 0xff, h->N * sizeof(int));
   cudaMemset(h->indc, 0xff, h->N * sizeof(int));
+  launch_drop_reset(h->s, (long long)h->N, h->drop);
   h->tbub.assign(d->numk, 0.0);
   h->h_active.assign(d->numk + 1, 0);
   std::memset(&h->stats, 0, sizeof(h->stats));
@@ -827,6 +841,7 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_int) cudaFreeHost(h->h_int);
   if (h->h_res) cudaFreeHost(h->h_res);
   for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
+  for (double *q : {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww}) if (q) cudaFree(q);
   for (float *q : {h->Sf.sys, h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->y2f})
     if (q) cudaFree(q);
   if (h->s) cudaStreamDestroy(h->s);
@@ -956,6 +971,29 @@ int cadmas_get_state(cadmas_handle *h, cadmas_state *st) {
   return CADMAS_OK;
 }
 
+int cadmas_get_drop(cadmas_handle *h, double *tx, double *ty, double *tz, double *uu, double *vv, double *ww) {
+  if (!h) return CADMAS_EINVAL;
+  const size_t b8 = h->N * sizeof(double);
+  double *dst[6] = {tx, ty, tz, uu, vv, ww};
+  const double *src[6] = {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww};
+  for (int a = 0; a < 6; ++a)
+    if (dst[a]) CK(cudaMemcpyAsync(dst[a], src[a], b8, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return CADMAS_OK;
+}
+
+int cadmas_set_drop(cadmas_handle *h, const double *tx, const double *ty, const double *tz, const double *uu,
+                    const double *vv, const double *ww) {
+  if (!h) return CADMAS_EINVAL;
+  const size_t b8 = h->N * sizeof(double);
+  const double *src[6] = {tx, ty, tz, uu, vv, ww};
+  double *dst[6] = {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww};
+  for (int a = 0; a < 6; ++a)
+    if (src[a]) CK(cudaMemcpyAsync(dst[a], src[a], b8, cudaMemcpyHostToDevice, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return CADMAS_OK;
+}
+
 int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   if (!h) return CADMAS_EINVAL;
   if (!h->have_static) return CADMAS_ENOSTATIC;
@@ -1003,6 +1041,7 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   launch_bwuwt(s, h->g, h->f);
   launch_bwpp(s, h->g, h->f);
   std::fill(h->tbub.begin(), h->tbub.end(), 0.0);
+  launch_drop_reset(s, (long long)h->N, h->drop);  // vf_cinit.f:416-427
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->h_res, h->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   int bits;

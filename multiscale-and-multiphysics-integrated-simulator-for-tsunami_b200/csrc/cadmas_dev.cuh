@@ -69,6 +69,11 @@ struct Fld {
   double *bcu, *bcv, *bcw, *bcp, *bcf;
 };
 
+// DROPTX, DROPTY, DROPTZ, DROPUU, DROPVV, DROPWW of the droplet model
+struct DropArrays {
+  double *tx, *ty, *tz, *uu, *vv, *ww;
+};
+
 __device__ __forceinline__ int indb(const Fld &f, int m, int l) { return f.indb[(m - 1) + 4 * (l - 1)]; }
 
 __device__ __forceinline__ void decode(const Geo &g, int ijk, int &i, int &j, int &k) {

@@ -171,6 +171,11 @@ struct WaveDev {
   const double *zz, *un, *ut;  // device copies of DMTBZZ, DMTBUN, DMTBUT
 };
 
+// k_drop.cu: VF_FDROPF (all its passes) and the start values of its arrays
+void launch_fdropf(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const DropArrays &d);
+void launch_drop_reset(cudaStream_t s, long long n, const DropArrays &d);
+bool drop_supported(const Geo &g);
+
 // k_momentum.cu
 void launch_flux(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl);
 void launch_predict(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl,

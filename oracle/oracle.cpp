@@ -10,7 +10,8 @@
 // (vf_cpara.f:80-98).  Options outside the configurations exercised here
 // (k-epsilon, temperature, scalars, wave-source terms ISCTYP, time-dependent
 // porosity IPRNT>1, air-pressure model PVCP0, matrix wave data MTBTYP=3,
-// log-law walls, droplet fall IDROP) are not restated and are rejected.
+// log-law walls) are not restated and are rejected.  The droplet model
+// VF_FDROPF (IDROP >= 1) is restated.
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -2012,6 +2013,190 @@ struct orc_handle {
     }
   }
 
+  // ----------------------------------------------------------- droplets
+  // DROPTX..DROPWW of the TimerDoor droplet model; vf_cinit.f:412-427
+  // starts every cell at (-1e10, 0, 0, 0, 0, 0).
+  vd DTX, DTY, DTZ, DUU, DVV, DWW;
+  vd DW[7];  // weighted sums of a directional pass
+  void drop_clear(size_t c) {
+    DTX[c] = -1.0e10; DTY[c] = 0.0; DTZ[c] = 0.0; DUU[c] = 0.0; DVV[c] = 0.0; DWW[c] = 0.0;
+  }
+  void drop_alloc() {
+    const size_t N = (size_t)NI * NJ * NK;
+    for (vd *a : {&DTX, &DTY, &DTZ, &DUU, &DVV, &DWW}) a->assign(N, 0.0);
+    std::fill(DTX.begin(), DTX.end(), -1.0e10);
+  }
+
+  // VF_FDROPF  vf_fdropf.f:69-290.  A droplet cell is a gas cell (NF=8)
+  // holding water (F > FLOWER).  A new one (DROPTX < 0) takes the mean
+  // cell-centre velocity of the neighbours along its 12 edges that are
+  // fluid and reachable past an open face, else of its 6 face neighbours
+  // that are fluid or surface, else its own; on an obstacle it is at
+  // rest.  An old one resting on an obstacle slides down the slope of the
+  // porosity around it.  Every other cell loses its droplet values.
+  void drop_start() {
+    const double FL = P.flower;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          if (!(FF[c] > FL && NF[c] == 8)) { drop_clear(c); continue; }
+          if (DTX[c] < 0.0) {
+            DTX[c] = TNOW; DTY[c] = TNOW; DTZ[c] = TNOW;
+            int IP = 0;
+            double UP = 0.0, VP = 0.0, WP = 0.0;
+            auto take = [&](int i, int j, int k) {
+              IP = IP + 1;
+              UP = UP + 0.5 * (UU[id(i + 1, j, k)] + UU[id(i, j, k)]);
+              VP = VP + 0.5 * (VV[id(i, j + 1, k)] + VV[id(i, j, k)]);
+              WP = WP + 0.5 * (WW[id(i, j, k + 1)] + WW[id(i, j, k)]);
+            };
+            // edge neighbour (i1,j1,k1) reached past face cell a or b
+            auto edge = [&](int i1, int j1, int k1, size_t a, size_t b) {
+              if (NF[id(i1, j1, k1)] == 0 && (NF[a] != -1 || NF[b] != -1)) take(i1, j1, k1);
+            };
+            for (int dk = -1; dk <= 1; dk += 2)  // x-z plane (:79-114)
+              for (int di = -1; di <= 1; di += 2) edge(I + di, J, K + dk, id(I + di, J, K), id(I, J, K + dk));
+            for (int dj = -1; dj <= 1; dj += 2)  // x-y plane (:115-150)
+              for (int di = -1; di <= 1; di += 2) edge(I + di, J + dj, K, id(I + di, J, K), id(I, J + dj, K));
+            for (int dk = -1; dk <= 1; dk += 2)  // y-z plane (:151-186)
+              for (int dj = -1; dj <= 1; dj += 2) edge(I, J + dj, K + dk, id(I, J + dj, K), id(I, J, K + dk));
+            if (IP == 0) {  // face neighbours, fluid or surface (:188-231)
+              const int nb[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, 0, -1}, {0, 0, 1}, {0, -1, 0}, {0, 1, 0}};
+              for (auto &d : nb) {
+                const int N1 = NF[id(I + d[0], J + d[1], K + d[2])];
+                if (N1 != -1 && N1 != 8) take(I + d[0], J + d[1], K + d[2]);
+              }
+            }
+            if (IP >= 1) {
+              const double CP = 1.0 / (double)IP;
+              DUU[c] = UP * CP; DVV[c] = VP * CP; DWW[c] = WP * CP;
+            } else {
+              DUU[c] = 0.5 * (UU[c] + UU[id(I + 1, J, K)]);
+              DVV[c] = 0.5 * (VV[c] + VV[id(I, J + 1, K)]);
+              DWW[c] = 0.5 * (WW[c] + WW[id(I, J, K + 1)]);
+            }
+            if (NF[id(I, J, K - 1)] == -1) { DUU[c] = 0.0; DVV[c] = 0.0; DWW[c] = 0.0; }
+          } else if (NF[id(I, J, K - 1)] == -1) {  // sliding on an obstacle (:253-280)
+            auto h = [&](size_t n) { return NF[n] == -1 ? 1.0 : 1.0 - GGV[n]; };
+            double HX = 0.5 * (h(id(I + 1, J, K)) - h(id(I - 1, J, K))) * Z_(2, K);
+            double HY = 0.5 * (h(id(I, J + 1, K)) - h(id(I, J - 1, K))) * Z_(2, K);
+            HX = HX / X_(2, I);
+            HY = HY / Y_(2, J);
+            const double DN = 1.0 / (HX * HX + HY * HY + 1.0);
+            HX = -(P.grz0 * HX * DN);
+            HY = -(P.grz0 * HY * DN);
+            DUU[c] = DUU[c] + DTNOW * HX;
+            DVV[c] = DVV[c] + DTNOW * HY;
+          }
+        }
+  }
+
+  // VF_FDROPF  vf_fdropf.f:292-610: droplet water moves one cell along
+  // axis ax (0 x, 1 y, 2 z), towards + (L = 1) or - (L = 2), once the time
+  // to cross its cell has passed since the droplet last moved that way; the
+  // droplet values of the cells that keep or receive water become the
+  // water-weighted means.  The line is swept against the motion so water
+  // moves at most one cell per pass.
+  void drop_move(int ax, int L) {
+    const double FL = P.flower, G = P.grz0;
+    // WKTX..WKFF (the reference lends WK05..WK11; separate arrays here keep
+    // the step's Poisson system readable by orc_get_poisson)
+    vd &WTX = DW[0], &WTY = DW[1], &WTZ = DW[2], &WUU = DW[3], &WVV = DW[4], &WWW = DW[5], &WFF = DW[6];
+    for (vd *a : {&WTX, &WTY, &WTZ, &WUU, &WVV, &WWW, &WFF})
+      if (a->size() != FF.size()) a->assign(FF.size(), 0.0);
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          WTX[c] = 0.0; WTY[c] = 0.0; WTZ[c] = 0.0; WUU[c] = 0.0; WVV[c] = 0.0; WWW[c] = 0.0; WFF[c] = 0.0;
+        }
+    const int NA = ax == 0 ? NI : (ax == 1 ? NJ : NK);
+    const int st = (L == 1) ? NA - 1 : 2, en = (L == 1) ? 2 : NA - 1, dl = (L == 1) ? -1 : 1;
+    const double SG = (L == 1) ? 1.0 : -1.0;
+    auto cell = [&](int I, int J, int K) {
+      const int I1 = I - (ax == 0 ? dl : 0), J1 = J - (ax == 1 ? dl : 0), K1 = K - (ax == 2 ? dl : 0);
+      const size_t c = id(I, J, K), c1 = id(I1, J1, K1);
+      double DT = 0.0;
+      const bool drop = FF[c] > FL && NF[c] == 8 && NF[c1] != -1;
+      bool go = false;
+      if (ax < 2) {
+        const double D = ax == 0 ? DUU[c] : DVV[c];
+        if (drop && SG * D > 0.0) {
+          DT = (ax == 0 ? X_(2, I) : Y_(2, J)) / std::fabs(D);
+          go = (TNOW - (ax == 0 ? DTX[c] : DTY[c])) > DT;
+          if (!go) DT = 0.0;
+        }
+      } else if (drop) {
+        const double X = std::sqrt(2.0 * G * Z_(2, K)), W = DWW[c];
+        if (L == 1) {
+          if (W > X) DT = (W - std::sqrt(W * W - X * X)) / G;
+        } else if (W <= X) {
+          if (W <= 0.0) DT = (W + std::sqrt(W * W + X * X)) / G;
+          else DT = 2.0 * W / G;
+        }
+        go = DT > 0.0 && (TNOW - DTZ[c]) > DT;
+        if (!go) DT = 0.0;
+      }
+      const double TX = DTX[c] + (ax == 0 ? DT : 0.0), TY = DTY[c] + (ax == 1 ? DT : 0.0),
+                   TZ = DTZ[c] + (ax == 2 ? DT : 0.0), WW2 = ax == 2 ? DWW[c] - DT * G : DWW[c];
+      // the unshifted values enter as they are (x + 0.0 would turn -0 into +0)
+      auto tx = [&]() { return ax == 0 ? TX : DTX[c]; };
+      auto ty = [&]() { return ax == 1 ? TY : DTY[c]; };
+      auto tz = [&]() { return ax == 2 ? TZ : DTZ[c]; };
+      auto ww = [&]() { return ax == 2 ? WW2 : DWW[c]; };
+      if (go) {
+        const double V0 = X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[c];
+        const double V1 = X_(2, I1) * Y_(2, J1) * Z_(2, K1) * GGV[c1];
+        const double FMOVE = dmin((1.0 - FF[c1]) * V1, FF[c] * V0);
+        FF[c] = FF[c] - FMOVE / V0;
+        FF[c1] = FF[c1] + FMOVE / V1;
+        if (NF[c1] == 8) {
+          WTX[c1] = WTX[c1] + FMOVE * tx(); WTY[c1] = WTY[c1] + FMOVE * ty();
+          WTZ[c1] = WTZ[c1] + FMOVE * tz(); WUU[c1] = WUU[c1] + FMOVE * DUU[c];
+          WVV[c1] = WVV[c1] + FMOVE * DVV[c]; WWW[c1] = WWW[c1] + FMOVE * ww();
+          WFF[c1] = WFF[c1] + FMOVE;
+        }
+      }
+      if (FF[c] > FL && NF[c] == 8) {
+        const double FOLD = FF[c] * X_(2, I) * Y_(2, J) * Z_(2, K) * GGV[c];
+        WTX[c] = WTX[c] + FOLD * tx(); WTY[c] = WTY[c] + FOLD * ty();
+        WTZ[c] = WTZ[c] + FOLD * tz(); WUU[c] = WUU[c] + FOLD * DUU[c];
+        WVV[c] = WVV[c] + FOLD * DVV[c]; WWW[c] = WWW[c] + FOLD * ww();
+        WFF[c] = WFF[c] + FOLD;
+      } else {
+        drop_clear(c);
+      }
+    };
+    // the reference's loop nests: the swept index outermost
+    for (int a = st; dl > 0 ? a <= en : a >= en; a += dl) {
+      if (ax == 0) { for (int K = 2; K <= NK - 1; ++K) for (int J = 2; J <= NJ - 1; ++J) cell(a, J, K); }
+      else if (ax == 1) { for (int K = 2; K <= NK - 1; ++K) for (int I = 2; I <= NI - 1; ++I) cell(I, a, K); }
+      else { for (int J = 2; J <= NJ - 1; ++J) for (int I = 2; I <= NI - 1; ++I) cell(I, J, a); }
+    }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          if (!(FF[c] > FL && NF[c] == 8)) continue;
+          const double W = 1.0 / WFF[c];
+          DTX[c] = WTX[c] * W; DTY[c] = WTY[c] * W; DTZ[c] = WTZ[c] * W;
+          DUU[c] = WUU[c] * W; DVV[c] = WVV[c] * W; DWW[c] = WWW[c] * W;
+          if (ax == 2 && L == 1) {  // stopped under a ceiling (:590-597)
+            const double X = std::sqrt(2.0 * G * Z_(2, K));
+            if (NF[id(I, J, K + 1)] == -1 && DWW[c] > X) { DUU[c] = 0.0; DVV[c] = 0.0; DWW[c] = 0.0; }
+          }
+        }
+  }
+
+  // VF_FDROPF  vf_fdropf.f:63-671
+  void fdropf() {
+    if (DTX.size() != FF.size()) drop_alloc();
+    drop_start();
+    for (int ax = 0; ax < 3; ++ax)
+      for (int L = 1; L <= 2; ++L) drop_move(ax, L);
+  }
+
   // VF_FNFPRV  vf_fnfprv.f:34-225
   int fnfprv() {
     for (int L = 0; L < NUMS; ++L) {
@@ -2204,6 +2389,11 @@ struct orc_handle {
       rc = fnfini();
       if (rc) return rc;
     }
+    if (P.idrop >= 1) {  // vf_f1cal.f:212-217
+      fdropf();
+      rc = fnfini();
+      if (rc) return rc;
+    }
     rc = fnfprv();
     if (rc) return rc;
     cindc();
@@ -2329,6 +2519,7 @@ int orc_init_state(orc_handle *h, int hydrostatic) {
   if (rc) return rc;
   h->bsuwt(); h->bsuwt2(); h->bsuwn3(); h->bspp(); h->bwuwt(); h->bwpp();
   std::fill(h->TBUB.begin(), h->TBUB.end(), 0.0);
+  h->drop_alloc();  // vf_cinit.f:416-427
   h->st.nums = h->NUMS;
   return CADMAS_OK;
 }
@@ -2390,6 +2581,25 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
 
 int orc_get_timers(orc_handle *h, double *t5) {
   for (int i = 0; i < 5; ++i) t5[i] = h->tmr[i];
+  return CADMAS_OK;
+}
+
+int orc_get_drop(orc_handle *h, double *tx, double *ty, double *tz, double *uu, double *vv, double *ww) {
+  if (h->DTX.size() != h->FF.size()) h->drop_alloc();
+  double *dst[6] = {tx, ty, tz, uu, vv, ww};
+  const vd *src[6] = {&h->DTX, &h->DTY, &h->DTZ, &h->DUU, &h->DVV, &h->DWW};
+  for (int a = 0; a < 6; ++a)
+    if (dst[a]) std::copy(src[a]->begin(), src[a]->end(), dst[a]);
+  return CADMAS_OK;
+}
+
+int orc_set_drop(orc_handle *h, const double *tx, const double *ty, const double *tz, const double *uu,
+                 const double *vv, const double *ww) {
+  if (h->DTX.size() != h->FF.size()) h->drop_alloc();
+  const double *src[6] = {tx, ty, tz, uu, vv, ww};
+  vd *dst[6] = {&h->DTX, &h->DTY, &h->DTZ, &h->DUU, &h->DVV, &h->DWW};
+  for (int a = 0; a < 6; ++a)
+    if (src[a]) std::copy(src[a], src[a] + dst[a]->size(), dst[a]->begin());
   return CADMAS_OK;
 }
 

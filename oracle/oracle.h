@@ -57,6 +57,10 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
 /* Seconds spent in the last orc_step by stage: [0] momentum predictor,
    [1] assembly, [2] solve, [3] correction+BC, [4] VOF+flags.              */
 int orc_get_timers(orc_handle *h, double *t5);
+/* DROPTX..DROPWW of the droplet model (NULL skipped), as cadmas_get_drop. */
+int orc_get_drop(orc_handle *h, double *tx, double *ty, double *tz, double *uu, double *vv, double *ww);
+int orc_set_drop(orc_handle *h, const double *tx, const double *ty, const double *tz, const double *uu,
+                 const double *vv, const double *ww);
 /* Threads the oracle's parallel loops use (OpenMP). */
 int orc_num_threads(void);
 

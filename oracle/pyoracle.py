@@ -59,6 +59,8 @@ def _load_lib():
     lib.orc_m1bcgs.argtypes = [C.c_void_p] + [dp] * 9 + [C.POINTER(C.c_int), C.POINTER(C.c_int), dp, dp]
     lib.orc_get_poisson.argtypes = [C.c_void_p, C.c_int, dp]
     lib.orc_get_timers.argtypes = [C.c_void_p, dp]
+    lib.orc_get_drop.argtypes = [C.c_void_p] + [dp] * 6
+    lib.orc_set_drop.argtypes = [C.c_void_p] + [dp] * 6
     lib.orc_num_threads.argtypes = []
     lib.orc_num_threads.restype = C.c_int
     _lib = lib
@@ -83,6 +85,7 @@ class Oracle:
             base.idamp[d] = -1
             base.damp[d][0], base.damp[d][1], base.damp[d][2], base.damp[d][3] = 0.6, 0.6, 0.0, 0.0
         base.icgtyp, base.icgmax, base.ibsuw0 = 1, 500, 0
+        base.idrop = 1
         self.params = P.make_params(case, base, **over)
         d = P.Dims(case.ni, case.nj, case.nk, case.numb)
         self.h = self.lib.orc_create(C.byref(d), C.byref(self.params), int(sum_mode))
@@ -114,6 +117,19 @@ class Oracle:
 
     def init_state(self, hydrostatic=True):
         self._rc(self.lib.orc_init_state(self.h, int(bool(hydrostatic))))
+
+    def get_drop(self):
+        """DROPTX..DROPWW as {droptx, ..., dropww}."""
+        c = self.case
+        arrs = {n: np.zeros(c.ni * c.nj * c.nk) for n in self.P.DROP_ARRAYS}
+        dp = C.POINTER(C.c_double)
+        self._rc(self.lib.orc_get_drop(self.h, *(arrs[n].ctypes.data_as(dp) for n in self.P.DROP_ARRAYS)))
+        return arrs
+
+    def set_drop(self, arrs):
+        keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64) for n in self.P.DROP_ARRAYS}
+        dp = C.POINTER(C.c_double)
+        self._rc(self.lib.orc_set_drop(self.h, *(keep[n].ctypes.data_as(dp) for n in self.P.DROP_ARRAYS)))
 
     def step(self, dt=None):
         self._rc(self.lib.orc_step(self.h, float(dt if dt is not None else self.case.dt)))

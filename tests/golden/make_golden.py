@@ -28,7 +28,9 @@ CASES = {
                                  steps=5, sum_mode=0, over={}),
     "bubble_tank_6": dict(builder="random_tank", kw=dict(seed=9), steps=6, sum_mode=0,
                           over=dict(wbub=0.2)),
+    "droplet_tank_0_20": dict(builder="droplet_tank", kw=dict(seed=0), steps=20, sum_mode=0, over={}),
 }
+DROP = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 FIELDS = ("uu", "vv", "ww", "pp", "ff", "nf", "indc", "bcu", "bcv", "bcw", "bcp", "bcf")
 
 
@@ -42,11 +44,17 @@ def run(name, spec):
     c = getattr(P.cases, spec["builder"])(**spec["kw"])
     o = O.Oracle(c, sum_mode=spec["sum_mode"], **spec["over"])
     o.init_state(c.hydrostatic)
+    drops = getattr(c, "drop_state", None)
+    if drops is not None:  # droplets already in flight (cases.droplet_tank)
+        o.set_drop(drops)
     for _ in range(spec["steps"]):
         o.step(c.dt)
     st = o.stats()
-    return dict(digest=digest(o.get_state()),
-                stats={k: st[k] for k in ("fsum", "fcut", "cgbnrm", "cgxnrm", "icgitr", "nums")})
+    dig = digest(o.get_state())
+    if drops is not None:
+        d = o.get_drop()
+        dig.update({n: hashlib.sha256(d[n].tobytes()).hexdigest()[:32] for n in DROP})
+    return dict(digest=dig, stats={k: st[k] for k in ("fsum", "fcut", "cgbnrm", "cgxnrm", "icgitr", "nums")})
 
 
 if __name__ == "__main__":

@@ -42,6 +42,32 @@ def run_pair(pkg, orc, case, steps, check_every=1, **over):
     return t, o
 
 
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_droplets_bitwise(gpu_lib, pkg, orc, seed):
+    """The TimerDoor droplet model (VF_FDROPF, k_drop.cu) with droplets
+    already in flight: every field, flag and droplet array equals the
+    oracle's bit for bit."""
+    c = pkg.cases.droplet_tank(seed)
+    t = pkg.Tank(c)
+    o = orc.Oracle(c, sum_mode=orc.SUM_GPU)
+    t.init_state(True)
+    o.init_state(True)
+    t.set_drop(c.drop_state)
+    o.set_drop(c.drop_state)
+    moved = 0
+    for n in range(1, 31):
+        t.step(c.dt)
+        o.step(c.dt)
+        if n % 5 == 0:
+            assert_same(t.get_state(), o.get_state(), f"step {n}")
+            dg, do = t.get_drop(), o.get_drop()
+            for k in pkg.DROP_ARRAYS:
+                assert dg[k].tobytes() == do[k].tobytes(), (n, k, np.abs(dg[k] - do[k]).max())
+            moved = max(moved, int((dg["droptx"] > -1e9).sum()))
+            assert t.stats()["fsum"] == o.stats()["fsum"]
+    assert moved >= 7  # droplets were present throughout
+
+
 def test_dam_break_bitwise(gpu_lib, pkg, orc):
     c = pkg.cases.dam_break()
     t, o = run_pair(pkg, orc, c, 30, check_every=5)

@@ -165,3 +165,55 @@ def test_wave_maker_injects_the_table_wave(pkg, orc):
         o.step(c.dt)
     assert o.stats()["fsum"] > v0
     assert o.stats()["icgitr"] < 500
+
+
+def test_droplets_move_water_and_conserve_it(pkg, orc):
+    """VF_FDROPF: with IDROP=1 the droplet water moves (cells' F change and
+    droplets split); the total volume FSUM + cut-off stays within rounding
+    plus the cut-off of tiny leftovers; with IDROP=0 the droplet cells keep
+    their water (gas cells carry no flux)."""
+    c = pkg.cases.droplet_tank(0)
+    runs = {}
+    for idrop in (0, 1):
+        o = orc.Oracle(c, idrop=idrop)
+        o.init_state(True)
+        o.set_drop(c.drop_state)
+        v0 = o.stats()["fsum"]
+        f0 = o.get_state()["ff"].copy()
+        cut = 0.0
+        for _ in range(20):
+            o.step(c.dt)
+            cut += o.stats()["fcut"]
+        st = o.get_state()
+        runs[idrop] = (f0, st["ff"], o.get_drop(), o.stats()["fsum"], v0, cut)
+    f0, f1, d1, v1, v0, cut = runs[1]
+    drop0 = c.drop_state["droptx"] > -1e9
+    assert np.abs(f1 - f0).max() > 0.1                       # droplet water moved
+    assert int((d1["droptx"] > -1e9).sum()) > int(drop0.sum())  # and split over more cells
+    assert abs(v1 + cut - v0) <= 1e-9 * v0
+    f0n, f1n = runs[0][0], runs[0][1]
+    np.testing.assert_array_equal(f1n.reshape(-1, order="F")[drop0], f0n.reshape(-1, order="F")[drop0])
+
+
+def test_droplet_free_fall_time(pkg, orc):
+    """A droplet at rest in the air leaves its cell after the free-fall time
+    of one cell, sqrt(2 dz / g) (vf_fdropf.f:548-556), and not before."""
+    c = pkg.cases.droplet_tank(1, ndrop=1)
+    o = orc.Oracle(c)
+    o.init_state(True)
+    ds = {k: v.copy() for k, v in c.drop_state.items()}
+    cell = int(np.argmax(ds["droptx"] > -1e9))
+    for k in ("dropuu", "dropvv", "dropww"):
+        ds[k][cell] = 0.0
+    o.set_drop(ds)
+    f0 = o.get_state()["ff"].reshape(-1, order="F")[cell]
+    ni, nj = c.ni, c.nj
+    kc = cell // (ni * nj)
+    dz = c.zz[1, kc]
+    t_fall = np.sqrt(2.0 * dz / 9.8)
+    left = None
+    for n in range(1, int(2 * t_fall / c.dt) + 3):
+        o.step(c.dt)
+        if o.get_state()["ff"].reshape(-1, order="F")[cell] < f0 and left is None:
+            left = n * c.dt
+    assert left is not None and t_fall < left <= t_fall + 2 * c.dt
