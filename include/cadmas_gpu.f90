@@ -25,7 +25,7 @@ module cadmas_gpu
   integer(c_int), parameter :: CADMAS_OK = 0, CADMAS_EINVAL = 1, CADMAS_ECUDA = 2, &
        CADMAS_ENOTCONV = 3, CADMAS_EDIVERGE = 4, CADMAS_EPIVOT = 5, CADMAS_EPG = 6, &
        CADMAS_ECAP = 7, CADMAS_ENOMEM = 8, CADMAS_EUNSUPPORTED = 9, CADMAS_ENOSTATIC = 10, &
-       CADMAS_ETIMEOUT = 11, CADMAS_ESCRATCH = 12
+       CADMAS_ETIMEOUT = 11, CADMAS_ESCRATCH = 12, CADMAS_EIO = 13
 
   type, bind(C) :: cadmas_dims
      integer(c_int) :: numi, numj, numk, numb
@@ -125,6 +125,27 @@ module cadmas_gpu
        real(c_double), intent(inout) :: tnow
        integer(c_int), intent(inout) :: nnow
      end function vf_step_gpu
+
+     ! Restart file of the reference (vf_or1ini.f / vf_or1trn.f / vf_ir1inp.f);
+     ! path is a NUL-terminated name (TRIM(NAME)//C_NULL_CHAR).
+     integer(c_int) function cadmas_restart_create(h, path) bind(C, name='cadmas_restart_create')
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+     end function cadmas_restart_create
+
+     integer(c_int) function cadmas_restart_append(h, path) bind(C, name='cadmas_restart_append')
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+     end function cadmas_restart_append
+
+     integer(c_int) function cadmas_restart_load(h, path, nnow) bind(C, name='cadmas_restart_load')
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+       integer(c_int), value :: nnow
+     end function cadmas_restart_load
 
      type(c_ptr) function cadmas_strerror(status) bind(C, name='cadmas_strerror')
        import :: c_int, c_ptr

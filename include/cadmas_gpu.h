@@ -27,6 +27,7 @@
  */
 #ifndef CADMAS_GPU_H
 #define CADMAS_GPU_H
+#include <stddef.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -47,6 +48,9 @@ extern "C" {
 #define CADMAS_ETIMEOUT     11  /* a device-side wait ran out of time (2 s)      */
 #define CADMAS_ESCRATCH     12  /* grid larger than the static scratch of
                                    cadmas_divnorm_noalloc                       */
+#define CADMAS_EIO          13  /* restart file: cannot open, read or write, or
+                                   a mismatch ('INVALID NUMBER OF GRID.' etc.,
+                                   vf_ir1inp.f); cadmas_strerror has the text */
 
 /* ---- sizes (/VF_ANUMBI/, VF_ANUMBI.h) ----------------------------------- */
 typedef struct cadmas_dims {
@@ -212,6 +216,34 @@ int cadmas_get_drop(cadmas_handle *h, double *droptx, double *dropty, double *dr
                     double *dropvv, double *dropww);
 int cadmas_set_drop(cadmas_handle *h, const double *droptx, const double *dropty, const double *droptz,
                     const double *dropuu, const double *dropvv, const double *dropww);
+
+/* ---- restart file (*.rsl / *.res) and list file ----------------------
+   The restart file of the reference, byte for byte: a Fortran unformatted
+   sequential file (each record framed by its byte count as a 4-byte
+   little-endian integer, as gfortran writes one WRITE statement), NPROCS=1.
+   cadmas_restart_create writes the header of VF_OR1INI (vf_or1ini.f:38-86):
+   version (0,1); NUMI,NUMJ,NUMK,NUMB; the flags LN..L1 of the fields
+   present (k-eps, temperature and scalars 0, droplets = IDROP >= 1); GGV.
+   cadmas_restart_append writes one output of VF_OR1TRN (vf_or1trn.f:
+   104-221) of the present state: NNOW,TNOW,DTNOW; FSUM,FCUT,CGBNRM,CGXNRM,
+   ICGITR; NF; UU,BCU; VV,BCV; WW,BCW; PP,BCP; FF,BCF; TBUB; with droplets
+   the count of cells with DROPTX >= 0 and one record I,J,K,DROPTX..DROPWW
+   each.  When to write (IRSTYP, vf_or1trn.f:87-101) is the caller's call.
+   cadmas_restart_load is VF_IR1INP (vf_ir1inp.f:96-336): it checks the
+   header against the handle (errors 'INVALID NUMBER OF GRID.', 'INVALID
+   NUMBER OF B.C.', 'INVALID EQUATION (...)' as CADMAS_EIO), reads the
+   outputs up to the one of step nnow ('INVALID STEP.' if absent) and makes
+   it the present state, INDC from NF as VF_CINDC.  Records of 2^31 bytes
+   or more (a single 3-D field above 268 M cells) are refused.            */
+int cadmas_restart_create(cadmas_handle *h, const char *path);
+int cadmas_restart_append(cadmas_handle *h, const char *path);
+int cadmas_restart_load(cadmas_handle *h, const char *path, int nnow);
+/* The two lines the time loop writes to the list file after each step
+   (vf_a1main.f:954-958, formats 9540 and 9550 of vf_a1main.f:1214-1223):
+   STEP, TIME, DT, FSUM, FCUT and !VD! (VF_CDIV00, computed here), then
+   !B!, !R! and ITR of the last solve; Fortran 1PE12.5 and I6 fields, each
+   line ending in a newline, NUL-terminated in buf (len >= 200 is ample). */
+int cadmas_list_step(cadmas_handle *h, char *buf, size_t len);
 
 /* Initial classification and boundary values of VF_CINIT
    (vf_cinit.f:202-207 and the BC calls after :283): FCUT01, BWFF, FNFINI,

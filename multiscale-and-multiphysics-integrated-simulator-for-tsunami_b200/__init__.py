@@ -25,7 +25,8 @@ from . import cases  # noqa: F401  (re-exported)
 HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = HERE / "libcadmas_gpu.so"
 
-OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC, ETIMEOUT, ESCRATCH = range(13)
+(OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC, ETIMEOUT, ESCRATCH,
+ EIO) = range(14)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -94,7 +95,8 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
             "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers", "cadmas_get_drop",
-            "cadmas_set_drop"]
+            "cadmas_set_drop", "cadmas_restart_create", "cadmas_restart_append", "cadmas_restart_load",
+            "cadmas_list_step"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 
@@ -136,6 +138,10 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_set_state.argtypes = [C.c_void_p, C.POINTER(State)]
     lib.cadmas_get_state.argtypes = [C.c_void_p, C.POINTER(State)]
     lib.cadmas_get_drop.argtypes = [C.c_void_p] + [_dp] * 6
+    lib.cadmas_restart_create.argtypes = [C.c_void_p, C.c_char_p]
+    lib.cadmas_restart_append.argtypes = [C.c_void_p, C.c_char_p]
+    lib.cadmas_restart_load.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+    lib.cadmas_list_step.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     lib.cadmas_set_drop.argtypes = [C.c_void_p] + [_dp] * 6
     lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
     lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
@@ -296,6 +302,24 @@ class Tank:
         arrs = {n: np.zeros(self.case.ni * self.case.nj * self.case.nk) for n in DROP_ARRAYS}
         _check(self.lib, self.lib.cadmas_get_drop(self.h, *(_dptr(arrs[n]) for n in DROP_ARRAYS)))
         return arrs
+
+    def restart_create(self, path):
+        """Header of a restart file (VF_OR1INI)."""
+        _check(self.lib, self.lib.cadmas_restart_create(self.h, str(path).encode()))
+
+    def restart_append(self, path):
+        """One output of the present state (VF_OR1TRN)."""
+        _check(self.lib, self.lib.cadmas_restart_append(self.h, str(path).encode()))
+
+    def restart_load(self, path, nnow):
+        """The state of step nnow from a restart file (VF_IR1INP)."""
+        _check(self.lib, self.lib.cadmas_restart_load(self.h, str(path).encode(), int(nnow)))
+
+    def list_step(self):
+        """The list-file lines of the last step (formats 9540 and 9550)."""
+        buf = C.create_string_buffer(512)
+        _check(self.lib, self.lib.cadmas_list_step(self.h, buf, 512))
+        return buf.value.decode()
 
     def set_drop(self, arrs):
         keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64) for n in DROP_ARRAYS}

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -691,6 +692,61 @@ static int do_f1cal(cadmas_handle *h) {
   return map_err(bits);
 }
 
+// ====================================================== restart and list I/O
+// Fortran unformatted sequential records as gfortran writes them: each
+// WRITE is one record, its bytes framed by their count as a 4-byte native
+// (little-endian) integer before and after.  Records of 2^31 bytes or more
+// would need split markers; they are refused.
+struct FRecordFile {
+  FILE *f = nullptr;
+  ~FRecordFile() { if (f) std::fclose(f); }
+  bool put(std::initializer_list<std::pair<const void *, size_t>> parts) {
+    size_t n = 0;
+    for (auto &p : parts) n += p.second;
+    if (n > 0x7fffffffu - 8) return false;
+    const int32_t m = (int32_t)n;
+    if (std::fwrite(&m, 4, 1, f) != 1) return false;
+    for (auto &p : parts)
+      if (p.second && std::fwrite(p.first, 1, p.second, f) != p.second) return false;
+    return std::fwrite(&m, 4, 1, f) == 1;
+  }
+  // One record into buf; false at the end of the file or on a bad frame.
+  bool get(std::vector<unsigned char> &buf, bool *eof = nullptr) {
+    int32_t m = 0, t = 0;
+    if (std::fread(&m, 4, 1, f) != 1) { if (eof) *eof = true; return false; }
+    if (m < 0) return false;
+    buf.resize((size_t)m);
+    if (m && std::fread(buf.data(), 1, (size_t)m, f) != (size_t)m) return false;
+    return std::fread(&t, 4, 1, f) == 1 && t == m;
+  }
+};
+template <typename T> static T rec_at(const std::vector<unsigned char> &b, size_t off) {
+  T v;
+  std::memcpy(&v, b.data() + off, sizeof(T));
+  return v;
+}
+
+// Fortran edit descriptors of the list file: 1PE12.5 and I6.
+static std::string f_e12_5(double v) {
+  char b[64];
+  if (std::isnan(v)) { std::snprintf(b, sizeof b, "%12s", "NaN"); return b; }
+  if (std::isinf(v)) { std::snprintf(b, sizeof b, "%12s", v < 0 ? "-Infinity" : "Infinity"); return b; }
+  std::snprintf(b, sizeof b, "%.5E", v);  // d.dddddE+xx or d.dddddE+xxx
+  std::string t(b);
+  const size_t e = t.find('E');
+  std::string mant = t.substr(0, e), ex = t.substr(e + 1);  // ex: sign and digits
+  const int digits = (int)ex.size() - 1;
+  std::string out = digits <= 2 ? mant + "E" + ex : mant + ex;  // E dropped for 3-digit exponents
+  if (out.size() < 12) out = std::string(12 - out.size(), ' ') + out;
+  return out.size() > 12 ? std::string(12, '*') : out;
+}
+static std::string f_i6(int v) {
+  char b[32];
+  std::snprintf(b, sizeof b, "%6d", v);
+  std::string t(b);
+  return t.size() > 6 ? std::string(6, '*') : t;
+}
+
 // ============================================================== C ABI
 extern "C" {
 
@@ -709,6 +765,7 @@ const char *cadmas_strerror(int status) {
     case CADMAS_ENOSTATIC: return "static fields not uploaded";
     case CADMAS_ETIMEOUT: return "a device-side wait ran out of time";
     case CADMAS_ESCRATCH: return "grid has more than CADMAS_NOALLOC_MAX_ROWS (65536) rows NUMJ*NUMK";
+    case CADMAS_EIO: return g_last_error.empty() ? "restart file I/O error" : g_last_error.c_str();
     default: return "unknown status";
   }
 }
@@ -991,6 +1048,199 @@ int cadmas_set_drop(cadmas_handle *h, const double *tx, const double *ty, const 
   for (int a = 0; a < 6; ++a)
     if (src[a]) CK(cudaMemcpyAsync(dst[a], src[a], b8, cudaMemcpyHostToDevice, h->s));
   CK(cudaStreamSynchronize(h->s));
+  return CADMAS_OK;
+}
+
+// VF_OR1INI (vf_or1ini.f:38-86) for NPROCS = 1: version, sizes, the
+// flags of the fields that follow every output, GGV.
+int cadmas_restart_create(cadmas_handle *h, const char *path) {
+  if (!h || !path) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  FRecordFile r;
+  r.f = std::fopen(path, "wb");
+  if (!r.f) { g_last_error = "CAN NOT OPEN (*****.rsl)."; return CADMAS_EIO; }
+  const int32_t ver[2] = {0, 1};  // IVR001, IVR002 (VF_A0PRM.h)
+  const int32_t dims[4] = {h->g.NI, h->g.NJ, h->g.NK, h->g.NB};
+  // LN, LV, LP, LF, LK, LT, LS, LG, LD, L1: no k-eps, temperature, scalars
+  // or time-dependent porosity here; droplets when IDROP >= 1
+  const int32_t flags[10] = {1, 1, 1, 1, 0, 0, 0, 0, h->P.idrop >= 1 ? 1 : 0, 0};
+  std::vector<double> ggv(h->N);
+  CK(cudaMemcpy(ggv.data(), h->ggv, h->N * sizeof(double), cudaMemcpyDeviceToHost));
+  if (!r.put({{ver, sizeof ver}}) || !r.put({{dims, sizeof dims}}) || !r.put({{flags, sizeof flags}}) ||
+      !r.put({{ggv.data(), h->N * sizeof(double)}})) {
+    g_last_error = "WRITE ERROR (*****.rsl).";
+    return CADMAS_EIO;
+  }
+  return CADMAS_OK;
+}
+
+// VF_OR1TRN (vf_or1trn.f:104-221): one output of the present state
+// appended to a file made by cadmas_restart_create.
+int cadmas_restart_append(cadmas_handle *h, const char *path) {
+  if (!h || !path) return CADMAS_EINVAL;
+  const size_t N = h->N, NB = (size_t)h->g.NB;
+  std::vector<double> a[5];
+  std::vector<double> bc[5];
+  std::vector<int32_t> nf(N);
+  cadmas_state st;
+  std::memset(&st, 0, sizeof st);
+  for (int k = 0; k < 5; ++k) { a[k].resize(N); bc[k].resize(NB); }
+  st.uu = a[0].data(); st.vv = a[1].data(); st.ww = a[2].data(); st.pp = a[3].data(); st.ff = a[4].data();
+  st.nf = nf.data();
+  if (NB) { st.bcu = bc[0].data(); st.bcv = bc[1].data(); st.bcw = bc[2].data(); st.bcp = bc[3].data(); st.bcf = bc[4].data(); }
+  int rc = cadmas_get_state(h, &st);
+  if (rc) return rc;
+  std::vector<double> dr[6];
+  for (auto &v : dr) v.resize(N);
+  if (h->P.idrop >= 1) {
+    rc = cadmas_get_drop(h, dr[0].data(), dr[1].data(), dr[2].data(), dr[3].data(), dr[4].data(), dr[5].data());
+    if (rc) return rc;
+  }
+  FRecordFile r;
+  r.f = std::fopen(path, "ab");
+  if (!r.f) { g_last_error = "CAN NOT OPEN (*****.rsl)."; return CADMAS_EIO; }
+  const int32_t nnow = h->nnow, icgitr = h->stats.icgitr;
+  const double tn = h->tnow, dtn = h->dtnow;
+  const double sums[4] = {h->stats.fsum, h->stats.fcut, h->stats.cgbnrm, h->stats.cgxnrm};
+  const size_t b8 = N * sizeof(double), bb = NB * sizeof(double);
+  bool ok = r.put({{&nnow, 4}, {&tn, 8}, {&dtn, 8}}) && r.put({{sums, sizeof sums}, {&icgitr, 4}}) &&
+            r.put({{nf.data(), N * 4}});
+  for (int k = 0; k < 5 && ok; ++k) ok = r.put({{a[k].data(), b8}}) && r.put({{bc[k].data(), bb}});
+  ok = ok && r.put({{h->tbub.data(), (size_t)h->g.NK * sizeof(double)}});
+  if (ok && h->P.idrop >= 1) {
+    // the droplet cells (DROPTX >= 0), K, J, I order
+    const int NI = h->g.NI, NJ = h->g.NJ, NK = h->g.NK;
+    std::vector<size_t> cells;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = (size_t)(I - 1) + (size_t)NI * ((size_t)(J - 1) + (size_t)NJ * (K - 1));
+          if (dr[0][c] >= 0.0) cells.push_back(c);
+        }
+    const int32_t nd = (int32_t)cells.size();
+    ok = r.put({{&nd, 4}});
+    for (size_t c : cells) {
+      if (!ok) break;
+      const int32_t ijk[3] = {(int32_t)(c % NI) + 1, (int32_t)((c / NI) % NJ) + 1, (int32_t)(c / ((size_t)NI * NJ)) + 1};
+      const double v[6] = {dr[0][c], dr[1][c], dr[2][c], dr[3][c], dr[4][c], dr[5][c]};
+      ok = r.put({{ijk, sizeof ijk}, {v, sizeof v}});
+    }
+  }
+  if (!ok) { g_last_error = "WRITE ERROR (*****.rsl)."; return CADMAS_EIO; }
+  return CADMAS_OK;
+}
+
+// VF_IR1INP (vf_ir1inp.f:96-336) for NPROCS = 1: read the outputs of a
+// restart file up to the one of step nnow and make it the present state
+// (time, step, sums, flags, fields, boundary values, TBUB, droplets), with
+// INDC from NF (VF_CINDC).
+int cadmas_restart_load(cadmas_handle *h, const char *path, int nnow) {
+  if (!h || !path) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  FRecordFile r;
+  r.f = std::fopen(path, "rb");
+  if (!r.f) { g_last_error = "CAN NOT OPEN (*****.res)."; return CADMAS_EIO; }
+  const size_t N = h->N, NB = (size_t)h->g.NB, NK = (size_t)h->g.NK;
+  auto bad = [&](const char *m) { g_last_error = m; return CADMAS_EIO; };
+  std::vector<unsigned char> b;
+  if (!r.get(b) || b.size() != 8) return bad("READ ERROR (*****.res).");
+  if (!r.get(b) || b.size() != 16) return bad("READ ERROR (*****.res).");
+  if (rec_at<int32_t>(b, 0) != h->g.NI || rec_at<int32_t>(b, 4) != h->g.NJ || rec_at<int32_t>(b, 8) != h->g.NK)
+    return bad("INVALID NUMBER OF GRID.");
+  if (rec_at<int32_t>(b, 12) != h->g.NB) return bad("INVALID NUMBER OF B.C.");
+  if (!r.get(b) || b.size() != 40) return bad("READ ERROR (*****.res).");
+  int32_t L[10];
+  std::memcpy(L, b.data(), sizeof L);
+  if (L[4] != 0) return bad("INVALID EQUATION (K-EPS).");
+  if (L[5] != 0) return bad("INVALID EQUATION (TEMP).");
+  if (L[6] != 0) return bad("INVALID EQUATION (CONC).");
+  const int LG = L[7], LD = L[8];
+  if (LG == 0 && (!r.get(b) || b.size() != N * 8)) return bad("READ ERROR (*****.res).");  // GGV, unused
+  std::vector<unsigned char> rec[14];
+  for (;;) {
+    bool eof = false;
+    if (!r.get(rec[0], &eof)) return bad(eof ? "INVALID STEP." : "READ ERROR (*****.res).");
+    if (rec[0].size() != 20) return bad("READ ERROR (*****.res).");
+    // rec[1] sums, [2] NF, [3] UU, [4] BCU, [5] VV, [6] BCV, [7] WW, [8] BCW,
+    // [9] PP, [10] BCP, [11] FF, [12] BCF, (GGV when LG != 0), [13] TBUB
+    const size_t want[12] = {36, N * 4, N * 8, NB * 8, N * 8, NB * 8, N * 8, NB * 8, N * 8, NB * 8, N * 8, NB * 8};
+    for (int k = 1; k <= 12; ++k)
+      if (!r.get(rec[k]) || rec[k].size() != want[k - 1]) return bad("READ ERROR (*****.res).");
+    if (LG != 0 && !r.get(b)) return bad("READ ERROR (*****.res).");  // GGV of IPRNT > 1, unused
+    if (!r.get(rec[13]) || rec[13].size() != NK * 8) return bad("READ ERROR (*****.res).");
+    const int32_t step = rec_at<int32_t>(rec[0], 0);
+    std::vector<double> dr[6];
+    if (LD >= 1) {
+      if (!r.get(b) || b.size() != 4) return bad("READ ERROR (*****.res).");
+      const int32_t nd = rec_at<int32_t>(b, 0);
+      const bool use = h->P.idrop >= 1 && step == nnow;
+      if (use) {
+        for (auto &v : dr) v.assign(N, 0.0);
+        std::fill(dr[0].begin(), dr[0].end(), -1.0e10);
+      }
+      for (int32_t n = 0; n < nd; ++n) {
+        if (!r.get(b) || b.size() != 60) return bad("READ ERROR (*****.res).");
+        if (!use) continue;
+        const int I = rec_at<int32_t>(b, 0), J = rec_at<int32_t>(b, 4), K = rec_at<int32_t>(b, 8);
+        if (I < 1 || I > h->g.NI || J < 1 || J > h->g.NJ || K < 1 || K > h->g.NK) return bad("READ ERROR (*****.res).");
+        const size_t c = (size_t)(I - 1) + (size_t)h->g.NI * ((size_t)(J - 1) + (size_t)h->g.NJ * (K - 1));
+        for (int a = 0; a < 6; ++a) dr[a][c] = rec_at<double>(b, 12 + 8 * a);
+      }
+    }
+    if (step != nnow) continue;
+    // the output of step nnow: make it the state
+    cadmas_state st;
+    std::memset(&st, 0, sizeof st);
+    st.nf = reinterpret_cast<int *>(rec[2].data());
+    st.uu = reinterpret_cast<double *>(rec[3].data()); st.vv = reinterpret_cast<double *>(rec[5].data());
+    st.ww = reinterpret_cast<double *>(rec[7].data()); st.pp = reinterpret_cast<double *>(rec[9].data());
+    st.ff = reinterpret_cast<double *>(rec[11].data());
+    if (NB) {
+      st.bcu = reinterpret_cast<double *>(rec[4].data()); st.bcv = reinterpret_cast<double *>(rec[6].data());
+      st.bcw = reinterpret_cast<double *>(rec[8].data()); st.bcp = reinterpret_cast<double *>(rec[10].data());
+      st.bcf = reinterpret_cast<double *>(rec[12].data());
+    }
+    st.tbub = reinterpret_cast<double *>(rec[13].data());
+    st.tnow = rec_at<double>(rec[0], 4);
+    st.nnow = step;
+    int rc = cadmas_set_state(h, &st);
+    if (rc) return rc;
+    h->dtnow = rec_at<double>(rec[0], 12);
+    h->stats.fsum = rec_at<double>(rec[1], 0); h->stats.fcut = rec_at<double>(rec[1], 8);
+    h->stats.cgbnrm = rec_at<double>(rec[1], 16); h->stats.cgxnrm = rec_at<double>(rec[1], 24);
+    h->stats.icgitr = rec_at<int32_t>(rec[1], 32);
+    if (h->P.idrop >= 1) {
+      if (LD >= 1) rc = cadmas_set_drop(h, dr[0].data(), dr[1].data(), dr[2].data(), dr[3].data(), dr[4].data(), dr[5].data());
+      else launch_drop_reset(h->s, (long long)N, h->drop);  // vf_ir1inp.f:96-108
+      if (rc) return rc;
+    }
+    // INDC from NF (vf_ir1inp.f:316-322)
+    refresh_fld(h);
+    CK(cudaMemsetAsync(h->indc, 0xff, N * sizeof(int), h->s));
+    CK(cudaMemsetAsync(h->dint + 4, 0, sizeof(int), h->s));
+    launch_cindc(h->s, h->g, h->f, h->dint + 4);
+    int bits;
+    rc = read_err(h, bits);
+    if (rc) return rc;
+    h->stats.nums = h->h_int[4];
+    return CADMAS_OK;
+  }
+}
+
+// The two lines the time loop writes to the list file after a step
+// (vf_a1main.f:954-958, formats 9540 and 9550), with !VD! from VF_CDIV00.
+int cadmas_list_step(cadmas_handle *h, char *buf, size_t len) {
+  if (!h || !buf || len == 0) return CADMAS_EINVAL;
+  double dv;
+  int rc = cadmas_divnorm(h, &dv);
+  if (rc) return rc;
+  const cadmas_stats &S = h->stats;
+  std::string t = " STEP=" + f_i6(h->nnow) + " : TIME= " + f_e12_5(h->tnow) + " : DT  = " + f_e12_5(h->dtnow) +
+                  " : FSUM= " + f_e12_5(S.fsum) + " : FCUT= " + f_e12_5(S.fcut) + " : !VD!= " + f_e12_5(dv) + "\n" +
+                  " " + std::string(11, ' ') + " : !B! = " + f_e12_5(S.cgbnrm) + " : !R! = " + f_e12_5(S.cgxnrm) +
+                  " : ITR = " + f_i6(S.icgitr) + "\n";
+  if (t.size() + 1 > len) return CADMAS_EINVAL;
+  std::memcpy(buf, t.c_str(), t.size() + 1);
   return CADMAS_OK;
 }
 
