@@ -55,7 +55,7 @@ STAGE_BYTES = {
 # cell of one launch of each stage's dominant kernel, from an ncu capture of
 # the 256x32x96 flume with 16x16 tiles; the bench size has the same tile
 # shape, so the traffic per launch scales with the cells.
-NCU_TRAFFIC_PER_CELL = {"fwd": 97.9, "bwd": 52.7}
+NCU_TRAFFIC_PER_CELL = {"fwd": 97.4, "bwd": 52.6}
 
 
 def _load_pkg():
