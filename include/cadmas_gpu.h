@@ -238,6 +238,18 @@ int cadmas_set_drop(cadmas_handle *h, const double *droptx, const double *dropty
 int cadmas_restart_create(cadmas_handle *h, const char *path);
 int cadmas_restart_append(cadmas_handle *h, const char *path);
 int cadmas_restart_load(cadmas_handle *h, const char *path, int nnow);
+/* VF_CDTCAL (vf_cdtcal.f:46-147), the adaptive time step of IDTTYP = 1
+   (the reference's default): the next step's DT from the present state,
+   DT = MAX(MIN(dtlim*DTSAFE, 1.2*W), DTMIN) with W = DTNOW of the last step
+   (DTINIT before the first), where dtlim is the smallest of DTMAX/DTSAFE
+   and every cell's advective limit V/max|face flux| and diffusive limit
+   0.5/(1/DX^2+1/DY^2+1/DZ^2)/ANU.  The reference folds the limits into a
+   running DT in K,J,I order, whose rounding can differ from the smallest
+   limit in the last bits; this function takes the smallest limit itself.
+   Reference defaults: DTINIT 1e-6, DTMIN 0, DTMAX 1e20, DTSAFE 0.1
+   (vf_a2dflt.f:230-234).                                                  */
+int cadmas_cdtcal(cadmas_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt);
+
 /* The two lines the time loop writes to the list file after each step
    (vf_a1main.f:954-958, formats 9540 and 9550 of vf_a1main.f:1214-1223):
    STEP, TIME, DT, FSUM, FCUT and !VD! (VF_CDIV00, computed here), then

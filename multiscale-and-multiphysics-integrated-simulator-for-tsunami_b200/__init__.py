@@ -96,7 +96,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers", "cadmas_get_drop",
             "cadmas_set_drop", "cadmas_restart_create", "cadmas_restart_append", "cadmas_restart_load",
-            "cadmas_list_step"]
+            "cadmas_list_step", "cadmas_cdtcal"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 
@@ -142,6 +142,7 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_restart_append.argtypes = [C.c_void_p, C.c_char_p]
     lib.cadmas_restart_load.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
     lib.cadmas_list_step.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.cadmas_cdtcal.argtypes = [C.c_void_p] + [C.c_double] * 4 + [C.POINTER(C.c_double)]
     lib.cadmas_set_drop.argtypes = [C.c_void_p] + [_dp] * 6
     lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
     lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
@@ -314,6 +315,12 @@ class Tank:
     def restart_load(self, path, nnow):
         """The state of step nnow from a restart file (VF_IR1INP)."""
         _check(self.lib, self.lib.cadmas_restart_load(self.h, str(path).encode(), int(nnow)))
+
+    def cdtcal(self, dtinit=1.0e-6, dtmin=0.0, dtmax=1.0e20, dtsafe=0.1):
+        """The next step's DT of VF_CDTCAL (defaults of vf_a2dflt.f:230-234)."""
+        dt = C.c_double()
+        _check(self.lib, self.lib.cadmas_cdtcal(self.h, dtinit, dtmin, dtmax, dtsafe, C.byref(dt)))
+        return dt.value
 
     def list_step(self):
         """The list-file lines of the last step (formats 9540 and 9550)."""

@@ -852,7 +852,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
       rc = rc ? rc : CADMAS_EINVAL;
     }
   }
-  AL(h->rb0, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->rb1, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->dres, 8);
+  AL(h->rb0, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->rb1, (size_t)std::max<long long>(nrows(h), h->nslab)); AL(h->dres, 10);
   AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
   AL(h->drop.tx, h->N); AL(h->drop.ty, h->N); AL(h->drop.tz, h->N);
   AL(h->drop.uu, h->N); AL(h->drop.vv, h->N); AL(h->drop.ww, h->N);
@@ -863,7 +863,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
 #undef AL
   if (!rc && cudaMallocHost((void **)&h->h_st, sizeof(SolveState)) != cudaSuccess) rc = CADMAS_ENOMEM;
   if (!rc && cudaMallocHost((void **)&h->h_int, 8 * sizeof(int)) != cudaSuccess) rc = CADMAS_ENOMEM;
-  if (!rc && cudaMallocHost((void **)&h->h_res, 8 * sizeof(double)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMallocHost((void **)&h->h_res, 10 * sizeof(double)) != cudaSuccess) rc = CADMAS_ENOMEM;
   if (rc) { cadmas_destroy(h); return rc; }
   // NF starts as all obstacle until set_state; INDC as non-computed.
   cudaMemset(h->nf, 0xff, h->N * sizeof(int));
@@ -1359,6 +1359,21 @@ int cadmas_step_ensemble(cadmas_handle **hs, int n, const double *dt, int *statu
   for (std::thread &t : pool) t.join();
   for (int i = 0; i < n; ++i)
     if (status[i]) return status[i];
+  return CADMAS_OK;
+}
+
+// VF_CDTCAL (vf_cdtcal.f:46-147): the time step for the next step from
+// the present state; the caller's DTINIT, DTMIN, DTMAX and DTSAFE.
+int cadmas_cdtcal(cadmas_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt) {
+  if (!h || !dt || !(dtsafe > 0.0)) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  refresh_fld(h);
+  const double w = (h->nnow == 0) ? dtinit : h->dtnow;
+  launch_cdtcal(h->s, h->g, h->f, h->rb0, dtmax / dtsafe, dtsafe, w, dtmin, h->dres + 8);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_res + 8, h->dres + 8, sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  *dt = h->h_res[8];
   return CADMAS_OK;
 }
 

@@ -506,6 +506,64 @@ __global__ void k_cdiv(Geo g, Fld f, double *rb) {
   row_store(s, rb, row, nrows);
 }
 
+// ----------------------------------------------------------- VF_CDTCAL
+// The time-step limits of vf_cdtcal.f:107-141 per cell with NF != -1: the
+// advective limit V/max|flux| (a boundary face of a dry cell and dry
+// boundary value does not count) and the diffusive limit
+// 0.5/(1/dx^2+1/dy^2+1/dz^2)/ANU.  The reference folds them into a running
+// DT = V/MAX(FL1..FL6, V/DT) in K,J,I order, which in exact arithmetic is
+// the minimum of the limits; here each limit is computed with the same
+// roundings and the minimum is taken directly (order-free), the form the
+// oracle's GPU order restates.  Row minima go to rb (+inf for none).
+__device__ __forceinline__ double dmin_ne(double a, double b) { return b < a ? b : a; }
+__global__ void k_cdtcal(Geo g, Fld f, double *rb) {
+  double m = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  const long long nrows = (long long)g.NJ * g.NK;
+  ROW_LOOP_BEGIN(g)
+  if (I >= 2 && I <= g.NI - 1 && J >= 2 && J <= g.NJ - 1 && K >= 2 && K <= g.NK - 1) {
+    const long long c = cid(g, I, J, K);
+    if (f.nf[c] != -1) {
+      const double DX = XX_(2, I), DY = YY_(2, J), DZ = ZZ_(2, K);
+      const double DXY = DX * DY, DXZ = DX * DZ, DYZ = DY * DZ, FC = f.ff[c];
+      const double V = f.ggv[c] * DX * DY * DZ;
+      double FL[6] = {fabs(DYZ * f.ggx[c] * f.uu[c]), fabs(DYZ * A(f.ggx, I + 1, J, K) * A(f.uu, I + 1, J, K)),
+                      fabs(DXZ * f.ggy[c] * f.vv[c]), fabs(DXZ * A(f.ggy, I, J + 1, K) * A(f.vv, I, J + 1, K)),
+                      fabs(DXY * f.ggz[c] * f.ww[c]), fabs(DXY * A(f.ggz, I, J, K + 1) * A(f.ww, I, J, K + 1))};
+      const int ind[6] = {f.indx[c], A(f.indx, I + 1, J, K), f.indy[c], A(f.indy, I, J + 1, K), f.indz[c],
+                          A(f.indz, I, J, K + 1)};
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        if (ind[q] >= 1 && dmax(FC, f.bcf[ind[q] - 1]) <= 0.0) FL[q] = 0.0;
+      double FM = FL[0];
+#pragma unroll
+      for (int q = 1; q < 6; ++q) FM = dmax(FM, FL[q]);
+      if (FM > 0.0) m = dmin_ne(m, V / FM);
+      const double V2 = 0.5 / (1.0 / (DX * DX) + 1.0 / (DY * DY) + 1.0 / (DZ * DZ));
+      if (f.anu[c] > 0.0) m = dmin_ne(m, V2 / f.anu[c]);
+    }
+  }
+  ROW_LOOP_END
+  for (int off = 16; off >= 1; off >>= 1) m = dmin_ne(m, __shfl_down_sync(0xffffffffu, m, off));
+  const long long row = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5);
+  if ((threadIdx.x & 31) == 0 && row < nrows) rb[row] = m;
+}
+// vf_cdtcal.f:46, 142-147: DT = MAX(MIN(min(DTMAX/DTSAFE, limits)*DTSAFE,
+// 1.2*W), DTMIN) with W = DTNOW, or DTINIT at NNOW = 0.
+__global__ void k_cdtcal_fin(const double *rb, long long nrows, double dt0, double dtsafe, double w, double dtmin,
+                             double *out) {
+  __shared__ double wm[32];
+  double m = dt0;
+  for (long long r = threadIdx.x; r < nrows; r += blockDim.x) m = dmin_ne(m, rb[r]);
+  for (int off = 16; off >= 1; off >>= 1) m = dmin_ne(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double DT = wm[0];
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) DT = dmin_ne(DT, wm[q]);
+    *out = dmax(dmin(DT * dtsafe, 1.20 * w), dtmin);
+  }
+}
+
 #undef A
 #undef XX_
 #undef YY_
@@ -527,6 +585,12 @@ void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f) { BL(k_bwuwt, g, f
 void launch_bwpp(cudaStream_t s, const Geo &g, const Fld &f) { BL(k_bwpp, g, f); }
 void launch_bwff(cudaStream_t s, const Geo &g, const Fld &f, int *err) { BL(k_bwff, g, f, err); }
 void launch_cdiv(cudaStream_t s, const Geo &g, const Fld &f, double *rb) { RL(k_cdiv, g, f, rb); }
+void launch_cdtcal(cudaStream_t s, const Geo &g, const Fld &f, double *rb, double dt0, double dtsafe, double w,
+                   double dtmin, double *out) {
+  RL(k_cdtcal, g, f, rb);
+  k_cdtcal_fin<<<1, 1024, 0, s>>>(rb, (long long)g.NJ * g.NK, dt0, dtsafe, w, dtmin, out);
+  count_launch();
+}
 #undef RL
 #undef BL
 

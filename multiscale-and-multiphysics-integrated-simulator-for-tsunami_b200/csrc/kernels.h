@@ -275,5 +275,8 @@ void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f);
 void launch_bwpp(cudaStream_t s, const Geo &g, const Fld &f);
 void launch_bwff(cudaStream_t s, const Geo &g, const Fld &f, int *err);
 void launch_cdiv(cudaStream_t s, const Geo &g, const Fld &f, double *rb);
+// VF_CDTCAL: the next step's DT into *out (device)
+void launch_cdtcal(cudaStream_t s, const Geo &g, const Fld &f, double *rb, double dt0, double dtsafe, double w,
+                   double dtmin, double *out);
 
 }  // namespace cadmas

@@ -2013,6 +2013,42 @@ struct orc_handle {
     }
   }
 
+  // VF_CDTCAL  vf_cdtcal.f:46-147 (no temperature or scalars: WK01 = ANU).
+  // Reference order: the running DT = V/MAX(FL1..FL6, V/DT) in K,J,I order.
+  // GPU order: the smallest of the cells' limits taken directly.
+  double cdtcal(double dtinit, double dtmin, double dtmax, double dtsafe) {
+    double DT = dtmax / dtsafe, M = DT;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          if (NF[c] == -1) continue;
+          const double DX = X_(2, I), DY = Y_(2, J), DZ = Z_(2, K);
+          const double DXY = DX * DY, DXZ = DX * DZ, DYZ = DY * DZ, FC = FF[c];
+          double V = GGV[c] * DX * DY * DZ;
+          double FL[6] = {std::fabs(DYZ * GGX[c] * UU[c]), std::fabs(DYZ * GGX[id(I + 1, J, K)] * UU[id(I + 1, J, K)]),
+                          std::fabs(DXZ * GGY[c] * VV[c]), std::fabs(DXZ * GGY[id(I, J + 1, K)] * VV[id(I, J + 1, K)]),
+                          std::fabs(DXY * GGZ[c] * WW[c]), std::fabs(DXY * GGZ[id(I, J, K + 1)] * WW[id(I, J, K + 1)])};
+          const int ind[6] = {INDX[c], INDX[id(I + 1, J, K)], INDY[c], INDY[id(I, J + 1, K)], INDZ[c],
+                              INDZ[id(I, J, K + 1)]};
+          for (int q = 0; q < 6; ++q)
+            if (ind[q] >= 1 && dmax(FC, BCF[ind[q] - 1]) <= 0.0) FL[q] = 0.0;
+          double FM = FL[0];
+          for (int q = 1; q < 6; ++q) FM = dmax(FM, FL[q]);
+          const double V2 = 0.5 / (1.0 / (DX * DX) + 1.0 / (DY * DY) + 1.0 / (DZ * DZ));
+          if (sum_mode == ORC_SUM_REF) {
+            DT = V / dmax(FM, V / DT);
+            DT = V2 / dmax(ANU[c], V2 / DT);
+          } else {
+            if (FM > 0.0) M = dmin(M, V / FM);
+            if (ANU[c] > 0.0) M = dmin(M, V2 / ANU[c]);
+          }
+        }
+    if (sum_mode != ORC_SUM_REF) DT = M;
+    const double W = (NNOW == 0) ? dtinit : DTNOW;
+    return dmax(dmin(DT * dtsafe, 1.20 * W), dtmin);
+  }
+
   // ----------------------------------------------------------- droplets
   // DROPTX..DROPWW of the TimerDoor droplet model; vf_cinit.f:412-427
   // starts every cell at (-1e10, 0, 0, 0, 0, 0).
@@ -2600,6 +2636,17 @@ int orc_set_drop(orc_handle *h, const double *tx, const double *ty, const double
   vd *dst[6] = {&h->DTX, &h->DTY, &h->DTZ, &h->DUU, &h->DVV, &h->DWW};
   for (int a = 0; a < 6; ++a)
     if (src[a]) std::copy(src[a], src[a] + dst[a]->size(), dst[a]->begin());
+  return CADMAS_OK;
+}
+
+int orc_set_time(orc_handle *h, double tnow, double dtnow, int nnow) {
+  h->TNOW = tnow; h->DTNOW = dtnow; h->NNOW = nnow;
+  return CADMAS_OK;
+}
+
+int orc_cdtcal(orc_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt) {
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  *dt = h->cdtcal(dtinit, dtmin, dtmax, dtsafe);
   return CADMAS_OK;
 }
 

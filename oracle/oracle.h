@@ -61,6 +61,10 @@ int orc_get_timers(orc_handle *h, double *t5);
 int orc_get_drop(orc_handle *h, double *tx, double *ty, double *tz, double *uu, double *vv, double *ww);
 int orc_set_drop(orc_handle *h, const double *tx, const double *ty, const double *tz, const double *uu,
                  const double *vv, const double *ww);
+/* TNOW, DTNOW, NNOW as cadmas_set_time. */
+int orc_set_time(orc_handle *h, double tnow, double dtnow, int nnow);
+/* VF_CDTCAL as cadmas_cdtcal (reference order: the running minimum). */
+int orc_cdtcal(orc_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt);
 /* Threads the oracle's parallel loops use (OpenMP). */
 int orc_num_threads(void);
 

@@ -61,6 +61,8 @@ def _load_lib():
     lib.orc_get_timers.argtypes = [C.c_void_p, dp]
     lib.orc_get_drop.argtypes = [C.c_void_p] + [dp] * 6
     lib.orc_set_drop.argtypes = [C.c_void_p] + [dp] * 6
+    lib.orc_cdtcal.argtypes = [C.c_void_p] + [C.c_double] * 4 + [dp]
+    lib.orc_set_time.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
     lib.orc_num_threads.argtypes = []
     lib.orc_num_threads.restype = C.c_int
     _lib = lib
@@ -117,6 +119,15 @@ class Oracle:
 
     def init_state(self, hydrostatic=True):
         self._rc(self.lib.orc_init_state(self.h, int(bool(hydrostatic))))
+
+    def set_time(self, tnow, dtnow, nnow):
+        self._rc(self.lib.orc_set_time(self.h, float(tnow), float(dtnow), int(nnow)))
+
+    def cdtcal(self, dtinit=1.0e-6, dtmin=0.0, dtmax=1.0e20, dtsafe=0.1):
+        """VF_CDTCAL in the handle's order (reference: running minimum)."""
+        dt = C.c_double()
+        self._rc(self.lib.orc_cdtcal(self.h, dtinit, dtmin, dtmax, dtsafe, C.byref(dt)))
+        return dt.value
 
     def get_drop(self):
         """DROPTX..DROPWW as {droptx, ..., dropww}."""

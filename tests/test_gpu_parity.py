@@ -263,3 +263,38 @@ def test_flume_full_size_properties(gpu_lib, pkg):
         assert s["true_relres"] < 1e-8
     assert abs(s["fsum"] + cut - v0) / v0 < 1e-10
     assert np.isfinite(t.divnorm())
+
+
+@pytest.mark.parametrize("builder,kw,active", [("random_tank", dict(seed=5), False),
+                                               ("droplet_tank", dict(seed=1), False), ("dam_break", {}, True)])
+def test_adaptive_time_step_bitwise(gpu_lib, pkg, orc, builder, kw, active):
+    """VF_CDTCAL: the next step's DT from the GPU equals the oracle's
+    (smallest-limit order) bit for bit, and within 1e-13 of the reference's
+    running minimum; ten steps each taken with that DT stay bitwise equal."""
+    c = getattr(pkg.cases, builder)(**kw)
+    t = pkg.Tank(c)
+    o = orc.Oracle(c, sum_mode=orc.SUM_GPU)
+    r = orc.Oracle(c, sum_mode=orc.SUM_REF)
+    for x in (t, o, r):
+        x.init_state(c.hydrostatic)
+    dt0 = t.cdtcal()
+    assert dt0 == o.cdtcal() and abs(dt0 - 1.2e-6) <= 1e-20  # NNOW = 0: 1.2 DTINIT caps it
+    dt = c.dt
+    # DTSAFE 1e-3: the cells' limits, not the 1.2*DTNOW cap, decide DT
+    kw = dict(dtmax=c.dt / 0.1, dtsafe=1.0e-3)
+    limited = 0
+    for n in range(1, 11):
+        t.step(dt)
+        o.step(dt)
+        dg, do = t.cdtcal(**kw), o.cdtcal(**kw)
+        st = o.get_state()
+        r.set_state(st)
+        r.set_time(st["tnow"], dt, st["nnow"])
+        dr = r.cdtcal(**kw)
+        assert dg == do, (n, dg, do)
+        assert abs(dg - dr) <= 1e-13 * dr
+        assert dg <= 1.2 * dt
+        limited += dg < 1.2 * dt
+        dt = dg
+    assert limited > 0 or not active  # the collapsing dam's velocities limit DT
+    assert_same(t.get_state(), o.get_state(), "after 10 adaptive steps")
