@@ -44,7 +44,7 @@ module cadmas_gpu
      integer(c_int) :: warm_start
      integer(c_int) :: precond_split
      integer(c_int) :: idrop
-     integer(c_int) :: reserved(1)
+     integer(c_int) :: iscmff
   end type cadmas_params
 
   ! c_loc() of the static arrays (XX(6,NUMI) ... INDB(4,NUMB))

@@ -117,7 +117,12 @@ typedef struct cadmas_params {
      flag update of every step (vf_f1cal.f:212-217), the reference's
      default (vf_a2dflt.f:151); 0 = off (DROP OFF).                       */
   int    idrop;
-  int    reserved[1];
+  /* ISCMFF /VF_ACOMPI/: scheme of the F advection in VF_F1CAL
+     (vf_f1cal.f:138-146).  0 = donor-acceptor VF_FCONV, the reference's
+     default (vf_a2dflt.f:41); 1 = FF-SLOPE VF_FCONVS (input
+     'COMP SCHM FF-SLOPE'): a surface cell with a tilted interface moves
+     the water under its plane in the swept strip.                      */
+  int    iscmff;
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */

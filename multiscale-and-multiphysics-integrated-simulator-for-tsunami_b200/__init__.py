@@ -69,7 +69,7 @@ class Params(C.Structure):
         ("icgtyp", C.c_int), ("icgmax", C.c_int), ("ibsuw0", C.c_int),
         ("precond_ti", C.c_int), ("precond_tj", C.c_int),
         ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("precond_split", C.c_int),
-        ("idrop", C.c_int), ("reserved", C.c_int * 1)]
+        ("idrop", C.c_int), ("iscmff", C.c_int)]
 
 
 class Static(C.Structure):

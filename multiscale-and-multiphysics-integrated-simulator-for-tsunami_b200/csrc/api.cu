@@ -619,7 +619,10 @@ static int do_f1cal(cadmas_handle *h) {
   const Geo &g = h->g;
   // fluxes and Euler update (vf_f1cal.f:124-163)
   TB(CADMAS_STAGE_VOF);
-  launch_fconv(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
+  if (h->P.iscmff == 0) launch_fconv(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
+  else  // VF_FCONVS: ISTYP in NLIM as in the reference (FMOD1 clears it), SX..SA in wk[3..6]
+    launch_fconvs(s, g, h->f, h->p, h->nlim, h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[0], h->wk[1],
+                  h->wk[2], h->dint);
   launch_feuler(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
   // surface redistribution, cut-off and volume (vf_f1cal.f:185-188)
   launch_fmod1(s, g, h->f, h->nlim);
@@ -783,6 +786,7 @@ void cadmas_default_params(cadmas_params *p) {
   p->icgtyp = 1; p->icgmax = 500; p->ibsuw0 = 0;
   p->precond_ti = 0; p->precond_tj = 0;
   p->idrop = 1;
+  p->iscmff = 0;
 }
 
 int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **out) {

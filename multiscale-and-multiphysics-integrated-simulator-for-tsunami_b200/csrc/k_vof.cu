@@ -30,6 +30,7 @@
 // FMOD1) is done as an ordered gather.
 #include "cadmas_dev.cuh"
 #include "kernels.h"
+#include "vof_face.cuh"
 
 namespace cadmas {
 
@@ -39,25 +40,6 @@ namespace cadmas {
 #define ZZ_(m, k) gz(g, m, k)
 
 // ------------------------------------------------------------ VF_FCONV
-__device__ __forceinline__ double fconv_face(double DT_G_U, int N, double FDv, int ndm, double FDMv,
-                                             double Vd, double Vo, double bcfv, int na, double FAv,
-                                             int d1, int d2, int d3, int d4, double FL) {
-  double C = DT_G_U;
-  double AC = fabs(C), FD, FDMW, V, FA;
-  if (N != -1) { FD = FDv; FDMW = 1.0; if (ndm != -1) FDMW = FDMv; V = Vd; }
-  else { FD = bcfv; FDMW = 1.0; V = Vo; }
-  FA = (na != -1) ? FAv : FD;
-  double FAD = FA;
-  if (N == -1 || N == d1 || N == d2 || N == d3 || N == d4)
-    if (FDMW != 0.0 && FA != 0.0) FAD = FD;
-  double FDM = dmax(FDMW, FD);
-  if (FDMW < FL && FA < FL) FDM = dmax(FDM, 0.1);
-  double CFX = dmax((FDM - FAD) * AC - (FDM - FD) * V, 0.0);
-  double FVX = FAD * AC + CFX;
-  double FVM = FD * V;
-  return dmin(FVX, FVM);
-}
-
 __global__ void k_fconv(Geo g, Fld f, Prm p, double *FLFU, double *FLFV, double *FLFW) {
   const double DT = p.dtnow, FL = p.flower;
   const int *NF = f.nf;

@@ -252,6 +252,10 @@ void launch_vmodif(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
 
 // k_vof.cu
 void launch_fconv(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *a, double *b, double *c);
+// VF_FCONVS (ISCMFF != 0): slope pass into ist/sx/sy/sz/sa (every cell
+// written), then the face fluxes into flfu/flfv/flfw; ERR_PG into err
+void launch_fconvs(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *ist, double *sx, double *sy,
+                   double *sz, double *sa, double *flfu, double *flfv, double *flfw, int *err);
 void launch_feuler(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const double *a,
                    const double *b, const double *c);
 void launch_fmod1(cudaStream_t s, const Geo &g, const Fld &f, int *nlim);

@@ -55,6 +55,266 @@ static double ipow(double x, int n) {
 static inline double dmax(double a, double b) { return (a < b) ? b : a; }
 static inline double dmin(double a, double b) { return (b < a) ? b : a; }
 
+// ------------------------------------------------ FF-SLOPE (ISCMFF = 1)
+// Elementary functions of VF_CROOT3 from +,-,*,/ and sqrt only, so that
+// the GPU kernels can evaluate the same operations in the same order and
+// agree bit for bit (the library's cbrt/atan/cos differ between glibc
+// and CUDA in the last bits).  Each is within a few ulps of the exact
+// value on the arguments VF_CROOT3 gives it (tests check them against
+// libm).
+//
+// Cube root: x = f 2^e with f in [0.5,1) (frexp, exact); m = f 2^r with
+// r = e mod 3 in [0.5,4); Newton's method on y^3 = m from y0 = (m+2)/3,
+// which lies above the root by the AM-GM inequality, so the iterates
+// fall monotonically; six steps take the worst start (m = 4, 26% high)
+// below one ulp.  The reference writes x**(1/3) with the exponent
+// rounded to double, which differs from the cube root by a few ulps.
+static double slope_cbrt(double x) {
+  if (x == 0.0) return 0.0;
+  int e;
+  double f = std::frexp(x, &e);
+  int r = ((e % 3) + 3) % 3;
+  double m = std::ldexp(f, r);
+  double y = (m + 2.0) / 3.0;
+  for (int it = 0; it < 6; ++it) y = y - (y * y * y - m) / (3.0 * y * y);
+  return std::ldexp(y, (e - r) / 3);
+}
+
+// Arctangent: odd symmetry; atan(a) = pi/2 - atan(1/a) for a > 1; two
+// half-angle steps atan(a) = 2 atan(a / (1 + sqrt(1 + a^2))) bring a
+// below tan(pi/16) = 0.199; then the Maclaurin series
+// z - z^3/3 + z^5/5 - ... to the z^25 term by Horner's rule.
+static double slope_atan(double y) {
+  const double HALF_PI = 1.5707963267948966;
+  double a = std::fabs(y);
+  bool inv = a > 1.0;
+  if (inv) a = 1.0 / a;
+  a = a / (1.0 + std::sqrt(1.0 + a * a));
+  a = a / (1.0 + std::sqrt(1.0 + a * a));
+  double z2 = a * a;
+  double p = 1.0 / 25.0;
+  for (int n = 11; n >= 0; --n) p = 1.0 / (double)(2 * n + 1) - z2 * p;
+  double t = 4.0 * (a * p);
+  if (inv) t = HALF_PI - t;
+  return (y < 0.0) ? -t : t;
+}
+
+// Cosine: the Maclaurin series in nested form
+// 1 - x^2/(1*2) (1 - x^2/(3*4) (1 - ... (1 - x^2/(27*28)))), accurate
+// to about 1e-15 for |x| <= 2.7; VF_CROOT3 calls it on
+// (-pi/6, 5pi/6] only.
+static double slope_cos(double x) {
+  double x2 = x * x;
+  double p = 1.0;
+  for (int n = 14; n >= 1; --n) p = 1.0 - x2 * p / (double)((2 * n - 1) * (2 * n));
+  return p;
+}
+
+// VF_CROOT2  vf_croot2.f:22-55
+static void croot2(double AA, double BB, double CC, double &XX1, double &XX2, int &NRT) {
+  if (AA == 0.0) {
+    if (BB != 0.0) { XX1 = -CC / BB; XX2 = 0.0; NRT = 1; }
+    else { XX1 = 0.0; XX2 = 0.0; NRT = 0; }
+  } else {
+    double B = 1.0 / AA;
+    double A = 0.5 * BB * B;
+    B = CC * B;
+    double D = A * A - B;
+    if (std::fabs(D) < 1.0e-20) { XX1 = -A; XX2 = 0.0; NRT = 1; }
+    else if (D < 0.0) { XX1 = 0.0; XX2 = 0.0; NRT = 0; }
+    else if (A >= 0.0) { XX1 = -A - std::sqrt(D); XX2 = B / XX1; NRT = 2; }
+    else { XX1 = -A + std::sqrt(D); XX2 = B / XX1; NRT = 2; }
+  }
+}
+
+// VF_CROOT3  vf_croot3.f:27-74 (Cardano)
+static void croot3(double AA, double BB, double CC, double DD, double &XX1, double &XX2, double &XX3,
+                   int &NRT) {
+  const double PI = 3.141592653589794;  // VF_A0PRM.h
+  if (AA == 0.0) {
+    croot2(BB, CC, DD, XX1, XX2, NRT);
+    XX3 = 0.0;
+    return;
+  }
+  double C = 1.0 / AA;
+  double A = BB * C;
+  double B = CC * C;
+  C = DD * C;
+  double P = B / 3.0 - A * A / 9.0;
+  double Q = C - A * B / 3.0 + 2.0 * A * A * A / 27.0;
+  double D = Q * Q + 4.0 * P * P * P;
+  if (D > 0.0) {
+    double R1 = (Q <= 0.0) ? 0.5 * (-Q + std::sqrt(D)) : 0.5 * (-Q - std::sqrt(D));
+    double R2 = -(P * P * P / R1);
+    double R13 = slope_cbrt(std::fabs(R1));
+    if (R1 < 0.0) R13 = -R13;
+    double R23 = slope_cbrt(std::fabs(R2));
+    if (R2 < 0.0) R23 = -R23;
+    XX1 = R13 + R23 - A / 3.0;
+    XX2 = 0.0; XX3 = 0.0; NRT = 1;
+  } else {
+    double T = (Q != 0.0) ? slope_atan(std::sqrt(-D) / (-Q)) : PI / 2.0;
+    if (Q > 0.0) T = PI + T;
+    double R = 2.0 * std::sqrt(-P);
+    double S = -A / 3.0;
+    XX1 = R * slope_cos(T / 3.0) + S;
+    XX2 = -(R * slope_cos((PI - T) / 3.0)) + S;
+    XX3 = -(R * slope_cos((PI + T) / 3.0)) + S;
+    NRT = 3;
+  }
+}
+
+// The root of VF_FSLP2A/3A in [XL-EP, XR+EP], else the midpoint (the
+// reference's WARNING branch); false when there is no root (P.G ERROR).
+static bool slope_pick(int NRT, double X1, double X2, double X3, double XL, double XR, double EP,
+                       double &AA) {
+  if (NRT == 0) return false;
+  if (X1 >= XL - EP && X1 <= XR + EP) AA = X1;
+  else if (NRT >= 2 && X2 >= XL - EP && X2 <= XR + EP) AA = X2;
+  else if (NRT >= 3 && X3 >= XL - EP && X3 <= XR + EP) AA = X3;
+  else AA = (XL + XR) / 2.0;
+  return true;
+}
+
+// Axis order of VF_FSLP2A/2F (vf_fslp2a.f:30-41): L1 the axis of the
+// smaller SD, the first on ties.
+// VF_FSLP2A  vf_fslp2a.f:30-101: the plane offset AA (|SX| x + |SY| y =
+// AA) that leaves FVAL of the DX*DY cell below the plane.  The volume
+// 2|SX||SY| V(a) is the piecewise quadratic a^2 - (a-SD1)+^2 - (a-SD2)+^2;
+// the interval holding VMX*FVAL is found from below and its quadratic
+// solved by VF_CROOT2.
+static bool fslp2a(double SX, double SY, double DX, double DY, double FVAL, double &AA) {
+  double SS[2] = {std::fabs(SX), std::fabs(SY)}, DD[2] = {DX, DY};
+  double SD[2] = {SS[0] * DX, SS[1] * DY};
+  int L1 = 0, L2 = 1;
+  if (!(SD[0] <= SD[1])) { L1 = 1; L2 = 0; }
+  double CNS = 2.0 * SS[0] * SS[1];
+  double XMX = SD[0] + SD[1];
+  double VMX = DD[0] * DD[1] * CNS;
+  double VIN = VMX * FVAL;
+  double XL = 0.0, XR = SD[L1], A = 1.0, B = 0.0, C = 0.0;
+  double VV = A * XR * XR;
+  const double bp[3] = {SD[L1], SD[L2], XMX};
+  int k = 0;
+  while (!(VIN <= VV)) {
+    if (++k == 3) return false;  // P.G ERROR(1)
+    double Q = bp[k - 1];
+    A = A - 1.0; B = B + 2.0 * Q; C = C - Q * Q;
+    XL = XR; XR = bp[k];
+    VV = (k == 2) ? VMX : A * XR * XR + B * XR + C;
+  }
+  double X1, X2; int NRT;
+  croot2(A, B, C - VIN, X1, X2, NRT);
+  return slope_pick(NRT > 2 ? 2 : NRT, X1, X2, 0.0, XL, XR, XMX * 1.0e-6, AA);  // P.G ERROR(2) if none
+}
+
+// VF_FSLP2F  vf_fslp2f.f:25-70: the water fraction below the plane AA.
+static double fslp2f(double SX, double SY, double DX, double DY, double AA) {
+  double SS[2] = {std::fabs(SX), std::fabs(SY)}, DD[2] = {DX, DY};
+  double SD[2] = {SS[0] * DX, SS[1] * DY};
+  int L1 = 0, L2 = 1;
+  if (!(SD[0] <= SD[1])) { L1 = 1; L2 = 0; }
+  double CNS = 2.0 * SS[0] * SS[1];
+  double XMX = SD[0] + SD[1];
+  double VMX = DD[0] * DD[1] * CNS;
+  double A = 1.0, B = 0.0, C = 0.0, VV;
+  if (AA <= 0.0) VV = 0.0;
+  else if (AA >= XMX) VV = VMX;
+  else if (AA <= SD[L1]) VV = A * AA * AA;
+  else {
+    double Q = SD[L1];
+    A = A - 1.0; B = B + 2.0 * Q; C = C - Q * Q;
+    if (AA <= SD[L2]) VV = A * AA * AA + B * AA + C;
+    else {
+      Q = SD[L2];
+      A = A - 1.0; B = B + 2.0 * Q; C = C - Q * Q;
+      VV = A * AA * AA + B * AA + C;
+    }
+  }
+  return VV / VMX;
+}
+
+// Breakpoints of the piecewise cubic volume of VF_FSLP3A/3F, sorted
+// SD(L1) <= SD(L2) <= SD(L3): six points before XMX, and the change of
+// the cubic's leading coefficient at each (-1 where the plane passes a
+// vertex on one axis, +1 on two).  The two orders are the two branches
+// of vf_fslp3a.f:63 / vf_fslp3f.f:63.
+struct SlopeCubic {
+  double SS[3], SD[3], bp[7], XMX, VMX;
+  int sg[6];
+  SlopeCubic(double SX, double SY, double SZ, double DX, double DY, double DZ) {
+    SS[0] = std::fabs(SX); SS[1] = std::fabs(SY); SS[2] = std::fabs(SZ);
+    SD[0] = SS[0] * DX; SD[1] = SS[1] * DY; SD[2] = SS[2] * DZ;
+    int L1 = 0, L2 = 1, L3 = 2, L;
+    if (SD[L1] > SD[L2]) { L = L1; L1 = L2; L2 = L; }
+    if (SD[L2] > SD[L3]) { L = L2; L2 = L3; L3 = L; }
+    if (SD[L1] > SD[L2]) { L = L1; L1 = L2; L2 = L; }
+    double CNS = 6.0 * SS[0] * SS[1] * SS[2];
+    XMX = SD[0] + SD[1] + SD[2];
+    VMX = DX * DY * DZ * CNS;
+    bp[0] = SD[L1]; bp[1] = SD[L2];
+    if (SD[L1] + SD[L2] <= SD[L3]) {
+      bp[2] = SD[L1] + SD[L2]; bp[3] = SD[L3];
+      const int s[6] = {-1, -1, 1, -1, 1, 1};
+      for (int i = 0; i < 6; ++i) sg[i] = s[i];
+    } else {
+      bp[2] = SD[L3]; bp[3] = SD[L1] + SD[L2];
+      const int s[6] = {-1, -1, -1, 1, 1, 1};
+      for (int i = 0; i < 6; ++i) sg[i] = s[i];
+    }
+    bp[4] = SD[L1] + SD[L3]; bp[5] = SD[L2] + SD[L3]; bp[6] = XMX;
+  }
+  // A*x^3 + B*x^2 + C*x + D past the breakpoint Q
+  static void pass(int s, double Q, double &A, double &B, double &C, double &D) {
+    if (s < 0) { A = A - 1.0; B = B + 3.0 * Q; C = C - 3.0 * Q * Q; D = D + Q * Q * Q; }
+    else { A = A + 1.0; B = B - 3.0 * Q; C = C + 3.0 * Q * Q; D = D - Q * Q * Q; }
+  }
+  static double poly(double A, double B, double C, double D, double x) {
+    return A * x * x * x + B * x * x + C * x + D;
+  }
+};
+
+// VF_FSLP3A  vf_fslp3a.f:30-266
+static bool fslp3a(double SX, double SY, double SZ, double DX, double DY, double DZ, double FVAL, double &AA) {
+  SlopeCubic c(SX, SY, SZ, DX, DY, DZ);
+  double VIN = c.VMX * FVAL;
+  double A = 1.0, B = 0.0, C = 0.0, D = 0.0, XL = 0.0, XR = c.bp[0];
+  double VV = A * XR * XR * XR;
+  int k = 0;
+  while (!(VIN <= VV)) {
+    if (++k == 7) return false;  // P.G ERROR(1)/(2)
+    SlopeCubic::pass(c.sg[k - 1], XR, A, B, C, D);
+    XL = XR; XR = c.bp[k];
+    VV = (k == 6) ? c.VMX : SlopeCubic::poly(A, B, C, D, XR);
+  }
+  double X1, X2, X3; int NRT;
+  croot3(A, B, C, D - VIN, X1, X2, X3, NRT);
+  return slope_pick(NRT, X1, X2, X3, XL, XR, c.XMX * 1.0e-6, AA);  // P.G ERROR(3) if none
+}
+
+// VF_FSLP3F  vf_fslp3f.f:30-181
+static double fslp3f(double SX, double SY, double SZ, double DX, double DY, double DZ, double AA) {
+  SlopeCubic c(SX, SY, SZ, DX, DY, DZ);
+  double VV;
+  if (AA <= 0.0) VV = 0.0;
+  else if (AA >= c.XMX) VV = c.VMX;
+  else {
+    double A = 1.0, B = 0.0, C = 0.0, D = 0.0, Q = c.bp[0];
+    if (AA <= Q) VV = A * AA * AA * AA;
+    else {
+      int k = 1;
+      for (;; ++k) {
+        SlopeCubic::pass(c.sg[k - 1], Q, A, B, C, D);
+        if (k == 6) break;
+        Q = c.bp[k];
+        if (AA <= Q) break;
+      }
+      VV = SlopeCubic::poly(A, B, C, D, AA);
+    }
+  }
+  return VV / c.VMX;
+}
+
 // Warp tree of the GPU reduction: lane 0 after shfl_down by 16,8,4,2,1.
 static double warp_tree(double *s) {
   for (int off = 16; off >= 1; off >>= 1)
@@ -1762,6 +2022,257 @@ struct orc_handle {
         }
   }
 
+  // VF_FCONVS  vf_fconvs.f:72-387: slope normals and plane offsets of
+  // the surface cells.  ISTYP = 0 (none), 3, 5, 6 or 7 (bits of the
+  // normal components with |S| >= 1e-4, two or more of them).
+  int ist_count[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // cells of each slope type, summed over the run
+  int fslope(std::vector<int> &IST, vd &SX, vd &SY, vd &SZ, vd &SA) {
+    const size_t N = UU.size();
+    IST.assign(N, 0); SX.assign(N, 0.0); SY.assign(N, 0.0); SZ.assign(N, 0.0); SA.assign(N, 0.0);
+    const double ZERO = 1.0e-20;
+    int rc = CADMAS_OK;
+    // one side of one axis (vf_fconvs.f:86-123 and its five copies):
+    // the neighbour's F (FO) and distance (DO) towards it.  a/b are the
+    // NF0 values of the cross-axis pair, e/o their cross-axis offsets;
+    // sgn = -1 for the minus side (metric entries of this cell), +1 for
+    // the plus side (of the neighbour); m3/m6 the 3rd and 6th metric
+    // entries, d2 the neighbour's width, DD0 this cell's.
+    auto side = [&](int NF0, double FF0, size_t cL, int NFL, double BCFv, const int *ns, const long long *off,
+                    double DD0, double d2, double m3, double m6, double &FO, double &DO) {
+      double FFL = FF[cL];
+      if (NFL == -1) { FO = BCFv; DO = DD0 * 0.5; }
+      else if (NFL == 8) {
+        if (NF0 == ns[0] || NF0 == ns[1] || NF0 == ns[2] || NF0 == ns[3]) { FO = FF0; DO = 0.0; }
+        else { FO = 0.0; DO = DD0 * 0.5; }
+      } else if (NFL == 0) {
+        FO = FFL; DO = DD0 * 0.5;
+        for (int q = 0; q < 4; ++q)
+          if (NF0 == ns[q]) {
+            size_t cq = (size_t)((long long)cL + off[q]);
+            if (NF[cq] != -1) { FO = FO + FF[cq]; DO = m3; }
+            break;
+          }
+      } else {
+        FO = m6 * (d2 * FF0 + DD0 * FFL);
+        DO = DD0 * 0.5;
+      }
+    };
+    const long long sI = 1, sJ = NI, sK = (long long)NI * NJ;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          const int NF0 = NF[c];
+          const double FF0 = FF[c];
+          if (!(NF0 > 0 && FF0 >= P.flower && FF0 <= P.fupper)) continue;
+          double FM, FP, DM, DP, S1, S2, S3;
+          auto bc = [&](int l, double &v) {
+            if (l < 1 || l > NB) return false;
+            v = BCF[l - 1];
+            return true;
+          };
+          double bm = 0.0, bp = 0.0;
+          // x: cross-axis partners NF0 = 3 (J+1), 4 (J-1), 5 (K+1), 6 (K-1)
+          {
+            const int ns[4] = {3, 4, 5, 6};
+            const long long off[4] = {sJ, -sJ, sK, -sK};
+            int nm = NF[c - sI], np = NF[c + sI];
+            if (nm == -1 && !bc(INDX[c], bm)) return CADMAS_EPG;
+            if (np == -1 && !bc(INDX[c + sI], bp)) return CADMAS_EPG;
+            side(NF0, FF0, c - sI, nm, bm, ns, off, X_(2, I), X_(2, I - 1), X_(3, I), X_(6, I), FM, DM);
+            side(NF0, FF0, c + sI, np, bp, ns, off, X_(2, I), X_(2, I + 1), X_(3, I + 1), X_(6, I + 1), FP, DP);
+            S1 = (DM + DP <= ZERO) ? 0.0 : (FM - FP) / (DM + DP);
+          }
+          {
+            const int ns[4] = {1, 2, 5, 6};
+            const long long off[4] = {sI, -sI, sK, -sK};
+            int nm = NF[c - sJ], np = NF[c + sJ];
+            if (nm == -1 && !bc(INDY[c], bm)) return CADMAS_EPG;
+            if (np == -1 && !bc(INDY[c + sJ], bp)) return CADMAS_EPG;
+            side(NF0, FF0, c - sJ, nm, bm, ns, off, Y_(2, J), Y_(2, J - 1), Y_(3, J), Y_(6, J), FM, DM);
+            side(NF0, FF0, c + sJ, np, bp, ns, off, Y_(2, J), Y_(2, J + 1), Y_(3, J + 1), Y_(6, J + 1), FP, DP);
+            S2 = (DM + DP <= ZERO) ? 0.0 : (FM - FP) / (DM + DP);
+          }
+          {
+            const int ns[4] = {1, 2, 3, 4};
+            const long long off[4] = {sI, -sI, sJ, -sJ};
+            int nm = NF[c - sK], np = NF[c + sK];
+            if (nm == -1 && !bc(INDZ[c], bm)) return CADMAS_EPG;
+            if (np == -1 && !bc(INDZ[c + sK], bp)) return CADMAS_EPG;
+            side(NF0, FF0, c - sK, nm, bm, ns, off, Z_(2, K), Z_(2, K - 1), Z_(3, K), Z_(6, K), FM, DM);
+            side(NF0, FF0, c + sK, np, bp, ns, off, Z_(2, K), Z_(2, K + 1), Z_(3, K + 1), Z_(6, K + 1), FP, DP);
+            S3 = (DM + DP <= ZERO) ? 0.0 : (FM - FP) / (DM + DP);
+          }
+          double RN = S1 * S1 + S2 * S2 + S3 * S3;
+          if (RN >= ZERO) {
+            RN = 1.0 / std::sqrt(RN);
+            S1 = S1 * RN; S2 = S2 * RN; S3 = S3 * RN;
+            int I1 = std::fabs(S1) >= 1.0e-4, I2 = std::fabs(S2) >= 1.0e-4, I3 = std::fabs(S3) >= 1.0e-4;
+            if (I1 + I2 + I3 >= 2) { IST[c] = I1 + 2 * I2 + 4 * I3; SX[c] = S1; SY[c] = S2; SZ[c] = S3; }
+          }
+          ist_count[IST[c]]++;
+          bool ok = true;
+          switch (IST[c]) {
+            case 0: break;
+            case 3: ok = fslp2a(SX[c], SY[c], X_(2, I), Y_(2, J), FF[c], SA[c]); break;
+            case 5: ok = fslp2a(SX[c], SZ[c], X_(2, I), Z_(2, K), FF[c], SA[c]); break;
+            case 6: ok = fslp2a(SY[c], SZ[c], Y_(2, J), Z_(2, K), FF[c], SA[c]); break;
+            default: ok = fslp3a(SX[c], SY[c], SZ[c], X_(2, I), Y_(2, J), Z_(2, K), FF[c], SA[c]); break;
+          }
+          if (!ok) rc = CADMAS_EPG;
+        }
+    return rc;
+  }
+
+  // VF_FCONVS  vf_fconvs.f:395-635: the face fluxes; a face whose donor
+  // has a slope type usable across it (X: 3, 5, 7; Y: 3, 6, 7; Z: 5, 6,
+  // 7) and INDX <= 1 takes the water under the donor's plane in the
+  // swept strip, every other face the donor-acceptor flux of VF_FCONV.
+  int fconvs(vd &FLFU, vd &FLFV, vd &FLFW) {
+    std::vector<int> IST;
+    vd SX, SY, SZ, SA;
+    int rc = fslope(IST, SX, SY, SZ, SA);
+    if (rc) return rc;
+    const double DT = DTNOW, FL = P.flower;
+    auto da = [&](double C, int N, double FDa, int ndm, double FDMa, double Vd, double Vo, double bcf, int na,
+                  double FAa, int d1, int d2, int d3, int d4) {
+      double AC = std::fabs(C), FD, FDMW, V, FA;
+      if (N != -1) { FD = FDa; FDMW = 1.0; if (ndm != -1) FDMW = FDMa; V = Vd; }
+      else { FD = bcf; FDMW = 1.0; V = Vo; }
+      FA = (na != -1) ? FAa : FD;
+      double FAD = FA;
+      if (N == -1 || N == d1 || N == d2 || N == d3 || N == d4)
+        if (FDMW != 0.0 && FA != 0.0) FAD = FD;
+      double FDM = dmax(FDMW, FD);
+      if (FDMW < FL && FA < FL) FDM = dmax(FDM, 0.1);
+      double CFX = dmax((FDM - FAD) * AC - (FDM - FD) * V, 0.0);
+      double FVX = FAD * AC + CFX;
+      double FVM = FD * V;
+      return dmin(FVX, FVM);
+    };
+    // Slope branch: the water that leaves is the donor's water below its
+    // plane in the strip of width AC next to the face, capped at the
+    // donor's content.  VF_FSLP2F/3F measure from the water side of the
+    // cell: when the normal points along the flow (LSW = 1) the water
+    // side is away from the face, and the strip's water is the donor's
+    // water minus that of the other DX-AC.
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          const size_t c = id(I, J, K);
+          if (INDX[c] == -1) continue;
+          double C = DT * GGX[c] * UU[c];
+          int LSN, LA, LD, LDM;
+          if (C >= 0.0) { LSN = 1; LA = I; LD = I - 1; LDM = I - 2; } else { LSN = -1; LA = I - 1; LD = I; LDM = I + 1; }
+          const size_t d = id(LD, J, K);
+          const int ist = IST[d];
+          double fl;
+          if (INDX[c] > 1 || ist <= 0 || ist == 6) {
+            int N = NF[d];
+            int ndm = (N != -1) ? NF[id(LDM, J, K)] : -1;
+            double fdm = (N != -1 && ndm != -1) ? FF[id(LDM, J, K)] : 0.0;
+            double vd_ = (N != -1) ? X_(2, LD) * GGV[d] : 0.0;
+            double bcf = (N == -1) ? BCF[INDX[c] - 1] : 0.0;
+            int na = NF[id(LA, J, K)];
+            fl = da(C, N, (N != -1) ? FF[d] : 0.0, ndm, fdm, vd_, X_(2, LD), bcf, na,
+                    (na != -1) ? FF[id(LA, J, K)] : 0.0, 3, 4, 5, 6);
+          } else {
+            double AC = std::fabs(C);
+            int LSW = LSN;
+            if (SX[d] < 0.0) LSW = -LSW;
+            double DD0 = AC;
+            if (LSW == 1) DD0 = X_(2, LD) - AC;
+            double DFF;
+            if (ist == 3) DFF = fslp2f(SX[d], SY[d], DD0, Y_(2, J), SA[d]);
+            else if (ist == 5) DFF = fslp2f(SX[d], SZ[d], DD0, Z_(2, K), SA[d]);
+            else DFF = fslp3f(SX[d], SY[d], SZ[d], DD0, Y_(2, J), Z_(2, K), SA[d]);
+            double VG = X_(2, LD) * FF[d];
+            double FVX = DFF * DD0;
+            if (LSW == 1) FVX = VG - FVX;
+            VG = VG * GGV[d];
+            fl = dmin(FVX, VG);
+          }
+          FLFU[c] = FLFU[c] - (double)LSN * fl;
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          if (INDY[c] == -1) continue;
+          double C = DT * GGY[c] * VV[c];
+          int LSN, LA, LD, LDM;
+          if (C >= 0.0) { LSN = 1; LA = J; LD = J - 1; LDM = J - 2; } else { LSN = -1; LA = J - 1; LD = J; LDM = J + 1; }
+          const size_t d = id(I, LD, K);
+          const int ist = IST[d];
+          double fl;
+          if (INDY[c] > 1 || ist <= 0 || ist == 5) {
+            int N = NF[d];
+            int ndm = (N != -1) ? NF[id(I, LDM, K)] : -1;
+            double fdm = (N != -1 && ndm != -1) ? FF[id(I, LDM, K)] : 0.0;
+            double vd_ = (N != -1) ? Y_(2, LD) * GGV[d] : 0.0;
+            double bcf = (N == -1) ? BCF[INDY[c] - 1] : 0.0;
+            int na = NF[id(I, LA, K)];
+            fl = da(C, N, (N != -1) ? FF[d] : 0.0, ndm, fdm, vd_, Y_(2, LD), bcf, na,
+                    (na != -1) ? FF[id(I, LA, K)] : 0.0, 1, 2, 5, 6);
+          } else {
+            double AC = std::fabs(C);
+            int LSW = LSN;
+            if (SY[d] < 0.0) LSW = -LSW;
+            double DD0 = AC;
+            if (LSW == 1) DD0 = Y_(2, LD) - AC;
+            double DFF;
+            if (ist == 3) DFF = fslp2f(SX[d], SY[d], X_(2, I), DD0, SA[d]);
+            else if (ist == 6) DFF = fslp2f(SY[d], SZ[d], DD0, Z_(2, K), SA[d]);
+            else DFF = fslp3f(SX[d], SY[d], SZ[d], X_(2, I), DD0, Z_(2, K), SA[d]);
+            double VG = Y_(2, LD) * FF[d];
+            double FVX = DFF * DD0;
+            if (LSW == 1) FVX = VG - FVX;
+            VG = VG * GGV[d];
+            fl = dmin(FVX, VG);
+          }
+          FLFV[c] = FLFV[c] - (double)LSN * fl;
+        }
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          if (INDZ[c] == -1) continue;
+          double C = DT * GGZ[c] * WW[c];
+          int LSN, LA, LD, LDM;
+          if (C >= 0.0) { LSN = 1; LA = K; LD = K - 1; LDM = K - 2; } else { LSN = -1; LA = K - 1; LD = K; LDM = K + 1; }
+          const size_t d = id(I, J, LD);
+          const int ist = IST[d];
+          double fl;
+          if (INDZ[c] > 1 || ist <= 0 || ist == 3) {
+            int N = NF[d];
+            int ndm = (N != -1) ? NF[id(I, J, LDM)] : -1;
+            double fdm = (N != -1 && ndm != -1) ? FF[id(I, J, LDM)] : 0.0;
+            double vd_ = (N != -1) ? Z_(2, LD) * GGV[d] : 0.0;
+            double bcf = (N == -1) ? BCF[INDZ[c] - 1] : 0.0;
+            int na = NF[id(I, J, LA)];
+            fl = da(C, N, (N != -1) ? FF[d] : 0.0, ndm, fdm, vd_, Z_(2, LD), bcf, na,
+                    (na != -1) ? FF[id(I, J, LA)] : 0.0, 1, 2, 3, 4);
+          } else {
+            double AC = std::fabs(C);
+            int LSW = LSN;
+            if (SZ[d] < 0.0) LSW = -LSW;
+            double DD0 = AC;
+            if (LSW == 1) DD0 = Z_(2, LD) - AC;
+            double DFF;
+            if (ist == 5) DFF = fslp2f(SX[d], SZ[d], X_(2, I), DD0, SA[d]);
+            else if (ist == 6) DFF = fslp2f(SY[d], SZ[d], Y_(2, J), DD0, SA[d]);
+            else DFF = fslp3f(SX[d], SY[d], SZ[d], X_(2, I), Y_(2, J), DD0, SA[d]);
+            double VG = Z_(2, LD) * FF[d];
+            double FVX = DFF * DD0;
+            if (LSW == 1) FVX = VG - FVX;
+            VG = VG * GGV[d];
+            fl = dmin(FVX, VG);
+          }
+          FLFW[c] = FLFW[c] - (double)LSN * fl;
+        }
+    return CADMAS_OK;
+  }
+
   // VF_FEULER  vf_feuler.f:43-56 (QF = 0, GGV0 = GGV, LOOPS = 1)
   void feuler(const vd &FLFU, const vd &FLFV, const vd &FLFW) {
     for (int K = 2; K <= NK - 1; ++K)
@@ -2407,7 +2918,11 @@ struct orc_handle {
     size_t N = UU.size();
     vd FLFU(N, 0.0), FLFV(N, 0.0), FLFW(N, 0.0);
     std::fill(NLIM.begin(), NLIM.end(), 0);
-    fconv(FLFU, FLFV, FLFW);
+    if (P.iscmff == 0) fconv(FLFU, FLFV, FLFW);  // vf_f1cal.f:138-146
+    else {
+      int rcs = fconvs(FLFU, FLFV, FLFW);
+      if (rcs) return rcs;
+    }
     feuler(FLFU, FLFV, FLFW);
     fmod1();
     double fs, fc;
@@ -2647,6 +3162,36 @@ int orc_set_time(orc_handle *h, double tnow, double dtnow, int nnow) {
 int orc_cdtcal(orc_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt) {
   if (!h->have_static) return CADMAS_ENOSTATIC;
   *dt = h->cdtcal(dtinit, dtmin, dtmax, dtsafe);
+  return CADMAS_OK;
+}
+
+int orc_slope_counts(orc_handle *h, int *counts) {
+  for (int i = 0; i < 8; ++i) counts[i] = h->ist_count[i];
+  return CADMAS_OK;
+}
+
+double orc_slope_fn(int fn, double x) {
+  switch (fn) {
+    case 0: return slope_cbrt(x);
+    case 1: return slope_atan(x);
+    default: return slope_cos(x);
+  }
+}
+
+int orc_fslp(int dim, const double *s, const double *d, double fval, double *aa, double *fback) {
+  bool ok;
+  if (dim == 2) {
+    ok = fslp2a(s[0], s[1], d[0], d[1], fval, *aa);
+    if (ok) *fback = fslp2f(s[0], s[1], d[0], d[1], *aa);
+  } else {
+    ok = fslp3a(s[0], s[1], s[2], d[0], d[1], d[2], fval, *aa);
+    if (ok) *fback = fslp3f(s[0], s[1], s[2], d[0], d[1], d[2], *aa);
+  }
+  return ok ? CADMAS_OK : CADMAS_EPG;
+}
+
+int orc_croot3(double a, double b, double c, double d, double *x, int *nrt) {
+  croot3(a, b, c, d, x[0], x[1], x[2], *nrt);
   return CADMAS_OK;
 }
 

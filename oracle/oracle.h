@@ -65,6 +65,14 @@ int orc_set_drop(orc_handle *h, const double *tx, const double *ty, const double
 int orc_set_time(orc_handle *h, double tnow, double dtnow, int nnow);
 /* VF_CDTCAL as cadmas_cdtcal (reference order: the running minimum). */
 int orc_cdtcal(orc_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt);
+/* FF-SLOPE checks: cells of each slope type (index 0..7) seen by the
+   VF_FCONVS passes so far; the elementary functions of VF_CROOT3
+   (fn 0 cube root, 1 arctangent, 2 cosine); VF_FSLP2A/3A followed by
+   VF_FSLP2F/3F on the same cell (dim 2 or 3); VF_CROOT3. */
+int orc_slope_counts(orc_handle *h, int *counts);
+double orc_slope_fn(int fn, double x);
+int orc_fslp(int dim, const double *s, const double *d, double fval, double *aa, double *fback);
+int orc_croot3(double a, double b, double c, double d, double *x, int *nrt);
 /* Threads the oracle's parallel loops use (OpenMP). */
 int orc_num_threads(void);
 

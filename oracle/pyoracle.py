@@ -63,6 +63,11 @@ def _load_lib():
     lib.orc_set_drop.argtypes = [C.c_void_p] + [dp] * 6
     lib.orc_cdtcal.argtypes = [C.c_void_p] + [C.c_double] * 4 + [dp]
     lib.orc_set_time.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+    lib.orc_slope_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.orc_slope_fn.argtypes = [C.c_int, C.c_double]
+    lib.orc_slope_fn.restype = C.c_double
+    lib.orc_fslp.argtypes = [C.c_int, dp, dp, C.c_double, dp, dp]
+    lib.orc_croot3.argtypes = [C.c_double] * 4 + [dp, C.POINTER(C.c_int)]
     lib.orc_num_threads.argtypes = []
     lib.orc_num_threads.restype = C.c_int
     _lib = lib
@@ -142,6 +147,12 @@ class Oracle:
         dp = C.POINTER(C.c_double)
         self._rc(self.lib.orc_set_drop(self.h, *(keep[n].ctypes.data_as(dp) for n in self.P.DROP_ARRAYS)))
 
+    def slope_counts(self):
+        """Cells of each slope type 0..7 seen by VF_FCONVS so far."""
+        n = (C.c_int * 8)()
+        self._rc(self.lib.orc_slope_counts(self.h, n))
+        return list(n)
+
     def step(self, dt=None):
         self._rc(self.lib.orc_step(self.h, float(dt if dt is not None else self.case.dt)))
 
@@ -192,3 +203,27 @@ class Oracle:
 def num_threads() -> int:
     """Threads of the oracle's parallel loops (OpenMP; OMP_NUM_THREADS)."""
     return int(_load_lib().orc_num_threads())
+
+
+def slope_fn(fn: int, x: float) -> float:
+    """The oracle's cube root (0), arctangent (1) or cosine (2) of VF_CROOT3."""
+    return float(_load_lib().orc_slope_fn(int(fn), float(x)))
+
+
+def fslp(s, d, fval):
+    """VF_FSLP2A/3A then VF_FSLP2F/3F for normal s and cell widths d:
+    (plane offset, water fraction recovered), or None on P.G ERROR."""
+    dim = len(s)
+    sa = (C.c_double * dim)(*s)
+    da = (C.c_double * dim)(*d)
+    aa, fb = C.c_double(), C.c_double()
+    rc = _load_lib().orc_fslp(dim, sa, da, float(fval), C.byref(aa), C.byref(fb))
+    return None if rc else (aa.value, fb.value)
+
+
+def croot3(a, b, c, d):
+    """VF_CROOT3: (roots, number of roots)."""
+    x = (C.c_double * 3)()
+    n = C.c_int()
+    _load_lib().orc_croot3(a, b, c, d, x, C.byref(n))
+    return list(x)[:n.value], n.value

@@ -29,6 +29,10 @@ CASES = {
     "bubble_tank_6": dict(builder="random_tank", kw=dict(seed=9), steps=6, sum_mode=0,
                           over=dict(wbub=0.2)),
     "droplet_tank_0_20": dict(builder="droplet_tank", kw=dict(seed=0), steps=20, sum_mode=0, over={}),
+    # FF-SLOPE advection of F (ISCMFF = 1, VF_FCONVS)
+    "ffslope_tank_1_20": dict(builder="random_tank", kw=dict(seed=1), steps=20, sum_mode=0,
+                              over=dict(iscmff=1)),
+    "ffslope_dam_break_10": dict(builder="dam_break", kw={}, steps=10, sum_mode=0, over=dict(iscmff=1)),
 }
 DROP = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 FIELDS = ("uu", "vv", "ww", "pp", "ff", "nf", "indc", "bcu", "bcv", "bcw", "bcp", "bcf")
