@@ -123,6 +123,20 @@ typedef struct cadmas_params {
      'COMP SCHM FF-SLOPE'): a surface cell with a tilted interface moves
      the water under its plane in the swept strip.                      */
   int    iscmff;
+  /* LEQK /VF_APHYSI/: 1 = the k-epsilon model: VF_K1CAL between V1CAL and
+     F1CAL, then VF_BSSS, VF_CNUT0, VF_CNU00 and VF_BWKE after F1CAL
+     (vf_a1main.f:1093-1126), so that ANU = ANU0 + ANUT changes every step;
+     0 = off, the reference's default (vf_a2dflt.f:139).  The constants
+     are /VF_APHYSR/'s with their defaults (vf_a2dflt.f:61,162,165-176).  */
+  int    leqk;
+  int    pad0;
+  double anu0;                     /* ANU0 molecular viscosity, 1e-6         */
+  double scmk;                     /* SCMK upwind weight of k, e convection,
+                                      1.0 (donor cell)                       */
+  double akmink, akmine;           /* AKMINK, AKMINE cut-offs, 1e-20         */
+  double akinik, akinie;           /* AKINIK, AKINIE initial k, e, 1e-20     */
+  double akcmu, aksgk, aksge;      /* C_mu 0.09, sigma_k 1.0, sigma_e 1.3    */
+  double akc1, akc2, akc3;         /* C1 1.44, C2 1.92, C3 0.0               */
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */
@@ -134,6 +148,15 @@ typedef struct cadmas_static {
   const double *anu;               /* ANU molecular (+eddy) viscosity          */
   const int    *indx, *indy, *indz;/* face index (-1 obstacle,0 normal,>0 bnd)*/
   const int    *indb;              /* INDB(4,NUMB)                             */
+  /* k-epsilon boundaries, read when leqk != 0 (else may be NULL):
+     INDBK(NUMB), INDBE(NUMB) the types of k and e on each boundary face
+     (1 fixed, 2 zero gradient, 6/8 log-law and rough wall as set from the
+     velocity type; negative, the input's FIX-A/FREE-A: no convective
+     flux through the face, vf_iiboun.f:256-330, vf_sconvd.f:86), and
+     BCK(NUMB), BCE(NUMB) the input values
+     (kept on fixed faces, vf_bwke.f:63-64).                               */
+  const int    *indbk, *indbe;
+  const double *bck, *bce;
 } cadmas_static;
 
 /* ---- dynamic state (host pointers; read by set_state, written by get_state)
@@ -221,6 +244,18 @@ int cadmas_get_drop(cadmas_handle *h, double *droptx, double *dropty, double *dr
                     double *dropvv, double *dropww);
 int cadmas_set_drop(cadmas_handle *h, const double *droptx, const double *dropty, const double *droptz,
                     const double *dropuu, const double *dropvv, const double *dropww);
+
+/* The k-epsilon state (params.leqk != 0): AK, AE, ANUT and ANU
+   (NUMI,NUMJ,NUMK) column-major, BCK, BCE (NUMB); NULL skipped.  They stay
+   on the device between steps.  cadmas_init_state sets them as VF_CINIT
+   does (vf_cinit.f:295-315,359-364,397-401).  cadmas_set_turb takes AK,
+   AE, BCK, BCE and then forms ANUT (VF_CNUT0) and ANU (VF_CNU00) as the
+   restart input does (vf_ir1inp.f:339-340).  CADMAS_EINVAL when leqk is
+   0.                                                                    */
+int cadmas_get_turb(cadmas_handle *h, double *ak, double *ae, double *anut, double *anu, double *bck,
+                    double *bce);
+int cadmas_set_turb(cadmas_handle *h, const double *ak, const double *ae, const double *bck,
+                    const double *bce);
 
 /* ---- restart file (*.rsl / *.res) and list file ----------------------
    The restart file of the reference, byte for byte: a Fortran unformatted
@@ -385,7 +420,9 @@ long long cadmas_kernel_launches(void);
 #define CADMAS_STAGE_VOF       9  /* FCONV, FEULER, FMOD1, FCUT01             */
 #define CADMAS_STAGE_FLAGS    10  /* FNFINI, FBUBUP, FNFPRV, CINDC            */
 #define CADMAS_STAGE_FBC      11  /* F1CAL boundary rules, BSPPFL             */
-#define CADMAS_NSTAGES        12
+#define CADMAS_STAGE_TURB     12  /* k-epsilon: VF_K1CAL and the updates after
+                                     F1CAL (LEQK != 0)                       */
+#define CADMAS_NSTAGES        13
 int cadmas_stage_timers(cadmas_handle *h, int enable, double *ms, long long *count, int n);
 
 const char *cadmas_strerror(int status);

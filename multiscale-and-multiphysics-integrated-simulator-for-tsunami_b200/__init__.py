@@ -69,13 +69,16 @@ class Params(C.Structure):
         ("icgtyp", C.c_int), ("icgmax", C.c_int), ("ibsuw0", C.c_int),
         ("precond_ti", C.c_int), ("precond_tj", C.c_int),
         ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("precond_split", C.c_int),
-        ("idrop", C.c_int), ("iscmff", C.c_int)]
+        ("idrop", C.c_int), ("iscmff", C.c_int), ("leqk", C.c_int), ("pad0", C.c_int)] + [
+        (n, C.c_double) for n in ("anu0", "scmk", "akmink", "akmine", "akinik", "akinie", "akcmu", "aksgk",
+                                  "aksge", "akc1", "akc2", "akc3")]
 
 
 class Static(C.Structure):
     _fields_ = [(n, _dp) for n in ("xx", "yy", "zz", "ggv", "ggx", "ggy", "ggz", "glv", "glx",
                                    "gly", "glz", "cd0", "anu")] + [
-        (n, _ip) for n in ("indx", "indy", "indz", "indb")]
+        (n, _ip) for n in ("indx", "indy", "indz", "indb", "indbk", "indbe")] + [
+        (n, _dp) for n in ("bck", "bce")]
 
 
 class State(C.Structure):
@@ -96,11 +99,13 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers", "cadmas_get_drop",
             "cadmas_set_drop", "cadmas_restart_create", "cadmas_restart_append", "cadmas_restart_load",
-            "cadmas_list_step", "cadmas_cdtcal"]
+            "cadmas_list_step", "cadmas_cdtcal", "cadmas_get_turb", "cadmas_set_turb"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
+TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
+TURB_FACES = ("bck", "bce")                # (NUMB)
 
-STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc"]
+STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc", "turb"]
 
 
 class CadmasError(RuntimeError):
@@ -144,6 +149,8 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_list_step.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     lib.cadmas_cdtcal.argtypes = [C.c_void_p] + [C.c_double] * 4 + [C.POINTER(C.c_double)]
     lib.cadmas_set_drop.argtypes = [C.c_void_p] + [_dp] * 6
+    lib.cadmas_get_turb.argtypes = [C.c_void_p] + [_dp] * 6
+    lib.cadmas_set_turb.argtypes = [C.c_void_p] + [_dp] * 4
     lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
     lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
     lib.cadmas_set_time.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
@@ -203,8 +210,6 @@ def make_params(case, base: Params | None = None, **over) -> Params:
             jd = {"damp_xm": 0, "damp_xp": 1, "damp_ym": 2, "damp_yp": 3}[k]
             for m in range(4):
                 p.damp[jd][m] = float(v[m])
-        elif k == "anu0":
-            continue
         elif hasattr(p, k):
             setattr(p, k, type(getattr(p, k))(v))
         else:
@@ -222,6 +227,17 @@ def static_of(case) -> Static:
         a = getattr(case, n)
         assert a.dtype == np.int32 and a.flags.f_contiguous
         setattr(s, n, _iptr(a))
+    # k-epsilon boundaries (read only when leqk != 0)
+    for n in ("indbk", "indbe"):
+        a = getattr(case, n, None)
+        if a is not None:
+            assert a.dtype == np.int32 and a.ndim == 1
+            setattr(s, n, _iptr(a))
+    for n in ("bck", "bce"):
+        a = getattr(case, n, None)
+        if a is not None:
+            assert a.dtype == np.float64 and a.ndim == 1
+            setattr(s, n, _dptr(a))
     return s
 
 
@@ -331,6 +347,20 @@ class Tank:
     def set_drop(self, arrs):
         keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64) for n in DROP_ARRAYS}
         _check(self.lib, self.lib.cadmas_set_drop(self.h, *(_dptr(keep[n]) for n in DROP_ARRAYS)))
+
+    def get_turb(self):
+        """The k-epsilon state {ak, ae, anut, anu} (flat, cells) and {bck, bce}."""
+        c = self.case
+        arrs = {n: np.zeros(c.ni * c.nj * c.nk) for n in TURB_CELLS}
+        arrs.update({n: np.zeros(max(c.numb, 1)) for n in TURB_FACES})
+        _check(self.lib, self.lib.cadmas_get_turb(self.h, *(_dptr(arrs[n]) for n in TURB_CELLS + TURB_FACES)))
+        return arrs
+
+    def set_turb(self, arrs):
+        """AK, AE, BCK, BCE; ANUT and ANU follow (VF_CNUT0, VF_CNU00)."""
+        keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64).reshape(-1, order="F")
+                for n in ("ak", "ae", "bck", "bce")}
+        _check(self.lib, self.lib.cadmas_set_turb(self.h, *(_dptr(keep[n]) for n in ("ak", "ae", "bck", "bce"))))
 
     # ------------------------------------------------------------ step
     def step(self, dt=None):

@@ -359,6 +359,13 @@ def finish(c: Case, vp_type=VP_SLIP, f_type=F_FREE, faces=None, fast=None):
         fast = c.ni * c.nj * c.nk > 200_000
     (build_inertia_fast if fast else build_inertia)(c)
     build_viscosity(c, c.params.get("anu0", 1.0e-6))
+    # k-epsilon boundaries: zero gradient ('K FREE+A', 'E FREE+A') on every
+    # face (read only when leqk != 0)
+    nb = max(c.numb, 1)
+    c.indbk = np.full(nb, 2, dtype=np.int32)
+    c.indbe = np.full(nb, 2, dtype=np.int32)
+    c.bck = np.zeros(nb)
+    c.bce = np.zeros(nb)
     shape = (c.ni, c.nj, c.nk)
     c.uu = _z3(*shape)
     c.vv = _z3(*shape)
@@ -506,6 +513,31 @@ def random_tank(seed=0, nx=12, ny=6, nz=10, d=0.01, nobst=2, nporous=2,
     c.dt = dt
     finish(c, vp_type=VP_SLIP if slip else VP_NOSLIP)
     return c
+
+
+def turbulence(c: Case, k0=1.0e-4, e0=1.0e-5, seed=None, **consts):
+    """Switch the k-epsilon model on (LEQK = 1) with initial k0, e0
+    (AKINIK, AKINIE).  With a seed, each boundary face gets a random k and
+    e type among fixed/zero gradient with and without convective inflow
+    (1, 2, -1, -2: 'FIX+A', 'FREE+A', 'FIX-A', 'FREE-A') and fixed values
+    near k0, e0."""
+    c.params.update(leqk=1, akinik=k0, akinie=e0, **consts)
+    if seed is not None:
+        rng = np.random.Generator(np.random.Philox(seed + 1000))
+        nb = c.indbk.size
+        c.indbk = rng.choice(np.array([1, 2, -1, -2], dtype=np.int32), size=nb)
+        c.indbe = rng.choice(np.array([1, 2, -1, -2], dtype=np.int32), size=nb)
+        c.bck = rng.uniform(0.5, 2.0, size=nb) * k0
+        c.bce = rng.uniform(0.5, 2.0, size=nb) * e0
+    return c
+
+
+def turbulent_tank(seed=0, k0=1.0e-4, e0=1.0e-5, **kw):
+    """A random tank (obstacles, porous blocks, F boxes) with the k-epsilon
+    model on and random k, e boundary types."""
+    c = random_tank(seed, **kw)
+    c.name = f"turbulent_tank_{seed}"
+    return turbulence(c, k0, e0, seed=seed)
 
 
 def droplet_tank(seed=0, nx=24, ny=6, nz=20, d=0.01, ndrop=8, level=0.3, dt=2.0e-3, speed=1.0):

@@ -153,6 +153,11 @@ struct cadmas_handle {
   // host-side scalars
   std::vector<double> tbub;
   DropArrays drop{};  // DROPTX..DROPWW (the droplet model's state)
+  // k-epsilon (LEQK != 0): AK, AE and their second buffers, ANUT; BCK, BCE,
+  // the input values BCK0, BCE0 and the types INDBK, INDBE
+  double *ak = nullptr, *ae_k = nullptr, *ak2 = nullptr, *ae2 = nullptr, *anut = nullptr;
+  double *bck = nullptr, *bce = nullptr, *bck0 = nullptr, *bce0 = nullptr;
+  int *indbk = nullptr, *indbe = nullptr;
   std::vector<double> zz2;  // ZZ(2,K) on the host, K = 1..NK
   std::vector<unsigned char> h_active;
   double tnow = 0.0, dtnow = 0.0;
@@ -612,11 +617,53 @@ static int do_v1cal(cadmas_handle *h) {
   return CADMAS_OK;
 }
 
+// ------------------------------------------------------------ k-epsilon
+static KeConst ke_const(const cadmas_handle *h) {
+  const cadmas_params &P = h->P;
+  return KeConst{P.anu0, P.scmk, P.akmink, P.akmine, P.akinik, P.akinie, P.akcmu, P.aksgk, P.aksge,
+                 P.akc1, P.akc2, P.akc3};
+}
+static KeArrays ke_arrays(const cadmas_handle *h) {
+  return KeArrays{h->ak, h->ae_k, h->anut, h->bck, h->bce, h->indbk, h->indbe};
+}
+
+// VF_K1CAL (vf_k1cal.f:84-170): k and e into the second buffers, which
+// then become the present ones; surface and gas values; boundary values.
+static void do_k1cal(cadmas_handle *h) {
+  cudaStream_t s = h->s;
+  TB(CADMAS_STAGE_TURB);
+  const KeConst kc = ke_const(h);
+  launch_kstep(s, h->g, h->f, h->p, kc, ke_arrays(h), h->ak2, h->ae2, h->dint);
+  std::swap(h->ak, h->ak2);
+  std::swap(h->ae_k, h->ae2);
+  launch_kbsss(s, h->g, h->f, kc, h->ak, h->ae_k, h->anut, h->anu, true, false);
+  launch_bwke(s, h->g, h->f, ke_arrays(h), h->dint);
+  TE();
+}
+
+// ANUT and ANU from the present k and e (VF_CNUT0, VF_CNU00)
+static void ke_nut(cadmas_handle *h) {
+  refresh_fld(h);
+  launch_kbsss(h->s, h->g, h->f, ke_const(h), h->ak, h->ae_k, h->anut, h->anu, false, true);
+}
+
+// After VF_F1CAL (vf_a1main.f:1119-1127): VF_BSSS with the new NF, ANUT and
+// ANU, VF_BWKE, VF_BWUWT.
+static void do_kpost(cadmas_handle *h) {
+  cudaStream_t s = h->s;
+  TB(CADMAS_STAGE_TURB);
+  launch_kbsss(s, h->g, h->f, ke_const(h), h->ak, h->ae_k, h->anut, h->anu, true, true);
+  launch_bwke(s, h->g, h->f, ke_arrays(h), h->dint);
+  launch_bwuwt(s, h->g, h->f);
+  TE();
+}
+
 static int do_f1cal(cadmas_handle *h) {
   cudaStream_t s = h->s;
   refresh_prm(h);
   refresh_fld(h);
   const Geo &g = h->g;
+  if (h->P.leqk != 0) do_k1cal(h);  // vf_a1main.f:1093-1100, just before VF_F1CAL
   // fluxes and Euler update (vf_f1cal.f:124-163)
   TB(CADMAS_STAGE_VOF);
   if (h->P.iscmff == 0) launch_fconv(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
@@ -683,6 +730,7 @@ static int do_f1cal(cadmas_handle *h) {
   launch_bwuwt(s, g, h->f);
   launch_bwpp(s, g, h->f);
   TE();
+  if (h->P.leqk != 0) do_kpost(h);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(h->h_res, h->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   int bits;
@@ -787,6 +835,11 @@ void cadmas_default_params(cadmas_params *p) {
   p->precond_ti = 0; p->precond_tj = 0;
   p->idrop = 1;
   p->iscmff = 0;
+  // k-epsilon (vf_a2dflt.f:61,139,162,165-176)
+  p->leqk = 0;
+  p->anu0 = 1.0e-6; p->scmk = 1.0;
+  p->akmink = 1.0e-20; p->akmine = 1.0e-20; p->akinik = 1.0e-20; p->akinie = 1.0e-20;
+  p->akcmu = 0.09; p->aksgk = 1.0; p->aksge = 1.3; p->akc1 = 1.44; p->akc2 = 1.92; p->akc3 = 0.0;
 }
 
 int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **out) {
@@ -860,6 +913,11 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   AL(h->st, 1); AL(h->dint, 8); AL(h->active, (size_t)d->numk + 1);
   AL(h->drop.tx, h->N); AL(h->drop.ty, h->N); AL(h->drop.tz, h->N);
   AL(h->drop.uu, h->N); AL(h->drop.vv, h->N); AL(h->drop.ww, h->N);
+  if (p->leqk != 0) {
+    AL(h->ak, h->N); AL(h->ae_k, h->N); AL(h->ak2, h->N); AL(h->ae2, h->N); AL(h->anut, h->N);
+    AL(h->bck, h->NB); AL(h->bce, h->NB); AL(h->bck0, h->NB); AL(h->bce0, h->NB);
+    AL(h->indbk, h->NB); AL(h->indbe, h->NB);
+  }
   if (p->idrop >= 1 && !drop_supported(h->g)) {
     g_last_error = "x lines too long for the droplet model's shared-memory walk";
     rc = rc ? rc : CADMAS_EUNSUPPORTED;
@@ -903,6 +961,8 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_res) cudaFreeHost(h->h_res);
   for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
   for (double *q : {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww}) if (q) cudaFree(q);
+  for (double *q : {h->ak, h->ae_k, h->ak2, h->ae2, h->anut, h->bck, h->bce, h->bck0, h->bce0}) if (q) cudaFree(q);
+  for (int *q : {h->indbk, h->indbe}) if (q) cudaFree(q);
   for (float *q : {h->Sf.sys, h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->y2f})
     if (q) cudaFree(q);
   if (h->s) cudaStreamDestroy(h->s);
@@ -970,6 +1030,16 @@ int cadmas_upload_static(cadmas_handle *h, const cadmas_static *st) {
   CK(cudaMemcpyAsync(h->indy, st->indy, b4, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(h->indz, st->indz, b4, cudaMemcpyHostToDevice, s));
   if (h->g.NB > 0) CK(cudaMemcpyAsync(h->indb, st->indb, 4 * h->g.NB * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (h->P.leqk != 0 && h->g.NB > 0) {  // k-epsilon boundaries (vf_iiboun.f:250-330)
+    if (!st->indbk || !st->indbe || !st->bck || !st->bce) return CADMAS_EINVAL;
+    const size_t nb = (size_t)h->g.NB;
+    CK(cudaMemcpyAsync(h->indbk, st->indbk, nb * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->indbe, st->indbe, nb * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->bck0, st->bck, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->bce0, st->bce, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->bck, st->bck, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->bce, st->bce, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
   // host copy of ZZ(2,K) for the bubble timers
   h->zz2.assign(h->g.NK + 1, 0.0);
   std::vector<double> zz(6 * h->g.NK);
@@ -1065,9 +1135,10 @@ int cadmas_restart_create(cadmas_handle *h, const char *path) {
   if (!r.f) { g_last_error = "CAN NOT OPEN (*****.rsl)."; return CADMAS_EIO; }
   const int32_t ver[2] = {0, 1};  // IVR001, IVR002 (VF_A0PRM.h)
   const int32_t dims[4] = {h->g.NI, h->g.NJ, h->g.NK, h->g.NB};
-  // LN, LV, LP, LF, LK, LT, LS, LG, LD, L1: no k-eps, temperature, scalars
-  // or time-dependent porosity here; droplets when IDROP >= 1
-  const int32_t flags[10] = {1, 1, 1, 1, 0, 0, 0, 0, h->P.idrop >= 1 ? 1 : 0, 0};
+  // LN, LV, LP, LF, LK, LT, LS, LG, LD, L1: k-eps when LEQK != 0, no
+  // temperature, scalars or time-dependent porosity here; droplets when
+  // IDROP >= 1
+  const int32_t flags[10] = {1, 1, 1, 1, h->P.leqk != 0 ? 1 : 0, 0, 0, 0, h->P.idrop >= 1 ? 1 : 0, 0};
   std::vector<double> ggv(h->N);
   CK(cudaMemcpy(ggv.data(), h->ggv, h->N * sizeof(double), cudaMemcpyDeviceToHost));
   if (!r.put({{ver, sizeof ver}}) || !r.put({{dims, sizeof dims}}) || !r.put({{flags, sizeof flags}}) ||
@@ -1100,6 +1171,13 @@ int cadmas_restart_append(cadmas_handle *h, const char *path) {
     rc = cadmas_get_drop(h, dr[0].data(), dr[1].data(), dr[2].data(), dr[3].data(), dr[4].data(), dr[5].data());
     if (rc) return rc;
   }
+  std::vector<double> ke[4];  // AK, BCK, AE, BCE
+  if (h->P.leqk != 0) {
+    ke[0].resize(N); ke[2].resize(N); ke[1].resize(NB); ke[3].resize(NB);
+    rc = cadmas_get_turb(h, ke[0].data(), ke[2].data(), nullptr, nullptr, NB ? ke[1].data() : nullptr,
+                         NB ? ke[3].data() : nullptr);
+    if (rc) return rc;
+  }
   FRecordFile r;
   r.f = std::fopen(path, "ab");
   if (!r.f) { g_last_error = "CAN NOT OPEN (*****.rsl)."; return CADMAS_EIO; }
@@ -1110,6 +1188,8 @@ int cadmas_restart_append(cadmas_handle *h, const char *path) {
   bool ok = r.put({{&nnow, 4}, {&tn, 8}, {&dtn, 8}}) && r.put({{sums, sizeof sums}, {&icgitr, 4}}) &&
             r.put({{nf.data(), N * 4}});
   for (int k = 0; k < 5 && ok; ++k) ok = r.put({{a[k].data(), b8}}) && r.put({{bc[k].data(), bb}});
+  if (h->P.leqk != 0)  // vf_or1trn.f:134-146
+    for (int k = 0; k < 4 && ok; ++k) ok = r.put({{ke[k].data(), (k % 2 ? bb : b8)}});
   ok = ok && r.put({{h->tbub.data(), (size_t)h->g.NK * sizeof(double)}});
   if (ok && h->P.idrop >= 1) {
     // the droplet cells (DROPTX >= 0), K, J, I order
@@ -1155,12 +1235,12 @@ int cadmas_restart_load(cadmas_handle *h, const char *path, int nnow) {
   if (!r.get(b) || b.size() != 40) return bad("READ ERROR (*****.res).");
   int32_t L[10];
   std::memcpy(L, b.data(), sizeof L);
-  if (L[4] != 0) return bad("INVALID EQUATION (K-EPS).");
+  if (L[4] != (h->P.leqk != 0 ? 1 : 0)) return bad("INVALID EQUATION (K-EPS).");
   if (L[5] != 0) return bad("INVALID EQUATION (TEMP).");
   if (L[6] != 0) return bad("INVALID EQUATION (CONC).");
   const int LG = L[7], LD = L[8];
   if (LG == 0 && (!r.get(b) || b.size() != N * 8)) return bad("READ ERROR (*****.res).");  // GGV, unused
-  std::vector<unsigned char> rec[14];
+  std::vector<unsigned char> rec[14], kr[4];  // kr: AK, BCK, AE, BCE
   for (;;) {
     bool eof = false;
     if (!r.get(rec[0], &eof)) return bad(eof ? "INVALID STEP." : "READ ERROR (*****.res).");
@@ -1170,6 +1250,11 @@ int cadmas_restart_load(cadmas_handle *h, const char *path, int nnow) {
     const size_t want[12] = {36, N * 4, N * 8, NB * 8, N * 8, NB * 8, N * 8, NB * 8, N * 8, NB * 8, N * 8, NB * 8};
     for (int k = 1; k <= 12; ++k)
       if (!r.get(rec[k]) || rec[k].size() != want[k - 1]) return bad("READ ERROR (*****.res).");
+    if (L[4] != 0) {  // vf_ir1inp.f:213-225
+      const size_t kw[4] = {N * 8, NB * 8, N * 8, NB * 8};
+      for (int k = 0; k < 4; ++k)
+        if (!r.get(kr[k]) || kr[k].size() != kw[k]) return bad("READ ERROR (*****.res).");
+    }
     if (LG != 0 && !r.get(b)) return bad("READ ERROR (*****.res).");  // GGV of IPRNT > 1, unused
     if (!r.get(rec[13]) || rec[13].size() != NK * 8) return bad("READ ERROR (*****.res).");
     const int32_t step = rec_at<int32_t>(rec[0], 0);
@@ -1213,6 +1298,11 @@ int cadmas_restart_load(cadmas_handle *h, const char *path, int nnow) {
     h->stats.fsum = rec_at<double>(rec[1], 0); h->stats.fcut = rec_at<double>(rec[1], 8);
     h->stats.cgbnrm = rec_at<double>(rec[1], 16); h->stats.cgxnrm = rec_at<double>(rec[1], 24);
     h->stats.icgitr = rec_at<int32_t>(rec[1], 32);
+    if (h->P.leqk != 0) {  // k, e, their boundary values, then ANUT, ANU (vf_ir1inp.f:339-340)
+      rc = cadmas_set_turb(h, reinterpret_cast<double *>(kr[0].data()), reinterpret_cast<double *>(kr[2].data()),
+                           reinterpret_cast<double *>(kr[1].data()), reinterpret_cast<double *>(kr[3].data()));
+      if (rc) return rc;
+    }
     if (h->P.idrop >= 1) {
       if (LD >= 1) rc = cadmas_set_drop(h, dr[0].data(), dr[1].data(), dr[2].data(), dr[3].data(), dr[4].data(), dr[5].data());
       else launch_drop_reset(h->s, (long long)N, h->drop);  // vf_ir1inp.f:96-108
@@ -1294,6 +1384,17 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   launch_bspp(s, h->g, h->f);
   launch_bwuwt(s, h->g, h->f);
   launch_bwpp(s, h->g, h->f);
+  if (h->P.leqk != 0) {
+    // vf_cinit.f:295-315 and 359-364 (k, e, ANUT, ANU), then 397-401
+    const KeConst kc = ke_const(h);
+    launch_kinit(s, h->g, h->f, kc, h->ak, h->ae_k, h->anut, h->anu);
+    if (h->g.NB > 0) {
+      CK(cudaMemcpyAsync(h->bck, h->bck0, (size_t)h->g.NB * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      CK(cudaMemcpyAsync(h->bce, h->bce0, (size_t)h->g.NB * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    launch_kbsss(s, h->g, h->f, kc, h->ak, h->ae_k, h->anut, h->anu, true, false);
+    launch_bwke(s, h->g, h->f, ke_arrays(h), h->dint);
+  }
   std::fill(h->tbub.begin(), h->tbub.end(), 0.0);
   launch_drop_reset(s, (long long)h->N, h->drop);  // vf_cinit.f:416-427
   CK(cudaGetLastError());
@@ -1305,6 +1406,37 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   h->stats.fcut = h->h_res[1];
   h->stats.nums = h->h_int[4];
   return map_err(bits);
+}
+
+int cadmas_get_turb(cadmas_handle *h, double *ak, double *ae, double *anut, double *anu, double *bck,
+                    double *bce) {
+  if (!h || h->P.leqk == 0) return CADMAS_EINVAL;
+  cudaStream_t s = h->s;
+  const size_t b8 = h->N * sizeof(double), bb = (size_t)h->g.NB * sizeof(double);
+  if (ak) CK(cudaMemcpyAsync(ak, h->ak, b8, cudaMemcpyDeviceToHost, s));
+  if (ae) CK(cudaMemcpyAsync(ae, h->ae_k, b8, cudaMemcpyDeviceToHost, s));
+  if (anut) CK(cudaMemcpyAsync(anut, h->anut, b8, cudaMemcpyDeviceToHost, s));
+  if (anu) CK(cudaMemcpyAsync(anu, h->anu, b8, cudaMemcpyDeviceToHost, s));
+  if (bck && bb) CK(cudaMemcpyAsync(bck, h->bck, bb, cudaMemcpyDeviceToHost, s));
+  if (bce && bb) CK(cudaMemcpyAsync(bce, h->bce, bb, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return CADMAS_OK;
+}
+
+int cadmas_set_turb(cadmas_handle *h, const double *ak, const double *ae, const double *bck, const double *bce) {
+  if (!h || h->P.leqk == 0 || !ak || !ae || (h->g.NB > 0 && (!bck || !bce))) return CADMAS_EINVAL;
+  if (!h->have_static) return CADMAS_ENOSTATIC;
+  cudaStream_t s = h->s;
+  const size_t b8 = h->N * sizeof(double), bb = (size_t)h->g.NB * sizeof(double);
+  CK(cudaMemcpyAsync(h->ak, ak, b8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->ae_k, ae, b8, cudaMemcpyHostToDevice, s));
+  if (bb) {
+    CK(cudaMemcpyAsync(h->bck, bck, bb, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->bce, bce, bb, cudaMemcpyHostToDevice, s));
+  }
+  ke_nut(h);  // vf_ir1inp.f:339-340
+  CK(cudaStreamSynchronize(s));
+  return CADMAS_OK;
 }
 
 int cadmas_set_time(cadmas_handle *h, double tnow, double dtnow, int nnow) {

@@ -74,6 +74,16 @@ struct DropArrays {
   double *tx, *ty, *tz, *uu, *vv, *ww;
 };
 
+// k-epsilon state (AK, AE, ANUT per cell; BCK, BCE and the types INDBK,
+// INDBE per boundary face) and the constants of /VF_APHYSR/
+struct KeArrays {
+  double *ak, *ae, *anut, *bck, *bce;
+  const int *indbk, *indbe;
+};
+struct KeConst {
+  double anu0, scmk, akmink, akmine, akinik, akinie, akcmu, aksgk, aksge, akc1, akc2, akc3;
+};
+
 __device__ __forceinline__ int indb(const Fld &f, int m, int l) { return f.indb[(m - 1) + 4 * (l - 1)]; }
 
 __device__ __forceinline__ void decode(const Geo &g, int ijk, int &i, int &j, int &k) {

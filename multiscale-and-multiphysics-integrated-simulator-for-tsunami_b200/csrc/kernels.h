@@ -252,6 +252,15 @@ void launch_vmodif(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
 
 // k_vof.cu
 void launch_fconv(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *a, double *b, double *c);
+// k-epsilon (k_keps.cu): VF_K1CAL into akn/aen; VF_BSSS (+ VF_CNUT0 and
+// VF_CNU00 with nut); VF_BWKE; the k, e, ANUT, ANU of VF_CINIT
+void launch_kstep(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, const KeArrays &t,
+                  double *akn, double *aen, int *err);
+void launch_kbsss(cudaStream_t s, const Geo &g, const Fld &f, const KeConst &kc, double *ak, double *ae, double *anut,
+                  double *anu, bool bsss, bool nut);
+void launch_bwke(cudaStream_t s, const Geo &g, const Fld &f, const KeArrays &t, int *err);
+void launch_kinit(cudaStream_t s, const Geo &g, const Fld &f, const KeConst &kc, double *ak, double *ae, double *anut,
+                  double *anu);
 // VF_FCONVS (ISCMFF != 0): slope pass into ist/sx/sy/sz/sa (every cell
 // written), then the face fluxes into flfu/flfv/flfw; ERR_PG into err
 void launch_fconvs(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *ist, double *sx, double *sy,

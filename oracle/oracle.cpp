@@ -337,6 +337,11 @@ struct orc_handle {
   // state
   vd UU, VV, WW, PP, FF, BCU, BCV, BCW, BCP, BCF, TBUB;
   vi NF, INDC, INDS, NLIM;
+  // k-epsilon (LEQK != 0): AK, AE (here AEPS: AE names a solver vector
+  // below), ANUT, BCK, BCE; the boundary types INDBK, INDBE and the input
+  // boundary values BCK0, BCE0
+  vd AK, AEPS, ANUT, BCK, BCE, BCK0, BCE0;
+  vi INDBK, INDBE;
   int NUMS = 0;
   double TNOW = 0, DTNOW = 0;
   // wave maker, matrix table (WAVE-BC ... FUNC MATRIX): IBCTYP/BCTYP of
@@ -2911,6 +2916,308 @@ struct orc_handle {
     return CADMAS_OK;
   }
 
+  // ------------------------------------------------------------ k-epsilon
+  // VF_SCONVD  vf_sconvd.f:37-175 (ISW = -1: SU = SCMK): donor-cell flux
+  // of CC through the faces next to a fluid cell.
+  void sconvd(const vd &CC, const vd &BCC, const vi &INDBC, vd &FU, vd &FV, vd &FW) {
+    const double SU = P.scmk, SC = 1.0 - SU;
+    const size_t sI = 1, sJ = NI, sK = (size_t)NI * NJ;
+    auto face = [&](size_t c, size_t m, double WIN, int IND, double w6, double wm, double wc, double &FL) {
+      if (IND == 0) {
+        double FLC = WIN * w6 * (wm * CC[c] + wc * CC[m]);
+        FL = FL - SU * (dmax(WIN, 0.0) * CC[m] - dmax(-WIN, 0.0) * CC[c]) - SC * FLC;
+      } else if (INDBC[IND - 1] >= 1) {
+        double FLC = WIN * BCC[IND - 1];
+        if (NF[c] == 0) {
+          if (WIN >= 0.0) FL = FL - FLC;
+          else FL = FL - SU * WIN * CC[c] - SC * FLC;
+        } else {
+          if (WIN <= 0.0) FL = FL - FLC;
+          else FL = FL - SU * WIN * CC[m] - SC * FLC;
+        }
+      }
+    };
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c - sI] * NF[c] == 0) face(c, c - sI, GGX[c] * UU[c], INDX[c], X_(6, I), X_(2, I - 1), X_(2, I), FU[c]);
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c - sJ] * NF[c] == 0) face(c, c - sJ, GGY[c] * VV[c], INDY[c], Y_(6, J), Y_(2, J - 1), Y_(2, J), FV[c]);
+        }
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c - sK] * NF[c] == 0) face(c, c - sK, GGZ[c] * WW[c], INDZ[c], Z_(6, K), Z_(2, K - 1), Z_(2, K), FW[c]);
+        }
+  }
+
+  // VF_SDIFF  vf_sdiff.f:47-159 (ISW = -1: AL = 1): diffusive flux with
+  // the diffusivity DD of the cells.
+  void sdiff(const vd &CC, const vd &BCC, const vd &DDv, vd &FU, vd &FV, vd &FW) {
+    const double AL = 1.0;
+    const size_t sI = 1, sJ = NI, sK = (size_t)NI * NJ;
+    // w6, wm, wc: metric 6 and the widths of the face's two cells; w5 the
+    // metric 5 of the face; w4c, w4m the metric 4 of the two cells
+    auto face = [&](size_t c, size_t m, double G, int IND, double w6, double wm, double wc, double w5, double w4c,
+                    double w4m, double &FL) {
+      if (IND == 0) {
+        double D = w6 * (wm * DDv[c] + wc * DDv[m]);
+        D = D * AL;
+        FL = FL + G * D * w5 * (CC[c] - CC[m]);
+      } else {
+        double CW = BCC[IND - 1];
+        if (NF[c] == 0) {
+          double D = DDv[c] * AL;
+          FL = FL + G * D * w4c * (CC[c] - CW) * 2.0;
+        } else {
+          double D = DDv[m] * AL;
+          FL = FL + G * D * w4m * (CW - CC[m]) * 2.0;
+        }
+      }
+    };
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c - sI] * NF[c] == 0)
+            face(c, c - sI, GGX[c], INDX[c], X_(6, I), X_(2, I - 1), X_(2, I), X_(5, I), X_(4, I), X_(4, I - 1), FU[c]);
+        }
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c - sJ] * NF[c] == 0)
+            face(c, c - sJ, GGY[c], INDY[c], Y_(6, J), Y_(2, J - 1), Y_(2, J), Y_(5, J), Y_(4, J), Y_(4, J - 1), FV[c]);
+        }
+    for (int K = 2; K <= NK; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c - sK] * NF[c] == 0)
+            face(c, c - sK, GGZ[c], INDZ[c], Z_(6, K), Z_(2, K - 1), Z_(2, K), Z_(5, K), Z_(4, K), Z_(4, K - 1), FW[c]);
+        }
+  }
+
+  // VF_KGENE  vf_kgene.f:51-182: production and dissipation of the fluid
+  // cells (GT = 0: no buoyancy term).
+  void kgene(vd &QK, vd &QE) {
+    const double ZERO = 1.0e-20;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] != 0) continue;
+          const int IM = I - 1, IP = I + 1, JM = J - 1, JP = J + 1, KM = K - 1, KP = K + 1;
+          double UXM = UU[id(I, J, K)], UXP = UU[id(IP, J, K)];
+          double VYM = VV[id(I, J, K)], VYP = VV[id(I, JP, K)];
+          double WZM = WW[id(I, J, K)], WZP = WW[id(I, J, KP)];
+          double VXM, WXM, VXP, WXP, UYM, WYM, UYP, WYP, UZM, VZM, UZP, VZP;
+          int IND = INDX[id(I, J, K)];
+          if (IND == 0) {
+            VXM = 0.5 * X_(6, I) * (X_(2, IM) * (VV[id(I, J, K)] + VV[id(I, JP, K)]) + X_(2, I) * (VV[id(IM, J, K)] + VV[id(IM, JP, K)]));
+            WXM = 0.5 * X_(6, I) * (X_(2, IM) * (WW[id(I, J, K)] + WW[id(I, J, KP)]) + X_(2, I) * (WW[id(IM, J, K)] + WW[id(IM, J, KP)]));
+          } else { VXM = BCV[IND - 1]; WXM = BCW[IND - 1]; }
+          IND = INDX[id(IP, J, K)];
+          if (IND == 0) {
+            VXP = 0.5 * X_(6, IP) * (X_(2, I) * (VV[id(IP, J, K)] + VV[id(IP, JP, K)]) + X_(2, IP) * (VV[id(I, J, K)] + VV[id(I, JP, K)]));
+            WXP = 0.5 * X_(6, IP) * (X_(2, I) * (WW[id(IP, J, K)] + WW[id(IP, J, KP)]) + X_(2, IP) * (WW[id(I, J, K)] + WW[id(I, J, KP)]));
+          } else { VXP = BCV[IND - 1]; WXP = BCW[IND - 1]; }
+          IND = INDY[id(I, J, K)];
+          if (IND == 0) {
+            UYM = 0.5 * Y_(6, J) * (Y_(2, JM) * (UU[id(I, J, K)] + UU[id(IP, J, K)]) + Y_(2, J) * (UU[id(I, JM, K)] + UU[id(IP, JM, K)]));
+            WYM = 0.5 * Y_(6, J) * (Y_(2, JM) * (WW[id(I, J, K)] + WW[id(I, J, KP)]) + Y_(2, J) * (WW[id(I, JM, K)] + WW[id(I, JM, KP)]));
+          } else { UYM = BCU[IND - 1]; WYM = BCW[IND - 1]; }
+          IND = INDY[id(I, JP, K)];
+          if (IND == 0) {
+            UYP = 0.5 * Y_(6, JP) * (Y_(2, J) * (UU[id(I, JP, K)] + UU[id(IP, JP, K)]) + Y_(2, JP) * (UU[id(I, J, K)] + UU[id(IP, J, K)]));
+            WYP = 0.5 * Y_(6, JP) * (Y_(2, J) * (WW[id(I, JP, K)] + WW[id(I, JP, KP)]) + Y_(2, JP) * (WW[id(I, J, K)] + WW[id(I, J, KP)]));
+          } else { UYP = BCU[IND - 1]; WYP = BCW[IND - 1]; }
+          IND = INDZ[id(I, J, K)];
+          if (IND == 0) {
+            UZM = 0.5 * Z_(6, K) * (Z_(2, KM) * (UU[id(I, J, K)] + UU[id(IP, J, K)]) + Z_(2, K) * (UU[id(I, J, KM)] + UU[id(IP, J, KM)]));
+            VZM = 0.5 * Z_(6, K) * (Z_(2, KM) * (VV[id(I, J, K)] + VV[id(I, JP, K)]) + Z_(2, K) * (VV[id(I, J, KM)] + VV[id(I, JP, KM)]));
+          } else { UZM = BCU[IND - 1]; VZM = BCV[IND - 1]; }
+          IND = INDZ[id(I, J, KP)];
+          if (IND == 0) {
+            UZP = 0.5 * Z_(6, KP) * (Z_(2, K) * (UU[id(I, J, KP)] + UU[id(IP, J, KP)]) + Z_(2, KP) * (UU[id(I, J, K)] + UU[id(IP, J, K)]));
+            VZP = 0.5 * Z_(6, KP) * (Z_(2, K) * (VV[id(I, J, KP)] + VV[id(I, JP, KP)]) + Z_(2, KP) * (VV[id(I, J, K)] + VV[id(I, JP, K)]));
+          } else { UZP = BCU[IND - 1]; VZP = BCV[IND - 1]; }
+          double DLR = X_(4, I);
+          double DUDX = DLR * (UXP - UXM), DVDX = DLR * (VXP - VXM), DWDX = DLR * (WXP - WXM);
+          DLR = Y_(4, J);
+          double DUDY = DLR * (UYP - UYM), DVDY = DLR * (VYP - VYM), DWDY = DLR * (WYP - WYM);
+          DLR = Z_(4, K);
+          double DUDZ = DLR * (UZP - UZM), DVDZ = DLR * (VZP - VZM), DWDZ = DLR * (WZP - WZM);
+          double GS = ANUT[c] * (2.0 * (DUDX * DUDX + DVDY * DVDY + DWDZ * DWDZ) + ipow(DUDY + DVDX, 2) +
+                                 ipow(DVDZ + DWDY, 2) + ipow(DWDX + DUDZ, 2));
+          double GT = 0.0;
+          double GST = GS + GT;
+          double RF = -GT / dmax(GST, ZERO);
+          double AK0 = dmax(AK[c], P.akmink);
+          double AE0 = AEPS[c];
+          double AEK = AE0 / AK0;
+          double GG = GGV[c];
+          QK[c] = QK[c] + GG * (GST - AE0);
+          QE[c] = QE[c] + GG * (P.akc1 * AEK * GST * (1.0 + P.akc3 * RF) - P.akc2 * AEK * AE0);
+        }
+  }
+
+  // VF_SEULER  vf_seuler.f:43-56 (GGV0 = GGV): Euler step of the fluid cells.
+  void seuler(vd &CC, const vd &FU, const vd &FV, const vd &FW, const vd &QC) {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] != 0) continue;
+          double G0 = GGV[c] - (GGV[c] - GGV[c]) * 1.0;
+          double DS = (X_(4, I) * (FU[id(I + 1, J, K)] - FU[c]) + Y_(4, J) * (FV[id(I, J + 1, K)] - FV[c]) +
+                       Z_(4, K) * (FW[id(I, J, K + 1)] - FW[c]) + QC[c]);
+          CC[c] = (G0 * CC[c] + DTNOW * DS) / GGV[c];
+        }
+  }
+
+  // VF_BSSS  vf_bsss.f:27-66: gas cells 0, surface cells the mean of their
+  // fluid neighbours (none is written in the pass, so it is in place).
+  void bsss(vd &SC) {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] == 8) SC[c] = 0.0;
+          else if (NF[c] >= 1) {
+            int N = 0;
+            double S = 0.0;
+            const size_t nb[6] = {id(I - 1, J, K), id(I + 1, J, K), id(I, J - 1, K), id(I, J + 1, K), id(I, J, K - 1),
+                                  id(I, J, K + 1)};
+            for (int q = 0; q < 6; ++q)
+              if (NF[nb[q]] == 0) { N = N + 1; S = S + SC[nb[q]]; }
+            SC[c] = S / (double)N;
+          }
+        }
+  }
+
+  // VF_BWKE  vf_bwke.f:33-108: boundary values of k and e.
+  int bwke() {
+    for (int L = 1; L <= NB; ++L) {
+      int I, J, K;
+      decode(IB_(1, L), I, J, K);
+      const int NS = IB_(2, L), IBK = std::abs(INDBK[L - 1]), IBE = std::abs(INDBE[L - 1]);
+      size_t c;
+      if (NS == 1) c = id(I, J, K);
+      else if (NS == 2) c = id(I - 1, J, K);
+      else if (NS == 3) c = id(I, J, K);
+      else if (NS == 4) c = id(I, J - 1, K);
+      else if (NS == 5) c = id(I, J, K);
+      else c = id(I, J, K - 1);
+      const double AKC = AK[c], AEC = AEPS[c];
+      if (IBK == 1) BCK[L - 1] = BCK[L - 1];
+      else if (IBK == 2 || IBK == 6 || IBK == 8) BCK[L - 1] = AKC;
+      else return CADMAS_EPG;
+      if (IBE == 1) BCE[L - 1] = BCE[L - 1];
+      else if (IBE == 2 || IBE == 6 || IBE == 8) BCE[L - 1] = AEC;
+      else return CADMAS_EPG;
+    }
+    return CADMAS_OK;
+  }
+
+  // VF_CNUT0  vf_cnut0.f:37-49 and VF_CNU00  vf_cnu00.f:52-61: the eddy
+  // viscosity C_mu k^2 / max(e, AKMINE) and ANU = ANU0 + ANUT.
+  void cnut0() {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] != -1) {
+            double W = dmax(AEPS[c], P.akmine);
+            ANUT[c] = P.akcmu * AK[c] * AK[c] / W;
+          } else ANUT[c] = 0.0;
+        }
+  }
+  void cnu00() {
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          ANU[c] = (NF[c] != -1) ? P.anu0 + ANUT[c] : 0.0;
+        }
+  }
+
+  // VF_K1CAL  vf_k1cal.f:84-170 (ISCMK = 0; VF_BWKELG acts on log-law and
+  // rough walls only, which cadmas_create refuses)
+  int k1cal() {
+    const size_t N = UU.size();
+    vd FLKU(N, 0.0), FLKV(N, 0.0), FLKW(N, 0.0), QK(N, 0.0), FLEU(N, 0.0), FLEV(N, 0.0), FLEW(N, 0.0),
+        QE(N, 0.0), WKNU(N, 0.0);
+    sconvd(AK, BCK, INDBK, FLKU, FLKV, FLKW);
+    sconvd(AEPS, BCE, INDBE, FLEU, FLEV, FLEW);
+    double W = 1.0 / P.aksgk;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I)
+          if (NF[id(I, J, K)] != -1) WKNU[id(I, J, K)] = P.anu0 + ANUT[id(I, J, K)] * W;
+    sdiff(AK, BCK, WKNU, FLKU, FLKV, FLKW);
+    W = 1.0 / P.aksge;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I)
+          if (NF[id(I, J, K)] != -1) WKNU[id(I, J, K)] = P.anu0 + ANUT[id(I, J, K)] * W;
+    sdiff(AEPS, BCE, WKNU, FLEU, FLEV, FLEW);
+    kgene(QK, QE);
+    seuler(AK, FLKU, FLKV, FLKW, QK);
+    seuler(AEPS, FLEU, FLEV, FLEW, QE);
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          size_t c = id(I, J, K);
+          if (NF[c] == 0) {
+            if (AEPS[c] < P.akmine) { AK[c] = P.akmink; AEPS[c] = P.akmine; }
+            else if (AK[c] < P.akmink) AK[c] = P.akmink;
+          }
+        }
+    bsss(AK);
+    bsss(AEPS);
+    return bwke();
+  }
+
+  // After VF_F1CAL (vf_a1main.f:1119-1127): the new NF's surface and gas
+  // values, the eddy viscosity, boundary values.
+  int kpost() {
+    bsss(AK);
+    bsss(AEPS);
+    cnut0();
+    cnu00();
+    int rc = bwke();
+    if (rc) return rc;
+    bwuwt();
+    return CADMAS_OK;
+  }
+
+  // VF_CINIT's k-epsilon part (vf_cinit.f:295-315, 359-364; the boundary
+  // part 397-401 is kinit_bc)
+  void kinit() {
+    const size_t N = UU.size();
+    AK.assign(N, 0.0); AEPS.assign(N, 0.0); ANUT.assign(N, 0.0);
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I)
+          if (INDC[id(I, J, K)] != -1) { AK[id(I, J, K)] = P.akinik; AEPS[id(I, J, K)] = P.akinie; }
+    cnut0();
+    std::fill(ANU.begin(), ANU.end(), 0.0);
+    cnu00();
+  }
+  int kinit_bc() {
+    BCK = BCK0; BCE = BCE0;
+    bsss(AK);
+    bsss(AEPS);
+    return bwke();
+  }
+
   // VF_F1CAL  vf_f1cal.f:121-243
   int f1cal() {
     Timer T;
@@ -2992,6 +3299,14 @@ int orc_upload_static(orc_handle *h, const cadmas_static *s) {
   h->INDZ.assign(s->indz, s->indz + N);
   h->INDB.assign(s->indb, s->indb + 4 * (size_t)h->NB);
   if (h->NB == 0) h->INDB.assign(4, 0);
+  if (h->P.leqk != 0) {
+    if (!s->indbk || !s->indbe || !s->bck || !s->bce) return CADMAS_EINVAL;
+    const size_t B = (size_t)h->NB;
+    h->INDBK.assign(s->indbk, s->indbk + B); h->INDBE.assign(s->indbe, s->indbe + B);
+    h->BCK0.assign(s->bck, s->bck + B); h->BCE0.assign(s->bce, s->bce + B);
+    h->BCK = h->BCK0; h->BCE = h->BCE0;
+    h->AK.assign(N, 0.0); h->AEPS.assign(N, 0.0); h->ANUT.assign(N, 0.0);
+  }
   h->have_static = true;
   return CADMAS_OK;
 }
@@ -3068,7 +3383,12 @@ int orc_init_state(orc_handle *h, int hydrostatic) {
   }
   rc = h->bwuwn();
   if (rc) return rc;
+  if (h->P.leqk != 0) h->kinit();  // vf_cinit.f:295-315, 359-364
   h->bsuwt(); h->bsuwt2(); h->bsuwn3(); h->bspp(); h->bwuwt(); h->bwpp();
+  if (h->P.leqk != 0) {  // vf_cinit.f:397-401
+    rc = h->kinit_bc();
+    if (rc) return rc;
+  }
   std::fill(h->TBUB.begin(), h->TBUB.end(), 0.0);
   h->drop_alloc();  // vf_cinit.f:416-427
   h->st.nums = h->NUMS;
@@ -3082,7 +3402,9 @@ int orc_step(orc_handle *h, double dt) {
   h->NNOW = h->NNOW + 1;
   h->TNOW = h->TNOW + h->DTNOW;
   int rc = h->v1cal();
+  if (rc == CADMAS_OK && h->P.leqk != 0) rc = h->k1cal();  // vf_a1main.f:1093-1100
   if (rc == CADMAS_OK) rc = h->f1cal();
+  if (rc == CADMAS_OK && h->P.leqk != 0) rc = h->kpost();  // vf_a1main.f:1119-1127
   h->st.last_status = rc;
   return rc;
 }
@@ -3162,6 +3484,23 @@ int orc_set_time(orc_handle *h, double tnow, double dtnow, int nnow) {
 int orc_cdtcal(orc_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt) {
   if (!h->have_static) return CADMAS_ENOSTATIC;
   *dt = h->cdtcal(dtinit, dtmin, dtmax, dtsafe);
+  return CADMAS_OK;
+}
+
+int orc_get_turb(orc_handle *h, double *ak, double *ae, double *anut, double *anu, double *bck, double *bce) {
+  if (h->P.leqk == 0) return CADMAS_EINVAL;
+  auto put = [](const vd &v, double *o) { if (o) std::copy(v.begin(), v.end(), o); };
+  put(h->AK, ak); put(h->AEPS, ae); put(h->ANUT, anut); put(h->ANU, anu); put(h->BCK, bck); put(h->BCE, bce);
+  return CADMAS_OK;
+}
+
+int orc_set_turb(orc_handle *h, const double *ak, const double *ae, const double *bck, const double *bce) {
+  if (h->P.leqk == 0 || !ak || !ae || !bck || !bce) return CADMAS_EINVAL;
+  const size_t N = (size_t)h->NI * h->NJ * h->NK, B = (size_t)h->NB;
+  h->AK.assign(ak, ak + N); h->AEPS.assign(ae, ae + N);
+  h->BCK.assign(bck, bck + B); h->BCE.assign(bce, bce + B);
+  h->cnut0();  // vf_ir1inp.f:339-340
+  h->cnu00();
   return CADMAS_OK;
 }
 

@@ -65,6 +65,9 @@ int orc_set_drop(orc_handle *h, const double *tx, const double *ty, const double
 int orc_set_time(orc_handle *h, double tnow, double dtnow, int nnow);
 /* VF_CDTCAL as cadmas_cdtcal (reference order: the running minimum). */
 int orc_cdtcal(orc_handle *h, double dtinit, double dtmin, double dtmax, double dtsafe, double *dt);
+/* The k-epsilon state as cadmas_get_turb / cadmas_set_turb. */
+int orc_get_turb(orc_handle *h, double *ak, double *ae, double *anut, double *anu, double *bck, double *bce);
+int orc_set_turb(orc_handle *h, const double *ak, const double *ae, const double *bck, const double *bce);
 /* FF-SLOPE checks: cells of each slope type (index 0..7) seen by the
    VF_FCONVS passes so far; the elementary functions of VF_CROOT3
    (fn 0 cube root, 1 arctangent, 2 cosine); VF_FSLP2A/3A followed by

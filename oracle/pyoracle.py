@@ -63,6 +63,8 @@ def _load_lib():
     lib.orc_set_drop.argtypes = [C.c_void_p] + [dp] * 6
     lib.orc_cdtcal.argtypes = [C.c_void_p] + [C.c_double] * 4 + [dp]
     lib.orc_set_time.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+    lib.orc_get_turb.argtypes = [C.c_void_p] + [dp] * 6
+    lib.orc_set_turb.argtypes = [C.c_void_p] + [dp] * 4
     lib.orc_slope_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     lib.orc_slope_fn.argtypes = [C.c_int, C.c_double]
     lib.orc_slope_fn.restype = C.c_double
@@ -93,6 +95,9 @@ class Oracle:
             base.damp[d][0], base.damp[d][1], base.damp[d][2], base.damp[d][3] = 0.6, 0.6, 0.0, 0.0
         base.icgtyp, base.icgmax, base.ibsuw0 = 1, 500, 0
         base.idrop = 1
+        base.anu0, base.scmk = 1.0e-6, 1.0
+        base.akmink = base.akmine = base.akinik = base.akinie = 1.0e-20
+        base.akcmu, base.aksgk, base.aksge, base.akc1, base.akc2, base.akc3 = 0.09, 1.0, 1.3, 1.44, 1.92, 0.0
         self.params = P.make_params(case, base, **over)
         d = P.Dims(case.ni, case.nj, case.nk, case.numb)
         self.h = self.lib.orc_create(C.byref(d), C.byref(self.params), int(sum_mode))
@@ -146,6 +151,22 @@ class Oracle:
         keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64) for n in self.P.DROP_ARRAYS}
         dp = C.POINTER(C.c_double)
         self._rc(self.lib.orc_set_drop(self.h, *(keep[n].ctypes.data_as(dp) for n in self.P.DROP_ARRAYS)))
+
+    def get_turb(self):
+        """The k-epsilon state {ak, ae, anut, anu} (flat) and {bck, bce}."""
+        c = self.case
+        cells, faces = self.P.TURB_CELLS, self.P.TURB_FACES
+        arrs = {n: np.zeros(c.ni * c.nj * c.nk) for n in cells}
+        arrs.update({n: np.zeros(max(c.numb, 1)) for n in faces})
+        dp = C.POINTER(C.c_double)
+        self._rc(self.lib.orc_get_turb(self.h, *(arrs[n].ctypes.data_as(dp) for n in cells + faces)))
+        return arrs
+
+    def set_turb(self, arrs):
+        keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64).reshape(-1, order="F")
+                for n in ("ak", "ae", "bck", "bce")}
+        dp = C.POINTER(C.c_double)
+        self._rc(self.lib.orc_set_turb(self.h, *(keep[n].ctypes.data_as(dp) for n in ("ak", "ae", "bck", "bce"))))
 
     def slope_counts(self):
         """Cells of each slope type 0..7 seen by VF_FCONVS so far."""

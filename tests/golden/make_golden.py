@@ -33,8 +33,11 @@ CASES = {
     "ffslope_tank_1_20": dict(builder="random_tank", kw=dict(seed=1), steps=20, sum_mode=0,
                               over=dict(iscmff=1)),
     "ffslope_dam_break_10": dict(builder="dam_break", kw={}, steps=10, sum_mode=0, over=dict(iscmff=1)),
+    # k-epsilon (LEQK = 1) with random k, e boundary types
+    "turbulent_tank_0_10": dict(builder="turbulent_tank", kw=dict(seed=0), steps=10, sum_mode=0, over={}),
 }
 DROP = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
+TURB = ("ak", "ae", "anut", "anu", "bck", "bce")
 FIELDS = ("uu", "vv", "ww", "pp", "ff", "nf", "indc", "bcu", "bcv", "bcw", "bcp", "bcf")
 
 
@@ -58,6 +61,9 @@ def run(name, spec):
     if drops is not None:
         d = o.get_drop()
         dig.update({n: hashlib.sha256(d[n].tobytes()).hexdigest()[:32] for n in DROP})
+    if c.params.get("leqk", 0):
+        t = o.get_turb()
+        dig.update({n: hashlib.sha256(t[n].tobytes()).hexdigest()[:32] for n in TURB})
     return dict(digest=dig, stats={k: st[k] for k in ("fsum", "fcut", "cgbnrm", "cgxnrm", "icgitr", "nums")})
 
 
