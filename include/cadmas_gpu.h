@@ -257,6 +257,29 @@ int cadmas_get_turb(cadmas_handle *h, double *ak, double *ae, double *anut, doub
 int cadmas_set_turb(cadmas_handle *h, const double *ak, const double *ae, const double *bck,
                     const double *bce);
 
+/* ---- learned warm start: the 3-D U-Net ---------------------------------
+   A 3-level U-Net (3x3x3 convolutions, channels 16/32/64, BF16 weights and
+   activations, FP32 accumulation on the tensor cores) from 4 input
+   channels per voxel to 1 output.  Volumes are nx x ny x nz voxels (each a
+   multiple of 4), batch of them; host arrays are C-ordered
+   [batch][nz][ny][nx] (x fastest), inputs with 4 channels innermost.
+   Parameters: cadmas_unet_param_count() FP32 values.  _grad returns the
+   masked mean-square loss against t (mask m, 1 = counted) and its
+   parameter gradient; _train_step applies Adam (beta 0.9/0.999, eps 1e-8)
+   with learning rate lr.  CADMAS_ETIMEOUT when a tensor-core wait ran
+   out of time.                                                         */
+typedef struct cadmas_unet cadmas_unet;
+size_t cadmas_unet_param_count(void);
+int cadmas_unet_create(int nx, int ny, int nz, int batch, cadmas_unet **net);
+int cadmas_unet_destroy(cadmas_unet *net);
+int cadmas_unet_set_params(cadmas_unet *net, const float *params);
+int cadmas_unet_get_params(cadmas_unet *net, float *params);
+int cadmas_unet_forward(cadmas_unet *net, const float *x, float *y);
+int cadmas_unet_grad(cadmas_unet *net, const float *x, const float *t, const float *m, float *loss,
+                     float *grad);
+int cadmas_unet_train_step(cadmas_unet *net, const float *x, const float *t, const float *m, float lr,
+                           float *loss);
+
 /* ---- restart file (*.rsl / *.res) and list file ----------------------
    The restart file of the reference, byte for byte: a Fortran unformatted
    sequential file (each record framed by its byte count as a 4-byte

@@ -99,7 +99,9 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers", "cadmas_get_drop",
             "cadmas_set_drop", "cadmas_restart_create", "cadmas_restart_append", "cadmas_restart_load",
-            "cadmas_list_step", "cadmas_cdtcal", "cadmas_get_turb", "cadmas_set_turb"]
+            "cadmas_list_step", "cadmas_cdtcal", "cadmas_get_turb", "cadmas_set_turb",
+            "cadmas_unet_param_count", "cadmas_unet_create", "cadmas_unet_destroy", "cadmas_unet_set_params",
+            "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
@@ -150,6 +152,16 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_cdtcal.argtypes = [C.c_void_p] + [C.c_double] * 4 + [C.POINTER(C.c_double)]
     lib.cadmas_set_drop.argtypes = [C.c_void_p] + [_dp] * 6
     lib.cadmas_get_turb.argtypes = [C.c_void_p] + [_dp] * 6
+    _fp = C.POINTER(C.c_float)
+    lib.cadmas_unet_param_count.restype = C.c_size_t
+    lib.cadmas_unet_param_count.argtypes = []
+    lib.cadmas_unet_create.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_void_p)]
+    lib.cadmas_unet_destroy.argtypes = [C.c_void_p]
+    lib.cadmas_unet_set_params.argtypes = [C.c_void_p, _fp]
+    lib.cadmas_unet_get_params.argtypes = [C.c_void_p, _fp]
+    lib.cadmas_unet_forward.argtypes = [C.c_void_p, _fp, _fp]
+    lib.cadmas_unet_grad.argtypes = [C.c_void_p, _fp, _fp, _fp, _fp, _fp]
+    lib.cadmas_unet_train_step.argtypes = [C.c_void_p, _fp, _fp, _fp, C.c_float, _fp]
     lib.cadmas_set_turb.argtypes = [C.c_void_p] + [_dp] * 4
     lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
     lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
@@ -275,6 +287,69 @@ def initial_state(case):
     for n in ("bcu", "bcv", "bcw", "bcp", "bcf"):
         st[n][...] = getattr(case, n)
     return st
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+class UNet:
+    """The learned warm start's 3-D U-Net on the GPU (cadmas_unet_*):
+    volumes (batch, nz, ny, nx) of 4 input channels and one output."""
+
+    def __init__(self, nx, ny, nz, batch=1, lib=None):
+        self.lib = lib or load_library()
+        self.shape = (batch, nz, ny, nx)
+        self.h = C.c_void_p()
+        _check(self.lib, self.lib.cadmas_unet_create(nx, ny, nz, batch, C.byref(self.h)))
+        self.nparam = int(self.lib.cadmas_unet_param_count())
+
+    def set_params(self, p):
+        p = _f32(p)
+        assert p.size == self.nparam
+        _check(self.lib, self.lib.cadmas_unet_set_params(self.h, _fptr(p)))
+
+    def get_params(self):
+        p = np.zeros(self.nparam, np.float32)
+        _check(self.lib, self.lib.cadmas_unet_get_params(self.h, _fptr(p)))
+        return p
+
+    def forward(self, x):
+        x = _f32(x)
+        assert x.shape == self.shape + (4,)
+        y = np.zeros(self.shape, np.float32)
+        _check(self.lib, self.lib.cadmas_unet_forward(self.h, _fptr(x), _fptr(y)))
+        return y
+
+    def grad(self, x, t, m):
+        """(loss, gradient over the parameters) of the masked MSE."""
+        x, t, m = _f32(x), _f32(t), _f32(m)
+        loss = C.c_float()
+        g = np.zeros(self.nparam, np.float32)
+        _check(self.lib, self.lib.cadmas_unet_grad(self.h, _fptr(x), _fptr(t), _fptr(m), C.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def train_step(self, x, t, m, lr=1.0e-3):
+        x, t, m = _f32(x), _f32(t), _f32(m)
+        loss = C.c_float()
+        _check(self.lib, self.lib.cadmas_unet_train_step(self.h, _fptr(x), _fptr(t), _fptr(m), float(lr),
+                                                         C.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.cadmas_unet_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Tank:

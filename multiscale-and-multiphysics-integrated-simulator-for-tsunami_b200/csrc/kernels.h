@@ -252,6 +252,36 @@ void launch_vmodif(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
 
 // k_vof.cu
 void launch_fconv(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *a, double *b, double *c);
+// learned warm start (k_unet.cu): tcgen05 implicit-GEMM 3x3x3 convolution
+// (mode: BF16 out, ReLU + BF16, ReLU-backward mask + BF16, FP32 out), its
+// weight gradient, and the U-Net's elementwise kernels
+enum { CONV_BF16 = 0, CONV_RELU_BF16 = 1, CONV_MASK_BF16 = 2, CONV_F32 = 3 };
+bool unet_kernels_configure();
+size_t conv_smem_bytes(int Cin, int Cout);
+size_t wgrad_smem_bytes(int Cout);
+void launch_conv(cudaStream_t s, int X, int Y, int Z, int B, const void *x, int Cin, const void *w, const float *bias,
+                 int Cout, int mode, const void *mask, void *y, int *err);
+void launch_wgrad(cudaStream_t s, int X, int Y, int Z, int B, const void *x, int Cin, const void *dy, int Cout,
+                  long long slice, float *part, float *dw, int *err);
+void launch_bias_grad(cudaStream_t s, long long V, const void *dy, int C, float *part, float *db);
+void launch_pool(cudaStream_t s, int Xc, int Yc, int Zc, int B, const void *f, int C, void *c);
+void launch_pool_bwd(cudaStream_t s, int Xc, int Yc, int Zc, int B, const void *dc, int C, void *df, int acc);
+void launch_upcat(cudaStream_t s, int X, int Y, int Z, int B, const void *c, int C1, const void *sk, int C2, void *o);
+void launch_upcat_bwd(cudaStream_t s, int X, int Y, int Z, int B, const void *d, int C1, int C2, void *dc, void *dsk,
+                      int acc);
+void launch_relu_mask(cudaStream_t s, long long n, const void *act, void *d);
+void launch_head(cudaStream_t s, long long V, const void *a, int C, const float *wh, const float *bh, float *y);
+void launch_mse(cudaStream_t s, long long V, const float *y, const float *t, const float *m, float inv_n, float *dy,
+                float *lpart);
+void launch_head_bwd(cudaStream_t s, long long V, const float *dy, const void *a, int C, const float *wh, void *da,
+                     float *part);
+void launch_adam(cudaStream_t s, long long n, float *p, const float *g, float *m, float *v, float lr, float b1,
+                 float b2, float eps, float c1, float c2);
+void launch_wcast(cudaStream_t s, const float *w, int Cin, int Cout, void *wf, void *wt);
+void launch_f32_to_bf16(cudaStream_t s, long long n, const float *a, void *b);
+void launch_fill_bf16(cudaStream_t s, long long n, void *a);
+void launch_pack_in(cudaStream_t s, long long V, const float *x4, void *x16);
+void launch_bias_reduce(cudaStream_t s, const float *part, int n, int C, float *out);
 // k-epsilon (k_keps.cu): VF_K1CAL into akn/aen; VF_BSSS (+ VF_CNUT0 and
 // VF_CNU00 with nut); VF_BWKE; the k, e, ANUT, ANU of VF_CINIT
 void launch_kstep(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, const KeArrays &t,
