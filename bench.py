@@ -97,7 +97,7 @@ def params_for(args):
     return dict(cgepsr=1.0e-8 if getattr(args, "case", "flume") == "beach" else 1.0e-10,
                 precond_ti=args.ti, precond_tj=args.tj, precond_split=getattr(args, "split", 1),
                 solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
-                warm_start=1 if getattr(args, "guess", "zero") == "previous" else 0)
+                warm_start={"zero": 0, "previous": 1, "learned": 2}[getattr(args, "guess", "zero")])
 
 
 class ClockSampler:
@@ -229,6 +229,9 @@ def workload_config(case, args):
                 "l2": "inputs larger than L2"}
     if getattr(args, "guess", "zero") == "previous":
         solver += ", previous-step initial guess,"
+    if getattr(args, "guess", "zero") == "learned":
+        solver += (f", learned initial guess (U-Net trained on the first {args.train_steps} steps' solves, "
+                   f"timed after them),")
     return {"workload": f"porous wave flume {case.ni-2}x{case.nj-2}x{case.nk-2} {solver} SMAC step "
                         f"(wave maker H=0.08 T=1.5 at x=0 on a developed first-order wave train, "
                         f"dt={case.dt}, tol 1e-10, block-Jacobi MILU "
@@ -272,9 +275,25 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     case = build_case(args)
+    learned = None
+    if getattr(args, "guess", "zero") == "learned":
+        # train the guess on the solver's own solves of the first steps
+        # (outside the timing), then time the steps after them
+        import importlib
+        ws = importlib.import_module(P.__name__ + ".warmstart")
+        t0 = time.time()
+        samples = ws.collect(case, args.train_steps, precond_ti=args.ti, precond_tj=args.tj)
+        params, cscale = ws.train(samples, epochs=args.train_epochs, batch=1, lr=1.0e-3, w_mse=0.1, w_res=1.0)
+        learned = {"train_steps": args.train_steps, "epochs": args.train_epochs,
+                   "train_s": round(time.time() - t0, 1), "out_scale": cscale}
+        del samples
     tank = P.Tank(case, **params_for(args))
+    if learned is not None:
+        tank.set_warm_net(params, cscale)
     tank.init_state(True)
     stream = torch.cuda.ExternalStream(tank.stream(), device=dev)
+    for _ in range(args.train_steps if learned is not None else 0):
+        tank.step(case.dt)
     for _ in range(args.warmup):
         tank.step(case.dt)
     tank.sync()
@@ -377,16 +396,74 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": v_cpu, "unit": UNIT, "cores": thr, "kind": "port",
                "sample": f"{n_cpu} steps of the same flume after 1 warm-up step, {t_cpu:.1f} s, "
                          f"oracle (reference summation order) with its solver on {thr} OpenMP threads"}
+    if learned is not None:
+        # kept/dropped guesses, and the zero guess's iterations on the same steps
+        kept, dropped = tank.warm_stats()
+        z = P.Tank(case, **{**params_for(args), "warm_start": 0})
+        z.init_state(True)
+        for _ in range(args.train_steps + args.warmup):
+            z.step(case.dt)
+        zi = []
+        for _ in range(args.steps):
+            z.step(case.dt)
+            zi.append(z.stats()["icgitr"])
+        z.close()
+        learned.update(kept=kept, dropped=dropped, zero_guess_mean_iters_same_steps=float(np.mean(zi)))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {**workload_config(case, args), "parallelism": f"replicas x{world}",
-                       "mean_bicgstab_iters": float(np.mean(iters)), "true_relres": relres},
+                       "mean_bicgstab_iters": float(np.mean(iters)), "true_relres": relres,
+                       **({"learned_guess": learned} if learned is not None else {})},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks,
             "stage_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()}}
     print(json.dumps(line), flush=True)
     tank.close()
+
+
+def measured_peak_bf16():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+        except Exception:
+            pass
+    return 1590.0, "fallback"
+
+
+# (cin, cout, level) of the warm-start U-Net's 3x3x3 convolutions
+UNET_LAYERS = [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2),
+               (64, 64, 2), (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0)]
+
+
+def run_unet(args, rank, world, local_rank):
+    """The learned guess's network alone: device time of its forward on one
+    volume (the tcgen05 convolutions), FLOP/s against the bf16 peak."""
+    import importlib
+    P = _load_pkg()
+    P.build_library()
+    ws = importlib.import_module(P.__name__ + ".warmstart")
+    X, Y, Z = (int(v) for v in args.unet_volume.split("x"))
+    net = P.UNet(X, Y, Z, 1)
+    net.set_params(ws.init_params(2))
+    x = np.random.default_rng(0).normal(size=(1, Z, Y, X, 4)).astype(np.float32)
+    net.forward(x)
+    net.time_forward(max(1, args.warmup))
+    ms = net.time_forward(args.steps)
+    vox = [X * Y * Z // 8 ** lv for lv in range(3)]
+    flop = sum(2 * 27 * ci * co * vox[lv] for ci, co, lv in UNET_LAYERS) + 2 * 16 * vox[0]
+    tf = flop / (ms * 1e-3) / 1e12
+    peak, kind = measured_peak_bf16()
+    if rank == 0:
+        print(json.dumps({"metric": "U-Net forward TFLOP/s (learned initial guess)", "value": tf, "unit": "TFLOP/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+                          "data": "synthetic", "config": {"workload": f"warm-start U-Net forward on a {X}x{Y}x{Z} "
+                                                                      f"volume (16/32/64 channels)"},
+                          "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                                       "frac": tf / peak, "peak_kind": kind, "traffic": None}}), flush=True)
+    net.close()
 
 
 def run_ensemble(args, rank, world, local_rank):
@@ -463,10 +540,14 @@ def main():
                     help="2: each preconditioner block swept by a cluster of two thread blocks")
     ap.add_argument("--members", type=int, default=8, help="ensemble members (--case ensemble)")
     ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
-    ap.add_argument("--case", choices=["flume", "beach", "ensemble"], default="flume",
+    ap.add_argument("--case", choices=["flume", "beach", "ensemble", "unet"], default="flume",
                     help="flume: 512x32x96 porous wave flume (default); beach: 1024x128x128 solitary "
-                         "wave on a 1:20 beach with 40 porous boxes")
-    ap.add_argument("--guess", choices=["zero", "previous"], default="zero",
+                         "wave on a 1:20 beach with 40 porous boxes; unet: the learned guess's network alone")
+    ap.add_argument("--unet-volume", default="64x32x64", help="--case unet: XxYxZ (multiples of 4)")
+    ap.add_argument("--train-steps", type=int, default=40,
+                    help="--guess learned: steps whose solves train the network")
+    ap.add_argument("--train-epochs", type=int, default=15, help="--guess learned: epochs over them")
+    ap.add_argument("--guess", choices=["zero", "previous", "learned"], default="zero",
                     help="initial guess of each pressure solve: 0 as the reference, or the previous "
                          "step's solution")
     ap.add_argument("--nx", type=int, default=512)
@@ -493,6 +574,8 @@ def main():
             run_reference(args, rank, world)
         elif args.case == "ensemble":
             run_ensemble(args, rank, world, local_rank)
+        elif args.case == "unet":
+            run_unet(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -103,7 +103,8 @@ typedef struct cadmas_params {
   /* Initial guess of the pressure solve (no counterpart in the reference,
      which always starts from PT = 0, vf_vpsol.f:52-58):
        0  PT = 0;
-       1  the previous step's solution (0 on cells with INDC = -1 now).
+       1  the previous step's solution (0 on cells with INDC = -1 now);
+       2  the learned guess of cadmas_set_warm_net (below).
      The stopping test is unchanged (|M^-1 r| against |M^-1 b| for
      solver 0), so the result meets the same tolerance.                  */
   int    warm_start;
@@ -275,10 +276,41 @@ int cadmas_unet_destroy(cadmas_unet *net);
 int cadmas_unet_set_params(cadmas_unet *net, const float *params);
 int cadmas_unet_get_params(cadmas_unet *net, float *params);
 int cadmas_unet_forward(cadmas_unet *net, const float *x, float *y);
+/* Mean device time (CUDA events on the network's stream) of reps forwards
+   of the input already on the device (from the last _forward).        */
+int cadmas_unet_time_forward(cadmas_unet *net, int reps, float *ms);
 int cadmas_unet_grad(cadmas_unet *net, const float *x, const float *t, const float *m, float *loss,
                      float *grad);
 int cadmas_unet_train_step(cadmas_unet *net, const float *x, const float *t, const float *m, float lr,
                            float *loss);
+/* The loss of the learned guess: w_mse * |m (y - t)|^2 / n + w_res *
+   |m (b - c A (m y))|^2 / n, n = sum(m), with b the input's channel 0 and A the
+   sample's pressure system a7 ([batch][nz][ny][nx][7] FP32: AD, ALI, ALJ,
+   ALK, AUI, AUJ, AUK as VF_MZAX applies them) in the network's volume.
+   update != 0: one Adam step; grad (NULL skipped): the gradient.        */
+int cadmas_unet_train_sys(cadmas_unet *net, const float *x, const float *t, const float *m, const float *a7,
+                          float c, float w_mse, float w_res, float lr, int update, float *loss, float *grad);
+
+/* The learned initial guess of the pressure solve (params.warm_start = 2):
+   a network with the given parameters (cadmas_unet_param_count values) is
+   run before each solve on (BB / s, F, GGV, INDC != -1), s the RMS of BB
+   over computed cells, and PT0 = s * out_scale * output.  PT0 is
+   dropped for PT = 0
+   (the reference's start, vf_vpsol.f:52-58) unless |BB - A PT0|_2 <
+   |BB|_2.  The solve's stopping test is unchanged.  Without a network
+   loaded, warm_start 2 starts from PT = 0.  cadmas_warm_stats: guesses
+   kept and dropped so far.                                             */
+int cadmas_set_warm_net(cadmas_handle *h, const float *params, double out_scale);
+int cadmas_warm_stats(cadmas_handle *h, long long *kept, long long *dropped);
+/* The right-hand side BB and the solution PT of the last pressure solve
+   ((NUMI,NUMJ,NUMK) column-major host arrays, NULL skipped): the training
+   pairs of the learned guess.                                          */
+int cadmas_get_solve(cadmas_handle *h, double *bb, double *pt);
+/* The coefficients AD, ALI, ALJ, ALK, AUI, AUJ, AUK of the last pressure
+   system (VF_VPCOEF), valid between cadmas_v1cal and cadmas_f1cal (the
+   arrays are the step's work space afterwards).                        */
+int cadmas_get_system(cadmas_handle *h, double *ad, double *ali, double *alj, double *alk, double *aui,
+                      double *auj, double *auk);
 
 /* ---- restart file (*.rsl / *.res) and list file ----------------------
    The restart file of the reference, byte for byte: a Fortran unformatted
@@ -445,7 +477,8 @@ long long cadmas_kernel_launches(void);
 #define CADMAS_STAGE_FBC      11  /* F1CAL boundary rules, BSPPFL             */
 #define CADMAS_STAGE_TURB     12  /* k-epsilon: VF_K1CAL and the updates after
                                      F1CAL (LEQK != 0)                       */
-#define CADMAS_NSTAGES        13
+#define CADMAS_STAGE_WARM     13  /* learned initial guess (warm_start 2)      */
+#define CADMAS_NSTAGES        14
 int cadmas_stage_timers(cadmas_handle *h, int enable, double *ms, long long *count, int n);
 
 const char *cadmas_strerror(int status);

@@ -101,13 +101,16 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_set_drop", "cadmas_restart_create", "cadmas_restart_append", "cadmas_restart_load",
             "cadmas_list_step", "cadmas_cdtcal", "cadmas_get_turb", "cadmas_set_turb",
             "cadmas_unet_param_count", "cadmas_unet_create", "cadmas_unet_destroy", "cadmas_unet_set_params",
-            "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step"]
+            "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step",
+            "cadmas_set_warm_net", "cadmas_warm_stats", "cadmas_get_solve", "cadmas_get_system",
+            "cadmas_unet_train_sys", "cadmas_unet_time_forward"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
 TURB_FACES = ("bck", "bce")                # (NUMB)
 
-STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc", "turb"]
+STAGES = ["flux", "predict", "vpcoef", "dcmp", "fwd", "bwd", "dot", "vec", "modif", "vof", "flags", "fbc", "turb",
+          "warm"]
 
 
 class CadmasError(RuntimeError):
@@ -160,8 +163,17 @@ def load_library(path: pathlib.Path | None = None):
     lib.cadmas_unet_set_params.argtypes = [C.c_void_p, _fp]
     lib.cadmas_unet_get_params.argtypes = [C.c_void_p, _fp]
     lib.cadmas_unet_forward.argtypes = [C.c_void_p, _fp, _fp]
+    lib.cadmas_unet_time_forward.argtypes = [C.c_void_p, C.c_int, _fp]
     lib.cadmas_unet_grad.argtypes = [C.c_void_p, _fp, _fp, _fp, _fp, _fp]
     lib.cadmas_unet_train_step.argtypes = [C.c_void_p, _fp, _fp, _fp, C.c_float, _fp]
+    lib.cadmas_set_warm_net.argtypes = [C.c_void_p, _fp, C.c_double]
+    lib.cadmas_get_system.argtypes = [C.c_void_p] + [_dp] * 7
+    lib.cadmas_unet_train_sys.argtypes = [C.c_void_p, _fp, _fp, _fp, _fp, C.c_float, C.c_float, C.c_float,
+                                          C.c_float, C.c_int, _fp, _fp]
+    lib.cadmas_warm_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.cadmas_get_solve.argtypes = [C.c_void_p, _dp, _dp]
+    lib.cadmas_v1cal.argtypes = [C.c_void_p]
+    lib.cadmas_f1cal.argtypes = [C.c_void_p]
     lib.cadmas_set_turb.argtypes = [C.c_void_p] + [_dp] * 4
     lib.cadmas_init_state.argtypes = [C.c_void_p, C.c_int]
     lib.cadmas_step.argtypes = [C.c_void_p, C.c_double]
@@ -325,12 +337,29 @@ class UNet:
         _check(self.lib, self.lib.cadmas_unet_forward(self.h, _fptr(x), _fptr(y)))
         return y
 
+    def time_forward(self, reps=5):
+        """Mean device milliseconds of a forward of the resident input."""
+        ms = C.c_float()
+        _check(self.lib, self.lib.cadmas_unet_time_forward(self.h, int(reps), C.byref(ms)))
+        return ms.value
+
     def grad(self, x, t, m):
         """(loss, gradient over the parameters) of the masked MSE."""
         x, t, m = _f32(x), _f32(t), _f32(m)
         loss = C.c_float()
         g = np.zeros(self.nparam, np.float32)
         _check(self.lib, self.lib.cadmas_unet_grad(self.h, _fptr(x), _fptr(t), _fptr(m), C.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def train_sys(self, x, t, m, a7, c=1.0, w_mse=1.0, w_res=1.0, lr=1.0e-3, update=True, want_grad=False):
+        """MSE plus residual loss against the samples' systems a7; (loss,
+        gradient or None)."""
+        x, t, m, a7 = _f32(x), _f32(t), _f32(m), _f32(a7)
+        loss = C.c_float()
+        g = np.zeros(self.nparam, np.float32) if want_grad else None
+        _check(self.lib, self.lib.cadmas_unet_train_sys(self.h, _fptr(x), _fptr(t), _fptr(m), _fptr(a7), float(c),
+                                                        float(w_mse), float(w_res), float(lr), int(update),
+                                                        C.byref(loss), _fptr(g)))
         return loss.value, g
 
     def train_step(self, x, t, m, lr=1.0e-3):
@@ -422,6 +451,40 @@ class Tank:
     def set_drop(self, arrs):
         keep = {n: np.ascontiguousarray(arrs[n], dtype=np.float64) for n in DROP_ARRAYS}
         _check(self.lib, self.lib.cadmas_set_drop(self.h, *(_dptr(keep[n]) for n in DROP_ARRAYS)))
+
+    def set_warm_net(self, params, out_scale=1.0):
+        """Load the learned guess's network (used with warm_start=2)."""
+        p = _f32(params)
+        _check(self.lib, self.lib.cadmas_set_warm_net(self.h, _fptr(p), float(out_scale)))
+
+    def get_system(self):
+        """The last pressure system {ad, ali, alj, alk, aui, auj, auk}; call
+        between v1cal() and f1cal()."""
+        c = self.case
+        names = ("ad", "ali", "alj", "alk", "aui", "auj", "auk")
+        arrs = {n: np.zeros((c.ni, c.nj, c.nk), order="F") for n in names}
+        _check(self.lib, self.lib.cadmas_get_system(self.h, *(_dptr(arrs[n]) for n in names)))
+        return arrs
+
+    def warm_stats(self):
+        """(kept, dropped) learned guesses so far."""
+        k, d = C.c_longlong(), C.c_longlong()
+        _check(self.lib, self.lib.cadmas_warm_stats(self.h, C.byref(k), C.byref(d)))
+        return k.value, d.value
+
+    def get_solve(self):
+        """(BB, PT) of the last pressure solve, (ni, nj, nk) Fortran order."""
+        c = self.case
+        bb = np.zeros((c.ni, c.nj, c.nk), order="F")
+        pt = np.zeros((c.ni, c.nj, c.nk), order="F")
+        _check(self.lib, self.lib.cadmas_get_solve(self.h, _dptr(bb), _dptr(pt)))
+        return bb, pt
+
+    def v1cal(self):
+        _check(self.lib, self.lib.cadmas_v1cal(self.h))
+
+    def f1cal(self):
+        _check(self.lib, self.lib.cadmas_f1cal(self.h))
 
     def get_turb(self):
         """The k-epsilon state {ak, ae, anut, anu} (flat, cells) and {bck, bce}."""

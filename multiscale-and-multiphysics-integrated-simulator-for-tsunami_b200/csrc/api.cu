@@ -158,6 +158,11 @@ struct cadmas_handle {
   double *ak = nullptr, *ae_k = nullptr, *ak2 = nullptr, *ae2 = nullptr, *anut = nullptr;
   double *bck = nullptr, *bce = nullptr, *bck0 = nullptr, *bce0 = nullptr;
   int *indbk = nullptr, *indbe = nullptr;
+  // learned initial guess (warm_start 2): the network, two row buffers,
+  // [scale, |r|^2, |b|^2] and [kept, dropped, dropped now]
+  cadmas_unet *wnet = nullptr;
+  double *ws_rows = nullptr, *ws_scal = nullptr;
+  int *ws_cnt = nullptr;
   std::vector<double> zz2;  // ZZ(2,K) on the host, K = 1..NK
   std::vector<unsigned char> h_active;
   double tnow = 0.0, dtnow = 0.0;
@@ -588,6 +593,11 @@ static int do_v1cal(cadmas_handle *h) {
   // VF_VPSOL: PT = 0, solve (vf_vpsol.f:52-76)
   double *PT = h->wk[8];
   CK(cudaMemsetAsync(PT, 0, h->N * sizeof(double), s));
+  if (h->P.warm_start == 2 && h->wnet) {  // the learned PT0 in place of PT = 0
+    TB(CADMAS_STAGE_WARM);
+    launch_warm_guess(s, h->g, h->f, a, h->wnet, h->ws_rows, h->ws_rows + nrows(h), h->ws_scal, h->ws_cnt, PT);
+    TE();
+  }
   int iter;
   double bn, xn;
   const bool mixed = (h->P.solver == 1);
@@ -962,6 +972,9 @@ int cadmas_destroy(cadmas_handle *h) {
   for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
   for (double *q : {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww}) if (q) cudaFree(q);
   for (double *q : {h->ak, h->ae_k, h->ak2, h->ae2, h->anut, h->bck, h->bce, h->bck0, h->bce0}) if (q) cudaFree(q);
+  if (h->wnet) cadmas_unet_destroy(h->wnet);
+  for (double *q : {h->ws_rows, h->ws_scal}) if (q) cudaFree(q);
+  if (h->ws_cnt) cudaFree(h->ws_cnt);
   for (int *q : {h->indbk, h->indbe}) if (q) cudaFree(q);
   for (float *q : {h->Sf.sys, h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->y2f})
     if (q) cudaFree(q);
@@ -1436,6 +1449,54 @@ int cadmas_set_turb(cadmas_handle *h, const double *ak, const double *ae, const 
   }
   ke_nut(h);  // vf_ir1inp.f:339-340
   CK(cudaStreamSynchronize(s));
+  return CADMAS_OK;
+}
+
+int cadmas_set_warm_net(cadmas_handle *h, const float *params, double out_scale) {
+  if (!h || !params || !(out_scale > 0.0)) return CADMAS_EINVAL;
+  if (!h->wnet) {
+    const int X = (h->g.NI + 3) & ~3, Y = (h->g.NJ + 3) & ~3, Z = (h->g.NK + 3) & ~3;
+    int rc = unet_new(X, Y, Z, 1, h->s, &h->wnet);
+    if (rc) return rc;
+    if (dalloc(&h->ws_rows, 2 * (size_t)nrows(h)) || dalloc(&h->ws_scal, 4) || dalloc(&h->ws_cnt, 4))
+      return CADMAS_ENOMEM;
+    CK(cudaMemsetAsync(h->ws_cnt, 0, 4 * sizeof(int), h->s));
+  }
+  // scal = [s, |r|^2, |b|^2, output scale]
+  CK(cudaMemcpyAsync(h->ws_scal + 3, &out_scale, sizeof(double), cudaMemcpyHostToDevice, h->s));
+  return cadmas_unet_set_params(h->wnet, params);
+}
+
+int cadmas_warm_stats(cadmas_handle *h, long long *kept, long long *dropped) {
+  if (!h) return CADMAS_EINVAL;
+  int c[2] = {0, 0};
+  if (h->ws_cnt) {
+    CK(cudaMemcpyAsync(c, h->ws_cnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    const int e = unet_error_host(h->wnet);
+    if (e) return e;
+  }
+  if (kept) *kept = c[0];
+  if (dropped) *dropped = c[1];
+  return CADMAS_OK;
+}
+
+int cadmas_get_system(cadmas_handle *h, double *ad, double *ali, double *alj, double *alk, double *aui,
+                      double *auj, double *auk) {
+  if (!h) return CADMAS_EINVAL;
+  double *out[7] = {ad, ali, alj, alk, aui, auj, auk};
+  for (int k = 0; k < 7; ++k)
+    if (out[k]) CK(cudaMemcpyAsync(out[k], h->wk[k], h->N * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
+  return CADMAS_OK;
+}
+
+int cadmas_get_solve(cadmas_handle *h, double *bb, double *pt) {
+  if (!h) return CADMAS_EINVAL;
+  const size_t b8 = h->N * sizeof(double);
+  if (bb) CK(cudaMemcpyAsync(bb, h->wk[7], b8, cudaMemcpyDeviceToHost, h->s));
+  if (pt) CK(cudaMemcpyAsync(pt, h->wk[8], b8, cudaMemcpyDeviceToHost, h->s));
+  CK(cudaStreamSynchronize(h->s));
   return CADMAS_OK;
 }
 

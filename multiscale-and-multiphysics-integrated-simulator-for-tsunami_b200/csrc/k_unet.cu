@@ -114,10 +114,11 @@ __global__ void __launch_bounds__(128) k_conv(Vol g, const bf16 *__restrict__ X,
       if (nv >= 0) q = *reinterpret_cast<const uint4 *>(X + nv * Cin + c8 * 8);
       *reinterpret_cast<uint4 *>(As[s] + umma::kmajor_offset(CONV_M, tid, c8 * 8)) = q;
     }
-    // B: the tap's N x KC weights
+    // B: the tap's N x KC weights; consecutive threads take consecutive
+    // rows n, whose 16-byte chunks are adjacent in the core matrices
     const int nq = N * (KC / 8);
     for (int q = tid; q < nq; q += 128) {
-      const int n = q / (KC / 8), c8 = q % (KC / 8);
+      const int n = q % N, c8 = q / N;
       const uint4 w = *reinterpret_cast<const uint4 *>(W + ((long long)n * 27 + t) * Cin + c8 * 8);
       *reinterpret_cast<uint4 *>(Bs[s] + umma::kmajor_offset(N, n, c8 * 8)) = w;
     }
@@ -447,6 +448,59 @@ __global__ void k_head_bwd_par(long long V, const float *dy, const bf16 *A, int 
   part[(long long)blockIdx.x * (C + 1) + c] = s;
 }
 
+// ---------------------------------------------------- residual loss
+// The pressure system of each sample in the network's volume: per voxel
+// the 7 coefficients (AD, ALI, ALJ, ALK, AUI, AUJ, AUK, FP32) of VF_MZAX's
+// row (vf_mzax.f:42-56), b = the input's channel 0 (BB/s).  With the output
+// y, taken as 0 off the counted cells as the solver's guess is, and the
+// fixed scale c: r = m (b - c A (m y)); loss |r|^2 / sum(m).
+__device__ __forceinline__ float vget(const Vol &g, const float *a, const float *Mk, int x, int y, int z, int b,
+                                      int dx, int dy, int dz) {
+  const long long v = nbr(g, x, y, z, b, dx, dy, dz);
+  return v >= 0 ? a[v] * Mk[v] : 0.0f;
+}
+__global__ void k_res_fwd(Vol g, const float *Yo, const float *A7, const float *X4, const float *Mk, float c,
+                          float *R, float *lpart) {
+  __shared__ float red[256];
+  const long long v = (long long)blockIdx.x * 256 + threadIdx.x;
+  float l = 0.0f;
+  if (v < g.n()) {
+    int x, y, z, b;
+    decomp(g, v, x, y, z, b);
+    const float *a = A7 + 7 * v;
+    const float ay = a[0] * Yo[v] * Mk[v] + a[1] * vget(g, Yo, Mk, x, y, z, b, -1, 0, 0) +
+                     a[2] * vget(g, Yo, Mk, x, y, z, b, 0, -1, 0) + a[3] * vget(g, Yo, Mk, x, y, z, b, 0, 0, -1) +
+                     a[4] * vget(g, Yo, Mk, x, y, z, b, 1, 0, 0) + a[5] * vget(g, Yo, Mk, x, y, z, b, 0, 1, 0) +
+                     a[6] * vget(g, Yo, Mk, x, y, z, b, 0, 0, 1);
+    const float r = Mk[v] * (X4[4 * v] - c * ay);
+    R[v] = r;
+    l = r * r;
+  }
+  red[threadIdx.x] = l;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) lpart[blockIdx.x] = red[0];
+}
+// dy += w * d(|r|^2 / n)/dy = -2 w c / n * m[v] (A^T r)[v]; (A^T r)[v] =
+// AD[v] r[v] + the coefficients of the neighbours' rows that point at v
+__global__ void k_res_bwd(Vol g, const float *A7, const float *R, const float *Mk, float scale, float *dy) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= g.n()) return;
+  int x, y, z, b;
+  decomp(g, v, x, y, z, b);
+  auto term = [&](int dx, int dyy, int dz, int k) {
+    const long long u = nbr(g, x, y, z, b, dx, dyy, dz);
+    return u >= 0 ? A7[7 * u + k] * R[u] : 0.0f;
+  };
+  // row u = v+1 holds ALI (index 1) toward v, row v-1 holds AUI (4) ...
+  const float atr = A7[7 * v] * R[v] + term(1, 0, 0, 1) + term(0, 1, 0, 2) + term(0, 0, 1, 3) + term(-1, 0, 0, 4) +
+                    term(0, -1, 0, 5) + term(0, 0, -1, 6);
+  dy[v] += scale * Mk[v] * atr;
+}
+
 // -------------------------------------------------------- Adam, casts
 // FP32 master p, moments m, v; step t (1-based); then the BF16 copy
 __global__ void k_adam(long long n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2,
@@ -573,6 +627,18 @@ void launch_head_bwd(cudaStream_t s, long long V, const float *dy, const void *a
   k_head_bwd_act<<<nb(V * C, 256), 256, 0, s>>>(V, dy, (const bf16 *)a, C, wh, (bf16 *)da);
   k_head_bwd_par<<<nb(V, 1024), 32, 0, s>>>(V, dy, (const bf16 *)a, C, part);
   count_launch(2);
+}
+void launch_res_fwd(cudaStream_t s, int X, int Y, int Z, int B, const float *y, const float *a7, const float *x4,
+                    const float *m, float c, float *r, float *lpart) {
+  const Vol g{X, Y, Z, B};
+  k_res_fwd<<<nb(g.n(), 256), 256, 0, s>>>(g, y, a7, x4, m, c, r, lpart);
+  count_launch();
+}
+void launch_res_bwd(cudaStream_t s, int X, int Y, int Z, int B, const float *a7, const float *r, const float *m,
+                    float scale, float *dy) {
+  const Vol g{X, Y, Z, B};
+  k_res_bwd<<<nb(g.n(), 256), 256, 0, s>>>(g, a7, r, m, scale, dy);
+  count_launch();
 }
 void launch_adam(cudaStream_t s, long long n, float *p, const float *g, float *m, float *v, float lr, float b1,
                  float b2, float eps, float c1, float c2) {

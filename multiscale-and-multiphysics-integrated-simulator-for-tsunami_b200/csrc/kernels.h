@@ -281,7 +281,23 @@ void launch_wcast(cudaStream_t s, const float *w, int Cin, int Cout, void *wf, v
 void launch_f32_to_bf16(cudaStream_t s, long long n, const float *a, void *b);
 void launch_fill_bf16(cudaStream_t s, long long n, void *a);
 void launch_pack_in(cudaStream_t s, long long V, const float *x4, void *x16);
+void launch_res_fwd(cudaStream_t s, int X, int Y, int Z, int B, const float *y, const float *a7, const float *x4,
+                    const float *m, float c, float *r, float *lpart);
+void launch_res_bwd(cudaStream_t s, int X, int Y, int Z, int B, const float *a7, const float *r, const float *m,
+                    float scale, float *dy);
 void launch_bias_reduce(cudaStream_t s, const float *part, int n, int C, float *out);
+// the network as a part of a solver handle (unet.cu): created on the
+// handle's stream; the warm-start glue (warmstart.cu) fills its FP32
+// input (4 channels per voxel), runs it and reads its output
+int unet_new(int nx, int ny, int nz, int batch, cudaStream_t stream, cadmas_unet **out);
+void unet_dims(const cadmas_unet *n, int &X, int &Y, int &Z);
+float *unet_input(cadmas_unet *n);
+const float *unet_output(const cadmas_unet *n);
+const int *unet_error(const cadmas_unet *n);
+void unet_run_forward(cadmas_unet *n);
+int unet_error_host(cadmas_unet *n);
+void launch_warm_guess(cudaStream_t s, const Geo &g, const Fld &f, const SysPtr &a, cadmas_unet *net, double *rows0,
+                       double *rows1, double *scal, int *cnt, double *PT);
 // k-epsilon (k_keps.cu): VF_K1CAL into akn/aen; VF_BSSS (+ VF_CNUT0 and
 // VF_CNU00 with nut); VF_BWKE; the k, e, ANUT, ANU of VF_CINIT
 void launch_kstep(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, const KeArrays &t,

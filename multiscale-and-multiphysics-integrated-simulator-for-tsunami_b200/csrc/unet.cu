@@ -56,6 +56,7 @@ int dmalloc(T **p, size_t n) {
 
 struct cadmas_unet {
   cudaStream_t s = nullptr;
+  bool own_stream = true;
   int X = 0, Y = 0, Z = 0, B = 0;
   long long V[3] = {0, 0, 0};
   float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
@@ -66,6 +67,7 @@ struct cadmas_unet {
   void *d[NL] = {}, *du2 = nullptr, *du1 = nullptr, *dp1 = nullptr, *dp2 = nullptr;
   float *x4 = nullptr, *y = nullptr, *t = nullptr, *mk = nullptr, *dy = nullptr;
   float *part = nullptr, *bpart = nullptr, *lpart = nullptr;
+  float *a7 = nullptr, *r = nullptr;  // pressure systems and residual (residual loss)
   size_t part_n = 0;
   long long slice = 8192;
   int *err = nullptr;
@@ -210,7 +212,7 @@ size_t cadmas_unet_param_count(void) { return TAB.n; }
 
 int cadmas_unet_destroy(cadmas_unet *n) {
   if (!n) return CADMAS_OK;
-  for (float *q : {n->p, n->g, n->m, n->v, n->x4, n->y, n->t, n->mk, n->dy, n->part, n->bpart, n->lpart})
+  for (float *q : {n->p, n->g, n->m, n->v, n->x4, n->y, n->t, n->mk, n->dy, n->part, n->bpart, n->lpart, n->a7, n->r})
     if (q) cudaFree(q);
   for (int l = 0; l < NL; ++l)
     for (void *q : {n->wf[l], n->wt[l], n->a[l], n->d[l]})
@@ -218,18 +220,33 @@ int cadmas_unet_destroy(cadmas_unet *n) {
   for (void *q : {n->xin, n->p1, n->p2, n->u2, n->u1, n->du2, n->du1, n->dp1, n->dp2})
     if (q) cudaFree(q);
   if (n->err) cudaFree(n->err);
-  if (n->s) cudaStreamDestroy(n->s);
+  if (n->s && n->own_stream) cudaStreamDestroy(n->s);
   delete n;
   return CADMAS_OK;
 }
 
 int cadmas_unet_create(int nx, int ny, int nz, int batch, cadmas_unet **out) {
+  return cadmas::unet_new(nx, ny, nz, batch, nullptr, out);
+}
+
+}  // extern "C"
+
+namespace cadmas {
+
+// A network on the given stream (its own stream when null).
+int unet_new(int nx, int ny, int nz, int batch, cudaStream_t stream, cadmas_unet **out) {
   if (!out || nx < 4 || ny < 4 || nz < 4 || batch < 1 || nx % 4 || ny % 4 || nz % 4) return CADMAS_EINVAL;
   if (!unet_kernels_configure()) return CADMAS_ECUDA;
   cadmas_unet *n = new cadmas_unet();
   n->X = nx; n->Y = ny; n->Z = nz; n->B = batch;
   for (int r = 0; r < 3; ++r) n->V[r] = (long long)(nx >> r) * (ny >> r) * (nz >> r) * batch;
-  int rc = cudaStreamCreateWithFlags(&n->s, cudaStreamNonBlocking) == cudaSuccess ? CADMAS_OK : CADMAS_ECUDA;
+  int rc = CADMAS_OK;
+  if (stream) {
+    n->s = stream;
+    n->own_stream = false;
+  } else if (cudaStreamCreateWithFlags(&n->s, cudaStreamNonBlocking) != cudaSuccess) {
+    rc = CADMAS_ECUDA;
+  }
   const size_t P = TAB.n;
 #define AL(ptr, cnt) if (!rc) rc = dmalloc(&(ptr), (cnt))
   AL(n->p, P); AL(n->g, P); AL(n->m, P); AL(n->v, P);
@@ -269,6 +286,17 @@ int cadmas_unet_create(int nx, int ny, int nz, int batch, cadmas_unet **out) {
   return CADMAS_OK;
 }
 
+void unet_dims(const cadmas_unet *n, int &X, int &Y, int &Z) { X = n->X; Y = n->Y; Z = n->Z; }
+float *unet_input(cadmas_unet *n) { return n->x4; }
+const float *unet_output(const cadmas_unet *n) { return n->y; }
+const int *unet_error(const cadmas_unet *n) { return n->err; }
+void unet_run_forward(cadmas_unet *n) { forward(n); }
+int unet_error_host(cadmas_unet *n) { return check(n); }
+
+}  // namespace cadmas
+
+extern "C" {
+
 int cadmas_unet_set_params(cadmas_unet *n, const float *p) {
   if (!n || !p) return CADMAS_EINVAL;
   if (cudaMemcpyAsync(n->p, p, TAB.n * sizeof(float), cudaMemcpyHostToDevice, n->s) != cudaSuccess)
@@ -297,6 +325,22 @@ int cadmas_unet_forward(cadmas_unet *n, const float *x, float *y) {
   return check(n);
 }
 
+int cadmas_unet_time_forward(cadmas_unet *n, int reps, float *ms) {
+  if (!n || reps < 1 || !ms) return CADMAS_EINVAL;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return CADMAS_ECUDA;
+  cudaEventRecord(e0, n->s);
+  for (int r = 0; r < reps; ++r) forward(n);
+  cudaEventRecord(e1, n->s);
+  int rc = check(n);
+  float t = 0.0f;
+  if (!rc && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) rc = CADMAS_ECUDA;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / reps;
+  return rc;
+}
+
 int cadmas_unet_grad(cadmas_unet *n, const float *x, const float *t, const float *m, float *loss, float *grad) {
   if (!n || !x || !t || !m || !loss) return CADMAS_EINVAL;
   int rc = upload(n, x, t, m);
@@ -307,6 +351,58 @@ int cadmas_unet_grad(cadmas_unet *n, const float *x, const float *t, const float
   backward(n);
   if (grad && cudaMemcpyAsync(grad, n->g, TAB.n * sizeof(float), cudaMemcpyDeviceToHost, n->s) != cudaSuccess)
     return CADMAS_ECUDA;
+  return check(n);
+}
+
+// Sum of the per-block loss partials of the last loss kernel, in order.
+static int lsum(cadmas_unet *n, double &out) {
+  const int nbk = (int)((n->V[0] + 255) / 256);
+  n->hl.resize((size_t)nbk);
+  if (cudaMemcpyAsync(n->hl.data(), n->lpart, nbk * sizeof(float), cudaMemcpyDeviceToHost, n->s) != cudaSuccess)
+    return CADMAS_ECUDA;
+  if (cudaStreamSynchronize(n->s) != cudaSuccess) return CADMAS_ECUDA;
+  out = 0.0;
+  for (float q : n->hl) out += q;
+  return CADMAS_OK;
+}
+
+int cadmas_unet_train_sys(cadmas_unet *n, const float *x, const float *t, const float *m, const float *a7, float c,
+                          float w_mse, float w_res, float lr, int update, float *loss, float *grad) {
+  if (!n || !x || !t || !m || !a7 || !loss || !(c > 0.0f)) return CADMAS_EINVAL;
+  const long long V = n->V[0];
+  if (!n->a7 && (dmalloc(&n->a7, (size_t)V * 7) || dmalloc(&n->r, (size_t)V))) return CADMAS_ENOMEM;
+  int rc = upload(n, x, t, m);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(n->a7, a7, V * 7 * sizeof(float), cudaMemcpyHostToDevice, n->s) != cudaSuccess)
+    return CADMAS_ECUDA;
+  forward(n);
+  // counted cells
+  std::vector<float> mh((size_t)V);
+  if (cudaMemcpyAsync(mh.data(), n->mk, V * sizeof(float), cudaMemcpyDeviceToHost, n->s) != cudaSuccess)
+    return CADMAS_ECUDA;
+  if (cudaStreamSynchronize(n->s) != cudaSuccess) return CADMAS_ECUDA;
+  double cnt = 0.0;
+  for (float q : mh) cnt += q;
+  const double inv = cnt > 0.0 ? 1.0 / cnt : 0.0;
+  // mean-square error of y against t, weighted by w_mse in the gradient
+  launch_mse(n->s, V, n->y, n->t, n->mk, (float)(inv * w_mse), n->dy, n->lpart);
+  double lm, lr2;
+  if ((rc = lsum(n, lm))) return rc;
+  // residual |m (b - c A y)|^2 / n, weighted by w_res
+  launch_res_fwd(n->s, n->X, n->Y, n->Z, n->B, n->y, n->a7, n->x4, n->mk, c, n->r, n->lpart);
+  if ((rc = lsum(n, lr2))) return rc;
+  launch_res_bwd(n->s, n->X, n->Y, n->Z, n->B, n->a7, n->r, n->mk, (float)(-2.0 * c * w_res * inv), n->dy);
+  *loss = (float)(w_mse * lm * inv + w_res * lr2 * inv);
+  backward(n);
+  if (grad && cudaMemcpyAsync(grad, n->g, TAB.n * sizeof(float), cudaMemcpyDeviceToHost, n->s) != cudaSuccess)
+    return CADMAS_ECUDA;
+  if (update) {
+    n->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)n->step), c2 = 1.0f - std::pow(b2, (float)n->step);
+    launch_adam(n->s, (long long)TAB.n, n->p, n->g, n->m, n->v, lr, b1, b2, 1.0e-8f, c1, c2);
+    cast_weights(n);
+  }
   return check(n);
 }
 

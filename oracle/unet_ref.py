@@ -139,15 +139,35 @@ def forward(p, x4, q=ident):
     return y, A
 
 
-def loss_grad(p, x4, t, m, q=ident):
-    """Masked mean-square loss and its gradient over the parameters."""
+def apply_sys(a7, f):
+    """A f with the 7 coefficients (AD, ALI, ALJ, ALK, AUI, AUJ, AUK) per
+    voxel, zero outside the volume (VF_MZAX)."""
+    s = lambda dz, dy, dx: _shift(f[..., None], dz, dy, dx)[..., 0]
+    return (a7[..., 0] * f + a7[..., 1] * s(0, 0, -1) + a7[..., 2] * s(0, -1, 0) + a7[..., 3] * s(-1, 0, 0) +
+            a7[..., 4] * s(0, 0, 1) + a7[..., 5] * s(0, 1, 0) + a7[..., 6] * s(1, 0, 0))
+
+
+def apply_sys_t(a7, r):
+    """A^T r for the same coefficients."""
+    s = lambda f, dz, dy, dx: _shift(f[..., None], dz, dy, dx)[..., 0]
+    return (a7[..., 0] * r + s(a7[..., 1] * r, 0, 0, 1) + s(a7[..., 2] * r, 0, 1, 0) + s(a7[..., 3] * r, 1, 0, 0) +
+            s(a7[..., 4] * r, 0, 0, -1) + s(a7[..., 5] * r, 0, -1, 0) + s(a7[..., 6] * r, -1, 0, 0))
+
+
+def loss_grad(p, x4, t, m, q=ident, a7=None, c=1.0, w_mse=1.0, w_res=0.0):
+    """w_mse |m (y - t)|^2 / n + w_res |m (b - c A (m y))|^2 / n (n = sum m,
+    b = x4[..., 0], A from a7) and its gradient over the parameters."""
     ws, wh, bh = unpack(p)
     wq = [q(W) for W, _ in ws]
     y, A = forward(p, x4, q)
     cnt = m.sum()
     e = (y - t) * m
-    loss = (e * e).sum() / cnt
-    dy = 2.0 * e / cnt
+    loss = w_mse * (e * e).sum() / cnt
+    dy = w_mse * 2.0 * e / cnt
+    if a7 is not None and w_res != 0.0:
+        r = m * (x4[..., 0] - c * apply_sys(a7, m * y))
+        loss += w_res * (r * r).sum() / cnt
+        dy += -2.0 * c * w_res / cnt * m * apply_sys_t(a7, r)
     g = np.zeros_like(p)
     g[HEAD_W:HEAD_B] = np.einsum("bzyx,bzyxc->c", dy, A["a9"])
     g[HEAD_B] = dy.sum()

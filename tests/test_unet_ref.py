@@ -50,3 +50,26 @@ def test_bf16_rounding():
     assert r[0] == 1.0 and r[1] == 1.0  # tie to even
     assert r[2] == 1.0 + 2 ** -7
     assert abs(r[3] + 3.140625) < 1e-12
+
+
+def test_residual_loss_gradient_matches_finite_differences():
+    p = R.he_init(4)
+    x, t, m = sample(5)
+    rng = np.random.default_rng(6)
+    a7 = rng.normal(size=x.shape[:4] + (7,))
+    a7[..., 0] += 6.0
+    kw = dict(a7=a7, c=0.7, w_mse=0.3, w_res=1.0)
+    loss, g = R.loss_grad(p, x, t, m, **kw)
+    h = 1e-6
+    for _ in range(3):
+        v = rng.normal(size=p.size)
+        v /= np.linalg.norm(v)
+        fd = (R.loss_grad(p + h * v, x, t, m, **kw)[0] - R.loss_grad(p - h * v, x, t, m, **kw)[0]) / (2 * h)
+        assert abs(fd - g @ v) <= 1e-6 * max(abs(fd), 1e-3 * abs(loss)), (fd, g @ v)
+
+
+def test_transposed_system_is_the_adjoint():
+    rng = np.random.default_rng(7)
+    a7 = rng.normal(size=(2, 4, 4, 8, 7))
+    f, r = rng.normal(size=(2, 4, 4, 8)), rng.normal(size=(2, 4, 4, 8))
+    assert abs((R.apply_sys(a7, f) * r).sum() - (f * R.apply_sys_t(a7, r)).sum()) < 1e-10
