@@ -478,7 +478,19 @@ def run_ensemble(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     cases = P.cases.ensemble_flumes(args.members, seed=1000 * rank, scale=args.scale)
-    tanks = [P.Tank(c, **params_for(args)) for c in cases]
+    tiles = [(args.ti, args.tj)] * len(cases)
+    tune_s = None
+    if args.autotune:
+        # block shapes per member from the tile autotuner (untimed; cached by grid size)
+        import importlib
+        at = importlib.import_module(P.__name__ + ".autotune")
+        cache = at.TileCache()
+        t0 = time.time()
+        base = {k: v for k, v in params_for(args).items() if k not in ("precond_ti", "precond_tj")}
+        tiles = [at.pick_tiles(c, cache=cache, **base) for c in cases]
+        tune_s = round(time.time() - t0, 1)
+    tanks = [P.Tank(c, **{**params_for(args), "precond_ti": ti, "precond_tj": tj}) for c, (ti, tj) in
+             zip(cases, tiles)]
     for t in tanks:
         t.init_state(True)
     cells = sum(c.interior_cells for c in cases)
@@ -515,11 +527,13 @@ def run_ensemble(args, rank, world, local_rank):
             "config": {"workload": f"ensemble of {args.members} independent porous wave flumes of uneven "
                                    f"size (nx U{{256..1024}}x{args.scale:g}, ny U{{16..64}}, nz U{{64..128}}, "
                                    f"wave makers, {'mixed' if args.solver == 'mixed' else 'plain FP64'} "
-                                   f"SMAC step, block-Jacobi MILU {args.ti}x{args.tj})",
+                                   f"SMAC step, block-Jacobi MILU "
+                                   f"{'blocks chosen per grid by the tile autotuner' if args.autotune else f'{args.ti}x{args.tj}'})",
                        "cells": cells, "members": args.members,
                        "sizes": [[c.ni - 2, c.nj - 2, c.nk - 2] for c in cases],
                        "sequential_value": cells * args.steps / (t_seq / 1e3) / 1e6,
                        "mean_bicgstab_iters": statistics.mean(iters),
+                       **({"tiles": [list(t) for t in tiles], "autotune_s": tune_s} if args.autotune else {}),
                        "parallelism": f"{args.members} streams side by side x{world} replicas"},
             "gpu_launches": launches, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -539,6 +553,8 @@ def main():
     ap.add_argument("--split", type=int, choices=[1, 2], default=1,
                     help="2: each preconditioner block swept by a cluster of two thread blocks")
     ap.add_argument("--members", type=int, default=8, help="ensemble members (--case ensemble)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="--case ensemble: preconditioner block shape per member by the tile autotuner")
     ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
     ap.add_argument("--case", choices=["flume", "beach", "ensemble", "unet"], default="flume",
                     help="flume: 512x32x96 porous wave flume (default); beach: 1024x128x128 solitary "
