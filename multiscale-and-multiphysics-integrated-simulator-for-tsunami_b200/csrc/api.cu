@@ -13,6 +13,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -666,6 +668,20 @@ static void do_kpost(cadmas_handle *h) {
   launch_bwke(s, h->g, h->f, ke_arrays(h), h->dint);
   launch_bwuwt(s, h->g, h->f);
   TE();
+}
+
+// ------------------------------------------ kernel shared-memory limits
+void cadmas::raise_dynamic_smem(const void *kern, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> cur;  // (device, kernel) -> limit set
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t &c = cur[{dev, kern}];
+  if (bytes > c) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    c = bytes;
+  }
 }
 
 static int do_f1cal(cadmas_handle *h) {

@@ -19,6 +19,7 @@
 // registers and finishes that cell -- its F and its means -- right after
 // the next step: the same terms added in the same order as the
 // reference's arrays, with no scratch arrays.
+#include <mutex>
 #include "cadmas_dev.cuh"
 #include "kernels.h"
 
@@ -271,7 +272,9 @@ void launch_fdropf(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
   int wpb = drop_x_warps(g);
   if (wpb == 0) wpb = 1;
   const size_t xsm = (size_t)g.NI * 12 * wpb;
-  cudaFuncSetAttribute(k_drop_line_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
+  // the limit only rises (handles of other grids may be stepped from other
+  // host threads at the same time)
+  raise_dynamic_smem((const void *)k_drop_line_x, xsm);
   const long long nx = (long long)(g.NJ - 2) * (g.NK - 2);
   const long long ny = (long long)(g.NI - 2) * (g.NK - 2), nz = (long long)(g.NI - 2) * (g.NJ - 2);
   for (int L = 1; L <= 2; ++L) {

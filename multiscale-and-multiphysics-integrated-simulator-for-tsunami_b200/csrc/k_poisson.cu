@@ -20,6 +20,7 @@
 // runs on NPI x NPJ MPI ranks (each rank factors and sweeps its own x-y
 // block; neighbour terms outside the block are coef*0*0 because the rank's
 // halo DD and coefficients are zero).
+#include <mutex>
 #include "cadmas_dev.cuh"
 #include "kernels.h"
 #include <algorithm>
@@ -1101,8 +1102,12 @@ static void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sme
   cudaLaunchKernelEx(&cfg, kern, ((KArgs)args)...);
   count_launch();
 }
+// The kernel's dynamic shared-memory limit, raised to the bytes of this
+// launch and never lowered: handles stepped from several host threads at
+// once (cadmas_step_ensemble) with different tile shapes then never lower
+// it under one another's launches.
 template <class K> static void set_smem(K kern, size_t bytes) {
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  raise_dynamic_smem((const void *)kern, bytes);
 }
 
 static inline dim3 skew_grid(const SkewGeo &q) { return dim3((unsigned)q.ntx, (unsigned)(q.nb / q.ntx)); }

@@ -9,6 +9,11 @@ namespace cadmas {
 // Kernels launched by this library in the process (cadmas_kernel_launches).
 extern std::atomic<long long> g_kernel_launches;
 inline void count_launch(long long n = 1) { g_kernel_launches.fetch_add(n, std::memory_order_relaxed); }
+// Raise the dynamic shared-memory limit of the kernel at `kern` (on the
+// current device) to at least `bytes`; it is never lowered, so handles
+// stepped from several host threads at once never take it away from one
+// another's launches.
+void raise_dynamic_smem(const void *kern, size_t bytes);
 
 // The eight arrays of the Poisson system, WK01..WK08 of VF_V1CAL.
 struct SysPtr {

@@ -298,3 +298,55 @@ def test_adaptive_time_step_bitwise(gpu_lib, pkg, orc, builder, kw, active):
         dt = dg
     assert limited > 0 or not active  # the collapsing dam's velocities limit DT
     assert_same(t.get_state(), o.get_state(), "after 10 adaptive steps")
+
+
+def test_solitary_beach_small_bitwise(gpu_lib, pkg, orc):
+    """Config 2's shape at small size: staircase beach, porous boxes and an
+    injected solitary wave (set as the initial state), 16x8 blocks."""
+    c = pkg.cases.solitary_beach(nx=128, ny=32, nz=48, x_toe=1.0, x0=0.6, amp=0.08, depth=0.3, nbox=6, seed=3,
+                                 dt=1.0e-3)
+    t = pkg.Tank(c, precond_ti=16, precond_tj=8)
+    o = orc.Oracle(c, sum_mode=orc.SUM_GPU, precond_ti=16, precond_tj=8)
+    init = pkg.initial_state(c)
+    t.set_state(init)
+    o.set_state(init)
+    t.init_state(c.hydrostatic)
+    o.init_state(c.hydrostatic)
+    for n in range(1, 13):
+        t.step(c.dt)
+        o.step(c.dt)
+        if n % 4 == 0:
+            assert_same(t.get_state(), o.get_state(), f"step {n}")
+
+
+def test_wave_maker_flume_with_turbulence_bitwise(gpu_lib, pkg, orc):
+    """k-epsilon in the porous flume driven by the wave maker."""
+    c = pkg.cases.porous_flume(nx=96, ny=4, nz=64, block=(1.2, 1.4, 0.6), sponge_width=0.4)
+    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5, ramp=1.0)
+    pkg.cases.turbulence(c, 1e-4, 1e-5)
+    t, o = run_pair(pkg, orc, c, 16, check_every=8)
+    gt, ot = t.get_turb(), o.get_turb()
+    for k in ("ak", "ae", "anut", "anu", "bck", "bce"):
+        assert gt[k].tobytes() == ot[k].tobytes(), k
+
+
+def test_ensemble_of_mixed_tile_shapes(gpu_lib, pkg):
+    """Handles of different grids and preconditioner block shapes stepped
+    together (cadmas_step_ensemble, one host thread each) give exactly what
+    each gives stepped alone."""
+    shapes = [(16, 16), (8, 8), (16, 8), (32, 8)]
+    mk = lambda: [pkg.cases.porous_flume(nx=96 + 32 * i, ny=16, nz=48, depth=0.3, block=(1.0, 1.3, 0.4),
+                                         sponge_width=0.4)
+                  for i in range(len(shapes))]
+    together = [pkg.Tank(c, precond_ti=ti, precond_tj=tj) for c, (ti, tj) in zip(mk(), shapes)]
+    alone = [pkg.Tank(c, precond_ti=ti, precond_tj=tj) for c, (ti, tj) in zip(mk(), shapes)]
+    for t in together + alone:
+        t.init_state(True)
+    for _ in range(6):
+        pkg.step_ensemble(together)
+        for t in alone:
+            t.step()
+    for a, b in zip(together, alone):
+        sa, sb = a.get_state(), b.get_state()
+        for k in ("uu", "pp", "ff", "nf"):
+            assert sa[k].tobytes() == sb[k].tobytes(), k
