@@ -388,6 +388,26 @@ int cadmas_step_ensemble(cadmas_handle **h, int n, const double *dt, int *status
    Sides and tables persist until cadmas_destroy. */
 int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *tab);
 
+/* ---- open (radiation) boundary (MODEL OPEN-BC, vf_iimdl.f:176-213) ----
+   Side o->side radiates with the phase speed C = L/T of the linear wave of
+   period T in still-water depth D (VF_COMAK0, vf_csetup.f:128-143).  Its
+   faces are those of INDB with INDB(3,L) = 7 on that side; VF_BWUWN
+   blends their values toward the interior each step (vf_bwuwn.f:481-598).
+   A side is either a wave maker or open ('DEFINED DOUBLY' otherwise).     */
+typedef struct cadmas_open_bc {
+  int side;              /* JD: 1 X-, 2 X+, 3 Y-, 4 Y+                      */
+  int pad;
+  double depth;          /* BCTYP(1,JD) still-water depth D (> 0)            */
+  double period;         /* BCTYP(3,JD) period T (> 0)                       */
+} cadmas_open_bc;
+
+int cadmas_set_open(cadmas_handle *h, const cadmas_open_bc *o);
+
+/* The phase speed C = BCTYP(6,JD) of an open side: the wave length of
+   VF_COMAK0 (Newton on the dispersion relation, vf_comak0.f:31-55) over
+   the period.  Host arithmetic only; needs no device. */
+int cadmas_open_speed(double depth, double period, double grav, double *c);
+
 /* ---- Fortran-callable step (drop-in for the two CALLs of the time loop) --
    Arguments by reference, as gfortran passes them.  The arrays are the
    caller's host arrays; they are copied in before and out after the step,

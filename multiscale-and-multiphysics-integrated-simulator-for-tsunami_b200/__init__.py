@@ -46,6 +46,10 @@ class WaveBC(C.Structure):
                 ("depth", C.c_double), ("period", C.c_double), ("ramp", C.c_double)]
 
 
+class OpenBC(C.Structure):
+    _fields_ = [("side", C.c_int), ("pad", C.c_int), ("depth", C.c_double), ("period", C.c_double)]
+
+
 def wave_structs(wave):
     """(WaveBC, WaveTable, keep-alive arrays) of a case's wave-maker dict
     (cases.wave_maker)."""
@@ -96,7 +100,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_set_state", "cadmas_get_state", "cadmas_init_state", "cadmas_step",
             "cadmas_set_time", "cadmas_v1cal", "cadmas_f1cal", "cadmas_divnorm", "cadmas_get_stats",
             "cadmas_sync", "vf_step_gpu_", "vf_v1cal_gpu_", "vf_f1cal_gpu_", "cadmas_m1bcgs_dev",
-            "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_step_ensemble",
+            "cadmas_strerror", "cadmas_divnorm_noalloc", "cadmas_set_wave", "cadmas_set_open", "cadmas_open_speed", "cadmas_step_ensemble",
             "cadmas_get_stream", "cadmas_kernel_launches", "cadmas_stage_timers", "cadmas_get_drop",
             "cadmas_set_drop", "cadmas_restart_create", "cadmas_restart_append", "cadmas_restart_load",
             "cadmas_list_step", "cadmas_cdtcal", "cadmas_get_turb", "cadmas_set_turb",
@@ -194,6 +198,8 @@ def load_library(path: pathlib.Path | None = None):
     vf.argtypes = [C.POINTER(C.c_void_p), _dp] + [_dp] * 5 + [_ip, _ip] + [_dp] * 5 + [_dp, _ip]
     lib.cadmas_divnorm_noalloc.argtypes = [C.POINTER(Dims)] + [C.c_void_p] * 11 + [_dp]
     lib.cadmas_set_wave.argtypes = [C.c_void_p, C.POINTER(WaveBC), C.POINTER(WaveTable)]
+    lib.cadmas_set_open.argtypes = [C.c_void_p, C.POINTER(OpenBC)]
+    lib.cadmas_open_speed.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
     lib.cadmas_step_ensemble.argtypes = [C.POINTER(C.c_void_p), C.c_int, _dp, _ip]
     if path is None:
         _lib = lib
@@ -396,7 +402,15 @@ class Tank:
         _check(self.lib, self.lib.cadmas_upload_static(self.h, C.byref(self._static)))
         if getattr(case, "wave", None):
             self.set_wave(case.wave)
+        for op in getattr(case, "open", None) or []:
+            self.set_open(op)
         self.set_state(initial_state(case))
+
+    def set_open(self, op):
+        """Open (radiation) side from a dict made by cases.open_boundary
+        (cadmas_set_open)."""
+        o = OpenBC(int(op["side"]), 0, float(op["depth"]), float(op["period"]))
+        _check(self.lib, self.lib.cadmas_set_open(self.h, C.byref(o)))
 
     def set_wave(self, wave):
         """Wave-maker side from a dict made by cases.wave_maker (cadmas_set_wave)."""
@@ -584,6 +598,14 @@ def divnorm_noalloc(dims, xx, yy, zz, ggx, ggy, ggz, uu, vv, ww, indc, stream=0,
     args = [C.c_void_p(int(a)) for a in (xx, yy, zz, ggx, ggy, ggz, uu, vv, ww, indc)]
     _check(lib, lib.cadmas_divnorm_noalloc(C.byref(d), *args, C.c_void_p(int(stream)), C.byref(v)))
     return v.value
+
+
+def open_speed(depth, period, grav=9.8, lib=None) -> float:
+    """Phase speed C = L/T of an open side (cadmas_open_speed; host only)."""
+    lib = lib or load_library()
+    c = C.c_double()
+    _check(lib, lib.cadmas_open_speed(float(depth), float(period), float(grav), C.byref(c)))
+    return c.value
 
 
 def step_ensemble(tanks, dts=None, lib=None):

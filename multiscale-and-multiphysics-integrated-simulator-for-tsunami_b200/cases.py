@@ -29,8 +29,8 @@ import numpy as np
 
 # Velocity/pressure boundary types INDB(3,L) and F boundary types INDB(4,L)
 # (vf_a1main.f:151-170).
-VP_SLIP, VP_NOSLIP, VP_FIXED, VP_FREE, VP_WAVE = 1, 2, 3, 4, 5
-F_FIXED, F_FREE, F_WAVE = 1, 2, 5
+VP_SLIP, VP_NOSLIP, VP_FIXED, VP_FREE, VP_WAVE, VP_OPEN = 1, 2, 3, 4, 5, 7
+F_FIXED, F_FREE, F_WAVE, F_OPEN = 1, 2, 5, 7
 
 
 def grid_metrics(coords: np.ndarray) -> np.ndarray:
@@ -98,6 +98,7 @@ class Case:
     bcf: np.ndarray = None
     params: dict = dataclasses.field(default_factory=dict)
     wave: dict = None          # wave-maker side (wave_maker), or None
+    open: list = None          # open (radiation) sides (open_boundary), or None
     dt: float = 1e-3
     hydrostatic: bool = True
 
@@ -688,6 +689,48 @@ def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: f
     first, last = 2, (c.nj - 1 if side <= 2 else c.ni - 1)
     c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp,
                   table=table if table is not None else first_order_wave_table(H, T, depth))
+    return c
+
+
+def open_boundary(c: Case, depth: float, T: float, side: int = 2) -> Case:
+    """Make side `side` (1 X-, 2 X+, 3 Y-, 4 Y+) an open (radiation)
+    boundary for waves of period T in still-water depth `depth` (MODEL
+    OPEN-BC, vf_iimdl.f:176-213): its domain-boundary faces get B.C. type 7
+    for velocity and F with zero values (vf_csetup.f:146-213)."""
+    for L in range(c.indb.shape[1]):
+        ijk, NS = int(c.indb[0, L]), int(c.indb[1, L])
+        if NS != side:
+            continue
+        i = (ijk - 1) % c.ni + 1
+        j = ((ijk - 1) // c.ni) % c.nj + 1
+        if (side == 1 and i == 2) or (side == 2 and i == c.ni) or (side == 3 and j == 2) or \
+                (side == 4 and j == c.nj):
+            c.indb[2, L] = VP_OPEN
+            c.indb[3, L] = F_OPEN
+            for a in (c.bcu, c.bcv, c.bcw, c.bcp, c.bcf):
+                if a is not None:
+                    a[L] = 0.0
+    c.open = (c.open or []) + [dict(side=side, depth=depth, period=T)]
+    return c
+
+
+def open_flume(nx=160, ny=4, nz=64, dx=0.02, dz=0.01, depth=0.4, H=0.06, T=1.2, seed=0,
+               y_open=False) -> Case:
+    """Wave flume with a wave maker at X- and a radiation outlet at X+ in
+    place of a damping zone, a developed wave train already in it and
+    seeded noise (Philox) on the velocities; `y_open` opens the Y+ side too."""
+    c = porous_flume(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, depth=depth,
+                     block=(0.6 * nx * dx, 0.6 * nx * dx + 0.2, depth + H), gamma=0.5)
+    c.params.update(idamp=[-1, -1, -1, -1])  # no damping zone
+    linear_wave_initial(c, H, T, depth)
+    rng = np.random.Generator(np.random.Philox(seed))
+    for a in (c.uu, c.vv, c.ww):
+        a += rng.normal(0.0, 0.002, a.shape) * (c.ff > 0.0)
+    wave_maker(c, H, T, depth, side=1)
+    open_boundary(c, depth, T, side=2)
+    if y_open:
+        open_boundary(c, depth, T, side=4)
+    c.name = "open_flume"
     return c
 
 

@@ -178,6 +178,12 @@ struct cadmas_handle {
     int first = 0, last = 0;
     double d = 0.0, t = 0.0, a = 0.0;
   } wave[4];
+  // open (radiation) boundary: sides JD = 1..4 and their phase speed C
+  struct OpenSide {
+    bool on = false;
+    double c = 0.0;
+  } open[4];
+  long long n_open_faces = 0;  // faces with INDB(3,L) = 7
   int mtbtyp = 0, mtbnow = 0;  // MTBTYP, MTBNOW (persists between calls, vf_a2dflt.f:114)
   double dmtbt0 = 0.0;
   std::vector<double> wtt, whh;  // DMTBTT, DMTBHH (host)
@@ -286,6 +292,24 @@ static int wave_bc(cadmas_handle *h) {
     w.sb = (jd == 2) ? 1.0 : (jd == 3 ? -1.0 : 0.0);
     w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
     launch_wave(h->s, h->g, h->f, w, h->dint);
+  }
+  return CADMAS_OK;
+}
+
+// Open (radiation) part of VF_BWUWN (vf_bwuwn.f:481-598): the phase speed
+// of each open side was fixed by cadmas_set_open; the faces are set on the
+// device (k_open) from the velocities ub, vb, wb.
+static int open_bc(cadmas_handle *h, const double *ub, const double *vb, const double *wb) {
+  bool any = false;
+  for (int jd = 0; jd < 4; ++jd) {
+    if (!h->open[jd].on) continue;
+    any = true;
+    const OpenDev o{jd + 1, h->nnow, h->open[jd].c, h->dtnow};
+    launch_open(h->s, h->g, h->f, o, ub, vb, wb, h->dint);
+  }
+  if (!any && h->n_open_faces > 0) {
+    g_last_error = "faces of type 7 (open boundary) but no side declared open (cadmas_set_open)";
+    return CADMAS_EINVAL;
   }
   return CADMAS_OK;
 }
@@ -588,6 +612,8 @@ static int do_v1cal(cadmas_handle *h) {
   TB(CADMAS_STAGE_MODIF);
   launch_bwuwn(s, h->g, h->f, h->dint);
   { const int rw = wave_bc(h); if (rw) return rw; }
+  // UB, VB, WB: the velocities of the step's start (vf_v1cal.f:125-142)
+  { const int ro = open_bc(h, h->vel[nxt ^ 1][0], h->vel[nxt ^ 1][1], h->vel[nxt ^ 1][2]); if (ro) return ro; }
   TE();
   // Poisson system (vf_v1cal.f:259-271)
   SysPtr a{h->wk[0], h->wk[1], h->wk[2], h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[7]};
@@ -1007,6 +1033,10 @@ int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave
     return CADMAS_EUNSUPPORTED;
   }
   if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
+  if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
+    g_last_error = "side already declared open";
+    return CADMAS_EINVAL;
+  }
   const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;  // vf_iimdl.f:101-106
   if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
   for (int i = 1; i < t->ntt; ++i) if (!(t->tt[i] >= t->tt[i - 1])) return CADMAS_EINVAL;
@@ -1031,6 +1061,42 @@ int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave
   cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
   ws.on = true; ws.first = w->first; ws.last = w->last;
   ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
+  return CADMAS_OK;
+}
+
+int cadmas_open_speed(double depth, double period, double grav, double *c) {
+  if (!c || !(depth > 0.0) || !(period > 0.0) || !(grav > 0.0)) return CADMAS_EINVAL;
+  // VF_COMAK0 (vf_comak0.f:24-55): x = k D from x = d coth(x),
+  // d = 4 pi^2 D / (g T^2), Newton from d (deep) or sqrt(d) (shallow)
+  const double PI = 3.141592653589794;  // VF_A0PRM.h
+  const int MI = 10;
+  const double EPS = 1.0e-10;
+  const double D = 4.0 * PI * PI * depth / grav / period / period;
+  double X = (D >= 1.0) ? D : std::sqrt(D);
+  for (int it = 1; it <= MI; ++it) {
+    const double EXPX = std::exp(X);
+    const double EXPXI = 1.0 / EXPX;
+    const double COTHX = (EXPX + EXPXI) / (EXPX - EXPXI);
+    const double DX = (X - D * COTHX) / (1.0 + D * (COTHX * COTHX - 1.0));
+    X = X - DX;
+    if (std::fabs(DX / X) <= EPS) break;
+  }
+  const double WLN = 2.0 * PI * depth / X;
+  *c = WLN / period;  // BCTYP(6,JD) = WLN/T (vf_csetup.f:143)
+  return std::isfinite(*c) ? CADMAS_OK : CADMAS_EINVAL;
+}
+
+int cadmas_set_open(cadmas_handle *h, const cadmas_open_bc *o) {
+  if (!h || !o || o->side < 1 || o->side > 4) return CADMAS_EINVAL;
+  if (h->wave[o->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
+    g_last_error = "side already declared a wave maker";
+    return CADMAS_EINVAL;
+  }
+  double c;
+  const int rc = cadmas_open_speed(o->depth, o->period, h->P.grz0, &c);
+  if (rc) return rc;
+  h->open[o->side - 1].on = true;
+  h->open[o->side - 1].c = c;
   return CADMAS_OK;
 }
 
@@ -1059,6 +1125,8 @@ int cadmas_upload_static(cadmas_handle *h, const cadmas_static *st) {
   CK(cudaMemcpyAsync(h->indy, st->indy, b4, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(h->indz, st->indz, b4, cudaMemcpyHostToDevice, s));
   if (h->g.NB > 0) CK(cudaMemcpyAsync(h->indb, st->indb, 4 * h->g.NB * sizeof(int), cudaMemcpyHostToDevice, s));
+  h->n_open_faces = 0;
+  for (long long L = 0; L < h->g.NB; ++L) h->n_open_faces += (st->indb[4 * L + 2] == 7);
   if (h->P.leqk != 0 && h->g.NB > 0) {  // k-epsilon boundaries (vf_iiboun.f:250-330)
     if (!st->indbk || !st->indbe || !st->bck || !st->bce) return CADMAS_EINVAL;
     const size_t nb = (size_t)h->g.NB;
@@ -1404,9 +1472,15 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
     CK(cudaMemcpyAsync(h->f.pp, pp.data(), h->N * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
   }
-  // vf_cinit.f:388-394
+  // vf_cinit.f:376-394: the open boundary reads a copy of the present
+  // velocities as those of the previous step
+  const bool any_open = h->open[0].on || h->open[1].on || h->open[2].on || h->open[3].on;
+  if (any_open)
+    for (int c = 0; c < 3; ++c)
+      CK(cudaMemcpyAsync(h->wk[c], h->vel[h->cur][c], h->N * sizeof(double), cudaMemcpyDeviceToDevice, s));
   launch_bwuwn(s, h->g, h->f, h->dint);
   { const int rw = wave_bc(h); if (rw) return rw; }
+  { const int ro = open_bc(h, h->wk[0], h->wk[1], h->wk[2]); if (ro) return ro; }
   launch_bsuwt(s, h->g, h->f, h->p);
   launch_bsuwt2(s, h->g, h->f);
   launch_bsuwn3(s, h->g, h->f, h->p);

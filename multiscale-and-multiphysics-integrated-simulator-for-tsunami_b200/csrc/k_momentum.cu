@@ -583,7 +583,8 @@ __global__ void k_bwuwn(Geo g, Fld f, int *err) {
     // the per-face rule of vf_bwuwn.f:161-216 applies to MTBTYP 3 only,
     // which cadmas_set_wave does not accept
   } else if (IB == 7) {
-    atomicOr(err, ERR_UNSUP);
+    // open (radiation) faces: set by k_open after this pass
+    // (vf_bwuwn.f:234-235, 481-598)
   } else {
     atomicOr(err, ERR_PG);
   }
@@ -676,11 +677,97 @@ __global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
   }
 }
 
+// ------------------------------------------------- VF_BWUWN, open boundary
+// Radiation faces of one side (vf_bwuwn.f:481-598), one thread per
+// boundary line (J on the X sides, I on the Y sides), its faces in the
+// reference's K order.  A face next to a fluid cell blends its stored
+// value toward the interior of the step's start: the normal component
+// toward the face one cell inside with ALN = min(C DTNOW / DX, 1), the
+// tangential ones toward the cell-centre averages with ALT = min(2 ALN, 1)
+// (both 1 at NNOW = 0); a face next to any other cell gets zero.  Then the
+// faces of surface cells open downward (NF 5) or upward (NF 6) copy the
+// face below or above; the upward ones leave the normal velocity 0 on the
+// X sides and the copied value on the Y sides, as the reference does.
+__global__ void k_open(Geo g, Fld f, OpenDev o, const double *UB, const double *VB, const double *WB, int *err) {
+  const int n = 2 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int NI = g.NI, NJ = g.NJ, NK = g.NK;
+  const bool xs = (o.side <= 2);
+  if (n > (xs ? NJ - 1 : NI - 1)) return;
+  int I, J, IC, JC, I2, J2;
+  if (xs) {
+    J = n; JC = n; J2 = n;
+    I = (o.side == 1) ? 2 : NI;
+    IC = (o.side == 1) ? 2 : NI - 1;
+    I2 = (o.side == 1) ? 3 : IC;
+  } else {
+    I = n; IC = n; I2 = n;
+    J = (o.side == 3) ? 2 : NJ;
+    JC = (o.side == 3) ? 2 : NJ - 1;
+    J2 = (o.side == 3) ? 3 : JC;
+  }
+  double ALN = 1.0, ALT = 1.0;
+  if (o.nnow != 0) {
+    const double a = o.c * o.dtnow / (xs ? gx(g, 2, IC) : gy(g, 2, JC));
+    ALN = (a < 1.0) ? a : 1.0;
+    const double b = ALN * 2.0;
+    ALT = (b < 1.0) ? b : 1.0;
+  }
+  const int *ind = xs ? f.indx : f.indy;
+  for (int K = 2; K <= NK - 1; ++K) {
+    const long long c = cid(g, I, J, K);
+    const int L = ind[c];
+    if (L < 1) continue;
+    const long long cc = cid(g, IC, JC, K);
+    double &BU = f.bcu[L - 1], &BV = f.bcv[L - 1], &BW = f.bcw[L - 1];
+    if (f.nf[cc] == 0) {
+      const double WC = (WB[cc] + WB[cid(g, IC, JC, K + 1)]) * 0.5;
+      if (xs) {
+        const double VC = (VB[cc] + VB[cid(g, IC, JC + 1, K)]) * 0.5;
+        BU = (1.0 - ALN) * BU + ALN * UB[cid(g, I2, J, K)];
+        BV = (1.0 - ALT) * BV + ALT * VC;
+        BW = (1.0 - ALT) * BW + ALT * WC;
+        f.uu[c] = BU;
+      } else {
+        const double UC = (UB[cc] + UB[cid(g, IC + 1, JC, K)]) * 0.5;
+        BU = (1.0 - ALT) * BU + ALT * UC;
+        BV = (1.0 - ALN) * BV + ALN * VB[cid(g, I, J2, K)];
+        BW = (1.0 - ALT) * BW + ALT * WC;
+        f.vv[c] = BV;
+      }
+    } else {
+      BU = 0.0; BV = 0.0; BW = 0.0;
+      if (xs) f.uu[c] = 0.0;
+      else f.vv[c] = 0.0;
+    }
+  }
+  for (int K = 2; K <= NK - 1; ++K) {
+    const long long c = cid(g, I, J, K);
+    const int L = ind[c];
+    if (L < 1) continue;
+    const int NW = f.nf[cid(g, IC, JC, K)];
+    if (NW != 5 && NW != 6) continue;
+    const int L2 = ind[cid(g, I, J, NW == 5 ? K - 1 : K + 1)];
+    if (L2 < 1) { atomicOr(err, ERR_PG); return; }
+    f.bcu[L - 1] = f.bcu[L2 - 1];
+    f.bcv[L - 1] = f.bcv[L2 - 1];
+    f.bcw[L - 1] = f.bcw[L2 - 1];
+    if (xs) f.uu[c] = (NW == 5) ? f.bcu[L - 1] : 0.0;
+    else f.vv[c] = f.bcv[L - 1];
+  }
+}
+
 // ------------------------------------------------------------ launchers
 void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, int *err) {
   const int n = w.last - w.first + 1;
   if (n <= 0) return;
   k_wave<<<(n + 127) / 128, 128, 0, s>>>(g, f, w, err);
+  count_launch();
+}
+void launch_open(cudaStream_t s, const Geo &g, const Fld &f, const OpenDev &o, const double *ub,
+                 const double *vb, const double *wb, int *err) {
+  const int n = ((o.side <= 2) ? g.NJ : g.NI) - 2;
+  if (n <= 0) return;
+  k_open<<<(n + 127) / 128, 128, 0, s>>>(g, f, o, ub, vb, wb, err);
   count_launch();
 }
 void launch_flux(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl) {

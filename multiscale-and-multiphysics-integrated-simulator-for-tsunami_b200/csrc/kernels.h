@@ -169,6 +169,11 @@ enum FinMode { FIN_BNORM = 0, FIN_START = 1, FIN_STORE = 2, FIN_RELRES = 3,
                FIN_ALPHA = 10, FIN_OMEGA = 11, FIN_CONV = 12 };
 
 // Time-dependent part of one wave-maker side (host side of VF_BWUWN).
+struct OpenDev {
+  int side, nnow;   // JD and NNOW (0: full weights ALN = ALT = 1)
+  double c, dtnow;  // phase speed BCTYP(6,JD) and DTNOW
+};
+
 struct WaveDev {
   int side, first, last;  // JD and the range of boundary lines
   int mtbtyp, nzz, mtbnow;  // table type, MTBZZ, row MTBNOW (1-based)
@@ -187,6 +192,10 @@ void launch_predict(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, do
                     double *un, double *vn, double *wn);
 void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, int *err);
 void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, int *err);
+// Open (radiation) faces of one side; ub/vb/wb the velocities the blend
+// reads (the start of the step's, or a copy of the present ones at set-up)
+void launch_open(cudaStream_t s, const Geo &g, const Fld &f, const OpenDev &o, const double *ub,
+                 const double *vb, const double *wb, int *err);
 
 // k_poisson.cu
 void launch_vpcoef(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const SysPtr &a, int *err);

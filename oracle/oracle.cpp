@@ -347,6 +347,7 @@ struct orc_handle {
   // wave maker, matrix table (WAVE-BC ... FUNC MATRIX): IBCTYP/BCTYP of
   // the four sides and the table of /VF_AFILEI/ (vf_iimdl.f:49-106)
   struct Wave { int on = 0, l1 = 0, l2 = 0; double d = 0, t = 0, a = 0; } WV[4];
+  struct Open { int on = 0; double c = 0; } OP[4];  // IBCTYP(1,JD) = 2 and BCTYP(6,JD)
   int MTBTYP = 0, MTBNOW = 0;
   double DMTBT0 = 0;
   vd DMTBTT, DMTBHH, DMTBZZ, DMTBUN, DMTBUT;
@@ -1040,9 +1041,10 @@ struct orc_handle {
         }
   }
 
-  // VF_BWUWN  vf_bwuwn.f:93-160 (slip, no-slip, fixed, free; wave/open
-  // faces (IB=5,7) keep the values the caller set in BCU/BCV/BCW)
-  int bwuwn() {
+  // VF_BWUWN  vf_bwuwn.f:93-160 (slip, no-slip, fixed, free); wave and
+  // open faces (IB=5,7) by side afterwards (bwuwn_wave, bwuwn_open).
+  // UB, VB, WB are the velocities of the step's start.
+  int bwuwn(const vd &UB, const vd &VB, const vd &WB) {
     for (int L = 1; L <= NB; ++L) {
       int I, J, K;
       decode(IB_(1, L), I, J, K);
@@ -1072,12 +1074,105 @@ struct orc_handle {
       } else if (IB == 5) {
         // vf_bwuwn.f:161-216 acts for MTBTYP 3 only (not accepted here)
       } else if (IB == 7) {
-        return CADMAS_EUNSUPPORTED;
+        // vf_bwuwn.f:234-235: set below by side
       } else {
         return CADMAS_EPG;
       }
     }
-    return bwuwn_wave();
+    int rc = bwuwn_wave();
+    if (rc) return rc;
+    return bwuwn_open(UB, VB, WB);
+  }
+
+  // VF_BWUWN open-boundary part  vf_bwuwn.f:481-598 (IBCTYP(1,JD) = 2,
+  // one rank: IP = JP = 0 and the rank's range is the whole side)
+  int bwuwn_open(const vd &UB, const vd &VB, const vd &WB) {
+    bool any = false;
+    for (int JD = 1; JD <= 4; ++JD) {
+      if (!OP[JD - 1].on) continue;
+      any = true;
+      const double C = OP[JD - 1].c;
+      if (JD == 1 || JD == 2) {
+        int I, IC, I2;
+        if (JD == 1) { I = 2; IC = 2; I2 = 3; }
+        else { I = NI; IC = NI - 1; I2 = IC; }
+        double ALN, ALT;
+        if (NNOW == 0) { ALN = 1.0; ALT = 1.0; }
+        else { ALN = std::min(C * DTNOW / X_(2, IC), 1.0); ALT = std::min(ALN * 2.0, 1.0); }
+        for (int K = 2; K <= NK - 1; ++K)
+          for (int J = 2; J <= NJ - 1; ++J) {
+            const int L = INDX[id(I, J, K)];
+            if (L < 1) continue;
+            if (NF[id(IC, J, K)] == 0) {
+              const double VC = (VB[id(IC, J, K)] + VB[id(IC, J + 1, K)]) * 0.5;
+              const double WC = (WB[id(IC, J, K)] + WB[id(IC, J, K + 1)]) * 0.5;
+              BCU[L - 1] = (1.0 - ALN) * BCU[L - 1] + ALN * UB[id(I2, J, K)];
+              BCV[L - 1] = (1.0 - ALT) * BCV[L - 1] + ALT * VC;
+              BCW[L - 1] = (1.0 - ALT) * BCW[L - 1] + ALT * WC;
+              UU[id(I, J, K)] = BCU[L - 1];
+            } else {
+              BCU[L - 1] = 0.0; BCV[L - 1] = 0.0; BCW[L - 1] = 0.0;
+              UU[id(I, J, K)] = 0.0;
+            }
+          }
+        for (int K = 2; K <= NK - 1; ++K)
+          for (int J = 2; J <= NJ - 1; ++J) {
+            const int L = INDX[id(I, J, K)];
+            if (L < 1) continue;
+            const int NW = NF[id(IC, J, K)];
+            if (NW == 5) {
+              const int L2 = INDX[id(I, J, K - 1)];
+              if (L2 < 1) return CADMAS_EPG;
+              BCU[L - 1] = BCU[L2 - 1]; BCV[L - 1] = BCV[L2 - 1]; BCW[L - 1] = BCW[L2 - 1];
+              UU[id(I, J, K)] = BCU[L - 1];
+            } else if (NW == 6) {
+              const int L2 = INDX[id(I, J, K + 1)];
+              if (L2 < 1) return CADMAS_EPG;
+              BCU[L - 1] = BCU[L2 - 1]; BCV[L - 1] = BCV[L2 - 1]; BCW[L - 1] = BCW[L2 - 1];
+              UU[id(I, J, K)] = 0.0;
+            }
+          }
+      } else {
+        int J, JC, J2;
+        if (JD == 3) { J = 2; JC = 2; J2 = 3; }
+        else { J = NJ; JC = NJ - 1; J2 = JC; }
+        double ALN, ALT;
+        if (NNOW == 0) { ALN = 1.0; ALT = 1.0; }
+        else { ALN = std::min(C * DTNOW / Y_(2, JC), 1.0); ALT = std::min(ALN * 2.0, 1.0); }
+        for (int K = 2; K <= NK - 1; ++K)
+          for (int I = 2; I <= NI - 1; ++I) {
+            const int L = INDY[id(I, J, K)];
+            if (L < 1) continue;
+            if (NF[id(I, JC, K)] == 0) {
+              const double UC = (UB[id(I, JC, K)] + UB[id(I + 1, JC, K)]) * 0.5;
+              const double WC = (WB[id(I, JC, K)] + WB[id(I, JC, K + 1)]) * 0.5;
+              BCU[L - 1] = (1.0 - ALT) * BCU[L - 1] + ALT * UC;
+              BCV[L - 1] = (1.0 - ALN) * BCV[L - 1] + ALN * VB[id(I, J2, K)];
+              BCW[L - 1] = (1.0 - ALT) * BCW[L - 1] + ALT * WC;
+              VV[id(I, J, K)] = BCV[L - 1];
+            } else {
+              BCU[L - 1] = 0.0; BCV[L - 1] = 0.0; BCW[L - 1] = 0.0;
+              VV[id(I, J, K)] = 0.0;
+            }
+          }
+        for (int K = 2; K <= NK - 1; ++K)
+          for (int I = 2; I <= NI - 1; ++I) {
+            const int L = INDY[id(I, J, K)];
+            if (L < 1) continue;
+            const int NW = NF[id(I, JC, K)];
+            if (NW == 5 || NW == 6) {
+              const int L2 = INDY[id(I, J, NW == 5 ? K - 1 : K + 1)];
+              if (L2 < 1) return CADMAS_EPG;
+              BCU[L - 1] = BCU[L2 - 1]; BCV[L - 1] = BCV[L2 - 1]; BCW[L - 1] = BCW[L2 - 1];
+              VV[id(I, J, K)] = BCV[L - 1];
+            }
+          }
+      }
+    }
+    if (!any)
+      for (int L = 1; L <= NB; ++L)
+        if (IB_(3, L) == 7) return CADMAS_EINVAL;  // open faces on no open side
+    return CADMAS_OK;
   }
 
   // VF_CWMTB1  vf_cwmtb1.f:26-69
@@ -2891,7 +2986,7 @@ struct orc_handle {
     vflxdw(WK[9], WK[10], WK[11]);
     vgene(WK[4], WK[8], WK[12]);
     veuler(WK[1], WK[2], WK[3], WK[4], WK[5], WK[6], WK[7], WK[8], WK[9], WK[10], WK[11], WK[12]);
-    int rc = bwuwn();
+    int rc = bwuwn(WK[13], WK[14], WK[15]);
     if (rc) return rc;
     tmr[0] += T.stop();
     T.start();
@@ -3381,7 +3476,10 @@ int orc_init_state(orc_handle *h, int hydrostatic) {
           if (h->INDC[h->id(I, J, K)] != -1) h->PP[h->id(I, J, K)] = VAL;
     }
   }
-  rc = h->bwuwn();
+  {  // vf_cinit.f:376-390: the present velocities stand for the previous step's
+    const vd ub = h->UU, vb = h->VV, wb = h->WW;
+    rc = h->bwuwn(ub, vb, wb);
+  }
   if (rc) return rc;
   if (h->P.leqk != 0) h->kinit();  // vf_cinit.f:295-315, 359-364
   h->bsuwt(); h->bsuwt2(); h->bsuwn3(); h->bspp(); h->bwuwt(); h->bwpp();
@@ -3437,8 +3535,36 @@ int orc_get_poisson(orc_handle *h, int which, double *out) {
   return CADMAS_OK;
 }
 
+// VF_COMAK0  vf_comak0.f:24-55 with BCTYP(6,JD) = WLN/T (vf_csetup.f:139-143)
+int orc_open_speed(double depth, double period, double grav, double *c) {
+  if (!c || !(depth > 0.0) || !(period > 0.0) || !(grav > 0.0)) return CADMAS_EINVAL;
+  const double PI = 3.141592653589794;
+  const double D = 4.0 * PI * PI * depth / grav / period / period;
+  double X = D >= 1.0 ? D : std::sqrt(D);
+  for (int ITR = 1; ITR <= 10; ++ITR) {
+    const double EXPX = std::exp(X), EXPXI = 1.0 / EXPX;
+    const double COTHX = (EXPX + EXPXI) / (EXPX - EXPXI);
+    const double DX = (X - D * COTHX) / (1.0 + D * (COTHX * COTHX - 1.0));
+    X = X - DX;
+    if (std::fabs(DX / X) <= 1.0e-10) break;
+  }
+  *c = 2.0 * PI * depth / X / period;
+  return std::isfinite(*c) ? CADMAS_OK : CADMAS_EINVAL;
+}
+
+int orc_set_open(orc_handle *h, int side, double depth, double period) {
+  if (!h || side < 1 || side > 4 || h->WV[side - 1].on) return CADMAS_EINVAL;
+  double c;
+  const int rc = orc_open_speed(depth, period, h->P.grz0, &c);
+  if (rc) return rc;
+  h->OP[side - 1].on = 1;
+  h->OP[side - 1].c = c;
+  return CADMAS_OK;
+}
+
 int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
   if (!h || !w || !t || w->side < 1 || w->side > 4 || t->ntt < 2 || t->nzz < 2) return CADMAS_EINVAL;
+  if (h->OP[w->side - 1].on) return CADMAS_EINVAL;
   if (t->mtbtyp != 1 && t->mtbtyp != 2) return CADMAS_EUNSUPPORTED;
   h->DMTBTT.assign(t->tt, t->tt + t->ntt);
   h->DMTBHH.assign(t->hh, t->hh + t->ntt);

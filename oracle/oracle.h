@@ -54,6 +54,10 @@ int orc_m1bcgs(orc_handle *h, const double *ad, const double *ali,
 int orc_get_poisson(orc_handle *h, int which, double *out);
 /* Wave-maker side with its matrix table (as cadmas_set_wave). */
 int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t);
+/* Open (radiation) side JD with the phase speed of depth and period (as
+   cadmas_set_open); orc_open_speed is VF_COMAK0's C = L/T. */
+int orc_set_open(orc_handle *h, int side, double depth, double period);
+int orc_open_speed(double depth, double period, double grav, double *c);
 /* Seconds spent in the last orc_step by stage: [0] momentum predictor,
    [1] assembly, [2] solve, [3] correction+BC, [4] VOF+flags.              */
 int orc_get_timers(orc_handle *h, double *t5);

@@ -109,6 +109,9 @@ class Oracle:
             bc, tab, keep = P.wave_structs(case.wave)
             self.lib.orc_set_wave.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.WaveTable)]
             self._rc(self.lib.orc_set_wave(self.h, C.byref(bc), C.byref(tab)))
+        for op in getattr(case, "open", None) or []:
+            self.lib.orc_set_open.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+            self._rc(self.lib.orc_set_open(self.h, int(op["side"]), float(op["depth"]), float(op["period"])))
         self.set_state(P.initial_state(case))
 
     def _rc(self, rc):
@@ -240,6 +243,15 @@ def fslp(s, d, fval):
     aa, fb = C.c_double(), C.c_double()
     rc = _load_lib().orc_fslp(dim, sa, da, float(fval), C.byref(aa), C.byref(fb))
     return None if rc else (aa.value, fb.value)
+
+
+def open_speed(depth, period, grav=9.8):
+    """VF_COMAK0's wave length over the period (BCTYP(6,JD)), or None."""
+    c = C.c_double()
+    lib = _load_lib()
+    lib.orc_open_speed.argtypes = [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
+    rc = lib.orc_open_speed(float(depth), float(period), float(grav), C.byref(c))
+    return None if rc else c.value
 
 
 def croot3(a, b, c, d):

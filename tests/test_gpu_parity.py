@@ -154,6 +154,31 @@ def test_wave_maker_flume_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 24, check_every=8)
 
 
+def test_open_flume_bitwise(gpu_lib, pkg, orc):
+    """Wave maker at X- and a radiation outlet at X+ (MODEL OPEN-BC,
+    VF_BWUWN vf_bwuwn.f:481-598 in k_open) with a wave train and seeded
+    velocity noise in the flume: bit for bit."""
+    c = pkg.cases.open_flume()
+    run_pair(pkg, orc, c, 24, check_every=8)
+
+
+def test_open_flume_two_open_sides_tiles_bitwise(gpu_lib, pkg, orc):
+    """Open X+ and Y+ sides (the Y form of the blend), 16x8 blocks."""
+    c = pkg.cases.open_flume(nx=96, ny=16, nz=48, depth=0.3, H=0.05, seed=1, y_open=True)
+    run_pair(pkg, orc, c, 16, check_every=8, precond_ti=16, precond_tj=8)
+
+
+def test_open_faces_need_an_open_side(gpu_lib, pkg):
+    c = pkg.cases.open_flume(nx=32, ny=4, nz=32, depth=0.2, H=0.02)
+    c.open = None
+    t = pkg.Tank(c)
+    with pytest.raises(pkg.CadmasError):
+        t.init_state(True)
+    c.open = [dict(side=1, depth=0.2, period=1.2)]  # side 1 is the wave maker
+    with pytest.raises(pkg.CadmasError):
+        pkg.Tank(c)
+
+
 def test_wave_maker_flume_tiles_bitwise(gpu_lib, pkg, orc):
     """The same with a wave train already in the flume, no fade-in and
     16x2 preconditioner blocks."""
