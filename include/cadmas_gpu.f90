@@ -48,6 +48,7 @@ module cadmas_gpu
      integer(c_int) :: leqk, pad0
      real(c_double) :: anu0, scmk, akmink, akmine, akinik, akinie
      real(c_double) :: akcmu, aksgk, aksge, akc1, akc2, akc3
+     real(c_double) :: akk0, aka0                ! log law (IB 6, 8)
   end type cadmas_params
 
   ! c_loc() of the static arrays (XX(6,NUMI) ... INDB(4,NUMB))
@@ -58,6 +59,7 @@ module cadmas_gpu
      type(c_ptr) :: cd0, anu
      type(c_ptr) :: indx, indy, indz, indb
      type(c_ptr) :: indbk, indbe, bck, bce   ! k-epsilon (LEQK /= 0)
+     type(c_ptr) :: bcvi                     ! roughness of rough walls
   end type cadmas_static
 
   type, bind(C) :: cadmas_stats

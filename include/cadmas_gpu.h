@@ -138,6 +138,12 @@ typedef struct cadmas_params {
   double akinik, akinie;           /* AKINIK, AKINIE initial k, e, 1e-20     */
   double akcmu, aksgk, aksge;      /* C_mu 0.09, sigma_k 1.0, sigma_e 1.3    */
   double akc1, akc2, akc3;         /* C1 1.44, C2 1.92, C3 0.0               */
+  /* AKK0, AKA0 /VF_APHYSR/: kappa 0.4 and A 5.5 of the log law on
+     log-law walls (INDB(3,L) = 6, VF_CLOGLW): the speed over the friction
+     velocity is ln(y us / nu) / kappa + A, us the friction velocity; rough
+     walls (8) use ln(y / ks) / kappa + A + 3 (VF_CLOGKS)
+     (vf_a2dflt.f:175-176, input 'MODEL LOG-LAW', vf_iimdl.f:288-291).      */
+  double akk0, aka0;
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */
@@ -158,6 +164,9 @@ typedef struct cadmas_static {
      (kept on fixed faces, vf_bwke.f:63-64).                               */
   const int    *indbk, *indbe;
   const double *bck, *bce;
+  /* BCVI(NUMB) the roughness ks of rough-wall faces (INDB(3,L) = 8,
+     vf_iiboun.f); may be NULL when there are none (read as 0).           */
+  const double *bcvi;
 } cadmas_static;
 
 /* ---- dynamic state (host pointers; read by set_state, written by get_state)

@@ -75,14 +75,14 @@ class Params(C.Structure):
         ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("precond_split", C.c_int),
         ("idrop", C.c_int), ("iscmff", C.c_int), ("leqk", C.c_int), ("pad0", C.c_int)] + [
         (n, C.c_double) for n in ("anu0", "scmk", "akmink", "akmine", "akinik", "akinie", "akcmu", "aksgk",
-                                  "aksge", "akc1", "akc2", "akc3")]
+                                  "aksge", "akc1", "akc2", "akc3", "akk0", "aka0")]
 
 
 class Static(C.Structure):
     _fields_ = [(n, _dp) for n in ("xx", "yy", "zz", "ggv", "ggx", "ggy", "ggz", "glv", "glx",
                                    "gly", "glz", "cd0", "anu")] + [
         (n, _ip) for n in ("indx", "indy", "indz", "indb", "indbk", "indbe")] + [
-        (n, _dp) for n in ("bck", "bce")]
+        (n, _dp) for n in ("bck", "bce", "bcvi")]
 
 
 class State(C.Structure):
@@ -263,7 +263,7 @@ def static_of(case) -> Static:
         if a is not None:
             assert a.dtype == np.int32 and a.ndim == 1
             setattr(s, n, _iptr(a))
-    for n in ("bck", "bce"):
+    for n in ("bck", "bce", "bcvi"):
         a = getattr(case, n, None)
         if a is not None:
             assert a.dtype == np.float64 and a.ndim == 1

@@ -29,7 +29,7 @@ import numpy as np
 
 # Velocity/pressure boundary types INDB(3,L) and F boundary types INDB(4,L)
 # (vf_a1main.f:151-170).
-VP_SLIP, VP_NOSLIP, VP_FIXED, VP_FREE, VP_WAVE, VP_OPEN = 1, 2, 3, 4, 5, 7
+VP_SLIP, VP_NOSLIP, VP_FIXED, VP_FREE, VP_WAVE, VP_LOGLAW, VP_OPEN, VP_ROUGH = 1, 2, 3, 4, 5, 6, 7, 8
 F_FIXED, F_FREE, F_WAVE, F_OPEN = 1, 2, 5, 7
 
 
@@ -539,6 +539,44 @@ def turbulent_tank(seed=0, k0=1.0e-4, e0=1.0e-5, **kw):
     c = random_tank(seed, **kw)
     c.name = f"turbulent_tank_{seed}"
     return turbulence(c, k0, e0, seed=seed)
+
+
+def loglaw_walls(c: Case, seed=0, frac=0.6, ks=(2.0e-4, 2.0e-3)) -> Case:
+    """Turn a seeded fraction `frac` of the slip and no-slip faces into
+    log-law (6) or fully rough (8) walls, half each, the rough ones with a
+    roughness BCVI uniform in `ks` (input 'B.C. LOG-LAW', 'B.C. ROUGH'); the
+    k and e types of those faces follow the velocity type, as VF_IIBOUN
+    sets them."""
+    rng = np.random.Generator(np.random.Philox(seed + 2000))
+    nb = c.indb.shape[1]
+    c.bcvi = np.zeros(max(nb, 1))
+    for L in range(nb):
+        if c.indb[2, L] not in (VP_SLIP, VP_NOSLIP) or rng.uniform() >= frac:
+            continue
+        t = VP_LOGLAW if rng.uniform() < 0.5 else VP_ROUGH
+        c.indb[2, L] = t
+        if t == VP_ROUGH:
+            c.bcvi[L] = rng.uniform(*ks)
+        c.indbk[L] = t
+        c.indbe[L] = t
+    return c
+
+
+def loglaw_tank(seed=0, turb=False, speed=0.05, **kw):
+    """A random tank whose walls are partly log-law and rough walls, with
+    a seeded flow (|u|, |v|, |w| up to `speed`) in the water so that the
+    walls shear from the first step; `turb` switches the k-epsilon model on
+    (so that the cells next to those walls take VF_BWKELG's k and e)."""
+    c = random_tank(seed, **kw)
+    c.name = f"loglaw_tank_{seed}"
+    if turb:
+        turbulence(c, seed=None)
+    loglaw_walls(c, seed)
+    rng = np.random.Generator(np.random.Philox(seed + 3000))
+    wet = c.ff > 0.0
+    for a in (c.uu, c.vv, c.ww):
+        a += rng.uniform(-speed, speed, a.shape) * wet
+    return c
 
 
 def droplet_tank(seed=0, nx=24, ny=6, nz=20, d=0.01, ndrop=8, level=0.3, dt=2.0e-3, speed=1.0):

@@ -184,6 +184,8 @@ struct cadmas_handle {
     double c = 0.0;
   } open[4];
   long long n_open_faces = 0;  // faces with INDB(3,L) = 7
+  long long n_log_faces = 0;   // faces with INDB(3,L) = 6 or 8 (log-law, rough)
+  double *bcvi = nullptr;      // BCVI roughness (NUMB)
   int mtbtyp = 0, mtbnow = 0;  // MTBTYP, MTBNOW (persists between calls, vf_a2dflt.f:114)
   double dmtbt0 = 0.0;
   std::vector<double> wtt, whh;  // DMTBTT, DMTBHH (host)
@@ -205,6 +207,7 @@ static void refresh_fld(cadmas_handle *h) {
   f.pp = h->pbuf[h->pcur];
   f.ff = h->ff; f.nf = h->nf; f.indc = h->indc; f.nf0 = h->nf0;
   f.bcu = h->bcu; f.bcv = h->bcv; f.bcw = h->bcw; f.bcp = h->bcp; f.bcf = h->bcf;
+  f.bcvi = h->bcvi;
 }
 
 static void refresh_prm(cadmas_handle *h) {
@@ -216,6 +219,8 @@ static void refresh_prm(cadmas_handle *h) {
   p.glxmin = P.glxmin; p.glxmax = P.glxmax; p.glymin = P.glymin; p.glymax = P.glymax;
   p.dtnow = h->dtnow; p.tnow = h->tnow;
   p.icgtyp = P.icgtyp; p.icgmax = P.icgmax; p.ibsuw0 = P.ibsuw0;
+  p.akk0 = P.akk0; p.aka0 = P.aka0; p.anu0 = P.anu0;
+  p.loglaw = h->n_log_faces > 0 ? 1 : 0;
   // sponge parameters of vf_veuler.f:77-113
   p.ipa = 0;
   for (int d = 0; d < 4; ++d) {
@@ -562,6 +567,7 @@ static int read_err(cadmas_handle *h, int &errbits) {
 static int map_err(int bits) {
   if (bits & ERR_PG) return CADMAS_EPG;
   if (bits & ERR_UNSUP) return CADMAS_EUNSUPPORTED;
+  if (bits & ERR_NOTCONV) return CADMAS_ENOTCONV;
   if (bits & ERR_CAP) return CADMAS_ECAP;
   return CADMAS_OK;
 }
@@ -590,7 +596,7 @@ static int bc_tail_v1(cadmas_handle *h) {
   launch_bsuwt(s, h->g, h->f, h->p);
   launch_bsuwt2(s, h->g, h->f);
   launch_bsuwn(s, h->g, h->f);
-  launch_bwuwt(s, h->g, h->f);
+  launch_bwuwt(s, h->g, h->f, h->p, h->dint);
   launch_bwpp(s, h->g, h->f);
   return CADMAS_OK;
 }
@@ -690,9 +696,10 @@ static void ke_nut(cadmas_handle *h) {
 static void do_kpost(cadmas_handle *h) {
   cudaStream_t s = h->s;
   TB(CADMAS_STAGE_TURB);
+  if (h->p.loglaw) launch_bwkelg(s, h->g, h->f, h->p, ke_const(h), h->ak, h->ae_k, h->dint);
   launch_kbsss(s, h->g, h->f, ke_const(h), h->ak, h->ae_k, h->anut, h->anu, true, true);
   launch_bwke(s, h->g, h->f, ke_arrays(h), h->dint);
-  launch_bwuwt(s, h->g, h->f);
+  launch_bwuwt(s, h->g, h->f, h->p, h->dint);
   TE();
 }
 
@@ -779,7 +786,7 @@ static int do_f1cal(cadmas_handle *h) {
   launch_bsuwt2(s, g, h->f);
   launch_bsuwn3(s, g, h->f, h->p);
   launch_bspp(s, g, h->f);
-  launch_bwuwt(s, g, h->f);
+  launch_bwuwt(s, g, h->f, h->p, h->dint);
   launch_bwpp(s, g, h->f);
   TE();
   if (h->P.leqk != 0) do_kpost(h);
@@ -892,6 +899,7 @@ void cadmas_default_params(cadmas_params *p) {
   p->anu0 = 1.0e-6; p->scmk = 1.0;
   p->akmink = 1.0e-20; p->akmine = 1.0e-20; p->akinik = 1.0e-20; p->akinie = 1.0e-20;
   p->akcmu = 0.09; p->aksgk = 1.0; p->aksge = 1.3; p->akc1 = 1.44; p->akc2 = 1.92; p->akc3 = 0.0;
+  p->akk0 = 0.4; p->aka0 = 5.5;  // vf_a2dflt.f:175-176
 }
 
 int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **out) {
@@ -925,6 +933,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) AL(h->vel[b][c], h->N);
   AL(h->pbuf[0], h->N); AL(h->pbuf[1], h->N);
   AL(h->ff, h->N); AL(h->nf, h->N); AL(h->indc, h->N); AL(h->nf0, h->N); AL(h->nlim, h->N);
+  AL(h->bcvi, h->NB);
   AL(h->bcu, h->NB); AL(h->bcv, h->NB); AL(h->bcw, h->NB); AL(h->bcp, h->NB); AL(h->bcf, h->NB);
   for (int w = 0; w < 9; ++w) AL(h->wk[w], h->N);
   // layout tiles: TI x TJ, or TI x TJ/2 when each preconditioner block is
@@ -998,7 +1007,7 @@ int cadmas_destroy(cadmas_handle *h) {
   if (!h) return CADMAS_OK;
   cudaStreamSynchronize(h->s);
   double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
-                  h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
+                  h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcvi, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
                   h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->rb0, h->rb1, h->dres,
                   h->S.sys, h->bb_sl};
   for (double *q : dl) if (q) cudaFree(q);
@@ -1126,7 +1135,17 @@ int cadmas_upload_static(cadmas_handle *h, const cadmas_static *st) {
   CK(cudaMemcpyAsync(h->indz, st->indz, b4, cudaMemcpyHostToDevice, s));
   if (h->g.NB > 0) CK(cudaMemcpyAsync(h->indb, st->indb, 4 * h->g.NB * sizeof(int), cudaMemcpyHostToDevice, s));
   h->n_open_faces = 0;
-  for (long long L = 0; L < h->g.NB; ++L) h->n_open_faces += (st->indb[4 * L + 2] == 7);
+  h->n_log_faces = 0;
+  for (long long L = 0; L < h->g.NB; ++L) {
+    const int ib = st->indb[4 * L + 2];
+    h->n_open_faces += (ib == 7);
+    h->n_log_faces += (ib == 6 || ib == 8);
+  }
+  if (h->g.NB > 0) {
+    if (st->bcvi) CK(cudaMemcpyAsync(h->bcvi, st->bcvi, h->g.NB * sizeof(double), cudaMemcpyHostToDevice, s));
+    else CK(cudaMemsetAsync(h->bcvi, 0, h->g.NB * sizeof(double), s));
+  }
+  refresh_prm(h);
   if (h->P.leqk != 0 && h->g.NB > 0) {  // k-epsilon boundaries (vf_iiboun.f:250-330)
     if (!st->indbk || !st->indbe || !st->bck || !st->bce) return CADMAS_EINVAL;
     const size_t nb = (size_t)h->g.NB;
@@ -1481,16 +1500,18 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   launch_bwuwn(s, h->g, h->f, h->dint);
   { const int rw = wave_bc(h); if (rw) return rw; }
   { const int ro = open_bc(h, h->wk[0], h->wk[1], h->wk[2]); if (ro) return ro; }
+  // vf_cinit.f:295-315 and 359-364: k, e, ANUT and ANU before the wall
+  // functions of VF_BWUWT read ANU
+  if (h->P.leqk != 0) launch_kinit(s, h->g, h->f, ke_const(h), h->ak, h->ae_k, h->anut, h->anu);
   launch_bsuwt(s, h->g, h->f, h->p);
   launch_bsuwt2(s, h->g, h->f);
   launch_bsuwn3(s, h->g, h->f, h->p);
   launch_bspp(s, h->g, h->f);
-  launch_bwuwt(s, h->g, h->f);
+  launch_bwuwt(s, h->g, h->f, h->p, h->dint);
   launch_bwpp(s, h->g, h->f);
   if (h->P.leqk != 0) {
-    // vf_cinit.f:295-315 and 359-364 (k, e, ANUT, ANU), then 397-401
+    // vf_cinit.f:397-401
     const KeConst kc = ke_const(h);
-    launch_kinit(s, h->g, h->f, kc, h->ak, h->ae_k, h->anut, h->anu);
     if (h->g.NB > 0) {
       CK(cudaMemcpyAsync(h->bck, h->bck0, (size_t)h->g.NB * sizeof(double), cudaMemcpyDeviceToDevice, s));
       CK(cudaMemcpyAsync(h->bce, h->bce0, (size_t)h->g.NB * sizeof(double), cudaMemcpyDeviceToDevice, s));

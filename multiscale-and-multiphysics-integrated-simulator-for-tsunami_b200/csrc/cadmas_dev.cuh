@@ -56,6 +56,10 @@ struct Prm {
   // sponge (vf_veuler.f:77-113), precomputed on the host
   int ipa, ip[4];
   double sw[4], spx[4], spz[4];
+  // log-law and rough walls (IB 6, 8): kappa, A, ANU0; loglaw = 1 when the
+  // grid has such faces
+  double akk0, aka0, anu0;
+  int loglaw;
 };
 
 // ---------------------------------------------------------- device arrays
@@ -67,6 +71,7 @@ struct Fld {
   double *uu, *vv, *ww, *pp, *ff;
   int *nf, *indc, *nf0;
   double *bcu, *bcv, *bcw, *bcp, *bcf;
+  const double *bcvi;  // BCVI roughness of rough-wall faces
 };
 
 // DROPTX, DROPTY, DROPTZ, DROPUU, DROPVV, DROPWW of the droplet model
@@ -179,6 +184,7 @@ enum : int {
   ERR_PG = 1,       // P.G ERROR (unexpected NF in VPCOEF, undetermined direction)
   ERR_CAP = 2,      // iteration cap
   ERR_UNSUP = 4,    // boundary type outside the implemented set
+  ERR_NOTCONV = 8,  // the log-law friction velocity did not converge (VF_CLOGLW)
 };
 
 }  // namespace cadmas

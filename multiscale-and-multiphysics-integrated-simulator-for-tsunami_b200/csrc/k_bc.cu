@@ -21,6 +21,7 @@
 // NF=0, so no written value is read by another thread of the same pass.
 #include "cadmas_dev.cuh"
 #include "kernels.h"
+#include "loglaw.cuh"
 
 namespace cadmas {
 
@@ -433,14 +434,54 @@ __global__ void k_bspp(Geo g, Fld f) {
 }
 
 // ---------------------------------------------------- boundary-list rules
-__global__ void k_bwuwt(Geo g, Fld f) {
+// VF_BWUWT (vf_bwuwt.f:41-181): tangential boundary values.  Slip and free
+// faces take the adjacent cell's averages; log-law (6) and rough (8) faces
+// take them reduced by the wall shear, V (1 - DL u*^2 / (ANU VA)), with the
+// friction velocity u* of VF_CLOGLW or VF_CLOGKS.
+__global__ void k_bwuwt(Geo g, Fld f, Prm p, int *err) {
   int L = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (L > g.NB) return;
   int I, J, K;
   decode(g, indb(f, 1, L), I, J, K);
   const int NS = indb(f, 2, L), IB = indb(f, 3, L);
   const double *UU = f.uu, *VV = f.vv, *WW = f.ww;
-  if (IB == 1 || IB == 4) {
+  if (IB == 6 || IB == 8) {
+    double V1, V2, DL, AN;
+    if (NS == 1) {
+      V1 = (A(VV, I, J, K) + A(VV, I, J + 1, K)) * 0.5; V2 = (A(WW, I, J, K) + A(WW, I, J, K + 1)) * 0.5;
+      DL = XX_(2, I) * 0.5; AN = A(f.anu, I, J, K);
+    } else if (NS == 2) {
+      V1 = (A(VV, I - 1, J, K) + A(VV, I - 1, J + 1, K)) * 0.5; V2 = (A(WW, I - 1, J, K) + A(WW, I - 1, J, K + 1)) * 0.5;
+      DL = XX_(2, I - 1) * 0.5; AN = A(f.anu, I - 1, J, K);
+    } else if (NS == 3) {
+      V1 = (A(UU, I, J, K) + A(UU, I + 1, J, K)) * 0.5; V2 = (A(WW, I, J, K) + A(WW, I, J, K + 1)) * 0.5;
+      DL = YY_(2, J) * 0.5; AN = A(f.anu, I, J, K);
+    } else if (NS == 4) {
+      V1 = (A(UU, I, J - 1, K) + A(UU, I + 1, J - 1, K)) * 0.5; V2 = (A(WW, I, J - 1, K) + A(WW, I, J - 1, K + 1)) * 0.5;
+      DL = YY_(2, J - 1) * 0.5; AN = A(f.anu, I, J - 1, K);
+    } else if (NS == 5) {
+      V1 = (A(UU, I, J, K) + A(UU, I + 1, J, K)) * 0.5; V2 = (A(VV, I, J, K) + A(VV, I, J + 1, K)) * 0.5;
+      DL = ZZ_(2, K) * 0.5; AN = A(f.anu, I, J, K);
+    } else {
+      V1 = (A(UU, I, J, K - 1) + A(UU, I + 1, J, K - 1)) * 0.5; V2 = (A(VV, I, J, K - 1) + A(VV, I, J + 1, K - 1)) * 0.5;
+      DL = ZZ_(2, K - 1) * 0.5; AN = A(f.anu, I, J, K - 1);
+    }
+    const double ZERO = 1.0e-20;
+    double VA = sqrt(V1 * V1 + V2 * V2), VT;
+    if (VA < ZERO || AN < ZERO) {
+      V1 = 0.0; V2 = 0.0; DL = 1.0; AN = 1.0; VA = 1.0; VT = 1.0;
+    } else if (IB == 6) {
+      if (!cloglw(DL, VA, p.anu0, p.akk0, p.aka0, VT)) atomicOr(err, ERR_NOTCONV);
+    } else {
+      VT = clogks(DL, VA, f.bcvi[L - 1], p.anu0, p.akk0, p.aka0);
+    }
+    VA = DL / AN * VT * VT / VA;
+    V1 = V1 - VA * V1;
+    V2 = V2 - VA * V2;
+    if (NS == 1 || NS == 2) { f.bcv[L - 1] = V1; f.bcw[L - 1] = V2; }
+    else if (NS == 3 || NS == 4) { f.bcu[L - 1] = V1; f.bcw[L - 1] = V2; }
+    else { f.bcu[L - 1] = V1; f.bcv[L - 1] = V2; }
+  } else if (IB == 1 || IB == 4) {
     if (NS == 1) { f.bcv[L - 1] = (A(VV, I, J, K) + A(VV, I, J + 1, K)) * 0.5; f.bcw[L - 1] = (A(WW, I, J, K) + A(WW, I, J, K + 1)) * 0.5; }
     else if (NS == 2) { f.bcv[L - 1] = (A(VV, I - 1, J, K) + A(VV, I - 1, J + 1, K)) * 0.5; f.bcw[L - 1] = (A(WW, I - 1, J, K) + A(WW, I - 1, J, K + 1)) * 0.5; }
     else if (NS == 3) { f.bcu[L - 1] = (A(UU, I, J, K) + A(UU, I + 1, J, K)) * 0.5; f.bcw[L - 1] = (A(WW, I, J, K) + A(WW, I, J, K + 1)) * 0.5; }
@@ -581,7 +622,7 @@ void launch_bsuwem(cudaStream_t s, const Geo &g, const Fld &f, int *nlim) {
   RL(k_bsuwem_fix, g, f, nlim);
 }
 void launch_bspp(cudaStream_t s, const Geo &g, const Fld &f) { RL(k_bspp, g, f); }
-void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f) { BL(k_bwuwt, g, f); }
+void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *err) { BL(k_bwuwt, g, f, p, err); }
 void launch_bwpp(cudaStream_t s, const Geo &g, const Fld &f) { BL(k_bwpp, g, f); }
 void launch_bwff(cudaStream_t s, const Geo &g, const Fld &f, int *err) { BL(k_bwff, g, f, err); }
 void launch_cdiv(cudaStream_t s, const Geo &g, const Fld &f, double *rb) { RL(k_cdiv, g, f, rb); }

@@ -22,6 +22,7 @@
 // cadmas_create refuses, so it is not built.
 #include "cadmas_dev.cuh"
 #include "kernels.h"
+#include "loglaw.cuh"
 
 namespace cadmas {
 
@@ -86,6 +87,67 @@ __device__ __forceinline__ double kface(const Fld &f, const int NB, long long c,
     }
   }
   return FL;
+}
+
+// VF_BWKELG (vf_bwkelg.f:30-160) on fluid cell (I,J,K): when one of its
+// six faces is a log-law (6) or rough (8) wall, k and e become the
+// averages over those faces of u*^2/sqrt(C_mu) and u*^3/(kappa DL), u* the
+// friction velocity of the cell-centre speed along the face (VF_CLOGLW,
+// VF_CLOGKS) and DL half the cell width.  As in the reference, two z
+// log-law faces count once unless the cell's two y faces are log-law.
+// Returns false (k, e untouched) for a cell with no such face.
+__device__ bool bwkelg_cell(const Geo &g, const Fld &f, const Prm &p, double akcmu, long long c, int I, int J, int K,
+                            double &AK, double &AE, int *err) {
+  const int LXM = f.indx[c], LXP = f.indx[cid(g, I + 1, J, K)];
+  const int LYM = f.indy[c], LYP = f.indy[cid(g, I, J + 1, K)];
+  const int LZM = f.indz[c], LZP = f.indz[cid(g, I, J, K + 1)];
+  const int IXM = LXM >= 1 ? indb(f, 3, LXM) : 0, IXP = LXP >= 1 ? indb(f, 3, LXP) : 0;
+  const int IYM = LYM >= 1 ? indb(f, 3, LYM) : 0, IYP = LYP >= 1 ? indb(f, 3, LYP) : 0;
+  const int IZM = LZM >= 1 ? indb(f, 3, LZM) : 0, IZP = LZP >= 1 ? indb(f, 3, LZP) : 0;
+  auto wall = [](int t) { return t == 6 || t == 8; };
+  if (!(wall(IXM) || wall(IXP) || wall(IYM) || wall(IYP) || wall(IZM) || wall(IZP))) return false;
+  const double ZERO = 1.0e-20;
+  const double CMR = 1.0 / sqrt(akcmu), CKR = 1.0 / p.akk0;
+  const double UC = (f.uu[c] + f.uu[cid(g, I + 1, J, K)]) * 0.5;
+  const double VC = (f.vv[c] + f.vv[cid(g, I, J + 1, K)]) * 0.5;
+  const double WC = (f.ww[c] + f.ww[cid(g, I, J, K + 1)]) * 0.5;
+  const double VX = sqrt(VC * VC + WC * WC), VY = sqrt(UC * UC + WC * WC), VZ = sqrt(UC * UC + VC * VC);
+  const double DX = XX_(2, I) * 0.5, DY = YY_(2, J) * 0.5, DZ = ZZ_(2, K) * 0.5;
+  auto lw = [&](double D, double V, double &T) {
+    if (V >= ZERO && p.anu0 >= ZERO && !cloglw(D, V, p.anu0, p.akk0, p.aka0, T)) atomicOr(err, ERR_NOTCONV);
+  };
+  double SX = 0.0, UT = 0.0, SY = 0.0, VT = 0.0, SZ = 0.0, WT = 0.0;
+  if (IXM == 6 || IXP == 6) { lw(DX, VX, UT); SX = 1.0; if (IXM == 6 && IXP == 6) SX = 2.0; }
+  if (IYM == 6 || IYP == 6) { lw(DY, VY, VT); SY = 1.0; if (IYM == 6 && IYP == 6) SY = 2.0; }
+  if (IZM == 6 || IZP == 6) { lw(DZ, VZ, WT); SZ = 1.0; if (IYM == 6 && IYP == 6) SZ = 2.0; }
+  auto ks = [&](double D, double V, int L) { return (V >= ZERO) ? clogks(D, V, f.bcvi[L - 1], p.anu0, p.akk0, p.aka0) : 0.0; };
+  double SXM = 0.0, UTM = 0.0, SXP = 0.0, UTP = 0.0, SYM = 0.0, VTM = 0.0, SYP = 0.0, VTP = 0.0;
+  double SZM = 0.0, WTM = 0.0, SZP = 0.0, WTP = 0.0;
+  if (IXM == 8) { UTM = ks(DX, VX, LXM); SXM = 1.0; }
+  if (IXP == 8) { UTP = ks(DX, VX, LXP); SXP = 1.0; }
+  if (IYM == 8) { VTM = ks(DY, VY, LYM); SYM = 1.0; }
+  if (IYP == 8) { VTP = ks(DY, VY, LYP); SYP = 1.0; }
+  if (IZM == 8) { WTM = ks(DZ, VZ, LZM); SZM = 1.0; }
+  if (IZP == 8) { WTP = ks(DZ, VZ, LZP); SZP = 1.0; }
+  const double SR = 1.0 / (SX + SY + SZ + SXM + SXP + SYM + SYP + SZM + SZP);
+  AK = CMR * (UT * UT * SX + VT * VT * SY + WT * WT * SZ + UTM * UTM * SXM + UTP * UTP * SXP + VTM * VTM * SYM +
+              VTP * VTP * SYP + WTM * WTM * SZM + WTP * WTP * SZP) * SR;
+  AE = CKR * (UT * UT * UT / DX * SX + VT * VT * VT / DY * SY + WT * WT * WT / DZ * SZ + UTM * UTM * UTM / DX * SXM +
+              UTP * UTP * UTP / DX * SXP + VTM * VTM * VTM / DY * SYM + VTP * VTP * VTP / DY * SYP +
+              WTM * WTM * WTM / DZ * SZM + WTP * WTP * WTP / DZ * SZP) * SR;
+  return true;
+}
+
+// VF_BWKELG after VF_F1CAL (vf_a1main.f:1120): k and e in place on the
+// fluid cells (new NF) next to log-law or rough walls.
+__global__ void k_bwkelg(Geo g, Fld f, Prm p, KeConst kc, double *AK, double *AE, int *err) {
+  ROW_LOOP_BEGIN(g)
+  const long long c = cid(g, I, J, K);
+  if (kint(g, I, J, K) && f.nf[c] == 0) {
+    double ak, ae;
+    if (bwkelg_cell(g, f, p, kc.akcmu, c, I, J, K, ak, ae, err)) { AK[c] = ak; AE[c] = ae; }
+  }
+  ROW_LOOP_END
 }
 
 __global__ void k_kstep(Geo g, Fld f, Prm p, KeConst kc, KeArrays t, double *AKN, double *AEN, int *err) {
@@ -179,6 +241,8 @@ __global__ void k_kstep(Geo g, Fld f, Prm p, KeConst kc, KeArrays t, double *AKN
     const double DSE = (XX_(4, I) * (FE[1] - FE[0]) + YY_(4, J) * (FE[3] - FE[2]) + ZZ_(4, K) * (FE[5] - FE[4]) + QE);
     akn = (G0 * akn + p.dtnow * DSK) / GG;
     aen = (G0 * aen + p.dtnow * DSE) / GG;
+    // VF_BWKELG (vf_k1cal.f:147-149)
+    if (p.loglaw) bwkelg_cell(g, f, p, kc.akcmu, c, I, J, K, akn, aen, err);
     // cut-off (vf_k1cal.f:155-167)
     if (aen < kc.akmine) { akn = kc.akmink; aen = kc.akmine; }
     else if (akn < kc.akmink) akn = kc.akmink;
@@ -264,6 +328,11 @@ __global__ void k_kinit(Geo g, Fld f, KeConst kc, double *AK, double *AE, double
 #undef ZZ_
 
 #define RL(kern, ...) (kern<<<row_blocks(g), ROW_THREADS, 0, s>>>(__VA_ARGS__), count_launch())
+void launch_bwkelg(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, double *ak, double *ae,
+                   int *err) {
+  k_bwkelg<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, f, p, kc, ak, ae, err);
+  count_launch();
+}
 void launch_kstep(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, const KeArrays &t,
                   double *akn, double *aen, int *err) {
   RL(k_kstep, g, f, p, kc, t, akn, aen, err);

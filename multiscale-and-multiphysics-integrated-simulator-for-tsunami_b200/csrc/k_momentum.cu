@@ -573,11 +573,10 @@ __global__ void k_bwuwn(Geo g, Fld f, int *err) {
     else if (NS == 4) { VAL = VV[cid(g, I, J - 1, K)]; f.bcv[L - 1] = VAL; VV[cid(g, I, J, K)] = VAL; }
     else if (NS == 5) { VAL = WW[cid(g, I, J, K + 1)]; f.bcw[L - 1] = VAL; WW[cid(g, I, J, K)] = VAL; }
     else if (NS == 6) { VAL = WW[cid(g, I, J, K - 1)]; f.bcw[L - 1] = VAL; WW[cid(g, I, J, K)] = VAL; }
-  } else if (IB == 6 || IB == 8) {
+  } else if (IB == 6 || IB == 8) {  // log-law and rough walls (vf_bwuwn.f:237-249)
     if (NS == 1 || NS == 2) { f.bcu[L - 1] = 0.0; UU[cid(g, I, J, K)] = 0.0; }
     else if (NS == 3 || NS == 4) { f.bcv[L - 1] = 0.0; VV[cid(g, I, J, K)] = 0.0; }
     else { f.bcw[L - 1] = 0.0; WW[cid(g, I, J, K)] = 0.0; }
-    atomicOr(err, ERR_UNSUP);
   } else if (IB == 5) {
     // wave-maker faces: set by k_wave after this pass (vf_bwuwn.f:259-470);
     // the per-face rule of vf_bwuwn.f:161-216 applies to MTBTYP 3 only,

@@ -314,6 +314,9 @@ void launch_warm_guess(cudaStream_t s, const Geo &g, const Fld &f, const SysPtr 
                        double *rows1, double *scal, int *cnt, double *PT);
 // k-epsilon (k_keps.cu): VF_K1CAL into akn/aen; VF_BSSS (+ VF_CNUT0 and
 // VF_CNU00 with nut); VF_BWKE; the k, e, ANUT, ANU of VF_CINIT
+// VF_BWKELG in place on the fluid cells next to log-law or rough walls
+void launch_bwkelg(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, double *ak, double *ae,
+                   int *err);
 void launch_kstep(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const KeConst &kc, const KeArrays &t,
                   double *akn, double *aen, int *err);
 void launch_kbsss(cudaStream_t s, const Geo &g, const Fld &f, const KeConst &kc, double *ak, double *ae, double *anut,
@@ -344,7 +347,7 @@ void launch_bsuwn(cudaStream_t s, const Geo &g, const Fld &f);
 void launch_bsuwn3(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p);
 void launch_bsuwem(cudaStream_t s, const Geo &g, const Fld &f, int *nlim);
 void launch_bspp(cudaStream_t s, const Geo &g, const Fld &f);
-void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f);
+void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *err);
 void launch_bwpp(cudaStream_t s, const Geo &g, const Fld &f);
 void launch_bwff(cudaStream_t s, const Geo &g, const Fld &f, int *err);
 void launch_cdiv(cudaStream_t s, const Geo &g, const Fld &f, double *rb);

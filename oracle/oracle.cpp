@@ -55,6 +55,57 @@ static double ipow(double x, int n) {
 static inline double dmax(double a, double b) { return (a < b) ? b : a; }
 static inline double dmin(double a, double b) { return (b < a) ? b : a; }
 
+// Natural logarithm for the log-law wall functions, written out so that the
+// GPU kernels can take the same steps: x = m 2^e with m in
+// [sqrt(1/2), sqrt(2)) (frexp, exact), ln x = e ln 2 + 2 atanh(s),
+// s = (m-1)/(m+1), |s| <= 0.1716, and the Maclaurin series
+// 2 atanh(s) = 2 s (1 + z/3 + ... + z^13/27), z = s^2, by Horner's rule
+// (the first omitted term is below 2^-60 of the sum).  Tests check it
+// against libm.
+static double ln_series(double x) {
+  if (!(x > 0.0)) return (x == 0.0) ? -HUGE_VAL : (x - x) / (x - x);
+  if (x > 1.7976931348623157e308) return x;
+  int e;
+  double m = std::frexp(x, &e);
+  if (m < 0.70710678118654752) { m = m * 2.0; e = e - 1; }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double z = s * s;
+  double p = 1.0 / 27.0;
+  for (int k = 12; k >= 0; --k) p = p * z + 1.0 / (double)(2 * k + 1);
+  return (double)e * 0.69314718055994531 + 2.0 * s * p;
+}
+
+// VF_CLOGLW  vf_cloglw.f:29-52: Newton's method for the friction velocity
+// of the log law from u* = ANU0/DL; false on 'NOT CONVERGED.'.
+static bool cloglw(double DL, double VA, double ANU0, double AKK0, double AKA0, double &VT) {
+  const double ZERO = 1.0e-20;
+  VT = 0.0;
+  if (VA < ZERO || ANU0 < ZERO) return true;
+  const int NI = 20;
+  const double EPS = 1.0e-10;
+  const double AKR = 1.0 / AKK0, ANR = 1.0 / ANU0;
+  double XX = ANU0 / DL, DX = 0.0;
+  for (int I = 1; I <= NI; ++I) {
+    const double W = ln_series(DL * XX * ANR);
+    const double F = XX * AKR * W + XX * AKA0 - VA;
+    const double D = AKR * W + AKR + AKA0;
+    DX = -F / D;
+    XX = XX + DX;
+    if (std::fabs(DX) < XX * EPS) break;
+  }
+  if (std::fabs(DX) >= XX * EPS) return false;
+  VT = XX;
+  return true;
+}
+
+// VF_CLOGKS  vf_clogks.f:27-33
+static double clogks(double DL, double VA, double BKS, double ANU0, double AKK0, double AKA0) {
+  const double ZERO = 1.0e-20;
+  if (VA < ZERO || ANU0 < ZERO) return 0.0;
+  const double XX = ln_series(DL / BKS) / AKK0 + AKA0 + 3.0;
+  return VA / XX;
+}
+
 // ------------------------------------------------ FF-SLOPE (ISCMFF = 1)
 // Elementary functions of VF_CROOT3 from +,-,*,/ and sqrt only, so that
 // the GPU kernels can evaluate the same operations in the same order and
@@ -336,6 +387,7 @@ struct orc_handle {
   bool have_static = false;
   // state
   vd UU, VV, WW, PP, FF, BCU, BCV, BCW, BCP, BCF, TBUB;
+  vd BCVI;  // roughness of rough-wall faces
   vi NF, INDC, INDS, NLIM;
   // k-epsilon (LEQK != 0): AK, AE (here AEPS: AE names a solver vector
   // below), ANUT, BCK, BCE; the boundary types INDBK, INDBE and the input
@@ -348,6 +400,7 @@ struct orc_handle {
   // the four sides and the table of /VF_AFILEI/ (vf_iimdl.f:49-106)
   struct Wave { int on = 0, l1 = 0, l2 = 0; double d = 0, t = 0, a = 0; } WV[4];
   struct Open { int on = 0; double c = 0; } OP[4];  // IBCTYP(1,JD) = 2 and BCTYP(6,JD)
+  long long NLOG = 0;  // faces of type 6 or 8 (log-law, rough walls)
   int MTBTYP = 0, MTBNOW = 0;
   double DMTBT0 = 0;
   vd DMTBTT, DMTBHH, DMTBZZ, DMTBUN, DMTBUT;
@@ -1053,7 +1106,6 @@ struct orc_handle {
         if (NS == 1 || NS == 2) { BCU[L - 1] = 0.0; UU[id(I, J, K)] = 0.0; }
         else if (NS == 3 || NS == 4) { BCV[L - 1] = 0.0; VV[id(I, J, K)] = 0.0; }
         else { BCW[L - 1] = 0.0; WW[id(I, J, K)] = 0.0; }
-        if (IB != 1) return CADMAS_EUNSUPPORTED;
       } else if (IB == 2) {
         BCU[L - 1] = 0.0; BCV[L - 1] = 0.0; BCW[L - 1] = 0.0;
         if (NS == 1 || NS == 2) UU[id(I, J, K)] = BCU[L - 1];
@@ -2011,12 +2063,49 @@ struct orc_handle {
 
   // VF_BWUWT  vf_bwuwt.f:41-118 (slip/free, no-slip, fixed; wave faces
   // without matrix data and radiation faces untouched)
-  void bwuwt() {
+  // (vf_bwuwt.f:41-181; IB 5 acts for MTBTYP 3 only, IB 2, 3, 7 keep BC)
+  int bwuwt() {
     for (int L = 1; L <= NB; ++L) {
       int I, J, K;
       decode(IB_(1, L), I, J, K);
       int NS = IB_(2, L), IB = IB_(3, L);
-      if (IB == 1 || IB == 4) {
+      if (IB == 6 || IB == 8) {  // vf_bwuwt.f:116-176
+        double V1, V2, DL, AN;
+        if (NS == 1) {
+          V1 = (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5; V2 = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5;
+          DL = X_(2, I) * 0.5; AN = ANU[id(I, J, K)];
+        } else if (NS == 2) {
+          V1 = (VV[id(I - 1, J, K)] + VV[id(I - 1, J + 1, K)]) * 0.5; V2 = (WW[id(I - 1, J, K)] + WW[id(I - 1, J, K + 1)]) * 0.5;
+          DL = X_(2, I - 1) * 0.5; AN = ANU[id(I - 1, J, K)];
+        } else if (NS == 3) {
+          V1 = (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5; V2 = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5;
+          DL = Y_(2, J) * 0.5; AN = ANU[id(I, J, K)];
+        } else if (NS == 4) {
+          V1 = (UU[id(I, J - 1, K)] + UU[id(I + 1, J - 1, K)]) * 0.5; V2 = (WW[id(I, J - 1, K)] + WW[id(I, J - 1, K + 1)]) * 0.5;
+          DL = Y_(2, J - 1) * 0.5; AN = ANU[id(I, J - 1, K)];
+        } else if (NS == 5) {
+          V1 = (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5; V2 = (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5;
+          DL = Z_(2, K) * 0.5; AN = ANU[id(I, J, K)];
+        } else {
+          V1 = (UU[id(I, J, K - 1)] + UU[id(I + 1, J, K - 1)]) * 0.5; V2 = (VV[id(I, J, K - 1)] + VV[id(I, J + 1, K - 1)]) * 0.5;
+          DL = Z_(2, K - 1) * 0.5; AN = ANU[id(I, J, K - 1)];
+        }
+        const double ZERO = 1.0e-20;
+        double VA = std::sqrt(V1 * V1 + V2 * V2), VT;
+        if (VA < ZERO || AN < ZERO) {
+          V1 = 0.0; V2 = 0.0; DL = 1.0; AN = 1.0; VA = 1.0; VT = 1.0;
+        } else if (IB == 6) {
+          if (!cloglw(DL, VA, P.anu0, P.akk0, P.aka0, VT)) return CADMAS_ENOTCONV;
+        } else {
+          VT = clogks(DL, VA, BCVI[L - 1], P.anu0, P.akk0, P.aka0);
+        }
+        VA = DL / AN * VT * VT / VA;
+        V1 = V1 - VA * V1;
+        V2 = V2 - VA * V2;
+        if (NS == 1 || NS == 2) { BCV[L - 1] = V1; BCW[L - 1] = V2; }
+        else if (NS == 3 || NS == 4) { BCU[L - 1] = V1; BCW[L - 1] = V2; }
+        else { BCU[L - 1] = V1; BCV[L - 1] = V2; }
+      } else if (IB == 1 || IB == 4) {
         if (NS == 1) { BCV[L - 1] = (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5; }
         else if (NS == 2) { BCV[L - 1] = (VV[id(I - 1, J, K)] + VV[id(I - 1, J + 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I - 1, J, K)] + WW[id(I - 1, J, K + 1)]) * 0.5; }
         else if (NS == 3) { BCU[L - 1] = (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5; }
@@ -2025,6 +2114,7 @@ struct orc_handle {
         else if (NS == 6) { BCU[L - 1] = (UU[id(I, J, K - 1)] + UU[id(I + 1, J, K - 1)]) * 0.5; BCV[L - 1] = (VV[id(I, J, K - 1)] + VV[id(I, J + 1, K - 1)]) * 0.5; }
       }
     }
+    return CADMAS_OK;
   }
   // VF_BWPP  vf_bwpp.f:28-51
   void bwpp() {
@@ -3006,7 +3096,10 @@ struct orc_handle {
     if (P.diag_relres) st.true_relres = true_relres(WK[1], WK[2], WK[3], WK[4], WK[5], WK[6], WK[7], WK[8], WK[9], INDC.data());
     T.start();
     vmodif(WK[9]);
-    bsuwt(); bsuwt2(); bsuwn(); bwuwt(); bwpp();
+    bsuwt(); bsuwt2(); bsuwn();
+    int rcw = bwuwt();
+    if (rcw) return rcw;
+    bwpp();
     tmr[3] += T.stop();
     return CADMAS_OK;
   }
@@ -3245,6 +3338,73 @@ struct orc_handle {
 
   // VF_K1CAL  vf_k1cal.f:84-170 (ISCMK = 0; VF_BWKELG acts on log-law and
   // rough walls only, which cadmas_create refuses)
+  // VF_BWKELG  vf_bwkelg.f:30-160: k and e of the fluid cells next to
+  // log-law (6) or rough (8) faces from the faces' friction velocities.
+  // The z count tests the y faces for two log-law faces, as the reference.
+  int bwkelg() {
+    const double ZERO = 1.0e-20;
+    const double CMR = 1.0 / std::sqrt(P.akcmu), CKR = 1.0 / P.akk0;
+    bool bad = false;
+    for (int K = 2; K <= NK - 1; ++K)
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          const size_t c = id(I, J, K);
+          if (NF[c] != 0) continue;
+          const int LXM = INDX[c], LXP = INDX[id(I + 1, J, K)], LYM = INDY[c], LYP = INDY[id(I, J + 1, K)];
+          const int LZM = INDZ[c], LZP = INDZ[id(I, J, K + 1)];
+          int IXM = 0, IXP = 0, IYM = 0, IYP = 0, IZM = 0, IZP = 0;
+          if (LXM >= 1) IXM = IB_(3, LXM);
+          if (LXP >= 1) IXP = IB_(3, LXP);
+          if (LYM >= 1) IYM = IB_(3, LYM);
+          if (LYP >= 1) IYP = IB_(3, LYP);
+          if (LZM >= 1) IZM = IB_(3, LZM);
+          if (LZP >= 1) IZP = IB_(3, LZP);
+          if (!(IXM == 6 || IXP == 6 || IYM == 6 || IYP == 6 || IZM == 6 || IZP == 6 || IXM == 8 || IXP == 8 ||
+                IYM == 8 || IYP == 8 || IZM == 8 || IZP == 8))
+            continue;
+          const double UC = (UU[c] + UU[id(I + 1, J, K)]) * 0.5;
+          const double VC = (VV[c] + VV[id(I, J + 1, K)]) * 0.5;
+          const double WC = (WW[c] + WW[id(I, J, K + 1)]) * 0.5;
+          const double VX = std::sqrt(VC * VC + WC * WC);
+          const double VY = std::sqrt(UC * UC + WC * WC);
+          const double VZ = std::sqrt(UC * UC + VC * VC);
+          const double DX = X_(2, I) * 0.5, DY = Y_(2, J) * 0.5, DZ = Z_(2, K) * 0.5;
+          double SX = 0.0, UT = 0.0;
+          if (IXM == 6 || IXP == 6) {
+            if (VX >= ZERO && P.anu0 >= ZERO) bad |= !cloglw(DX, VX, P.anu0, P.akk0, P.aka0, UT);
+            SX = 1.0;
+            if (IXM == 6 && IXP == 6) SX = 2.0;
+          }
+          double SY = 0.0, VT = 0.0;
+          if (IYM == 6 || IYP == 6) {
+            if (VY >= ZERO && P.anu0 >= ZERO) bad |= !cloglw(DY, VY, P.anu0, P.akk0, P.aka0, VT);
+            SY = 1.0;
+            if (IYM == 6 && IYP == 6) SY = 2.0;
+          }
+          double SZ = 0.0, WT = 0.0;
+          if (IZM == 6 || IZP == 6) {
+            if (VZ >= ZERO && P.anu0 >= ZERO) bad |= !cloglw(DZ, VZ, P.anu0, P.akk0, P.aka0, WT);
+            SZ = 1.0;
+            if (IYM == 6 && IYP == 6) SZ = 2.0;
+          }
+          double SXM = 0.0, UTM = 0.0, SXP = 0.0, UTP = 0.0, SYM = 0.0, VTM = 0.0, SYP = 0.0, VTP = 0.0;
+          double SZM = 0.0, WTM = 0.0, SZP = 0.0, WTP = 0.0;
+          if (IXM == 8) { if (VX >= ZERO) UTM = clogks(DX, VX, BCVI[LXM - 1], P.anu0, P.akk0, P.aka0); SXM = 1.0; }
+          if (IXP == 8) { if (VX >= ZERO) UTP = clogks(DX, VX, BCVI[LXP - 1], P.anu0, P.akk0, P.aka0); SXP = 1.0; }
+          if (IYM == 8) { if (VY >= ZERO) VTM = clogks(DY, VY, BCVI[LYM - 1], P.anu0, P.akk0, P.aka0); SYM = 1.0; }
+          if (IYP == 8) { if (VY >= ZERO) VTP = clogks(DY, VY, BCVI[LYP - 1], P.anu0, P.akk0, P.aka0); SYP = 1.0; }
+          if (IZM == 8) { if (VZ >= ZERO) WTM = clogks(DZ, VZ, BCVI[LZM - 1], P.anu0, P.akk0, P.aka0); SZM = 1.0; }
+          if (IZP == 8) { if (VZ >= ZERO) WTP = clogks(DZ, VZ, BCVI[LZP - 1], P.anu0, P.akk0, P.aka0); SZP = 1.0; }
+          const double SR = 1.0 / (SX + SY + SZ + SXM + SXP + SYM + SYP + SZM + SZP);
+          AK[c] = CMR * (UT * UT * SX + VT * VT * SY + WT * WT * SZ + UTM * UTM * SXM + UTP * UTP * SXP +
+                         VTM * VTM * SYM + VTP * VTP * SYP + WTM * WTM * SZM + WTP * WTP * SZP) * SR;
+          AEPS[c] = CKR * (UT * UT * UT / DX * SX + VT * VT * VT / DY * SY + WT * WT * WT / DZ * SZ +
+                           UTM * UTM * UTM / DX * SXM + UTP * UTP * UTP / DX * SXP + VTM * VTM * VTM / DY * SYM +
+                           VTP * VTP * VTP / DY * SYP + WTM * WTM * WTM / DZ * SZM + WTP * WTP * WTP / DZ * SZP) * SR;
+        }
+    return bad ? CADMAS_ENOTCONV : CADMAS_OK;
+  }
+
   int k1cal() {
     const size_t N = UU.size();
     vd FLKU(N, 0.0), FLKV(N, 0.0), FLKW(N, 0.0), QK(N, 0.0), FLEU(N, 0.0), FLEV(N, 0.0), FLEW(N, 0.0),
@@ -3266,6 +3426,10 @@ struct orc_handle {
     kgene(QK, QE);
     seuler(AK, FLKU, FLKV, FLKW, QK);
     seuler(AEPS, FLEU, FLEV, FLEW, QE);
+    if (NLOG > 0) {  // vf_k1cal.f:147-149
+      const int rcl = bwkelg();
+      if (rcl) return rcl;
+    }
     for (int K = 2; K <= NK - 1; ++K)
       for (int J = 2; J <= NJ - 1; ++J)
         for (int I = 2; I <= NI - 1; ++I) {
@@ -3283,14 +3447,17 @@ struct orc_handle {
   // After VF_F1CAL (vf_a1main.f:1119-1127): the new NF's surface and gas
   // values, the eddy viscosity, boundary values.
   int kpost() {
+    if (NLOG > 0) {  // vf_a1main.f:1120
+      const int rcl = bwkelg();
+      if (rcl) return rcl;
+    }
     bsss(AK);
     bsss(AEPS);
     cnut0();
     cnu00();
     int rc = bwke();
     if (rc) return rc;
-    bwuwt();
-    return CADMAS_OK;
+    return bwuwt();
   }
 
   // VF_CINIT's k-epsilon part (vf_cinit.f:295-315, 359-364; the boundary
@@ -3351,7 +3518,10 @@ struct orc_handle {
     if (rc) return rc;
     cindc();
     bsppfl();
-    bsuwt(); bsuwt2(); bsuwn3(); bspp(); bwuwt(); bwpp();
+    bsuwt(); bsuwt2(); bsuwn3(); bspp();
+    int rcw = bwuwt();
+    if (rcw) return rcw;
+    bwpp();
     st.nums = NUMS;
     tmr[4] += T.stop();
     return CADMAS_OK;
@@ -3372,6 +3542,7 @@ orc_handle *orc_create(const cadmas_dims *d, const cadmas_params *p, int sum_mod
   h->NF.assign(N, -1); h->INDC.assign(N, -1); h->NLIM.assign(N, 0);
   size_t B = (size_t)std::max(h->NB, 1);
   h->BCU.assign(B, 0); h->BCV.assign(B, 0); h->BCW.assign(B, 0); h->BCP.assign(B, 0); h->BCF.assign(B, 0);
+  h->BCVI.assign(B, 0.0);
   h->TBUB.assign(h->NK, 0.0);
   std::memset(&h->st, 0, sizeof(h->st));
   h->st.true_relres = -1.0;
@@ -3394,6 +3565,10 @@ int orc_upload_static(orc_handle *h, const cadmas_static *s) {
   h->INDZ.assign(s->indz, s->indz + N);
   h->INDB.assign(s->indb, s->indb + 4 * (size_t)h->NB);
   if (h->NB == 0) h->INDB.assign(4, 0);
+  h->BCVI.assign((size_t)std::max(h->NB, 1), 0.0);
+  if (s->bcvi && h->NB > 0) h->BCVI.assign(s->bcvi, s->bcvi + h->NB);
+  h->NLOG = 0;
+  for (int L = 1; L <= h->NB; ++L) h->NLOG += (h->IB_(3, L) == 6 || h->IB_(3, L) == 8);
   if (h->P.leqk != 0) {
     if (!s->indbk || !s->indbe || !s->bck || !s->bce) return CADMAS_EINVAL;
     const size_t B = (size_t)h->NB;
@@ -3482,7 +3657,10 @@ int orc_init_state(orc_handle *h, int hydrostatic) {
   }
   if (rc) return rc;
   if (h->P.leqk != 0) h->kinit();  // vf_cinit.f:295-315, 359-364
-  h->bsuwt(); h->bsuwt2(); h->bsuwn3(); h->bspp(); h->bwuwt(); h->bwpp();
+  h->bsuwt(); h->bsuwt2(); h->bsuwn3(); h->bspp();
+  rc = h->bwuwt();
+  if (rc) return rc;
+  h->bwpp();
   if (h->P.leqk != 0) {  // vf_cinit.f:397-401
     rc = h->kinit_bc();
     if (rc) return rc;
@@ -3641,6 +3819,16 @@ double orc_slope_fn(int fn, double x) {
     case 1: return slope_atan(x);
     default: return slope_cos(x);
   }
+}
+
+double orc_ln(double x) { return ln_series(x); }
+
+int orc_cloglw(double dl, double va, double anu0, double akk0, double aka0, double *vt) {
+  return cloglw(dl, va, anu0, akk0, aka0, *vt) ? CADMAS_OK : CADMAS_ENOTCONV;
+}
+
+double orc_clogks(double dl, double va, double ks, double anu0, double akk0, double aka0) {
+  return clogks(dl, va, ks, anu0, akk0, aka0);
 }
 
 int orc_fslp(int dim, const double *s, const double *d, double fval, double *aa, double *fback) {

@@ -79,6 +79,12 @@ int orc_set_turb(orc_handle *h, const double *ak, const double *ae, const double
 int orc_slope_counts(orc_handle *h, int *counts);
 double orc_slope_fn(int fn, double x);
 int orc_fslp(int dim, const double *s, const double *d, double fval, double *aa, double *fback);
+/* The log-law wall functions: the logarithm the oracle and the kernels
+   share, VF_CLOGLW (status CADMAS_ENOTCONV when Newton did not converge)
+   and VF_CLOGKS. */
+double orc_ln(double x);
+int orc_cloglw(double dl, double va, double anu0, double akk0, double aka0, double *vt);
+double orc_clogks(double dl, double va, double ks, double anu0, double akk0, double aka0);
 int orc_croot3(double a, double b, double c, double d, double *x, int *nrt);
 /* Threads the oracle's parallel loops use (OpenMP). */
 int orc_num_threads(void);

@@ -98,6 +98,7 @@ class Oracle:
         base.anu0, base.scmk = 1.0e-6, 1.0
         base.akmink = base.akmine = base.akinik = base.akinie = 1.0e-20
         base.akcmu, base.aksgk, base.aksge, base.akc1, base.akc2, base.akc3 = 0.09, 1.0, 1.3, 1.44, 1.92, 0.0
+        base.akk0, base.aka0 = 0.4, 5.5
         self.params = P.make_params(case, base, **over)
         d = P.Dims(case.ni, case.nj, case.nk, case.numb)
         self.h = self.lib.orc_create(C.byref(d), C.byref(self.params), int(sum_mode))
@@ -252,6 +253,31 @@ def open_speed(depth, period, grav=9.8):
     lib.orc_open_speed.argtypes = [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
     rc = lib.orc_open_speed(float(depth), float(period), float(grav), C.byref(c))
     return None if rc else c.value
+
+
+def ln(x):
+    """The logarithm of the log-law wall functions."""
+    lib = _load_lib()
+    lib.orc_ln.argtypes = [C.c_double]
+    lib.orc_ln.restype = C.c_double
+    return lib.orc_ln(float(x))
+
+
+def cloglw(dl, va, anu0=1.0e-6, akk0=0.4, aka0=5.5):
+    """VF_CLOGLW's friction velocity, or None when it does not converge."""
+    lib = _load_lib()
+    lib.orc_cloglw.argtypes = [C.c_double] * 5 + [C.POINTER(C.c_double)]
+    vt = C.c_double()
+    rc = lib.orc_cloglw(float(dl), float(va), float(anu0), float(akk0), float(aka0), C.byref(vt))
+    return None if rc else vt.value
+
+
+def clogks(dl, va, ks, anu0=1.0e-6, akk0=0.4, aka0=5.5):
+    """VF_CLOGKS's friction velocity on a rough wall of roughness ks."""
+    lib = _load_lib()
+    lib.orc_clogks.argtypes = [C.c_double] * 6
+    lib.orc_clogks.restype = C.c_double
+    return lib.orc_clogks(float(dl), float(va), float(ks), float(anu0), float(akk0), float(aka0))
 
 
 def croot3(a, b, c, d):

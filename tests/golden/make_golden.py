@@ -35,6 +35,10 @@ CASES = {
     "ffslope_dam_break_10": dict(builder="dam_break", kw={}, steps=10, sum_mode=0, over=dict(iscmff=1)),
     # k-epsilon (LEQK = 1) with random k, e boundary types
     "turbulent_tank_0_10": dict(builder="turbulent_tank", kw=dict(seed=0), steps=10, sum_mode=0, over={}),
+    # log-law (6) and rough (8) walls, without and with k-epsilon (VF_BWKELG)
+    "loglaw_tank_1_20": dict(builder="loglaw_tank", kw=dict(seed=1), steps=20, sum_mode=0, over={}),
+    "loglaw_turb_tank_2_10": dict(builder="loglaw_tank", kw=dict(seed=2, turb=True), steps=10, sum_mode=0,
+                                  over={}),
     # wave maker at X-, open (radiation) boundaries at X+ and Y+
     "open_flume_0_10": dict(builder="open_flume", kw=dict(nx=64, ny=4, nz=48, y_open=True), steps=10,
                             sum_mode=0, over={}),

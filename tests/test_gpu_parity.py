@@ -168,6 +168,31 @@ def test_open_flume_two_open_sides_tiles_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 16, check_every=8, precond_ti=16, precond_tj=8)
 
 
+@pytest.mark.parametrize("seed", [0, 1, 3])
+def test_loglaw_walls_bitwise(gpu_lib, pkg, orc, seed):
+    """Log-law (6) and rough (8) walls (VF_BWUWT's wall functions with the
+    series logarithm, vf_bwuwt.f:116-176) in a random tank with a seeded
+    flow: bit for bit."""
+    c = pkg.cases.loglaw_tank(seed)
+    run_pair(pkg, orc, c, 20, check_every=5)
+
+
+@pytest.mark.parametrize("seed", [2, 4])
+def test_loglaw_walls_with_turbulence_bitwise(gpu_lib, pkg, orc, seed):
+    """The same with k-epsilon: VF_BWKELG fused into the k-e step and after
+    F1CAL; k, e, ANUT, ANU and their boundary values bit for bit too."""
+    c = pkg.cases.loglaw_tank(seed, turb=True)
+    t, o = run_pair(pkg, orc, c, 16, check_every=4)
+    tg, to = t.get_turb(), o.get_turb()
+    for k in ("ak", "ae", "anut", "anu", "bck", "bce"):
+        assert tg[k].tobytes() == to[k].tobytes(), k
+
+
+def test_loglaw_walls_larger_tank_tiles_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.loglaw_tank(5, turb=True, nx=40, ny=20, nz=24)
+    run_pair(pkg, orc, c, 10, check_every=5, precond_ti=16, precond_tj=8)
+
+
 def test_open_faces_need_an_open_side(gpu_lib, pkg):
     c = pkg.cases.open_flume(nx=32, ny=4, nz=32, depth=0.2, H=0.02)
     c.open = None
