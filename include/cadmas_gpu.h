@@ -203,7 +203,10 @@ typedef struct cadmas_stats {
 typedef struct cadmas_wave_table {
   int ntt, nzz;          /* MTBTT, MTBZZ                                     */
   int mtbtyp;            /* MTBTYP: 1 level and velocities (scaled to the
-                            column's water level), 2 velocities only        */
+                            column's water level), 2 velocities only,
+                            3 level only: the faces act as free faces and
+                            the column next to the side takes the level
+                            (VF_BWFFSF, vf_bwffsf.f)                      */
   int pad;
   double phase0;         /* DMTBT0: phase at TNOW = 0                        */
   const double *tt;      /* DMTBTT(MTBTT) phase, ascending in [0,1]         */

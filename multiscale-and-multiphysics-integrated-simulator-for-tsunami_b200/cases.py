@@ -730,6 +730,33 @@ def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: f
     return c
 
 
+def level_table(amp: float, ntt: int = 121, depth: float = 1.0) -> dict:
+    """A matrix table of type MTBTYP 3 (fixed water level): the level
+    above WVLVL over one period, amp sin^2(pi p) (a single long crest, as a
+    tsunami's leading wave), p the phase in [0,1].  The velocity columns
+    are placeholders; a level table sets no velocities."""
+    tt = np.linspace(0.0, 1.0, ntt)
+    zz = np.array([-depth, 0.0])
+    return dict(tt=tt, hh=amp * np.sin(np.pi * tt) ** 2, zz=zz, un=np.zeros((2, ntt), order="F"),
+                ut=np.zeros((2, ntt), order="F"), phase0=0.0, mtbtyp=3)
+
+
+def fixed_level_flume(nx=96, ny=4, nz=48, dx=0.05, dz=0.01, depth=0.3, amp=0.05, T=4.0, ramp=0.0,
+                      open_end=True) -> Case:
+    """Flume driven at X- by a fixed water level (WAVE-BC ... FUNC MATRIX
+    with MTBTYP 3) following `level_table`: the boundary faces act as free
+    faces and the column next to the side takes the level (VF_BWFFSF);
+    with `open_end` the X+ side radiates (MODEL OPEN-BC)."""
+    c = porous_flume(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, depth=depth,
+                     block=(0.6 * nx * dx, 0.6 * nx * dx + 0.2, depth + amp), gamma=0.5)
+    c.params.update(idamp=[-1, -1, -1, -1])
+    wave_maker(c, 2.0 * amp, T, depth, side=1, ramp=ramp, table=level_table(amp, depth=depth))
+    if open_end:
+        open_boundary(c, depth, T, side=2)
+    c.name = "fixed_level_flume"
+    return c
+
+
 def open_boundary(c: Case, depth: float, T: float, side: int = 2) -> Case:
     """Make side `side` (1 X-, 2 X+, 3 Y-, 4 Y+) an open (radiation)
     boundary for waves of period T in still-water depth `depth` (MODEL

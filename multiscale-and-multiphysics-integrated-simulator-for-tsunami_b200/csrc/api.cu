@@ -221,6 +221,7 @@ static void refresh_prm(cadmas_handle *h) {
   p.icgtyp = P.icgtyp; p.icgmax = P.icgmax; p.ibsuw0 = P.ibsuw0;
   p.akk0 = P.akk0; p.aka0 = P.aka0; p.anu0 = P.anu0;
   p.loglaw = h->n_log_faces > 0 ? 1 : 0;
+  for (int d = 0; d < 4; ++d) p.fixlvl[d] = (h->wave[d].on && h->mtbtyp == 3) ? 1 : 0;
   // sponge parameters of vf_veuler.f:77-113
   p.ipa = 0;
   for (int d = 0; d < 4; ++d) {
@@ -296,7 +297,34 @@ static int wave_bc(cadmas_handle *h) {
     w.sa = (jd == 0) ? 1.0 : (jd == 1 ? -1.0 : 0.0);  // normal incidence (vf_bwuwn.f:298-310)
     w.sb = (jd == 2) ? 1.0 : (jd == 3 ? -1.0 : 0.0);
     w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
-    launch_wave(h->s, h->g, h->f, w, h->dint);
+    // a fixed-water-level table sets no velocities (vf_bwuwn.f:330-331)
+    if (h->mtbtyp != 3) launch_wave(h->s, h->g, h->f, w, h->dint);
+  }
+  return CADMAS_OK;
+}
+
+// VF_BWFFSF (vf_bwffsf.f:43-128): on the sides whose table fixes the water
+// level (MTBTYP 3), F of the column next to the side from the level
+// WVLVL + the table's level (faded in as VF_BWUWN does) at TNOW.
+static int fixed_level_f(cadmas_handle *h) {
+  if (h->mtbtyp != 3) return CADMAS_OK;
+  const double PI = 3.141592653589794, ZERO = 1.0e-20;
+  for (int jd = 0; jd < 4; ++jd) {
+    const cadmas_handle::WaveSide &ws = h->wave[jd];
+    if (!ws.on) continue;
+    const double T = ws.t, T0 = h->dmtbt0;
+    float R4TN = (float)(T0 - h->tnow / T);
+    R4TN = R4TN - (float)(int)R4TN;
+    if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
+    double AW = 1.0, A = ws.a;
+    if (A >= ZERO) {
+      A = h->tnow / T / A;
+      if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
+    }
+    double W1, W2, WVZ;
+    if (!cwmtb1(h, (double)R4TN, W1, W2, WVZ)) return CADMAS_EPG;
+    h->wave_level[jd] = WVZ * AW;
+    launch_bwffsf(h->s, h->g, h->f, jd + 1, ws.first, ws.last, h->P.wvlvl + h->wave_level[jd]);
   }
   return CADMAS_OK;
 }
@@ -616,7 +644,7 @@ static int do_v1cal(cadmas_handle *h) {
   refresh_fld(h);
   // normal boundary velocities (vf_v1cal.f:251-254)
   TB(CADMAS_STAGE_MODIF);
-  launch_bwuwn(s, h->g, h->f, h->dint);
+  launch_bwuwn(s, h->g, h->f, h->p, h->dint);
   { const int rw = wave_bc(h); if (rw) return rw; }
   // UB, VB, WB: the velocities of the step's start (vf_v1cal.f:125-142)
   { const int ro = open_bc(h, h->vel[nxt ^ 1][0], h->vel[nxt ^ 1][1], h->vel[nxt ^ 1][2]); if (ro) return ro; }
@@ -730,6 +758,7 @@ static int do_f1cal(cadmas_handle *h) {
     launch_fconvs(s, g, h->f, h->p, h->nlim, h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[0], h->wk[1],
                   h->wk[2], h->dint);
   launch_feuler(s, g, h->f, h->p, h->wk[0], h->wk[1], h->wk[2]);
+  { const int rl = fixed_level_f(h); if (rl) return rl; }  // vf_f1cal.f:180
   // surface redistribution, cut-off and volume (vf_f1cal.f:185-188)
   launch_fmod1(s, g, h->f, h->nlim);
   launch_fcut(s, g, h->f, h->p, h->rb0, h->rb1);
@@ -1037,10 +1066,7 @@ int cadmas_destroy(cadmas_handle *h) {
 int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
   if (!h || !w || !t || !t->tt || !t->hh || !t->zz || !t->un || !t->ut) return CADMAS_EINVAL;
   if (w->side < 1 || w->side > 4 || t->ntt < 2 || t->nzz < 2) return CADMAS_EINVAL;
-  if (t->mtbtyp != 1 && t->mtbtyp != 2) {
-    g_last_error = "wave table type MTBTYP 3 (fixed water level) is not implemented";
-    return CADMAS_EUNSUPPORTED;
-  }
+  if (t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
   if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
   if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
     g_last_error = "side already declared open";
@@ -1461,6 +1487,7 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   refresh_prm(h);
   refresh_fld(h);
   CK(cudaMemsetAsync(h->dint, 0, 8 * sizeof(int), s));
+  { const int rl = fixed_level_f(h); if (rl) return rl; }  // vf_cinit.f:177
   // vf_cinit.f:202-207
   launch_fcut(s, h->g, h->f, h->p, h->rb0, h->rb1);
   launch_fin(s, FIN_STORE, h->rb0, h->rb1, nrows(h), h->st, h->dres, 0, 0, 0, 0);
@@ -1497,7 +1524,7 @@ int cadmas_init_state(cadmas_handle *h, int hydrostatic) {
   if (any_open)
     for (int c = 0; c < 3; ++c)
       CK(cudaMemcpyAsync(h->wk[c], h->vel[h->cur][c], h->N * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  launch_bwuwn(s, h->g, h->f, h->dint);
+  launch_bwuwn(s, h->g, h->f, h->p, h->dint);
   { const int rw = wave_bc(h); if (rw) return rw; }
   { const int ro = open_bc(h, h->wk[0], h->wk[1], h->wk[2]); if (ro) return ro; }
   // vf_cinit.f:295-315 and 359-364: k, e, ANUT and ANU before the wall

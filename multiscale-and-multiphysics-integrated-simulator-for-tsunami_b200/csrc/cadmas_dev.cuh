@@ -60,7 +60,18 @@ struct Prm {
   // grid has such faces
   double akk0, aka0, anu0;
   int loglaw;
+  // fixlvl[JD-1] = 1: side JD is a wave side whose table fixes the water
+  // level (MTBTYP 3); its faces then act as free faces
+  int fixlvl[4];
 };
+
+// A boundary face of a fixed-water-level side: on the domain boundary of
+// the side its NS names (vf_bwuwn.f:161-216, vf_vmodif.f:89-112,
+// vf_bwuwt.f:80-115).
+__device__ __forceinline__ bool fixlvl_face(const Geo &g, const Prm &p, int NS, int I, int J) {
+  if (NS < 1 || NS > 4 || !p.fixlvl[NS - 1]) return false;
+  return NS == 1 ? I == 2 : NS == 2 ? I == g.NI : NS == 3 ? J == 2 : J == g.NJ;
+}
 
 // ---------------------------------------------------------- device arrays
 struct Fld {

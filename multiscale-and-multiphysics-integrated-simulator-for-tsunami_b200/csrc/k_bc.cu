@@ -481,7 +481,7 @@ __global__ void k_bwuwt(Geo g, Fld f, Prm p, int *err) {
     if (NS == 1 || NS == 2) { f.bcv[L - 1] = V1; f.bcw[L - 1] = V2; }
     else if (NS == 3 || NS == 4) { f.bcu[L - 1] = V1; f.bcw[L - 1] = V2; }
     else { f.bcu[L - 1] = V1; f.bcv[L - 1] = V2; }
-  } else if (IB == 1 || IB == 4) {
+  } else if (IB == 1 || IB == 4 || (IB == 5 && fixlvl_face(g, p, NS, I, J))) {
     if (NS == 1) { f.bcv[L - 1] = (A(VV, I, J, K) + A(VV, I, J + 1, K)) * 0.5; f.bcw[L - 1] = (A(WW, I, J, K) + A(WW, I, J, K + 1)) * 0.5; }
     else if (NS == 2) { f.bcv[L - 1] = (A(VV, I - 1, J, K) + A(VV, I - 1, J + 1, K)) * 0.5; f.bcw[L - 1] = (A(WW, I - 1, J, K) + A(WW, I - 1, J, K + 1)) * 0.5; }
     else if (NS == 3) { f.bcu[L - 1] = (A(UU, I, J, K) + A(UU, I + 1, J, K)) * 0.5; f.bcw[L - 1] = (A(WW, I, J, K) + A(WW, I, J, K + 1)) * 0.5; }
@@ -622,6 +622,28 @@ void launch_bsuwem(cudaStream_t s, const Geo &g, const Fld &f, int *nlim) {
   RL(k_bsuwem_fix, g, f, nlim);
 }
 void launch_bspp(cudaStream_t s, const Geo &g, const Fld &f) { RL(k_bspp, g, f); }
+// VF_BWFFSF (vf_bwffsf.f:48-128): F of the column next to a fixed-water-
+// level side from the level wl = WVLVL + the table's level, per cell
+// height; obstacle cells keep theirs.  One thread per cell of the column.
+__global__ void k_bwffsf(Geo g, Fld f, int side, int first, int last, double WL) {
+  const int n = first + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int K = 2 + (int)blockIdx.y;
+  if (n > last || K > g.NK - 1) return;
+  double VAL;
+  if (gz(g, 1, K) > WL) VAL = 0.0;
+  else if (gz(g, 1, K + 1) < WL) VAL = 1.0;
+  else VAL = (WL - gz(g, 1, K)) / (gz(g, 1, K + 1) - gz(g, 1, K));
+  long long c;
+  if (side <= 2) c = cid(g, side == 1 ? 2 : g.NI - 1, n, K);
+  else c = cid(g, n, side == 3 ? 2 : g.NJ - 1, K);
+  if (f.nf[c] != -1) f.ff[c] = VAL;
+}
+void launch_bwffsf(cudaStream_t s, const Geo &g, const Fld &f, int side, int first, int last, double wl) {
+  const int n = last - first + 1;
+  if (n <= 0 || g.NK <= 2) return;
+  k_bwffsf<<<dim3((n + 127) / 128, g.NK - 2), 128, 0, s>>>(g, f, side, first, last, wl);
+  count_launch();
+}
 void launch_bwuwt(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *err) { BL(k_bwuwt, g, f, p, err); }
 void launch_bwpp(cudaStream_t s, const Geo &g, const Fld &f) { BL(k_bwpp, g, f); }
 void launch_bwff(cudaStream_t s, const Geo &g, const Fld &f, int *err) { BL(k_bwff, g, f, err); }

@@ -542,7 +542,7 @@ __global__ void k_predict(Geo g, Fld f, Prm p, const double *FLUU, const double 
 }
 
 // ------------------------------------------------------------ VF_BWUWN
-__global__ void k_bwuwn(Geo g, Fld f, int *err) {
+__global__ void k_bwuwn(Geo g, Fld f, Prm p, int *err) {
   int L = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (L > g.NB) return;
   int I, J, K;
@@ -579,8 +579,17 @@ __global__ void k_bwuwn(Geo g, Fld f, int *err) {
     else { f.bcw[L - 1] = 0.0; WW[cid(g, I, J, K)] = 0.0; }
   } else if (IB == 5) {
     // wave-maker faces: set by k_wave after this pass (vf_bwuwn.f:259-470);
-    // the per-face rule of vf_bwuwn.f:161-216 applies to MTBTYP 3 only,
-    // which cadmas_set_wave does not accept
+    // on a fixed-water-level side (MTBTYP 3) they copy the face inside
+    // as free faces do (vf_bwuwn.f:161-216)
+    if (fixlvl_face(g, p, NS, I, J)) {
+      double VAL;
+      if (NS == 1) { VAL = UU[cid(g, I + 1, J, K)]; f.bcu[L - 1] = VAL; UU[cid(g, I, J, K)] = VAL; }
+      else if (NS == 2) { VAL = UU[cid(g, I - 1, J, K)]; f.bcu[L - 1] = VAL; UU[cid(g, I, J, K)] = VAL; }
+      else if (NS == 3) { VAL = VV[cid(g, I, J + 1, K)]; f.bcv[L - 1] = VAL; VV[cid(g, I, J, K)] = VAL; }
+      else { VAL = VV[cid(g, I, J - 1, K)]; f.bcv[L - 1] = VAL; VV[cid(g, I, J, K)] = VAL; }
+    } else if (NS > 4) {
+      atomicOr(err, ERR_PG);
+    }
   } else if (IB == 7) {
     // open (radiation) faces: set by k_open after this pass
     // (vf_bwuwn.f:234-235, 481-598)
@@ -780,9 +789,9 @@ void launch_predict(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p,
                                                    fl[5], fl[6], fl[7], fl[8], un, vn, wn);
   count_launch();
 }
-void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, int *err) {
+void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *err) {
   if (g.NB <= 0) return;
-  k_bwuwn<<<(g.NB + 255) / 256, 256, 0, s>>>(g, f, err);
+  k_bwuwn<<<(g.NB + 255) / 256, 256, 0, s>>>(g, f, p, err);
   count_launch();
 }
 

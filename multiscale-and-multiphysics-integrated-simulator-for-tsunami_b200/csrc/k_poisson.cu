@@ -52,7 +52,8 @@ __global__ void k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
       GV = XX_(6, I) * (XX_(2, I) * GGV[c] / GLV[c] + XX_(2, IM) * A(GGV, IM, J, K) / A(GLV, IM, J, K));
       AIM = AYZ * XX_(5, I) * f.ggx[c] * GV; ALI = -AIM;
     } else if (IS >= 1) {
-      if (indb(f, 3, IS) == 4) AIM = 2.0 * AYZ * XX_(4, I) * f.ggx[c] * GGV[c] / GLV[c];
+      if (indb(f, 3, IS) == 4 || (indb(f, 3, IS) == 5 && I == 2 && p.fixlvl[0]))  // vf_vpcoef.f:158-175
+        AIM = 2.0 * AYZ * XX_(4, I) * f.ggx[c] * GGV[c] / GLV[c];
       else AIM = 0.0;
     } else { AIM = 0.0; atomicOr(err, ERR_PG); }
     IS = A(f.indx, IP, J, K);
@@ -60,7 +61,8 @@ __global__ void k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
       GV = XX_(6, IP) * (XX_(2, IP) * A(GGV, IP, J, K) / A(GLV, IP, J, K) + XX_(2, I) * GGV[c] / GLV[c]);
       AIP = AYZ * XX_(5, IP) * A(f.ggx, IP, J, K) * GV; AUI = -AIP;
     } else if (IS >= 1) {
-      if (indb(f, 3, IS) == 4) AIP = 2.0 * AYZ * XX_(4, I) * A(f.ggx, IP, J, K) * GGV[c] / GLV[c];
+      if (indb(f, 3, IS) == 4 || (indb(f, 3, IS) == 5 && IP == g.NI && p.fixlvl[1]))
+        AIP = 2.0 * AYZ * XX_(4, I) * A(f.ggx, IP, J, K) * GGV[c] / GLV[c];
       else AIP = 0.0;
     } else { AIP = 0.0; atomicOr(err, ERR_PG); }
     IS = f.indy[c];
@@ -68,7 +70,8 @@ __global__ void k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
       GV = YY_(6, J) * (YY_(2, J) * GGV[c] / GLV[c] + YY_(2, JM) * A(GGV, I, JM, K) / A(GLV, I, JM, K));
       AJM = AXZ * YY_(5, J) * f.ggy[c] * GV; ALJ = -AJM;
     } else if (IS >= 1) {
-      if (indb(f, 3, IS) == 4) AJM = 2.0 * AXZ * YY_(4, J) * f.ggy[c] * GGV[c] / GLV[c];
+      if (indb(f, 3, IS) == 4 || (indb(f, 3, IS) == 5 && J == 2 && p.fixlvl[2]))
+        AJM = 2.0 * AXZ * YY_(4, J) * f.ggy[c] * GGV[c] / GLV[c];
       else AJM = 0.0;
     } else { AJM = 0.0; atomicOr(err, ERR_PG); }
     IS = A(f.indy, I, JP, K);
@@ -76,7 +79,8 @@ __global__ void k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
       GV = YY_(6, JP) * (YY_(2, JP) * A(GGV, I, JP, K) / A(GLV, I, JP, K) + YY_(2, J) * GGV[c] / GLV[c]);
       AJP = AXZ * YY_(5, JP) * A(f.ggy, I, JP, K) * GV; AUJ = -AJP;
     } else if (IS >= 1) {
-      if (indb(f, 3, IS) == 4) AJP = 2.0 * AXZ * YY_(4, J) * A(f.ggy, I, JP, K) * GGV[c] / GLV[c];
+      if (indb(f, 3, IS) == 4 || (indb(f, 3, IS) == 5 && JP == g.NJ && p.fixlvl[3]))
+        AJP = 2.0 * AXZ * YY_(4, J) * A(f.ggy, I, JP, K) * GGV[c] / GLV[c];
       else AJP = 0.0;
     } else { AJP = 0.0; atomicOr(err, ERR_PG); }
     IS = f.indz[c];
@@ -1032,7 +1036,7 @@ __global__ void k_vmodif(Geo g, Fld f, Prm p, const double *PT) {
     if (IS == 0) {
       double GV = XX_(6, I) * (XX_(2, I) * GGV[c] / GLV[c] + XX_(2, I - 1) * A(GGV, I - 1, J, K) / A(GLV, I - 1, J, K));
       f.uu[c] = f.uu[c] + XX_(5, I) * GV * (PT[c] - A(PT, I - 1, J, K));
-    } else if (IS > 0 && indb(f, 3, IS) == 4) {
+    } else if (IS > 0 && (indb(f, 3, IS) == 4 || (indb(f, 3, IS) == 5 && fixlvl_face(g, p, indb(f, 2, IS), I, J)))) {
       if (indb(f, 2, IS) == 1) f.uu[c] = f.uu[c] + 2.0 * XX_(4, I) * GGV[c] / GLV[c] * PT[c];
       else f.uu[c] = f.uu[c] - 2.0 * XX_(4, I - 1) * A(GGV, I - 1, J, K) / A(GLV, I - 1, J, K) * A(PT, I - 1, J, K);
       f.bcu[IS - 1] = f.uu[c];
@@ -1043,7 +1047,7 @@ __global__ void k_vmodif(Geo g, Fld f, Prm p, const double *PT) {
     if (IS == 0) {
       double GV = YY_(6, J) * (YY_(2, J) * GGV[c] / GLV[c] + YY_(2, J - 1) * A(GGV, I, J - 1, K) / A(GLV, I, J - 1, K));
       f.vv[c] = f.vv[c] + YY_(5, J) * GV * (PT[c] - A(PT, I, J - 1, K));
-    } else if (IS > 0 && indb(f, 3, IS) == 4) {
+    } else if (IS > 0 && (indb(f, 3, IS) == 4 || (indb(f, 3, IS) == 5 && fixlvl_face(g, p, indb(f, 2, IS), I, J)))) {
       if (indb(f, 2, IS) == 3) f.vv[c] = f.vv[c] + 2.0 * YY_(4, J) * GGV[c] / GLV[c] * PT[c];
       else f.vv[c] = f.vv[c] - 2.0 * YY_(4, J - 1) * A(GGV, I, J - 1, K) / A(GLV, I, J - 1, K) * A(PT, I, J - 1, K);
       f.bcv[IS - 1] = f.vv[c];

@@ -190,7 +190,9 @@ bool drop_supported(const Geo &g);
 void launch_flux(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl);
 void launch_predict(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, double *const *fl,
                     double *un, double *vn, double *wn);
-void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, int *err);
+void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int *err);
+// VF_BWFFSF: F of the cells next to a fixed-water-level side set to the level wl
+void launch_bwffsf(cudaStream_t s, const Geo &g, const Fld &f, int side, int first, int last, double wl);
 void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, int *err);
 // Open (radiation) faces of one side; ub/vb/wb the velocities the blend
 // reads (the start of the step's, or a copy of the present ones at set-up)

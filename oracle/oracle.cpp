@@ -401,6 +401,13 @@ struct orc_handle {
   struct Wave { int on = 0, l1 = 0, l2 = 0; double d = 0, t = 0, a = 0; } WV[4];
   struct Open { int on = 0; double c = 0; } OP[4];  // IBCTYP(1,JD) = 2 and BCTYP(6,JD)
   long long NLOG = 0;  // faces of type 6 or 8 (log-law, rough walls)
+  // IBCTYP(2,JD) = -3 with MTBTYP 3: side JD fixes the water level
+  bool FIXLVL(int JD) const { return JD >= 1 && JD <= 4 && WV[JD - 1].on && MTBTYP == 3; }
+  // a type 5 face on the domain boundary of the side its NS names
+  bool fixlvl_face(int NS, int I, int J) const {
+    if (NS < 1 || NS > 4 || !FIXLVL(NS)) return false;
+    return NS == 1 ? I == 2 : NS == 2 ? I == NI : NS == 3 ? J == 2 : J == NJ;
+  }
   int MTBTYP = 0, MTBNOW = 0;
   double DMTBT0 = 0;
   vd DMTBTT, DMTBHH, DMTBZZ, DMTBUN, DMTBUT;
@@ -1123,8 +1130,16 @@ struct orc_handle {
         else if (NS == 4) { VAL = VV[id(I, J - 1, K)]; BCV[L - 1] = VAL; VV[id(I, J, K)] = VAL; }
         else if (NS == 5) { VAL = WW[id(I, J, K + 1)]; BCW[L - 1] = VAL; WW[id(I, J, K)] = VAL; }
         else if (NS == 6) { VAL = WW[id(I, J, K - 1)]; BCW[L - 1] = VAL; WW[id(I, J, K)] = VAL; }
-      } else if (IB == 5) {
-        // vf_bwuwn.f:161-216 acts for MTBTYP 3 only (not accepted here)
+      } else if (IB == 5) {  // vf_bwuwn.f:161-216 (fixed water level only)
+        if (fixlvl_face(NS, I, J)) {
+          double VAL;
+          if (NS == 1) { VAL = UU[id(I + 1, J, K)]; BCU[L - 1] = VAL; UU[id(I, J, K)] = VAL; }
+          else if (NS == 2) { VAL = UU[id(I - 1, J, K)]; BCU[L - 1] = VAL; UU[id(I, J, K)] = VAL; }
+          else if (NS == 3) { VAL = VV[id(I, J + 1, K)]; BCV[L - 1] = VAL; VV[id(I, J, K)] = VAL; }
+          else { VAL = VV[id(I, J - 1, K)]; BCV[L - 1] = VAL; VV[id(I, J, K)] = VAL; }
+        } else if (NS > 4) {
+          return CADMAS_EPG;
+        }
       } else if (IB == 7) {
         // vf_bwuwn.f:234-235: set below by side
       } else {
@@ -1297,6 +1312,41 @@ struct orc_handle {
     return true;
   }
 
+  // VF_BWFFSF  vf_bwffsf.f:43-128: F of the column next to each side whose
+  // table fixes the water level (MTBTYP 3) from WVLVL + the table's level
+  int bwffsf() {
+    if (MTBTYP != 3) return CADMAS_OK;
+    const double PI = 3.141592653589794, ZERO = 1.0e-20;
+    for (int JD = 1; JD <= 4; ++JD) {
+      const Wave &w = WV[JD - 1];
+      if (!w.on) continue;
+      const double T = w.t, T0 = DMTBT0;
+      double A = w.a;
+      float R4TN = (float)(T0 - TNOW / T);
+      R4TN = R4TN - (float)(int)R4TN;
+      if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
+      double AW = 1.0;
+      if (A >= ZERO) {
+        A = TNOW / T / A;
+        if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
+      }
+      double WMT1, WMT2, WVZ;
+      if (!cwmtb1((double)R4TN, WMT1, WMT2, WVZ)) return CADMAS_EPG;
+      const double WL = P.wvlvl + WVZ * AW;
+      for (int K = 2; K <= NK - 1; ++K) {
+        double VAL;
+        if (Z_(1, K) > WL) VAL = 0.0;
+        else if (Z_(1, K + 1) < WL) VAL = 1.0;
+        else VAL = (WL - Z_(1, K)) / (Z_(1, K + 1) - Z_(1, K));
+        for (int n = w.l1; n <= w.l2; ++n) {
+          const size_t c = (JD <= 2) ? id(JD == 1 ? 2 : NI - 1, n, K) : id(n, JD == 3 ? 2 : NJ - 1, K);
+          if (NF[c] != -1) FF[c] = VAL;
+        }
+      }
+    }
+    return CADMAS_OK;
+  }
+
   // VF_BWUWN wave-maker part  vf_bwuwn.f:259-470, matrix-table inflow
   // (IBCTYP(2,JD) = -3, MTBTYP 1 or 2; normal incidence, one rank).
   int bwuwn_wave() {
@@ -1322,6 +1372,7 @@ struct orc_handle {
       else if (JD == 2) { SA = -1.0; SB = 0.0; }
       else if (JD == 3) { SA = 0.0; SB = 1.0; }
       else { SA = 0.0; SB = -1.0; }
+      if (MTBTYP == 3) continue;  // vf_bwuwn.f:330: no velocities from a level table
       const bool xs = (JD == 1 || JD == 2);
       const int I0 = (JD == 1) ? 2 : NI, IC0 = (JD == 1) ? 2 : NI - 1;
       const int J0 = (JD == 3) ? 2 : NJ, JC0 = (JD == 3) ? 2 : NJ - 1;
@@ -1387,7 +1438,7 @@ struct orc_handle {
               GV = X_(6, I) * (X_(2, I) * GGV[c] / GLV[c] + X_(2, IM) * GGV[id(IM, J, K)] / GLV[id(IM, J, K)]);
               AIM = AYZ * X_(5, I) * GGX[c] * GV; ALI[c] = -AIM;
             } else if (IS >= 1) {
-              if (IB_(3, IS) == 4) { AIM = 2.0 * AYZ * X_(4, I) * GGX[c] * GGV[c] / GLV[c]; ALI[c] = 0.0; }
+              if (IB_(3, IS) == 4 || (IB_(3, IS) == 5 && I == 2 && FIXLVL(1))) { AIM = 2.0 * AYZ * X_(4, I) * GGX[c] * GGV[c] / GLV[c]; ALI[c] = 0.0; }
               else { AIM = 0.0; ALI[c] = 0.0; }
             } else return CADMAS_EPG;
             IS = INDX[id(IP, J, K)];
@@ -1395,7 +1446,7 @@ struct orc_handle {
               GV = X_(6, IP) * (X_(2, IP) * GGV[id(IP, J, K)] / GLV[id(IP, J, K)] + X_(2, I) * GGV[c] / GLV[c]);
               AIP = AYZ * X_(5, IP) * GGX[id(IP, J, K)] * GV; AUI[c] = -AIP;
             } else if (IS >= 1) {
-              if (IB_(3, IS) == 4) { AIP = 2.0 * AYZ * X_(4, I) * GGX[id(IP, J, K)] * GGV[c] / GLV[c]; AUI[c] = 0.0; }
+              if (IB_(3, IS) == 4 || (IB_(3, IS) == 5 && IP == NI && FIXLVL(2))) { AIP = 2.0 * AYZ * X_(4, I) * GGX[id(IP, J, K)] * GGV[c] / GLV[c]; AUI[c] = 0.0; }
               else { AIP = 0.0; AUI[c] = 0.0; }
             } else return CADMAS_EPG;
             IS = INDY[c];
@@ -1403,7 +1454,7 @@ struct orc_handle {
               GV = Y_(6, J) * (Y_(2, J) * GGV[c] / GLV[c] + Y_(2, JM) * GGV[id(I, JM, K)] / GLV[id(I, JM, K)]);
               AJM = AXZ * Y_(5, J) * GGY[c] * GV; ALJ[c] = -AJM;
             } else if (IS >= 1) {
-              if (IB_(3, IS) == 4) { AJM = 2.0 * AXZ * Y_(4, J) * GGY[c] * GGV[c] / GLV[c]; ALJ[c] = 0.0; }
+              if (IB_(3, IS) == 4 || (IB_(3, IS) == 5 && J == 2 && FIXLVL(3))) { AJM = 2.0 * AXZ * Y_(4, J) * GGY[c] * GGV[c] / GLV[c]; ALJ[c] = 0.0; }
               else { AJM = 0.0; ALJ[c] = 0.0; }
             } else return CADMAS_EPG;
             IS = INDY[id(I, JP, K)];
@@ -1411,7 +1462,7 @@ struct orc_handle {
               GV = Y_(6, JP) * (Y_(2, JP) * GGV[id(I, JP, K)] / GLV[id(I, JP, K)] + Y_(2, J) * GGV[c] / GLV[c]);
               AJP = AXZ * Y_(5, JP) * GGY[id(I, JP, K)] * GV; AUJ[c] = -AJP;
             } else if (IS >= 1) {
-              if (IB_(3, IS) == 4) { AJP = 2.0 * AXZ * Y_(4, J) * GGY[id(I, JP, K)] * GGV[c] / GLV[c]; AUJ[c] = 0.0; }
+              if (IB_(3, IS) == 4 || (IB_(3, IS) == 5 && JP == NJ && FIXLVL(4))) { AJP = 2.0 * AXZ * Y_(4, J) * GGY[id(I, JP, K)] * GGV[c] / GLV[c]; AUJ[c] = 0.0; }
               else { AJP = 0.0; AUJ[c] = 0.0; }
             } else return CADMAS_EPG;
             IS = INDZ[c];
@@ -1684,7 +1735,7 @@ struct orc_handle {
             double GV = X_(6, I) * (X_(2, I) * GGV[id(I, J, K)] / GLV[id(I, J, K)] +
                                     X_(2, I - 1) * GGV[id(I - 1, J, K)] / GLV[id(I - 1, J, K)]);
             UU[id(I, J, K)] = UU[id(I, J, K)] + X_(5, I) * GV * (PT[id(I, J, K)] - PT[id(I - 1, J, K)]);
-          } else if (IS > 0 && IB_(3, IS) == 4) {
+          } else if (IS > 0 && (IB_(3, IS) == 4 || (IB_(3, IS) == 5 && fixlvl_face(IB_(2, IS), I, J)))) {
             if (IB_(2, IS) == 1)
               UU[id(I, J, K)] = UU[id(I, J, K)] + 2.0 * X_(4, I) * GGV[id(I, J, K)] / GLV[id(I, J, K)] * PT[id(I, J, K)];
             else
@@ -1701,7 +1752,7 @@ struct orc_handle {
             double GV = Y_(6, J) * (Y_(2, J) * GGV[id(I, J, K)] / GLV[id(I, J, K)] +
                                     Y_(2, J - 1) * GGV[id(I, J - 1, K)] / GLV[id(I, J - 1, K)]);
             VV[id(I, J, K)] = VV[id(I, J, K)] + Y_(5, J) * GV * (PT[id(I, J, K)] - PT[id(I, J - 1, K)]);
-          } else if (IS > 0 && IB_(3, IS) == 4) {
+          } else if (IS > 0 && (IB_(3, IS) == 4 || (IB_(3, IS) == 5 && fixlvl_face(IB_(2, IS), I, J)))) {
             if (IB_(2, IS) == 3)
               VV[id(I, J, K)] = VV[id(I, J, K)] + 2.0 * Y_(4, J) * GGV[id(I, J, K)] / GLV[id(I, J, K)] * PT[id(I, J, K)];
             else
@@ -2105,7 +2156,7 @@ struct orc_handle {
         if (NS == 1 || NS == 2) { BCV[L - 1] = V1; BCW[L - 1] = V2; }
         else if (NS == 3 || NS == 4) { BCU[L - 1] = V1; BCW[L - 1] = V2; }
         else { BCU[L - 1] = V1; BCV[L - 1] = V2; }
-      } else if (IB == 1 || IB == 4) {
+      } else if (IB == 1 || IB == 4 || (IB == 5 && fixlvl_face(NS, I, J))) {  // vf_bwuwt.f:51-115
         if (NS == 1) { BCV[L - 1] = (VV[id(I, J, K)] + VV[id(I, J + 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5; }
         else if (NS == 2) { BCV[L - 1] = (VV[id(I - 1, J, K)] + VV[id(I - 1, J + 1, K)]) * 0.5; BCW[L - 1] = (WW[id(I - 1, J, K)] + WW[id(I - 1, J, K + 1)]) * 0.5; }
         else if (NS == 3) { BCU[L - 1] = (UU[id(I, J, K)] + UU[id(I + 1, J, K)]) * 0.5; BCW[L - 1] = (WW[id(I, J, K)] + WW[id(I, J, K + 1)]) * 0.5; }
@@ -3493,6 +3544,10 @@ struct orc_handle {
       if (rcs) return rcs;
     }
     feuler(FLFU, FLFV, FLFW);
+    {
+      const int rl = bwffsf();  // vf_f1cal.f:180
+      if (rl) return rl;
+    }
     fmod1();
     double fs, fc;
     fcut01(fs, fc);
@@ -3631,6 +3686,10 @@ int orc_get_state(orc_handle *h, cadmas_state *s) {
 // VF_CINIT vf_cinit.f:202-283 and the BC calls that follow it.
 int orc_init_state(orc_handle *h, int hydrostatic) {
   if (!h->have_static) return CADMAS_ENOSTATIC;
+  {
+    const int rl = h->bwffsf();  // vf_cinit.f:177
+    if (rl) return rl;
+  }
   double fs, fc;
   h->fcut01(fs, fc);
   h->st.fsum = fs; h->st.fcut = fc;
@@ -3743,7 +3802,7 @@ int orc_set_open(orc_handle *h, int side, double depth, double period) {
 int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
   if (!h || !w || !t || w->side < 1 || w->side > 4 || t->ntt < 2 || t->nzz < 2) return CADMAS_EINVAL;
   if (h->OP[w->side - 1].on) return CADMAS_EINVAL;
-  if (t->mtbtyp != 1 && t->mtbtyp != 2) return CADMAS_EUNSUPPORTED;
+  if (t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
   h->DMTBTT.assign(t->tt, t->tt + t->ntt);
   h->DMTBHH.assign(t->hh, t->hh + t->ntt);
   h->DMTBZZ.assign(t->zz, t->zz + t->nzz);

@@ -39,6 +39,9 @@ CASES = {
     "loglaw_tank_1_20": dict(builder="loglaw_tank", kw=dict(seed=1), steps=20, sum_mode=0, over={}),
     "loglaw_turb_tank_2_10": dict(builder="loglaw_tank", kw=dict(seed=2, turb=True), steps=10, sum_mode=0,
                                   over={}),
+    # fixed water level at X- (MTBTYP 3), open X+
+    "fixed_level_flume_20": dict(builder="fixed_level_flume", kw=dict(nx=48, nz=40, amp=0.04, T=2.0), steps=20,
+                                 sum_mode=0, over={}),
     # wave maker at X-, open (radiation) boundaries at X+ and Y+
     "open_flume_0_10": dict(builder="open_flume", kw=dict(nx=64, ny=4, nz=48, y_open=True), steps=10,
                             sum_mode=0, over={}),

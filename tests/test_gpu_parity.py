@@ -193,6 +193,19 @@ def test_loglaw_walls_larger_tank_tiles_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 10, check_every=5, precond_ti=16, precond_tj=8)
 
 
+def test_fixed_level_flume_bitwise(gpu_lib, pkg, orc):
+    """Fixed water level at X- (MTBTYP 3: free faces in VF_BWUWN, VF_VPCOEF,
+    VF_VMODIF and VF_BWUWT, F from the level in VF_BWFFSF) and an open X+
+    side: bit for bit."""
+    c = pkg.cases.fixed_level_flume()
+    run_pair(pkg, orc, c, 40, check_every=10)
+
+
+def test_fixed_level_flume_fade_in_tiles_bitwise(gpu_lib, pkg, orc):
+    c = pkg.cases.fixed_level_flume(nx=128, ny=16, nz=40, amp=0.08, T=1.5, ramp=0.5, open_end=False)
+    run_pair(pkg, orc, c, 24, check_every=8, precond_ti=16, precond_tj=8)
+
+
 def test_open_faces_need_an_open_side(gpu_lib, pkg):
     c = pkg.cases.open_flume(nx=32, ny=4, nz=32, depth=0.2, H=0.02)
     c.open = None
