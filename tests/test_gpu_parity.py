@@ -206,6 +206,19 @@ def test_fixed_level_flume_fade_in_tiles_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 24, check_every=8, precond_ti=16, precond_tj=8)
 
 
+def test_all_boundary_models_together_bitwise(gpu_lib, pkg, orc):
+    """Wave maker, open outlet, log-law and rough walls, k-epsilon and
+    FF-SLOPE in one flume: every field, k, e and the eddy viscosity bit for
+    bit."""
+    c = pkg.cases.open_flume(nx=96, ny=8, nz=48, depth=0.3, H=0.05, seed=3)
+    pkg.cases.turbulence(c)
+    pkg.cases.loglaw_walls(c, seed=3)
+    t, o = run_pair(pkg, orc, c, 20, check_every=5, iscmff=1, precond_ti=16, precond_tj=8)
+    tg, to = t.get_turb(), o.get_turb()
+    for k in ("ak", "ae", "anut", "anu", "bck", "bce"):
+        assert tg[k].tobytes() == to[k].tobytes(), k
+
+
 def test_open_faces_need_an_open_side(gpu_lib, pkg):
     c = pkg.cases.open_flume(nx=32, ny=4, nz=32, depth=0.2, H=0.02)
     c.open = None

@@ -161,3 +161,30 @@ def test_list_step_lines(gpu_lib, pkg):
     assert text == want
     assert re.fullmatch(r" STEP= {0,5}\d+ : TIME= .{12} : DT  = .{12} : FSUM= .{12} : FCUT= .{12} : !VD!= .{12}",
                         text.splitlines()[0])
+
+
+@pytest.mark.parametrize("builder", ["open_flume", "fixed_level_flume"])
+def test_restart_continues_wave_and_open_boundaries(gpu_lib, pkg, tmp_path, builder):
+    """The open boundary blends from the stored BCU/BCV/BCW and the fixed
+    level follows TNOW, both of which the restart records carry
+    (vf_or1trn.f:102-118): a run restarted at step 4 reaches step 10 bit
+    for bit."""
+    c = getattr(pkg.cases, builder)(nx=64, ny=4, nz=40) if builder == "open_flume" else \
+        pkg.cases.fixed_level_flume(nx=48, nz=40, amp=0.04, T=2.0)
+    path = tmp_path / "b.rsl"
+    t = pkg.Tank(c)
+    t.init_state(True)
+    t.restart_create(path)
+    for n in range(1, 11):
+        t.step(c.dt)
+        if n == 4:
+            t.restart_append(path)
+    ref = t.get_state()
+    u = pkg.Tank(c)
+    u.init_state(True)
+    u.restart_load(path, 4)
+    for n in range(6):
+        u.step(c.dt)
+    got = u.get_state()
+    for k in ("nf", "indc", "uu", "vv", "ww", "pp", "ff", "bcu", "bcv", "bcw", "bcp", "bcf"):
+        assert got[k].tobytes() == ref[k].tobytes(), k
