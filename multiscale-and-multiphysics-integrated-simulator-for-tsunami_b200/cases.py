@@ -742,15 +742,15 @@ def level_table(amp: float, ntt: int = 121, depth: float = 1.0) -> dict:
 
 
 def fixed_level_flume(nx=96, ny=4, nz=48, dx=0.05, dz=0.01, depth=0.3, amp=0.05, T=4.0, ramp=0.0,
-                      open_end=True) -> Case:
-    """Flume driven at X- by a fixed water level (WAVE-BC ... FUNC MATRIX
-    with MTBTYP 3) following `level_table`: the boundary faces act as free
+                      open_end=True, side=1) -> Case:
+    """Flume driven on side `side` (1 = X-) by a fixed water level (WAVE-BC
+    ... FUNC MATRIX with MTBTYP 3) following `level_table`: the boundary faces act as free
     faces and the column next to the side takes the level (VF_BWFFSF);
     with `open_end` the X+ side radiates (MODEL OPEN-BC)."""
     c = porous_flume(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, depth=depth,
                      block=(0.6 * nx * dx, 0.6 * nx * dx + 0.2, depth + amp), gamma=0.5)
     c.params.update(idamp=[-1, -1, -1, -1])
-    wave_maker(c, 2.0 * amp, T, depth, side=1, ramp=ramp, table=level_table(amp, depth=depth))
+    wave_maker(c, 2.0 * amp, T, depth, side=side, ramp=ramp, table=level_table(amp, depth=depth))
     if open_end:
         open_boundary(c, depth, T, side=2)
     c.name = "fixed_level_flume"

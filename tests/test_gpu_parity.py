@@ -206,6 +206,21 @@ def test_fixed_level_flume_fade_in_tiles_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 24, check_every=8, precond_ti=16, precond_tj=8)
 
 
+@pytest.mark.parametrize("side", [3, 4])
+def test_fixed_level_on_a_y_side_bitwise(gpu_lib, pkg, orc, side):
+    """The Y forms of the fixed-level rules (VF_VPCOEF's y faces,
+    VF_VMODIF's y loop, VF_BWUWT's NS 3/4, VF_BWFFSF's y column)."""
+    c = pkg.cases.fixed_level_flume(nx=48, ny=24, nz=40, amp=0.05, T=1.5, side=side)
+    run_pair(pkg, orc, c, 24, check_every=8, precond_ti=16, precond_tj=8)
+
+
+def test_open_y_minus_side_bitwise(gpu_lib, pkg, orc):
+    """An open Y- side (J = 2, the blend toward J = 3) beside the X+ one."""
+    c = pkg.cases.open_flume(nx=64, ny=12, nz=40, depth=0.25, H=0.04, seed=4)
+    pkg.cases.open_boundary(c, 0.25, 1.2, side=3)
+    run_pair(pkg, orc, c, 20, check_every=5)
+
+
 def test_all_boundary_models_together_bitwise(gpu_lib, pkg, orc):
     """Wave maker, open outlet, log-law and rough walls, k-epsilon and
     FF-SLOPE in one flume: every field, k, e and the eddy viscosity bit for
