@@ -1,23 +1,31 @@
 """Benchmark of the B200 SMAC step (CADMAS-SURF/3D VF_V1CAL + VF_F1CAL).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--case beach|flume|ensemble|unet]
 
-Workload (one GPU): the plain FP64 wave flume with a porous breakwater,
-512 x 32 x 96 cells (dx=dy=0.02 m, dz=0.01 m), still-water depth 0.5 m,
-porous block x in [6,7] m, z < 0.6 m, porosity 0.4, CM 1.2, CD 1.0, 2 m
-sponge at the outlet, dt = 2e-3 s, BiCGSTAB relative tolerance 1e-10.
-The wave H = 0.08 m, T = 1.5 s enters through a wave-maker boundary at
-x = 0 (the reference's matrix-table inflow, filled from first-order wave
-theory) and, so that the timed steps see the developed wave field, the
-same first-order wave train is also the initial state.
+Default workload (one GPU): the solitary wave on a 1:20 beach with 40
+seeded porous boxes, 1024 x 128 x 128 cells (dx=dy=0.02 m, dz=0.01 m,
+depth 0.6 m, amplitude 0.15 m, dt = 1e-3 s), pressure solved to a 1e-8
+relative residual.  Two solvers step it from the same initial state:
 
-One step = one full SMAC step on the GPU (momentum predictor, Poisson
-assembly, MILU-BiCGSTAB solve, correction, VOF advection and flags).
-value = interior cells x steps / device time (CUDA events on the library's
-stream) over all ranks; with N GPUs every rank runs its own replica of the
-flume (independent instances, no data exchange).  e2e = the same through
-the Fortran-callable entry point vf_step_gpu_ with the state in pinned host
-arrays copied in and out every step.
+  * plain: the reference's MILU-BiCGSTAB in FP64 (VF_M1BCGS, converged on
+    |M^-1 r| <= 1e-8 |M^-1 b| as the reference does);
+  * mixed: FP32 MILU factor and FP32 BiCGSTAB inner solves under FP64
+    iterative refinement, converged on the true residual
+    ||b - Ax|| <= 1e-8 ||b|| in FP64 (optionally with an initial guess:
+    --guess previous|learned).
+
+value = interior cells x steps / device time of the mixed solver's steps
+(CUDA events on the library's stream); the plain run's number, the ratio,
+the plain solver's roofline and the per-field error of the mixed run
+against the plain one after --acc-steps steps go into `config`.  With N
+GPUs every rank runs its own replica (independent instances, no data
+exchange).  e2e = the mixed run through the Fortran-callable entry point
+vf_step_gpu_ with the state in pinned host arrays copied in and out every
+step.
+
+--case flume: the plain FP64 wave flume with a porous breakwater, 512 x 32
+x 96 cells, tolerance 1e-10 (the reference's configuration of that run).
 """
 from __future__ import annotations
 
@@ -86,7 +94,7 @@ def combine_ranks(t_local: float, units_local: float, device=None):
 def build_case(args):
     P = _load_pkg()
     if getattr(args, "case", "flume") == "beach":
-        return P.cases.solitary_beach()
+        return P.cases.solitary_beach(nx=args.beach_nx, ny=args.beach_ny, nz=args.beach_nz)
     c = P.cases.porous_flume(nx=args.nx, ny=args.ny, nz=args.nz)
     P.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
     P.cases.wave_maker(c, 0.08, 1.5, 0.5)
@@ -97,7 +105,8 @@ def params_for(args):
     return dict(cgepsr=1.0e-8 if getattr(args, "case", "flume") == "beach" else 1.0e-10,
                 precond_ti=args.ti, precond_tj=args.tj, precond_split=getattr(args, "split", 1),
                 solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
-                warm_start={"zero": 0, "previous": 1, "learned": 2}[getattr(args, "guess", "zero")])
+                warm_start={"zero": 0, "previous": 1, "learned": 2}[getattr(args, "guess", "zero")],
+                mixed_eps_inner=getattr(args, "eps_inner", 1.0e-5))
 
 
 class ClockSampler:
@@ -167,17 +176,19 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(case, args, max_seconds=25.0, min_steps=1):
+def cpu_baseline(case, args, max_seconds=25.0, min_steps=1, warm=1):
     """The oracle (CPU restatement, reference summation order, its solver on
-    all host threads: one emulated rank per preconditioner block) on the
-    same flume: one warm-up step, then timed steps until max_seconds.
-    Returns Mcell-steps/s, steps, seconds and threads."""
+    all host threads: one emulated rank per preconditioner block, plain FP64
+    solver) on the same case: `warm` warm-up steps, then timed steps until
+    max_seconds.  Returns Mcell-steps/s, steps, seconds and threads."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     sys.path.pop(0)
-    o = pyoracle.Oracle(case, sum_mode=pyoracle.SUM_REF, **params_for(args))
+    prm = dict(params_for(args), solver=0, warm_start=0)
+    o = pyoracle.Oracle(case, sum_mode=pyoracle.SUM_REF, **prm)
     o.init_state(True)
-    o.step(case.dt)
+    for _ in range(warm):
+        o.step(case.dt)
     n, t0 = 0, time.perf_counter()
     while n < min_steps or (time.perf_counter() - t0 < max_seconds and n < 50):
         o.step(case.dt)
@@ -195,9 +206,12 @@ def run_reference(args, rank, world):
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     sys.path.pop(0)
-    o = pyoracle.Oracle(case, sum_mode=pyoracle.SUM_REF, **params_for(args))
+    # the reference's own solver: VF_M1BCGS in FP64 from PT = 0
+    o = pyoracle.Oracle(case, sum_mode=pyoracle.SUM_REF, **dict(params_for(args), solver=0, warm_start=0))
     o.init_state(True)
-    for _ in range(min(args.warmup, 1)):
+    beach = args.case == "beach"
+    nwarm = 0 if beach else min(args.warmup, 1)  # a beach step takes the oracle many seconds
+    for _ in range(nwarm):
         o.step(case.dt)
     n, t0 = 0, time.perf_counter()
     while n < args.steps and (n == 0 or time.perf_counter() - t0 < budget):
@@ -206,13 +220,15 @@ def run_reference(args, rank, world):
     dt = time.perf_counter() - t0
     v = case.interior_cells * n / dt / 1e6
     threads = pyoracle.num_threads()
-    sample = (f"{n} of {args.steps} steps of the {case.ni-2}x{case.nj-2}x{case.nk-2} flume after "
-              f"{min(args.warmup, 1)} warm-up step(s), {dt:.1f} s, oracle solver on {threads} OpenMP threads "
-              f"(one emulated rank per preconditioner block)")
+    what = "beach" if beach else "flume"
+    sample = (f"{n} of {args.steps} steps of the {case.ni-2}x{case.nj-2}x{case.nk-2} {what} after "
+              f"{nwarm} warm-up step(s), {dt:.1f} s, oracle (plain FP64 solver, reference summation order) "
+              f"on {threads} OpenMP threads (one emulated rank per preconditioner block)")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
-            "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / n,
+            "steps": n, "warmup": nwarm, "ms_per_step": 1e3 * dt / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": workload_config(case, args),
+            "solver": "plain FP64 MILU-BiCGSTAB (the reference's VF_M1BCGS) in the CPU oracle",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -222,11 +238,12 @@ def workload_config(case, args):
     solver = ("mixed FP32-inner/FP64-refinement" if getattr(args, "solver", "fp64") == "mixed"
               else "plain FP64")
     if getattr(args, "case", "flume") == "beach":
-        return {"workload": f"solitary wave on a 1:20 beach with 40 porous boxes "
-                            f"{case.ni-2}x{case.nj-2}x{case.nk-2} {solver} SMAC step (dt={case.dt}, "
-                            f"tol 1e-8, block-Jacobi MILU {args.ti}x{args.tj} columns)",
+        # the same for both arms: the solver of a line is its "solver" key
+        return {"workload": f"solitary wave on a 1:20 beach with 40 seeded porous boxes "
+                            f"{case.ni-2}x{case.nj-2}x{case.nk-2} SMAC step (dt={case.dt}, pressure to a "
+                            f"1e-8 relative residual, block-Jacobi MILU {args.ti}x{args.tj} columns)",
                 "cells": case.interior_cells, "precond_block": [args.ti, args.tj],
-                "l2": "inputs larger than L2"}
+                "l2": "inputs larger than L2 (about 60 arrays of 139 MB resident)"}
     if getattr(args, "guess", "zero") == "previous":
         solver += ", previous-step initial guess,"
     if getattr(args, "guess", "zero") == "learned":
@@ -422,6 +439,242 @@ def run_ours(args, rank, world, local_rank):
     tank.close()
 
 
+# Algorithmic bytes per interior cell of the FP32 sweeps of the mixed
+# solver (the same arrays as the FP64 ones, 4 B each).
+STAGE_BYTES_F32 = {"fwd": 10 * 4, "bwd": 6 * 4}
+
+
+def roofline_of(stages, cells, peak, peak_kind, bytes_table, traffic_per_cell=None):
+    """Roofline object of the stage with the largest device time among the
+    stages whose algorithmic bytes are known."""
+    dom = max((k for k in bytes_table), key=lambda k: stages[k][0])
+    ms_dom, n_dom = stages[dom]
+    bytes_launch = bytes_table[dom] * cells
+    achieved = bytes_launch / (ms_dom / n_dom / 1e3) / 1e9 if n_dom else 0.0
+    total_ms = sum(v[0] for v in stages.values())
+    tr = traffic_per_cell.get(dom) if traffic_per_cell else None
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": tr * cells if tr is not None else None,
+            "algorithmic_bytes_per_launch": bytes_launch, "launches": n_dom,
+            "avg_launch_ms": ms_dom / n_dom if n_dom else None,
+            "share_of_step": ms_dom / total_ms if total_ms else None}
+
+
+# DRAM bytes per interior cell of one launch of the dominant sweeps on the
+# beach (1024x128x128, 16x16 tiles), from ncu captures of a smaller beach
+# of the same tile shape (traffic per launch scales with the cells).
+NCU_TRAFFIC_BEACH = {"fwd": None, "bwd": None}
+NCU_TRAFFIC_BEACH_F32 = {"fwd": None, "bwd": None}
+
+
+def field_errors(a, b, case):
+    """Per-field max-abs and RMS of a - b over the interior cells, with the
+    max-abs of b for scale; NF mismatches."""
+    sl = (slice(1, case.ni - 1), slice(1, case.nj - 1), slice(1, case.nk - 1))
+    out = {}
+    for n, lab in (("ff", "F"), ("pp", "p"), ("uu", "u"), ("vv", "v"), ("ww", "w")):
+        d = (a[n][sl] - b[n][sl]).ravel()
+        ref = np.abs(b[n][sl]).max()
+        out[lab] = {"max_abs": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d))),
+                    "ref_max_abs": float(ref)}
+    out["nf_mismatch_cells"] = int((a["nf"][sl] != b["nf"][sl]).sum())
+    return out
+
+
+def run_headline(args, rank, world, local_rank):
+    """Config 2 (the solitary beach): the plain FP64 solver and the mixed
+    solver (with the chosen initial guess) from the same initial state."""
+    import torch
+    import torch.distributed as dist
+    P = _load_pkg()
+    if rank == 0:
+        P.build_library()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    case = build_case(args)
+    cells = case.interior_cells
+    base = {k: v for k, v in params_for(args).items() if k not in ("solver", "warm_start")}
+    arms = {"plain": dict(base, solver=0, warm_start=0),
+            "mixed": dict(base, solver=1, warm_start={"zero": 0, "previous": 1, "learned": 2}[args.guess])}
+    learned = None
+    if args.guess == "learned":
+        # train the guess on the solver's own solves of the first steps
+        # (outside the timing)
+        import importlib
+        ws = importlib.import_module(P.__name__ + ".warmstart")
+        t0 = time.time()
+        samples = ws.collect(case, args.train_steps, precond_ti=args.ti, precond_tj=args.tj)
+        wparams, cscale = ws.train(samples, epochs=args.train_epochs, batch=1, lr=1.0e-3, w_mse=0.1, w_res=1.0)
+        learned = {"train_steps": args.train_steps, "epochs": args.train_epochs,
+                   "train_s": round(time.time() - t0, 1), "out_scale": cscale}
+        del samples
+    res = {}
+    tanks = {}
+    for name in ("plain", "mixed"):
+        tank = P.Tank(case, **arms[name])
+        if name == "mixed" and learned is not None:
+            tank.set_warm_net(wparams, cscale)
+        tank.init_state(True)
+        stream = torch.cuda.ExternalStream(tank.stream(), device=dev)
+        for _ in range(args.warmup):
+            tank.step(case.dt)
+        tank.sync()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        iters = []
+        l0 = P.kernel_launches()
+        with ClockSampler(local_rank) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                tank.step(case.dt)
+                iters.append(tank.stats()["icgitr"])
+            ev1.record(stream)
+            ev1.synchronize()
+        torch.cuda.synchronize()
+        launches = P.kernel_launches() - l0
+        t_ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            dist.barrier()
+        t_max, units = combine_ranks(t_ms / 1e3, cells * args.steps, device=dev)
+        res[name] = {"value": units / t_max / 1e6, "ms_per_step": t_max * 1e3 / args.steps,
+                     "mean_iters": float(np.mean(iters)), "launches": launches, "clocks": clk.summary(),
+                     "stream": stream}
+        tanks[name] = tank
+    # Continue both runs (untimed, per-stage event timers on) to the
+    # accuracy horizon, then compare the fields.
+    n_done = args.warmup + args.steps
+    n_acc = max(args.acc_steps, n_done)
+    stage = {}
+    for name, tank in tanks.items():
+        tank.stage_timers(enable=1)
+        nst = 0
+        while n_done + nst < n_acc or nst < min(args.steps, 5):
+            tank.step(case.dt)
+            nst += 1
+        tank.sync()
+        stage[name] = (tank.stage_timers(enable=0), nst)
+    n_acc = n_done + stage["plain"][1]
+    sp, sm = tanks["plain"].get_state(), tanks["mixed"].get_state()
+    stp, stm = tanks["plain"].stats(), tanks["mixed"].stats()
+    f0 = None
+    try:
+        f0 = float(np.sum(case.ff[1:-1, 1:-1, 1:-1] * case.ggv[1:-1, 1:-1, 1:-1]))
+    except Exception:
+        f0 = None
+    acc = {"steps": n_acc, "fields_mixed_minus_plain": field_errors(sm, sp, case),
+           "fsum_plain": stp["fsum"], "fsum_mixed": stm["fsum"],
+           "volume_drift_rel": abs(stm["fsum"] - stp["fsum"]) / abs(stp["fsum"]) if stp["fsum"] else None,
+           "mixed_last_solve_true_relres": (stm["cgxnrm"] / stm["cgbnrm"]) if stm["cgbnrm"] else None,
+           "mixed_fp64_fallbacks": stm["fallbacks"]}
+    if learned is not None:
+        kept, dropped = tanks["mixed"].warm_stats()
+        learned.update(kept=kept, dropped=dropped)
+    # True residual of one plain solve from the plain run's state
+    # (diagnostic outside the timing: one more handle with the check on).
+    relres_plain = None
+    try:
+        t2 = P.Tank(case, diag_relres=1, **arms["plain"])
+        t2.set_state(sp)
+        t2.step(case.dt)
+        relres_plain = t2.stats()["true_relres"]
+        t2.close()
+    except Exception:
+        relres_plain = None
+    tanks["plain"].close()
+    # ---- e2e through vf_step_gpu_ with pinned host buffers (mixed solver)
+    tank = tanks["mixed"]
+    stream = res["mixed"]["stream"]
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_run(P, tank, case, stream, args, world, dev)
+    peak, peak_kind = measured_peak_hbm()
+    st_p, nst_p = stage["plain"]
+    st_m, nst_m = stage["mixed"]
+    roof_plain = roofline_of(st_p, cells, peak, peak_kind, STAGE_BYTES, NCU_TRAFFIC_BEACH)
+    bytes_m = dict(STAGE_BYTES)
+    bytes_m.update(STAGE_BYTES_F32)
+    roof_mixed = roofline_of(st_m, cells, peak, peak_kind, bytes_m, NCU_TRAFFIC_BEACH_F32)
+    tank.close()
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu:
+        v_cpu, n_cpu, t_cpu, thr = cpu_baseline(case, args, warm=0)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"{n_cpu} step(s) of the same beach from its initial state, {t_cpu:.1f} s, "
+                         f"oracle (reference summation order, plain FP64 solver) on {thr} OpenMP threads"}
+    rp, rm = res["plain"], res["mixed"]
+    guess = {"zero": "zero initial guess", "previous": "previous-step initial guess",
+             "learned": "learned initial guess"}[args.guess]
+    line = {"metric": METRIC, "value": rm["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": rm["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "config": workload_config(case, args),
+            "solver": f"mixed FP32-inner/FP64-refinement with {guess}",
+            "parallelism": f"replicas x{world}",
+            "arms": {"mixed": {"value": rm["value"], "ms_per_step": rm["ms_per_step"],
+                               "mean_inner_iters": rm["mean_iters"], "eps_inner_floor": args.eps_inner,
+                               "roofline": roof_mixed,
+                               "stage_ms_per_step": {k: v[0] / nst_m for k, v in st_m.items()}},
+                     "plain_fp64": {"value": rp["value"], "ms_per_step": rp["ms_per_step"],
+                                    "mean_bicgstab_iters": rp["mean_iters"], "true_relres": relres_plain,
+                                    "roofline": roof_plain, "clocks": rp["clocks"],
+                                    "stage_ms_per_step": {k: v[0] / nst_p for k, v in st_p.items()}}},
+            "speedup_vs_plain_fp64": rm["value"] / rp["value"],
+            "plain_fp64_roofline_frac": roof_plain["frac"],
+            "accuracy": acc,
+            **({"learned_guess": learned} if learned is not None else {}),
+            "roofline": roof_mixed, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": rm["launches"],
+            "clocks": rm["clocks"]}
+    print(json.dumps(line), flush=True)
+
+
+def e2e_run(P, tank, case, stream, args, world, dev):
+    """The same steps through vf_step_gpu_ with the state in pinned host
+    arrays, copied in and out every step."""
+    import torch
+    import torch.distributed as dist
+    keep, arrs = pinned_state(P, case, torch)
+    st = tank.get_state()
+    for n in arrs:
+        arrs[n][...] = st[n][: arrs[n].shape[0]] if arrs[n].ndim == 1 else st[n]
+    lib = tank.lib
+    hp = ctypes.c_void_p(tank.h.value)
+    dtc = ctypes.c_double(case.dt)
+    tnow = ctypes.c_double(st["tnow"])
+    nnow = ctypes.c_int(st["nnow"])
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    argv = [ctypes.byref(hp), ctypes.byref(dtc), dp(arrs["uu"]), dp(arrs["vv"]), dp(arrs["ww"]),
+            dp(arrs["pp"]), dp(arrs["ff"]), ip(arrs["nf"]), ip(arrs["indc"]), dp(arrs["bcu"]),
+            dp(arrs["bcv"]), dp(arrs["bcw"]), dp(arrs["bcp"]), dp(arrs["bcf"]), ctypes.byref(tnow),
+            ctypes.byref(nnow)]
+    nsteps_e2e = max(1, min(args.steps, 10))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(nsteps_e2e):
+        rc = lib.vf_step_gpu_(*argv)
+        if rc != 0:
+            raise P.CadmasError(rc, "vf_step_gpu_")
+    e1.record(stream)
+    e1.synchronize()
+    te_max, ue = combine_ranks(e0.elapsed_time(e1) / 1e3, case.interior_cells * nsteps_e2e, device=dev)
+    bytes_io = sum(a.nbytes for a in arrs.values())
+    return {"value": ue / te_max / 1e6, "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+            "d2h_bytes_per_step": bytes_io, "steps": nsteps_e2e,
+            "path": "vf_step_gpu_ (pinned host state in/out every step)"}
+
+
 def measured_peak_bf16():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -556,9 +809,18 @@ def main():
     ap.add_argument("--autotune", action="store_true",
                     help="--case ensemble: preconditioner block shape per member by the tile autotuner")
     ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
-    ap.add_argument("--case", choices=["flume", "beach", "ensemble", "unet"], default="flume",
-                    help="flume: 512x32x96 porous wave flume (default); beach: 1024x128x128 solitary "
-                         "wave on a 1:20 beach with 40 porous boxes; unet: the learned guess's network alone")
+    ap.add_argument("--case", choices=["flume", "beach", "ensemble", "unet"], default="beach",
+                    help="beach: 1024x128x128 solitary wave on a 1:20 beach with 40 porous boxes, plain "
+                         "FP64 and mixed solvers (default); flume: 512x32x96 porous wave flume; "
+                         "unet: the learned guess's network alone")
+    ap.add_argument("--acc-steps", type=int, default=200,
+                    help="--case beach: steps after which the mixed run's fields are compared with the "
+                         "plain run's")
+    ap.add_argument("--eps-inner", type=float, default=1.0e-5,
+                    help="floor of the FP32 inner tolerance of the mixed solver")
+    ap.add_argument("--beach-nx", type=int, default=1024)
+    ap.add_argument("--beach-ny", type=int, default=128)
+    ap.add_argument("--beach-nz", type=int, default=128)
     ap.add_argument("--unet-volume", default="64x32x64", help="--case unet: XxYxZ (multiples of 4)")
     ap.add_argument("--train-steps", type=int, default=40,
                     help="--guess learned: steps whose solves train the network")
@@ -592,6 +854,8 @@ def main():
             run_ensemble(args, rank, world, local_rank)
         elif args.case == "unet":
             run_unet(args, rank, world, local_rank)
+        elif args.case == "beach":
+            run_headline(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

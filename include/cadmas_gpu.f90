@@ -49,6 +49,8 @@ module cadmas_gpu
      real(c_double) :: anu0, scmk, akmink, akmine, akinik, akinie
      real(c_double) :: akcmu, aksgk, aksge, akc1, akc2, akc3
      real(c_double) :: akk0, aka0                ! log law (IB 6, 8)
+     real(c_double) :: mixed_eps_inner           ! floor of the FP32 inner tolerance (solver 1)
+     real(c_double) :: wait_limit_s              ! device-side wait limit, seconds
   end type cadmas_params
 
   ! c_loc() of the static arrays (XX(6,NUMI) ... INDB(4,NUMB))

@@ -144,6 +144,17 @@ typedef struct cadmas_params {
      walls (8) use ln(y / ks) / kappa + A + 3 (VF_CLOGKS)
      (vf_a2dflt.f:175-176, input 'MODEL LOG-LAW', vf_iimdl.f:288-291).      */
   double akk0, aka0;
+  /* Inner tolerance of the mixed-precision solver (solver 1; no
+     counterpart in the reference).  Each FP32 inner solve is asked for
+     the reduction the FP64 residual still needs to reach CGEPSR, times
+     0.5, but not below this floor (FP32 sweeps stop gaining near 1e-6).
+     0 = the default 1e-5.                                                */
+  double mixed_eps_inner;
+  /* Time limit in seconds of every device-side wait of the MILU sweeps
+     (their bulk-copy mbarriers): a wait that runs out ends the solve
+     with CADMAS_ETIMEOUT and leaves the handle usable.  0 = the default
+     2 s.                                                                 */
+  double wait_limit_s;
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */
@@ -476,12 +487,26 @@ int cadmas_m1bcgs_dev(cadmas_handle *h,
        another.
      - The first call on a device looks the scratch up
        (cudaGetSymbolAddress) and may load the module; make it before any
-       phase that must not see such set-up work.                          */
+       phase that must not see such set-up work.
+     - `stream` must belong to the current device: the scratch address
+       is the current device's.  A stream of another device gets
+       CADMAS_EINVAL and nothing runs.
+     - A CUDA error that earlier work left pending is reported as
+       CADMAS_ECUDA before anything is launched; cadmas_strerror names
+       the failing call.                                                  */
 #define CADMAS_NOALLOC_MAX_ROWS 65536
 int cadmas_divnorm_noalloc(const cadmas_dims *d, const double *xx, const double *yy,
                            const double *zz, const double *ggx, const double *ggy,
                            const double *ggz, const double *uu, const double *vv,
                            const double *ww, const int *indc, void *stream, double *val);
+
+/* Failure injection for tests (no counterpart in the reference): from
+   wavefront step `from_step` on (>= 0), the MILU sweeps of this handle
+   issue no bulk copies, so their bounded waits run out after
+   wait_limit_s and the next solve returns CADMAS_ETIMEOUT; the kernels
+   end normally and the handle stays usable.  A negative from_step turns
+   the injection off.                                                    */
+int cadmas_test_stall_sweeps(cadmas_handle *h, int from_step);
 
 /* The CUDA stream (cudaStream_t) on which every call of the handle issues
    its work; callers may record CUDA events on it or wait on it. */

@@ -75,7 +75,8 @@ class Params(C.Structure):
         ("diag_relres", C.c_int), ("solver", C.c_int), ("warm_start", C.c_int), ("precond_split", C.c_int),
         ("idrop", C.c_int), ("iscmff", C.c_int), ("leqk", C.c_int), ("pad0", C.c_int)] + [
         (n, C.c_double) for n in ("anu0", "scmk", "akmink", "akmine", "akinik", "akinie", "akcmu", "aksgk",
-                                  "aksge", "akc1", "akc2", "akc3", "akk0", "aka0")]
+                                  "aksge", "akc1", "akc2", "akc3", "akk0", "aka0",
+                                  "mixed_eps_inner", "wait_limit_s")]
 
 
 class Static(C.Structure):
@@ -107,7 +108,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_unet_param_count", "cadmas_unet_create", "cadmas_unet_destroy", "cadmas_unet_set_params",
             "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step",
             "cadmas_set_warm_net", "cadmas_warm_stats", "cadmas_get_solve", "cadmas_get_system",
-            "cadmas_unet_train_sys", "cadmas_unet_time_forward"]
+            "cadmas_unet_train_sys", "cadmas_unet_time_forward", "cadmas_test_stall_sweeps"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
@@ -521,11 +522,11 @@ class Tank:
     def set_time(self, tnow, dtnow, nnow):
         _check(self.lib, self.lib.cadmas_set_time(self.h, float(tnow), float(dtnow), int(nnow)))
 
-    def v1cal(self):
-        _check(self.lib, self.lib.cadmas_v1cal(self.h))
-
-    def f1cal(self):
-        _check(self.lib, self.lib.cadmas_f1cal(self.h))
+    def test_stall_sweeps(self, from_step):
+        """Failure injection: the MILU sweeps issue no bulk copies from
+        wavefront step `from_step` on (negative: off), so their bounded
+        waits run out (cadmas_test_stall_sweeps)."""
+        _check(self.lib, self.lib.cadmas_test_stall_sweeps(self.h, int(from_step)))
 
     def divnorm(self):
         v = C.c_double()

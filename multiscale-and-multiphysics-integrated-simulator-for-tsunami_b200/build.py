@@ -34,14 +34,32 @@ def needs_build() -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
+OBJ = HERE / "_build"
+
+
 def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
+    """Compile each source to an object file in parallel (no device code
+    crosses files), then link the shared object."""
     if not force and not needs_build():
         return LIB
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, *FLAGS, "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+    from concurrent.futures import ThreadPoolExecutor
+    OBJ.mkdir(exist_ok=True)
+    compile_flags = [f for f in FLAGS if f != "-shared"]
+    cmds = [[nvcc(), *ARCH, *compile_flags, "-c", "-o", str(OBJ / (s[:-3] + ".o")), str(CSRC / s)]
+            for s in SOURCES]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c))
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for c, r in zip(cmds, results):
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed: {' '.join(c)}\n{r.stdout}{r.stderr}")
+    tmp = LIB.with_suffix(".so.tmp")
+    link = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *[str(OBJ / (s[:-3] + ".o")) for s in SOURCES]]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB
 

@@ -554,9 +554,14 @@ static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int 
     if (r2 <= tol2 * b2) { converged = true; break; }
     const double rn = std::sqrt(r2);
     launch_scale_to_f(s, q, ic, h->y2, 1.0 / rn, h->bf);
-    // each pass reduces the residual by about the inner tolerance
+    // Each pass reduces the residual by about its inner tolerance: ask
+    // for half the reduction still needed, no less than the FP32 floor,
+    // so the last pass stops near CGEPSR instead of far below it.
+    const double need = std::sqrt(tol2 * b2 / r2);
+    const double floor_eps = h->P.mixed_eps_inner > 0.0 ? h->P.mixed_eps_inner : 1.0e-5;
+    const double eps_in = std::min(0.5, std::max(0.5 * need, floor_eps));
     int it = 0;
-    int rc = solve_inner_f(h, 1.0e-5, it);
+    int rc = solve_inner_f(h, eps_in, it);
     if (rc) return rc;
     if (it < 0 || it > h->P.icgmax) {  // factor, divergence or cap: FP64 takes over
       h->mixed_fallback++;
@@ -729,6 +734,10 @@ static void do_kpost(cadmas_handle *h) {
   launch_bwke(s, h->g, h->f, ke_arrays(h), h->dint);
   launch_bwuwt(s, h->g, h->f, h->p, h->dint);
   TE();
+}
+
+void cadmas::set_cuda_error(const char *call, cudaError_t e) {
+  g_last_error = std::string(call) + ": " + cudaGetErrorString(e);
 }
 
 // ------------------------------------------ kernel shared-memory limits
@@ -929,6 +938,8 @@ void cadmas_default_params(cadmas_params *p) {
   p->akmink = 1.0e-20; p->akmine = 1.0e-20; p->akinik = 1.0e-20; p->akinie = 1.0e-20;
   p->akcmu = 0.09; p->aksgk = 1.0; p->aksge = 1.3; p->akc1 = 1.44; p->akc2 = 1.92; p->akc3 = 0.0;
   p->akk0 = 0.4; p->aka0 = 5.5;  // vf_a2dflt.f:175-176
+  p->mixed_eps_inner = 1.0e-5;
+  p->wait_limit_s = 2.0;
 }
 
 int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **out) {
@@ -975,6 +986,11 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   h->q.W = (d->numk - 2) + (TI - 1) + (TJl - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJl - 1) / TJl);
+  {
+    const double lim = p->wait_limit_s > 0.0 ? std::min(p->wait_limit_s, 60.0) : 2.0;
+    h->q.wait_ns = (long long)(lim * 1.0e9);
+    h->q.stall_from = 1 << 30;
+  }
   if (!sweep_supported(h->q)) {
     g_last_error = "preconditioner block too large for the MILU sweeps; set precond_ti/precond_tj";
     rc = CADMAS_EUNSUPPORTED;
@@ -1729,6 +1745,12 @@ int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st) {
   if (!h || !st) return CADMAS_EINVAL;
   h->stats.fallbacks = (int)h->mixed_fallback;
   *st = h->stats;
+  return CADMAS_OK;
+}
+
+int cadmas_test_stall_sweeps(cadmas_handle *h, int from_step) {
+  if (!h) return CADMAS_EINVAL;
+  h->q.stall_from = from_step >= 0 ? from_step : (1 << 30);
   return CADMAS_OK;
 }
 

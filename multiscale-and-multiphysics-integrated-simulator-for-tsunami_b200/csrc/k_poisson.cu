@@ -410,8 +410,8 @@ __device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, 2000000000ull);
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
+  return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, limit_ns);
 }
 
 // ------------------------------------- cluster exchange (precond_split 2)
@@ -448,17 +448,17 @@ __device__ __forceinline__ bool mbar_try_cluster(unsigned bar, unsigned parity) 
       : "memory");
   return ok != 0;
 }
-// Bounded wait (2 s) acquiring what other CTAs of the cluster released.
-__device__ __noinline__ bool mbar_wait_cluster_slow(unsigned bar, unsigned parity) {
+// Bounded wait (limit_ns) acquiring what other CTAs of the cluster released.
+__device__ __noinline__ bool mbar_wait_cluster_slow(unsigned bar, unsigned parity, unsigned long long limit_ns) {
   const unsigned long long t0 = global_ns();
   for (;;) {
     for (int i = 0; i < 64; ++i)
       if (mbar_try_cluster(bar, parity)) return true;
-    if (global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
-__device__ __forceinline__ bool mbar_wait_cluster(unsigned bar, unsigned parity) {
-  return mbar_try_cluster(bar, parity) || mbar_wait_cluster_slow(bar, parity);
+__device__ __forceinline__ bool mbar_wait_cluster(unsigned bar, unsigned parity, unsigned long long limit_ns) {
+  return mbar_try_cluster(bar, parity) || mbar_wait_cluster_slow(bar, parity, limit_ns);
 }
 __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release;\nbarrier.cluster.wait.acquire;\n" ::: "memory");
@@ -587,8 +587,9 @@ __global__ void __launch_bounds__(MAXT, 1)
     src0 = (l0.arr == 0 ? S.sys : vin) + l0.base;
   else { l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; }
   const unsigned bar0 = smem_u32(bar), ring0 = smem_u32(ring);
+  const unsigned long long wait_ns = (unsigned long long)q.wait_ns;
   auto issue = [&](int u, int slot) {
-    if (u >= nsteps) return;
+    if (u >= nsteps || u >= q.stall_from) return;
     const int w = (MODE == SWEEP_BWD) ? nsteps - 1 - u : u;
     const unsigned bslot = bar0 + 8u * slot;
     const unsigned dslot = ring0 + (unsigned)ES * (unsigned)(slot * SS);
@@ -600,7 +601,7 @@ __global__ void __launch_bounds__(MAXT, 1)
   };
   // data of step u sits in slot u % R, phase (u / R) & 1
   auto wait_data = [&](int u, int slot, unsigned parity) -> bool {
-    return u >= nsteps || mbar_wait(bar0 + 8u * slot, parity);
+    return u >= nsteps || mbar_wait(bar0 + 8u * slot, parity, wait_ns);
   };
 
   if (producer) {
@@ -671,12 +672,12 @@ __global__ void __launch_bounds__(MAXT, 1)
   bool ok = true;
   if (!producer) {
     for (int u = 0; u < AHEAD; ++u) if (ok) ok = wait_data(u, u % R, (unsigned)((u / R) & 1));
-    if (CS == 2 && ok && rrow && col && 0 >= slo && 0 <= shi) ok = mbar_wait_cluster(smem_u32(xfull + lag), 0u);
+    if (CS == 2 && ok && rrow && col && 0 >= slo && 0 <= shi) ok = mbar_wait_cluster(smem_u32(xfull + lag), 0u, wait_ns);
     if (ok) prepare(0, slot_ptr(0), slot_ptr(R - 1), slot_ptr(1 % R));
     else s_abort[0] = 1;
   }
   bool aborted = false;
-  int issued = min(D, nsteps) - 1;  // last step whose copies were issued (producer)
+  int issued = min(min(D, nsteps), q.stall_from) - 1;  // last step whose copies were issued (producer)
   unsigned ph = 0;                  // (s0 / R) & 1, also the ring cycle's s_abort entry
 #pragma unroll 1
   for (int s0 = 0; s0 < nsteps && !aborted; s0 += R, ph ^= 1u) {
@@ -686,7 +687,7 @@ __global__ void __launch_bounds__(MAXT, 1)
       if (s >= nsteps) break;
       if (producer) {
         issue(s + D, (r + D) % R);
-        if (s + D < nsteps) issued = s + D;
+        if (s + D < nsteps && s + D < q.stall_from) issued = s + D;
       } else {
         // Test the data of the step to prepare next now, so the test's
         // latency overlaps the recurrence; wait only if it is not there.
@@ -723,11 +724,11 @@ __global__ void __launch_bounds__(MAXT, 1)
         }
         // prepare step s+1
         if (!ready) {
-          ok = mbar_wait_slow(ubar, upar, 2000000000ull);
+          ok = mbar_wait_slow(ubar, upar, wait_ns);
           if (!ok) s_abort[ph] = 1;
         }
         if (CS == 2 && ok && rrow && col && s + 1 >= slo && s + 1 <= shi) {
-          ok = mbar_wait_cluster(smem_u32(xfull + (s + 1 + lag)), 0u);
+          ok = mbar_wait_cluster(smem_u32(xfull + (s + 1 + lag)), 0u, wait_ns);
           if (!ok) s_abort[ph] = 1;
         }
         if (ok && s + 1 < nsteps) prepare(s + 1, slot_ptr((r + 1) % R), slot_ptr(r), slot_ptr((r + 2) % R));

@@ -14,6 +14,9 @@ inline void count_launch(long long n = 1) { g_kernel_launches.fetch_add(n, std::
 // stepped from several host threads at once never take it away from one
 // another's launches.
 void raise_dynamic_smem(const void *kern, size_t bytes);
+// Record the failing CUDA call and its message as the text cadmas_strerror
+// gives for CADMAS_ECUDA on this host thread.
+void set_cuda_error(const char *call, cudaError_t e);
 
 // The eight arrays of the Poisson system, WK01..WK08 of VF_V1CAL.
 struct SysPtr {
@@ -39,6 +42,13 @@ struct SkewGeo {
   int TI, TJ, TIp, T, W;  // layout tile TI x TJ columns (T = TIp*TJ slots), W slabs per tile
   int ntx, nb;            // layout tiles along x, tiles in total
   int split;  // layout tiles per preconditioner block along y (1 or 2)
+  // Bounded waits of the sweeps: an mbarrier wait gives up after wait_ns
+  // nanoseconds and the solve ends with CADMAS_ETIMEOUT.  stall_from: the
+  // producer warp issues no bulk copy for wavefront steps >= stall_from
+  // (failure injection for tests, cadmas_test_stall_sweeps; a large value
+  // in normal runs), so the waits of those steps run out.
+  long long wait_ns;
+  int stall_from, pad_;
 };
 
 __host__ __device__ inline long long sys_at(long long slab, int c, int T, int t) {

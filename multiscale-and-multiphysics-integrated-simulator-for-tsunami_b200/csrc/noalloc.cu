@@ -29,7 +29,13 @@
 //   - the first call on a device looks up the scratch's device address
 //     (cudaGetSymbolAddress, which may load the module); make that first
 //     call before anything that must not see such set-up work, e.g.
-//     before stream capture begins.
+//     before stream capture begins;
+//   - `stream` must belong to the current device (the scratch address is
+//     the current device's); a stream of another device gets
+//     CADMAS_EINVAL and nothing runs;
+//   - a CUDA failure returns CADMAS_ECUDA with the failing call and its
+//     message in cadmas_strerror; an error that earlier work left pending
+//     is not blamed on this call: it is reported before any launch.
 #include <cuda_runtime.h>
 #include <atomic>
 #include <cmath>
@@ -59,7 +65,11 @@ int scratch_for(int dev, double **out) {
     p = g_scratch_ptr[dev].load(std::memory_order_acquire);
     if (!p) {
       void *addr = nullptr;
-      if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return CADMAS_ECUDA;
+      const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+      if (e != cudaSuccess || !addr) {
+        set_cuda_error("cudaGetSymbolAddress(g_noalloc_scratch)", e != cudaSuccess ? e : cudaErrorInvalidSymbol);
+        return CADMAS_ECUDA;
+      }
       p = static_cast<double *>(addr);
       g_scratch_ptr[dev].store(p, std::memory_order_release);
     }
@@ -78,8 +88,31 @@ extern "C" int cadmas_divnorm_noalloc(const cadmas_dims *d, const double *xx, co
   if (d->numi < 3 || d->numj < 3 || d->numk < 3) return CADMAS_EINVAL;
   const long long rows = (long long)d->numj * d->numk;
   if (rows > CADMAS_NOALLOC_MAX_ROWS) return CADMAS_ESCRATCH;
+#define NA_CK(call)                        \
+  do {                                     \
+    const cudaError_t e_ = (call);         \
+    if (e_ != cudaSuccess) {               \
+      set_cuda_error(#call, e_);           \
+      return CADMAS_ECUDA;                 \
+    }                                      \
+  } while (0)
+  // an error left pending by the caller's earlier work is theirs: report
+  // it as such before this call launches anything
+  {
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+      set_cuda_error("error pending before cadmas_divnorm_noalloc", pending);
+      return CADMAS_ECUDA;
+    }
+  }
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess) return CADMAS_ECUDA;
+  NA_CK(cudaGetDevice(&dev));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (s != nullptr) {  // the legacy/default stream follows the current device
+    int sdev = -1;
+    NA_CK(cudaStreamGetDevice(s, &sdev));
+    if (sdev != dev) return CADMAS_EINVAL;
+  }
   double *scratch = nullptr;
   int rc = scratch_for(dev, &scratch);
   if (rc) return rc;
@@ -93,14 +126,14 @@ extern "C" int cadmas_divnorm_noalloc(const cadmas_dims *d, const double *xx, co
   f.uu = const_cast<double *>(uu); f.vv = const_cast<double *>(vv); f.ww = const_cast<double *>(ww);
   f.indc = const_cast<int *>(indc);
 
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   double *res = scratch + CADMAS_NOALLOC_MAX_ROWS;  // k_fin writes res[0], res[1]
   launch_cdiv(s, g, f, scratch);
   launch_fin(s, FIN_STORE, scratch, scratch, rows, nullptr, res, 0, 0, 0, 0);
-  if (cudaGetLastError() != cudaSuccess) return CADMAS_ECUDA;
+  NA_CK(cudaGetLastError());
   double h = 0.0;
-  if (cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return CADMAS_ECUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return CADMAS_ECUDA;
+  NA_CK(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, s));
+  NA_CK(cudaStreamSynchronize(s));
   *val = std::sqrt(h);
   return CADMAS_OK;
+#undef NA_CK
 }

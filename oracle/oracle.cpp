@@ -7,11 +7,15 @@
 // Built with -O2 -ffp-contract=off so that no fused multiply-add changes a
 // rounding.  Loops run on the serial (NPROCS=1) index ranges: MYIS=2,
 // MYIE=NUMI-1, MYJS=2, MYJE=NUMJ-1, MYMIS=MYMIE=MYMJS=MYMJE=1
-// (vf_cpara.f:80-98).  Options outside the configurations exercised here
-// (k-epsilon, temperature, scalars, wave-source terms ISCTYP, time-dependent
-// porosity IPRNT>1, air-pressure model PVCP0, matrix wave data MTBTYP=3,
-// log-law walls) are not restated and are rejected.  The droplet model
-// VF_FDROPF (IDROP >= 1) is restated.
+// (vf_cpara.f:80-98).  Restated beyond the plain step: the droplet model
+// VF_FDROPF (IDROP >= 1), FF-SLOPE advection (ISCMFF = 1), k-epsilon
+// (LEQK = 1), log-law and rough walls (IB 6, 8) with VF_BWKELG, the
+// matrix-table wave maker (MTBTYP 1, 2) and the fixed-water-level table
+// (MTBTYP 3), the open (radiation) boundary and the adaptive time step
+// VF_CDTCAL.  Options outside these (wave-source terms ISCTYP, temperature,
+// scalars, time-dependent
+// porosity IPRNT>1, the air-pressure model PVCP0) are not restated and
+// are rejected.
 #ifdef _OPENMP
 #include <omp.h>
 #endif

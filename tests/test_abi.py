@@ -32,3 +32,4 @@ def test_params_layout_matches_header(pkg):
     assert p.icgmax == 500 and p.cgpara == 0.95 and p.cgepsr == 1e-12
     assert list(p.idamp) == [-1, -1, -1, -1] and p.damp[1][0] == 0.6
     assert p.diag_relres == 0 and p.precond_ti == 0
+    assert p.mixed_eps_inner == 1e-5 and p.wait_limit_s == 2.0  # the last two fields
