@@ -106,7 +106,8 @@ def params_for(args):
                 precond_ti=args.ti, precond_tj=args.tj, precond_split=getattr(args, "split", 1),
                 solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
                 warm_start={"zero": 0, "previous": 1, "learned": 2}[getattr(args, "guess", "zero")],
-                mixed_eps_inner=getattr(args, "eps_inner", 1.0e-5))
+                mixed_eps_inner=getattr(args, "eps_inner", 1.0e-5),
+                sweep_occupancy=getattr(args, "occ", 0))
 
 
 class ClockSampler:
@@ -818,6 +819,8 @@ def main():
                          "plain run's")
     ap.add_argument("--eps-inner", type=float, default=1.0e-5,
                     help="floor of the FP32 inner tolerance of the mixed solver")
+    ap.add_argument("--occ", type=int, choices=[0, 1, 2], default=0,
+                    help="thread blocks of the MILU sweeps per SM (0: the library's default)")
     ap.add_argument("--beach-nx", type=int, default=1024)
     ap.add_argument("--beach-ny", type=int, default=128)
     ap.add_argument("--beach-nz", type=int, default=128)

@@ -155,6 +155,16 @@ typedef struct cadmas_params {
      with CADMAS_ETIMEOUT and leaves the handle usable.  0 = the default
      2 s.                                                                 */
   double wait_limit_s;
+  /* Thread blocks of the MILU sweeps per SM (no counterpart in the
+     reference): 1 = one block per SM with the deepest bulk-copy ring; 2 =
+     two blocks per SM (registers capped, shallower ring), so that the
+     wavefronts of two tiles interleave on each SM; it needs blocks of at
+     most 256 columns and applies where the ring fits.  0 = the default:
+     two blocks for the backward sweeps and the FP32 sweeps when the grid
+     has at least two preconditioner blocks per SM, one otherwise.  The
+     results do not depend on it.                                         */
+  int    sweep_occupancy;
+  int    pad1;
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */

@@ -76,7 +76,8 @@ class Params(C.Structure):
         ("idrop", C.c_int), ("iscmff", C.c_int), ("leqk", C.c_int), ("pad0", C.c_int)] + [
         (n, C.c_double) for n in ("anu0", "scmk", "akmink", "akmine", "akinik", "akinie", "akcmu", "aksgk",
                                   "aksge", "akc1", "akc2", "akc3", "akk0", "aka0",
-                                  "mixed_eps_inner", "wait_limit_s")]
+                                  "mixed_eps_inner", "wait_limit_s")] + [
+        ("sweep_occupancy", C.c_int), ("pad1", C.c_int)]
 
 
 class Static(C.Structure):

@@ -131,6 +131,7 @@ struct cadmas_handle {
   double *xw = nullptr, *y2 = nullptr, *r0 = nullptr, *rr = nullptr, *pv = nullptr,
          *ap = nullptr, *ae = nullptr;
   double *rb0 = nullptr, *rb1 = nullptr, *dres = nullptr;
+  double *rb5 = nullptr;  // 5 x nslab sum partials of the regrouped FP32 iteration (solver 1)
   // skewed-layout copies of the system for the MILU kernels, and the
   // forward-sweep result
   SkewGeo q;
@@ -144,7 +145,8 @@ struct cadmas_handle {
   int warm_now = 0;  // the next solve starts from the previous solution (warm_start 1)
   bool have_prev = false;  // xw holds a converged solution of an earlier step
   size_t nsl = 0;        // entries of a skewed vector
-  long long nslab = 0;   // slabs (dot-product rows) of a skewed vector
+  long long nslab = 0;   // slabs of a skewed vector
+  long long nrb = 0;     // block partials of a slab sum (slabs / 8, rounded up)
   SolveState *st = nullptr;
   int *dint = nullptr;            // [0] err [1] nch [2] done [3] iter [4] nums
   unsigned char *active = nullptr;
@@ -360,7 +362,7 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   const double epsa2 = h->P.cgepsa * h->P.cgepsa, epsr2 = h->P.cgepsr * h->P.cgepsr,
                div2 = h->P.cgdiv * h->P.cgdiv;
   const int icgmax = h->P.icgmax;
-  const long long nr = h->nslab;
+  const long long nr = h->nrb;
   SolveState *st = h->st;
   const SkewGeo &q = h->q;
   const SkewSys &S = h->S;
@@ -368,7 +370,7 @@ static int solve(cadmas_handle *h, const SysPtr &a, double *x0, const int *indc,
   // vf_m1bcgs.f:79-95: XW = X0, work vectors zero
   double *zero_list[] = {h->y2, h->r0, h->rr, h->pv, h->ap, h->ae};
   for (double *z : zero_list) CK(cudaMemsetAsync(z, 0, vbytes, s));
-  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
   const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
   TB(CADMAS_STAGE_DCMP);
   launch_to_skew(s, g, q, a, indc, S, x0, h->bb_sl, h->xw, h->warm_now);
@@ -452,14 +454,14 @@ static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
   const SkewGeo &q = h->q;
   const SkewSysF &S = h->Sf;
   const int *ic = S.indc;
-  const long long nr = h->nslab;
+  const long long nr = h->nrb;
   SolveState *st = h->st;
   const double epsa2 = h->P.cgepsa * h->P.cgepsa, epsr2 = eps * eps, div2 = h->P.cgdiv * h->P.cgdiv;
   const int icgmax = h->P.icgmax;
   const size_t vb = h->nsl * sizeof(float);
   float *zl[] = {h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef};
   for (float *z : zl) CK(cudaMemsetAsync(z, 0, vb, s));
-  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
   // YY = MINV*BB, BNORM = (YY,YY); with XW = 0, R0 = YY and S = BNORM
   TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, h->bf, nullptr, st, h->y2f); TE();
   TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->r0f, st); TE();
@@ -472,23 +474,25 @@ static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
   int batch = std::max(2, std::min(h->last_iter, 64));
   for (int guard = 0; guard < 100000; ++guard) {
     for (int b = 0; b < batch; ++b) {
+      // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP
       TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->pvf, st, h->y2f); TE();
       TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->apf, st); TE();
       TB(CADMAS_STAGE_DOT);
-      launch_dot_t<float>(s, q, ic, h->r0f, h->apf, nullptr, nullptr, h->rb0, nullptr, st);
+      launch_dot2f(s, q, h->r0f, h->apf, h->rb0, st);
       launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
-      TB(CADMAS_STAGE_VEC); launch_axpy_rr_t<float>(s, q, ic, h->apf, h->rrf, st); TE();
+      TB(CADMAS_STAGE_VEC); launch_axpyf(s, q, h->apf, h->rrf, st); TE();
+      // AE = MINV*(A*RR); the five sums; OMEGA, convergence, BETA; XW,
+      // RR and PP in one pass
       TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->rrf, st, h->y2f); TE();
       TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->aef, st); TE();
       TB(CADMAS_STAGE_DOT);
-      launch_dot_t<float>(s, q, ic, h->rrf, h->aef, h->aef, h->aef, h->rb0, h->rb1, st);
-      launch_fin(s, FIN_OMEGA, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      launch_dot5f(s, q, h->r0f, h->rrf, h->aef, h->rb5, st);
+      launch_fin5(s, h->rb5, nr, st, epsa2, epsr2, div2, icgmax);
       TE();
       TB(CADMAS_STAGE_VEC);
-      launch_upd_xr_t<float>(s, q, ic, h->pvf, h->aef, h->r0f, h->xf, h->rrf, h->rb0, h->rb1, st);
-      launch_fin(s, FIN_CONV, h->rb0, h->rb1, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
-      launch_upd_p_t<float>(s, q, ic, h->rrf, h->apf, h->pvf, st);
+      launch_upd3f(s, q, h->aef, h->apf, h->xf, h->rrf, h->pvf, st);
+      launch_commit(s, st);
       TE();
     }
     CK(cudaGetLastError());
@@ -518,14 +522,14 @@ static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int 
   const Geo &g = h->g;
   const SkewGeo &q = h->q;
   const int *ic = h->S.indc;
-  const long long nr = h->nslab;
+  const long long nr = h->nrb;
   SolveState *st = h->st;
   h->Sf.indc = h->S.indc;
   const double U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
   TB(CADMAS_STAGE_DCMP);
   launch_to_skew(s, g, q, a, indc, h->S, x0, h->bb_sl, h->xw, h->warm_now);
   launch_sys_to_f(s, q, h->S.sys, h->Sf.sys);
-  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
   launch_dcmp_f(s, g, q, U, h->Sf, &st->pivot_bad);
   TE();
   CK(cudaMemcpyAsync(h->h_st, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
@@ -537,7 +541,7 @@ static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int 
   double b2 = 0.0, r2 = 0.0;
   for (int outer = 0; outer < 40; ++outer) {
     // r = b - A x and the two norms in FP64
-    CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+    CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
     TB(CADMAS_STAGE_VEC);
     launch_spmv(s, g, q, h->S, h->xw, h->y2, st);
     launch_bmy(s, q, ic, h->bb_sl, h->y2, st);
@@ -575,7 +579,7 @@ static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int 
     return solve(h, a, x0, indc, iter, bnorm, xnorm);
   }
   // X0 = XW on INDC != -1 (k_x0 requires ITER >= 0: the state is clear)
-  CK(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+  CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
   launch_x0(s, g, q, ic, h->xw, x0, st);
   CK(cudaGetLastError());
   iter = total;
@@ -680,7 +684,7 @@ static int do_v1cal(cadmas_handle *h) {
   if (rc) return rc;
   if (h->P.diag_relres) {
     launch_relres(s, h->g, h->q, h->S, h->bb_sl, h->xw, h->rb0, h->rb1);
-    launch_fin(s, FIN_STORE, h->rb0, h->rb1, h->nslab, h->st, h->dres + 2, 0, 0, 0, 0);
+    launch_fin(s, FIN_STORE, h->rb0, h->rb1, h->nrb, h->st, h->dres + 2, 0, 0, 0, 0);
     CK(cudaMemcpyAsync(h->h_res, h->dres, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     h->stats.true_relres = h->h_res[3] > 0.0 ? std::sqrt(h->h_res[2]) / std::sqrt(h->h_res[3]) : 0.0;
@@ -986,10 +990,12 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   h->q.W = (d->numk - 2) + (TI - 1) + (TJl - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJl - 1) / TJl);
+  h->q.occ = (p->sweep_occupancy == 1 || p->sweep_occupancy == 2) ? p->sweep_occupancy : 0;
+  h->q.nsm = 148;
   {
-    const double lim = p->wait_limit_s > 0.0 ? std::min(p->wait_limit_s, 60.0) : 2.0;
-    h->q.wait_ns = (long long)(lim * 1.0e9);
-    h->q.stall_from = 1 << 30;
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device) == cudaSuccess && nsm > 0)
+      h->q.nsm = nsm;
   }
   if (!sweep_supported(h->q)) {
     g_last_error = "preconditioner block too large for the MILU sweeps; set precond_ti/precond_tj";
@@ -997,6 +1003,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   }
   h->nsl = (size_t)h->q.nb * h->q.W * h->q.T;
   h->nslab = (long long)h->q.nb * h->q.W;
+  h->nrb = (h->nslab + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK;
   {
     const size_t nsl = h->nsl;
     AL(h->S.sys, (size_t)SYS_N * nsl);
@@ -1011,6 +1018,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
       AL(h->Sf.sys, (size_t)SYS_N * nsl);
       AL(h->bf, nsl); AL(h->xf, nsl); AL(h->r0f, nsl); AL(h->rrf, nsl); AL(h->pvf, nsl);
       AL(h->apf, nsl); AL(h->aef, nsl); AL(h->y2f, nsl);
+      AL(h->rb5, 5 * (size_t)h->nrb);
     } else if (p->solver != 0) {
       rc = rc ? rc : CADMAS_EINVAL;
     }
@@ -1032,6 +1040,13 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   if (!rc && cudaMallocHost((void **)&h->h_st, sizeof(SolveState)) != cudaSuccess) rc = CADMAS_ENOMEM;
   if (!rc && cudaMallocHost((void **)&h->h_int, 8 * sizeof(int)) != cudaSuccess) rc = CADMAS_ENOMEM;
   if (!rc && cudaMallocHost((void **)&h->h_res, 10 * sizeof(double)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc) {  // the sweeps' wait limit and (no) stall, kept across solves
+    const double lim = p->wait_limit_s > 0.0 ? std::min(p->wait_limit_s, 60.0) : 2.0;
+    std::memset(h->h_st, 0, sizeof(SolveState));
+    h->h_st->wait_ns = (long long)(lim * 1.0e9);
+    h->h_st->stall_from = 1 << 30;
+    if (cudaMemcpy(h->st, h->h_st, sizeof(SolveState), cudaMemcpyHostToDevice) != cudaSuccess) rc = CADMAS_ECUDA;
+  }
   if (rc) { cadmas_destroy(h); return rc; }
   // NF starts as all obstacle until set_state; INDC as non-computed.
   cudaMemset(h->nf, 0xff, h->N * sizeof(int));
@@ -1054,7 +1069,7 @@ int cadmas_destroy(cadmas_handle *h) {
   double *dl[] = {h->xx, h->yy, h->zz, h->ggv, h->ggx, h->ggy, h->ggz, h->glv, h->glx, h->gly, h->glz,
                   h->cd0, h->anu, h->pbuf[0], h->pbuf[1], h->ff, h->bcvi, h->bcu, h->bcv, h->bcw, h->bcp, h->bcf,
                   h->xw, h->y2, h->r0, h->rr, h->pv, h->ap, h->ae, h->rb0, h->rb1, h->dres,
-                  h->S.sys, h->bb_sl};
+                  h->S.sys, h->bb_sl, h->rb5};
   for (double *q : dl) if (q) cudaFree(q);
   for (int b = 0; b < 2; ++b) for (int c = 0; c < 3; ++c) if (h->vel[b][c]) cudaFree(h->vel[b][c]);
   for (double *q : h->wk) if (q) cudaFree(q);
@@ -1750,7 +1765,9 @@ int cadmas_get_stats(cadmas_handle *h, cadmas_stats *st) {
 
 int cadmas_test_stall_sweeps(cadmas_handle *h, int from_step) {
   if (!h) return CADMAS_EINVAL;
-  h->q.stall_from = from_step >= 0 ? from_step : (1 << 30);
+  const int v = from_step >= 0 ? from_step : (1 << 30);
+  CK(cudaMemcpyAsync(&h->st->stall_from, &v, sizeof(int), cudaMemcpyHostToDevice, h->s));
+  CK(cudaStreamSynchronize(h->s));
   return CADMAS_OK;
 }
 

@@ -8,6 +8,7 @@
 // Global sums use one fixed tree (row_reduce below); no atomics touch a
 // floating-point value.
 #pragma once
+#include <cstddef>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/cadmas_gpu.h"
@@ -187,8 +188,21 @@ __device__ __forceinline__ double block_final(const double *rowbuf, long long nr
 struct SolveState {
   double S, alpha, omega, beta, bnorm, xnorm, w1, w2, rn, bn;
   int iter, done, status, pivot_bad;
-  int timeout, pad_;  // a bulk-copy wait of a sweep ran out of time
+  int timeout;  // a bulk-copy wait of a sweep ran out of time
+  int stop;     // regrouped FP32 iteration: finished, `done` after its last update
+  // Set once per handle, kept when a solve clears the fields above (they
+  // are read only where a sweep starts to wait, or by its producer warp,
+  // so they add nothing to the sweeps' register load):
+  //   wait_ns     an mbarrier wait of the sweeps gives up after this long
+  //               and the solve ends with CADMAS_ETIMEOUT;
+  //   stall_from  the producer warp issues no bulk copy for wavefront
+  //               steps >= stall_from (failure injection for tests,
+  //               cadmas_test_stall_sweeps; 2^30 otherwise).
+  long long wait_ns;
+  int stall_from, pad_;
 };
+// Bytes of SolveState that a new solve clears (everything before wait_ns).
+#define SOLVE_CLEAR_BYTES offsetof(cadmas::SolveState, wait_ns)
 
 // Error flags raised by kernels (bitmask in a device int).
 enum : int {

@@ -410,8 +410,13 @@ __device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
-  return mbar_try(bar, parity) || mbar_wait_slow(bar, parity, limit_ns);
+// The limit comes from the solve state, read only once a wait has to
+// spin, so that it occupies no register in the sweeps' step loop.
+__device__ __noinline__ bool mbar_wait_st(unsigned bar, unsigned parity, const SolveState *st) {
+  return mbar_wait_slow(bar, parity, (unsigned long long)st->wait_ns);
+}
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, const SolveState *st) {
+  return mbar_try(bar, parity) || mbar_wait_st(bar, parity, st);
 }
 
 // ------------------------------------- cluster exchange (precond_split 2)
@@ -457,8 +462,11 @@ __device__ __noinline__ bool mbar_wait_cluster_slow(unsigned bar, unsigned parit
     if (global_ns() - t0 > limit_ns) return false;
   }
 }
-__device__ __forceinline__ bool mbar_wait_cluster(unsigned bar, unsigned parity, unsigned long long limit_ns) {
-  return mbar_try_cluster(bar, parity) || mbar_wait_cluster_slow(bar, parity, limit_ns);
+__device__ __noinline__ bool mbar_wait_cluster_st(unsigned bar, unsigned parity, const SolveState *st) {
+  return mbar_wait_cluster_slow(bar, parity, (unsigned long long)st->wait_ns);
+}
+__device__ __forceinline__ bool mbar_wait_cluster(unsigned bar, unsigned parity, const SolveState *st) {
+  return mbar_try_cluster(bar, parity) || mbar_wait_cluster_st(bar, parity, st);
 }
 __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release;\nbarrier.cluster.wait.acquire;\n" ::: "memory");
@@ -489,8 +497,8 @@ __device__ __forceinline__ void cluster_barrier() {
 // and their evaluation order are those of the reference loops, so the
 // results do not change.  The step loop is unrolled by the ring length so
 // slot addresses and mbarrier phases are constants.
-template <int D, int MODE, int MAXT, typename V, int CS>
-__global__ void __launch_bounds__(MAXT, 1)
+template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB)
     k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st) {
   pdl_enter();
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
@@ -587,9 +595,9 @@ __global__ void __launch_bounds__(MAXT, 1)
     src0 = (l0.arr == 0 ? S.sys : vin) + l0.base;
   else { l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; }
   const unsigned bar0 = smem_u32(bar), ring0 = smem_u32(ring);
-  const unsigned long long wait_ns = (unsigned long long)q.wait_ns;
+  const int stall_from = producer ? st->stall_from : 0;  // read by the producer warp only
   auto issue = [&](int u, int slot) {
-    if (u >= nsteps || u >= q.stall_from) return;
+    if (u >= nsteps || u >= stall_from) return;
     const int w = (MODE == SWEEP_BWD) ? nsteps - 1 - u : u;
     const unsigned bslot = bar0 + 8u * slot;
     const unsigned dslot = ring0 + (unsigned)ES * (unsigned)(slot * SS);
@@ -601,7 +609,7 @@ __global__ void __launch_bounds__(MAXT, 1)
   };
   // data of step u sits in slot u % R, phase (u / R) & 1
   auto wait_data = [&](int u, int slot, unsigned parity) -> bool {
-    return u >= nsteps || mbar_wait(bar0 + 8u * slot, parity, wait_ns);
+    return u >= nsteps || mbar_wait(bar0 + 8u * slot, parity, st);
   };
 
   if (producer) {
@@ -672,12 +680,12 @@ __global__ void __launch_bounds__(MAXT, 1)
   bool ok = true;
   if (!producer) {
     for (int u = 0; u < AHEAD; ++u) if (ok) ok = wait_data(u, u % R, (unsigned)((u / R) & 1));
-    if (CS == 2 && ok && rrow && col && 0 >= slo && 0 <= shi) ok = mbar_wait_cluster(smem_u32(xfull + lag), 0u, wait_ns);
+    if (CS == 2 && ok && rrow && col && 0 >= slo && 0 <= shi) ok = mbar_wait_cluster(smem_u32(xfull + lag), 0u, st);
     if (ok) prepare(0, slot_ptr(0), slot_ptr(R - 1), slot_ptr(1 % R));
     else s_abort[0] = 1;
   }
   bool aborted = false;
-  int issued = min(min(D, nsteps), q.stall_from) - 1;  // last step whose copies were issued (producer)
+  int issued = min(min(D, nsteps), stall_from) - 1;  // last step whose copies were issued (producer)
   unsigned ph = 0;                  // (s0 / R) & 1, also the ring cycle's s_abort entry
 #pragma unroll 1
   for (int s0 = 0; s0 < nsteps && !aborted; s0 += R, ph ^= 1u) {
@@ -687,7 +695,7 @@ __global__ void __launch_bounds__(MAXT, 1)
       if (s >= nsteps) break;
       if (producer) {
         issue(s + D, (r + D) % R);
-        if (s + D < nsteps && s + D < q.stall_from) issued = s + D;
+        if (s + D < nsteps && s + D < stall_from) issued = s + D;
       } else {
         // Test the data of the step to prepare next now, so the test's
         // latency overlaps the recurrence; wait only if it is not there.
@@ -724,11 +732,11 @@ __global__ void __launch_bounds__(MAXT, 1)
         }
         // prepare step s+1
         if (!ready) {
-          ok = mbar_wait_slow(ubar, upar, wait_ns);
+          ok = mbar_wait_st(ubar, upar, st);
           if (!ok) s_abort[ph] = 1;
         }
         if (CS == 2 && ok && rrow && col && s + 1 >= slo && s + 1 <= shi) {
-          ok = mbar_wait_cluster(smem_u32(xfull + (s + 1 + lag)), 0u, wait_ns);
+          ok = mbar_wait_cluster(smem_u32(xfull + (s + 1 + lag)), 0u, st);
           if (!ok) s_abort[ph] = 1;
         }
         if (ok && s + 1 < nsteps) prepare(s + 1, slot_ptr((r + 1) % R), slot_ptr(r), slot_ptr((r + 2) % R));
@@ -769,6 +777,25 @@ __global__ void __launch_bounds__(MAXT, 1)
     }                 \
   }
 #define SLAB_ROW ((long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5))
+// Partial of one block of a slab sum: each warp's slab sum (warp tree),
+// then the block's ROWS_PER_BLOCK slabs added in slab order by thread 0,
+// into rb[blockIdx.x].  The finaliser then reduces one partial per block
+// (nslab / 8 of them) instead of one per slab.  Every thread of the block
+// calls it (it holds block barriers).
+__device__ __forceinline__ void slab_store(double s, double *rb, long long nslab) {
+  __shared__ double ws[ROWS_PER_BLOCK];
+  s = warp_tree(s);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const long long first = (long long)blockIdx.x * ROWS_PER_BLOCK;
+    double t = 0.0;
+    for (int i = 0; i < ROWS_PER_BLOCK; ++i)
+      if (first + i < nslab) t = t + ws[i];
+    rb[blockIdx.x] = t;
+  }
+  __syncthreads();
+}
 
 __device__ __forceinline__ bool interior(const Geo &g, int I, int J, int K) {
   return I >= 2 && I <= g.NI - 1 && J >= 2 && J <= g.NJ - 1 && K >= 2 && K <= g.NK - 1;
@@ -834,8 +861,8 @@ __global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, cons
     if (x1) s1 = s1 + a1;
   }
   SLAB_LOOP_END
-  row_store(s0, rb0, SLAB_ROW, nslab);
-  if (x1) row_store(s1, rb1, SLAB_ROW, nslab);
+  slab_store(s0, rb0, nslab);
+  if (x1) slab_store(s1, rb1, nslab);
 }
 
 // RR = R0, PP = R0
@@ -882,8 +909,8 @@ __global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, c
     s1 = s1 + (double)r0 * (double)r;
   }
   SLAB_LOOP_END
-  row_store(s0, rb0, SLAB_ROW, nslab);
-  row_store(s1, rb1, SLAB_ROW, nslab);
+  slab_store(s0, rb0, nslab);
+  slab_store(s1, rb1, nslab);
 }
 
 // PP = RR + BETA*(PP - OMEGA*AP) (vf_m1bcgs.f:229-238)
@@ -897,6 +924,145 @@ __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V 
   const V rr = RR[e], pp = PP[e], ap = AP[e];
   if (ic != -1) PP[e] = (V)(rr + beta * (pp - omega * ap));
   SLAB_LOOP_END
+}
+
+// --------------------------------- FP32 inner solves of the mixed solver
+// The inner BiCGSTAB of the mixed solver (V = float) runs a regrouped
+// iteration with fewer passes over the vectors; it is the same method and
+// ends on the same criterion, but its sums are not those of VF_M1BCGS,
+// whose FP64 form (above) keeps the reference's order.
+//   * Every vector is zero wherever INDC = -1 and on the layout's padding
+//     (zeroed at the start of a solve and never written there: the
+//     sweeps write 0 for non-computed cells), so these kernels read no
+//     INDC: an update leaves a zero entry zero and adds nothing to a sum.
+//   * One lane moves 4 consecutive entries (16-byte loads; T is a multiple
+//     of 4 and every slab starts on a 16-byte boundary).
+//   * After the second sweep pair one pass forms the five sums (RR,AE),
+//     (AE,AE), (RR,RR), (R0,RR), (R0,AE); OMEGA, the new |RR|^2 =
+//     (RR,RR) - 2 OMEGA (RR,AE) + OMEGA^2 (AE,AE), the new (R0,RR) =
+//     (R0,RR) - OMEGA (R0,AE), the convergence test and BETA follow from
+//     them (k_fin5), and one pass updates XW, RR and PP together (k_upd3f).
+//     Per iteration a sum drops by about 25 times, so the expansion loses
+//     nothing to cancellation at the tolerances used (FP64 sums).
+#define SLAB4_LOOP_BEGIN(q)                                                         \
+  const int lane_ = threadIdx.x & 31;                                               \
+  const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
+  if (slab_ < (long long)(q).nb * (q).W) {                                          \
+    const int T4_ = (q).T >> 2;                                                     \
+    _Pragma("unroll 2")                                                             \
+    for (int t_ = lane_; t_ < T4_; t_ += 32) {                                      \
+      const long long e4 = slab_ * T4_ + t_;
+#define SLAB4_LOOP_END \
+    }                  \
+  }
+__device__ __forceinline__ double dot4(const float4 &a, const float4 &b) {
+  return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z +
+         (double)a.w * (double)b.w;
+}
+// slab partials of (R0,AP)
+__global__ void k_dot2f(SkewGeo q, const float *R0, const float *AP, double *rb, const SolveState *st) {
+  pdl_enter();
+  if (st->done) return;
+  const float4 *r0 = reinterpret_cast<const float4 *>(R0), *ap = reinterpret_cast<const float4 *>(AP);
+  double s0 = 0.0;
+  const long long nslab = (long long)q.nb * q.W;
+  SLAB4_LOOP_BEGIN(q)
+  s0 += dot4(r0[e4], ap[e4]);
+  SLAB4_LOOP_END
+  slab_store(s0, rb, nslab);
+}
+// RR = RR - ALPHA*AP
+__global__ void k_axpyf(SkewGeo q, const float *AP, float *RR, const SolveState *st) {
+  pdl_enter();
+  if (st->done) return;
+  const double alpha = st->alpha;
+  const float4 *ap = reinterpret_cast<const float4 *>(AP);
+  float4 *rr = reinterpret_cast<float4 *>(RR);
+  SLAB4_LOOP_BEGIN(q)
+  const float4 a = ap[e4];
+  float4 r = rr[e4];
+  r.x = (float)(r.x - alpha * a.x); r.y = (float)(r.y - alpha * a.y);
+  r.z = (float)(r.z - alpha * a.z); r.w = (float)(r.w - alpha * a.w);
+  rr[e4] = r;
+  SLAB4_LOOP_END
+}
+// block partials of (RR,AE), (AE,AE), (RR,RR), (R0,RR), (R0,AE) into
+// rb + c*nrb, c = 0..4 (nrb = blocks of the launch)
+__global__ void k_dot5f(SkewGeo q, const float *R0, const float *RR, const float *AE, double *rb,
+                        const SolveState *st) {
+  pdl_enter();
+  if (st->done) return;
+  const float4 *r0 = reinterpret_cast<const float4 *>(R0), *rr = reinterpret_cast<const float4 *>(RR),
+               *ae = reinterpret_cast<const float4 *>(AE);
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+  const long long nslab = (long long)q.nb * q.W;
+  SLAB4_LOOP_BEGIN(q)
+  const float4 a = r0[e4], r = rr[e4], e = ae[e4];
+  s0 += dot4(r, e);
+  s1 += dot4(e, e);
+  s2 += dot4(r, r);
+  s3 += dot4(a, r);
+  s4 += dot4(a, e);
+  SLAB4_LOOP_END
+  const long long nrb = gridDim.x;  // block partials of each sum
+  slab_store(s0, rb, nslab);
+  slab_store(s1, rb + nrb, nslab);
+  slab_store(s2, rb + 2 * nrb, nslab);
+  slab_store(s3, rb + 3 * nrb, nslab);
+  slab_store(s4, rb + 4 * nrb, nslab);
+}
+// XW = XW + (ALPHA*PP + OMEGA*RR); RR' = RR - OMEGA*AE;
+// PP = RR' + BETA*(PP - OMEGA*AP); RR = RR'
+__global__ void k_upd3f(SkewGeo q, const float *AE, const float *AP, float *XW, float *RR, float *PP,
+                        const SolveState *st) {
+  pdl_enter();
+  if (st->done) return;
+  const double alpha = st->alpha, omega = st->omega, beta = st->beta;
+  const float4 *ae = reinterpret_cast<const float4 *>(AE), *ap = reinterpret_cast<const float4 *>(AP);
+  float4 *xw = reinterpret_cast<float4 *>(XW), *rr = reinterpret_cast<float4 *>(RR),
+         *pp = reinterpret_cast<float4 *>(PP);
+  SLAB4_LOOP_BEGIN(q)
+  const float4 e = ae[e4], a = ap[e4], r = rr[e4], p = pp[e4];
+  float4 x = xw[e4], rn, pn;
+#define UPD3_(c)                                                   \
+  x.c = (float)(x.c + (alpha * p.c + omega * r.c));                \
+  rn.c = (float)(r.c - omega * e.c);                               \
+  pn.c = (float)(rn.c + beta * (p.c - omega * a.c));
+  UPD3_(x) UPD3_(y) UPD3_(z) UPD3_(w)
+#undef UPD3_
+  xw[e4] = x;
+  rr[e4] = rn;
+  pp[e4] = pn;
+  SLAB4_LOOP_END
+}
+// OMEGA, the new |RR|^2 and (R0,RR), convergence and BETA from the five
+// sums (vf_m1bcgs.f:196-241 regrouped).  A finished solve sets `stop`;
+// k_commit turns it into `done` once the last update has run.
+__global__ void k_fin5(const double *rb, long long nrows, SolveState *st, double epsa2, double epsr2, double div2,
+                       int icgmax) {
+  pdl_enter();
+  if (st->done) return;
+  const double rae = block_final(rb, nrows), aeae = block_final(rb + nrows, nrows),
+               rrrr = block_final(rb + 2 * nrows, nrows), r0rr = block_final(rb + 3 * nrows, nrows),
+               r0ae = block_final(rb + 4 * nrows, nrows);
+  if (threadIdx.x != 0) return;
+  const double omega = rae / aeae;
+  st->omega = omega;
+  st->w1 = rae;
+  st->w2 = aeae;
+  const double xn = rrrr - 2.0 * omega * rae + omega * omega * aeae;
+  st->xnorm = xn;
+  if (xn <= st->bnorm * epsr2 + epsa2) { st->stop = 1; st->beta = 0.0; return; }
+  if (xn > div2) { st->iter = -2; st->stop = 1; st->beta = 0.0; return; }
+  const double W1 = r0rr - omega * r0ae;
+  st->beta = W1 * st->alpha / (st->S * omega);
+  st->S = W1;
+  st->iter = st->iter + 1;
+  if (st->iter > icgmax) st->stop = 1;
+}
+__global__ void k_commit(SolveState *st) {
+  pdl_enter();
+  if (st->stop) st->done = 1;
 }
 
 // ------------------------------------------- mixed-precision conversions
@@ -956,8 +1122,8 @@ __global__ void k_relres(Geo g, SkewGeo q, SkewSys S, const double *B, const dou
     s1 = s1 + B[e] * B[e];
   }
   SLAB_LOOP_END
-  row_store(s0, rb0, SLAB_ROW, nslab);
-  row_store(s1, rb1, SLAB_ROW, nslab);
+  slab_store(s0, rb0, nslab);
+  slab_store(s1, rb1, nslab);
 }
 
 // ------------------------------------------------------------- finalisers
@@ -1164,6 +1330,20 @@ static int sweep_depth(const SkewGeo &q, int mode, int es) {
   }
   return 0;
 }
+// Two thread blocks per SM (q.occ == 2): blocks of at most SWEEP2_THREADS
+// threads, registers capped for two resident blocks, and a ring that
+// leaves room for the second block's (228 KB per SM, 1 KB reserved per
+// block).  Two tiles' wavefronts then interleave on every SM.
+// The register cap (96 for two 288-thread blocks) makes deeper rings
+// spill: depths up to 3 (fused forward sweep) or 4 (the others) are used.
+constexpr int SWEEP2_THREADS = 288;
+static int sweep_depth2(const SkewGeo &q, int mode, int es) {
+  if (q.split != 1 || sweep_threads(q.T) > SWEEP2_THREADS) return 0;
+  const int dmax = mode == SWEEP_FWD_AX ? 3 : 4;
+  for (int d : {4, 3, 2})
+    if (d <= dmax && sweep_bytes(q, mode, d, es) <= 113 * 1024) return d;
+  return 0;
+}
 template <int MODE, typename V>
 static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *vin,
                          V *vout, SolveState *st) {
@@ -1193,6 +1373,27 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
     return;
   }
   const dim3 grid = skew_grid(q);
+  // Two blocks per SM pay where the tiles fill the SMs twice over: there
+  // the sweeps' per-step latency, not the bandwidth, sets the time and a
+  // second tile's wavefront fills it.  The fused FP64 forward sweep keeps
+  // one block: its ring of 8 arrays needs the depth and registers.
+  const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm && (ES == 4 || MODE == SWEEP_BWD));
+  if (two) {
+    const int d2 = sweep_depth2(q, MODE, ES);
+    if (d2 > 0) {
+      const size_t bytes2 = sweep_bytes(q, MODE, d2, ES);
+      switch (d2) {
+#define SWEEP_CASE_OCC2(DD)                                                                            \
+  case DD:                                                                                             \
+    set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, bytes2);                                      \
+    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, grid, block, bytes2, s, 1, g, q, S, vin, vout, st); \
+    return;
+        SWEEP_CASE_OCC2(4) SWEEP_CASE_OCC2(3) SWEEP_CASE_OCC2(2)
+#undef SWEEP_CASE_OCC2
+        default: break;
+      }
+    }
+  }
   switch (d * 4096 + mt) {
 #define SWEEP_CASE(DD, MT)                                                              \
   case DD * 4096 + MT:                                                                  \
@@ -1314,6 +1515,20 @@ void launch_x0(cudaStream_t s, const Geo &g, const SkewGeo &q, const int *indc, 
                const SolveState *st) { SL(k_x0, g, q, indc, xw, x0, st); }
 void launch_relres(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S, const double *b,
                    const double *x, double *rb0, double *rb1) { SL(k_relres, g, q, S, b, x, rb0, rb1); }
+void launch_dot2f(cudaStream_t s, const SkewGeo &q, const float *r0, const float *ap, double *rb,
+                  const SolveState *st) { SL(k_dot2f, q, r0, ap, rb, st); }
+void launch_axpyf(cudaStream_t s, const SkewGeo &q, const float *ap, float *rr, const SolveState *st) {
+  SL(k_axpyf, q, ap, rr, st);
+}
+void launch_dot5f(cudaStream_t s, const SkewGeo &q, const float *r0, const float *rr, const float *ae, double *rb,
+                  const SolveState *st) { SL(k_dot5f, q, r0, rr, ae, rb, st); }
+void launch_upd3f(cudaStream_t s, const SkewGeo &q, const float *ae, const float *ap, float *xw, float *rr,
+                  float *pp, const SolveState *st) { SL(k_upd3f, q, ae, ap, xw, rr, pp, st); }
+void launch_fin5(cudaStream_t s, const double *rb, long long nrows, SolveState *st, double epsa2, double epsr2,
+                 double div2, int icgmax) {
+  launch_pdl(k_fin5, dim3(1), dim3(1024), 0, s, 1, rb, nrows, st, epsa2, epsr2, div2, icgmax);
+}
+void launch_commit(cudaStream_t s, SolveState *st) { launch_pdl(k_commit, dim3(1), dim3(1), 0, s, 1, st); }
 void launch_sys_to_f(cudaStream_t s, const SkewGeo &q, const double *sys, float *sysf) {
   const long long n = (long long)q.nb * q.W * q.T;
   launch_pdl(k_sys_to_f, dim3((unsigned)std::min<long long>((n + 255) / 256, 148LL * 16)), dim3(256), 0, s, 1, q, sys,

@@ -42,13 +42,10 @@ struct SkewGeo {
   int TI, TJ, TIp, T, W;  // layout tile TI x TJ columns (T = TIp*TJ slots), W slabs per tile
   int ntx, nb;            // layout tiles along x, tiles in total
   int split;  // layout tiles per preconditioner block along y (1 or 2)
-  // Bounded waits of the sweeps: an mbarrier wait gives up after wait_ns
-  // nanoseconds and the solve ends with CADMAS_ETIMEOUT.  stall_from: the
-  // producer warp issues no bulk copy for wavefront steps >= stall_from
-  // (failure injection for tests, cadmas_test_stall_sweeps; a large value
-  // in normal runs), so the waits of those steps run out.
-  long long wait_ns;
-  int stall_from, pad_;
+  // Thread blocks of the sweeps per SM (k_poisson.cu): 1, 2, or 0 = by
+  // the rule of launch_sweep (two for the backward sweeps and the FP32
+  // sweeps when there are at least two tiles per SM); nsm = the SMs.
+  int occ, nsm;
 };
 
 __host__ __device__ inline long long sys_at(long long slab, int c, int T, int t) {
@@ -244,6 +241,21 @@ void launch_upd_xr_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V 
 template <typename V>
 void launch_upd_p_t(cudaStream_t s, const SkewGeo &q, const int *indc, const V *rr, const V *ap, V *pp,
                     const SolveState *st);
+// Regrouped FP32 inner iteration (k_poisson.cu): vectors zero where
+// INDC = -1, four entries per lane; rb5 holds 5 x nslab partials.
+void launch_dot2f(cudaStream_t s, const SkewGeo &q, const float *r0, const float *ap, double *rb,
+                  const SolveState *st);
+void launch_axpyf(cudaStream_t s, const SkewGeo &q, const float *ap, float *rr, const SolveState *st);
+void launch_dot5f(cudaStream_t s, const SkewGeo &q, const float *r0, const float *rr, const float *ae, double *rb5,
+                  const SolveState *st);
+// One iteration's tail: launch_dot5f, launch_fin5 (scalars; a finished
+// solve sets SolveState::stop), launch_upd3f (runs while `done` is clear,
+// so also in the finishing iteration), launch_commit (done = stop).
+void launch_upd3f(cudaStream_t s, const SkewGeo &q, const float *ae, const float *ap, float *xw, float *rr,
+                  float *pp, const SolveState *st);
+void launch_fin5(cudaStream_t s, const double *rb5, long long nrows, SolveState *st, double epsa2, double epsr2,
+                 double div2, int icgmax);
+void launch_commit(cudaStream_t s, SolveState *st);
 void launch_sys_to_f(cudaStream_t s, const SkewGeo &q, const double *sys, float *sysf);
 void launch_scale_to_f(cudaStream_t s, const SkewGeo &q, const int *indc, const double *r, double scale,
                        float *rf);

@@ -481,8 +481,10 @@ struct orc_handle {
   // tile b (x fastest), wavefront slab w = (k-2)+ti+tj, slab entry
   // t = ti + TIp*tj (TIp = TI rounded up to a multiple of 4; columns
   // ti >= TI are padding); lane l of a slab sums t = l, l+32, ... in order,
-  // warp tree per slab, then the 1024-thread tree over the slabs.  This is
-  // the order of the dot products of VF_M1BCGS in the GPU library.
+  // warp tree per slab, the slabs of each group of 8 (a thread block of the
+  // GPU's slab kernels: slabs 8g .. 8g+7) added in slab order starting
+  // from 0, then the 1024-thread tree over the groups.  This is the order
+  // of the dot products of VF_M1BCGS in the GPU library.
   template <class F> double gsum_skew(F f) const {
     const int TI = std::min(P.precond_ti > 0 ? P.precond_ti : NI - 2, NI - 2);
     const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2) /
@@ -507,10 +509,17 @@ struct orc_handle {
       }
       R[sl] = warp_tree(lane);
     }
+    const long long NG = (NS + 7) / 8;
+    std::vector<double> G(NG);
+    for (long long gi = 0; gi < NG; ++gi) {
+      double s = 0.0;
+      for (long long sl = 8 * gi; sl < 8 * gi + 8 && sl < NS; ++sl) s = s + R[sl];
+      G[gi] = s;
+    }
     double u[1024];
     for (int t = 0; t < 1024; ++t) {
       double s = 0.0;
-      for (long long r = t; r < NS; r += 1024) s = s + R[r];
+      for (long long r = t; r < NG; r += 1024) s = s + G[r];
       u[t] = s;
     }
     double wv[32];
