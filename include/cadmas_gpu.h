@@ -248,6 +248,29 @@ typedef struct cadmas_wave_bc {
                             0 = none                                        */
 } cadmas_wave_bc;
 
+/* ---- wave source (MODEL WAVE-SRC ... FUNC MATRIX) ------------------------
+   A line of cells inside the domain that makes waves on both sides by a
+   mass source (ISCTYP /VF_APHYSI/, SCTYP /VF_APHYSR/; vf_iimdl.f:115-172).
+   Every step the source velocity SRCUV of the line is taken from the
+   matrix table at TNOW (VF_CWMSRC, vf_cwmsrc.f:46-143, scaled to the
+   column's water level for MTBTYP 1 and faded in over `ramp` periods); it
+   enters the momentum sources (VF_VGENE, vf_vgene.f:149-152,225-228,
+   304-315), the right-hand side of the pressure equation (VF_VPCOEF,
+   vf_vpcoef.f:349-350), the surface cells of the line (VF_BSUWN,
+   vf_bsuwn.f:81-118) and F (VF_FGENE, vf_fgene.f:42-70, through
+   VF_FEULER's QF).  The table is the one of cadmas_set_wave (MTBTYP 1 or
+   2; 3 is 'MTBTYP ERROR.' in the reference, vf_csetup.f:267).  The wave
+   theories (STREAM, STOKES, CNOIDAL) are not built for the source.       */
+typedef struct cadmas_wave_src {
+  int line;              /* ISCTYP(1): > 0 the x source at I = line (1-based
+                            with ghosts, 2..NUMI-1); < 0 the y source at
+                            J = -line (2..NUMJ-1)                           */
+  int pad;
+  double depth;          /* SCTYP(1) still-water depth D                     */
+  double period;         /* SCTYP(3) period T                                */
+  double ramp;           /* SCTYP(8) AMPL: periods of the sine fade-in; 0 = none */
+} cadmas_wave_src;
+
 typedef struct cadmas_handle cadmas_handle;
 
 /* Defaults of vf_a2dflt.f for every field of cadmas_params. */
@@ -517,6 +540,12 @@ int cadmas_divnorm_noalloc(const cadmas_dims *d, const double *xx, const double 
    end normally and the handle stays usable.  A negative from_step turns
    the injection off.                                                    */
 int cadmas_test_stall_sweeps(cadmas_handle *h, int from_step);
+
+/* The wave source of the handle (one line, as the reference allows),
+   with the matrix table `t` (NULL: the table already given to
+   cadmas_set_wave is used).  CADMAS_EINVAL for a line outside the
+   interior, MTBTYP 3 or no table.                                         */
+int cadmas_set_wave_source(cadmas_handle *h, const cadmas_wave_src *s, const cadmas_wave_table *t);
 
 /* The CUDA stream (cudaStream_t) on which every call of the handle issues
    its work; callers may record CUDA events on it or wait on it. */

@@ -46,6 +46,22 @@ class WaveBC(C.Structure):
                 ("depth", C.c_double), ("period", C.c_double), ("ramp", C.c_double)]
 
 
+class WaveSrc(C.Structure):
+    _fields_ = [("line", C.c_int), ("pad", C.c_int), ("depth", C.c_double), ("period", C.c_double),
+                ("ramp", C.c_double)]
+
+
+def source_structs(src):
+    """(WaveSrc, WaveTable or None, keep-alive arrays) of a case's wave
+    source dict (cases.wave_source)."""
+    tab, arrs = None, {}
+    if src.get("table") is not None:
+        _, tab, arrs = wave_structs(dict(side=1, first=2, last=2, depth=src["depth"], period=src["period"],
+                                         table=src["table"]))
+    ws = WaveSrc(int(src["line"]), 0, float(src["depth"]), float(src["period"]), float(src.get("ramp", 0.0)))
+    return ws, tab, arrs
+
+
 class OpenBC(C.Structure):
     _fields_ = [("side", C.c_int), ("pad", C.c_int), ("depth", C.c_double), ("period", C.c_double)]
 
@@ -109,7 +125,8 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_unet_param_count", "cadmas_unet_create", "cadmas_unet_destroy", "cadmas_unet_set_params",
             "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step",
             "cadmas_set_warm_net", "cadmas_warm_stats", "cadmas_get_solve", "cadmas_get_system",
-            "cadmas_unet_train_sys", "cadmas_unet_time_forward", "cadmas_test_stall_sweeps"]
+            "cadmas_unet_train_sys", "cadmas_unet_time_forward", "cadmas_test_stall_sweeps",
+            "cadmas_set_wave_source"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
@@ -406,7 +423,16 @@ class Tank:
             self.set_wave(case.wave)
         for op in getattr(case, "open", None) or []:
             self.set_open(op)
+        if getattr(case, "source", None):
+            self.set_wave_source(case.source)
         self.set_state(initial_state(case))
+
+    def set_wave_source(self, src):
+        """Wave source line from a dict made by cases.wave_source
+        (cadmas_set_wave_source)."""
+        ws, tab, keep = source_structs(src)
+        self.lib.cadmas_set_wave_source.argtypes = [C.c_void_p, C.POINTER(WaveSrc), C.POINTER(WaveTable)]
+        _check(self.lib, self.lib.cadmas_set_wave_source(self.h, C.byref(ws), C.byref(tab) if tab else None))
 
     def set_open(self, op):
         """Open (radiation) side from a dict made by cases.open_boundary

@@ -99,6 +99,7 @@ class Case:
     params: dict = dataclasses.field(default_factory=dict)
     wave: dict = None          # wave-maker side (wave_maker), or None
     open: list = None          # open (radiation) sides (open_boundary), or None
+    source: dict = None        # wave source line (wave_source), or None
     dt: float = 1e-3
     hydrostatic: bool = True
 
@@ -727,6 +728,45 @@ def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: f
     first, last = 2, (c.nj - 1 if side <= 2 else c.ni - 1)
     c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp,
                   table=table if table is not None else first_order_wave_table(H, T, depth))
+    return c
+
+
+def wave_source(c: Case, line: int, H: float, T: float, depth: float, ramp: float = 0.0, axis: str = "x",
+                table: dict | None = None) -> Case:
+    """A wave source line (MODEL WAVE-SRC X|Y ... FUNC MATRIX): the cell
+    column I = `line` (axis x, 1-based with ghosts) or row J = `line`
+    (axis y) emits waves to both sides, its strength the velocity column of
+    a first-order wave table unless `table` is given (the table is the one
+    of a wave maker, if the case has one)."""
+    if table is None and getattr(c, "wave", None) is None:
+        table = first_order_wave_table(H, T, depth)
+    c.source = dict(line=int(line) if axis == "x" else -int(line), depth=depth, period=T, ramp=ramp,
+                    table=table)
+    return c
+
+
+def source_flume(nx=120, ny=4, nz=40, dx=0.05, dz=0.01, depth=0.25, H=0.03, T=1.2, ramp=0.5,
+                 axis="x", sponge_width=1.0, dt=2.0e-3) -> Case:
+    """Still water between two damping zones with a wave source line in
+    the middle: along x, the column I = nx/2 + 2 of an nx x ny x nz flume;
+    along y, the row J = nx/2 + 2 of the same flume turned by 90 degrees
+    (ny x nx x nz).  The source is faded in over `ramp` periods."""
+    L, W = np.arange(nx + 1) * dx, np.arange(ny + 1) * dx
+    zs = np.arange(nz + 1) * dz
+    damp = [0.6, 0.6, sponge_width, depth]
+    if axis == "x":
+        c = new_case("source_flume_x", L, W, zs)
+        c.params.update(glxmin=0.0, glxmax=nx * dx, glymin=0.0, glymax=ny * dx, idamp=[2, 2, -1, -1],
+                        damp_xm=damp, damp_xp=damp)
+    else:
+        c = new_case("source_flume_y", W, L, zs)
+        c.params.update(glxmin=0.0, glxmax=ny * dx, glymin=0.0, glymax=nx * dx, idamp=[-1, -1, 2, 2],
+                        damp_ym=damp, damp_yp=damp)
+    c.params.update(wvlvl=depth, wbub=-1.0, cgepsr=1.0e-10)
+    init_f_still_water(c, depth)
+    c.dt = dt
+    finish(c)
+    wave_source(c, nx // 2 + 2, H, T, depth, ramp=ramp, axis=axis)
     return c
 
 

@@ -194,6 +194,14 @@ struct cadmas_handle {
   int nzz = 0;
   double *wzz = nullptr, *wun = nullptr, *wut = nullptr;  // DMTBZZ, DMTBUN, DMTBUT (device)
   double wave_level[4] = {0, 0, 0, 0};  // BCTYP(7,JD) = WVZ*AW of the last call
+  // wave source (ISCTYP(1) = line, SCTYP(1,3,8) = d, t, a) and its SRCUV
+  struct WaveSrc {
+    bool on = false;
+    int line = 0;
+    double d = 0.0, t = 0.0, a = 0.0;
+  } src;
+  double *srcuv = nullptr;
+  double src_level = 0.0;  // SCTYP(7) = WVZ*AW of the last step
 };
 
 #define TB(stage) h->tm.begin(h->s, (stage))
@@ -210,6 +218,7 @@ static void refresh_fld(cadmas_handle *h) {
   f.ff = h->ff; f.nf = h->nf; f.indc = h->indc; f.nf0 = h->nf0;
   f.bcu = h->bcu; f.bcv = h->bcv; f.bcw = h->bcw; f.bcp = h->bcp; f.bcf = h->bcf;
   f.bcvi = h->bcvi;
+  f.srcuv = h->srcuv;
 }
 
 static void refresh_prm(cadmas_handle *h) {
@@ -224,6 +233,8 @@ static void refresh_prm(cadmas_handle *h) {
   p.akk0 = P.akk0; p.aka0 = P.aka0; p.anu0 = P.anu0;
   p.loglaw = h->n_log_faces > 0 ? 1 : 0;
   for (int d = 0; d < 4; ++d) p.fixlvl[d] = (h->wave[d].on && h->mtbtyp == 3) ? 1 : 0;
+  p.iws = (h->src.on && h->src.line > 0) ? h->src.line : 0;
+  p.jws = (h->src.on && h->src.line < 0) ? -h->src.line : 0;
   // sponge parameters of vf_veuler.f:77-113
   p.ipa = 0;
   for (int d = 0; d < 4; ++d) {
@@ -302,6 +313,34 @@ static int wave_bc(cadmas_handle *h) {
     // a fixed-water-level table sets no velocities (vf_bwuwn.f:330-331)
     if (h->mtbtyp != 3) launch_wave(h->s, h->g, h->f, w, h->dint);
   }
+  return CADMAS_OK;
+}
+
+// VF_CWMSRC (vf_cwmsrc.f:46-143) for the matrix table: the phase and
+// fade-in at TNOW and VF_CWMTB1's row weights on the host, SRCUV of every
+// line of the source on the device (k_srcuv).  The reference calls it at
+// TNOW + DT before the step's V1CAL, which is this step's TNOW.
+static int wave_src(cadmas_handle *h) {
+  const double PI = 3.141592653589794, ZERO = 1.0e-20;  // VF_A0PRM.h
+  const cadmas_handle::WaveSrc &ws = h->src;
+  const double T = ws.t, T0 = h->dmtbt0;
+  float R4TN = (float)(T0 - h->tnow / T);
+  R4TN = R4TN - (float)(int)R4TN;
+  if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
+  double AW = 1.0, A = ws.a;
+  if (A >= ZERO) {
+    A = h->tnow / T / A;
+    if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
+  }
+  WaveDev w;
+  if (!cwmtb1(h, (double)R4TN, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
+  h->src_level = w.wvz * AW;
+  w.side = ws.line; w.first = 0; w.last = 0;
+  w.mtbtyp = h->mtbtyp; w.nzz = h->nzz; w.mtbnow = h->mtbnow;
+  w.d = ws.d; w.aw = AW; w.wvlvl = h->P.wvlvl;
+  w.sa = 0.0; w.sb = 0.0;
+  w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
+  launch_srcuv(h->s, h->g, h->f, w, h->srcuv, h->dint);
   return CADMAS_OK;
 }
 
@@ -633,6 +672,7 @@ static int bc_tail_v1(cadmas_handle *h) {
   launch_bsuwt(s, h->g, h->f, h->p);
   launch_bsuwt2(s, h->g, h->f);
   launch_bsuwn(s, h->g, h->f);
+  if (h->src.on) launch_bsuwn_src(s, h->g, h->f, h->p);
   launch_bwuwt(s, h->g, h->f, h->p, h->dint);
   launch_bwpp(s, h->g, h->f);
   return CADMAS_OK;
@@ -643,6 +683,8 @@ static int do_v1cal(cadmas_handle *h) {
   refresh_prm(h);
   refresh_fld(h);
   CK(cudaMemsetAsync(h->dint, 0, sizeof(int), s));
+  // the wave source's velocities of this step (vf_a1main.f:1035-1040)
+  if (h->src.on) { const int rs = wave_src(h); if (rs) return rs; }
   // fluxes, sources, provisional velocity (vf_v1cal.f:153-230)
   TB(CADMAS_STAGE_FLUX); launch_flux(s, h->g, h->f, h->p, h->wk); TE();
   const int nxt = h->cur ^ 1;
@@ -1080,7 +1122,7 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_st) cudaFreeHost(h->h_st);
   if (h->h_int) cudaFreeHost(h->h_int);
   if (h->h_res) cudaFreeHost(h->h_res);
-  for (double *q : {h->wzz, h->wun, h->wut}) if (q) cudaFree(q);
+  for (double *q : {h->wzz, h->wun, h->wut, h->srcuv}) if (q) cudaFree(q);
   for (double *q : {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww}) if (q) cudaFree(q);
   for (double *q : {h->ak, h->ae_k, h->ak2, h->ae2, h->anut, h->bck, h->bce, h->bck0, h->bce0}) if (q) cudaFree(q);
   if (h->wnet) cadmas_unet_destroy(h->wnet);
@@ -1094,17 +1136,11 @@ int cadmas_destroy(cadmas_handle *h) {
   return CADMAS_OK;
 }
 
-int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
-  if (!h || !w || !t || !t->tt || !t->hh || !t->zz || !t->un || !t->ut) return CADMAS_EINVAL;
-  if (w->side < 1 || w->side > 4 || t->ntt < 2 || t->nzz < 2) return CADMAS_EINVAL;
-  if (t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
-  if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
-  if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
-    g_last_error = "side already declared open";
-    return CADMAS_EINVAL;
-  }
-  const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;  // vf_iimdl.f:101-106
-  if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
+// The matrix table (/VF_AFILEI/ DMTB*), one for the wave sides and the
+// wave source as in the reference.
+static int set_table(cadmas_handle *h, const cadmas_wave_table *t) {
+  if (!t->tt || !t->hh || !t->zz || !t->un || !t->ut) return CADMAS_EINVAL;
+  if (t->ntt < 2 || t->nzz < 2 || t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
   for (int i = 1; i < t->ntt; ++i) if (!(t->tt[i] >= t->tt[i - 1])) return CADMAS_EINVAL;
   for (int k = 1; k < t->nzz; ++k) if (!(t->zz[k] > t->zz[k - 1])) return CADMAS_EINVAL;
   const size_t nzt = (size_t)t->nzz * t->ntt;
@@ -1124,9 +1160,43 @@ int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave
   h->nzz = t->nzz;
   h->mtbtyp = t->mtbtyp;
   h->dmtbt0 = t->phase0;
+  return CADMAS_OK;
+}
+
+int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
+  if (!h || !w || !t) return CADMAS_EINVAL;
+  if (w->side < 1 || w->side > 4) return CADMAS_EINVAL;
+  if (t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
+  if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
+  if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
+    g_last_error = "side already declared open";
+    return CADMAS_EINVAL;
+  }
+  const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;  // vf_iimdl.f:101-106
+  if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
+  { const int rt = set_table(h, t); if (rt) return rt; }
   cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
   ws.on = true; ws.first = w->first; ws.last = w->last;
   ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
+  return CADMAS_OK;
+}
+
+int cadmas_set_wave_source(cadmas_handle *h, const cadmas_wave_src *src, const cadmas_wave_table *t) {
+  if (!h || !src) return CADMAS_EINVAL;
+  const int L = src->line;
+  if (L == 0 || (L > 0 && (L < 2 || L > h->g.NI - 1)) || (L < 0 && (-L < 2 || -L > h->g.NJ - 1)))
+    return CADMAS_EINVAL;  // vf_iimdl.f:119-133
+  if (t) { const int rt = set_table(h, t); if (rt) return rt; }
+  if (h->nzz == 0) { g_last_error = "the wave source needs a matrix table"; return CADMAS_EINVAL; }
+  if (h->mtbtyp == 3) { g_last_error = "(WAVE-SRC) MTBTYP ERROR."; return CADMAS_EINVAL; }  // vf_csetup.f:267
+  if (!(src->period > 0.0) || (h->mtbtyp == 1 && !(src->depth > 0.0))) return CADMAS_EINVAL;
+  const size_t n = (size_t)(L > 0 ? h->g.NJ : h->g.NI) * h->g.NK;
+  if (h->srcuv) { cudaFree(h->srcuv); h->srcuv = nullptr; }
+  { const int ra = dalloc(&h->srcuv, n); if (ra) return ra; }  // SRCUV = 0 (vf_a1main.f:690)
+  h->src.on = true; h->src.line = L;
+  h->src.d = src->depth; h->src.t = src->period; h->src.a = src->ramp;
+  refresh_fld(h);
+  refresh_prm(h);
   return CADMAS_OK;
 }
 

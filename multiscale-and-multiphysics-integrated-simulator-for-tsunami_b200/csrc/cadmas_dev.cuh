@@ -64,6 +64,9 @@ struct Prm {
   // fixlvl[JD-1] = 1: side JD is a wave side whose table fixes the water
   // level (MTBTYP 3); its faces then act as free faces
   int fixlvl[4];
+  // wave source (ISCTYP(1)): IWS > 0 the x source's column I, JWS > 0 the
+  // y source's row J (0: none); SRCUV in Fld::srcuv
+  int iws, jws;
 };
 
 // A boundary face of a fixed-water-level side: on the domain boundary of
@@ -84,6 +87,9 @@ struct Fld {
   int *nf, *indc, *nf0;
   double *bcu, *bcv, *bcw, *bcp, *bcf;
   const double *bcvi;  // BCVI roughness of rough-wall faces
+  // SRCUV(NUMIJ,NUMK) of the wave source (NUMIJ = NUMJ for an x source,
+  // NUMI for a y source); read only where Prm::iws or jws is set
+  const double *srcuv;
 };
 
 // DROPTX, DROPTY, DROPTZ, DROPUU, DROPVV, DROPWW of the droplet model

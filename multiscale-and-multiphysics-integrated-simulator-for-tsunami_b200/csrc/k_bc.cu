@@ -615,7 +615,50 @@ __global__ void k_cdtcal_fin(const double *rb, long long nrows, double dt0, doub
 #define BL(kern, ...) if (g.NB > 0) (kern<<<(g.NB + 255) / 256, 256, 0, s>>>(__VA_ARGS__), count_launch())
 void launch_bsuwt(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p) { RL(k_bsuwt, g, f, p); }
 void launch_bsuwt2(cudaStream_t s, const Geo &g, const Fld &f) { RL(k_bsuwt2, g, f); }
+// Wave-source part of VF_BSUWN (vf_bsuwn.f:81-118): on the source's line,
+// the first surface cell of each column from the bottom (obstacle, fluid
+// and gas cells skipped) passes the source flow 2 XX(4,I) SRCUV (or
+// YY(4,J)) through its face toward the gas.  One thread per column.  A
+// column writes a face whose other cell is fluid or gas at that height
+// (the surface cell's orientation, VF_FNFPRV), never a face another
+// column of the line writes at the same height.
+__global__ void k_bsuwn_src(Geo g, Fld f, Prm p) {
+  const bool xs = p.iws != 0;
+  const int IJ = 2 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (IJ > (xs ? g.NJ : g.NI) - 1) return;
+  const int I = xs ? p.iws : IJ, J = xs ? IJ : p.jws;
+  for (int K = 2; K <= g.NK - 1; ++K) {
+    const long long c = cid(g, I, J, K);
+    const int N = f.nf[c];
+    if (N == -1 || N == 0 || N == 8) continue;
+    const double Q = xs ? 2.0 * gx(g, 4, I) * f.srcuv[(J - 1) + (long long)g.NJ * (K - 1)]
+                        : 2.0 * gy(g, 4, J) * f.srcuv[(I - 1) + (long long)g.NI * (K - 1)];
+    if (N == 1) {
+      const long long d = cid(g, I + 1, J, K);
+      f.uu[d] = f.uu[d] + gx(g, 2, I) * Q / f.ggx[d];
+    } else if (N == 2) {
+      f.uu[c] = f.uu[c] - gx(g, 2, I) * Q / f.ggx[c];
+    } else if (N == 3) {
+      const long long d = cid(g, I, J + 1, K);
+      f.vv[d] = f.vv[d] + gy(g, 2, J) * Q / f.ggy[d];
+    } else if (N == 4) {
+      f.vv[c] = f.vv[c] - gy(g, 2, J) * Q / f.ggy[c];
+    } else if (N == 5) {
+      const long long d = cid(g, I, J, K + 1);
+      f.ww[d] = f.ww[d] + gz(g, 2, K) * Q / f.ggz[d];
+    } else if (N == 6) {
+      f.ww[c] = f.ww[c] - gz(g, 2, K) * Q / f.ggz[c];
+    }
+    break;
+  }
+}
+
 void launch_bsuwn(cudaStream_t s, const Geo &g, const Fld &f) { RL(k_bsuwn, g, f); }
+void launch_bsuwn_src(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p) {
+  const int n = (p.iws != 0 ? g.NJ : g.NI) - 2;
+  k_bsuwn_src<<<(n + 127) / 128, 128, 0, s>>>(g, f, p);
+  count_launch();
+}
 void launch_bsuwn3(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p) { RL(k_bsuwn3, g, f, p); }
 void launch_bsuwem(cudaStream_t s, const Geo &g, const Fld &f, int *nlim) {
   RL(k_bsuwem_count, g, f, nlim);

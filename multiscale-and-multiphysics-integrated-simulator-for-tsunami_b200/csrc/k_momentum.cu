@@ -445,6 +445,11 @@ __global__ void k_predict(Geo g, Fld f, Prm p, const double *FLUU, const double 
                               XX_(2, I) * (A(WW, I1, J, K) + A(WW, I1, J, K + 1))) * 0.5;
       double UVW = sqrt(Uc * Uc + V * V + W * W);
       Q = Q - 0.5 * CD * XX_(5, I) * (1.0 - f.ggx[c]) * Uc * UVW;
+      // wave source of an x line (vf_vgene.f:149-152)
+      if (p.iws != 0 && (p.iws == I || p.iws + 1 == I)) {
+        const double QS = 2.0 * XX_(4, p.iws) * f.srcuv[(J - 1) + (long long)NJ * (K - 1)];
+        Q = Q + UU[c] * QS * XX_(2, p.iws) * XX_(5, I) * 0.5;
+      }
       // VF_VEULER vf_veuler.f:119-128
       double GV = XX_(6, I) * (XX_(2, I) * GLV[c] + XX_(2, I - 1) * A(GLV, I - 1, J, K));
       double GV0 = XX_(6, I) * (XX_(2, I) * GLV[c] + XX_(2, I - 1) * A(GLV, I - 1, J, K));
@@ -480,6 +485,11 @@ __global__ void k_predict(Geo g, Fld f, Prm p, const double *FLUU, const double 
                               YY_(2, J) * (A(WW, I, J1, K) + A(WW, I, J1, K + 1))) * 0.5;
       double UVW = sqrt(U * U + Vc * Vc + W * W);
       Q = Q - 0.5 * CD * YY_(5, J) * (1.0 - f.ggy[c]) * Vc * UVW;
+      // wave source of a y line (vf_vgene.f:225-228)
+      if (p.jws != 0 && (p.jws == J || p.jws + 1 == J)) {
+        const double QS = 2.0 * YY_(4, p.jws) * f.srcuv[(I - 1) + (long long)NI * (K - 1)];
+        Q = Q + VV[c] * QS * YY_(2, p.jws) * YY_(5, J) * 0.5;
+      }
       double GV = YY_(6, J) * (YY_(2, J) * GLV[c] + YY_(2, J - 1) * A(GLV, I, J - 1, K));
       double GV0 = YY_(6, J) * (YY_(2, J) * GLV[c] + YY_(2, J - 1) * A(GLV, I, J - 1, K));
       double DV = (XX_(4, I) * (A(FLVU, I + 1, J, K) - FLVU[c]) + YY_(5, J) * (FLVV[c] - A(FLVV, I, J - 1, K)) +
@@ -515,6 +525,19 @@ __global__ void k_predict(Geo g, Fld f, Prm p, const double *FLUU, const double 
       double UVW = sqrt(U * U + V * V + Wc * Wc);
       Q = Q - 0.5 * CD * ZZ_(5, K) * (1.0 - f.ggz[c]) * Wc * UVW;
       Q = Q - GVg * p.grz0;
+      // wave source (vf_vgene.f:304-315)
+      if (p.iws == I) {
+        const double Q1 = 2.0 * XX_(4, I) * f.srcuv[(J - 1) + (long long)NJ * (K - 2)];
+        const double Q2 = 2.0 * XX_(4, I) * f.srcuv[(J - 1) + (long long)NJ * (K - 1)];
+        Q = Q + ZZ_(5, K) * (Q2 - Q1) * p.anu0 / 3.0;
+        Q = Q + WW[c] * (Q1 + Q2) * 0.5;
+      }
+      if (p.jws == J) {
+        const double Q1 = 2.0 * YY_(4, J) * f.srcuv[(I - 1) + (long long)NI * (K - 2)];
+        const double Q2 = 2.0 * YY_(4, J) * f.srcuv[(I - 1) + (long long)NI * (K - 1)];
+        Q = Q + ZZ_(5, K) * (Q2 - Q1) * p.anu0 / 3.0;
+        Q = Q + WW[c] * (Q1 + Q2) * 0.5;
+      }
       double DR = 0.0;
       Q = Q - GVg * p.grz0 * DR / p.rho0;
       double GV = ZZ_(6, K) * (ZZ_(2, K) * GLV[c] + ZZ_(2, K - 1) * A(GLV, I, J, K - 1));
@@ -595,6 +618,70 @@ __global__ void k_bwuwn(Geo g, Fld f, Prm p, int *err) {
     // (vf_bwuwn.f:234-235, 481-598)
   } else {
     atomicOr(err, ERR_PG);
+  }
+}
+
+// ------------------------------------------------------- VF_CWMSRC
+// The wave source's velocity SRCUV(IJ,K) of every line IJ = 2..NUMIJ-1
+// (vf_cwmsrc.f:100-143) from the matrix table: the column's water level
+// scales the heights (MTBTYP 1), VF_CWMTB2's height interpolation between
+// the rows the host chose (phase weights wt1/wt2 at row mtbnow), times
+// the fade-in AW.  One thread per line.
+__global__ void k_srcuv(Geo g, Fld f, WaveDev w, double *SRCUV, int *err) {
+  const int IJ = 2 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const bool xs = (w.side > 0);  // x source at I = side, y source at J = -side
+  const int NIJ = xs ? g.NJ : g.NI, NK = g.NK;
+  if (IJ > NIJ - 1) return;
+  const int I = xs ? w.side : IJ, J = xs ? IJ : -w.side;
+  double VWS;
+  if (w.mtbtyp == 1) {
+    double VAL = 0.0;
+    for (int K = 2; K <= NK - 1; ++K) {
+      const int NW = f.nf[cid(g, I, J, K)];
+      if (NW == -1) {
+        VAL = VAL + gz(g, 2, K) * 1.0;
+      } else if (NW == 0) {
+        VAL = VAL + gz(g, 2, K) * f.ff[cid(g, I, J, K)];
+      } else if (NW != 8) {
+        VAL = VAL + gz(g, 2, K) * f.ff[cid(g, I, J, K)];
+        break;
+      }
+    }
+    VAL = VAL - (w.wvlvl - gz(g, 1, 2));
+    VWS = (w.wvz + w.d) / (VAL + w.d);
+  } else {
+    VWS = 1.0;
+  }
+  int KM = 1;
+  const int nz = w.nzz;
+  for (int K = 2; K <= NK - 1; ++K) {
+    double ZC = (gz(g, 1, K) + gz(g, 1, K + 1)) * 0.5 - w.wvlvl;
+    ZC = VWS * (ZC + w.d) - w.d;
+    double W1, W2;
+    if (ZC <= w.zz[0]) {
+      KM = 1; W1 = 1.0; W2 = 0.0;
+    } else if (ZC >= w.zz[nz - 1]) {
+      KM = nz - 1; W1 = 0.0; W2 = 1.0;
+    } else {
+      int KP = 0;
+      W1 = 0.0; W2 = 0.0;
+      for (int k = KM; k <= nz - 1; ++k) {
+        if (w.zz[k - 1] <= ZC && ZC <= w.zz[k]) {
+          KP = k;
+          W2 = 1.0 / (w.zz[k] - w.zz[k - 1]);
+          W1 = (w.zz[k] - ZC) * W2;
+          W2 = (ZC - w.zz[k - 1]) * W2;
+          break;
+        }
+      }
+      if (KP == 0) { atomicOr(err, ERR_PG); return; }
+      KM = KP;
+    }
+    const long long i0 = (long long)nz * (w.mtbnow - 1), i1 = i0 + nz;
+    const double P1 = W1 * w.un[i0 + KM - 1] + W2 * w.un[i0 + KM];
+    const double P2 = W1 * w.un[i1 + KM - 1] + W2 * w.un[i1 + KM];
+    const double UN = w.wt1 * P1 + w.wt2 * P2;
+    SRCUV[(IJ - 1) + (long long)NIJ * (K - 1)] = UN * VWS * w.aw;
   }
 }
 
@@ -769,6 +856,11 @@ void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, i
   const int n = w.last - w.first + 1;
   if (n <= 0) return;
   k_wave<<<(n + 127) / 128, 128, 0, s>>>(g, f, w, err);
+  count_launch();
+}
+void launch_srcuv(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, double *srcuv, int *err) {
+  const int n = (w.side > 0 ? g.NJ : g.NI) - 2;
+  k_srcuv<<<(n + 127) / 128, 128, 0, s>>>(g, f, w, srcuv, err);
   count_launch();
 }
 void launch_open(cudaStream_t s, const Geo &g, const Fld &f, const OpenDev &o, const double *ub,

@@ -104,6 +104,9 @@ __global__ void k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
                 AXZ * (A(f.ggy, I, JP, K) * A(f.vv, I, JP, K) - f.ggy[c] * f.vv[c]) +
                 AXY * (A(f.ggz, I, J, KP) * A(f.ww, I, J, KP) - f.ggz[c] * f.ww[c]);
     double VQ = -(GGV[c] - GGV[c]) * DTI * AVL;
+    // wave source line (vf_vpcoef.f:349-350)
+    if (p.iws == I) VQ = 2.0 * ZZ_(2, K) * f.srcuv[(J - 1) + (long long)g.NJ * (K - 1)] * YY_(2, J);
+    if (p.jws == J) VQ = 2.0 * ZZ_(2, K) * f.srcuv[(I - 1) + (long long)g.NI * (K - 1)] * XX_(2, I);
     BB = VD - VQ;
   } else if (N == 5) {
     double PSI = ZZ_(3, K) / (0.5 * ZZ_(2, K - 1) + FF[c] * ZZ_(2, K));

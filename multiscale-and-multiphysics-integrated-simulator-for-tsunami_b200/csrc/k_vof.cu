@@ -102,8 +102,23 @@ __global__ void k_feuler(Geo g, Fld f, Prm p, const double *FLFU, const double *
     if (f.nf[c] != -1) {
       double G = f.ggv[c];
       double G0 = G - (G - G) * 1.0;
+      // QF of VF_FGENE (vf_fgene.f:42-70): on the wave source's line, the
+      // fluid cells up to and the first surface cell of the column (gas
+      // cells below it skipped) gain F * 2 XX(4,I) SRCUV (or YY(4,J))
+      double QF = 0.0;
+      if ((p.iws == I || p.jws == J) && f.nf[c] != 8) {
+        bool below = true;  // no surface cell under this one
+        for (int K2 = 2; K2 < K; ++K2) {
+          const int n2 = A(f.nf, I, J, K2);
+          if (n2 != -1 && n2 != 0 && n2 != 8) { below = false; break; }
+        }
+        if (below) {
+          if (p.iws == I) QF = QF + f.ff[c] * (2.0 * XX_(4, I) * f.srcuv[(J - 1) + (long long)g.NJ * (K - 1)]);
+          if (p.jws == J) QF = QF + f.ff[c] * (2.0 * YY_(4, J) * f.srcuv[(I - 1) + (long long)g.NI * (K - 1)]);
+        }
+      }
       double DF = (XX_(4, I) * (A(FLFU, I + 1, J, K) - FLFU[c]) + YY_(4, J) * (A(FLFV, I, J + 1, K) - FLFV[c]) +
-                   ZZ_(4, K) * (A(FLFW, I, J, K + 1) - FLFW[c]) + p.dtnow * 0.0);
+                   ZZ_(4, K) * (A(FLFW, I, J, K + 1) - FLFW[c]) + p.dtnow * QF);
       f.ff[c] = (G0 * f.ff[c] + DF) / G;
     }
   }

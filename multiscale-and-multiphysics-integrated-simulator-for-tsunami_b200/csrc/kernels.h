@@ -201,6 +201,9 @@ void launch_bwuwn(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, int 
 // VF_BWFFSF: F of the cells next to a fixed-water-level side set to the level wl
 void launch_bwffsf(cudaStream_t s, const Geo &g, const Fld &f, int side, int first, int last, double wl);
 void launch_wave(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, int *err);
+// VF_CWMSRC: SRCUV(NUMIJ,NUMK) of the wave source from the matrix table;
+// w.side = ISCTYP(1) (> 0 x source at I, < 0 y source at J = -side)
+void launch_srcuv(cudaStream_t s, const Geo &g, const Fld &f, const WaveDev &w, double *srcuv, int *err);
 // Open (radiation) faces of one side; ub/vb/wb the velocities the blend
 // reads (the start of the step's, or a copy of the present ones at set-up)
 void launch_open(cudaStream_t s, const Geo &g, const Fld &f, const OpenDev &o, const double *ub,
@@ -368,6 +371,8 @@ void launch_bsppfl(cudaStream_t s, const Geo &g, const Fld &f, const double *pp0
 void launch_bsuwt(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p);
 void launch_bsuwt2(cudaStream_t s, const Geo &g, const Fld &f);
 void launch_bsuwn(cudaStream_t s, const Geo &g, const Fld &f);
+// the wave source's part of VF_BSUWN (p.iws or p.jws set)
+void launch_bsuwn_src(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p);
 void launch_bsuwn3(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p);
 void launch_bsuwem(cudaStream_t s, const Geo &g, const Fld &f, int *nlim);
 void launch_bspp(cudaStream_t s, const Geo &g, const Fld &f);

@@ -414,6 +414,14 @@ struct orc_handle {
   }
   int MTBTYP = 0, MTBNOW = 0;
   double DMTBT0 = 0;
+  // wave source (MODEL WAVE-SRC, FUNC MATRIX): ISCTYP(1) = ISC (> 0 the x
+  // line I, < 0 the y line -J), SCTYP(1,3,8) = SD, ST, SA; SRCUV(NUMIJ,NUMK)
+  int ISC = 0;
+  double SD = 0, ST = 0, SA = 0;
+  vd SRCUV;
+  int IWS() const { return ISC > 0 ? ISC : 0; }
+  int JWS() const { return ISC < 0 ? -ISC : 0; }
+  double SRC(int ij, int k) const { return SRCUV[(size_t)(ij - 1) + (size_t)(ISC > 0 ? NJ : NI) * (size_t)(k - 1)]; }
   vd DMTBTT, DMTBHH, DMTBZZ, DMTBUN, DMTBUT;
   int NNOW = 0;
   // work arrays WK01..WK17
@@ -953,7 +961,7 @@ struct orc_handle {
         }
   }
 
-  // VF_VGENE  vf_vgene.f:84-332 (IDRGN<=0 drag, no k-eps/T/C/wave source)
+  // VF_VGENE  vf_vgene.f:84-332 (IDRGN<=0 drag, wave source, no T/C)
   void vgene(vd &QU, vd &QV, vd &QW) {
     const double RI = 1.0 / P.rho0;
     for (int K = 2; K <= NK - 1; ++K)
@@ -972,6 +980,12 @@ struct orc_handle {
                                  X_(2, I) * (WW[id(I1, J, K)] + WW[id(I1, J, K + 1)])) * 0.5;
           double UVW = std::sqrt(U * U + V * V + W * W);
           Q = Q - 0.5 * CD * X_(5, I) * (1.0 - GGX[id(I, J, K)]) * U * UVW;
+          // wave source  vf_vgene.f:149-152
+          const int IWS_ = IWS();
+          if (IWS_ != 0 && (IWS_ == I || IWS_ + 1 == I)) {
+            double QS = 2.0 * X_(4, IWS_) * SRC(J, K);
+            Q = Q + UU[id(I, J, K)] * QS * X_(2, IWS_) * X_(5, I) * 0.5;
+          }
         }
     for (int K = 2; K <= NK - 1; ++K)
       for (int J = 3; J <= NJ - 1; ++J)
@@ -989,6 +1003,12 @@ struct orc_handle {
                                  Y_(2, J) * (WW[id(I, J1, K)] + WW[id(I, J1, K + 1)])) * 0.5;
           double UVW = std::sqrt(U * U + V * V + W * W);
           Q = Q - 0.5 * CD * Y_(5, J) * (1.0 - GGY[id(I, J, K)]) * V * UVW;
+          // wave source  vf_vgene.f:225-228
+          const int JWS_ = JWS();
+          if (JWS_ != 0 && (JWS_ == J || JWS_ + 1 == J)) {
+            double QS = 2.0 * Y_(4, JWS_) * SRC(I, K);
+            Q = Q + VV[id(I, J, K)] * QS * Y_(2, JWS_) * Y_(5, J) * 0.5;
+          }
         }
     for (int K = 3; K <= NK - 1; ++K) {
       int K1 = K - 1;
@@ -1007,6 +1027,19 @@ struct orc_handle {
           double UVW = std::sqrt(U * U + V * V + W * W);
           Q = Q - 0.5 * CD * Z_(5, K) * (1.0 - GGZ[id(I, J, K)]) * W * UVW;
           Q = Q - GV * P.grz0;
+          // wave source  vf_vgene.f:304-315
+          if (IWS() == I) {
+            double Q1 = 2.0 * X_(4, I) * SRC(J, K - 1);
+            double Q2 = 2.0 * X_(4, I) * SRC(J, K);
+            Q = Q + Z_(5, K) * (Q2 - Q1) * P.anu0 / 3.0;
+            Q = Q + WW[id(I, J, K)] * (Q1 + Q2) * 0.5;
+          }
+          if (JWS() == J) {
+            double Q1 = 2.0 * Y_(4, J) * SRC(I, K - 1);
+            double Q2 = 2.0 * Y_(4, J) * SRC(I, K);
+            Q = Q + Z_(5, K) * (Q2 - Q1) * P.anu0 / 3.0;
+            Q = Q + WW[id(I, J, K)] * (Q1 + Q2) * 0.5;
+          }
           double DR = 0.0;  // no temperature / concentration (vf_vgene.f:318-327)
           Q = Q - GV * P.grz0 * DR / P.rho0;
         }
@@ -1499,6 +1532,8 @@ struct orc_handle {
                         AXZ * (GGY[id(I, JP, K)] * VV[id(I, JP, K)] - GGY[c] * VV[c]) +
                         AXY * (GGZ[id(I, J, KP)] * WW[id(I, J, KP)] - GGZ[c] * WW[c]);
             double VQ = -(GGV[c] - GGV[c]) * DTI * AVL;
+            if (IWS() == I) VQ = 2.0 * Z_(2, K) * SRC(J, K) * Y_(2, J);  // vf_vpcoef.f:349-350
+            if (JWS() == J) VQ = 2.0 * Z_(2, K) * SRC(I, K) * X_(2, I);
             BB[c] = VD - VQ;
           } else if (N == 5) {
             double PSI = Z_(3, K) / (0.5 * Z_(2, K - 1) + FF[c] * Z_(2, K));
@@ -2004,7 +2039,7 @@ struct orc_handle {
     }
   }
 
-  // VF_BSUWN  vf_bsuwn.f:57-86 (no wave source)
+  // VF_BSUWN  vf_bsuwn.f:57-118
   void bsuwn() {
     for (int L = 0; L < NUMS; ++L) {
       int I, J, K;
@@ -2020,6 +2055,29 @@ struct orc_handle {
       else if (NF0 == 4) VV[id(I, J, K)] = (FYP + Y_(2, J) * (X_(4, I) * (FXP - FXM) + Z_(4, K) * (FZP - FZM))) / GGY[id(I, J, K)];
       else if (NF0 == 1) UU[id(I1, J, K)] = (FXM - X_(2, I) * (Y_(4, J) * (FYP - FYM) + Z_(4, K) * (FZP - FZM))) / GGX[id(I1, J, K)];
       else if (NF0 == 2) UU[id(I, J, K)] = (FXP + X_(2, I) * (Y_(4, J) * (FYP - FYM) + Z_(4, K) * (FZP - FZM))) / GGX[id(I, J, K)];
+    }
+    // wave source  vf_bsuwn.f:81-118
+    const int IWS_ = IWS(), JWS_ = JWS();
+    if (IWS_ != 0 || JWS_ != 0) {
+      for (int J = 2; J <= NJ - 1; ++J)
+        for (int I = 2; I <= NI - 1; ++I) {
+          if (!(IWS_ == I || JWS_ == J)) continue;
+          for (int K = 2; K <= NK - 1; ++K) {
+            const int N = NF[id(I, J, K)];
+            if (N == -1 || N == 0) continue;
+            if (N == 8) continue;
+            double Q = 0.0;
+            if (IWS_ == I) Q = 2.0 * X_(4, I) * SRC(J, K);
+            if (JWS_ == J) Q = 2.0 * Y_(4, J) * SRC(I, K);
+            if (N == 1) UU[id(I + 1, J, K)] = UU[id(I + 1, J, K)] + X_(2, I) * Q / GGX[id(I + 1, J, K)];
+            else if (N == 2) UU[id(I, J, K)] = UU[id(I, J, K)] - X_(2, I) * Q / GGX[id(I, J, K)];
+            else if (N == 3) VV[id(I, J + 1, K)] = VV[id(I, J + 1, K)] + Y_(2, J) * Q / GGY[id(I, J + 1, K)];
+            else if (N == 4) VV[id(I, J, K)] = VV[id(I, J, K)] - Y_(2, J) * Q / GGY[id(I, J, K)];
+            else if (N == 5) WW[id(I, J, K + 1)] = WW[id(I, J, K + 1)] + Z_(2, K) * Q / GGZ[id(I, J, K + 1)];
+            else if (N == 6) WW[id(I, J, K)] = WW[id(I, J, K)] - Z_(2, K) * Q / GGZ[id(I, J, K)];
+            break;
+          }
+        }
     }
   }
 
@@ -2527,16 +2585,53 @@ struct orc_handle {
     return CADMAS_OK;
   }
 
-  // VF_FEULER  vf_feuler.f:43-56 (QF = 0, GGV0 = GGV, LOOPS = 1)
+  // VF_FGENE  vf_fgene.f:42-70: QF of the wave source's line
+  void fgene(vd &QF) const {
+    const int IWS_ = IWS(), JWS_ = JWS();
+    if (IWS_ == 0 && JWS_ == 0) return;
+    for (int J = 2; J <= NJ - 1; ++J)
+      for (int I = 2; I <= NI - 1; ++I)
+        for (int K = 2; K <= NK - 1; ++K) {
+          if (IWS_ == I) {
+            const size_t c = id(I, J, K);
+            if (NF[c] == -1) {
+            } else if (NF[c] == 0) {
+              double Q = 2.0 * X_(4, I) * SRC(J, K);
+              QF[c] = QF[c] + FF[c] * Q;
+            } else if (NF[c] != 8) {
+              double Q = 2.0 * X_(4, I) * SRC(J, K);
+              QF[c] = QF[c] + FF[c] * Q;
+              break;
+            }
+          }
+          if (JWS_ == J) {
+            const size_t c = id(I, J, K);
+            if (NF[c] == -1) {
+            } else if (NF[c] == 0) {
+              double Q = 2.0 * Y_(4, J) * SRC(I, K);
+              QF[c] = QF[c] + FF[c] * Q;
+            } else if (NF[c] != 8) {
+              double Q = 2.0 * Y_(4, J) * SRC(I, K);
+              QF[c] = QF[c] + FF[c] * Q;
+              break;
+            }
+          }
+        }
+  }
+
+  // VF_FEULER  vf_feuler.f:43-56 (GGV0 = GGV, LOOPS = 1); QF from VF_FGENE
   void feuler(const vd &FLFU, const vd &FLFV, const vd &FLFW) {
+    vd QF;
+    if (ISC != 0) { QF.assign(FF.size(), 0.0); fgene(QF); }
     for (int K = 2; K <= NK - 1; ++K)
       for (int J = 2; J <= NJ - 1; ++J)
         for (int I = 2; I <= NI - 1; ++I) {
           size_t c = id(I, J, K);
           if (NF[c] == -1) continue;
           double G0 = GGV[c] - (GGV[c] - GGV[c]) * 1.0;
+          const double qf = ISC != 0 ? QF[c] : 0.0;
           double DF = (X_(4, I) * (FLFU[id(I + 1, J, K)] - FLFU[c]) + Y_(4, J) * (FLFV[id(I, J + 1, K)] - FLFV[c]) +
-                       Z_(4, K) * (FLFW[id(I, J, K + 1)] - FLFW[c]) + DTNOW * 0.0);
+                       Z_(4, K) * (FLFW[id(I, J, K + 1)] - FLFW[c]) + DTNOW * qf);
           FF[c] = (G0 * FF[c] + DF) / GGV[c];
         }
   }
@@ -3127,11 +3222,60 @@ struct orc_handle {
     return std::sqrt(v);
   }
 
+  // VF_CWMSRC  vf_cwmsrc.f:46-143 (N = -3, the matrix table) at TDMY =
+  // TNOW: SRCUV of every line of the source
+  int cwmsrc() {
+    const double PI = 3.141592653589794, ZERO = 1.0e-20;
+    const int IJ1 = 2, IJ2 = (ISC > 0 ? NJ : NI) - 1;
+    const double D = SD, T = ST, T0 = DMTBT0;
+    double A = SA;
+    float R4TN = (float)(T0 - TNOW / T);
+    R4TN = R4TN - (float)(int)R4TN;
+    if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
+    double AW = 1.0;
+    if (A >= ZERO) {
+      A = TNOW / T / A;
+      if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
+    }
+    const double WVT = (double)R4TN;
+    double WMT1, WMT2, WVZ;
+    if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
+    const int NIJ = ISC > 0 ? NJ : NI;
+    for (int IJ = IJ1; IJ <= IJ2; ++IJ) {
+      const int I = ISC > 0 ? ISC : IJ, J = ISC > 0 ? IJ : -ISC;
+      double VWS;
+      if (MTBTYP == 1) {
+        double VAL = 0.0;
+        for (int K = 2; K <= NK - 1; ++K) {
+          const int NW = NF[id(I, J, K)];
+          if (NW == -1) VAL = VAL + Z_(2, K) * 1.0;
+          else if (NW == 0) VAL = VAL + Z_(2, K) * FF[id(I, J, K)];
+          else if (NW != 8) { VAL = VAL + Z_(2, K) * FF[id(I, J, K)]; break; }
+        }
+        VAL = VAL - (P.wvlvl - Z_(1, 2));
+        VWS = (WVZ + D) / (VAL + D);
+      } else {
+        VWS = 1.0;
+      }
+      int KMT = 1;
+      for (int K = 2; K <= NK - 1; ++K) {
+        double ZC = (Z_(1, K) + Z_(1, K + 1)) * 0.5 - P.wvlvl;
+        ZC = VWS * (ZC + D) - D;
+        double UN, UT;
+        if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
+        SRCUV[(size_t)(IJ - 1) + (size_t)NIJ * (size_t)(K - 1)] = UN * VWS * AW;
+      }
+    }
+    return CADMAS_OK;
+  }
+
   // ---------------------------------------------------------------- drivers
-  // VF_V1CAL  vf_v1cal.f:118-297 (ILOOP = 1)
+  // VF_V1CAL  vf_v1cal.f:118-297 (ILOOP = 1), after the time loop's
+  // VF_CWMSRC (vf_a1main.f:1035-1040)
   int v1cal() {
     Timer T;
     size_t N = UU.size();
+    if (ISC != 0) { const int rs = cwmsrc(); if (rs) return rs; }
     T.start();
     for (int w = 1; w <= 12; ++w) WK[w].assign(N, 0.0);
     WK[13] = UU; WK[14] = VV; WK[15] = WW;
@@ -3825,6 +3969,25 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
   h->DMTBT0 = t->phase0;
   orc_handle::Wave &v = h->WV[w->side - 1];
   v.on = 1; v.l1 = w->first; v.l2 = w->last; v.d = w->depth; v.t = w->period; v.a = w->ramp;
+  return CADMAS_OK;
+}
+
+int orc_set_wave_source(orc_handle *h, const cadmas_wave_src *src, const cadmas_wave_table *t) {
+  if (!h || !src || src->line == 0) return CADMAS_EINVAL;
+  if (t) {
+    if (t->ntt < 2 || t->nzz < 2 || t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
+    h->DMTBTT.assign(t->tt, t->tt + t->ntt);
+    h->DMTBHH.assign(t->hh, t->hh + t->ntt);
+    h->DMTBZZ.assign(t->zz, t->zz + t->nzz);
+    h->DMTBUN.assign(t->un, t->un + (size_t)t->nzz * t->ntt);
+    h->DMTBUT.assign(t->ut, t->ut + (size_t)t->nzz * t->ntt);
+    h->MTBTYP = t->mtbtyp;
+    h->DMTBT0 = t->phase0;
+  }
+  if (h->DMTBZZ.empty() || h->MTBTYP == 3) return CADMAS_EINVAL;  // vf_csetup.f:267
+  h->ISC = src->line;
+  h->SD = src->depth; h->ST = src->period; h->SA = src->ramp;
+  h->SRCUV.assign((size_t)(src->line > 0 ? h->NJ : h->NI) * h->NK, 0.0);
   return CADMAS_OK;
 }
 

@@ -113,6 +113,10 @@ class Oracle:
         for op in getattr(case, "open", None) or []:
             self.lib.orc_set_open.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
             self._rc(self.lib.orc_set_open(self.h, int(op["side"]), float(op["depth"]), float(op["period"])))
+        if getattr(case, "source", None):
+            ws, tab, keep = P.source_structs(case.source)
+            self.lib.orc_set_wave_source.argtypes = [C.c_void_p, C.POINTER(P.WaveSrc), C.POINTER(P.WaveTable)]
+            self._rc(self.lib.orc_set_wave_source(self.h, C.byref(ws), C.byref(tab) if tab else None))
         self.set_state(P.initial_state(case))
 
     def _rc(self, rc):

@@ -45,6 +45,9 @@ CASES = {
     # wave maker at X-, open (radiation) boundaries at X+ and Y+
     "open_flume_0_10": dict(builder="open_flume", kw=dict(nx=64, ny=4, nz=48, y_open=True), steps=10,
                             sum_mode=0, over={}),
+    # wave source line (MODEL WAVE-SRC ... FUNC MATRIX) along x
+    "source_flume_x_40": dict(builder="source_flume", kw=dict(nx=64, nz=32, ramp=0.2), steps=40, sum_mode=0,
+                              over={}),
 }
 DROP = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB = ("ak", "ae", "anut", "anu", "bck", "bce")

@@ -463,3 +463,15 @@ def test_ensemble_of_mixed_tile_shapes(gpu_lib, pkg):
         sa, sb = a.get_state(), b.get_state()
         for k in ("uu", "pp", "ff", "nf"):
             assert sa[k].tobytes() == sb[k].tobytes(), k
+
+
+@pytest.mark.parametrize("axis", ["x", "y"])
+def test_wave_source_bitwise(gpu_lib, pkg, orc, axis):
+    """A wave source line (MODEL WAVE-SRC ... FUNC MATRIX: k_srcuv for
+    VF_CWMSRC, the source terms of VF_VGENE, VF_VPCOEF, VF_BSUWN and
+    VF_FGENE) along x and along y: bit for bit with the oracle, through the
+    fade-in and beyond."""
+    c = pkg.cases.source_flume(nx=64, nz=32, axis=axis, ramp=0.2)
+    t, o = run_pair(pkg, orc, c, 60, check_every=10)
+    st = t.get_state()
+    assert np.abs(st["ww"]).max() > 1e-3  # the source moves the water
