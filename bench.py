@@ -25,7 +25,9 @@ vf_step_gpu_ with the state in pinned host arrays copied in and out every
 step.
 
 --case flume: the plain FP64 wave flume with a porous breakwater, 512 x 32
-x 96 cells, tolerance 1e-10 (the reference's configuration of that run).
+x 96 cells, tolerance 1e-10, driven by the first-order stream-function
+wave maker (WAVE-BC X- FUNC STREAM 1), the reference's configuration of
+that run.
 """
 from __future__ import annotations
 
@@ -96,8 +98,10 @@ def build_case(args):
     if getattr(args, "case", "flume") == "beach":
         return P.cases.solitary_beach(nx=args.beach_nx, ny=args.beach_ny, nz=args.beach_nz)
     c = P.cases.porous_flume(nx=args.nx, ny=args.ny, nz=args.nz)
-    P.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
-    P.cases.wave_maker(c, 0.08, 1.5, 0.5)
+    # WAVE-BC X- FUNC STREAM 1: the first-order stream-function wave, and
+    # the train it would have made as the initial state
+    P.cases.wave_maker(c, 0.08, 1.5, 0.5, stream=1)
+    P.cases.linear_wave_initial(c, 0.08, 1.5, 0.5, phase0=c.wave["stream"].phase0)
     return c
 
 
@@ -251,7 +255,8 @@ def workload_config(case, args):
         solver += (f", learned initial guess (U-Net trained on the first {args.train_steps} steps' solves, "
                    f"timed after them),")
     return {"workload": f"porous wave flume {case.ni-2}x{case.nj-2}x{case.nk-2} {solver} SMAC step "
-                        f"(wave maker H=0.08 T=1.5 at x=0 on a developed first-order wave train, "
+                        f"(stream-function wave maker FUNC STREAM 1, H=0.08 T=1.5, at x=0 on a developed "
+                        f"first-order wave train, "
                         f"dt={case.dt}, tol 1e-10, block-Jacobi MILU "
                         f"{args.ti}x{args.tj} columns)",
             "cells": case.interior_cells, "precond_block": [args.ti, args.tj],

@@ -51,6 +51,8 @@ extern "C" {
 #define CADMAS_EIO          13  /* restart file: cannot open, read or write, or
                                    a mismatch ('INVALID NUMBER OF GRID.' etc.,
                                    vf_ir1inp.f); cadmas_strerror has the text */
+#define CADMAS_EWAVE        14  /* the wave theory did not converge:
+                                   '(VF_SFMB02C) NOT CONVERGED.' vf_cwmak0.f:54 */
 
 /* ---- sizes (/VF_ANUMBI/, VF_ANUMBI.h) ----------------------------------- */
 typedef struct cadmas_dims {
@@ -236,6 +238,45 @@ typedef struct cadmas_wave_table {
   const double *un;      /* DMTBUN(MTBZZ,MTBTT) velocity normal to the side  */
   const double *ut;      /* DMTBUT(MTBZZ,MTBTT) vertical velocity            */
 } cadmas_wave_table;
+
+/* ---- wave-maker boundary, wave-theory form (WAVE-BC ... FUNC STREAM N) --
+   A steady periodic wave of order N (1..22) by the stream-function
+   (Fourier) method with no mean mass transport, the reference's default
+   wave theory (vf_cwmak0.f:43-56).  In the frame moving with the wave,
+     psi = -ubar (z+d) + sum_j b[j-1] sinh(j k (z+d)) / cosh(j k d) cos(j k X),
+   z from the still water level.  cadmas_stream_solve computes it on the
+   host (the reference's vf_wsfmb2.f is third-party code; this is
+   Fenton's collocation form of the same method), cadmas_set_wave_theory
+   drives a side with it: each step the level at the side's phase and the
+   face velocities at the heights scaled to the column's water level, as
+   VF_BWUWN does with VF_CWMAK1/VF_CWMAK2 (vf_bwuwn.f:259-470), rounded to
+   single precision like the reference's REAL*4 wave routines.          */
+#define CADMAS_STREAM_NMAX 22
+typedef struct cadmas_stream_wave {
+  int order;             /* N                                                 */
+  int iterations;        /* Newton iterations over all height steps           */
+  double depth, period, height, grav;  /* d, T, H, g of the solution         */
+  double k;              /* wave number 2 pi / L                              */
+  double length;         /* wave length L                                      */
+  double celerity;       /* c = L / T                                          */
+  double ubar;           /* mean speed of the water past the wave, moving frame */
+  double q;              /* volume flux past the wave, moving frame (= c d)    */
+  double r;              /* Bernoulli constant                                 */
+  double phase0;         /* the phase at TNOW = 0 (BCTYP(6,JD)): where the
+                            level crosses zero between the crest (phase 1)
+                            and the trough (phase 0.5), found in single
+                            precision as VF_CWZERO does (vf_cwzero.f)       */
+  double b[CADMAS_STREAM_NMAX];  /* B_1 .. B_N                                 */
+} cadmas_stream_wave;
+/* Solve for the wave (host only).  CADMAS_EINVAL beyond the reference's
+   steepness limits (H/L0 > 0.3 or H/d > 1.5, vf_wsfmb2.f:64-65),
+   CADMAS_EWAVE when Newton's method does not converge.                  */
+int cadmas_stream_solve(int order, double depth, double period, double height, double grav,
+                        cadmas_stream_wave *out);
+/* The surface eta at `phase` (theta = 2 pi phase; a crest at 0) and the
+   velocities u (direction of travel) and w at height z above the still
+   water level, as the wave maker uses them (host only; NULL skips).    */
+int cadmas_stream_eval(const cadmas_stream_wave *s, double phase, double z, double *eta, double *u, double *w);
 
 typedef struct cadmas_wave_bc {
   int side;              /* JD: 1 X-, 2 X+, 3 Y-, 4 Y+                      */
@@ -540,6 +581,12 @@ int cadmas_divnorm_noalloc(const cadmas_dims *d, const double *xx, const double 
    end normally and the handle stays usable.  A negative from_step turns
    the injection off.                                                    */
 int cadmas_test_stall_sweeps(cadmas_handle *h, int from_step);
+
+/* Side w->side as a wave maker driven by the wave `s` (WAVE-BC ... FUNC
+   STREAM N): depth, period and fade-in from `w`; replaces
+   VF_CWMAK0/1/2 calls of VF_BWUWN (vf_bwuwn.f:259-470) for that side.
+   Oblique incidence is not built.                                        */
+int cadmas_set_wave_theory(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *s);
 
 /* The wave source of the handle (one line, as the reference allows),
    with the matrix table `t` (NULL: the table already given to

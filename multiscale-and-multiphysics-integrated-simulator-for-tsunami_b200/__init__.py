@@ -26,7 +26,7 @@ HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = HERE / "libcadmas_gpu.so"
 
 (OK, EINVAL, ECUDA, ENOTCONV, EDIVERGE, EPIVOT, EPG, ECAP, ENOMEM, EUNSUPPORTED, ENOSTATIC, ETIMEOUT, ESCRATCH,
- EIO) = range(14)
+ EIO, EWAVE) = range(15)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -44,6 +44,35 @@ class WaveTable(C.Structure):
 class WaveBC(C.Structure):
     _fields_ = [("side", C.c_int), ("first", C.c_int), ("last", C.c_int), ("pad", C.c_int),
                 ("depth", C.c_double), ("period", C.c_double), ("ramp", C.c_double)]
+
+
+STREAM_NMAX = 22
+
+
+class StreamWave(C.Structure):
+    _fields_ = [("order", C.c_int), ("iterations", C.c_int)] + [
+        (n, C.c_double) for n in ("depth", "period", "height", "grav", "k", "length", "celerity", "ubar", "q",
+                                  "r", "phase0")] + [("b", C.c_double * STREAM_NMAX)]
+
+
+def stream_solve(order, depth, period, height, grav=9.8, lib=None) -> StreamWave:
+    """The stream-function wave of order N (cadmas_stream_solve, host only)."""
+    lib = lib or load_library()
+    out = StreamWave()
+    lib.cadmas_stream_solve.argtypes = [C.c_int] + [C.c_double] * 4 + [C.POINTER(StreamWave)]
+    _check(lib, lib.cadmas_stream_solve(int(order), float(depth), float(period), float(height), float(grav),
+                                        C.byref(out)))
+    return out
+
+
+def stream_eval(sw: StreamWave, phase, z=0.0, lib=None):
+    """(eta, u, w) of a stream-function wave at `phase` and height z above
+    the still water level, as the wave maker uses them (cadmas_stream_eval)."""
+    lib = lib or load_library()
+    e, u, w = C.c_double(), C.c_double(), C.c_double()
+    lib.cadmas_stream_eval.argtypes = [C.POINTER(StreamWave), C.c_double, C.c_double, _dp, _dp, _dp]
+    _check(lib, lib.cadmas_stream_eval(C.byref(sw), float(phase), float(z), C.byref(e), C.byref(u), C.byref(w)))
+    return e.value, u.value, w.value
 
 
 class WaveSrc(C.Structure):
@@ -126,7 +155,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step",
             "cadmas_set_warm_net", "cadmas_warm_stats", "cadmas_get_solve", "cadmas_get_system",
             "cadmas_unet_train_sys", "cadmas_unet_time_forward", "cadmas_test_stall_sweeps",
-            "cadmas_set_wave_source"]
+            "cadmas_set_wave_source", "cadmas_stream_solve", "cadmas_stream_eval", "cadmas_set_wave_theory"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
@@ -441,7 +470,16 @@ class Tank:
         _check(self.lib, self.lib.cadmas_set_open(self.h, C.byref(o)))
 
     def set_wave(self, wave):
-        """Wave-maker side from a dict made by cases.wave_maker (cadmas_set_wave)."""
+        """Wave-maker side from a dict made by cases.wave_maker
+        (cadmas_set_wave with a table, cadmas_set_wave_theory with a
+        stream-function wave)."""
+        if wave.get("stream") is not None:
+            bc = WaveBC(int(wave["side"]), int(wave["first"]), int(wave["last"]), 0, float(wave["depth"]),
+                        float(wave["period"]), float(wave.get("ramp", 0.0)))
+            sw = wave["stream"]
+            self.lib.cadmas_set_wave_theory.argtypes = [C.c_void_p, C.POINTER(WaveBC), C.POINTER(StreamWave)]
+            _check(self.lib, self.lib.cadmas_set_wave_theory(self.h, C.byref(bc), C.byref(sw)))
+            return
         bc, tab, keep = wave_structs(wave)
         _check(self.lib, self.lib.cadmas_set_wave(self.h, C.byref(bc), C.byref(tab)))
 

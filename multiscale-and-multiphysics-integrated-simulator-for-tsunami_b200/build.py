@@ -13,7 +13,7 @@ import subprocess
 HERE = pathlib.Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libcadmas_gpu.so"
-SOURCES = ["api.cu", "k_momentum.cu", "k_poisson.cu", "k_vof.cu", "k_bc.cu", "k_drop.cu", "k_slope.cu", "k_keps.cu", "k_unet.cu", "unet.cu", "warmstart.cu", "noalloc.cu"]
+SOURCES = ["api.cu", "k_momentum.cu", "k_poisson.cu", "k_vof.cu", "k_bc.cu", "k_drop.cu", "k_slope.cu", "k_keps.cu", "k_unet.cu", "unet.cu", "warmstart.cu", "noalloc.cu", "wavetheory.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

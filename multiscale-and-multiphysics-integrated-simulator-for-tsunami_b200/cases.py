@@ -630,12 +630,13 @@ def droplet_tank(seed=0, nx=24, ny=6, nz=20, d=0.01, ndrop=8, level=0.3, dt=2.0e
     return c
 
 
-def linear_wave_initial(c: Case, H: float, T: float, depth: float, g0: float = 9.8):
+def linear_wave_initial(c: Case, H: float, T: float, depth: float, g0: float = 9.8, phase0: float = 0.0):
     """Fill the tank with a first-order (Airy) progressive wave train,
-    eta = H/2 cos(kx), u = H/2 w cosh(kz)/sinh(kh) cos(kx),
-    w = H/2 w sinh(kz)/sinh(kh) sin(kx) (z from the bed), with
-    w^2 = g k tanh(k h).  Used as the initial state of the flume workload
-    in place of a wave maker at the inflow boundary."""
+    eta = H/2 cos(kx + 2 pi phase0), u = H/2 w cosh(kz)/sinh(kh) cos(kx + 2 pi phase0),
+    w = H/2 w sinh(kz)/sinh(kh) sin(kx + 2 pi phase0) (z from the bed), with
+    w^2 = g k tanh(k h): the train a wave maker at x = 0 whose phase at
+    TNOW = 0 is phase0 would have made (phase 0: a crest at x = 0)."""
+    ph = 2.0 * np.pi * phase0
     om = 2.0 * np.pi / T
     k = om * om / g0
     for _ in range(60):  # Newton on f(k) = g k tanh(kh) - w^2
@@ -646,7 +647,7 @@ def linear_wave_initial(c: Case, H: float, T: float, depth: float, g0: float = 9
     a = 0.5 * H
     x1, z1 = c.xx[0], c.zz[0]
     xc = 0.5 * (x1[1:-1] + x1[2:])                    # cell centres I = 2..NI-1
-    level = depth + a * np.cos(k * xc)
+    level = depth + a * np.cos(k * xc + ph)
     for i in range(1, c.ni - 1):
         lv = level[i - 1]
         for kk in range(1, c.nk - 1):
@@ -661,12 +662,12 @@ def linear_wave_initial(c: Case, H: float, T: float, depth: float, g0: float = 9
     sk = np.sinh(k * depth)
     wet = c.ff > 0.0
     for i0 in range(2, c.ni - 1):                     # x faces between interior cells
-        prof = a * om * np.cosh(k * zc) / sk * np.cos(k * x1[i0])
+        prof = a * om * np.cosh(k * zc) / sk * np.cos(k * x1[i0] + ph)
         m = (c.nf[i0 - 1, 1:-1, 1:-1] != -1) & (c.nf[i0, 1:-1, 1:-1] != -1) & \
             (wet[i0 - 1, 1:-1, 1:-1] | wet[i0, 1:-1, 1:-1])
         c.uu[i0, 1:-1, 1:-1] = np.where(m, prof[None, :], 0.0)
     for kk in range(2, c.nk - 1):                     # z faces between interior cells
-        prof = a * om * np.sinh(k * z1[kk]) / sk * np.sin(k * xc)
+        prof = a * om * np.sinh(k * z1[kk]) / sk * np.sin(k * xc + ph)
         m = (c.nf[1:-1, 1:-1, kk - 1] != -1) & (c.nf[1:-1, 1:-1, kk] != -1) & \
             (wet[1:-1, 1:-1, kk - 1] | wet[1:-1, 1:-1, kk])
         c.ww[1:-1, 1:-1, kk] = np.where(m, prof[:, None], 0.0)
@@ -709,11 +710,13 @@ def first_order_wave_table(H: float, T: float, depth: float, g0: float = 9.8, nt
 
 
 def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: float = 0.0,
-               table: dict | None = None) -> Case:
+               table: dict | None = None, stream: int = 0) -> Case:
     """Make side `side` (1 X-, 2 X+, 3 Y-, 4 Y+) a wave-maker boundary:
     its domain-boundary faces get B.C. type 5 for velocity and F
-    (WAVE-BC, INDB(3,L) = INDB(4,L) = 5) over the whole side, driven by a
-    first-order wave table unless `table` is given."""
+    (WAVE-BC, INDB(3,L) = INDB(4,L) = 5) over the whole side, driven by
+    the stream-function wave of order `stream` (WAVE-BC ... FUNC STREAM N)
+    when stream >= 1, else by a first-order wave table unless `table` is
+    given."""
     ns = {1: 1, 2: 2, 3: 3, 4: 4}[side]
     for L in range(c.indb.shape[1]):
         ijk, NS = int(c.indb[0, L]), int(c.indb[1, L])
@@ -726,6 +729,11 @@ def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: f
             c.indb[2, L] = VP_WAVE
             c.indb[3, L] = F_WAVE
     first, last = 2, (c.nj - 1 if side <= 2 else c.ni - 1)
+    if stream >= 1:
+        from . import stream_solve
+        c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp, table=None,
+                      stream=stream_solve(stream, depth, T, H, c.params.get("grz0", 9.8)))
+        return c
     c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp,
                   table=table if table is not None else first_order_wave_table(H, T, depth))
     return c

@@ -179,6 +179,8 @@ struct cadmas_handle {
     bool on = false;
     int first = 0, last = 0;
     double d = 0.0, t = 0.0, a = 0.0;
+    bool theory = false;     // FUNC STREAM N: the wave `sw`, not the table
+    cadmas_stream_wave sw{};
   } wave[4];
   // open (radiation) boundary: sides JD = 1..4 and their phase speed C
   struct OpenSide {
@@ -232,7 +234,7 @@ static void refresh_prm(cadmas_handle *h) {
   p.icgtyp = P.icgtyp; p.icgmax = P.icgmax; p.ibsuw0 = P.ibsuw0;
   p.akk0 = P.akk0; p.aka0 = P.aka0; p.anu0 = P.anu0;
   p.loglaw = h->n_log_faces > 0 ? 1 : 0;
-  for (int d = 0; d < 4; ++d) p.fixlvl[d] = (h->wave[d].on && h->mtbtyp == 3) ? 1 : 0;
+  for (int d = 0; d < 4; ++d) p.fixlvl[d] = (h->wave[d].on && !h->wave[d].theory && h->mtbtyp == 3) ? 1 : 0;
   p.iws = (h->src.on && h->src.line > 0) ? h->src.line : 0;
   p.jws = (h->src.on && h->src.line < 0) ? -h->src.line : 0;
   // sponge parameters of vf_veuler.f:77-113
@@ -291,7 +293,7 @@ static int wave_bc(cadmas_handle *h) {
   for (int jd = 0; jd < 4; ++jd) {
     const cadmas_handle::WaveSide &ws = h->wave[jd];
     if (!ws.on) continue;
-    const double T = ws.t, T0 = h->dmtbt0;
+    const double T = ws.t, T0 = ws.theory ? ws.sw.phase0 : h->dmtbt0;
     float R4TN = (float)(T0 - h->tnow / T);
     R4TN = R4TN - (float)(int)R4TN;
     if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
@@ -302,16 +304,24 @@ static int wave_bc(cadmas_handle *h) {
     }
     const double WVT = (double)R4TN;
     WaveDev w;
-    if (!cwmtb1(h, WVT, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
+    w.theory = ws.theory ? 1 : 0;
+    if (ws.theory) {  // VF_CWMAK1: the level at the phase; VF_CWMAK2 per face on the device
+      w.wvz = stream_eta(ws.sw, WVT);
+      stream_phase(ws.sw, WVT, w.ph);
+      w.wt1 = w.wt2 = 0.0;
+    } else {
+      if (!cwmtb1(h, WVT, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
+      w.ph.n = 0;
+    }
     h->wave_level[jd] = w.wvz * AW;
     w.side = jd + 1; w.first = ws.first; w.last = ws.last;
-    w.mtbtyp = h->mtbtyp; w.nzz = h->nzz; w.mtbnow = h->mtbnow;
+    w.mtbtyp = ws.theory ? 1 : h->mtbtyp; w.nzz = h->nzz; w.mtbnow = h->mtbnow;
     w.d = ws.d; w.aw = AW; w.wvlvl = h->P.wvlvl;
     w.sa = (jd == 0) ? 1.0 : (jd == 1 ? -1.0 : 0.0);  // normal incidence (vf_bwuwn.f:298-310)
     w.sb = (jd == 2) ? 1.0 : (jd == 3 ? -1.0 : 0.0);
     w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
     // a fixed-water-level table sets no velocities (vf_bwuwn.f:330-331)
-    if (h->mtbtyp != 3) launch_wave(h->s, h->g, h->f, w, h->dint);
+    if (ws.theory || h->mtbtyp != 3) launch_wave(h->s, h->g, h->f, w, h->dint);
   }
   return CADMAS_OK;
 }
@@ -352,7 +362,7 @@ static int fixed_level_f(cadmas_handle *h) {
   const double PI = 3.141592653589794, ZERO = 1.0e-20;
   for (int jd = 0; jd < 4; ++jd) {
     const cadmas_handle::WaveSide &ws = h->wave[jd];
-    if (!ws.on) continue;
+    if (!ws.on || ws.theory) continue;
     const double T = ws.t, T0 = h->dmtbt0;
     float R4TN = (float)(T0 - h->tnow / T);
     R4TN = R4TN - (float)(int)R4TN;
@@ -960,6 +970,7 @@ const char *cadmas_strerror(int status) {
     case CADMAS_ETIMEOUT: return "a device-side wait ran out of time";
     case CADMAS_ESCRATCH: return "grid has more than CADMAS_NOALLOC_MAX_ROWS (65536) rows NUMJ*NUMK";
     case CADMAS_EIO: return g_last_error.empty() ? "restart file I/O error" : g_last_error.c_str();
+    case CADMAS_EWAVE: return "(VF_SFMB02C) NOT CONVERGED. (the stream-function wave has no solution found)";
     default: return "unknown status";
   }
 }
@@ -1178,6 +1189,23 @@ int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave
   cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
   ws.on = true; ws.first = w->first; ws.last = w->last;
   ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
+  return CADMAS_OK;
+}
+
+int cadmas_set_wave_theory(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *sw) {
+  if (!h || !w || !sw) return CADMAS_EINVAL;
+  if (w->side < 1 || w->side > 4 || sw->order < 1 || sw->order > CADMAS_STREAM_NMAX) return CADMAS_EINVAL;
+  if (!(w->period > 0.0) || !(w->depth > 0.0) || !(sw->k > 0.0)) return CADMAS_EINVAL;
+  if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
+    g_last_error = "side already declared open";
+    return CADMAS_EINVAL;
+  }
+  const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;
+  if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
+  cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
+  ws.on = true; ws.first = w->first; ws.last = w->last;
+  ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
+  ws.theory = true; ws.sw = *sw;
   return CADMAS_OK;
 }
 

@@ -737,6 +737,16 @@ __global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
     if (L < 1) continue;
     double ZC = (gz(g, 1, K) + gz(g, 1, K + 1)) * 0.5 - w.wvlvl;
     ZC = VWS * (ZC + w.d) - w.d;
+    if (w.theory) {  // VF_CWMAK2 of the stream-function wave (wavetheory.cuh)
+      double UN, UT;
+      wt_velocity(w.ph, ZC, UN, UT);
+      f.bcu[L - 1] = UN * VWS * w.aw * w.sa;
+      f.bcv[L - 1] = UN * VWS * w.aw * w.sb;
+      f.bcw[L - 1] = UT * VWS * w.aw;
+      if (xs) f.uu[c] = f.bcu[L - 1];
+      else f.vv[c] = f.bcv[L - 1];
+      continue;
+    }
     double W1, W2;
     if (ZC <= w.zz[0]) {
       KM = 1; W1 = 1.0; W2 = 0.0;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <atomic>
 #include "cadmas_dev.cuh"
+#include "wavetheory.cuh"
 
 namespace cadmas {
 
@@ -186,7 +187,14 @@ struct WaveDev {
   int mtbtyp, nzz, mtbnow;  // table type, MTBZZ, row MTBNOW (1-based)
   double d, wvz, wt1, wt2, aw, sa, sb, wvlvl;
   const double *zz, *un, *ut;  // device copies of DMTBZZ, DMTBUN, DMTBUT
+  int theory;                  // 1: the stream-function wave of `ph` instead of the table
+  WavePhase ph;
 };
+
+// wavetheory.cu: the series coefficients of a stream-function wave at a
+// phase, and its surface there (single precision, as the reference's)
+void stream_phase(const cadmas_stream_wave &s, double wvt, WavePhase &ph);
+double stream_eta(const cadmas_stream_wave &s, double wvt);
 
 // k_drop.cu: VF_FDROPF (all its passes) and the start values of its arrays
 void launch_fdropf(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const DropArrays &d);

@@ -402,11 +402,16 @@ struct orc_handle {
   double TNOW = 0, DTNOW = 0;
   // wave maker, matrix table (WAVE-BC ... FUNC MATRIX): IBCTYP/BCTYP of
   // the four sides and the table of /VF_AFILEI/ (vf_iimdl.f:49-106)
-  struct Wave { int on = 0, l1 = 0, l2 = 0; double d = 0, t = 0, a = 0; } WV[4];
+  struct Wave {
+    int on = 0, l1 = 0, l2 = 0;
+    double d = 0, t = 0, a = 0;
+    int theory = 0;             // FUNC STREAM N: the wave `sw`, not the table
+    cadmas_stream_wave sw{};
+  } WV[4];
   struct Open { int on = 0; double c = 0; } OP[4];  // IBCTYP(1,JD) = 2 and BCTYP(6,JD)
   long long NLOG = 0;  // faces of type 6 or 8 (log-law, rough walls)
   // IBCTYP(2,JD) = -3 with MTBTYP 3: side JD fixes the water level
-  bool FIXLVL(int JD) const { return JD >= 1 && JD <= 4 && WV[JD - 1].on && MTBTYP == 3; }
+  bool FIXLVL(int JD) const { return JD >= 1 && JD <= 4 && WV[JD - 1].on && !WV[JD - 1].theory && MTBTYP == 3; }
   // a type 5 face on the domain boundary of the side its NS names
   bool fixlvl_face(int NS, int I, int J) const {
     if (NS < 1 || NS > 4 || !FIXLVL(NS)) return false;
@@ -1365,7 +1370,7 @@ struct orc_handle {
     const double PI = 3.141592653589794, ZERO = 1.0e-20;
     for (int JD = 1; JD <= 4; ++JD) {
       const Wave &w = WV[JD - 1];
-      if (!w.on) continue;
+      if (!w.on || w.theory) continue;
       const double T = w.t, T0 = DMTBT0;
       double A = w.a;
       float R4TN = (float)(T0 - TNOW / T);
@@ -1393,14 +1398,75 @@ struct orc_handle {
     return CADMAS_OK;
   }
 
-  // VF_BWUWN wave-maker part  vf_bwuwn.f:259-470, matrix-table inflow
-  // (IBCTYP(2,JD) = -3, MTBTYP 1 or 2; normal incidence, one rank).
+  // ---- the stream-function wave (FUNC STREAM N) at a phase: VF_CWMAK1's
+  // level and VF_CWMAK2's velocities, evaluated from the coefficients of
+  // the wave (the series of psi = -UB (z+d) + sum B_j sinh(jk(z+d)) /
+  // cosh(jkd) cos(jkX), the moving frame; fixed-frame velocities c - UB +
+  // ...).  exp by the reduction x = n ln2 + r and r's Taylor series to
+  // r^14, 2^n applied by ldexp; cosh, sinh from it; the level by Newton's
+  // method on psi = -Q from 0; results rounded to single precision.
+  static double sw_exp(double x) {
+    const double L2H = 0.6931471803691238, L2T = 1.9082149292705877e-10, IL2 = 1.4426950408889634;
+    const double n = std::floor(x * IL2 + 0.5);
+    const double r = (x - n * L2H) - n * L2T;
+    const double inv_fact[15] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0, 1.0 / 5040.0,
+                                 1.0 / 40320.0, 1.0 / 362880.0, 1.0 / 3628800.0, 1.0 / 39916800.0,
+                                 1.0 / 479001600.0, 1.0 / 6227020800.0, 1.0 / 87178291200.0};
+    double p = inv_fact[14];
+    for (int i = 13; i >= 0; --i) p = p * r + inv_fact[i];
+    return std::ldexp(p, (int)n);
+  }
+  static void sw_chsh(double x, double &ch, double &sh) {
+    const double e = sw_exp(x), ei = 1.0 / e;
+    ch = 0.5 * (e + ei);
+    sh = 0.5 * (e - ei);
+  }
+  static double sw_level(const cadmas_stream_wave &s, double wvt) {
+    const double th = 2.0 * 3.141592653589793 * wvt, d = s.depth, k = s.k;
+    double e = 0.0;
+    for (int it = 0; it < 60; ++it) {
+      double f = -s.ubar * (e + d) + s.q, df = -s.ubar;
+      for (int j = 1; j <= s.order; ++j) {
+        double chd, shd, ch, sh;
+        sw_chsh((double)j * k * d, chd, shd);
+        sw_chsh((double)j * k * (e + d), ch, sh);
+        const double cs = std::cos((double)j * th);
+        f = f + s.b[j - 1] * sh / chd * cs;
+        df = df + (double)j * k * s.b[j - 1] * ch / chd * cs;
+      }
+      const double de = f / df;
+      e = e - de;
+      if (std::fabs(de) < 1e-14 * d) break;
+    }
+    return (double)(float)e;
+  }
+  static void sw_velocity(const cadmas_stream_wave &s, double wvt, double z, double &u, double &w) {
+    const double th = 2.0 * 3.141592653589793 * wvt;
+    double zd = z + s.depth;
+    if (zd < 0.0) zd = 0.0;
+    double su = s.celerity - s.ubar, sv = 0.0;
+    for (int j = 1; j <= s.order; ++j) {
+      double chd, shd, ch, sh;
+      sw_chsh((double)j * s.k * s.depth, chd, shd);
+      const double a = (double)j * s.k * s.b[j - 1] / chd;
+      const double cj = a * std::cos((double)j * th), sj = a * std::sin((double)j * th);
+      sw_chsh((double)j * s.k * zd, ch, sh);
+      su = su + cj * ch;
+      sv = sv + sj * sh;
+    }
+    u = (double)(float)su;
+    w = (double)(float)sv;
+  }
+
+  // VF_BWUWN wave-maker part  vf_bwuwn.f:259-470: the matrix-table inflow
+  // (IBCTYP(2,JD) = -3, MTBTYP 1 or 2) or the stream-function wave
+  // (IBCTYP(2,JD) = N >= 1, VF_CWMAK1/VF_CWMAK2); normal incidence, one rank.
   int bwuwn_wave() {
     const double PI = 3.141592653589794, ZERO = 1.0e-20;
     for (int JD = 1; JD <= 4; ++JD) {
       const Wave &w = WV[JD - 1];
       if (!w.on) continue;
-      const double D = w.d, T = w.t, T0 = DMTBT0;
+      const double D = w.d, T = w.t, T0 = w.theory ? w.sw.phase0 : DMTBT0;
       double A = w.a;
       float R4TN = (float)(T0 - TNOW / T);
       R4TN = R4TN - (float)(int)R4TN;
@@ -1411,14 +1477,16 @@ struct orc_handle {
         if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
       }
       const double WVT = (double)R4TN;
-      double WMT1, WMT2, WVZ;
-      if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
+      double WMT1 = 0.0, WMT2 = 0.0, WVZ;
+      if (w.theory) WVZ = sw_level(w.sw, WVT);
+      else if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
       double SA, SB;
       if (JD == 1) { SA = 1.0; SB = 0.0; }
       else if (JD == 2) { SA = -1.0; SB = 0.0; }
       else if (JD == 3) { SA = 0.0; SB = 1.0; }
       else { SA = 0.0; SB = -1.0; }
-      if (MTBTYP == 3) continue;  // vf_bwuwn.f:330: no velocities from a level table
+      if (!w.theory && MTBTYP == 3) continue;  // vf_bwuwn.f:330: no velocities from a level table
+      const int MT = w.theory ? 1 : MTBTYP;
       const bool xs = (JD == 1 || JD == 2);
       const int I0 = (JD == 1) ? 2 : NI, IC0 = (JD == 1) ? 2 : NI - 1;
       const int J0 = (JD == 3) ? 2 : NJ, JC0 = (JD == 3) ? 2 : NJ - 1;
@@ -1426,7 +1494,7 @@ struct orc_handle {
         const int I = xs ? I0 : n, J = xs ? n : J0, IC = xs ? IC0 : n, JC = xs ? n : JC0;
         if (xs ? (J < 2 || J > NJ - 1) : (I < 2 || I > NI - 1)) continue;
         double VWS;
-        if (MTBTYP != 1) {
+        if (MT != 1) {
           VWS = 1.0;
         } else {
           double VAL = 0.0;
@@ -1446,7 +1514,8 @@ struct orc_handle {
           double ZC = (Z_(1, K) + Z_(1, K + 1)) * 0.5 - P.wvlvl;
           ZC = VWS * (ZC + D) - D;
           double UN, UT;
-          if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
+          if (w.theory) sw_velocity(w.sw, WVT, ZC, UN, UT);
+          else if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
           BCU[L - 1] = UN * VWS * AW * SA;
           BCV[L - 1] = UN * VWS * AW * SB;
           BCW[L - 1] = UT * VWS * AW;
@@ -3969,6 +4038,16 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
   h->DMTBT0 = t->phase0;
   orc_handle::Wave &v = h->WV[w->side - 1];
   v.on = 1; v.l1 = w->first; v.l2 = w->last; v.d = w->depth; v.t = w->period; v.a = w->ramp;
+  return CADMAS_OK;
+}
+
+int orc_set_wave_theory(orc_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *sw) {
+  if (!h || !w || !sw || w->side < 1 || w->side > 4 || sw->order < 1 || sw->order > CADMAS_STREAM_NMAX)
+    return CADMAS_EINVAL;
+  if (h->OP[w->side - 1].on) return CADMAS_EINVAL;
+  orc_handle::Wave &v = h->WV[w->side - 1];
+  v.on = 1; v.l1 = w->first; v.l2 = w->last; v.d = w->depth; v.t = w->period; v.a = w->ramp;
+  v.theory = 1; v.sw = *sw;
   return CADMAS_OK;
 }
 

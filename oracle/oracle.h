@@ -55,6 +55,7 @@ int orc_get_poisson(orc_handle *h, int which, double *out);
 /* Wave-maker side with its matrix table (as cadmas_set_wave). */
 int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t);
 int orc_set_wave_source(orc_handle *h, const cadmas_wave_src *s, const cadmas_wave_table *t);
+int orc_set_wave_theory(orc_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *sw);
 /* Open (radiation) side JD with the phase speed of depth and period (as
    cadmas_set_open); orc_open_speed is VF_COMAK0's C = L/T. */
 int orc_set_open(orc_handle *h, int side, double depth, double period);

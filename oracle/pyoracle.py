@@ -106,7 +106,13 @@ class Oracle:
             raise RuntimeError("orc_create failed")
         self._static = P.static_of(case)
         self._rc(self.lib.orc_upload_static(self.h, C.byref(self._static)))
-        if getattr(case, "wave", None):
+        if getattr(case, "wave", None) and case.wave.get("stream") is not None:
+            wv = case.wave
+            bc = P.WaveBC(int(wv["side"]), int(wv["first"]), int(wv["last"]), 0, float(wv["depth"]),
+                          float(wv["period"]), float(wv.get("ramp", 0.0)))
+            self.lib.orc_set_wave_theory.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.StreamWave)]
+            self._rc(self.lib.orc_set_wave_theory(self.h, C.byref(bc), C.byref(wv["stream"])))
+        elif getattr(case, "wave", None):
             bc, tab, keep = P.wave_structs(case.wave)
             self.lib.orc_set_wave.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.WaveTable)]
             self._rc(self.lib.orc_set_wave(self.h, C.byref(bc), C.byref(tab)))

@@ -15,9 +15,10 @@
         FSUM           relative difference 1e-12,
     about 100 times the differences seen over the 2000 steps (velocity
     1.2e-14, p 7.3e-11, F 3.6e-14, FSUM 2.5e-14 relative).
-* Config 1, the full 512x32x96 porous flume with its wave maker, 20 steps
-  with 16x16 preconditioner blocks: bit for bit against the oracle in the
-  GPU order every 5 steps.
+* Config 1, the full 512x32x96 porous flume with its wave maker (the
+  first-order stream-function wave, FUNC STREAM 1), 20 steps with 16x16
+  preconditioner blocks: bit for bit against the oracle in the GPU order
+  every 5 steps.
 """
 import numpy as np
 import pytest
@@ -71,8 +72,8 @@ def test_dam_break_2000_steps(gpu_lib, pkg, orc):
 
 def test_flume_full_size_20_steps_bitwise(gpu_lib, pkg, orc):
     c = pkg.cases.porous_flume()
-    pkg.cases.linear_wave_initial(c, 0.08, 1.5, 0.5)
-    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5)
+    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5, stream=1)  # WAVE-BC X- FUNC STREAM 1
+    pkg.cases.linear_wave_initial(c, 0.08, 1.5, 0.5, phase0=c.wave["stream"].phase0)
     assert (c.ni - 2, c.nj - 2, c.nk - 2) == (512, 32, 96)
     over = dict(precond_ti=16, precond_tj=16)
     t = pkg.Tank(c, **over)

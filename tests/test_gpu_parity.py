@@ -475,3 +475,15 @@ def test_wave_source_bitwise(gpu_lib, pkg, orc, axis):
     t, o = run_pair(pkg, orc, c, 60, check_every=10)
     st = t.get_state()
     assert np.abs(st["ww"]).max() > 1e-3  # the source moves the water
+
+
+@pytest.mark.parametrize("order", [1, 5])
+def test_stream_function_wave_maker_bitwise(gpu_lib, pkg, orc, order):
+    """The wave maker driven by the stream-function wave (WAVE-BC ... FUNC
+    STREAM N): the level at the phase on the host, the face velocities at
+    the scaled heights in k_wave from the wave's series; bit for bit with
+    the oracle's own evaluation of the same wave."""
+    c = pkg.cases.porous_flume(nx=96, ny=4, nz=64, block=(1.2, 1.4, 0.6), sponge_width=0.4)
+    pkg.cases.wave_maker(c, 0.08, 1.5, 0.5, ramp=0.5, stream=order)
+    t, o = run_pair(pkg, orc, c, 30, check_every=10)
+    assert np.abs(t.get_state()["uu"][1, :, :]).max() > 1e-3  # the wave maker drives the inflow
