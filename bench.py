@@ -681,6 +681,81 @@ def e2e_run(P, tank, case, stream, args, world, dev):
             "path": "vf_step_gpu_ (pinned host state in/out every step)"}
 
 
+def run_learned(args, rank, world, local_rank):
+    """The learned initial guess on held-out grids: the network is trained
+    on the solver's own (BB, PT, system) triples from the first steps of
+    beaches with seeds 0..n_train-1 (the config-2 beach scaled down to a
+    small grid, seeded boxes), then beaches with seeds 50.. are stepped
+    with the zero guess, the previous step's solution and the learned
+    guess; the line reports BiCGSTAB iterations, kept/dropped guesses and
+    the device time per step of each."""
+    import importlib
+    import torch
+    P = _load_pkg()
+    P.build_library()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ws = importlib.import_module(P.__name__ + ".warmstart")
+    nx, ny, nz = (int(v) for v in args.learn_grid.split("x"))
+    sc = 1024 / nx
+
+    def beach(seed):
+        return P.cases.solitary_beach(nx=nx, ny=ny, nz=nz, dx=0.02 * sc, dy=0.02 * 128 / ny,
+                                      dz=0.01 * 128 / nz, seed=seed, nbox=40, dt=1.0e-3 * sc)
+
+    t0 = time.time()
+    samples = []
+    for sd in range(args.learn_train):
+        samples += ws.collect(beach(sd), args.learn_steps, precond_ti=args.ti, precond_tj=args.tj)
+    t_collect = time.time() - t0
+    t0 = time.time()
+    params, cscale = ws.train(samples, epochs=args.train_epochs, batch=4, lr=1.0e-3, w_mse=0.1, w_res=1.0)
+    t_train = time.time() - t0
+    del samples
+    out = {}
+    for guess, ws_mode in (("zero", 0), ("previous", 1), ("learned", 2)):
+        iters, ms, kept, dropped = [], 0.0, 0, 0
+        for sd in range(50, 50 + args.learn_eval):
+            c = beach(sd)
+            t = P.Tank(c, warm_start=ws_mode, precond_ti=args.ti, precond_tj=args.tj)
+            if ws_mode == 2:
+                t.set_warm_net(params, cscale)
+            t.init_state(True)
+            stream = torch.cuda.ExternalStream(t.stream(), device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.learn_steps):
+                t.step(c.dt)
+                iters.append(t.stats()["icgitr"])
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            if ws_mode == 2:
+                k, d = t.warm_stats()
+                kept, dropped = kept + k, dropped + d
+            t.close()
+        nst = args.learn_eval * args.learn_steps
+        out[guess] = {"mean_iters": float(np.mean(iters)), "ms_per_step": ms / nst,
+                      **({"kept": kept, "dropped": dropped, "fallback_rate": dropped / max(1, kept + dropped)}
+                         if ws_mode == 2 else {})}
+    if rank != 0:
+        return
+    z = out["zero"]["mean_iters"]
+    line = {"metric": "BiCGSTAB iterations per solve on held-out beaches (learned initial guess)",
+            "value": out["learned"]["mean_iters"], "unit": "iterations", "n_gpus": 1,
+            "steps": args.learn_steps, "warmup": 0, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network, f64 solver", "data": "synthetic",
+            "config": {"workload": f"solitary beach {nx}x{ny}x{nz} (the 1024x128x128 beach scaled to this grid), "
+                                   f"train seeds 0..{args.learn_train - 1} x {args.learn_steps} steps, "
+                                   f"held-out seeds 50..{49 + args.learn_eval} x {args.learn_steps} steps, "
+                                   f"{args.train_epochs} epochs, tol 1e-8",
+                       "collect_s": round(t_collect, 1), "train_s": round(t_train, 1)},
+            "guesses": out, "gain_vs_zero": 1.0 - out["learned"]["mean_iters"] / z,
+            "gain_previous_vs_zero": 1.0 - out["previous"]["mean_iters"] / z}
+    print(json.dumps(line), flush=True)
+
+
 def measured_peak_bf16():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -815,7 +890,11 @@ def main():
     ap.add_argument("--autotune", action="store_true",
                     help="--case ensemble: preconditioner block shape per member by the tile autotuner")
     ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
-    ap.add_argument("--case", choices=["flume", "beach", "ensemble", "unet"], default="beach",
+    ap.add_argument("--learn-grid", default="128x32x64", help="--case learned: beach grid NXxNYxNZ")
+    ap.add_argument("--learn-train", type=int, default=8, help="--case learned: training seeds")
+    ap.add_argument("--learn-eval", type=int, default=3, help="--case learned: held-out seeds")
+    ap.add_argument("--learn-steps", type=int, default=12, help="--case learned: steps per seed")
+    ap.add_argument("--case", choices=["flume", "beach", "ensemble", "unet", "learned"], default="beach",
                     help="beach: 1024x128x128 solitary wave on a 1:20 beach with 40 porous boxes, plain "
                          "FP64 and mixed solvers (default); flume: 512x32x96 porous wave flume; "
                          "unet: the learned guess's network alone")
@@ -866,6 +945,8 @@ def main():
             run_ensemble(args, rank, world, local_rank)
         elif args.case == "unet":
             run_unet(args, rank, world, local_rank)
+        elif args.case == "learned":
+            run_learned(args, rank, world, local_rank)
         elif args.case == "beach":
             run_headline(args, rank, world, local_rank)
         else:

@@ -857,8 +857,8 @@ def ensemble_flumes(members: int = 64, seed: int = 0, dx: float = 0.02, dz: floa
     rng = np.random.Generator(np.random.Philox(seed))
     out = []
     for m in range(members):
-        nx = int(rng.integers(256, 1025) * scale) // 16 * 16
-        ny = int(rng.integers(16, 65)) // 16 * 16
+        nx = max(16, int(rng.integers(256, 1025) * scale))
+        ny = int(rng.integers(16, 65))
         nz = int(rng.integers(64, 129))
         depth = min(float(rng.uniform(0.4, 0.8)), 0.75 * nz * dz)
         H = min(float(rng.uniform(0.05, 0.2)), 0.3 * depth)

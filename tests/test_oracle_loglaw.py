@@ -26,6 +26,19 @@ def test_ln_is_within_one_ulp_of_libm(orc):
     assert np.isnan(orc.ln(-1.0))
 
 
+def test_ln_ulp_bound_on_the_wall_function_range(orc):
+    """The largest difference from libm's log over the arguments the wall
+    functions take: DL u*/nu (log law) and DL/ks (rough walls) from 1e-2 to
+    1e7.  At most 1 ulp of the result from 10 up (where the log law holds),
+    2 ulps below 10, where |ln x| is small and its ulp finer than the
+    series' absolute error of about 1e-16."""
+    rng = np.random.default_rng(7)
+    for lo, hi, bound in ((1.0, 7.0, 1.0), (-2.0, 1.0, 2.0)):
+        xs = 10.0 ** rng.uniform(lo, hi, 4000)
+        ulps = np.array([abs(orc.ln(x) - np.log(x)) / np.spacing(abs(np.log(x))) for x in xs])
+        assert ulps.max() <= bound, (lo, hi, ulps.max())
+
+
 @pytest.mark.parametrize("dl,va", [(0.005, 0.05), (0.005, 1e-6), (0.01, 2.0), (5e-4, 1e-3), (0.1, 10.0)])
 def test_friction_velocity_satisfies_the_log_law(orc, dl, va):
     vt = orc.cloglw(dl, va)
