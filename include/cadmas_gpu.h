@@ -166,14 +166,7 @@ typedef struct cadmas_params {
      has at least two preconditioner blocks per SM, one otherwise.  The
      results do not depend on it.                                         */
   int    sweep_occupancy;
-  /* k-planes per wavefront step of the MILU sweeps (no counterpart in the
-     reference): 1, or 2 = two cells of each column per step (the solver
-     arrays stored two planes to a slab), which halves the steps and their
-     barriers for blocks of up to 480 columns; 0 = the default.  The
-     per-cell arithmetic and the results of the sweeps do not depend on
-     it; the BiCGSTAB sums group their terms by slab, so with the GPU's
-     summation order the last bits of a solve do.                         */
-  int    sweep_planes;
+  int    pad1;
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */

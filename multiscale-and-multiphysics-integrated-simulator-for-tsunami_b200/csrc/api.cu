@@ -1040,11 +1040,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   const int TJl = TJ / split;
   h->q.split = split;
   h->q.TI = TI; h->q.TJ = TJl; h->q.TIp = (TI + 3) & ~3; h->q.T = h->q.TIp * TJl;
-  // two planes per slab (sweep_planes 2) for blocks of one thread block;
-  // the cluster form keeps one
-  h->q.PL = (p->sweep_planes == 2 && split == 1) ? 2 : 1;
-  h->q.ST = h->q.PL * h->q.T;
-  h->q.W = (d->numk - 2 + h->q.PL - 1) / h->q.PL + (TI - 1) + (TJl - 1);
+  h->q.W = (d->numk - 2) + (TI - 1) + (TJl - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJl - 1) / TJl);
   h->q.occ = (p->sweep_occupancy == 1 || p->sweep_occupancy == 2) ? p->sweep_occupancy : 0;
@@ -1058,7 +1054,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
     g_last_error = "preconditioner block too large for the MILU sweeps; set precond_ti/precond_tj";
     rc = CADMAS_EUNSUPPORTED;
   }
-  h->nsl = (size_t)h->q.nb * h->q.W * h->q.ST;
+  h->nsl = (size_t)h->q.nb * h->q.W * h->q.T;
   h->nslab = (long long)h->q.nb * h->q.W;
   h->nrb = (h->nslab + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK;
   {

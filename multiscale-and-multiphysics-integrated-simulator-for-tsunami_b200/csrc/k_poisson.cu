@@ -209,22 +209,15 @@ inline size_t ring_bytes(int NV, int T, int R, size_t es = sizeof(double)) {
 }
 
 // ----------------------------------------------------- tile-skewed layout
-// The MILU sweeps visit, at wavefront step s, the PL cells (is+ti, js+tj,
-// k = 2 + PL*(s-ti-tj) + p), p = 0..PL-1, with thread t = ti + TIp*tj.
-// The arrays that stay constant through a solve (7 coefficients, DD,
-// INDC), the right-hand side and the BiCGSTAB vectors are stored tile by
-// tile in that visiting order,
-//     sl(b, w, p, t) = (b*W + w)*ST + p*T + t,   w = (k-2)/PL + ti + tj,
-// b = tile index, W = ceil((NK-2)/PL) + (TI-1) + (TJ-1), ST = PL*T, so
-// the ST values a block needs at one step are contiguous and every load of
-// the sweep coalesces.
+// The MILU kernels visit, at wavefront step s, cell (is+ti, js+tj,
+// k = 2+s-ti-tj) with thread t = ti + TIp*tj.  The arrays that stay constant
+// through a solve (7 coefficients, DD, INDC), the right-hand side and the
+// BiCGSTAB vectors are stored tile by tile in that visiting order,
+//     sl(b, w, t) = (b*W + w)*T + t,   w = (k-2) + ti + tj,
+// b = tile index, W = (NK-2) + (TI-1) + (TJ-1), so the T values a block
+// needs at one step are contiguous and every load of the sweep coalesces.
 __device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, int t) {
-  return ((long long)b * q.W + w) * q.ST + t;
-}
-// entry (w, p*T + ti + TIp*tj) of the cell at height k of column (ti, tj)
-__device__ __forceinline__ int skew_w(const SkewGeo &q, int ti, int tj, int k) { return (k - 2) / q.PL + ti + tj; }
-__device__ __forceinline__ int skew_t(const SkewGeo &q, int ti, int tj, int k) {
-  return ((k - 2) % q.PL) * q.T + ti + q.TIp * tj;
+  return ((long long)b * q.W + w) * q.T + t;
 }
 
 // Copy the Poisson system (7 coefficients, interleaved per slab; DD set to
@@ -235,18 +228,16 @@ __device__ __forceinline__ int skew_t(const SkewGeo &q, int ti, int tj, int k) {
 __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
                           double *bsl, double *xsl, int warm) {
   pdl_enter();
-  const long long n = (long long)q.nb * q.W * q.ST;
+  const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const int t = (int)(e % q.ST);
-    const long long bw = e / q.ST;
+    const int t = (int)(e % q.T);
+    const long long bw = e / q.T;
     const int w = (int)(bw % q.W), b = (int)(bw / q.W);
-    const int pl = t / q.T, t0 = t - pl * q.T;
-    const int ti = t0 % q.TIp, tj = t0 / q.TIp;
-    const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj;
-    const int k = 2 + q.PL * (w - ti - tj) + pl;
+    const int ti = t % q.TIp, tj = t / q.TIp;
+    const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
     double v[7] = {0, 0, 0, 0, 0, 0, 0}, bv = 0.0, xv = 0.0;
     int ic = -1;
-    if (ti < q.TI && I <= g.NI - 1 && J <= g.NJ - 1 && w >= ti + tj && k <= g.NK - 1) {
+    if (ti < q.TI && I <= g.NI - 1 && J <= g.NJ - 1 && k >= 2 && k <= g.NK - 1) {
       const long long c = cid(g, I, J, k);
       v[0] = A_.ad[c]; v[1] = A_.ali[c]; v[2] = A_.alj[c]; v[3] = A_.alk[c];
       v[4] = A_.aui[c]; v[5] = A_.auj[c]; v[6] = A_.auk[c];
@@ -256,9 +247,9 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
     }
     constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
 #pragma unroll
-    for (int c = 0; c < 7; ++c) S.sys[sys_at(bw, cs[c], q.ST, t)] = v[c];
-    S.sys[sys_at(bw, SYS_DD, q.ST, t)] = 0.0;
-    S.sys[sys_at(bw, SYS_T, q.ST, t)] = 0.0;
+    for (int c = 0; c < 7; ++c) S.sys[sys_at(bw, cs[c], q.T, t)] = v[c];
+    S.sys[sys_at(bw, SYS_DD, q.T, t)] = 0.0;
+    S.sys[sys_at(bw, SYS_T, q.T, t)] = 0.0;
     S.indc[e] = ic;
     bsl[e] = bv;
     xsl[e] = xv;
@@ -274,7 +265,7 @@ __device__ __forceinline__ long long skew_nb(const Geo &g, const SkewGeo &q, int
   if (tj < 0) { by -= 1; tj += q.TJ; } else if (tj >= q.TJ) { by += 1; tj -= q.TJ; }
   const int I = 2 + bx * q.TI + ti, J = 2 + by * q.TJ + tj;
   if (bx < 0 || by < 0 || I > g.NI - 1 || J > g.NJ - 1 || k < 2 || k > g.NK - 1) return -1;
-  return sl_index(q, bx + q.ntx * by, skew_w(q, ti, tj, k), skew_t(q, ti, tj, k));
+  return sl_index(q, bx + q.ntx * by, (k - 2) + ti + tj, ti + q.TIp * tj);
 }
 __device__ __forceinline__ double skew_at(const Geo &g, const SkewGeo &q, const double *X, int bx, int by,
                                           int ti, int tj, int k) {
@@ -308,21 +299,19 @@ __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
   const bool valid = ti < wi && tj < wj;
   const int r = tj / TJl, tjl = tj % TJl;
   const long long bl = blockIdx.x + (long long)q.ntx * (blockIdx.y * q.split + r);  // layout tile
-  // the cell of step s, k = 2+s-ti-tj, is entry (w, tl) of tile bl with
-  // w = (k-2)/PL + ti + tjl (one k per step here; the sweeps take PL)
-  (void)Tl;
+  // slab of step s: w = (k-2) + ti + tjl = s - r*TJl
+  const long long slab0 = bl * q.W - (long long)r * TJl;
+  const int tl = ti + TIp * tjl;
   const int nsteps = (g.NK - 2) + (wi - 1) + (wj - 1);
   auto prefetch = [&](int s) {
     const int k = 2 + s - ti - tj;
     if (valid && k >= 2 && k <= g.NK - 1) {
-      const long long slab = bl * q.W + skew_w(q, ti, tjl, k);
-      const int tl = skew_t(q, ti, tjl, k);
-      const long long e = slab * q.ST + tl;
-      const V *sy = S.sys + sys_at(slab, 0, q.ST, tl);
+      const long long slab = slab0 + s, e = slab * Tl + tl;
+      const V *sy = S.sys + sys_at(slab, 0, Tl, tl);
       const int sl = s % R;
       constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
 #pragma unroll
-      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)cs[c] * q.ST);
+      for (int c = 0; c < 7; ++c) cp_async_v(&rg.v(sl, c, tid), sy + (long long)cs[c] * Tl);
       cp_async4(&rg.ind(sl, tid), S.indc + e);
     }
     cp_commit();
@@ -359,7 +348,7 @@ __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
                     rg.v(sl, 3, tid) * dk1 * au3);
         if (dd <= z) bad = true;
       }
-      S.sys[sys_at(bl * q.W + skew_w(q, ti, tjl, k), SYS_DD, q.ST, skew_t(q, ti, tjl, k))] = dd;
+      S.sys[sys_at(slab0 + s, SYS_DD, Tl, tl)] = dd;
       rg.xb[cur * T + tid] = dd;
       dk1 = dd;
       au3 = rg.v(sl, 6, tid) + U * (rg.v(sl, 4, tid) + rg.v(sl, 5, tid));
@@ -511,18 +500,9 @@ __device__ __forceinline__ void cluster_barrier() {
 // and their evaluation order are those of the reference loops, so the
 // results do not change.  The step loop is unrolled by the ring length so
 // slot addresses and mbarrier phases are constants.
-//
-// PL = 2 (the layout's two planes per slab, q.PL): every step takes two
-// k of each column, the lower first (the forward sweeps) or the upper
-// first (the backward sweep).  The neighbours' values of both come from
-// step s-1 and the second cell's value at k-1 (k+1) is the first's, so
-// each cell's expression is unchanged; the barrier, the ring wait and the
-// step's copies are paid once per two cells.  The cluster form (CS = 2)
-// keeps one plane.
-template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1, int PL = 1>
+template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st) {
-  static_assert(PL == 1 || CS == 1, "the cluster form has one plane per slab");
   pdl_enter();
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
   // preconditioner block; every block of a cluster runs through the two
@@ -537,22 +517,21 @@ __global__ void __launch_bounds__(MAXT, MINB)
   constexpr int R = D + 2;
   constexpr int AHEAD = (MODE == SWEEP_FWD_AX) ? 2 : 1;  // preparing step s+1 reads the slot of step s+AHEAD
   extern __shared__ __align__(16) double sm[];
-  const int T = q.T, TIp = q.TIp, ST = PL * T;
+  const int T = q.T, TIp = q.TIp;
   const int Tc = (T + 31) & ~31;
   constexpr int ES = (int)sizeof(V);
   const int SS = sweep_slot(q, MODE, ES);
-  // slot offsets of the system arrays and of the vector (MODE 1)
+  // slot offsets of the system arrays
   constexpr int SF = sweep_sys_first(MODE) - sweep_sys_dst(MODE);
-  const int oDD = (SYS_DD - SF) * ST, oAD = (SYS_AD - SF) * ST, oALI = (SYS_ALI - SF) * ST,
-            oALJ = (SYS_ALJ - SF) * ST, oALK = (SYS_ALK - SF) * ST, oAUI = (SYS_AUI - SF) * ST,
-            oAUJ = (SYS_AUJ - SF) * ST, oAUK = (SYS_AUK - SF) * ST, oP = 8 * ST;
-  const int NKP = (g.NK - 2 + PL - 1) / PL;  // steps of a column
+  const int oDD = (SYS_DD - SF) * T, oAD = (SYS_AD - SF) * T, oALI = (SYS_ALI - SF) * T,
+            oALJ = (SYS_ALJ - SF) * T, oALK = (SYS_ALK - SF) * T, oAUI = (SYS_AUI - SF) * T,
+            oAUJ = (SYS_AUJ - SF) * T, oAUK = (SYS_AUK - SF) * T;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm);
   V *ring = reinterpret_cast<V *>(sm + ((R + 1) & ~1));
   V *xb = ring + (size_t)R * SS;
   const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
   TileGeo t = tile_geo(g, q);
-  const int nsteps = NKP + (t.wi - 1) + (t.wj - 1);
+  const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
   const bool producer = tid >= Tc;
   const int lane = tid & 31;
 
@@ -564,7 +543,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
   // which the receiver armed at start-up for one full row (TIp values of x,
   // and of DD for the forward sweeps); a slot is written once per sweep.
   const int NX = q.W;                                   // slots: steps of a tile at most
-  unsigned long long *xfull = reinterpret_cast<unsigned long long *>(xb + 2 * ST);
+  unsigned long long *xfull = reinterpret_cast<unsigned long long *>(xb + 2 * T);
   V *xin = reinterpret_cast<V *>(xfull + NX);
   V *din = xin + (size_t)NX * TIp;
   const int crank = (CS == 2) ? (int)(blockIdx.y & 1) : 0;
@@ -601,7 +580,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
   }
   if (MODE == SWEEP_FWD_AX) {  // halo values of absent neighbours stay 0 (ghost layer)
-    const int nh = 2 * halo_span(q, ES) + 2 * halo_row_span(q);
+    const int nh = 2 * halo_span(q, ES) + 2 * TIp;
     for (int r = 0; r < R; ++r)
       for (int i = tid; i < nh; i += blockDim.x) ring[(size_t)r * SS + halo_left(q, ES) + i] = V(0);
   }
@@ -644,72 +623,59 @@ __global__ void __launch_bounds__(MAXT, MINB)
   // Column geometry: active steps slo..shi (k inside 2..NK-1).
   const int ri = t.wi - 1 - t.ti, rj = t.wj - 1 - t.tj;
   const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
-  const int slo = (MODE == SWEEP_BWD) ? ri + rj : t.ti + t.tj, shi = slo + NKP - 1;
+  const int slo = (MODE == SWEEP_BWD) ? ri + rj : t.ti + t.tj, shi = slo + g.NK - 3;
   const bool col = t.valid && !producer;
   const int hl = halo_left(q, ES) + TIp * t.tj + halo_lofs(q, ES), hr = halo_right(q, ES) + TIp * t.tj,
             hd = halo_down(q, ES) + t.ti, hu = halo_up(q, ES) + t.ti;
   // forward: T into the system block; backward: X
-  V *vp = (MODE == SWEEP_BWD) ? vout + ((long long)b * q.W + nsteps - 1) * ST + tid
-                              : S.sys + sys_at((long long)b * q.W, SYS_T, ST, tid);
-  const long long vstep = (MODE == SWEEP_BWD) ? -(long long)ST : (long long)SYS_N * ST;
+  V *vp = (MODE == SWEEP_BWD) ? vout + ((long long)b * q.W + nsteps - 1) * T + tid
+                              : S.sys + sys_at((long long)b * q.W, SYS_T, T, tid);
+  const long long vstep = (MODE == SWEEP_BWD) ? -(long long)T : (long long)SYS_N * T;
 
-  // Prepared values of the next step, per plane (the cell at k = k0 + p).
-  bool act = false;             // the column has cells at this step
-  V dd[PL], y0[PL], c1[PL], c2[PL], c3[PL];  // DD (0: not computed); FWD: Y or A*P, ALI*DD(i-1),
-                                             // ALJ*DD(j-1), ALK*DD(k-1); BWD: T, AUI, AUJ, AUK
-#pragma unroll
-  for (int pl = 0; pl < PL; ++pl) { dd[pl] = y0[pl] = c1[pl] = c2[pl] = c3[pl] = V(0); }
-  V dk1 = V(0), pk1 = V(0);  // DD and P of this column at k-1 (FWD)
-  V xk1 = V(0);             // result of this column at the cell before (k-1 FWD, k+1 BWD)
+  // Prepared values of the next step.
+  bool act = false;             // the column has a cell at this step
+  V dd = V(0);              // DD of the cell (0: not computed)
+  V y0 = V(0);              // FWD: Y or A*P;  BWD: T
+  V c1 = V(0), c2 = V(0), c3 = V(0);  // FWD: ALI*DD(i-1), ALJ*DD(j-1), ALK*DD(k-1); BWD: AUI, AUJ, AUK
+  V dk1 = V(0), pk1 = V(0);  // DD and P of this column at the previous step (FWD)
+  V xk1 = V(0);             // result of this column at the previous step
   // Prepare step s: cs = slot of s, ps = slot of s-1, ns = slot of s+1.
   auto prepare = [&](int s, const V *cs, const V *ps, const V *ns) {
     act = col && s >= slo && s <= shi;
     if (!act) return;
     if (MODE == SWEEP_FWD_AX) {
-      const int k0 = 2 + PL * (s - slo);
-#pragma unroll
-      for (int pl = 0; pl < PL; ++pl) {
-        const int k = k0 + pl, o = pl * T + tid;
-        const V d = cs[oDD + o], pc = cs[oP + o];
-        if (d != V(0)) {
-          const V pxm = ex0 ? cs[hl + pl * T] : ps[oP + o - 1];
-          const V pym = ey0 ? cs[hd + pl * T] : ps[oP + o - TIp];
-          const V pzm = (k > 2) ? pk1 : V(0);
-          const V pxp = ex1 ? cs[hr + pl * T] : ns[oP + o + 1];
-          const V pyp = ey1 ? cs[hu + pl * T] : ns[oP + o + TIp];
-          const V pzp = (k < g.NK - 1) ? (pl + 1 < PL ? cs[oP + o + T] : ns[oP + tid]) : V(0);
-          y0[pl] = cs[oAD + o] * pc + cs[oALI + o] * pxm + cs[oALJ + o] * pym + cs[oALK + o] * pzm +
-                   cs[oAUI + o] * pxp + cs[oAUJ + o] * pyp + cs[oAUK + o] * pzp;
-          const V d1 = (t.ti > 0) ? ps[oDD + o - 1] : V(0);
-          const V d2 = (t.tj > 0) ? ps[oDD + o - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
-          c1[pl] = cs[oALI + o] * d1;
-          c2[pl] = cs[oALJ + o] * d2;
-          c3[pl] = cs[oALK + o] * dk1;
-        }
-        dd[pl] = d; dk1 = d; pk1 = pc;
+      const int k = 2 + s - t.ti - t.tj;
+      const V d = cs[oDD + tid], pc = cs[8 * T + tid];
+      if (d != V(0)) {
+        const V pxm = ex0 ? cs[hl] : ps[8 * T + tid - 1];
+        const V pym = ey0 ? cs[hd] : ps[8 * T + tid - TIp];
+        const V pzm = (k > 2) ? pk1 : V(0);
+        const V pxp = ex1 ? cs[hr] : ns[8 * T + tid + 1];
+        const V pyp = ey1 ? cs[hu] : ns[8 * T + tid + TIp];
+        const V pzp = (k < g.NK - 1) ? ns[8 * T + tid] : V(0);
+        y0 = cs[oAD + tid] * pc + cs[oALI + tid] * pxm + cs[oALJ + tid] * pym + cs[oALK + tid] * pzm +
+             cs[oAUI + tid] * pxp + cs[oAUJ + tid] * pyp + cs[oAUK + tid] * pzp;
+        const V d1 = (t.ti > 0) ? ps[oDD + tid - 1] : V(0);
+        const V d2 = (t.tj > 0) ? ps[oDD + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
+        c1 = cs[oALI + tid] * d1;
+        c2 = cs[oALJ + tid] * d2;
+        c3 = cs[oALK + tid] * dk1;
       }
+      dd = d; dk1 = d; pk1 = pc;
     } else if (MODE == SWEEP_FWD) {
-#pragma unroll
-      for (int pl = 0; pl < PL; ++pl) {
-        const int o = pl * T + tid;
-        const V d = cs[oDD + o];
-        if (d != V(0)) {
-          const V d1 = (t.ti > 0) ? ps[oDD + o - 1] : V(0);
-          const V d2 = (t.tj > 0) ? ps[oDD + o - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
-          y0[pl] = cs[o];
-          c1[pl] = cs[oALI + o] * d1;
-          c2[pl] = cs[oALJ + o] * d2;
-          c3[pl] = cs[oALK + o] * dk1;
-        }
-        dd[pl] = d; dk1 = d;
+      const V d = cs[oDD + tid];
+      if (d != V(0)) {
+        const V d1 = (t.ti > 0) ? ps[oDD + tid - 1] : V(0);
+        const V d2 = (t.tj > 0) ? ps[oDD + tid - TIp] : (rrow ? din[(size_t)(s + lag) * TIp + t.ti] : V(0));
+        y0 = cs[tid];
+        c1 = cs[oALI + tid] * d1;
+        c2 = cs[oALJ + tid] * d2;
+        c3 = cs[oALK + tid] * dk1;
       }
+      dd = d; dk1 = d;
     } else {
-#pragma unroll
-      for (int pl = 0; pl < PL; ++pl) {
-        const int o = pl * T + tid;
-        dd[pl] = cs[oDD + o];
-        if (dd[pl] != V(0)) { y0[pl] = cs[o]; c1[pl] = cs[oAUI + o]; c2[pl] = cs[oAUJ + o]; c3[pl] = cs[oAUK + o]; }
-      }
+      dd = cs[oDD + tid];
+      if (dd != V(0)) { y0 = cs[tid]; c1 = cs[oAUI + tid]; c2 = cs[oAUJ + tid]; c3 = cs[oAUK + tid]; }
     }
   };
   auto slot_ptr = [&](int r) -> const V * { return ring + (size_t)r * SS; };
@@ -739,37 +705,33 @@ __global__ void __launch_bounds__(MAXT, MINB)
         const int u = s + AHEAD;  // newest data that preparing s+1 reads
         const unsigned ubar = bar0 + 8u * ((r + AHEAD) % R), upar = ph ^ (unsigned)((r + AHEAD) / R);
         const bool ready = !ok || u >= nsteps || mbar_test(ubar, upar);
-        // the recurrence of step s: its planes in sweep order
+        // the recurrence of step s
         V xcur = V(0);
         if (act && ok) {
-          const int cur = (s & 1) * ST, prv = ST - cur;
-#pragma unroll
-          for (int j = 0; j < PL; ++j) {
-            const int pl = (MODE == SWEEP_BWD) ? PL - 1 - j : j, o = pl * T + tid;
-            V x = V(0);
-            if (dd[pl] != V(0)) {
-              const V xr = rrow ? xin[(size_t)(s + lag) * TIp + t.ti] : V(0);  // partner tile's row
-              if (MODE == SWEEP_BWD) {
-                const V x1 = (ri > 0) ? xb[prv + o + 1] : V(0);
-                const V x2 = (rj > 0) ? xb[prv + o + TIp] : xr;
-                x = (y0[pl] - c1[pl] * x1 - c2[pl] * x2 - c3[pl] * xk1) * dd[pl];
-              } else {
-                const V x1 = (t.ti > 0) ? xb[prv + o - 1] : V(0);
-                const V x2 = (t.tj > 0) ? xb[prv + o - TIp] : xr;
-                x = y0[pl] - c1[pl] * x1 - c2[pl] * x2 - c3[pl] * xk1;
-              }
+          const int cur = (s & 1) * T, prv = T - cur;
+          V x = V(0);
+          if (dd != V(0)) {
+            const V xr = rrow ? xin[(size_t)(s + lag) * TIp + t.ti] : V(0);  // partner tile's row
+            if (MODE == SWEEP_BWD) {
+              const V x1 = (ri > 0) ? xb[prv + tid + 1] : V(0);
+              const V x2 = (rj > 0) ? xb[prv + tid + TIp] : xr;
+              x = (y0 - c1 * x1 - c2 * x2 - c3 * xk1) * dd;
+            } else {
+              const V x1 = (t.ti > 0) ? xb[prv + tid - 1] : V(0);
+              const V x2 = (t.tj > 0) ? xb[prv + tid - TIp] : xr;
+              x = y0 - c1 * x1 - c2 * x2 - c3 * xk1;
             }
-            xb[cur + o] = x;
-            vp[pl * T] = x;
-            xk1 = x;
-            xcur = x;
           }
+          xb[cur + tid] = x;
+          *vp = x;
+          xk1 = x;
+          xcur = x;
         }
         vp += vstep;
         if (CS == 2 && srow) {  // this step's boundary-row values to the partner tile
           const unsigned off = (unsigned)(((size_t)s * TIp + t.ti) * ES), fb = r_full + 8u * (unsigned)s;
           st_async(r_xin + off, xcur, fb);
-          if (MODE != SWEEP_BWD) st_async(r_din + off, act ? dd[0] : V(0), fb);
+          if (MODE != SWEEP_BWD) st_async(r_din + off, act ? dd : V(0), fb);
         }
         // prepare step s+1
         if (!ready) {
@@ -812,8 +774,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
   const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
   if (slab_ < (long long)(q).nb * (q).W) {                                          \
     _Pragma("unroll 4")                                                             \
-    for (int t_ = lane_; t_ < (q).ST; t_ += 32) {                                   \
-      const long long e = slab_ * (q).ST + t_;
+    for (int t_ = lane_; t_ < (q).T; t_ += 32) {                                    \
+      const long long e = slab_ * (q).T + t_;
 #define SLAB_LOOP_END \
     }                 \
   }
@@ -846,14 +808,12 @@ __device__ __forceinline__ bool interior(const Geo &g, int I, int J, int K) {
 template <typename V>
 __device__ __forceinline__ V skew_ax(const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *X,
                                      long long e) {
-  const int t = (int)(e % q.ST);
-  const long long bw = e / q.ST;
+  const int t = (int)(e % q.T);
+  const long long bw = e / q.T;
   const int w = (int)(bw % q.W), b = (int)(bw / q.W);
-  const int pl = t / q.T, t0 = t - pl * q.T;
-  const int ti = t0 % q.TIp, tj = t0 / q.TIp, bx = b % q.ntx, by = b / q.ntx;
-  const int k = 2 + q.PL * (w - ti - tj) + pl;
-  const V *a = S.sys + sys_at(bw, 0, q.ST, t);
-  const long long T = q.ST;  // stride between the system arrays
+  const int ti = t % q.TIp, tj = t / q.TIp, bx = b % q.ntx, by = b / q.ntx, k = 2 + w - ti - tj;
+  const V *a = S.sys + sys_at(bw, 0, q.T, t);
+  const long long T = q.T;
   auto at = [&](int di, int dj, int dk) -> V {
     const long long n = skew_nb(g, q, bx, by, ti + di, tj + dj, k + dk);
     return n < 0 ? V(0) : X[n];
@@ -991,7 +951,7 @@ __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V 
   const int lane_ = threadIdx.x & 31;                                               \
   const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
   if (slab_ < (long long)(q).nb * (q).W) {                                          \
-    const int T4_ = (q).ST >> 2;                                                    \
+    const int T4_ = (q).T >> 2;                                                     \
     _Pragma("unroll 2")                                                             \
     for (int t_ = lane_; t_ < T4_; t_ += 32) {                                      \
       const long long e4 = slab_ * T4_ + t_;
@@ -1113,13 +1073,13 @@ __global__ void k_commit(SolveState *st) {
 // T from the FP32 forward sweeps).
 __global__ void k_sys_to_f(SkewGeo q, const double *sys, float *sysf) {
   pdl_enter();
-  const long long n = (long long)q.nb * q.W * q.ST;
+  const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const long long slab = e / q.ST;
-    const int t = (int)(e - slab * q.ST);
+    const long long slab = e / q.T;
+    const int t = (int)(e - slab * q.T);
     constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
 #pragma unroll
-    for (int c = 0; c < 7; ++c) sysf[sys_at(slab, cs[c], q.ST, t)] = (float)sys[sys_at(slab, cs[c], q.ST, t)];
+    for (int c = 0; c < 7; ++c) sysf[sys_at(slab, cs[c], q.T, t)] = (float)sys[sys_at(slab, cs[c], q.T, t)];
   }
 }
 // RF = R * scale on INDC != -1 (the right-hand side of an inner solve)
@@ -1144,11 +1104,9 @@ __global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double
   if (st->iter < 0) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) {
-    const int pl = t_ / q.T, t0 = t_ - pl * q.T;
-    const int ti = t0 % q.TIp, tj = t0 / q.TIp;
+    const int ti = t_ % q.TIp, tj = t_ / q.TIp;
     const int w = (int)(slab_ % q.W), b = (int)(slab_ / q.W);
-    const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj;
-    const int k = 2 + q.PL * (w - ti - tj) + pl;
+    const int I = 2 + (b % q.ntx) * q.TI + ti, J = 2 + (b / q.ntx) * q.TJ + tj, k = 2 + w - ti - tj;
     X0[cid(g, I, J, k)] = XW[e];
   }
   SLAB_LOOP_END
@@ -1330,7 +1288,7 @@ static inline dim3 skew_grid(const SkewGeo &q) { return dim3((unsigned)q.ntx, (u
 
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
                     const SkewSys &S, const double *x0, double *bsl, double *xsl, int warm) {
-  const long long n = (long long)q.nb * q.W * q.ST;
+  const long long n = (long long)q.nb * q.W * q.T;
   const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
   launch_pdl(k_to_skew, dim3(blocks), dim3(256), 0, s, 1, g, q, a, indc, S, x0, bsl, xsl, warm);
 }
@@ -1362,13 +1320,13 @@ void launch_dcmp_f(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, con
 // memory a block may use.
 static size_t sweep_bytes(const SkewGeo &q, int mode, int D, int es) {
   const int R = D + 2;
-  size_t b = (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode, es) * es + 2 * (size_t)q.ST * es;
+  size_t b = (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode, es) * es + 2 * (size_t)q.T * es;
   if (q.split == 2)  // cluster exchange: xfull[W] barriers, xin (and din) [W][TIp]
     b += (size_t)q.W * 8 + (size_t)q.W * q.TIp * es * (mode == SWEEP_BWD ? 1 : 2);
   return b;
 }
 static int sweep_depth(const SkewGeo &q, int mode, int es) {
-  if (sweep_threads(q.T) > (q.split == 2 || q.PL == 2 ? 512 : 1024)) return 0;
+  if (sweep_threads(q.T) > (q.split == 2 ? 512 : 1024)) return 0;
   for (int d : {8, 6, 4, 3, 2}) {
     if (q.split == 2 && (d == 6 || d == 3)) continue;  // depths built for the cluster form
     if (sweep_bytes(q, mode, d, es) <= 227 * 1024) return d;
@@ -1423,36 +1381,6 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   // second tile's wavefront fills it.  The fused FP64 forward sweep keeps
   // one block: its ring of 8 arrays needs the depth and registers.
   const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm && (ES == 4 || MODE == SWEEP_BWD));
-  if (q.PL == 2) {  // two planes per step (blocks of up to 480 columns)
-    if (two) {
-      const int d2 = sweep_depth2(q, MODE, ES);
-      if (d2 > 0) {
-        const size_t bytes2 = sweep_bytes(q, MODE, d2, ES);
-        switch (d2) {
-#define SWEEP_CASE_OCC2P(DD)                                                                               \
-  case DD:                                                                                                 \
-    set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2, 2>, bytes2);                                       \
-    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2, 2>, grid, block, bytes2, s, 1, g, q, S, vin, vout, st); \
-    return;
-          SWEEP_CASE_OCC2P(4) SWEEP_CASE_OCC2P(3) SWEEP_CASE_OCC2P(2)
-#undef SWEEP_CASE_OCC2P
-          default: break;
-        }
-      }
-    }
-    switch (d * 4096 + mt) {
-#define SWEEP_CASEP(DD, MT)                                                                  \
-  case DD * 4096 + MT:                                                                       \
-    set_smem(k_sweep<DD, MODE, MT, V, 1, 1, 2>, bytes);                                      \
-    launch_pdl(k_sweep<DD, MODE, MT, V, 1, 1, 2>, grid, block, bytes, s, 1, g, q, S, vin, vout, st); \
-    break;
-      SWEEP_CASEP(8, 256) SWEEP_CASEP(6, 256) SWEEP_CASEP(4, 256) SWEEP_CASEP(3, 256) SWEEP_CASEP(2, 256)
-      SWEEP_CASEP(8, 512) SWEEP_CASEP(6, 512) SWEEP_CASEP(4, 512) SWEEP_CASEP(3, 512) SWEEP_CASEP(2, 512)
-#undef SWEEP_CASEP
-      default: return;  // rejected by cadmas_create (sweep_supported)
-    }
-    return;
-  }
   if (two) {
     const int d2 = sweep_depth2(q, MODE, ES);
     if (d2 > 0) {
@@ -1605,7 +1533,7 @@ void launch_fin5(cudaStream_t s, const double *rb, long long nrows, SolveState *
 }
 void launch_commit(cudaStream_t s, SolveState *st) { launch_pdl(k_commit, dim3(1), dim3(1), 0, s, 1, st); }
 void launch_sys_to_f(cudaStream_t s, const SkewGeo &q, const double *sys, float *sysf) {
-  const long long n = (long long)q.nb * q.W * q.ST;
+  const long long n = (long long)q.nb * q.W * q.T;
   launch_pdl(k_sys_to_f, dim3((unsigned)std::min<long long>((n + 255) / 256, 148LL * 16)), dim3(256), 0, s, 1, q, sys,
              sysf);
 }

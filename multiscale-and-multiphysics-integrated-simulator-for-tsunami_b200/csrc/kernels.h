@@ -43,10 +43,6 @@ struct SkewGeo {
   int TI, TJ, TIp, T, W;  // layout tile TI x TJ columns (T = TIp*TJ slots), W slabs per tile
   int ntx, nb;            // layout tiles along x, tiles in total
   int split;  // layout tiles per preconditioner block along y (1 or 2)
-  // Planes per slab: PL consecutive k of a column share a slab, plane p
-  // of a slab at p*T, so a slab holds ST = PL*T entries and a sweep step
-  // of PL = 2 visits two k per column (k = 2 + PL*(w - ti - tj) + p).
-  int PL, ST;
   // Thread blocks of the sweeps per SM (k_poisson.cu): 1, 2, or 0 = by
   // the rule of launch_sweep (two for the backward sweeps and the FP32
   // sweeps when there are at least two tiles per SM); nsm = the SMs.
@@ -89,26 +85,21 @@ __host__ __device__ constexpr int sweep_sys_first(int mode) {
 __host__ __device__ constexpr int sweep_sys_dst(int mode) { return mode == SWEEP_FWD ? 1 : 0; }
 // Elements per 16 bytes.
 __host__ __device__ inline int sweep_g(int es) { return 16 / es; }
-// Elements of a left/right halo span: the planes' TIp*(TJ-1) + 16 bytes
-// (plane p's part at p*T).
-__host__ __device__ inline int halo_span(const SkewGeo &q, int es) {
-  return (q.PL - 1) * q.T + q.TIp * (q.TJ - 1) + sweep_g(es);
-}
-// Elements of a down/up halo span: one row of TIp per plane, T apart.
-__host__ __device__ inline int halo_row_span(const SkewGeo &q) { return (q.PL - 1) * q.T + q.TIp; }
+// Elements of a left/right halo span: TIp*(TJ-1) + 16 bytes.
+__host__ __device__ inline int halo_span(const SkewGeo &q, int es) { return q.TIp * (q.TJ - 1) + sweep_g(es); }
 // elements per ring slot (a multiple of 16 bytes, so slots stay aligned)
 __host__ __device__ inline int sweep_slot(const SkewGeo &q, int mode, int es) {
-  return sweep_nv(mode) * q.ST + (mode == SWEEP_FWD_AX ? 2 * halo_span(q, es) + 2 * halo_row_span(q) : 0);
+  return sweep_nv(mode) * q.T + (mode == SWEEP_FWD_AX ? 2 * halo_span(q, es) + 2 * q.TIp : 0);
 }
 // Offsets of the halo values inside a slot (MODE 1): the value of row tj
-// of plane p is at halo_left + p*T + TIp*tj + halo_lofs, halo_right +
-// p*T + TIp*tj, halo_down + p*T + ti and halo_up + p*T + ti.
+// is at halo_left + TIp*tj + halo_lofs, halo_right + TIp*tj,
+// halo_down + ti and halo_up + ti.
 __host__ __device__ inline int halo_lofs(const SkewGeo &q, int es) { return (q.TI - 1) & (sweep_g(es) - 1); }
-__host__ __device__ inline int halo_left(const SkewGeo &q, int) { return 9 * q.ST; }
-__host__ __device__ inline int halo_right(const SkewGeo &q, int es) { return 9 * q.ST + halo_span(q, es); }
-__host__ __device__ inline int halo_down(const SkewGeo &q, int es) { return 9 * q.ST + 2 * halo_span(q, es); }
+__host__ __device__ inline int halo_left(const SkewGeo &q, int) { return 9 * q.T; }
+__host__ __device__ inline int halo_right(const SkewGeo &q, int es) { return 9 * q.T + halo_span(q, es); }
+__host__ __device__ inline int halo_down(const SkewGeo &q, int es) { return 9 * q.T + 2 * halo_span(q, es); }
 __host__ __device__ inline int halo_up(const SkewGeo &q, int es) {
-  return 9 * q.ST + 2 * halo_span(q, es) + halo_row_span(q);
+  return 9 * q.T + 2 * halo_span(q, es) + q.TIp;
 }
 // Copy c of tile b, the part that does not change from step to step: the
 // slab of step u is w = u (forward) or nsteps-1-u (backward), and the copy
@@ -126,33 +117,33 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
   l.dlo = 0; l.dhi = q.W - 1;
   const int sys_c = (mode == SWEEP_FWD) ? 1 : 0;  // copy index of the system block
   if (c == sys_c) {
-    l.base = sys_at(slab0, sweep_sys_first(mode), q.ST, 0);
-    l.wstride = SYS_N * q.ST;
-    l.dst = sweep_sys_dst(mode) * q.ST;
-    l.bytes = (mode == SWEEP_FWD_AX ? 8 : 5) * q.ST * es;
+    l.base = sys_at(slab0, sweep_sys_first(mode), q.T, 0);
+    l.wstride = SYS_N * q.T;
+    l.dst = sweep_sys_dst(mode) * q.T;
+    l.bytes = (mode == SWEEP_FWD_AX ? 8 : 5) * q.T * es;
     l.arr = 0;
     return true;
   }
   if (mode == SWEEP_BWD) return false;
-  l.wstride = q.ST;
+  l.wstride = q.T;
   l.arr = 1;
   if (c == 1 - sys_c) {  // the vector: Y (MODE 0) or P (MODE 1)
-    l.base = slab0 * q.ST;
-    l.dst = (mode == SWEEP_FWD_AX) ? 8 * q.ST : 0;
-    l.bytes = q.ST * es;
+    l.base = slab0 * q.T;
+    l.dst = (mode == SWEEP_FWD_AX) ? 8 * q.T : 0;
+    l.bytes = q.T * es;
     return true;
   }
   if (mode != SWEEP_FWD_AX) return false;
   const int bx = b % q.ntx, by = b / q.ntx, nty = q.nb / q.ntx;
   int nb_tile, dw, toff;
-  if (c == 2) {  // down: row tj = TJ-1 of tile b-ntx (of every plane)
+  if (c == 2) {  // down: row tj = TJ-1 of tile b-ntx
     if (by == 0) return false;
     nb_tile = b - q.ntx; dw = q.TJ - 1; toff = q.TIp * (q.TJ - 1);
-    l.dst = halo_down(q, es); l.bytes = halo_row_span(q) * es;
+    l.dst = halo_down(q, es); l.bytes = q.TIp * es;
   } else if (c == 3) {  // up: row tj = 0 of tile b+ntx
     if (by == nty - 1) return false;
     nb_tile = b + q.ntx; dw = -(q.TJ - 1); toff = 0;
-    l.dst = halo_up(q, es); l.bytes = halo_row_span(q) * es;
+    l.dst = halo_up(q, es); l.bytes = q.TIp * es;
   } else if (c == 4) {  // left: tile b-1, from the 16 bytes holding column TI-1 of row 0 to those of row TJ-1
     if (bx == 0) return false;
     nb_tile = b - 1; dw = q.TI - 1; toff = (q.TI - 1) & ~(sweep_g(es) - 1);
@@ -164,7 +155,7 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
   } else {
     return false;
   }
-  l.base = ((long long)nb_tile * q.W + dw) * q.ST + toff;
+  l.base = ((long long)nb_tile * q.W + dw) * q.T + toff;
   l.dlo = dw < 0 ? -dw : 0;                 // 0 <= w + dw
   l.dhi = dw > 0 ? q.W - 1 - dw : q.W - 1;  // w + dw <= W-1
   return true;

@@ -503,10 +503,7 @@ struct orc_handle {
     const int TJ = std::min(P.precond_tj > 0 ? P.precond_tj : NJ - 2, NJ - 2) /
                    (P.precond_split == 2 ? 2 : 1);  // rows of a layout tile
     const int TIp = (TI + 3) & ~3;
-    // planes per slab: two with sweep_planes 2 (one thread block per
-    // preconditioner block); entry e of a slab is plane e / T, column e % T
-    const int PL = (P.sweep_planes == 2 && P.precond_split != 2) ? 2 : 1;
-    const int T = TIp * TJ, ST = PL * T, W = (NK - 2 + PL - 1) / PL + (TI - 1) + (TJ - 1);
+    const int T = TIp * TJ, W = (NK - 2) + (TI - 1) + (TJ - 1);
     const int ntx = (NI - 2 + TI - 1) / TI, nb = ntx * ((NJ - 2 + TJ - 1) / TJ);
     const long long NS = (long long)nb * W;
     std::vector<double> R(NS);
@@ -515,11 +512,10 @@ struct orc_handle {
       const int b = (int)(sl / W), w = (int)(sl % W), bx = b % ntx, by = b / ntx;
       for (int l = 0; l < 32; ++l) {
         double s = 0.0, c;
-        for (int e = l; e < ST; e += 32) {
-          const int pl = e / T, t = e % T;
+        for (int t = l; t < T; t += 32) {
           const int ti = t % TIp, tj = t / TIp;
-          const int I = 2 + bx * TI + ti, J = 2 + by * TJ + tj, k = 2 + PL * (w - ti - tj) + pl;
-          if (ti >= TI || I > NI - 1 || J > NJ - 1 || w < ti + tj || k > NK - 1) continue;
+          const int I = 2 + bx * TI + ti, J = 2 + by * TJ + tj, k = 2 + w - ti - tj;
+          if (ti >= TI || I > NI - 1 || J > NJ - 1 || k < 2 || k > NK - 1) continue;
           if (f(I, J, k, c)) s = s + c;
         }
         lane[l] = s;

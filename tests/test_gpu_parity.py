@@ -107,41 +107,6 @@ def test_two_sweep_blocks_per_sm_bitwise(gpu_lib, pkg, orc, solver):
         assert_same(a.get_state(), b.get_state(), f"mixed step {n}")
 
 
-@pytest.mark.parametrize("nz", [30, 31])
-def test_two_planes_per_step_bitwise(gpu_lib, pkg, orc, nz):
-    """Two k-planes per wavefront step (sweep_planes 2: the solver layout
-    holds two planes to a slab, the sweeps and the factorisation take two
-    cells of a column per step): bit for bit with the oracle summing in the
-    same slab order, for an even and an odd number of layers (the last
-    pair half padding), with 16x16 blocks and with one block per grid."""
-    c = pkg.cases.porous_flume(nx=96, ny=32, nz=nz, dx=0.05, dz=0.025, depth=0.4,
-                               block=(1.2, 1.8, 0.5), sponge_width=0.6, dt=2e-3)
-    run_pair(pkg, orc, c, 6, check_every=3, precond_ti=16, precond_tj=16, cgepsr=1e-10, sweep_planes=2)
-    t = pkg.cases.random_tank(6)
-    run_pair(pkg, orc, t, 8, check_every=4, sweep_planes=2)
-
-
-def test_two_planes_mixed_solver(gpu_lib, pkg):
-    """The mixed solver with two planes per step reaches the same tolerance
-    and agrees with its one-plane run to the solve's tolerance (the sums
-    group their terms by slab, so the bits differ)."""
-    c = pkg.cases.porous_flume(nx=96, ny=32, nz=31, dx=0.05, dz=0.025, depth=0.4,
-                               block=(1.2, 1.8, 0.5), sponge_width=0.6, dt=2e-3)
-    over = dict(precond_ti=16, precond_tj=16, cgepsr=1e-10, solver=1, diag_relres=1)
-    a = pkg.Tank(c, sweep_planes=2, **over)
-    b = pkg.Tank(c, sweep_planes=1, **over)
-    for t in (a, b):
-        t.init_state(True)
-    for _ in range(6):
-        a.step(c.dt)
-        b.step(c.dt)
-        assert a.stats()["true_relres"] <= 1e-10
-    sa, sb = a.get_state(), b.get_state()
-    assert np.abs(sa["pp"] - sb["pp"]).max() <= 1e-7 * np.abs(sb["pp"]).max()
-    assert np.abs(sa["uu"] - sb["uu"]).max() <= 1e-9
-    assert np.array_equal(sa["nf"], sb["nf"])
-
-
 def test_porous_flume_with_sponge_bitwise(gpu_lib, pkg, orc):
     c = pkg.cases.porous_flume(nx=64, ny=6, nz=30, dx=0.05, dz=0.025, depth=0.4,
                                block=(1.2, 1.8, 0.5), sponge_width=0.6, dt=2e-3)
