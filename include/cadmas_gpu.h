@@ -278,6 +278,72 @@ int cadmas_stream_solve(int order, double depth, double period, double height, d
    water level, as the wave maker uses them (host only; NULL skips).    */
 int cadmas_stream_eval(const cadmas_stream_wave *s, double phase, double z, double *eta, double *u, double *w);
 
+/* ---- wave theories of the wave maker and the wave source ----------------
+   FUNC STREAM N | STOKES | CNOIDAL | STK-CND of WAVE-BC and WAVE-SRC
+   (IBCTYP(2,JD) / ISCTYP(2), vf_iimdl.f:51-66,133-147).  cadmas_wave_solve
+   does at set-up what vf_csetup.f:96-124 (and 270-300 for the source) do:
+   the STK-CND choice by the Ursell number, VF_CWMAK0 (the wave and its
+   length) and VF_CWZERO (the start phase).  cadmas_wave_eval is
+   VF_CWMAK1 (level) and VF_CWMAK2 (velocities).
+     type >= 1  the stream-function wave of that order (cadmas_stream_solve);
+     type -1    cnoidal, third order (vf_wcnd0.f VF_CND0/1/2);
+     type -2    Stokes, fifth order (vf_wstk0.f VF_STK0/1/2);
+     type 0     STK-CND: Stokes when GRZ0 H T^2 / D^2 <= 25, else cnoidal.
+   The theories use g = 9.8 m/s^2 as the reference's routines do; only the
+   Ursell number uses grz0.  Stokes and cnoidal coefficients are kept in the
+   units of the reference's routines, centimetres and seconds.            */
+#define CADMAS_WAVE_STK_CND 0
+#define CADMAS_WAVE_CNOIDAL (-1)
+#define CADMAS_WAVE_STOKES (-2)
+typedef struct cadmas_stokes_wave {
+  double kd;             /* k d                                                */
+  double k;              /* wave number, 1/cm                                   */
+  double eps;            /* k H / 2, the expansion parameter                    */
+  double c0, c;          /* linear and fifth-order celerity, cm/s               */
+  double a[5];           /* eta = sum_i a[i-1] cos(i theta), cm                 */
+  double b[5];           /* u = b0 + sum_i b[i-1] cosh(i k (z+d)) cos(i theta),
+                            w = sum_i b[i-1] sinh(i k (z+d)) sin(i theta), cm/s */
+  double b0;             /* cm/s                                                */
+  double p0;             /* pressure-head constant, cm                          */
+  int iterations, pad;   /* iterations of the dispersion relation              */
+} cadmas_stokes_wave;
+typedef struct cadmas_cnoidal_wave {
+  double ql;             /* pi K'/K of the Jacobi elliptic functions (modulus) */
+  double s;              /* the vertical-velocity scale RK of VF_CND0          */
+  double d;              /* depth, cm                                           */
+  double c0, c;          /* sqrt(g d) and the celerity, cm/s                    */
+  double a[4];           /* eta = sum_i a[i-1] cn^(2(i-1)), cm                  */
+  double b[12];          /* B(j,i) at (i-1)*3 + j-1: u = sum_i cn^(2(i-1))
+                            sum_j B(j,i) Z^(2(j-1)), Z = 1 + z/d, cm/s           */
+  double bb[12];         /* BB(j,i): w = Z cn sn dn sum_i cn^(2(i-2))
+                            sum_j BB(j,i) Z^(2(j-1)), cm/s                        */
+  double p0;             /* pressure-head constant, cm                          */
+  int iterations, pad;   /* iterations for the elliptic parameter              */
+} cadmas_cnoidal_wave;
+typedef struct cadmas_wave_theory {
+  int type;              /* after the STK-CND choice: N >= 1, -1 or -2          */
+  int pad;
+  double depth, period, height;  /* D, T, H (m, s)                             */
+  double length;         /* WVLENG (BCTYP(4,JD), SCTYP(4))                      */
+  double ursell;         /* GRZ0 H T^2 / D^2 (BCTYP(5,JD), SCTYP(5))           */
+  double phase0;         /* VF_CWZERO: the phase in [0.5, 1] where the level
+                            crosses zero, found in single precision
+                            (BCTYP(6,JD), SCTYP(6))                            */
+  cadmas_stream_wave stream;     /* type >= 1                                  */
+  cadmas_stokes_wave stokes;     /* type -2                                    */
+  cadmas_cnoidal_wave cnoidal;   /* type -1                                    */
+} cadmas_wave_theory;
+/* Solve for the wave (host only).  CADMAS_EINVAL for an unknown type or
+   non-positive D, T, H; CADMAS_EWAVE when the stream-function solution
+   does not converge or a theory gives no finite wave.                    */
+int cadmas_wave_solve(int type, double depth, double period, double height, double grz0,
+                      cadmas_wave_theory *out);
+/* The level eta at `phase` (VF_CWMAK1) and the velocities normal to the
+   side (u) and vertical (w) at height z above the still water level
+   (VF_CWMAK2), in metres and m/s as the wave maker uses them (host only;
+   NULL skips).                                                           */
+int cadmas_wave_eval(const cadmas_wave_theory *t, double phase, double z, double *eta, double *u, double *w);
+
 typedef struct cadmas_wave_bc {
   int side;              /* JD: 1 X-, 2 X+, 3 Y-, 4 Y+                      */
   int first, last;       /* IBCTYP(3..4,JD): J (X sides) or I (Y sides) of
@@ -300,8 +366,9 @@ typedef struct cadmas_wave_bc {
    vf_vpcoef.f:349-350), the surface cells of the line (VF_BSUWN,
    vf_bsuwn.f:81-118) and F (VF_FGENE, vf_fgene.f:42-70, through
    VF_FEULER's QF).  The table is the one of cadmas_set_wave (MTBTYP 1 or
-   2; 3 is 'MTBTYP ERROR.' in the reference, vf_csetup.f:267).  The wave
-   theories (STREAM, STOKES, CNOIDAL) are not built for the source.       */
+   2; 3 is 'MTBTYP ERROR.' in the reference, vf_csetup.f:267).  With a
+   wave theory (cadmas_set_wave_source_func) the velocities come from
+   VF_CWMAK2 at the scaled heights instead, no table needed.              */
 typedef struct cadmas_wave_src {
   int line;              /* ISCTYP(1): > 0 the x source at I = line (1-based
                             with ghosts, 2..NUMI-1); < 0 the y source at
@@ -585,8 +652,34 @@ int cadmas_test_stall_sweeps(cadmas_handle *h, int from_step);
 /* Side w->side as a wave maker driven by the wave `s` (WAVE-BC ... FUNC
    STREAM N): depth, period and fade-in from `w`; replaces
    VF_CWMAK0/1/2 calls of VF_BWUWN (vf_bwuwn.f:259-470) for that side.
-   Oblique incidence is not built.                                        */
+   The same as cadmas_set_wave_func with a theory of type s->order.      */
 int cadmas_set_wave_theory(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *s);
+
+/* Side w->side as a wave maker driven by the theory `t` (WAVE-BC ... FUNC
+   STREAM N | STOKES | CNOIDAL | STK-CND, solved by cadmas_wave_solve with
+   the side's depth, height and period): each step the level at the side's
+   phase (T0 = t->phase0) and the face velocities at the heights scaled to
+   the column's water level (vf_bwuwn.f:259-470).                         */
+int cadmas_set_wave_func(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_theory *t);
+
+/* Oblique incidence of the wave-maker side `side` (WAVE-BC ... ANGLE a X Y,
+   BCTYP(9..11,JD)): the wave travels at `angle` degrees from the side's
+   inward normal (counter-clockwise), its phase at TNOW = 0 being the
+   theory's start phase on the line through (sx, sy) normal to the
+   direction of travel.  Each column of the side then has its own phase,
+   T0 - (TNOW/T - r/L) with r its distance along the direction of travel
+   (vf_bwuwn.f:312-356, 418-430), its own level and its own velocities,
+   the normal part times cos and the tangential part times sin of the
+   direction.  angle = 0 is normal incidence.  Only wave theories take an
+   angle: CADMAS_EINVAL for a matrix-table side ('(WAVE-BC ANGLE) CAN NOT
+   USE.', vf_csetup.f:97-99).  Call after the side is set.               */
+int cadmas_set_wave_angle(cadmas_handle *h, int side, double angle, double sx, double sy);
+
+/* The wave source of the handle driven by the theory `t` (WAVE-SRC ...
+   FUNC STREAM N | STOKES | CNOIDAL | STK-CND), solved with the source's
+   depth, height and period: SRCUV of each line from VF_CWMAK2 at the
+   heights scaled to the column's level (vf_cwmsrc.f:66-143).             */
+int cadmas_set_wave_source_func(cadmas_handle *h, const cadmas_wave_src *s, const cadmas_wave_theory *t);
 
 /* The wave source of the handle (one line, as the reference allows),
    with the matrix table `t` (NULL: the table already given to

@@ -75,6 +75,58 @@ def stream_eval(sw: StreamWave, phase, z=0.0, lib=None):
     return e.value, u.value, w.value
 
 
+WAVE_STK_CND, WAVE_CNOIDAL, WAVE_STOKES = 0, -1, -2
+_WAVE_FUNCS = {"stk-cnd": WAVE_STK_CND, "cnoidal": WAVE_CNOIDAL, "stokes": WAVE_STOKES}
+
+
+class StokesWave(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("kd", "k", "eps", "c0", "c")] + [
+        ("a", C.c_double * 5), ("b", C.c_double * 5), ("b0", C.c_double), ("p0", C.c_double),
+        ("iterations", C.c_int), ("pad", C.c_int)]
+
+
+class CnoidalWave(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("ql", "s", "d", "c0", "c")] + [
+        ("a", C.c_double * 4), ("b", C.c_double * 12), ("bb", C.c_double * 12), ("p0", C.c_double),
+        ("iterations", C.c_int), ("pad", C.c_int)]
+
+
+class WaveTheory(C.Structure):
+    _fields_ = [("type", C.c_int), ("pad", C.c_int)] + [
+        (n, C.c_double) for n in ("depth", "period", "height", "length", "ursell", "phase0")] + [
+        ("stream", StreamWave), ("stokes", StokesWave), ("cnoidal", CnoidalWave)]
+
+
+def wave_type(func) -> int:
+    """IWVTYP of a wave-theory name ("stokes", "cnoidal", "stk-cnd") or a
+    stream-function order N >= 1."""
+    if isinstance(func, str):
+        return _WAVE_FUNCS[func.lower()]
+    return int(func)
+
+
+def wave_solve(func, depth, period, height, grz0=9.8, lib=None) -> WaveTheory:
+    """A wave theory of the wave maker or the wave source (cadmas_wave_solve,
+    host only): `func` a stream-function order N or "stokes", "cnoidal",
+    "stk-cnd" (the choice by the Ursell number)."""
+    lib = lib or load_library()
+    out = WaveTheory()
+    lib.cadmas_wave_solve.argtypes = [C.c_int] + [C.c_double] * 4 + [C.POINTER(WaveTheory)]
+    _check(lib, lib.cadmas_wave_solve(wave_type(func), float(depth), float(period), float(height), float(grz0),
+                                      C.byref(out)))
+    return out
+
+
+def wave_eval(th: WaveTheory, phase, z=0.0, lib=None):
+    """(eta, u, w) of a wave theory at `phase` and height z above the still
+    water level, as the wave maker uses them (cadmas_wave_eval)."""
+    lib = lib or load_library()
+    e, u, w = C.c_double(), C.c_double(), C.c_double()
+    lib.cadmas_wave_eval.argtypes = [C.POINTER(WaveTheory), C.c_double, C.c_double, _dp, _dp, _dp]
+    _check(lib, lib.cadmas_wave_eval(C.byref(th), float(phase), float(z), C.byref(e), C.byref(u), C.byref(w)))
+    return e.value, u.value, w.value
+
+
 class WaveSrc(C.Structure):
     _fields_ = [("line", C.c_int), ("pad", C.c_int), ("depth", C.c_double), ("period", C.c_double),
                 ("ramp", C.c_double)]
@@ -155,7 +207,9 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_unet_get_params", "cadmas_unet_forward", "cadmas_unet_grad", "cadmas_unet_train_step",
             "cadmas_set_warm_net", "cadmas_warm_stats", "cadmas_get_solve", "cadmas_get_system",
             "cadmas_unet_train_sys", "cadmas_unet_time_forward", "cadmas_test_stall_sweeps",
-            "cadmas_set_wave_source", "cadmas_stream_solve", "cadmas_stream_eval", "cadmas_set_wave_theory"]
+            "cadmas_set_wave_source", "cadmas_stream_solve", "cadmas_stream_eval", "cadmas_set_wave_theory",
+            "cadmas_wave_solve", "cadmas_wave_eval", "cadmas_set_wave_func", "cadmas_set_wave_angle",
+            "cadmas_set_wave_source_func"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
@@ -458,8 +512,13 @@ class Tank:
 
     def set_wave_source(self, src):
         """Wave source line from a dict made by cases.wave_source
-        (cadmas_set_wave_source)."""
+        (cadmas_set_wave_source with a table, cadmas_set_wave_source_func
+        with a wave theory)."""
         ws, tab, keep = source_structs(src)
+        if src.get("theory") is not None:
+            self.lib.cadmas_set_wave_source_func.argtypes = [C.c_void_p, C.POINTER(WaveSrc), C.POINTER(WaveTheory)]
+            _check(self.lib, self.lib.cadmas_set_wave_source_func(self.h, C.byref(ws), C.byref(src["theory"])))
+            return
         self.lib.cadmas_set_wave_source.argtypes = [C.c_void_p, C.POINTER(WaveSrc), C.POINTER(WaveTable)]
         _check(self.lib, self.lib.cadmas_set_wave_source(self.h, C.byref(ws), C.byref(tab) if tab else None))
 
@@ -472,16 +531,23 @@ class Tank:
     def set_wave(self, wave):
         """Wave-maker side from a dict made by cases.wave_maker
         (cadmas_set_wave with a table, cadmas_set_wave_theory with a
-        stream-function wave)."""
-        if wave.get("stream") is not None:
-            bc = WaveBC(int(wave["side"]), int(wave["first"]), int(wave["last"]), 0, float(wave["depth"]),
-                        float(wave["period"]), float(wave.get("ramp", 0.0)))
-            sw = wave["stream"]
+        stream-function wave, cadmas_set_wave_func with a wave theory, then
+        cadmas_set_wave_angle for oblique incidence)."""
+        bc = WaveBC(int(wave["side"]), int(wave["first"]), int(wave["last"]), 0, float(wave["depth"]),
+                    float(wave["period"]), float(wave.get("ramp", 0.0)))
+        if wave.get("theory") is not None:
+            self.lib.cadmas_set_wave_func.argtypes = [C.c_void_p, C.POINTER(WaveBC), C.POINTER(WaveTheory)]
+            _check(self.lib, self.lib.cadmas_set_wave_func(self.h, C.byref(bc), C.byref(wave["theory"])))
+        elif wave.get("stream") is not None:
             self.lib.cadmas_set_wave_theory.argtypes = [C.c_void_p, C.POINTER(WaveBC), C.POINTER(StreamWave)]
-            _check(self.lib, self.lib.cadmas_set_wave_theory(self.h, C.byref(bc), C.byref(sw)))
-            return
-        bc, tab, keep = wave_structs(wave)
-        _check(self.lib, self.lib.cadmas_set_wave(self.h, C.byref(bc), C.byref(tab)))
+            _check(self.lib, self.lib.cadmas_set_wave_theory(self.h, C.byref(bc), C.byref(wave["stream"])))
+        else:
+            bc, tab, keep = wave_structs(wave)
+            _check(self.lib, self.lib.cadmas_set_wave(self.h, C.byref(bc), C.byref(tab)))
+        if wave.get("angle") is not None:
+            a, sx, sy = (float(v) for v in wave["angle"])
+            self.lib.cadmas_set_wave_angle.argtypes = [C.c_void_p, C.c_int] + [C.c_double] * 3
+            _check(self.lib, self.lib.cadmas_set_wave_angle(self.h, int(wave["side"]), a, sx, sy))
 
     # ------------------------------------------------------------ state
     def set_state(self, arrs):

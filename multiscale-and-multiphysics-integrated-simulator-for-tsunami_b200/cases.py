@@ -710,13 +710,16 @@ def first_order_wave_table(H: float, T: float, depth: float, g0: float = 9.8, nt
 
 
 def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: float = 0.0,
-               table: dict | None = None, stream: int = 0) -> Case:
+               table: dict | None = None, stream: int = 0, func: str | None = None,
+               angle: tuple | None = None) -> Case:
     """Make side `side` (1 X-, 2 X+, 3 Y-, 4 Y+) a wave-maker boundary:
     its domain-boundary faces get B.C. type 5 for velocity and F
     (WAVE-BC, INDB(3,L) = INDB(4,L) = 5) over the whole side, driven by
     the stream-function wave of order `stream` (WAVE-BC ... FUNC STREAM N)
-    when stream >= 1, else by a first-order wave table unless `table` is
-    given."""
+    when stream >= 1, by the theory `func` ("stokes", "cnoidal",
+    "stk-cnd": FUNC STOKES | CNOIDAL | STK-CND), else by a first-order wave
+    table unless `table` is given.  `angle` = (degrees, x, y) makes the
+    incidence oblique (WAVE-BC ... ANGLE; wave theories only)."""
     ns = {1: 1, 2: 2, 3: 3, 4: 4}[side]
     for L in range(c.indb.shape[1]):
         ijk, NS = int(c.indb[0, L]), int(c.indb[1, L])
@@ -729,32 +732,46 @@ def wave_maker(c: Case, H: float, T: float, depth: float, side: int = 1, ramp: f
             c.indb[2, L] = VP_WAVE
             c.indb[3, L] = F_WAVE
     first, last = 2, (c.nj - 1 if side <= 2 else c.ni - 1)
+    if func is not None:
+        from . import wave_solve
+        c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp, table=None,
+                      theory=wave_solve(func, depth, T, H, c.params.get("grz0", 9.8)), angle=angle)
+        return c
     if stream >= 1:
         from . import stream_solve
         c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp, table=None,
-                      stream=stream_solve(stream, depth, T, H, c.params.get("grz0", 9.8)))
+                      stream=stream_solve(stream, depth, T, H, c.params.get("grz0", 9.8)), angle=angle)
         return c
+    if angle is not None:
+        raise ValueError("(WAVE-BC ANGLE) CAN NOT USE.: an angle needs a wave theory")
     c.wave = dict(side=side, first=first, last=last, depth=depth, period=T, ramp=ramp,
                   table=table if table is not None else first_order_wave_table(H, T, depth))
     return c
 
 
 def wave_source(c: Case, line: int, H: float, T: float, depth: float, ramp: float = 0.0, axis: str = "x",
-                table: dict | None = None) -> Case:
-    """A wave source line (MODEL WAVE-SRC X|Y ... FUNC MATRIX): the cell
-    column I = `line` (axis x, 1-based with ghosts) or row J = `line`
-    (axis y) emits waves to both sides, its strength the velocity column of
-    a first-order wave table unless `table` is given (the table is the one
+                table: dict | None = None, func=None) -> Case:
+    """A wave source line (MODEL WAVE-SRC X|Y ...): the cell column
+    I = `line` (axis x, 1-based with ghosts) or row J = `line` (axis y)
+    emits waves to both sides, its strength the velocity of the wave theory
+    `func` (a stream-function order N, "stokes", "cnoidal" or "stk-cnd":
+    FUNC STREAM N | STOKES | CNOIDAL | STK-CND) or else of a first-order
+    wave table unless `table` is given (FUNC MATRIX; the table is the one
     of a wave maker, if the case has one)."""
+    ln = int(line) if axis == "x" else -int(line)
+    if func is not None:
+        from . import wave_solve
+        c.source = dict(line=ln, depth=depth, period=T, ramp=ramp, table=None,
+                        theory=wave_solve(func, depth, T, H, c.params.get("grz0", 9.8)))
+        return c
     if table is None and getattr(c, "wave", None) is None:
         table = first_order_wave_table(H, T, depth)
-    c.source = dict(line=int(line) if axis == "x" else -int(line), depth=depth, period=T, ramp=ramp,
-                    table=table)
+    c.source = dict(line=ln, depth=depth, period=T, ramp=ramp, table=table)
     return c
 
 
 def source_flume(nx=120, ny=4, nz=40, dx=0.05, dz=0.01, depth=0.25, H=0.03, T=1.2, ramp=0.5,
-                 axis="x", sponge_width=1.0, dt=2.0e-3) -> Case:
+                 axis="x", sponge_width=1.0, dt=2.0e-3, func=None) -> Case:
     """Still water between two damping zones with a wave source line in
     the middle: along x, the column I = nx/2 + 2 of an nx x ny x nz flume;
     along y, the row J = nx/2 + 2 of the same flume turned by 90 degrees
@@ -774,7 +791,7 @@ def source_flume(nx=120, ny=4, nz=40, dx=0.05, dz=0.01, depth=0.25, H=0.03, T=1.
     init_f_still_water(c, depth)
     c.dt = dt
     finish(c)
-    wave_source(c, nx // 2 + 2, H, T, depth, ramp=ramp, axis=axis)
+    wave_source(c, nx // 2 + 2, H, T, depth, ramp=ramp, axis=axis, func=func)
     return c
 
 

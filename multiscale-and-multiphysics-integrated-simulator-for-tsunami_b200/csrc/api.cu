@@ -179,9 +179,15 @@ struct cadmas_handle {
     bool on = false;
     int first = 0, last = 0;
     double d = 0.0, t = 0.0, a = 0.0;
-    bool theory = false;     // FUNC STREAM N: the wave `sw`, not the table
-    cadmas_stream_wave sw{};
+    bool theory = false;     // FUNC STREAM N | STOKES | CNOIDAL: the wave `th`, not the table
+    cadmas_wave_theory th{};
+    double angle = 0.0, sx = 0.0, sy = 0.0;  // ANGLE: BCTYP(9..11,JD)
+    int ncol = 0;                 // oblique incidence: lines first..last, their
+    WaveCol *col = nullptr;       // level and phase part (device),
+    WaveCol *col_h = nullptr;     // the pinned host copy they are filled in,
+    cudaEvent_t col_ev = nullptr; // and the end of its last upload
   } wave[4];
+  std::vector<double> xx1, yy1;  // XX(1,I), YY(1,J) on the host, 1-based
   // open (radiation) boundary: sides JD = 1..4 and their phase speed C
   struct OpenSide {
     bool on = false;
@@ -201,6 +207,8 @@ struct cadmas_handle {
     bool on = false;
     int line = 0;
     double d = 0.0, t = 0.0, a = 0.0;
+    bool theory = false;          // a wave theory `th` instead of the table
+    cadmas_wave_theory th{};
   } src;
   double *srcuv = nullptr;
   double src_level = 0.0;  // SCTYP(7) = WVZ*AW of the last step
@@ -286,14 +294,15 @@ static bool cwmtb1(cadmas_handle *h, double WVT, double &W1, double &W2, double 
   return true;
 }
 
-// Wave-maker part of VF_BWUWN (vf_bwuwn.f:259-470) for the matrix-table
-// inflow: the time part here, the faces on the device (k_wave).
+// Wave-maker part of VF_BWUWN (vf_bwuwn.f:259-470): the time part here
+// (phase, fade-in, the table's row weights or the theory's level and phase
+// part, per line under oblique incidence), the faces on the device (k_wave).
 static int wave_bc(cadmas_handle *h) {
   const double PI = 3.141592653589794, ZERO = 1.0e-20;  // VF_A0PRM.h
   for (int jd = 0; jd < 4; ++jd) {
-    const cadmas_handle::WaveSide &ws = h->wave[jd];
+    cadmas_handle::WaveSide &ws = h->wave[jd];
     if (!ws.on) continue;
-    const double T = ws.t, T0 = ws.theory ? ws.sw.phase0 : h->dmtbt0;
+    const double T = ws.t, T0 = ws.theory ? ws.th.phase0 : h->dmtbt0;
     float R4TN = (float)(T0 - h->tnow / T);
     R4TN = R4TN - (float)(int)R4TN;
     if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
@@ -305,13 +314,14 @@ static int wave_bc(cadmas_handle *h) {
     const double WVT = (double)R4TN;
     WaveDev w;
     w.theory = ws.theory ? 1 : 0;
+    w.col = nullptr;
     if (ws.theory) {  // VF_CWMAK1: the level at the phase; VF_CWMAK2 per face on the device
-      w.wvz = stream_eta(ws.sw, WVT);
-      stream_phase(ws.sw, WVT, w.ph);
+      w.wvz = theory_eta(ws.th, WVT);
+      theory_phase(ws.th, WVT, w.ph);
       w.wt1 = w.wt2 = 0.0;
     } else {
       if (!cwmtb1(h, WVT, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
-      w.ph.n = 0;
+      std::memset(&w.ph, 0, sizeof(w.ph));
     }
     h->wave_level[jd] = w.wvz * AW;
     w.side = jd + 1; w.first = ws.first; w.last = ws.last;
@@ -319,6 +329,36 @@ static int wave_bc(cadmas_handle *h) {
     w.d = ws.d; w.aw = AW; w.wvlvl = h->P.wvlvl;
     w.sa = (jd == 0) ? 1.0 : (jd == 1 ? -1.0 : 0.0);  // normal incidence (vf_bwuwn.f:298-310)
     w.sb = (jd == 2) ? 1.0 : (jd == 3 ? -1.0 : 0.0);
+    if (ws.theory && std::fabs(ws.angle) > ZERO) {
+      // oblique incidence (vf_bwuwn.f:312-324): the direction of travel,
+      // then each line's phase from its distance along it (345-356 on
+      // the X sides at the face's x and the cell's middle y, 418-430 on
+      // the Y sides the other way round)
+      const double off[4] = {0.0, 180.0, 90.0, 270.0};
+      double SA = (ws.angle + off[jd]) * PI / 180.0;
+      const double SB = std::sin(SA);
+      SA = std::cos(SA);
+      const double SC = -(SA * ws.sx + SB * ws.sy), DL = ws.th.length;
+      if (ws.col_ev) CK(cudaEventSynchronize(ws.col_ev));  // the last upload of col_h is done
+      const bool xs = jd <= 1;
+      const int NI = h->g.NI, NJ = h->g.NJ;
+      for (int n = ws.first; n <= ws.last; ++n) {
+        double X0, Y0;
+        if (xs) { X0 = h->xx1[jd == 0 ? 2 : NI]; Y0 = (h->yy1[n] + h->yy1[n + 1]) * 0.5; }
+        else { Y0 = h->yy1[jd == 2 ? 2 : NJ]; X0 = (h->xx1[n] + h->xx1[n + 1]) * 0.5; }
+        const double RR = (SA * X0 + SB * Y0 + SC) / std::sqrt(SA * SA + SB * SB);
+        float R4 = (float)(T0 - (h->tnow / T - RR / DL));
+        R4 = R4 - (float)(int)R4;
+        if (R4 < 0.0f) R4 = R4 + 1.0f;
+        WaveCol &c = ws.col_h[n - ws.first];
+        c.wvz = theory_eta(ws.th, (double)R4);
+        theory_phase(ws.th, (double)R4, c.ph);
+      }
+      CK(cudaMemcpyAsync(ws.col, ws.col_h, (size_t)ws.ncol * sizeof(WaveCol), cudaMemcpyHostToDevice, h->s));
+      CK(cudaEventRecord(ws.col_ev, h->s));
+      w.col = ws.col;
+      w.sa = SA; w.sb = SB;
+    }
     w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
     // a fixed-water-level table sets no velocities (vf_bwuwn.f:330-331)
     if (ws.theory || h->mtbtyp != 3) launch_wave(h->s, h->g, h->f, w, h->dint);
@@ -326,14 +366,15 @@ static int wave_bc(cadmas_handle *h) {
   return CADMAS_OK;
 }
 
-// VF_CWMSRC (vf_cwmsrc.f:46-143) for the matrix table: the phase and
-// fade-in at TNOW and VF_CWMTB1's row weights on the host, SRCUV of every
-// line of the source on the device (k_srcuv).  The reference calls it at
-// TNOW + DT before the step's V1CAL, which is this step's TNOW.
+// VF_CWMSRC (vf_cwmsrc.f:46-143): the phase and fade-in at TNOW and
+// VF_CWMTB1's row weights or the theory's level and phase part on the
+// host, SRCUV of every line of the source on the device (k_srcuv).  The
+// reference calls it at TNOW + DT before the step's V1CAL, which is this
+// step's TNOW.
 static int wave_src(cadmas_handle *h) {
   const double PI = 3.141592653589794, ZERO = 1.0e-20;  // VF_A0PRM.h
   const cadmas_handle::WaveSrc &ws = h->src;
-  const double T = ws.t, T0 = h->dmtbt0;
+  const double T = ws.t, T0 = ws.theory ? ws.th.phase0 : h->dmtbt0;
   float R4TN = (float)(T0 - h->tnow / T);
   R4TN = R4TN - (float)(int)R4TN;
   if (R4TN < 0.0f) R4TN = R4TN + 1.0f;
@@ -343,10 +384,19 @@ static int wave_src(cadmas_handle *h) {
     if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
   }
   WaveDev w;
-  if (!cwmtb1(h, (double)R4TN, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
+  w.col = nullptr;
+  w.theory = ws.theory ? 1 : 0;
+  if (ws.theory) {
+    w.wvz = theory_eta(ws.th, (double)R4TN);
+    theory_phase(ws.th, (double)R4TN, w.ph);
+    w.wt1 = w.wt2 = 0.0;
+  } else {
+    if (!cwmtb1(h, (double)R4TN, w.wt1, w.wt2, w.wvz)) return CADMAS_EPG;
+    std::memset(&w.ph, 0, sizeof(w.ph));
+  }
   h->src_level = w.wvz * AW;
   w.side = ws.line; w.first = 0; w.last = 0;
-  w.mtbtyp = h->mtbtyp; w.nzz = h->nzz; w.mtbnow = h->mtbnow;
+  w.mtbtyp = ws.theory ? 1 : h->mtbtyp; w.nzz = h->nzz; w.mtbnow = h->mtbnow;
   w.d = ws.d; w.aw = AW; w.wvlvl = h->P.wvlvl;
   w.sa = 0.0; w.sb = 0.0;
   w.zz = h->wzz; w.un = h->wun; w.ut = h->wut;
@@ -1134,6 +1184,11 @@ int cadmas_destroy(cadmas_handle *h) {
   if (h->h_int) cudaFreeHost(h->h_int);
   if (h->h_res) cudaFreeHost(h->h_res);
   for (double *q : {h->wzz, h->wun, h->wut, h->srcuv}) if (q) cudaFree(q);
+  for (auto &ws : h->wave) {
+    if (ws.col) cudaFree(ws.col);
+    if (ws.col_h) cudaFreeHost(ws.col_h);
+    if (ws.col_ev) cudaEventDestroy(ws.col_ev);
+  }
   for (double *q : {h->drop.tx, h->drop.ty, h->drop.tz, h->drop.uu, h->drop.vv, h->drop.ww}) if (q) cudaFree(q);
   for (double *q : {h->ak, h->ae_k, h->ak2, h->ae2, h->anut, h->bck, h->bce, h->bck0, h->bce0}) if (q) cudaFree(q);
   if (h->wnet) cadmas_unet_destroy(h->wnet);
@@ -1174,58 +1229,132 @@ static int set_table(cadmas_handle *h, const cadmas_wave_table *t) {
   return CADMAS_OK;
 }
 
-int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
-  if (!h || !w || !t) return CADMAS_EINVAL;
+// The side's oblique-incidence buffers: one WaveCol per line, on the
+// device and pinned on the host, (re)made for the side's line range.
+static int wave_cols(cadmas_handle::WaveSide &ws, bool need) {
+  const int n = need ? ws.last - ws.first + 1 : 0;
+  if (n == ws.ncol) return CADMAS_OK;
+  if (ws.col_ev) cudaEventSynchronize(ws.col_ev);
+  if (ws.col) cudaFree(ws.col);
+  if (ws.col_h) cudaFreeHost(ws.col_h);
+  ws.col = nullptr; ws.col_h = nullptr; ws.ncol = 0;
+  if (n == 0) return CADMAS_OK;
+  CK(cudaMalloc(&ws.col, (size_t)n * sizeof(WaveCol)));
+  CK(cudaMallocHost(&ws.col_h, (size_t)n * sizeof(WaveCol)));
+  if (!ws.col_ev) CK(cudaEventCreateWithFlags(&ws.col_ev, cudaEventDisableTiming));
+  ws.ncol = n;
+  return CADMAS_OK;
+}
+
+// The checks of a wave-maker side common to the table and the theories.
+static int wave_side_ok(cadmas_handle *h, const cadmas_wave_bc *w) {
   if (w->side < 1 || w->side > 4) return CADMAS_EINVAL;
-  if (t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
-  if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
   if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
     g_last_error = "side already declared open";
     return CADMAS_EINVAL;
   }
   const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;  // vf_iimdl.f:101-106
   if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
+  return CADMAS_OK;
+}
+
+int cadmas_set_wave(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t) {
+  if (!h || !w || !t) return CADMAS_EINVAL;
+  { const int rs = wave_side_ok(h, w); if (rs) return rs; }
+  if (t->mtbtyp < 1 || t->mtbtyp > 3) return CADMAS_EINVAL;
+  if (!(w->period > 0.0) || (t->mtbtyp == 1 && !(w->depth > 0.0))) return CADMAS_EINVAL;
+  cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
+  if (std::fabs(ws.angle) > 1.0e-20) {  // vf_csetup.f:97-99
+    g_last_error = "(WAVE-BC ANGLE) CAN NOT USE.";
+    return CADMAS_EINVAL;
+  }
   { const int rt = set_table(h, t); if (rt) return rt; }
+  ws.on = true; ws.first = w->first; ws.last = w->last;
+  ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
+  ws.theory = false;
+  refresh_prm(h);
+  return CADMAS_OK;
+}
+
+// A side driven by a solved wave theory.
+static int set_wave_side(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_theory &th) {
+  { const int rs = wave_side_ok(h, w); if (rs) return rs; }
+  if (!(w->period > 0.0) || !(w->depth > 0.0)) return CADMAS_EINVAL;
   cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
   ws.on = true; ws.first = w->first; ws.last = w->last;
   ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
+  ws.theory = true; ws.th = th;
+  { const int rc = wave_cols(ws, std::fabs(ws.angle) > 1.0e-20); if (rc) return rc; }
+  refresh_prm(h);
   return CADMAS_OK;
+}
+
+static bool theory_ok(const cadmas_wave_theory *t) {
+  if (!t || t->type == 0 || t->type < CADMAS_WAVE_STOKES || t->type > CADMAS_STREAM_NMAX) return false;
+  if (t->type >= 1) return t->stream.order == t->type && t->stream.k > 0.0;
+  if (t->type == CADMAS_WAVE_STOKES) return t->stokes.k > 0.0 && t->length > 0.0;
+  return t->cnoidal.ql > 0.0 && t->cnoidal.d > 0.0 && t->length > 0.0;
 }
 
 int cadmas_set_wave_theory(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *sw) {
   if (!h || !w || !sw) return CADMAS_EINVAL;
-  if (w->side < 1 || w->side > 4 || sw->order < 1 || sw->order > CADMAS_STREAM_NMAX) return CADMAS_EINVAL;
-  if (!(w->period > 0.0) || !(w->depth > 0.0) || !(sw->k > 0.0)) return CADMAS_EINVAL;
-  if (h->open[w->side - 1].on) {  // vf_iimdl.f: 'DEFINED DOUBLY.'
-    g_last_error = "side already declared open";
-    return CADMAS_EINVAL;
-  }
-  const int lim = (w->side <= 2) ? h->g.NJ - 1 : h->g.NI - 1;
-  if (w->first < 2 || w->last > lim || w->first > w->last) return CADMAS_EINVAL;
-  cadmas_handle::WaveSide &ws = h->wave[w->side - 1];
-  ws.on = true; ws.first = w->first; ws.last = w->last;
-  ws.d = w->depth; ws.t = w->period; ws.a = w->ramp;
-  ws.theory = true; ws.sw = *sw;
-  return CADMAS_OK;
+  if (sw->order < 1 || sw->order > CADMAS_STREAM_NMAX || !(sw->k > 0.0)) return CADMAS_EINVAL;
+  cadmas_wave_theory th;
+  theory_from_stream(*sw, th);
+  return set_wave_side(h, w, th);
 }
 
-int cadmas_set_wave_source(cadmas_handle *h, const cadmas_wave_src *src, const cadmas_wave_table *t) {
-  if (!h || !src) return CADMAS_EINVAL;
-  const int L = src->line;
-  if (L == 0 || (L > 0 && (L < 2 || L > h->g.NI - 1)) || (L < 0 && (-L < 2 || -L > h->g.NJ - 1)))
-    return CADMAS_EINVAL;  // vf_iimdl.f:119-133
-  if (t) { const int rt = set_table(h, t); if (rt) return rt; }
-  if (h->nzz == 0) { g_last_error = "the wave source needs a matrix table"; return CADMAS_EINVAL; }
-  if (h->mtbtyp == 3) { g_last_error = "(WAVE-SRC) MTBTYP ERROR."; return CADMAS_EINVAL; }  // vf_csetup.f:267
-  if (!(src->period > 0.0) || (h->mtbtyp == 1 && !(src->depth > 0.0))) return CADMAS_EINVAL;
-  const size_t n = (size_t)(L > 0 ? h->g.NJ : h->g.NI) * h->g.NK;
+int cadmas_set_wave_func(cadmas_handle *h, const cadmas_wave_bc *w, const cadmas_wave_theory *t) {
+  if (!h || !w || !theory_ok(t)) return CADMAS_EINVAL;
+  return set_wave_side(h, w, *t);
+}
+
+int cadmas_set_wave_angle(cadmas_handle *h, int side, double angle, double sx, double sy) {
+  if (!h || side < 1 || side > 4 || !std::isfinite(angle) || !std::isfinite(sx) || !std::isfinite(sy))
+    return CADMAS_EINVAL;
+  cadmas_handle::WaveSide &ws = h->wave[side - 1];
+  if (!ws.on || !ws.theory) {  // vf_csetup.f:97-99 (and vf_bwuwn.f:351-356)
+    g_last_error = "(WAVE-BC ANGLE) CAN NOT USE.";
+    return CADMAS_EINVAL;
+  }
+  ws.angle = angle; ws.sx = sx; ws.sy = sy;
+  return wave_cols(ws, std::fabs(angle) > 1.0e-20);
+}
+
+// The line and the SRCUV array of the wave source.
+static int set_source_line(cadmas_handle *h, const cadmas_wave_src *src) {
+  const size_t n = (size_t)(src->line > 0 ? h->g.NJ : h->g.NI) * h->g.NK;
   if (h->srcuv) { cudaFree(h->srcuv); h->srcuv = nullptr; }
   { const int ra = dalloc(&h->srcuv, n); if (ra) return ra; }  // SRCUV = 0 (vf_a1main.f:690)
-  h->src.on = true; h->src.line = L;
+  h->src.on = true; h->src.line = src->line;
   h->src.d = src->depth; h->src.t = src->period; h->src.a = src->ramp;
   refresh_fld(h);
   refresh_prm(h);
   return CADMAS_OK;
+}
+
+static bool source_line_ok(const cadmas_handle *h, int L) {  // vf_iimdl.f:119-133
+  return !(L == 0 || (L > 0 && (L < 2 || L > h->g.NI - 1)) || (L < 0 && (-L < 2 || -L > h->g.NJ - 1)));
+}
+
+int cadmas_set_wave_source(cadmas_handle *h, const cadmas_wave_src *src, const cadmas_wave_table *t) {
+  if (!h || !src) return CADMAS_EINVAL;
+  if (!source_line_ok(h, src->line)) return CADMAS_EINVAL;
+  if (t) { const int rt = set_table(h, t); if (rt) return rt; }
+  if (h->nzz == 0) { g_last_error = "the wave source needs a matrix table"; return CADMAS_EINVAL; }
+  if (h->mtbtyp == 3) { g_last_error = "(WAVE-SRC) MTBTYP ERROR."; return CADMAS_EINVAL; }  // vf_csetup.f:267
+  if (!(src->period > 0.0) || (h->mtbtyp == 1 && !(src->depth > 0.0))) return CADMAS_EINVAL;
+  h->src.theory = false;
+  return set_source_line(h, src);
+}
+
+int cadmas_set_wave_source_func(cadmas_handle *h, const cadmas_wave_src *src, const cadmas_wave_theory *t) {
+  if (!h || !src || !theory_ok(t)) return CADMAS_EINVAL;
+  if (!source_line_ok(h, src->line)) return CADMAS_EINVAL;
+  if (!(src->period > 0.0) || !(src->depth > 0.0)) return CADMAS_EINVAL;
+  h->src.theory = true;
+  h->src.th = *t;
+  return set_source_line(h, src);
 }
 
 int cadmas_open_speed(double depth, double period, double grav, double *c) {
@@ -1311,6 +1440,11 @@ int cadmas_upload_static(cadmas_handle *h, const cadmas_static *st) {
     CK(cudaMemcpyAsync(h->bck, st->bck, nb * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(h->bce, st->bce, nb * sizeof(double), cudaMemcpyHostToDevice, s));
   }
+  // host copies of XX(1,I), YY(1,J) (oblique wave makers)
+  h->xx1.assign(h->g.NI + 2, 0.0);
+  h->yy1.assign(h->g.NJ + 2, 0.0);
+  for (int i = 1; i <= h->g.NI; ++i) h->xx1[i] = st->xx[6 * (i - 1)];
+  for (int j = 1; j <= h->g.NJ; ++j) h->yy1[j] = st->yy[6 * (j - 1)];
   // host copy of ZZ(2,K) for the bubble timers
   h->zz2.assign(h->g.NK + 1, 0.0);
   std::vector<double> zz(6 * h->g.NK);

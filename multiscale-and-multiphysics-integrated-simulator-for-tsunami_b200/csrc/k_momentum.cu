@@ -623,10 +623,11 @@ __global__ void k_bwuwn(Geo g, Fld f, Prm p, int *err) {
 
 // ------------------------------------------------------- VF_CWMSRC
 // The wave source's velocity SRCUV(IJ,K) of every line IJ = 2..NUMIJ-1
-// (vf_cwmsrc.f:100-143) from the matrix table: the column's water level
-// scales the heights (MTBTYP 1), VF_CWMTB2's height interpolation between
-// the rows the host chose (phase weights wt1/wt2 at row mtbnow), times
-// the fade-in AW.  One thread per line.
+// (vf_cwmsrc.f:100-143) from the matrix table or a wave theory: the
+// column's water level scales the heights (a theory, or MTBTYP 1), then
+// VF_CWMTB2's height interpolation between the rows the host chose (phase
+// weights wt1/wt2 at row mtbnow) or the theory's velocity at the phase
+// (VF_CWMAK2), times the fade-in AW.  One thread per line.
 __global__ void k_srcuv(Geo g, Fld f, WaveDev w, double *SRCUV, int *err) {
   const int IJ = 2 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const bool xs = (w.side > 0);  // x source at I = side, y source at J = -side
@@ -657,6 +658,12 @@ __global__ void k_srcuv(Geo g, Fld f, WaveDev w, double *SRCUV, int *err) {
   for (int K = 2; K <= NK - 1; ++K) {
     double ZC = (gz(g, 1, K) + gz(g, 1, K + 1)) * 0.5 - w.wvlvl;
     ZC = VWS * (ZC + w.d) - w.d;
+    if (w.theory) {  // VF_CWMAK2 of the wave theory (wavetheory.cuh)
+      double UN, UT;
+      wt_velocity(w.ph, ZC, UN, UT);
+      SRCUV[(IJ - 1) + (long long)NIJ * (K - 1)] = UN * VWS * w.aw;
+      continue;
+    }
     double W1, W2;
     if (ZC <= w.zz[0]) {
       KM = 1; W1 = 1.0; W2 = 0.0;
@@ -686,10 +693,12 @@ __global__ void k_srcuv(Geo g, Fld f, WaveDev w, double *SRCUV, int *err) {
 }
 
 // ------------------------------------------------- VF_BWUWN, wave maker
-// Wave-maker faces of one side for the matrix-table inflow
-// (vf_bwuwn.f:330-470 with VF_CWMTB2, vf_cwmtb2.f), one thread per
-// boundary line (J on the X sides, I on the Y sides).  The host has done
-// the time part: phase, fade-in AW and VF_CWMTB1's weights and row MTBNOW.
+// Wave-maker faces of one side (vf_bwuwn.f:330-470), one thread per
+// boundary line (J on the X sides, I on the Y sides), from the matrix
+// table (VF_CWMTB2, vf_cwmtb2.f) or a wave theory (VF_CWMAK2).  The host
+// has done the time part: phase, fade-in AW, VF_CWMTB1's weights and row
+// MTBNOW or the theory's level and phase part, one per line under oblique
+// incidence.
 __global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
   const int n = w.first + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (n > w.last) return;
@@ -707,6 +716,9 @@ __global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
     J = (w.side == 3) ? 2 : NJ;
     JC = (w.side == 3) ? 2 : NJ - 1;
   }
+  // oblique incidence: this line's level and phase (vf_bwuwn.f:345-356)
+  const WavePhase &ph = w.col ? w.col[n - w.first].ph : w.ph;
+  const double WVZ = w.col ? w.col[n - w.first].wvz : w.wvz;
   // current water level of the column next to the boundary, scaling
   double VWS;
   if (w.mtbtyp != 1) {
@@ -725,7 +737,7 @@ __global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
       }
     }
     VAL = VAL - (w.wvlvl - gz(g, 1, 2));
-    VWS = (w.wvz + w.d) / (VAL + w.d);
+    VWS = (WVZ + w.d) / (VAL + w.d);
   }
   // boundary values face by face; the height search starts where the face
   // below found its interval
@@ -737,9 +749,9 @@ __global__ void k_wave(Geo g, Fld f, WaveDev w, int *err) {
     if (L < 1) continue;
     double ZC = (gz(g, 1, K) + gz(g, 1, K + 1)) * 0.5 - w.wvlvl;
     ZC = VWS * (ZC + w.d) - w.d;
-    if (w.theory) {  // VF_CWMAK2 of the stream-function wave (wavetheory.cuh)
+    if (w.theory) {  // VF_CWMAK2 of the wave theory (wavetheory.cuh)
       double UN, UT;
-      wt_velocity(w.ph, ZC, UN, UT);
+      wt_velocity(ph, ZC, UN, UT);
       f.bcu[L - 1] = UN * VWS * w.aw * w.sa;
       f.bcv[L - 1] = UN * VWS * w.aw * w.sb;
       f.bcw[L - 1] = UT * VWS * w.aw;

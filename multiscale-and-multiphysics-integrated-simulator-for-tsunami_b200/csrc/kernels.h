@@ -187,12 +187,19 @@ struct WaveDev {
   int mtbtyp, nzz, mtbnow;  // table type, MTBZZ, row MTBNOW (1-based)
   double d, wvz, wt1, wt2, aw, sa, sb, wvlvl;
   const double *zz, *un, *ut;  // device copies of DMTBZZ, DMTBUN, DMTBUT
-  int theory;                  // 1: the stream-function wave of `ph` instead of the table
+  int theory;                  // 1: the wave theory of `ph` instead of the table
   WavePhase ph;
+  const WaveCol *col;          // oblique incidence: level and phase part of
+                               // each line first..last (device), else null
 };
 
-// wavetheory.cu: the series coefficients of a stream-function wave at a
-// phase, and its surface there (single precision, as the reference's)
+// wavetheory.cu: a wave theory's level at a phase (VF_CWMAK1, single
+// precision as the reference's) and the phase's part of its velocities
+// (VF_CWMAK2); the start phase (VF_CWZERO); the stream-function forms
+void theory_phase(const cadmas_wave_theory &t, double wvt, WavePhase &ph);
+double theory_eta(const cadmas_wave_theory &t, double wvt);
+double theory_zero_phase(const cadmas_wave_theory &t);
+void theory_from_stream(const cadmas_stream_wave &s, cadmas_wave_theory &t);
 void stream_phase(const cadmas_stream_wave &s, double wvt, WavePhase &ph);
 double stream_eta(const cadmas_stream_wave &s, double wvt);
 

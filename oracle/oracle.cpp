@@ -405,8 +405,9 @@ struct orc_handle {
   struct Wave {
     int on = 0, l1 = 0, l2 = 0;
     double d = 0, t = 0, a = 0;
-    int theory = 0;             // FUNC STREAM N: the wave `sw`, not the table
-    cadmas_stream_wave sw{};
+    int theory = 0;             // FUNC STREAM N | STOKES | CNOIDAL: the wave `th`, not the table
+    cadmas_wave_theory th{};
+    double ang = 0, sx = 0, sy = 0;  // ANGLE: BCTYP(9..11,JD)
   } WV[4];
   struct Open { int on = 0; double c = 0; } OP[4];  // IBCTYP(1,JD) = 2 and BCTYP(6,JD)
   long long NLOG = 0;  // faces of type 6 or 8 (log-law, rough walls)
@@ -423,6 +424,8 @@ struct orc_handle {
   // line I, < 0 the y line -J), SCTYP(1,3,8) = SD, ST, SA; SRCUV(NUMIJ,NUMK)
   int ISC = 0;
   double SD = 0, ST = 0, SA = 0;
+  int STHEORY = 0;              // ISCTYP(2) a wave theory (the wave STH), not the table
+  cadmas_wave_theory STH{};
   vd SRCUV;
   int IWS() const { return ISC > 0 ? ISC : 0; }
   int JWS() const { return ISC < 0 ? -ISC : 0; }
@@ -1442,7 +1445,7 @@ struct orc_handle {
   }
   static void sw_velocity(const cadmas_stream_wave &s, double wvt, double z, double &u, double &w) {
     const double th = 2.0 * 3.141592653589793 * wvt;
-    double zd = z + s.depth;
+    double zd = (double)(float)z + s.depth;  // REAL(ZC) (vf_cwmak2.f)
     if (zd < 0.0) zd = 0.0;
     double su = s.celerity - s.ubar, sv = 0.0;
     for (int j = 1; j <= s.order; ++j) {
@@ -1458,15 +1461,124 @@ struct orc_handle {
     w = (double)(float)sv;
   }
 
+  // ---- Stokes (fifth order, VF_STK1/2 of vf_wstk0.f) and cnoidal (third
+  // order, VF_CND1/2 of vf_wcnd0.f) at a phase from their coefficients, in
+  // the routines' centimetres: the level sum a_i cos(i theta) or the
+  // polynomial in cn^2; the velocities b0 + sum b_i cosh(i k (z+d))
+  // cos(i theta), sum b_i sinh(...) sin(i theta), or the polynomials in
+  // cn^2 and (1 + z/d)^2 times Z cn sn dn for w.  Jacobi's functions at
+  // u = 4 K x by the arithmetic-geometric mean (Abramowitz and Stegun
+  // 16.4), the moduli from the theta series of the smaller nome.  Heights
+  // enter as REAL(ZC*100), results leave in single precision, times 0.01.
+  static void th_jacobi(double ql, double x, double &cn, double &sn, double &dn) {
+    const double PI = 3.141592653589793;
+    double t2, t3, t4;
+    auto thetas = [&](double q) {
+      double s2 = 0.0, s3 = 0.0, s4 = 0.0;
+      for (int n = 6; n >= 1; --n) {
+        s3 = s3 + std::pow(q, (double)(n * n));
+        s4 = s4 + ((n & 1) ? -1.0 : 1.0) * std::pow(q, (double)(n * n));
+      }
+      for (int n = 6; n >= 0; --n) s2 = s2 + std::pow(q, (double)(n * (n + 1)));
+      t2 = 2.0 * std::pow(q, 0.25) * s2;
+      t3 = 1.0 + 2.0 * s3;
+      t4 = 1.0 + 2.0 * s4;
+    };
+    double k, kp;
+    if (ql >= PI) {
+      thetas(std::exp(-ql));
+      k = (t2 / t3) * (t2 / t3);
+      kp = (t4 / t3) * (t4 / t3);
+    } else {
+      thetas(std::exp(-PI * PI / ql));
+      kp = (t2 / t3) * (t2 / t3);
+      k = (t4 / t3) * (t4 / t3);
+    }
+    double x1 = x - std::floor(x + 0.5), sig = 1.0;
+    if (x1 > 0.25) { x1 = x1 - 0.5; sig = -1.0; }
+    else if (x1 < -0.25) { x1 = x1 + 0.5; sig = -1.0; }
+    std::vector<double> a(1, 1.0), c(1, k);
+    double b = kp;
+    while ((int)a.size() < 47 && std::fabs(c.back()) > 1e-15 * a.back()) {
+      const double an = a.back();
+      a.push_back(0.5 * (an + b));
+      c.push_back(0.5 * (an - b));
+      b = std::sqrt(an * b);
+    }
+    const int N = (int)a.size() - 1;
+    double phi = std::ldexp(2.0 * PI * x1, N), phi1 = phi;
+    for (int m = N; m >= 1; --m) {
+      phi1 = phi;
+      phi = 0.5 * (phi + std::asin(c[m] / a[m] * std::sin(phi)));
+    }
+    sn = sig * std::sin(phi);
+    cn = sig * std::cos(phi);
+    dn = (N == 0) ? 1.0 : std::cos(phi) / std::cos(phi1 - phi);
+  }
+  // VF_CWMAK1  vf_cwmak1.f: the level at phase wvt (m)
+  static double th_level(const cadmas_wave_theory &t, double wvt) {
+    if (t.type >= 1) return sw_level(t.stream, wvt);
+    double zs = 0.0;
+    if (t.type == -2) {
+      const double th = 2.0 * 3.141592653589793 * wvt;
+      for (int i = 1; i <= 5; ++i) zs = zs + t.stokes.a[i - 1] * std::cos((double)i * th);
+    } else {
+      double cn, sn, dn;
+      th_jacobi(t.cnoidal.ql, wvt / 2.0, cn, sn, dn);
+      const double cn2 = cn * cn;
+      for (int L = 4; L >= 1; --L) zs = zs * cn2 + t.cnoidal.a[L - 1];
+    }
+    return (double)(float)zs * 0.01;
+  }
+  // VF_CWMAK2  vf_cwmak2.f: normal and vertical velocity at height z (m/s)
+  static void th_velocity(const cadmas_wave_theory &t, double wvt, double z, double &u, double &w) {
+    if (t.type >= 1) { sw_velocity(t.stream, wvt, z, u, w); return; }
+    const double zt = (double)(float)(z * 100.0);
+    double su, sv;
+    if (t.type == -2) {
+      const double th = 2.0 * 3.141592653589793 * wvt, zd = zt + t.depth * 100.0;
+      su = t.stokes.b0;
+      sv = 0.0;
+      for (int i = 1; i <= 5; ++i) {
+        const double cj = t.stokes.b[i - 1] * std::cos((double)i * th);
+        const double sj = t.stokes.b[i - 1] * std::sin((double)i * th);
+        double ch, sh;
+        sw_chsh((double)i * t.stokes.k * zd, ch, sh);
+        su = su + cj * ch;
+        sv = sv + sj * sh;
+      }
+    } else {
+      double cn, sn, dn;
+      th_jacobi(t.cnoidal.ql, wvt / 2.0, cn, sn, dn);
+      const double cn2 = cn * cn, csd = cn * sn * dn;
+      const double Z = 1.0 + zt / t.cnoidal.d, ZZ = Z * Z;
+      su = 0.0;
+      sv = 0.0;
+      for (int K = 4; K >= 1; --K) {
+        double pu = 0.0, pw = 0.0;
+        for (int L = 3; L >= 1; --L) {
+          pu = pu * ZZ + t.cnoidal.b[(K - 1) * 3 + (L - 1)];
+          pw = pw * ZZ + t.cnoidal.bb[(K - 1) * 3 + (L - 1)];
+        }
+        su = su * cn2 + pu;
+        if (K > 1) sv = sv * cn2 + pw;
+      }
+      sv = sv * csd * Z;
+    }
+    u = (double)(float)su * 0.01;
+    w = (double)(float)sv * 0.01;
+  }
+
   // VF_BWUWN wave-maker part  vf_bwuwn.f:259-470: the matrix-table inflow
-  // (IBCTYP(2,JD) = -3, MTBTYP 1 or 2) or the stream-function wave
-  // (IBCTYP(2,JD) = N >= 1, VF_CWMAK1/VF_CWMAK2); normal incidence, one rank.
+  // (IBCTYP(2,JD) = -3, MTBTYP 1 or 2) or a wave theory (IBCTYP(2,JD) =
+  // N >= 1, -1, -2: VF_CWMAK1/VF_CWMAK2), normal or oblique incidence
+  // (BCTYP(9..11,JD)), one rank.
   int bwuwn_wave() {
     const double PI = 3.141592653589794, ZERO = 1.0e-20;
     for (int JD = 1; JD <= 4; ++JD) {
       const Wave &w = WV[JD - 1];
       if (!w.on) continue;
-      const double D = w.d, T = w.t, T0 = w.theory ? w.sw.phase0 : DMTBT0;
+      const double D = w.d, T = w.t, T0 = w.theory ? w.th.phase0 : DMTBT0;
       double A = w.a;
       float R4TN = (float)(T0 - TNOW / T);
       R4TN = R4TN - (float)(int)R4TN;
@@ -1478,13 +1590,27 @@ struct orc_handle {
       }
       const double WVT = (double)R4TN;
       double WMT1 = 0.0, WMT2 = 0.0, WVZ;
-      if (w.theory) WVZ = sw_level(w.sw, WVT);
+      if (w.theory) WVZ = th_level(w.th, WVT);
       else if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
-      double SA, SB;
-      if (JD == 1) { SA = 1.0; SB = 0.0; }
-      else if (JD == 2) { SA = -1.0; SB = 0.0; }
-      else if (JD == 3) { SA = 0.0; SB = 1.0; }
-      else { SA = 0.0; SB = -1.0; }
+      double SA = w.ang, SB, SC;
+      const int ISA = (std::fabs(SA) <= ZERO) ? 0 : 1;
+      if (ISA == 0) {
+        if (JD == 1) { SA = 1.0; SB = 0.0; }
+        else if (JD == 2) { SA = -1.0; SB = 0.0; }
+        else if (JD == 3) { SA = 0.0; SB = 1.0; }
+        else { SA = 0.0; SB = -1.0; }
+        SC = 0.0;
+      } else {
+        if (!w.theory) return CADMAS_EPG;  // vf_bwuwn.f:351-356
+        if (JD == 2) SA = SA + 180.0;
+        else if (JD == 3) SA = SA + 90.0;
+        else if (JD == 4) SA = SA + 270.0;
+        SA = SA * PI / 180.0;
+        SB = std::sin(SA);
+        SA = std::cos(SA);
+        SC = -(SA * w.sx + SB * w.sy);
+      }
+      const double DL = w.th.length;
       if (!w.theory && MTBTYP == 3) continue;  // vf_bwuwn.f:330: no velocities from a level table
       const int MT = w.theory ? 1 : MTBTYP;
       const bool xs = (JD == 1 || JD == 2);
@@ -1493,6 +1619,17 @@ struct orc_handle {
       for (int n = w.l1; n <= w.l2; ++n) {
         const int I = xs ? I0 : n, J = xs ? n : J0, IC = xs ? IC0 : n, JC = xs ? n : JC0;
         if (xs ? (J < 2 || J > NJ - 1) : (I < 2 || I > NI - 1)) continue;
+        double WVTC = WVT;
+        if (ISA != 0) {  // this line's phase and level (vf_bwuwn.f:345-356, 418-430)
+          const double X0 = xs ? X_(1, I) : (X_(1, I) + X_(1, I + 1)) * 0.5;
+          const double Y0 = xs ? (Y_(1, J) + Y_(1, J + 1)) * 0.5 : Y_(1, J);
+          const double RR = (SA * X0 + SB * Y0 + SC) / std::sqrt(SA * SA + SB * SB);
+          float R4 = (float)(T0 - (TNOW / T - RR / DL));
+          R4 = R4 - (float)(int)R4;
+          if (R4 < 0.0f) R4 = R4 + 1.0f;
+          WVTC = (double)R4;
+          WVZ = th_level(w.th, WVTC);
+        }
         double VWS;
         if (MT != 1) {
           VWS = 1.0;
@@ -1514,7 +1651,7 @@ struct orc_handle {
           double ZC = (Z_(1, K) + Z_(1, K + 1)) * 0.5 - P.wvlvl;
           ZC = VWS * (ZC + D) - D;
           double UN, UT;
-          if (w.theory) sw_velocity(w.sw, WVT, ZC, UN, UT);
+          if (w.theory) th_velocity(w.th, WVTC, ZC, UN, UT);
           else if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
           BCU[L - 1] = UN * VWS * AW * SA;
           BCV[L - 1] = UN * VWS * AW * SB;
@@ -3291,12 +3428,12 @@ struct orc_handle {
     return std::sqrt(v);
   }
 
-  // VF_CWMSRC  vf_cwmsrc.f:46-143 (N = -3, the matrix table) at TDMY =
-  // TNOW: SRCUV of every line of the source
+  // VF_CWMSRC  vf_cwmsrc.f:46-143 (N = -3, the matrix table, or a wave
+  // theory) at TDMY = TNOW: SRCUV of every line of the source
   int cwmsrc() {
     const double PI = 3.141592653589794, ZERO = 1.0e-20;
     const int IJ1 = 2, IJ2 = (ISC > 0 ? NJ : NI) - 1;
-    const double D = SD, T = ST, T0 = DMTBT0;
+    const double D = SD, T = ST, T0 = STHEORY ? STH.phase0 : DMTBT0;
     double A = SA;
     float R4TN = (float)(T0 - TNOW / T);
     R4TN = R4TN - (float)(int)R4TN;
@@ -3307,13 +3444,14 @@ struct orc_handle {
       if (A < 1.0) AW = 0.5 * std::sin(PI * (A - 0.5)) + 0.5;
     }
     const double WVT = (double)R4TN;
-    double WMT1, WMT2, WVZ;
-    if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
+    double WMT1 = 0.0, WMT2 = 0.0, WVZ;
+    if (STHEORY) WVZ = th_level(STH, WVT);
+    else if (!cwmtb1(WVT, WMT1, WMT2, WVZ)) return CADMAS_EPG;
     const int NIJ = ISC > 0 ? NJ : NI;
     for (int IJ = IJ1; IJ <= IJ2; ++IJ) {
       const int I = ISC > 0 ? ISC : IJ, J = ISC > 0 ? IJ : -ISC;
       double VWS;
-      if (MTBTYP == 1) {
+      if (STHEORY || MTBTYP == 1) {
         double VAL = 0.0;
         for (int K = 2; K <= NK - 1; ++K) {
           const int NW = NF[id(I, J, K)];
@@ -3331,7 +3469,8 @@ struct orc_handle {
         double ZC = (Z_(1, K) + Z_(1, K + 1)) * 0.5 - P.wvlvl;
         ZC = VWS * (ZC + D) - D;
         double UN, UT;
-        if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
+        if (STHEORY) th_velocity(STH, WVT, ZC, UN, UT);
+        else if (!cwmtb2(KMT, WMT1, WMT2, ZC, UN, UT)) return CADMAS_EPG;
         SRCUV[(size_t)(IJ - 1) + (size_t)NIJ * (size_t)(K - 1)] = UN * VWS * AW;
       }
     }
@@ -4038,6 +4177,7 @@ int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table
   h->DMTBT0 = t->phase0;
   orc_handle::Wave &v = h->WV[w->side - 1];
   v.on = 1; v.l1 = w->first; v.l2 = w->last; v.d = w->depth; v.t = w->period; v.a = w->ramp;
+  v.theory = 0;
   return CADMAS_OK;
 }
 
@@ -4045,9 +4185,52 @@ int orc_set_wave_theory(orc_handle *h, const cadmas_wave_bc *w, const cadmas_str
   if (!h || !w || !sw || w->side < 1 || w->side > 4 || sw->order < 1 || sw->order > CADMAS_STREAM_NMAX)
     return CADMAS_EINVAL;
   if (h->OP[w->side - 1].on) return CADMAS_EINVAL;
+  cadmas_wave_theory th;
+  std::memset(&th, 0, sizeof(th));
+  th.type = sw->order;
+  th.depth = sw->depth; th.period = sw->period; th.height = sw->height;
+  th.length = (double)(float)sw->length;  // WVLENG = DBLE(R4L) (vf_cwmak0.f:50)
+  th.phase0 = sw->phase0;
+  th.stream = *sw;
+  return orc_set_wave_func(h, w, &th);
+}
+
+int orc_set_wave_func(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_theory *th) {
+  if (!h || !w || !th || w->side < 1 || w->side > 4 || th->type == 0 || th->type < -2 || th->type > CADMAS_STREAM_NMAX)
+    return CADMAS_EINVAL;
+  if (h->OP[w->side - 1].on) return CADMAS_EINVAL;
   orc_handle::Wave &v = h->WV[w->side - 1];
   v.on = 1; v.l1 = w->first; v.l2 = w->last; v.d = w->depth; v.t = w->period; v.a = w->ramp;
-  v.theory = 1; v.sw = *sw;
+  v.theory = 1; v.th = *th;
+  return CADMAS_OK;
+}
+
+// VF_CWMAK1/VF_CWMAK2 of a solved wave theory at one phase and height
+int orc_wave_eval(const cadmas_wave_theory *t, double phase, double z, double *eta, double *u, double *w) {
+  if (!t || t->type == 0 || t->type < -2 || t->type > CADMAS_STREAM_NMAX) return CADMAS_EINVAL;
+  if (eta) *eta = orc_handle::th_level(*t, phase);
+  double uu, ww;
+  orc_handle::th_velocity(*t, phase, z, uu, ww);
+  if (u) *u = uu;
+  if (w) *w = ww;
+  return CADMAS_OK;
+}
+
+int orc_set_wave_angle(orc_handle *h, int side, double angle, double sx, double sy) {
+  if (!h || side < 1 || side > 4 || !h->WV[side - 1].on || !h->WV[side - 1].theory) return CADMAS_EINVAL;
+  orc_handle::Wave &v = h->WV[side - 1];
+  v.ang = angle; v.sx = sx; v.sy = sy;
+  return CADMAS_OK;
+}
+
+int orc_set_wave_source_func(orc_handle *h, const cadmas_wave_src *src, const cadmas_wave_theory *th) {
+  if (!h || !src || src->line == 0 || !th || th->type == 0 || th->type < -2 || th->type > CADMAS_STREAM_NMAX)
+    return CADMAS_EINVAL;
+  h->ISC = src->line;
+  h->SD = src->depth; h->ST = src->period; h->SA = src->ramp;
+  h->STHEORY = 1;
+  h->STH = *th;
+  h->SRCUV.assign((size_t)(src->line > 0 ? h->NJ : h->NI) * h->NK, 0.0);
   return CADMAS_OK;
 }
 
@@ -4064,6 +4247,7 @@ int orc_set_wave_source(orc_handle *h, const cadmas_wave_src *src, const cadmas_
     h->DMTBT0 = t->phase0;
   }
   if (h->DMTBZZ.empty() || h->MTBTYP == 3) return CADMAS_EINVAL;  // vf_csetup.f:267
+  h->STHEORY = 0;
   h->ISC = src->line;
   h->SD = src->depth; h->ST = src->period; h->SA = src->ramp;
   h->SRCUV.assign((size_t)(src->line > 0 ? h->NJ : h->NI) * h->NK, 0.0);

@@ -56,6 +56,10 @@ int orc_get_poisson(orc_handle *h, int which, double *out);
 int orc_set_wave(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_table *t);
 int orc_set_wave_source(orc_handle *h, const cadmas_wave_src *s, const cadmas_wave_table *t);
 int orc_set_wave_theory(orc_handle *h, const cadmas_wave_bc *w, const cadmas_stream_wave *sw);
+int orc_set_wave_func(orc_handle *h, const cadmas_wave_bc *w, const cadmas_wave_theory *th);
+int orc_set_wave_angle(orc_handle *h, int side, double angle, double sx, double sy);
+int orc_wave_eval(const cadmas_wave_theory *t, double phase, double z, double *eta, double *u, double *w);
+int orc_set_wave_source_func(orc_handle *h, const cadmas_wave_src *src, const cadmas_wave_theory *th);
 /* Open (radiation) side JD with the phase speed of depth and period (as
    cadmas_set_open); orc_open_speed is VF_COMAK0's C = L/T. */
 int orc_set_open(orc_handle *h, int side, double depth, double period);

@@ -106,23 +106,36 @@ class Oracle:
             raise RuntimeError("orc_create failed")
         self._static = P.static_of(case)
         self._rc(self.lib.orc_upload_static(self.h, C.byref(self._static)))
-        if getattr(case, "wave", None) and case.wave.get("stream") is not None:
-            wv = case.wave
+        wv = getattr(case, "wave", None)
+        if wv:
             bc = P.WaveBC(int(wv["side"]), int(wv["first"]), int(wv["last"]), 0, float(wv["depth"]),
                           float(wv["period"]), float(wv.get("ramp", 0.0)))
-            self.lib.orc_set_wave_theory.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.StreamWave)]
-            self._rc(self.lib.orc_set_wave_theory(self.h, C.byref(bc), C.byref(wv["stream"])))
-        elif getattr(case, "wave", None):
-            bc, tab, keep = P.wave_structs(case.wave)
-            self.lib.orc_set_wave.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.WaveTable)]
-            self._rc(self.lib.orc_set_wave(self.h, C.byref(bc), C.byref(tab)))
+            if wv.get("theory") is not None:
+                self.lib.orc_set_wave_func.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.WaveTheory)]
+                self._rc(self.lib.orc_set_wave_func(self.h, C.byref(bc), C.byref(wv["theory"])))
+            elif wv.get("stream") is not None:
+                self.lib.orc_set_wave_theory.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.StreamWave)]
+                self._rc(self.lib.orc_set_wave_theory(self.h, C.byref(bc), C.byref(wv["stream"])))
+            else:
+                bc, tab, keep = P.wave_structs(wv)
+                self.lib.orc_set_wave.argtypes = [C.c_void_p, C.POINTER(P.WaveBC), C.POINTER(P.WaveTable)]
+                self._rc(self.lib.orc_set_wave(self.h, C.byref(bc), C.byref(tab)))
+            if wv.get("angle") is not None:
+                a, sx, sy = (float(v) for v in wv["angle"])
+                self.lib.orc_set_wave_angle.argtypes = [C.c_void_p, C.c_int] + [C.c_double] * 3
+                self._rc(self.lib.orc_set_wave_angle(self.h, int(wv["side"]), a, sx, sy))
         for op in getattr(case, "open", None) or []:
             self.lib.orc_set_open.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
             self._rc(self.lib.orc_set_open(self.h, int(op["side"]), float(op["depth"]), float(op["period"])))
         if getattr(case, "source", None):
             ws, tab, keep = P.source_structs(case.source)
-            self.lib.orc_set_wave_source.argtypes = [C.c_void_p, C.POINTER(P.WaveSrc), C.POINTER(P.WaveTable)]
-            self._rc(self.lib.orc_set_wave_source(self.h, C.byref(ws), C.byref(tab) if tab else None))
+            if case.source.get("theory") is not None:
+                self.lib.orc_set_wave_source_func.argtypes = [C.c_void_p, C.POINTER(P.WaveSrc),
+                                                              C.POINTER(P.WaveTheory)]
+                self._rc(self.lib.orc_set_wave_source_func(self.h, C.byref(ws), C.byref(case.source["theory"])))
+            else:
+                self.lib.orc_set_wave_source.argtypes = [C.c_void_p, C.POINTER(P.WaveSrc), C.POINTER(P.WaveTable)]
+                self._rc(self.lib.orc_set_wave_source(self.h, C.byref(ws), C.byref(tab) if tab else None))
         self.set_state(P.initial_state(case))
 
     def _rc(self, rc):
@@ -254,6 +267,20 @@ def fslp(s, d, fval):
     aa, fb = C.c_double(), C.c_double()
     rc = _load_lib().orc_fslp(dim, sa, da, float(fval), C.byref(aa), C.byref(fb))
     return None if rc else (aa.value, fb.value)
+
+
+def wave_eval(th, phase, z=0.0):
+    """(eta, u, w) of a solved wave theory (the package's WaveTheory) by the
+    oracle's restatement of VF_CWMAK1/VF_CWMAK2."""
+    lib = _load_lib()
+    P = _pkg()
+    e, u, w = C.c_double(), C.c_double(), C.c_double()
+    dp = C.POINTER(C.c_double)
+    lib.orc_wave_eval.argtypes = [C.POINTER(P.WaveTheory), C.c_double, C.c_double, dp, dp, dp]
+    rc = lib.orc_wave_eval(C.byref(th), float(phase), float(z), C.byref(e), C.byref(u), C.byref(w))
+    if rc != 0:
+        raise P.CadmasError(rc, f"oracle status {rc}")
+    return e.value, u.value, w.value
 
 
 def open_speed(depth, period, grav=9.8):

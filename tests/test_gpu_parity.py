@@ -487,3 +487,50 @@ def test_stream_function_wave_maker_bitwise(gpu_lib, pkg, orc, order):
     pkg.cases.wave_maker(c, 0.08, 1.5, 0.5, ramp=0.5, stream=order)
     t, o = run_pair(pkg, orc, c, 30, check_every=10)
     assert np.abs(t.get_state()["uu"][1, :, :]).max() > 2e-4  # the wave maker drives the inflow (faded in)
+
+
+@pytest.mark.parametrize("func,H,T,ramp", [("stokes", 0.08, 1.5, 0.5), ("cnoidal", 0.05, 4.0, 0.05),
+                                            ("stk-cnd", 0.05, 4.0, 0.05)])
+def test_stokes_cnoidal_wave_maker_bitwise(gpu_lib, pkg, orc, func, H, T, ramp):
+    """The wave maker driven by the fifth-order Stokes or the third-order
+    cnoidal wave (WAVE-BC ... FUNC STOKES | CNOIDAL | STK-CND, the last
+    choosing cnoidal at an Ursell number of 31): the level at the phase and
+    the phase's part of the series on the host, the face velocities in
+    k_wave; bit for bit with the oracle's evaluation of the same wave."""
+    c = pkg.cases.porous_flume(nx=96, ny=4, nz=64, block=(1.2, 1.4, 0.6), sponge_width=0.4)
+    pkg.cases.wave_maker(c, H, T, 0.5, ramp=ramp, func=func)
+    assert c.wave["theory"].type == (pkg.WAVE_STOKES if func == "stokes" else pkg.WAVE_CNOIDAL)
+    t, o = run_pair(pkg, orc, c, 30, check_every=10)
+    assert np.abs(t.get_state()["uu"][1, :, :]).max() > 2e-4  # the wave maker drives the inflow (faded in)
+
+
+@pytest.mark.parametrize("func,side,angle", [(5, 1, (25.0, 0.3, 0.2)), ("stokes", 3, (-30.0, 0.1, 0.4)),
+                                             ("cnoidal", 2, (15.0, 0.0, 0.0))])
+def test_oblique_wave_maker_bitwise(gpu_lib, pkg, orc, func, side, angle):
+    """Oblique incidence (WAVE-BC ... ANGLE a X Y) on an X side and a Y
+    side: each line's phase from its distance along the direction of
+    travel, its own level and velocities (the table of lines uploaded each
+    step), the normal and tangential parts of the face velocity; bit for
+    bit with the oracle."""
+    c = pkg.cases.porous_flume(nx=48, ny=24, nz=64, block=(0.6, 0.7, 0.3), sponge_width=0.3)
+    kw = dict(stream=func) if isinstance(func, int) else dict(func=func)
+    H, T, ramp = (0.05, 4.0, 0.02) if func == "cnoidal" else (0.06, 1.5, 0.2)
+    pkg.cases.wave_maker(c, H, T, 0.5, side=side, ramp=ramp, angle=angle, **kw)
+    t, o = run_pair(pkg, orc, c, 20, check_every=10, precond_ti=16, precond_tj=8)
+    st = t.get_state()
+    if side <= 2:
+        I = 1 if side == 1 else c.ni - 1
+        face = st["uu"][I, 1:-1, 10]  # below the still water level, along the side
+    else:
+        face = st["vv"][1:-1, 1, 10]
+    assert np.ptp(face) > 1e-5  # the phase varies along the side
+
+
+@pytest.mark.parametrize("func", [3, "stokes"])
+def test_wave_source_with_a_theory_bitwise(gpu_lib, pkg, orc, func):
+    """A wave source line driven by a wave theory (WAVE-SRC ... FUNC STREAM
+    N | STOKES): SRCUV from VF_CWMAK2 at the heights scaled to each
+    column's level in k_srcuv; bit for bit with the oracle."""
+    c = pkg.cases.source_flume(nx=64, nz=32, ramp=0.2, func=func)
+    t, o = run_pair(pkg, orc, c, 40, check_every=10)
+    assert np.abs(t.get_state()["ww"]).max() > 1e-3  # the source moves the water
