@@ -111,7 +111,7 @@ def params_for(args):
                 solver=1 if getattr(args, "solver", "fp64") == "mixed" else 0,
                 warm_start={"zero": 0, "previous": 1, "learned": 2}[getattr(args, "guess", "zero")],
                 mixed_eps_inner=getattr(args, "eps_inner", 1.0e-5),
-                sweep_occupancy=getattr(args, "occ", 0))
+                sweep_occupancy=getattr(args, "occ", 0), dot_passes=getattr(args, "dot_passes", 0))
 
 
 class ClockSampler:
@@ -905,6 +905,8 @@ def main():
                     help="floor of the FP32 inner tolerance of the mixed solver")
     ap.add_argument("--occ", type=int, choices=[0, 1, 2], default=0,
                     help="thread blocks of the MILU sweeps per SM (0: the library's default)")
+    ap.add_argument("--dot-passes", type=int, choices=[0, 1], default=0,
+                    help="mixed solver: 0 inner products summed by the backward sweeps, 1 separate passes")
     ap.add_argument("--beach-nx", type=int, default=1024)
     ap.add_argument("--beach-ny", type=int, default=128)
     ap.add_argument("--beach-nz", type=int, default=128)

@@ -51,7 +51,7 @@ module cadmas_gpu
      real(c_double) :: akk0, aka0                ! log law (IB 6, 8)
      real(c_double) :: mixed_eps_inner           ! floor of the FP32 inner tolerance (solver 1)
      real(c_double) :: wait_limit_s              ! device-side wait limit, seconds
-     integer(c_int) :: sweep_occupancy, pad1     ! MILU sweep blocks per SM (0 = default)
+     integer(c_int) :: sweep_occupancy, dot_passes  ! MILU sweep blocks per SM (0 = default); FP32 sums in the sweeps (0)
   end type cadmas_params
 
   ! c_loc() of the static arrays (XX(6,NUMI) ... INDB(4,NUMB))

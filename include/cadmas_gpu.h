@@ -166,7 +166,13 @@ typedef struct cadmas_params {
      has at least two preconditioner blocks per SM, one otherwise.  The
      results do not depend on it.                                         */
   int    sweep_occupancy;
-  int    pad1;
+  /* Inner products of the mixed solver's FP32 iteration (solver 1; no
+     counterpart in the reference): 0 = summed by the backward MILU sweeps
+     that produce AP and AE, one partial per preconditioner block, where
+     the layout allows (one layout tile per block, at most 512 columns);
+     1 = by passes of their own after the sweeps.  The two differ only in
+     the order of the double-precision sums of exact products.            */
+  int    dot_passes;
 } cadmas_params;
 
 /* ---- static fields (set once; host pointers) ---------------------------- */

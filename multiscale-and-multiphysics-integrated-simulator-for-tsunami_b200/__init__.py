@@ -174,7 +174,7 @@ class Params(C.Structure):
         (n, C.c_double) for n in ("anu0", "scmk", "akmink", "akmine", "akinik", "akinie", "akcmu", "aksgk",
                                   "aksge", "akc1", "akc2", "akc3", "akk0", "aka0",
                                   "mixed_eps_inner", "wait_limit_s")] + [
-        ("sweep_occupancy", C.c_int), ("pad1", C.c_int)]
+        ("sweep_occupancy", C.c_int), ("dot_passes", C.c_int)]
 
 
 class Static(C.Structure):

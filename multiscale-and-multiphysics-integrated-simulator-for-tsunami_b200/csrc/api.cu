@@ -558,6 +558,7 @@ static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
   const double epsa2 = h->P.cgepsa * h->P.cgepsa, epsr2 = eps * eps, div2 = h->P.cgdiv * h->P.cgdiv;
   const int icgmax = h->P.icgmax;
   const size_t vb = h->nsl * sizeof(float);
+  const bool fused_dots = h->P.dot_passes == 0;
   float *zl[] = {h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef};
   for (float *z : zl) CK(cudaMemsetAsync(z, 0, vb, s));
   CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
@@ -573,21 +574,29 @@ static int solve_inner_f(cadmas_handle *h, double eps, int &iter) {
   int batch = std::max(2, std::min(h->last_iter, 64));
   for (int guard = 0; guard < 100000; ++guard) {
     for (int b = 0; b < batch; ++b) {
-      // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP
+      // AP = MINV*(A*PP); ALPHA = S/(R0,AP); RR -= ALPHA*AP.  (R0,AP) is
+      // summed by the backward sweep itself where the layout allows
+      // (one partial per tile), else by its own pass.
       TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->pvf, st, h->y2f); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->apf, st); TE();
+      TB(CADMAS_STAGE_BWD);
+      const bool d1 = fused_dots && launch_bwd_f_dot1(s, g, q, S, h->r0f, h->apf, h->rb0, st);
+      if (!d1) launch_bwd_f(s, g, q, S, h->apf, st);
+      TE();
       TB(CADMAS_STAGE_DOT);
-      launch_dot2f(s, q, h->r0f, h->apf, h->rb0, st);
-      launch_fin(s, FIN_ALPHA, h->rb0, nullptr, nr, st, nullptr, epsa2, epsr2, div2, icgmax);
+      if (!d1) launch_dot2f(s, q, h->r0f, h->apf, h->rb0, st);
+      launch_fin(s, FIN_ALPHA, h->rb0, nullptr, d1 ? (long long)q.nb : nr, st, nullptr, epsa2, epsr2, div2, icgmax);
       TE();
       TB(CADMAS_STAGE_VEC); launch_axpyf(s, q, h->apf, h->rrf, st); TE();
       // AE = MINV*(A*RR); the five sums; OMEGA, convergence, BETA; XW,
       // RR and PP in one pass
       TB(CADMAS_STAGE_FWD); launch_fwd_f(s, g, q, S, nullptr, h->rrf, st, h->y2f); TE();
-      TB(CADMAS_STAGE_BWD); launch_bwd_f(s, g, q, S, h->aef, st); TE();
+      TB(CADMAS_STAGE_BWD);
+      const bool d5 = fused_dots && launch_bwd_f_dot5(s, g, q, S, h->r0f, h->rrf, h->aef, h->rb5, st);
+      if (!d5) launch_bwd_f(s, g, q, S, h->aef, st);
+      TE();
       TB(CADMAS_STAGE_DOT);
-      launch_dot5f(s, q, h->r0f, h->rrf, h->aef, h->rb5, st);
-      launch_fin5(s, h->rb5, nr, st, epsa2, epsr2, div2, icgmax);
+      if (!d5) launch_dot5f(s, q, h->r0f, h->rrf, h->aef, h->rb5, st);
+      launch_fin5(s, h->rb5, d5 ? (long long)q.nb : nr, st, epsa2, epsr2, div2, icgmax);
       TE();
       TB(CADMAS_STAGE_VEC);
       launch_upd3f(s, q, h->aef, h->apf, h->xf, h->rrf, h->pvf, st);
@@ -633,7 +642,12 @@ static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int 
   TE();
   CK(cudaMemcpyAsync(h->h_st, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  if (h->h_st->pivot_bad) { h->mixed_fallback++; return solve(h, a, x0, indc, iter, bnorm, xnorm); }
+  // FP64 takes over
+  auto fallback = [&]() {
+    h->mixed_fallback++;
+    return solve(h, a, x0, indc, iter, bnorm, xnorm);
+  };
+  if (h->h_st->pivot_bad) return fallback();
   const double tol2 = h->P.cgepsr * h->P.cgepsr;
   int total = 0;
   bool converged = false;
@@ -666,17 +680,11 @@ static int solve_mixed(cadmas_handle *h, const SysPtr &a, double *x0, const int 
     int it = 0;
     int rc = solve_inner_f(h, eps_in, it);
     if (rc) return rc;
-    if (it < 0 || it > h->P.icgmax) {  // factor, divergence or cap: FP64 takes over
-      h->mixed_fallback++;
-      return solve(h, a, x0, indc, iter, bnorm, xnorm);
-    }
+    if (it < 0 || it > h->P.icgmax) return fallback();  // factor, divergence or cap
     total += it;
     launch_add_f(s, q, ic, h->xf, rn, h->xw);
   }
-  if (!converged) {
-    h->mixed_fallback++;
-    return solve(h, a, x0, indc, iter, bnorm, xnorm);
-  }
+  if (!converged) return fallback();
   // X0 = XW on INDC != -1 (k_x0 requires ITER >= 0: the state is clear)
   CK(cudaMemsetAsync(st, 0, SOLVE_CLEAR_BYTES, s));
   launch_x0(s, g, q, ic, h->xw, x0, st);

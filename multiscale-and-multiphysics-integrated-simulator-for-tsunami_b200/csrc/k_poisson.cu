@@ -502,7 +502,9 @@ __device__ __forceinline__ void cluster_barrier() {
 // slot addresses and mbarrier phases are constants.
 template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1>
 __global__ void __launch_bounds__(MAXT, MINB)
-    k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st) {
+    k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st, const V *vin2, double *rb) {
+  constexpr bool BWD = MODE >= SWEEP_BWD;
+  constexpr int NDOT = sweep_ndot(MODE);
   pdl_enter();
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
   // preconditioner block; every block of a cluster runs through the two
@@ -550,12 +552,12 @@ __global__ void __launch_bounds__(MAXT, MINB)
   const int nty = q.nb / q.ntx;
   const bool has_up = CS == 2 && crank == 0 && (int)blockIdx.y + 1 < nty;
   const bool has_lo = CS == 2 && crank == 1;
-  const bool recv = (MODE == SWEEP_BWD) ? has_up : has_lo;
-  const bool send = (MODE == SWEEP_BWD) ? has_lo : has_up;
-  const bool srow = send && ((MODE == SWEEP_BWD) ? t.tj == 0 : t.tj == q.TJ - 1) && !producer;
-  const bool rrow = recv && ((MODE == SWEEP_BWD) ? t.tj == t.wj - 1 : t.tj == 0) && !producer;
+  const bool recv = BWD ? has_up : has_lo;
+  const bool send = BWD ? has_lo : has_up;
+  const bool srow = send && (BWD ? t.tj == 0 : t.tj == q.TJ - 1) && !producer;
+  const bool rrow = recv && (BWD ? t.tj == t.wj - 1 : t.tj == 0) && !producer;
   // receiver's step lag: rows of the sending tile minus one
-  const int lag = (MODE == SWEEP_BWD) ? min(q.TJ, g.NJ - (2 + ((int)blockIdx.y + 1) * q.TJ)) - 1 : q.TJ - 1;
+  const int lag = BWD ? min(q.TJ, g.NJ - (2 + ((int)blockIdx.y + 1) * q.TJ)) - 1 : q.TJ - 1;
   unsigned r_xin = 0, r_din = 0, r_full = 0;            // the partner's xin, din, xfull
   if (CS == 2 && send) {
     const unsigned peer = cluster_rank() ^ 1u;
@@ -573,7 +575,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     s_abort[0] = s_abort[1] = 0;
   }
   if (CS == 2 && recv) {
-    const unsigned row_bytes = (unsigned)(TIp * ES * (MODE == SWEEP_BWD ? 1 : 2));
+    const unsigned row_bytes = (unsigned)(TIp * ES * (BWD ? 1 : 2));
     for (int u = tid; u < NX; u += blockDim.x) {
       mbar_init(smem_u32(xfull + u), 1u);
       mbar_expect_tx(smem_u32(xfull + u), row_bytes);
@@ -595,13 +597,13 @@ __global__ void __launch_bounds__(MAXT, MINB)
   SweepLane l0;
   l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; l0.dst = 0; l0.wstride = 0;  // empty range: no copy
   if (producer && lane < sweep_ncopy(q, MODE) && sweep_lane(q, MODE, b, lane, l0, ES))
-    src0 = (l0.arr == 0 ? S.sys : vin) + l0.base;
+    src0 = (l0.arr == 0 ? S.sys : (l0.arr == 1 ? vin : vin2)) + l0.base;
   else { l0.dlo = 1; l0.dhi = 0; l0.bytes = 0; }
   const unsigned bar0 = smem_u32(bar), ring0 = smem_u32(ring);
   const int stall_from = producer ? st->stall_from : 0;  // read by the producer warp only
   auto issue = [&](int u, int slot) {
     if (u >= nsteps || u >= stall_from) return;
-    const int w = (MODE == SWEEP_BWD) ? nsteps - 1 - u : u;
+    const int w = BWD ? nsteps - 1 - u : u;
     const unsigned bslot = bar0 + 8u * slot;
     const unsigned dslot = ring0 + (unsigned)ES * (unsigned)(slot * SS);
     const bool v0 = (w >= l0.dlo && w <= l0.dhi);
@@ -623,14 +625,14 @@ __global__ void __launch_bounds__(MAXT, MINB)
   // Column geometry: active steps slo..shi (k inside 2..NK-1).
   const int ri = t.wi - 1 - t.ti, rj = t.wj - 1 - t.tj;
   const bool ex0 = (t.ti == 0), ex1 = (t.ti == t.wi - 1), ey0 = (t.tj == 0), ey1 = (t.tj == t.wj - 1);
-  const int slo = (MODE == SWEEP_BWD) ? ri + rj : t.ti + t.tj, shi = slo + g.NK - 3;
+  const int slo = BWD ? ri + rj : t.ti + t.tj, shi = slo + g.NK - 3;
   const bool col = t.valid && !producer;
   const int hl = halo_left(q, ES) + TIp * t.tj + halo_lofs(q, ES), hr = halo_right(q, ES) + TIp * t.tj,
             hd = halo_down(q, ES) + t.ti, hu = halo_up(q, ES) + t.ti;
   // forward: T into the system block; backward: X
-  V *vp = (MODE == SWEEP_BWD) ? vout + ((long long)b * q.W + nsteps - 1) * T + tid
+  V *vp = BWD ? vout + ((long long)b * q.W + nsteps - 1) * T + tid
                               : S.sys + sys_at((long long)b * q.W, SYS_T, T, tid);
-  const long long vstep = (MODE == SWEEP_BWD) ? -(long long)T : (long long)SYS_N * T;
+  const long long vstep = BWD ? -(long long)T : (long long)SYS_N * T;
 
   // Prepared values of the next step.
   bool act = false;             // the column has a cell at this step
@@ -639,6 +641,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
   V c1 = V(0), c2 = V(0), c3 = V(0);  // FWD: ALI*DD(i-1), ALJ*DD(j-1), ALK*DD(k-1); BWD: AUI, AUJ, AUK
   V dk1 = V(0), pk1 = V(0);  // DD and P of this column at the previous step (FWD)
   V xk1 = V(0);             // result of this column at the previous step
+  V q0 = V(0), q1 = V(0);   // NDOT: R0 and RR of the cell
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;  // NDOT: this column's sums
   // Prepare step s: cs = slot of s, ps = slot of s-1, ns = slot of s+1.
   auto prepare = [&](int s, const V *cs, const V *ps, const V *ns) {
     act = col && s >= slo && s <= shi;
@@ -676,6 +680,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
     } else {
       dd = cs[oDD + tid];
       if (dd != V(0)) { y0 = cs[tid]; c1 = cs[oAUI + tid]; c2 = cs[oAUJ + tid]; c3 = cs[oAUK + tid]; }
+      if (NDOT > 0) q0 = cs[5 * T + tid];
+      if (NDOT == 5) q1 = cs[6 * T + tid];
     }
   };
   auto slot_ptr = [&](int r) -> const V * { return ring + (size_t)r * SS; };
@@ -712,7 +718,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
           V x = V(0);
           if (dd != V(0)) {
             const V xr = rrow ? xin[(size_t)(s + lag) * TIp + t.ti] : V(0);  // partner tile's row
-            if (MODE == SWEEP_BWD) {
+            if (BWD) {
               const V x1 = (ri > 0) ? xb[prv + tid + 1] : V(0);
               const V x2 = (rj > 0) ? xb[prv + tid + TIp] : xr;
               x = (y0 - c1 * x1 - c2 * x2 - c3 * xk1) * dd;
@@ -726,12 +732,22 @@ __global__ void __launch_bounds__(MAXT, MINB)
           *vp = x;
           xk1 = x;
           xcur = x;
+          // products of two single-precision values are exact in double
+          if (NDOT == 1) a0 += (double)q0 * (double)x;
+          if (NDOT == 5) {
+            const double r = (double)q1, e = (double)x, z = (double)q0;
+            a0 += r * e;
+            a1 += e * e;
+            a2 += r * r;
+            a3 += z * r;
+            a4 += z * e;
+          }
         }
         vp += vstep;
         if (CS == 2 && srow) {  // this step's boundary-row values to the partner tile
           const unsigned off = (unsigned)(((size_t)s * TIp + t.ti) * ES), fb = r_full + 8u * (unsigned)s;
           st_async(r_xin + off, xcur, fb);
-          if (MODE != SWEEP_BWD) st_async(r_din + off, act ? dd : V(0), fb);
+          if (!BWD) st_async(r_din + off, act ? dd : V(0), fb);
         }
         // prepare step s+1
         if (!ready) {
@@ -756,6 +772,30 @@ __global__ void __launch_bounds__(MAXT, MINB)
       for (int u = max(0, issued - R + 1); u <= issued; ++u)
         mbar_wait_slow(bar0 + 8u * (u % R), (unsigned)((u / R) & 1), 100000000ull);
     if (lane == 0) { st->timeout = 1; st->done = 1; }
+  }
+  if (NDOT > 0) {
+    // the tile's sums: warps by a butterfly, then the warps' partials by
+    // warp 0, in a fixed order; one partial per tile into rb[c*nb + b]
+    __shared__ double s_red[5][32];
+    double a[5] = {a0, a1, a2, a3, a4};
+#pragma unroll
+    for (int c = 0; c < NDOT; ++c) {
+      double v = a[c];
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) s_red[c][tid >> 5] = v;
+    }
+    __syncthreads();
+    if (tid < 32) {
+      const int nw = (int)(blockDim.x >> 5);
+#pragma unroll
+      for (int c = 0; c < NDOT; ++c) {
+        double v = (tid < nw) ? s_red[c][tid] : 0.0;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (tid == 0) rb[(long long)c * q.nb + b] = v;
+      }
+    }
   }
   if (CS == 2) cluster_barrier();  // the partner may still write into this block's shared memory
 }
@@ -1322,7 +1362,7 @@ static size_t sweep_bytes(const SkewGeo &q, int mode, int D, int es) {
   const int R = D + 2;
   size_t b = (size_t)((R + 1) & ~1) * 8 + (size_t)R * sweep_slot(q, mode, es) * es + 2 * (size_t)q.T * es;
   if (q.split == 2)  // cluster exchange: xfull[W] barriers, xin (and din) [W][TIp]
-    b += (size_t)q.W * 8 + (size_t)q.W * q.TIp * es * (mode == SWEEP_BWD ? 1 : 2);
+    b += (size_t)q.W * 8 + (size_t)q.W * q.TIp * es * (mode >= SWEEP_BWD ? 1 : 2);
   return b;
 }
 static int sweep_depth(const SkewGeo &q, int mode, int es) {
@@ -1338,11 +1378,12 @@ static int sweep_depth(const SkewGeo &q, int mode, int es) {
 // leaves room for the second block's (228 KB per SM, 1 KB reserved per
 // block).  Two tiles' wavefronts then interleave on every SM.
 // The register cap (96 for two 288-thread blocks) makes deeper rings
-// spill: depths up to 3 (fused forward sweep) or 4 (the others) are used.
+// spill: depths up to 3 (fused forward sweep, backward sweep with five
+// sums) or 4 (the others) are used.
 constexpr int SWEEP2_THREADS = 288;
 static int sweep_depth2(const SkewGeo &q, int mode, int es) {
   if (q.split != 1 || sweep_threads(q.T) > SWEEP2_THREADS) return 0;
-  const int dmax = mode == SWEEP_FWD_AX ? 3 : 4;
+  const int dmax = (mode == SWEEP_FWD_AX || mode == SWEEP_BWD5) ? 3 : 4;
   for (int d : {4, 3, 2})
     if (d <= dmax && sweep_bytes(q, mode, d, es) <= 113 * 1024) return d;
   return 0;
@@ -1351,6 +1392,8 @@ template <int MODE, typename V>
 static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *vin,
                          V *vout, SolveState *st) {
   constexpr int ES = (int)sizeof(V);
+  const V *vnull = nullptr;
+  double *rnull = nullptr;
   const int d = sweep_depth(q, MODE, ES);
   const size_t bytes = sweep_bytes(q, MODE, d, ES);
   const int nty = q.nb / q.ntx;
@@ -1366,7 +1409,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
 #define SWEEP_CASE2(DD, MT)                                                             \
   case DD * 4096 + MT:                                                                  \
     set_smem(k_sweep<DD, MODE, MT, V, 2>, bytes);                                       \
-    launch_pdl(k_sweep<DD, MODE, MT, V, 2>, grid, block, bytes, s, 2, g, q, S, vin, vout, st); \
+    launch_pdl(k_sweep<DD, MODE, MT, V, 2>, grid, block, bytes, s, 2, g, q, S, vin, vout, st, vnull, rnull); \
     break;
       SWEEP_CASE2(8, 256) SWEEP_CASE2(4, 256) SWEEP_CASE2(2, 256)
       SWEEP_CASE2(8, 512) SWEEP_CASE2(4, 512) SWEEP_CASE2(2, 512)
@@ -1380,7 +1423,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   // the sweeps' per-step latency, not the bandwidth, sets the time and a
   // second tile's wavefront fills it.  The fused FP64 forward sweep keeps
   // one block: its ring of 8 arrays needs the depth and registers.
-  const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm && (ES == 4 || MODE == SWEEP_BWD));
+  const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm && (ES == 4 || MODE >= SWEEP_BWD));
   if (two) {
     const int d2 = sweep_depth2(q, MODE, ES);
     if (d2 > 0) {
@@ -1389,7 +1432,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
 #define SWEEP_CASE_OCC2(DD)                                                                            \
   case DD:                                                                                             \
     set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, bytes2);                                      \
-    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, grid, block, bytes2, s, 1, g, q, S, vin, vout, st); \
+    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, grid, block, bytes2, s, 1, g, q, S, vin, vout, st, vnull, rnull); \
     return;
         SWEEP_CASE_OCC2(4) SWEEP_CASE_OCC2(3) SWEEP_CASE_OCC2(2)
 #undef SWEEP_CASE_OCC2
@@ -1401,7 +1444,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
 #define SWEEP_CASE(DD, MT)                                                              \
   case DD * 4096 + MT:                                                                  \
     set_smem(k_sweep<DD, MODE, MT, V, 1>, bytes);                                       \
-    launch_pdl(k_sweep<DD, MODE, MT, V, 1>, grid, block, bytes, s, 1, g, q, S, vin, vout, st); \
+    launch_pdl(k_sweep<DD, MODE, MT, V, 1>, grid, block, bytes, s, 1, g, q, S, vin, vout, st, vnull, rnull); \
     break;
     SWEEP_CASE(8, 256) SWEEP_CASE(6, 256) SWEEP_CASE(4, 256) SWEEP_CASE(3, 256) SWEEP_CASE(2, 256)
     SWEEP_CASE(8, 512) SWEEP_CASE(6, 512) SWEEP_CASE(4, 512) SWEEP_CASE(3, 512) SWEEP_CASE(2, 512)
@@ -1445,6 +1488,55 @@ void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S
 }
 void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, float *x, SolveState *st) {
   launch_sweep<SWEEP_BWD, float>(s, g, q, S, nullptr, x, st);
+}
+// The FP32 backward sweep with the inner products that follow it summed
+// on the way (mode 3: (R0,X); mode 4: the five sums of k_dot5f), one
+// partial per tile into rb (rb + c*nb for sum c).  Ring depths 2..4, one
+// layout tile per preconditioner block, blocks of up to 512 threads;
+// false (nothing launched) where that does not hold.
+template <int MODE>
+static bool launch_bwd_dots(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *r0,
+                            const float *rr, float *x, double *rb, SolveState *st) {
+  constexpr int ES = 4;
+  if (q.split != 1) return false;
+  const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
+  const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm);
+  if (two) {
+    const int d2 = sweep_depth2(q, MODE, ES);
+    const size_t bytes2 = sweep_bytes(q, MODE, d2, ES);
+    switch (d2) {
+#define DOTS_OCC2(DD)                                                                                              \
+  case DD:                                                                                                         \
+    set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, bytes2);                                              \
+    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, grid, block, bytes2, s, 1, g, q, S, r0, x, st, rr, rb); \
+    return true;
+      DOTS_OCC2(4) DOTS_OCC2(3) DOTS_OCC2(2)
+#undef DOTS_OCC2
+      default: break;
+    }
+  }
+  const int d = std::min(sweep_depth(q, MODE, ES), 4), nt = sweep_threads(q.T);
+  const int mt = nt <= 256 ? 256 : (nt <= 512 ? 512 : 0);
+  if (mt == 0 || d < 2) return false;
+  const size_t bytes = sweep_bytes(q, MODE, d, ES);
+  switch (d * 4096 + mt) {
+#define DOTS_CASE(DD, MT)                                                                            \
+  case DD * 4096 + MT:                                                                               \
+    set_smem(k_sweep<DD, MODE, MT, float, 1>, bytes);                                                \
+    launch_pdl(k_sweep<DD, MODE, MT, float, 1>, grid, block, bytes, s, 1, g, q, S, r0, x, st, rr, rb); \
+    return true;
+    DOTS_CASE(4, 256) DOTS_CASE(3, 256) DOTS_CASE(2, 256) DOTS_CASE(4, 512) DOTS_CASE(3, 512) DOTS_CASE(2, 512)
+#undef DOTS_CASE
+    default: return false;
+  }
+}
+bool launch_bwd_f_dot1(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *r0, float *x,
+                       double *rb, SolveState *st) {
+  return launch_bwd_dots<SWEEP_BWD1>(s, g, q, S, r0, nullptr, x, rb, st);
+}
+bool launch_bwd_f_dot5(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *r0,
+                       const float *rr, float *x, double *rb, SolveState *st) {
+  return launch_bwd_dots<SWEEP_BWD5>(s, g, q, S, r0, rr, x, rb, st);
 }
 static inline unsigned slab_blocks(const SkewGeo &q) {
   return (unsigned)(((long long)q.nb * q.W + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK);

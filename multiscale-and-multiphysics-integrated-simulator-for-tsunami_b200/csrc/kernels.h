@@ -64,19 +64,29 @@ __host__ __device__ inline long long sys_at(long long slab, int c, int T, int t)
 //         that of row TJ-1), copies: system arrays AUI..ALK, P, down, up,
 //         left, right;
 // MODE 2: backward sweep: {T, AUI, AUJ, AUK, DD}, copy: system arrays
-//         T..DD.
+//         T..DD;
+// MODE 3, 4: backward sweep that also sums products of its result with
+//         given vectors (the BiCGSTAB inner products that follow it):
+//         {T, AUI, AUJ, AUK, DD, R0} and {T, AUI, AUJ, AUK, DD, R0, RR},
+//         copies: system arrays T..DD, R0 (and RR).
 // Offsets are in elements of the sweep's type (es bytes: 8 for double, 4
-// for float); `arr` 0 is the interleaved system, 1 the vector.
-enum SweepMode { SWEEP_FWD = 0, SWEEP_FWD_AX = 1, SWEEP_BWD = 2 };
+// for float); `arr` 0 is the interleaved system, 1 the vector (R0 in
+// modes 3 and 4), 2 the second vector (RR in mode 4).
+enum SweepMode { SWEEP_FWD = 0, SWEEP_FWD_AX = 1, SWEEP_BWD = 2, SWEEP_BWD1 = 3, SWEEP_BWD5 = 4 };
+// inner products a backward sweep sums (mode 3: (R0,X); mode 4: (RR,X),
+// (X,X), (RR,RR), (R0,RR), (R0,X))
+__host__ __device__ constexpr int sweep_ndot(int mode) {
+  return mode == SWEEP_BWD1 ? 1 : (mode == SWEEP_BWD5 ? 5 : 0);
+}
 struct SweepCopy {
   long long src;
   int dst, bytes, arr;
 };
 __host__ __device__ inline int sweep_nv(int mode) {
-  return mode == SWEEP_FWD_AX ? 9 : (mode == SWEEP_FWD ? 6 : 5);
+  return mode == SWEEP_FWD_AX ? 9 : (mode == SWEEP_FWD ? 6 : 5 + (mode - SWEEP_BWD));
 }
 __host__ __device__ inline int sweep_ncopy(const SkewGeo &, int mode) {
-  return mode == SWEEP_FWD_AX ? 6 : (mode == SWEEP_FWD ? 2 : 1);
+  return mode == SWEEP_FWD_AX ? 6 : (mode == SWEEP_FWD ? 2 : 1 + (mode - SWEEP_BWD));
 }
 // First system array of a mode's slot and its position there.
 __host__ __device__ constexpr int sweep_sys_first(int mode) {
@@ -124,7 +134,15 @@ __host__ __device__ inline bool sweep_lane(const SkewGeo &q, int mode, int b, in
     l.arr = 0;
     return true;
   }
-  if (mode == SWEEP_BWD) return false;
+  if (mode >= SWEEP_BWD) {  // R0 (copy 1) at 5T, RR (copy 2) at 6T
+    if (c < 1 || c >= sweep_ncopy(q, mode)) return false;
+    l.base = slab0 * q.T;
+    l.wstride = q.T;
+    l.dst = (4 + c) * q.T;
+    l.bytes = q.T * es;
+    l.arr = c;
+    return true;
+  }
   l.wstride = q.T;
   l.arr = 1;
   if (c == 1 - sys_c) {  // the vector: Y (MODE 0) or P (MODE 1)
@@ -166,7 +184,7 @@ __host__ __device__ inline bool sweep_copy(const SkewGeo &q, int mode, int b, in
                                            SweepCopy &cp, int es) {
   SweepLane l;
   if (!sweep_lane(q, mode, b, c, l, es)) return false;
-  const int w = (mode == SWEEP_BWD) ? nsteps - 1 - u : u;
+  const int w = (mode >= SWEEP_BWD) ? nsteps - 1 - u : u;
   if (w < l.dlo || w > l.dhi) return false;
   cp.src = l.base + (long long)w * l.wstride;
   cp.dst = l.dst; cp.bytes = l.bytes; cp.arr = l.arr;
@@ -238,6 +256,13 @@ void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S
 void launch_fwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *y,
                   const float *spmv_x, SolveState *st, float *ybuf);
 void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, float *x, SolveState *st);
+// the FP32 backward sweep with the inner products after it summed on the
+// way, one partial per tile (rb + c*nb); false when not available for the
+// layout (nothing launched)
+bool launch_bwd_f_dot1(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *r0, float *x,
+                       double *rb, SolveState *st);
+bool launch_bwd_f_dot5(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *r0,
+                       const float *rr, float *x, double *rb, SolveState *st);
 void launch_dcmp_f(cudaStream_t s, const Geo &g, const SkewGeo &q, double U, const SkewSysF &S, int *pivot_bad);
 bool sweep_supported_f(const SkewGeo &q);
 // Vector kernels for both precisions (explicitly instantiated for double

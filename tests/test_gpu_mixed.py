@@ -70,3 +70,33 @@ def test_mixed_solver_against_oracle(gpu_lib, pkg, orc):
     print("mixed vs oracle:", err)
     for k, v in err.items():
         assert v <= TOL[k], (k, v)
+
+
+@pytest.mark.parametrize("over", [dict(precond_ti=16, precond_tj=4), dict(precond_ti=16, precond_tj=4,
+                                                                           sweep_occupancy=2), {}])
+def test_inner_products_in_the_sweeps(gpu_lib, pkg, over):
+    """The FP32 iteration's inner products summed by the backward sweeps
+    (dot_passes 0: (R0,AP) and the five sums after AE, one partial per
+    preconditioner block) against separate passes (dot_passes 1).  The
+    products are exact in double and only the order of the sums differs;
+    the FP32 iteration's path reacts to last-bit differences (single solves
+    take a few iterations more or fewer either way), so the iterations of
+    12 steps agree within 6 % in total and the fields within the solver's
+    tolerance; six blocks with one or two sweep blocks per SM, and one
+    block."""
+    c = _flume(pkg)
+    res = []
+    for dp in (0, 1):
+        t = pkg.Tank(c, diag_relres=1, cgepsr=1e-10, solver=1, dot_passes=dp, **over)
+        t.init_state(True)
+        its, rel = [], []
+        for _ in range(12):
+            t.step(c.dt)
+            its.append(t.stats()["icgitr"])
+            rel.append(t.stats()["true_relres"])
+        assert max(rel) <= 1e-10 and t.stats()["fallbacks"] == 0
+        res.append((sum(its), t.get_state()))
+    assert abs(res[0][0] - res[1][0]) <= 0.06 * res[1][0], (res[0][0], res[1][0])
+    err = _errors(res[0][1], res[1][1])
+    for k, v in err.items():
+        assert v <= TOL[k], (k, v)
