@@ -814,7 +814,19 @@ def run_ensemble(args, rank, world, local_rank):
     cases = P.cases.ensemble_flumes(args.members, seed=1000 * rank, scale=args.scale)
     tiles = [(args.ti, args.tj)] * len(cases)
     tune_s = None
-    if args.autotune:
+    tune_timings = None
+    if args.autotune and args.batch:
+        # one block shape for the batch, timed with all members stepping
+        # together (untimed here)
+        import importlib
+        at = importlib.import_module(P.__name__ + ".autotune")
+        t0 = time.time()
+        base = {k: v for k, v in params_for(args).items() if k not in ("precond_ti", "precond_tj")}
+        shape, tune_timings = at.pick_batch_tiles(cases, **base)
+        tiles = [shape] * len(cases)
+        args.ti, args.tj = shape
+        tune_s = round(time.time() - t0, 1)
+    elif args.autotune:
         # block shapes per member from the tile autotuner (untimed; cached by grid size)
         import importlib
         at = importlib.import_module(P.__name__ + ".autotune")
@@ -843,32 +855,64 @@ def run_ensemble(args, rank, world, local_rank):
         torch.cuda.synchronize()
         return max(e0.elapsed_time(e) for e in ends)
 
+    batch = P.Batch(tanks) if args.batch else None
+    step_all = batch.step if batch is not None else (lambda: P.step_ensemble(tanks))
     for _ in range(args.warmup):
-        P.step_ensemble(tanks)
+        step_all()
     l0 = P.kernel_launches()
     with ClockSampler(local_rank) as clk:
-        t_par = timed(lambda: [P.step_ensemble(tanks) for _ in range(args.steps)])
+        t_par = timed(lambda: [step_all() for _ in range(args.steps)])
     launches = P.kernel_launches() - l0
     t_seq = timed(lambda: [t.step() for _ in range(args.steps) for t in tanks])
     t_max, units = combine_ranks(t_par / 1e3, cells * args.steps, device=dev)
     iters = [t.stats()["icgitr"] for t in tanks]
+    if batch is not None:
+        batch.close()
+    # Agreement of every member with a solo plain-FP64 run of the same steps
+    # from the same initial state (untimed; one solo handle at a time).
+    agree = None
+    if args.solver == "mixed" and not args.no_agreement:
+        errs = []
+        base = {k: v for k, v in params_for(args).items() if k not in ("solver", "warm_start")}
+        for c, t in zip(cases, tanks):
+            st = t.get_state()
+            solo = P.Tank(c, **{**base, "solver": 0, "warm_start": 0, "precond_ti": args.ti, "precond_tj": args.tj})
+            solo.init_state(True)
+            for _ in range(int(st["nnow"])):
+                solo.step()
+            ref = solo.get_state()
+            e = field_errors(st, ref, c)
+            fs, fr = t.stats()["fsum"], solo.stats()["fsum"]
+            errs.append({"p_rel": e["p"]["max_abs"] / e["p"]["ref_max_abs"], "u_max": max(e[k]["max_abs"] for k in "uvw"),
+                         "F_max": e["F"]["max_abs"], "nf_mismatch": e["nf_mismatch_cells"],
+                         "volume_rel": abs(fs - fr) / abs(fr)})
+            solo.close()
+        agree = {"steps": int(tanks[0].get_state()["nnow"]),
+                 "max_p_rel": max(x["p_rel"] for x in errs), "max_u_abs": max(x["u_max"] for x in errs),
+                 "max_F_abs": max(x["F_max"] for x in errs), "nf_mismatch_cells": sum(x["nf_mismatch"] for x in errs),
+                 "max_volume_rel": max(x["volume_rel"] for x in errs)}
     if rank != 0:
         return
     line = {"metric": METRIC, "value": units / t_max / 1e6, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_par / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner / f64 refinement" if args.solver == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": f"ensemble of {args.members} independent porous wave flumes of uneven "
                                    f"size (nx U{{256..1024}}x{args.scale:g}, ny U{{16..64}}, nz U{{64..128}}, "
                                    f"wave makers, {'mixed' if args.solver == 'mixed' else 'plain FP64'} "
                                    f"SMAC step, block-Jacobi MILU "
-                                   f"{'blocks chosen per grid by the tile autotuner' if args.autotune else f'{args.ti}x{args.tj}'})",
+                                   f"{('blocks chosen per grid by the tile autotuner' if not args.batch else f'{args.ti}x{args.tj} chosen by the batch autotuner') if args.autotune else f'{args.ti}x{args.tj}'})",
                        "cells": cells, "members": args.members,
                        "sizes": [[c.ni - 2, c.nj - 2, c.nk - 2] for c in cases],
                        "sequential_value": cells * args.steps / (t_seq / 1e3) / 1e6,
                        "mean_bicgstab_iters": statistics.mean(iters),
                        **({"tiles": [list(t) for t in tiles], "autotune_s": tune_s} if args.autotune else {}),
-                       "parallelism": f"{args.members} streams side by side x{world} replicas"},
+                       **({"autotune_s_per_step": tune_timings} if tune_timings else {}),
+                       "parallelism": (f"{args.members} grids, one launch per solver kernel for all of them "
+                                       f"(cadmas_batch_step) x{world} replicas" if args.batch else
+                                       f"{args.members} streams side by side x{world} replicas")},
+            "agreement_with_solo_fp64": agree,
             "gpu_launches": launches, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     for t in tanks:
@@ -890,6 +934,11 @@ def main():
     ap.add_argument("--autotune", action="store_true",
                     help="--case ensemble: preconditioner block shape per member by the tile autotuner")
     ap.add_argument("--scale", type=float, default=1.0, help="x-size factor of ensemble members")
+    ap.add_argument("--batch", action="store_true",
+                    help="--case ensemble with --solver mixed: the members' pressure solves together, one "
+                         "launch per solver kernel (cadmas_batch_step)")
+    ap.add_argument("--no-agreement", action="store_true",
+                    help="--case ensemble --solver mixed: skip the members' comparison with solo FP64 runs")
     ap.add_argument("--learn-grid", default="128x32x64", help="--case learned: beach grid NXxNYxNZ")
     ap.add_argument("--learn-train", type=int, default=8, help="--case learned: training seeds")
     ap.add_argument("--learn-eval", type=int, default=3, help="--case learned: held-out seeds")

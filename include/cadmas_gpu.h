@@ -552,6 +552,27 @@ int cadmas_sync(cadmas_handle *h);
    cadmas_step status.  Returns the first non-zero status, or CADMAS_OK. */
 int cadmas_step_ensemble(cadmas_handle **h, int n, const double *dt, int *status);
 
+/* ---- batch of grids solved together (no counterpart in the reference) --
+   A batch steps n handles of the mixed solver (solver 1, dot_passes 0) on
+   one device, all with the same preconditioner block (precond_ti,
+   precond_tj; no split).  Each step runs, per grid on its own stream and
+   host thread, V1CAL up to the pressure system; then the pressure solves
+   of all the grids together on the batch's stream, every solver kernel one
+   launch over all the grids' tiles or slabs (a block finds its grid in a
+   table of the grids' block ranges); then, per grid again, the rest of
+   V1CAL and F1CAL.  The iterations run in lockstep: a grid that has
+   converged is marked done and its blocks return at once.  Each grid gets
+   the results, iterations and statistics a cadmas_step of its own gives.
+   The handles must stay alive and unchanged in their solver parameters
+   while the batch exists.  CADMAS_EINVAL for handles that do not match,
+   CADMAS_EUNSUPPORTED for blocks too large for the batched sweeps.       */
+typedef struct cadmas_batch cadmas_batch;
+int cadmas_batch_create(cadmas_handle **h, int n, cadmas_batch **out);
+/* One SMAC step of every grid of the batch; dt[i] and status[i] as in
+   cadmas_step_ensemble.  Returns the first non-zero status.              */
+int cadmas_batch_step(cadmas_batch *b, const double *dt, int *status);
+int cadmas_batch_destroy(cadmas_batch *b);
+
 /* Declare side w->side a wave-maker boundary driven by `tab` (copied).  Its
    boundary faces are those of INDB with INDB(3,L) = 5 on that side.  One
    table serves every wave side, as the reference's matrix data does.

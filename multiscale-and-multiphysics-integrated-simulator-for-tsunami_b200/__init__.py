@@ -209,7 +209,7 @@ EXPORTED = ["cadmas_default_params", "cadmas_create", "cadmas_destroy", "cadmas_
             "cadmas_unet_train_sys", "cadmas_unet_time_forward", "cadmas_test_stall_sweeps",
             "cadmas_set_wave_source", "cadmas_stream_solve", "cadmas_stream_eval", "cadmas_set_wave_theory",
             "cadmas_wave_solve", "cadmas_wave_eval", "cadmas_set_wave_func", "cadmas_set_wave_angle",
-            "cadmas_set_wave_source_func"]
+            "cadmas_set_wave_source_func", "cadmas_batch_create", "cadmas_batch_step", "cadmas_batch_destroy"]
 
 DROP_ARRAYS = ("droptx", "dropty", "droptz", "dropuu", "dropvv", "dropww")
 TURB_CELLS = ("ak", "ae", "anut", "anu")   # (NUMI,NUMJ,NUMK)
@@ -738,6 +738,44 @@ def open_speed(depth, period, grav=9.8, lib=None) -> float:
     c = C.c_double()
     _check(lib, lib.cadmas_open_speed(float(depth), float(period), float(grav), C.byref(c)))
     return c.value
+
+
+class Batch:
+    """Tanks of the mixed solver whose pressure solves run together, one
+    launch per solver kernel for all of them (cadmas_batch_*).  The tanks
+    stay owned by the caller and must outlive the batch."""
+
+    def __init__(self, tanks, lib=None):
+        self.lib = lib or load_library()
+        self.tanks = list(tanks)
+        n = len(self.tanks)
+        hs = (C.c_void_p * n)(*[t.h.value for t in self.tanks])
+        self.h = C.c_void_p()
+        self.lib.cadmas_batch_create.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
+        _check(self.lib, self.lib.cadmas_batch_create(hs, n, C.byref(self.h)))
+
+    def step(self, dts=None):
+        """One SMAC step of every tank; returns the per-tank statuses."""
+        n = len(self.tanks)
+        dt = (C.c_double * n)(*[float(d) for d in (dts if dts is not None else [t.case.dt for t in self.tanks])])
+        st = (C.c_int * n)()
+        self.lib.cadmas_batch_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        rc = self.lib.cadmas_batch_step(self.h, dt, st)
+        if rc != OK:
+            raise CadmasError(rc, self.lib.cadmas_strerror(rc).decode())
+        return list(st)
+
+    def close(self):
+        if self.h:
+            self.lib.cadmas_batch_destroy.argtypes = [C.c_void_p]
+            self.lib.cadmas_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def step_ensemble(tanks, dts=None, lib=None):

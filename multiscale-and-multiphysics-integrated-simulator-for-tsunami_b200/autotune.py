@@ -83,3 +83,57 @@ def pick_tiles(case, candidates=CANDIDATES, cache=None, measure=None, **params):
     if cache is not None:
         cache.put(key, tiles, timings)
     return tiles
+
+
+# ---- co-scheduled tuning of a batch -------------------------------------
+# A batch (cadmas_batch_step) solves all its grids together with one block
+# shape, so the shape is chosen by timing the whole batch stepping together
+# for each candidate: the members' kernels then share the SMs as they will
+# in the run, which timing each member alone does not show.
+BATCH_CANDIDATES = [(16, 16), (16, 8), (8, 16), (32, 8)]
+
+
+def measure_batch(cases, ti, tj, steps=2, warmup=2, **params):
+    """Seconds per step of all the cases stepped together as one batch with
+    ti x tj blocks (None if the library refuses the shape)."""
+    from . import Batch, CadmasError, Tank
+    tanks, batch = [], None
+    try:
+        try:
+            for c in cases:
+                tanks.append(Tank(c, precond_ti=ti, precond_tj=tj, **params))
+            batch = Batch(tanks)
+        except CadmasError:
+            return None
+        for t, c in zip(tanks, cases):
+            t.init_state(c.hydrostatic)
+        for _ in range(warmup):
+            batch.step()
+        for t in tanks:
+            t.sync()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            batch.step()
+        for t in tanks:
+            t.sync()
+        return (time.perf_counter() - t0) / steps
+    finally:
+        if batch is not None:
+            batch.close()
+        for t in tanks:
+            t.close()
+
+
+def pick_batch_tiles(cases, candidates=BATCH_CANDIDATES, measure=None, **params):
+    """(ti, tj) of the candidates with which the batch of `cases` steps
+    fastest, timed co-scheduled; and the seconds per step of each."""
+    measure = measure or measure_batch
+    timings = {}
+    for ti, tj in candidates:
+        s = measure(cases, ti, tj, **params)
+        if s is not None:
+            timings[f"{ti}x{tj}"] = s
+    if not timings:
+        raise RuntimeError("no candidate tile shape runs the batch")
+    best = min(timings, key=timings.get)
+    return tuple(int(v) for v in best.split("x")), timings

@@ -746,7 +746,14 @@ static int bc_tail_v1(cadmas_handle *h) {
   return CADMAS_OK;
 }
 
-static int do_v1cal(cadmas_handle *h) {
+// VF_V1CAL in three parts, so that a batch can solve the pressure of
+// several grids together: up to the Poisson system and PT's start value
+// (vf_v1cal.f:118-271, vf_vpsol.f:52-58), the solve (vf_vpsol.f:59-76),
+// and the rest (vf_v1cal.f:272-297).
+static SysPtr poisson_sys(const cadmas_handle *h) {
+  return SysPtr{h->wk[0], h->wk[1], h->wk[2], h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[7]};
+}
+static int v1cal_pre(cadmas_handle *h) {
   cudaStream_t s = h->s;
   refresh_prm(h);
   refresh_fld(h);
@@ -769,7 +776,7 @@ static int do_v1cal(cadmas_handle *h) {
   { const int ro = open_bc(h, h->vel[nxt ^ 1][0], h->vel[nxt ^ 1][1], h->vel[nxt ^ 1][2]); if (ro) return ro; }
   TE();
   // Poisson system (vf_v1cal.f:259-271)
-  SysPtr a{h->wk[0], h->wk[1], h->wk[2], h->wk[3], h->wk[4], h->wk[5], h->wk[6], h->wk[7]};
+  const SysPtr a = poisson_sys(h);
   TB(CADMAS_STAGE_VPCOEF); launch_vpcoef(s, h->g, h->f, h->p, a, h->dint); TE();
   // VF_VPSOL: PT = 0, solve (vf_vpsol.f:52-76)
   double *PT = h->wk[8];
@@ -779,12 +786,21 @@ static int do_v1cal(cadmas_handle *h) {
     launch_warm_guess(s, h->g, h->f, a, h->wnet, h->ws_rows, h->ws_rows + nrows(h), h->ws_scal, h->ws_cnt, PT);
     TE();
   }
-  int iter;
-  double bn, xn;
+  return CADMAS_OK;
+}
+static int v1cal_solve(cadmas_handle *h, int &iter, double &bn, double &xn) {
+  const SysPtr a = poisson_sys(h);
+  double *PT = h->wk[8];
   const bool mixed = (h->P.solver == 1);
   h->warm_now = (h->P.warm_start == 1 && h->have_prev) ? 1 : 0;
-  int rc = mixed ? solve_mixed(h, a, PT, h->indc, iter, bn, xn) : solve(h, a, PT, h->indc, iter, bn, xn);
+  const int rc = mixed ? solve_mixed(h, a, PT, h->indc, iter, bn, xn) : solve(h, a, PT, h->indc, iter, bn, xn);
   h->warm_now = 0;
+  return rc;
+}
+static int v1cal_post(cadmas_handle *h, int rc, int iter, double bn, double xn) {
+  cudaStream_t s = h->s;
+  double *PT = h->wk[8];
+  const bool mixed = (h->P.solver == 1);
   if (rc) return rc;
   h->have_prev = (iter >= 0);
   h->stats.icgitr = iter;
@@ -806,6 +822,14 @@ static int do_v1cal(cadmas_handle *h) {
   TE();
   CK(cudaGetLastError());
   return CADMAS_OK;
+}
+static int do_v1cal(cadmas_handle *h) {
+  int rc = v1cal_pre(h);
+  if (rc) return rc;
+  int iter = 0;
+  double bn = 0.0, xn = 0.0;
+  rc = v1cal_solve(h, iter, bn, xn);
+  return v1cal_post(h, rc, iter, bn, xn);
 }
 
 // ------------------------------------------------------------ k-epsilon
@@ -1963,6 +1987,326 @@ int cadmas_step_ensemble(cadmas_handle **hs, int n, const double *dt, int *statu
       status[i] = cadmas_step(hs[i], dt[i]);
     });
   for (std::thread &t : pool) t.join();
+  for (int i = 0; i < n; ++i)
+    if (status[i]) return status[i];
+  return CADMAS_OK;
+}
+
+// ------------------------------------------------------------ batches
+// Grids stepped together with one launch of each solver kernel for all of
+// them (the mixed solver's FP32 iteration, its FP64 residuals, the layout
+// conversions and the factorisation).  The parts of a step around the
+// solve run per grid on the grid's own stream and host thread.
+struct cadmas_batch {
+  std::vector<cadmas_handle *> h;
+  int device = 0, nsm = 148, occ = 0;
+  cudaStream_t s = nullptr;
+  BatchMember *d_m = nullptr, *h_m = nullptr;  // member table (device, pinned host)
+  int *d_pre = nullptr;                          // block prefixes (BR_N x (n+1))
+  double *d_g = nullptr, *h_g = nullptr;         // gathered per member
+  cudaEvent_t ev = nullptr;
+  std::vector<cudaEvent_t> ev_m;
+  long long launches_solve = 0;
+};
+
+namespace {
+// A member's part of the batched solve from its handle.
+BatchMember batch_member_of(cadmas_handle *h) {
+  BatchMember m;
+  std::memset(&m, 0, sizeof(m));
+  h->Sf.indc = h->S.indc;
+  m.g = h->g; m.q = h->q; m.S = h->S; m.Sf = h->Sf; m.a = poisson_sys(h);
+  m.indc = h->indc; m.pt = h->wk[8];
+  float *vf[BF_N] = {h->bf, h->xf, h->r0f, h->rrf, h->pvf, h->apf, h->aef, h->y2f};
+  for (int i = 0; i < BF_N; ++i) m.vf[i] = vf[i];
+  m.vd[BD_B] = h->bb_sl; m.vd[BD_X] = h->xw; m.vd[BD_Y2] = h->y2;
+  m.rb0 = h->rb0; m.rb1 = h->rb1; m.rb5 = h->rb5; m.dres = h->dres;
+  m.st = h->st; m.pivot_bad = &h->st->pivot_bad;
+  m.nrb = h->nrb;
+  m.epsa2 = h->P.cgepsa * h->P.cgepsa; m.div2 = h->P.cgdiv * h->P.cgdiv; m.tol2 = h->P.cgepsr * h->P.cgepsr;
+  m.U = (h->P.icgtyp != 0) ? h->P.cgpara : 0.0;
+  m.icgmax = h->P.icgmax;
+  m.warm = (h->P.warm_start == 1 && h->have_prev) ? 1 : 0;
+  m.active = 1;
+  return m;
+}
+}  // namespace
+
+// The mixed solve (solve_mixed, solve_inner_f) of the members `idx` of a
+// batch in lockstep: every refinement pass and every FP32 iteration is one
+// launch per kernel over all members still refining; a member that has
+// converged is marked done and its blocks return at once.  A member whose
+// FP32 factor or inner solve fails is solved alone by the FP64 solver, as
+// solve_mixed does.  Results, iterations and status per member.
+static void solve_mixed_batch(cadmas_batch *b, const std::vector<int> &idx, std::vector<int> &iter,
+                              std::vector<double> &bn, std::vector<double> &xn, std::vector<int> &rc) {
+  cudaStream_t s = b->s;
+  const int nm = (int)idx.size();
+  std::vector<cadmas_handle *> hs(nm);
+  for (int j = 0; j < nm; ++j) hs[j] = b->h[idx[j]];
+  iter.assign(nm, 0); bn.assign(nm, 0.0); xn.assign(nm, 0.0); rc.assign(nm, CADMAS_OK);
+  if (nm == 0) return;
+  auto fail = [&](int code) { for (int j = 0; j < nm; ++j) if (!rc[j]) rc[j] = code; };
+  // member table and block prefixes
+  std::vector<int> pre((size_t)BR_N * (nm + 1), 0);
+  long long ntiles = 0, nslab = 0, nelem = 0;
+  for (int j = 0; j < nm; ++j) {
+    b->h_m[j] = batch_member_of(hs[j]);
+    const SkewGeo &q = hs[j]->q;
+    const long long n = (long long)q.nb * q.W * q.T;
+    pre[BR_TILE * (nm + 1) + j] = (int)ntiles;
+    pre[BR_SLAB * (nm + 1) + j] = (int)nslab;
+    pre[BR_ELEM * (nm + 1) + j] = (int)nelem;
+    ntiles += q.nb;
+    nslab += hs[j]->nrb;
+    nelem += (n + BATCH_ELEM - 1) / BATCH_ELEM;
+  }
+  pre[BR_TILE * (nm + 1) + nm] = (int)ntiles;
+  pre[BR_SLAB * (nm + 1) + nm] = (int)nslab;
+  pre[BR_ELEM * (nm + 1) + nm] = (int)nelem;
+  const SkewGeo qref = hs[0]->q;
+  const BatchMember *bm = b->d_m;
+  const int *dp = b->d_pre;
+  const int nsm = b->nsm, occ = b->occ;
+  auto upload = [&]() -> bool {
+    return cudaMemcpyAsync(b->d_m, b->h_m, (size_t)nm * sizeof(BatchMember), cudaMemcpyHostToDevice, s) ==
+           cudaSuccess;
+  };
+  auto gather = [&]() -> bool {
+    launch_b_gather(s, bm, nm, b->d_g);
+    return cudaMemcpyAsync(b->h_g, b->d_g, (size_t)nm * BATCH_GATHER * sizeof(double), cudaMemcpyDeviceToHost,
+                           s) == cudaSuccess &&
+           cudaStreamSynchronize(s) == cudaSuccess;
+  };
+  auto G = [&](int j, int c) { return b->h_g[(size_t)j * BATCH_GATHER + c]; };
+  if (cudaMemcpyAsync(b->d_pre, pre.data(), pre.size() * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      !upload()) { set_cuda_error("batch upload", cudaGetLastError()); fail(CADMAS_ECUDA); return; }
+  // the FP64 system, INDC, B and the initial guess in the skewed layout;
+  // the FP32 system and its factor
+  launch_b_to_skew(s, bm, dp, nm, nelem);
+  launch_b_sys_to_f(s, bm, dp, nm, nelem);
+  launch_b_clear(s, bm, nm);
+  if (!launch_b_dcmp_f(s, bm, dp, nm, ntiles, qref.T) || !gather()) { fail(CADMAS_ECUDA); return; }
+  std::vector<char> fallback(nm, 0), conv(nm, 0);
+  std::vector<double> b2(nm, 0.0), r2(nm, 0.0);
+  std::vector<int> total(nm, 0);
+  for (int j = 0; j < nm; ++j)
+    if (G(j, 3) != 0.0) { fallback[j] = 1; b->h_m[j].active = 0; }
+  bool error = false;
+  for (int outer = 0; outer < 40 && !error; ++outer) {
+    // r = b - A x and the two norms in FP64 for every member still refining
+    if (!upload()) { error = true; break; }
+    launch_b_clear(s, bm, nm);
+    launch_b_residual(s, bm, dp, nm, nslab);
+    launch_b_fin(s, FIN_STORE, bm, nm, false);
+    if (!gather()) { error = true; break; }
+    int nact = 0;
+    for (int j = 0; j < nm; ++j) {
+      BatchMember &M = b->h_m[j];
+      if (!M.active) continue;
+      cadmas_handle *h = hs[j];
+      b2[j] = G(j, 4);
+      r2[j] = G(j, 5);
+      h->mixed_outer++;
+      if (r2[j] <= M.tol2 * b2[j]) { conv[j] = 1; M.active = 0; continue; }
+      const double rn = std::sqrt(r2[j]);
+      const double need = std::sqrt(M.tol2 * b2[j] / r2[j]);
+      const double floor_eps = h->P.mixed_eps_inner > 0.0 ? h->P.mixed_eps_inner : 1.0e-5;
+      const double eps_in = std::min(0.5, std::max(0.5 * need, floor_eps));
+      M.rn = rn; M.scale = 1.0 / rn; M.eps2 = eps_in * eps_in;
+      ++nact;
+    }
+    if (nact == 0) break;
+    if (!upload()) { error = true; break; }
+    // the inner FP32 solve of every member refining (solve_inner_f)
+    launch_b_start_f(s, bm, dp, nm, nslab);
+    launch_b_clear(s, bm, nm);
+    bool ok = launch_b_sweep(s, SWEEP_FWD, bm, dp, nm, ntiles, qref, BF_B, -1, -1, false, nsm, occ) &&
+              launch_b_sweep(s, SWEEP_BWD, bm, dp, nm, ntiles, qref, -1, BF_R0, -1, false, nsm, occ);
+    launch_b_dot_r0f(s, bm, dp, nm, nslab);
+    launch_b_fin(s, FIN_BNORM, bm, nm, false);
+    launch_b_fin(s, FIN_START, bm, nm, false);
+    launch_b_copy2_f(s, bm, dp, nm, nslab);
+    int last = 8;
+    for (int j = 0; j < nm; ++j) last = std::max(last, hs[j]->last_iter);
+    int batch = std::max(2, std::min(last, 64));
+    for (int guard = 0; guard < 100000 && ok; ++guard) {
+      for (int k = 0; k < batch && ok; ++k) {
+        ok = launch_b_sweep(s, SWEEP_FWD_AX, bm, dp, nm, ntiles, qref, BF_PV, -1, -1, false, nsm, occ) &&
+             launch_b_sweep(s, SWEEP_BWD1, bm, dp, nm, ntiles, qref, BF_R0, BF_AP, -1, false, nsm, occ);
+        launch_b_fin(s, FIN_ALPHA, bm, nm, true);
+        launch_b_axpyf(s, bm, dp, nm, nslab);
+        ok = ok && launch_b_sweep(s, SWEEP_FWD_AX, bm, dp, nm, ntiles, qref, BF_RR, -1, -1, false, nsm, occ) &&
+             launch_b_sweep(s, SWEEP_BWD5, bm, dp, nm, ntiles, qref, BF_R0, BF_AE, BF_RR, true, nsm, occ);
+        launch_b_fin5(s, bm, nm);
+        launch_b_upd3f(s, bm, dp, nm, nslab);
+        launch_b_commit(s, bm, nm);
+      }
+      if (!ok || !gather()) { ok = false; break; }
+      bool all = true;
+      for (int j = 0; j < nm; ++j) {
+        if (!b->h_m[j].active) continue;
+        if (G(j, 1) != 0.0) {  // a bounded wait ran out: this member's step fails
+          g_last_error = "a bulk-copy wait of the MILU sweep ran out of time";
+          rc[j] = CADMAS_ETIMEOUT;
+        }
+        if (G(j, 0) == 0.0) all = false;
+      }
+      if (all) break;
+      batch = 4;
+    }
+    if (!ok) { error = true; break; }
+    for (int j = 0; j < nm; ++j) {
+      BatchMember &M = b->h_m[j];
+      if (!M.active) continue;
+      if (rc[j]) { M.active = 0; continue; }
+      const int it = (int)G(j, 2);
+      if (it < 0 || it > M.icgmax) { fallback[j] = 1; M.active = 0; continue; }  // FP64 takes over
+      total[j] += it;
+    }
+    launch_b_add_f(s, bm, dp, nm, nslab);  // XW += |r| D where the inner solve ended in ICGMAX
+  }
+  if (error) { set_cuda_error("batched solve", cudaGetLastError()); fail(CADMAS_ECUDA); return; }
+  for (int j = 0; j < nm; ++j)
+    if (b->h_m[j].active && !rc[j]) { fallback[j] = 1; b->h_m[j].active = 0; }  // not converged in 40 passes
+  // X0 = XW of the converged members (k_x0 needs ITER >= 0: the state cleared)
+  for (int j = 0; j < nm; ++j) b->h_m[j].active = (conv[j] && !rc[j]) ? 1 : 0;
+  if (!upload()) { fail(CADMAS_ECUDA); return; }
+  launch_b_clear(s, bm, nm);
+  launch_b_x0(s, bm, dp, nm, nslab);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) { fail(CADMAS_ECUDA); return; }
+  for (int j = 0; j < nm; ++j) {
+    if (rc[j]) continue;
+    cadmas_handle *h = hs[j];
+    if (fallback[j]) {  // the FP64 solver alone, from the guess of this step (solve_mixed's fallback)
+      h->mixed_fallback++;
+      h->warm_now = b->h_m[j].warm;
+      rc[j] = solve(h, poisson_sys(h), h->wk[8], h->indc, iter[j], bn[j], xn[j]);
+      h->warm_now = 0;
+      if (cudaStreamSynchronize(h->s) != cudaSuccess) rc[j] = CADMAS_ECUDA;
+      continue;
+    }
+    iter[j] = total[j];
+    bn[j] = std::sqrt(b2[j]);
+    xn[j] = std::sqrt(r2[j]);
+  }
+}
+
+int cadmas_batch_create(cadmas_handle **hs, int n, cadmas_batch **out) {
+  if (!hs || !out || n < 1) return CADMAS_EINVAL;
+  *out = nullptr;
+  long long ntiles = 0;
+  for (int i = 0; i < n; ++i) {
+    cadmas_handle *h = hs[i];
+    if (!h) return CADMAS_EINVAL;
+    if (h->P.solver != 1 || h->P.dot_passes != 0) {
+      g_last_error = "a batch takes handles of the mixed solver (solver 1, dot_passes 0)";
+      return CADMAS_EINVAL;
+    }
+    if (h->device != hs[0]->device || h->q.split != 1 || h->q.TI != hs[0]->q.TI || h->q.TJ != hs[0]->q.TJ ||
+        h->q.TIp != hs[0]->q.TIp) {
+      g_last_error = "a batch takes handles of one device with the same preconditioner block, unsplit";
+      return CADMAS_EINVAL;
+    }
+    for (int j = 0; j < i; ++j)
+      if (hs[j] == h) { g_last_error = "a handle twice in a batch"; return CADMAS_EINVAL; }
+    ntiles += h->q.nb;
+  }
+  cadmas_batch *b = new cadmas_batch();
+  b->h.assign(hs, hs + n);
+  b->device = hs[0]->device;
+  b->nsm = hs[0]->q.nsm;
+  b->occ = hs[0]->q.occ;
+  if (!b_sweeps_supported(hs[0]->q, b->nsm, b->occ, ntiles)) {
+    delete b;
+    g_last_error = "preconditioner block too large for the batched FP32 sweeps";
+    return CADMAS_EUNSUPPORTED;
+  }
+  int rc = CADMAS_OK;
+  if (cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking) != cudaSuccess) rc = CADMAS_ECUDA;
+  if (!rc && cudaMalloc(&b->d_m, (size_t)n * sizeof(BatchMember)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMallocHost(&b->h_m, (size_t)n * sizeof(BatchMember)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMalloc(&b->d_pre, (size_t)BR_N * (n + 1) * sizeof(int)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMalloc(&b->d_g, (size_t)n * BATCH_GATHER * sizeof(double)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaMallocHost(&b->h_g, (size_t)n * BATCH_GATHER * sizeof(double)) != cudaSuccess) rc = CADMAS_ENOMEM;
+  if (!rc && cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) rc = CADMAS_ECUDA;
+  b->ev_m.assign(n, nullptr);
+  for (int i = 0; i < n && !rc; ++i)
+    if (cudaEventCreateWithFlags(&b->ev_m[i], cudaEventDisableTiming) != cudaSuccess) rc = CADMAS_ECUDA;
+  if (rc) { cadmas_batch_destroy(b); return rc; }
+  *out = b;
+  return CADMAS_OK;
+}
+
+int cadmas_batch_destroy(cadmas_batch *b) {
+  if (!b) return CADMAS_OK;
+  if (b->s) cudaStreamSynchronize(b->s);
+  if (b->d_m) cudaFree(b->d_m);
+  if (b->h_m) cudaFreeHost(b->h_m);
+  if (b->d_pre) cudaFree(b->d_pre);
+  if (b->d_g) cudaFree(b->d_g);
+  if (b->h_g) cudaFreeHost(b->h_g);
+  if (b->ev) cudaEventDestroy(b->ev);
+  for (cudaEvent_t e : b->ev_m) if (e) cudaEventDestroy(e);
+  if (b->s) cudaStreamDestroy(b->s);
+  delete b;
+  return CADMAS_OK;
+}
+
+int cadmas_batch_step(cadmas_batch *b, const double *dt, int *status) {
+  if (!b || !dt || !status) return CADMAS_EINVAL;
+  const int n = (int)b->h.size();
+  std::vector<int> rc1(n, CADMAS_OK);
+  auto par = [&](auto fn) {  // fn(i) on one host thread per member
+    std::vector<std::thread> pool;
+    pool.reserve((size_t)n);
+    for (int i = 0; i < n; ++i)
+      pool.emplace_back([&, i]() { cudaSetDevice(b->device); fn(i); });
+    for (std::thread &t : pool) t.join();
+  };
+  // V1CAL up to the pressure system (vf_a1main.f:1029-1058)
+  par([&](int i) {
+    cadmas_handle *h = b->h[i];
+    if (!h->have_static) { rc1[i] = CADMAS_ENOSTATIC; return; }
+    if (!(dt[i] > 0.0)) { rc1[i] = CADMAS_EINVAL; return; }
+    h->dtnow = dt[i];
+    h->nnow = h->nnow + 1;
+    h->tnow = h->tnow + h->dtnow;
+    rc1[i] = v1cal_pre(h);
+    if (!rc1[i] && cudaEventRecord(b->ev_m[i], h->s) != cudaSuccess) rc1[i] = CADMAS_ECUDA;
+  });
+  cudaSetDevice(b->device);
+  std::vector<int> idx;
+  for (int i = 0; i < n; ++i)
+    if (!rc1[i]) {
+      idx.push_back(i);
+      cudaStreamWaitEvent(b->s, b->ev_m[i], 0);
+    }
+  // the pressure solves together
+  std::vector<int> iter, rc2;
+  std::vector<double> bn, xn;
+  solve_mixed_batch(b, idx, iter, bn, xn, rc2);
+  cudaEventRecord(b->ev, b->s);
+  std::vector<int> slot(n, -1);
+  for (int j = 0; j < (int)idx.size(); ++j) slot[idx[j]] = j;
+  // the rest of V1CAL and F1CAL (vf_a1main.f:1058-1115)
+  par([&](int i) {
+    cadmas_handle *h = b->h[i];
+    int rc = rc1[i];
+    if (!rc) {
+      const int j = slot[i];
+      cudaStreamWaitEvent(h->s, b->ev, 0);
+      rc = v1cal_post(h, rc2[j], iter[j], bn[j], xn[j]);
+      if (rc == CADMAS_OK) {
+        int bits;
+        rc = read_err(h, bits);
+        if (rc == CADMAS_OK) rc = map_err(bits);
+      }
+      if (rc == CADMAS_OK) rc = do_f1cal(h);
+    }
+    h->stats.last_status = rc;
+    status[i] = rc;
+  });
   for (int i = 0; i < n; ++i)
     if (status[i]) return status[i];
   return CADMAS_OK;

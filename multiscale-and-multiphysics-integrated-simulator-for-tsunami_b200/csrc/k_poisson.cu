@@ -146,10 +146,10 @@ struct TileGeo {
   int ti, tj;          // thread coordinates
   bool valid;
 };
-__device__ __forceinline__ TileGeo tile_geo(const Geo &g, const SkewGeo &q) {
+__device__ __forceinline__ TileGeo tile_geo(const Geo &g, const SkewGeo &q, int bx, int by) {
   TileGeo t;
-  t.is = 2 + blockIdx.x * q.TI;
-  t.js = 2 + blockIdx.y * q.TJ;
+  t.is = 2 + bx * q.TI;
+  t.js = 2 + by * q.TJ;
   t.wi = min(q.TI, g.NI - t.is);  // interior cells is..NI-1
   t.wj = min(q.TJ, g.NJ - t.js);
   t.ti = threadIdx.x % q.TIp;
@@ -225,11 +225,10 @@ __device__ __forceinline__ long long sl_index(const SkewGeo &q, int b, int w, in
 // outside the tile or the interior get 0 (INDC -1).  warm: keep the
 // previous solution already in xsl as the initial guess (0 where INDC is
 // now -1) instead of X0.
-__global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
-                          double *bsl, double *xsl, int warm) {
-  pdl_enter();
-  const long long n = (long long)q.nb * q.W * q.T;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void to_skew_elem(const Geo &g, const SkewGeo &q, const SysPtr &A_, const int *INDC,
+                                             const SkewSys &S, const double *X0, double *bsl, double *xsl, int warm,
+                                             long long e) {
+  {
     const int t = (int)(e % q.T);
     const long long bw = e / q.T;
     const int w = (int)(bw % q.W), b = (int)(bw / q.W);
@@ -254,6 +253,13 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
     bsl[e] = bv;
     xsl[e] = xv;
   }
+}
+__global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
+                          double *bsl, double *xsl, int warm) {
+  pdl_enter();
+  const long long n = (long long)q.nb * q.W * q.T;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    to_skew_elem(g, q, A_, INDC, S, X0, bsl, xsl, warm, e);
 }
 
 // Value of a skewed vector at the cell (ti,tj,k) of tile (bx,by), where ti
@@ -286,19 +292,19 @@ __device__ __forceinline__ void skew_fetch(double *dst, const Geo &g, const Skew
 // column, wavefront step s at k = 2+s-ti-tj.  Ring values: 0 AD, 1 ALI,
 // 2 ALJ, 3 ALK, 4 AUI, 5 AUJ, 6 AUK; DD is written in the skewed layout.
 template <int D, typename V>
-__global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
-  pdl_enter();
+__device__ __forceinline__ void dcmp_body(const Geo &g, const SkewGeo &q, V U, const SkewSysT<V> &S, int *pivot_bad,
+                                          int bx, int by) {
   constexpr int NV = 7, R = D + 3;
   const int TIp = q.TIp, TJl = q.TJ, Tl = q.T;      // layout tile
   const int TJb = TJl * q.split, Tb = TIp * TJb;    // preconditioner block
   Ring<NV, V> rg = ring_setup<NV, V>(Tb, R);
   const int tid = threadIdx.x;
   const int ti = tid % TIp, tj = tid / TIp;
-  const int is = 2 + blockIdx.x * q.TI, js = 2 + blockIdx.y * TJb;
+  const int is = 2 + bx * q.TI, js = 2 + by * TJb;
   const int wi = min(q.TI, g.NI - is), wj = min(TJb, g.NJ - js);
   const bool valid = ti < wi && tj < wj;
   const int r = tj / TJl, tjl = tj % TJl;
-  const long long bl = blockIdx.x + (long long)q.ntx * (blockIdx.y * q.split + r);  // layout tile
+  const long long bl = bx + (long long)q.ntx * (by * q.split + r);  // layout tile
   // slab of step s: w = (k-2) + ti + tjl = s - r*TJl
   const long long slab0 = bl * q.W - (long long)r * TJl;
   const int tl = ti + TIp * tjl;
@@ -356,6 +362,11 @@ __global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
   }
   cp_wait<0>();
   if (bad) atomicOr(pivot_bad, 1);
+}
+template <int D, typename V>
+__global__ void k_dcmp(Geo g, SkewGeo q, V U, SkewSysT<V> S, int *pivot_bad) {
+  pdl_enter();
+  dcmp_body<D, V>(g, q, U, S, pivot_bad, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // ------------------------------------------------ bulk-copy slab pipeline
@@ -500,16 +511,15 @@ __device__ __forceinline__ void cluster_barrier() {
 // and their evaluation order are those of the reference loops, so the
 // results do not change.  The step loop is unrolled by the ring length so
 // slot addresses and mbarrier phases are constants.
-template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1>
-__global__ void __launch_bounds__(MAXT, MINB)
-    k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st, const V *vin2, double *rb) {
+template <int D, int MODE, typename V, int CS>
+__device__ __forceinline__ void sweep_body(const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *vin,
+                                           V *vout, SolveState *st, const V *vin2, double *rb, int bx, int by) {
   constexpr bool BWD = MODE >= SWEEP_BWD;
   constexpr int NDOT = sweep_ndot(MODE);
-  pdl_enter();
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
   // preconditioner block; every block of a cluster runs through the two
   // cluster barriers below, so none returns early.
-  const bool skip = st->done || (CS == 2 && (int)blockIdx.y >= q.nb / q.ntx);
+  const bool skip = st->done || (CS == 2 && by >= q.nb / q.ntx);
   if (CS == 1 && skip) return;
   if (CS == 2 && skip) {
     cluster_barrier();
@@ -531,8 +541,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm);
   V *ring = reinterpret_cast<V *>(sm + ((R + 1) & ~1));
   V *xb = ring + (size_t)R * SS;
-  const int tid = threadIdx.x, b = blockIdx.x + q.ntx * blockIdx.y;
-  TileGeo t = tile_geo(g, q);
+  const int tid = threadIdx.x, b = bx + q.ntx * by;
+  TileGeo t = tile_geo(g, q, bx, by);
   const int nsteps = (g.NK - 2) + (t.wi - 1) + (t.wj - 1);
   const bool producer = tid >= Tc;
   const int lane = tid & 31;
@@ -548,16 +558,16 @@ __global__ void __launch_bounds__(MAXT, MINB)
   unsigned long long *xfull = reinterpret_cast<unsigned long long *>(xb + 2 * T);
   V *xin = reinterpret_cast<V *>(xfull + NX);
   V *din = xin + (size_t)NX * TIp;
-  const int crank = (CS == 2) ? (int)(blockIdx.y & 1) : 0;
+  const int crank = (CS == 2) ? (by & 1) : 0;
   const int nty = q.nb / q.ntx;
-  const bool has_up = CS == 2 && crank == 0 && (int)blockIdx.y + 1 < nty;
+  const bool has_up = CS == 2 && crank == 0 && by + 1 < nty;
   const bool has_lo = CS == 2 && crank == 1;
   const bool recv = BWD ? has_up : has_lo;
   const bool send = BWD ? has_lo : has_up;
   const bool srow = send && (BWD ? t.tj == 0 : t.tj == q.TJ - 1) && !producer;
   const bool rrow = recv && (BWD ? t.tj == t.wj - 1 : t.tj == 0) && !producer;
   // receiver's step lag: rows of the sending tile minus one
-  const int lag = BWD ? min(q.TJ, g.NJ - (2 + ((int)blockIdx.y + 1) * q.TJ)) - 1 : q.TJ - 1;
+  const int lag = BWD ? min(q.TJ, g.NJ - (2 + (by + 1) * q.TJ)) - 1 : q.TJ - 1;
   unsigned r_xin = 0, r_din = 0, r_full = 0;            // the partner's xin, din, xfull
   if (CS == 2 && send) {
     const unsigned peer = cluster_rank() ^ 1u;
@@ -799,6 +809,12 @@ __global__ void __launch_bounds__(MAXT, MINB)
   }
   if (CS == 2) cluster_barrier();  // the partner may still write into this block's shared memory
 }
+template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB)
+    k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st, const V *vin2, double *rb) {
+  pdl_enter();
+  sweep_body<D, MODE, V, CS>(g, q, S, vin, vout, st, vin2, rb, (int)blockIdx.x, (int)blockIdx.y);
+}
 
 // ------------------------------------------------------------ slab kernels
 // The BiCGSTAB vectors live in the skewed layout; a vector kernel maps one
@@ -811,7 +827,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 // several entries' loads in flight.
 #define SLAB_LOOP_BEGIN(q)                                                          \
   const int lane_ = threadIdx.x & 31;                                               \
-  const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
+  const long long slab_ = (long long)BX_ * ROWS_PER_BLOCK + (threadIdx.x >> 5);      \
   if (slab_ < (long long)(q).nb * (q).W) {                                          \
     _Pragma("unroll 4")                                                             \
     for (int t_ = lane_; t_ < (q).T; t_ += 32) {                                    \
@@ -819,23 +835,22 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #define SLAB_LOOP_END \
     }                 \
   }
-#define SLAB_ROW ((long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5))
 // Partial of one block of a slab sum: each warp's slab sum (warp tree),
 // then the block's ROWS_PER_BLOCK slabs added in slab order by thread 0,
-// into rb[blockIdx.x].  The finaliser then reduces one partial per block
-// (nslab / 8 of them) instead of one per slab.  Every thread of the block
-// calls it (it holds block barriers).
-__device__ __forceinline__ void slab_store(double s, double *rb, long long nslab) {
+// into rb[bx] (bx the block's index).  The finaliser then reduces one
+// partial per block (nslab / 8 of them) instead of one per slab.  Every
+// thread of the block calls it (it holds block barriers).
+__device__ __forceinline__ void slab_store(double s, double *rb, long long nslab, unsigned bx) {
   __shared__ double ws[ROWS_PER_BLOCK];
   s = warp_tree(s);
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const long long first = (long long)blockIdx.x * ROWS_PER_BLOCK;
+    const long long first = (long long)bx * ROWS_PER_BLOCK;
     double t = 0.0;
     for (int i = 0; i < ROWS_PER_BLOCK; ++i)
       if (first + i < nslab) t = t + ws[i];
-    rb[blockIdx.x] = t;
+    rb[bx] = t;
   }
   __syncthreads();
 }
@@ -865,21 +880,28 @@ __device__ __forceinline__ V skew_ax(const Geo &g, const SkewGeo &q, const SkewS
 
 // Y = A X on INDC != -1 (VF_MZAX); Y untouched elsewhere.
 template <typename V>
-__global__ void k_spmv(Geo g, SkewGeo q, SkewSysT<V> S, const V *X, V *Y, const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void spmv_body(Geo g, SkewGeo q, SkewSysT<V> S, const V *X, V *Y, const SolveState *st, unsigned BX_) {
   if (st && st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (S.indc[e] != -1) Y[e] = skew_ax(g, q, S, X, e);
   SLAB_LOOP_END
 }
+template <typename V>
+__global__ void k_spmv(Geo g, SkewGeo q, SkewSysT<V> S, const V *X, V *Y, const SolveState *st) {
+  pdl_enter();
+  spmv_body<V>(g, q, S, X, Y, st, blockIdx.x);
+}
 
 // Y = B - Y on INDC != -1 (vf_m1bcgs.f:124-132)
-__global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void bmy_body(SkewGeo q, const int *INDC, const double *B, double *Y, const SolveState *st, unsigned BX_) {
   if (st && st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) Y[e] = B[e] - Y[e];
   SLAB_LOOP_END
+}
+__global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, const SolveState *st) {
+  pdl_enter();
+  bmy_body(q, INDC, B, Y, st, blockIdx.x);
 }
 
 // The BiCGSTAB vector kernels below serve the FP64 solve (V = double) and
@@ -889,9 +911,8 @@ __global__ void k_bmy(SkewGeo q, const int *INDC, const double *B, double *Y, co
 
 // Slab partials of up to two dot products (VF_MZIP).
 template <typename V>
-__global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, const V *x1, const V *y1,
-                      double *rb0, double *rb1, const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void dot_body(SkewGeo q, const int *INDC, const V *x0, const V *y0, const V *x1, const V *y1,
+                      double *rb0, double *rb1, const SolveState *st, unsigned BX_) {
   if (st && st->done) return;
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
@@ -904,24 +925,35 @@ __global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, cons
     if (x1) s1 = s1 + a1;
   }
   SLAB_LOOP_END
-  slab_store(s0, rb0, nslab);
-  if (x1) slab_store(s1, rb1, nslab);
+  slab_store(s0, rb0, nslab, BX_);
+  if (x1) slab_store(s1, rb1, nslab, BX_);
+}
+template <typename V>
+__global__ void k_dot(SkewGeo q, const int *INDC, const V *x0, const V *y0, const V *x1, const V *y1,
+                      double *rb0, double *rb1, const SolveState *st) {
+  pdl_enter();
+  dot_body<V>(q, INDC, x0, y0, x1, y1, rb0, rb1, st, blockIdx.x);
 }
 
 // RR = R0, PP = R0
 template <typename V>
-__global__ void k_copy2(SkewGeo q, const int *INDC, const V *R0, V *RR, V *PP, const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void copy2_body(SkewGeo q, const int *INDC, const V *R0, V *RR, V *PP, const SolveState *st, unsigned BX_) {
   if (st->done) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) { RR[e] = R0[e]; PP[e] = R0[e]; }
   SLAB_LOOP_END
+}
+template <typename V>
+__global__ void k_copy2(SkewGeo q, const int *INDC, const V *R0, V *RR, V *PP, const SolveState *st) {
+  pdl_enter();
+  copy2_body<V>(q, INDC, R0, RR, PP, st, blockIdx.x);
 }
 
 // RR = RR - ALPHA*AP (vf_m1bcgs.f:181-189)
 template <typename V>
 __global__ void k_axpy_rr(SkewGeo q, const int *INDC, const V *AP, V *RR, const SolveState *st) {
   pdl_enter();
+  const unsigned BX_ = blockIdx.x;
   if (st->done) return;
   const double alpha = st->alpha;
   SLAB_LOOP_BEGIN(q)
@@ -937,6 +969,7 @@ template <typename V>
 __global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, const V *R0, V *XW, V *RR,
                          double *rb0, double *rb1, const SolveState *st) {
   pdl_enter();
+  const unsigned BX_ = blockIdx.x;
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega;
   double s0 = 0.0, s1 = 0.0;
@@ -952,14 +985,15 @@ __global__ void k_upd_xr(SkewGeo q, const int *INDC, const V *PP, const V *AE, c
     s1 = s1 + (double)r0 * (double)r;
   }
   SLAB_LOOP_END
-  slab_store(s0, rb0, nslab);
-  slab_store(s1, rb1, nslab);
+  slab_store(s0, rb0, nslab, BX_);
+  slab_store(s1, rb1, nslab, BX_);
 }
 
 // PP = RR + BETA*(PP - OMEGA*AP) (vf_m1bcgs.f:229-238)
 template <typename V>
 __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V *PP, const SolveState *st) {
   pdl_enter();
+  const unsigned BX_ = blockIdx.x;
   if (st->done) return;
   const double beta = st->beta, omega = st->omega;
   SLAB_LOOP_BEGIN(q)
@@ -989,7 +1023,7 @@ __global__ void k_upd_p(SkewGeo q, const int *INDC, const V *RR, const V *AP, V 
 //     nothing to cancellation at the tolerances used (FP64 sums).
 #define SLAB4_LOOP_BEGIN(q)                                                         \
   const int lane_ = threadIdx.x & 31;                                               \
-  const long long slab_ = (long long)blockIdx.x * ROWS_PER_BLOCK + (threadIdx.x >> 5); \
+  const long long slab_ = (long long)BX_ * ROWS_PER_BLOCK + (threadIdx.x >> 5);      \
   if (slab_ < (long long)(q).nb * (q).W) {                                          \
     const int T4_ = (q).T >> 2;                                                     \
     _Pragma("unroll 2")                                                             \
@@ -1005,6 +1039,7 @@ __device__ __forceinline__ double dot4(const float4 &a, const float4 &b) {
 // slab partials of (R0,AP)
 __global__ void k_dot2f(SkewGeo q, const float *R0, const float *AP, double *rb, const SolveState *st) {
   pdl_enter();
+  const unsigned BX_ = blockIdx.x;
   if (st->done) return;
   const float4 *r0 = reinterpret_cast<const float4 *>(R0), *ap = reinterpret_cast<const float4 *>(AP);
   double s0 = 0.0;
@@ -1012,11 +1047,10 @@ __global__ void k_dot2f(SkewGeo q, const float *R0, const float *AP, double *rb,
   SLAB4_LOOP_BEGIN(q)
   s0 += dot4(r0[e4], ap[e4]);
   SLAB4_LOOP_END
-  slab_store(s0, rb, nslab);
+  slab_store(s0, rb, nslab, BX_);
 }
 // RR = RR - ALPHA*AP
-__global__ void k_axpyf(SkewGeo q, const float *AP, float *RR, const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void axpyf_body(SkewGeo q, const float *AP, float *RR, const SolveState *st, unsigned BX_) {
   if (st->done) return;
   const double alpha = st->alpha;
   const float4 *ap = reinterpret_cast<const float4 *>(AP);
@@ -1029,11 +1063,16 @@ __global__ void k_axpyf(SkewGeo q, const float *AP, float *RR, const SolveState 
   rr[e4] = r;
   SLAB4_LOOP_END
 }
+__global__ void k_axpyf(SkewGeo q, const float *AP, float *RR, const SolveState *st) {
+  pdl_enter();
+  axpyf_body(q, AP, RR, st, blockIdx.x);
+}
 // block partials of (RR,AE), (AE,AE), (RR,RR), (R0,RR), (R0,AE) into
 // rb + c*nrb, c = 0..4 (nrb = blocks of the launch)
 __global__ void k_dot5f(SkewGeo q, const float *R0, const float *RR, const float *AE, double *rb,
                         const SolveState *st) {
   pdl_enter();
+  const unsigned BX_ = blockIdx.x;
   if (st->done) return;
   const float4 *r0 = reinterpret_cast<const float4 *>(R0), *rr = reinterpret_cast<const float4 *>(RR),
                *ae = reinterpret_cast<const float4 *>(AE);
@@ -1048,17 +1087,16 @@ __global__ void k_dot5f(SkewGeo q, const float *R0, const float *RR, const float
   s4 += dot4(a, e);
   SLAB4_LOOP_END
   const long long nrb = gridDim.x;  // block partials of each sum
-  slab_store(s0, rb, nslab);
-  slab_store(s1, rb + nrb, nslab);
-  slab_store(s2, rb + 2 * nrb, nslab);
-  slab_store(s3, rb + 3 * nrb, nslab);
-  slab_store(s4, rb + 4 * nrb, nslab);
+  slab_store(s0, rb, nslab, BX_);
+  slab_store(s1, rb + nrb, nslab, BX_);
+  slab_store(s2, rb + 2 * nrb, nslab, BX_);
+  slab_store(s3, rb + 3 * nrb, nslab, BX_);
+  slab_store(s4, rb + 4 * nrb, nslab, BX_);
 }
 // XW = XW + (ALPHA*PP + OMEGA*RR); RR' = RR - OMEGA*AE;
 // PP = RR' + BETA*(PP - OMEGA*AP); RR = RR'
-__global__ void k_upd3f(SkewGeo q, const float *AE, const float *AP, float *XW, float *RR, float *PP,
-                        const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void upd3f_body(SkewGeo q, const float *AE, const float *AP, float *XW, float *RR, float *PP,
+                        const SolveState *st, unsigned BX_) {
   if (st->done) return;
   const double alpha = st->alpha, omega = st->omega, beta = st->beta;
   const float4 *ae = reinterpret_cast<const float4 *>(AE), *ap = reinterpret_cast<const float4 *>(AP);
@@ -1078,12 +1116,16 @@ __global__ void k_upd3f(SkewGeo q, const float *AE, const float *AP, float *XW, 
   pp[e4] = pn;
   SLAB4_LOOP_END
 }
+__global__ void k_upd3f(SkewGeo q, const float *AE, const float *AP, float *XW, float *RR, float *PP,
+                        const SolveState *st) {
+  pdl_enter();
+  upd3f_body(q, AE, AP, XW, RR, PP, st, blockIdx.x);
+}
 // OMEGA, the new |RR|^2 and (R0,RR), convergence and BETA from the five
 // sums (vf_m1bcgs.f:196-241 regrouped).  A finished solve sets `stop`;
 // k_commit turns it into `done` once the last update has run.
-__global__ void k_fin5(const double *rb, long long nrows, SolveState *st, double epsa2, double epsr2, double div2,
-                       int icgmax) {
-  pdl_enter();
+__device__ __forceinline__ void fin5_body(const double *rb, long long nrows, SolveState *st, double epsa2,
+                                          double epsr2, double div2, int icgmax) {
   if (st->done) return;
   const double rae = block_final(rb, nrows), aeae = block_final(rb + nrows, nrows),
                rrrr = block_final(rb + 2 * nrows, nrows), r0rr = block_final(rb + 3 * nrows, nrows),
@@ -1103,6 +1145,11 @@ __global__ void k_fin5(const double *rb, long long nrows, SolveState *st, double
   st->iter = st->iter + 1;
   if (st->iter > icgmax) st->stop = 1;
 }
+__global__ void k_fin5(const double *rb, long long nrows, SolveState *st, double epsa2, double epsr2, double div2,
+                       int icgmax) {
+  pdl_enter();
+  fin5_body(rb, nrows, st, epsa2, epsr2, div2, icgmax);
+}
 __global__ void k_commit(SolveState *st) {
   pdl_enter();
   if (st->stop) st->done = 1;
@@ -1111,36 +1158,43 @@ __global__ void k_commit(SolveState *st) {
 // ------------------------------------------- mixed-precision conversions
 // FP32 copy of the 7 coefficients (DD comes from the FP32 factorisation,
 // T from the FP32 forward sweeps).
+__device__ __forceinline__ void sys_to_f_elem(const SkewGeo &q, const double *sys, float *sysf, long long e) {
+  const long long slab = e / q.T;
+  const int t = (int)(e - slab * q.T);
+  constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
+#pragma unroll
+  for (int c = 0; c < 7; ++c) sysf[sys_at(slab, cs[c], q.T, t)] = (float)sys[sys_at(slab, cs[c], q.T, t)];
+}
 __global__ void k_sys_to_f(SkewGeo q, const double *sys, float *sysf) {
   pdl_enter();
   const long long n = (long long)q.nb * q.W * q.T;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-    const long long slab = e / q.T;
-    const int t = (int)(e - slab * q.T);
-    constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
-#pragma unroll
-    for (int c = 0; c < 7; ++c) sysf[sys_at(slab, cs[c], q.T, t)] = (float)sys[sys_at(slab, cs[c], q.T, t)];
-  }
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    sys_to_f_elem(q, sys, sysf, e);
 }
 // RF = R * scale on INDC != -1 (the right-hand side of an inner solve)
-__global__ void k_scale_to_f(SkewGeo q, const int *INDC, const double *R, double scale, float *RF) {
-  pdl_enter();
+__device__ __forceinline__ void scale_to_f_body(SkewGeo q, const int *INDC, const double *R, double scale, float *RF, unsigned BX_) {
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) RF[e] = (float)(R[e] * scale);
   SLAB_LOOP_END
 }
-// X = X + D * inv_scale on INDC != -1 (the correction of an inner solve)
-__global__ void k_add_f(SkewGeo q, const int *INDC, const float *D, double inv_scale, double *X) {
+__global__ void k_scale_to_f(SkewGeo q, const int *INDC, const double *R, double scale, float *RF) {
   pdl_enter();
+  scale_to_f_body(q, INDC, R, scale, RF, blockIdx.x);
+}
+// X = X + D * inv_scale on INDC != -1 (the correction of an inner solve)
+__device__ __forceinline__ void add_f_body(SkewGeo q, const int *INDC, const float *D, double inv_scale, double *X, unsigned BX_) {
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) X[e] = X[e] + (double)D[e] * inv_scale;
   SLAB_LOOP_END
 }
+__global__ void k_add_f(SkewGeo q, const int *INDC, const float *D, double inv_scale, double *X) {
+  pdl_enter();
+  add_f_body(q, INDC, D, inv_scale, X, blockIdx.x);
+}
 
 // X0 = XW on INDC != -1 when ITER >= 0 (vf_m1bcgs.f:251-261), back to the
 // standard layout.
-__global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double *X0, const SolveState *st) {
-  pdl_enter();
+__device__ __forceinline__ void x0_body(Geo g, SkewGeo q, const int *INDC, const double *XW, double *X0, const SolveState *st, unsigned BX_) {
   if (st->iter < 0) return;
   SLAB_LOOP_BEGIN(q)
   if (INDC[e] != -1) {
@@ -1151,11 +1205,16 @@ __global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double
   }
   SLAB_LOOP_END
 }
+__global__ void k_x0(Geo g, SkewGeo q, const int *INDC, const double *XW, double *X0, const SolveState *st) {
+  pdl_enter();
+  x0_body(g, q, INDC, XW, X0, st, blockIdx.x);
+}
 
 // ||b-Ax||^2 and ||b||^2 slab partials (diagnostic of the metric)
 __global__ void k_relres(Geo g, SkewGeo q, SkewSys S, const double *B, const double *X, double *rb0,
                          double *rb1) {
   pdl_enter();
+  const unsigned BX_ = blockIdx.x;
   double s0 = 0.0, s1 = 0.0;
   const long long nslab = (long long)q.nb * q.W;
   SLAB_LOOP_BEGIN(q)
@@ -1165,17 +1224,16 @@ __global__ void k_relres(Geo g, SkewGeo q, SkewSys S, const double *B, const dou
     s1 = s1 + B[e] * B[e];
   }
   SLAB_LOOP_END
-  slab_store(s0, rb0, nslab);
-  slab_store(s1, rb1, nslab);
+  slab_store(s0, rb0, nslab, BX_);
+  slab_store(s1, rb1, nslab, BX_);
 }
 
 // ------------------------------------------------------------- finalisers
 // One block of 1024 threads: reduce the row partials and advance the
 // BiCGSTAB scalars exactly as the host code of vf_m1bcgs.f would.
-__global__ void k_fin(int mode, const double *rb0, const double *rb1, long long nrows,
-                      SolveState *st, double *out, double epsa2, double epsr2, double div2,
-                      int icgmax) {
-  pdl_enter();
+__device__ __forceinline__ void fin_body(int mode, const double *rb0, const double *rb1, long long nrows,
+                                         SolveState *st, double *out, double epsa2, double epsr2, double div2,
+                                         int icgmax) {
   if (mode < FIN_ALPHA && mode != FIN_STORE && mode != FIN_RELRES && st->done) return;
   if (mode >= FIN_ALPHA && st->done) return;
   double a = block_final(rb0, nrows);
@@ -1225,6 +1283,12 @@ __global__ void k_fin(int mode, const double *rb0, const double *rb1, long long 
     default:
       break;
   }
+}
+__global__ void k_fin(int mode, const double *rb0, const double *rb1, long long nrows,
+                      SolveState *st, double *out, double epsa2, double epsr2, double div2,
+                      int icgmax) {
+  pdl_enter();
+  fin_body(mode, rb0, rb1, nrows, st, out, epsa2, epsr2, div2, icgmax);
 }
 
 // Factorisation failure ends the solve with ITER = -1 (vf_m1bcgs.f:101-102).
@@ -1645,5 +1709,249 @@ void launch_vmodif(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
   k_vmodif<<<row_blocks(g), ROW_THREADS, 0, s>>>(g, f, p, pt);
   count_launch();
 }
+
+
+// ---------------------------------------------------- batched solves
+// A block's member: the largest m with pre[m] <= blk (pre ascending).
+__device__ __forceinline__ int batch_member(const int *pre, int nm, int blk) {
+  int lo = 0, hi = nm - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+#define BATCH_BLOCK(range)                                                     \
+  const int *pr_ = pre + (range) * (nm + 1);                                   \
+  const int m_ = batch_member(pr_, nm, (int)blockIdx.x);                       \
+  const BatchMember &M = bm[m_];                                               \
+  const unsigned lb_ = blockIdx.x - (unsigned)pr_[m_];
+
+__global__ void kb_to_skew(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_ELEM)
+  if (!M.active) return;
+  const long long e = (long long)lb_ * BATCH_ELEM + threadIdx.x;
+  if (e < (long long)M.q.nb * M.q.W * M.q.T)
+    to_skew_elem(M.g, M.q, M.a, M.indc, M.S, M.pt, M.vd[BD_B], M.vd[BD_X], M.warm, e);
+}
+__global__ void kb_sys_to_f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_ELEM)
+  if (!M.active) return;
+  const long long e = (long long)lb_ * BATCH_ELEM + threadIdx.x;
+  if (e < (long long)M.q.nb * M.q.W * M.q.T) sys_to_f_elem(M.q, M.S.sys, M.Sf.sys, e);
+}
+template <int D>
+__global__ void kb_dcmp_f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_TILE)
+  if (!M.active) return;
+  dcmp_body<D, float>(M.g, M.q, (float)M.U, M.Sf, M.pivot_bad, (int)(lb_ % M.q.ntx), (int)(lb_ / M.q.ntx));
+}
+template <int D, int MODE, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) kb_sweep(const BatchMember *bm, const int *pre, int nm, int vin,
+                                                       int vout, int vin2, int rb5) {
+  pdl_enter();
+  BATCH_BLOCK(BR_TILE)
+  sweep_body<D, MODE, float, 1>(M.g, M.q, M.Sf, vin >= 0 ? M.vf[vin] : nullptr, vout >= 0 ? M.vf[vout] : nullptr,
+                                M.st, vin2 >= 0 ? M.vf[vin2] : nullptr, rb5 ? M.rb5 : M.rb0,
+                                (int)(lb_ % M.q.ntx), (int)(lb_ / M.q.ntx));
+}
+// the solve state of every member cleared up to the wait limit; members
+// outside the pass marked done, so every solver kernel skips them
+__global__ void kb_clear(const BatchMember *bm, int nm) {
+  pdl_enter();
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nm) return;
+  unsigned char *p = reinterpret_cast<unsigned char *>(bm[m].st);
+  for (int i = 0; i < (int)SOLVE_CLEAR_BYTES; ++i) p[i] = 0;
+  bm[m].st->done = bm[m].active ? 0 : 1;
+  if (bm[m].pivot_bad) *bm[m].pivot_bad = 0;
+}
+__global__ void kb_gather(const BatchMember *bm, int nm, double *out) {
+  pdl_enter();
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nm) return;
+  const SolveState *st = bm[m].st;
+  double *o = out + (long long)m * BATCH_GATHER;
+  o[0] = st->done; o[1] = st->timeout; o[2] = st->iter; o[3] = st->pivot_bad;
+  o[4] = bm[m].dres[6]; o[5] = bm[m].dres[7];
+}
+// r = b - A x in FP64 and the slab partials of (b,b) and (r,r)
+__global__ void kb_residual(const BatchMember *bm, const int *pre, int nm, int part) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  if (part == 0) spmv_body<double>(M.g, M.q, M.S, M.vd[BD_X], M.vd[BD_Y2], M.st, lb_);
+  else if (part == 1) bmy_body(M.q, M.S.indc, M.vd[BD_B], M.vd[BD_Y2], M.st, lb_);
+  else dot_body<double>(M.q, M.S.indc, M.vd[BD_B], M.vd[BD_B], M.vd[BD_Y2], M.vd[BD_Y2], M.rb0, M.rb1, M.st, lb_);
+}
+// one block per member: the finaliser of its sums (tile partials after a
+// backward sweep with sums, slab-block partials otherwise)
+__global__ void kb_fin(const BatchMember *bm, int nm, int mode, int tile_partials) {
+  pdl_enter();
+  const BatchMember &M = bm[blockIdx.x];
+  if (mode == FIN_STORE && !M.active) return;
+  const long long nrows = tile_partials ? (long long)M.q.nb : M.nrb;
+  fin_body(mode, M.rb0, mode == FIN_STORE ? M.rb1 : nullptr, nrows, M.st, M.dres + 6, M.epsa2, M.eps2, M.div2,
+           M.icgmax);
+}
+__global__ void kb_fin5(const BatchMember *bm, int nm) {
+  pdl_enter();
+  const BatchMember &M = bm[blockIdx.x];
+  fin5_body(M.rb5, (long long)M.q.nb, M.st, M.epsa2, M.eps2, M.div2, M.icgmax);
+}
+__global__ void kb_commit(const BatchMember *bm, int nm) {
+  pdl_enter();
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < nm && bm[m].st->stop) bm[m].st->done = 1;
+}
+// the inner solve's start: BF = R/|r|, its vectors zeroed
+__global__ void kb_start_f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  if (!M.active) return;
+  scale_to_f_body(M.q, M.S.indc, M.vd[BD_Y2], M.scale, M.vf[BF_B], lb_);
+  const long long slab = (long long)lb_ * ROWS_PER_BLOCK + (threadIdx.x >> 5);
+  if (slab < (long long)M.q.nb * M.q.W) {
+    const int zs[6] = {BF_X, BF_R0, BF_RR, BF_PV, BF_AP, BF_AE};
+    for (int t = threadIdx.x & 31; t < M.q.T; t += 32)
+      for (int c = 0; c < 6; ++c) M.vf[zs[c]][slab * M.q.T + t] = 0.0f;
+  }
+}
+__global__ void kb_dot_r0f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  dot_body<float>(M.q, M.S.indc, M.vf[BF_R0], M.vf[BF_R0], nullptr, nullptr, M.rb0, nullptr, M.st, lb_);
+}
+__global__ void kb_copy2_f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  copy2_body<float>(M.q, M.S.indc, M.vf[BF_R0], M.vf[BF_RR], M.vf[BF_PV], M.st, lb_);
+}
+__global__ void kb_axpyf(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  axpyf_body(M.q, M.vf[BF_AP], M.vf[BF_RR], M.st, lb_);
+}
+__global__ void kb_upd3f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  upd3f_body(M.q, M.vf[BF_AE], M.vf[BF_AP], M.vf[BF_X], M.vf[BF_RR], M.vf[BF_PV], M.st, lb_);
+}
+// XW += |r| D on the members whose inner solve ended within ICGMAX
+__global__ void kb_add_f(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  if (!M.active || M.st->iter < 0 || M.st->iter > M.icgmax) return;
+  add_f_body(M.q, M.S.indc, M.vf[BF_X], M.rn, M.vd[BD_X], lb_);
+}
+__global__ void kb_x0(const BatchMember *bm, const int *pre, int nm) {
+  pdl_enter();
+  BATCH_BLOCK(BR_SLAB)
+  if (!M.active) return;
+  x0_body(M.g, M.q, M.S.indc, M.vd[BD_X], M.pt, M.st, lb_);
+}
+#undef BATCH_BLOCK
+
+static inline dim3 bgrid(long long n) { return dim3((unsigned)n); }
+void launch_b_to_skew(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nblk) {
+  launch_pdl(kb_to_skew, bgrid(nblk), dim3(BATCH_ELEM), 0, s, 1, bm, pre, nm);
+}
+void launch_b_sys_to_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nblk) {
+  launch_pdl(kb_sys_to_f, bgrid(nblk), dim3(BATCH_ELEM), 0, s, 1, bm, pre, nm);
+}
+bool launch_b_dcmp_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long ntiles, int T) {
+  const int d = ring_depth(7, T, sizeof(float));
+  const size_t bytes = ring_bytes(7, T, d + 3, sizeof(float));
+  switch (d) {
+#define BDCMP(DD)                                                                          \
+  case DD:                                                                                 \
+    set_smem(kb_dcmp_f<DD>, bytes);                                                        \
+    launch_pdl(kb_dcmp_f<DD>, bgrid(ntiles), dim3(T), bytes, s, 1, bm, pre, nm);          \
+    return true;
+    BDCMP(8) BDCMP(4) BDCMP(2) BDCMP(1)
+#undef BDCMP
+    default: return false;
+  }
+}
+// The batched FP32 sweeps: two blocks per SM (the rule of launch_sweep,
+// counted over all the members' tiles) or one, ring depths 2..4.
+static int b_sweep_depth(const SkewGeo &q, int mode, bool two) {
+  return two ? sweep_depth2(q, mode, 4) : std::min(sweep_depth(q, mode, 4), 4);
+}
+static bool b_two(const SkewGeo &q, int nsm, int occ, long long ntiles) {
+  return occ == 2 || (occ == 0 && ntiles >= 2LL * nsm);
+}
+bool b_sweeps_supported(const SkewGeo &q, int nsm, int occ, long long ntiles) {
+  if (q.split != 1 || sweep_threads(q.T) > 512) return false;
+  const bool two = b_two(q, nsm, occ, ntiles) && sweep_threads(q.T) <= SWEEP2_THREADS;
+  for (int mode : {(int)SWEEP_FWD, (int)SWEEP_FWD_AX, (int)SWEEP_BWD, (int)SWEEP_BWD1, (int)SWEEP_BWD5})
+    if (b_sweep_depth(q, mode, two) < 2) return false;
+  return true;
+}
+template <int MODE>
+static bool launch_b_sweep_t(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long ntiles,
+                             const SkewGeo &q, int vin, int vout, int vin2, int rb5, int nsm, int occ) {
+  const bool two = b_two(q, nsm, occ, ntiles) && sweep_threads(q.T) <= SWEEP2_THREADS;
+  const int d = b_sweep_depth(q, MODE, two);
+  if (d < 2) return false;
+  const size_t bytes = sweep_bytes(q, MODE, d, 4);
+  const dim3 block((unsigned)sweep_threads(q.T));
+  switch (d * 2 + (two ? 1 : 0)) {
+#define BSWEEP(DD, TWO, MT, MB)                                                                        \
+  case DD * 2 + TWO:                                                                                   \
+    set_smem(kb_sweep<DD, MODE, MT, MB>, bytes);                                                       \
+    launch_pdl(kb_sweep<DD, MODE, MT, MB>, bgrid(ntiles), block, bytes, s, 1, bm, pre, nm, vin, vout, vin2, rb5); \
+    return true;
+    BSWEEP(2, 1, SWEEP2_THREADS, 2) BSWEEP(3, 1, SWEEP2_THREADS, 2) BSWEEP(4, 1, SWEEP2_THREADS, 2)
+    BSWEEP(2, 0, 512, 1) BSWEEP(3, 0, 512, 1) BSWEEP(4, 0, 512, 1)
+#undef BSWEEP
+    default: return false;
+  }
+}
+bool launch_b_sweep(cudaStream_t s, int mode, const BatchMember *bm, const int *pre, int nm, long long ntiles,
+                    const SkewGeo &q, int vin, int vout, int vin2, bool rb5, int nsm, int occ) {
+  switch (mode) {
+    case SWEEP_FWD: return launch_b_sweep_t<SWEEP_FWD>(s, bm, pre, nm, ntiles, q, vin, vout, vin2, rb5, nsm, occ);
+    case SWEEP_FWD_AX:
+      return launch_b_sweep_t<SWEEP_FWD_AX>(s, bm, pre, nm, ntiles, q, vin, vout, vin2, rb5, nsm, occ);
+    case SWEEP_BWD: return launch_b_sweep_t<SWEEP_BWD>(s, bm, pre, nm, ntiles, q, vin, vout, vin2, rb5, nsm, occ);
+    case SWEEP_BWD1: return launch_b_sweep_t<SWEEP_BWD1>(s, bm, pre, nm, ntiles, q, vin, vout, vin2, rb5, nsm, occ);
+    case SWEEP_BWD5: return launch_b_sweep_t<SWEEP_BWD5>(s, bm, pre, nm, ntiles, q, vin, vout, vin2, rb5, nsm, occ);
+    default: return false;
+  }
+}
+// one thread per member
+static inline dim3 bmem(int nm) { return dim3((unsigned)((nm + 255) / 256)); }
+void launch_b_clear(cudaStream_t s, const BatchMember *bm, int nm) {
+  launch_pdl(kb_clear, bmem(nm), dim3(256), 0, s, 1, bm, nm);
+}
+void launch_b_gather(cudaStream_t s, const BatchMember *bm, int nm, double *out) {
+  launch_pdl(kb_gather, bmem(nm), dim3(256), 0, s, 1, bm, nm, out);
+}
+void launch_b_residual(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) {
+  for (int part = 0; part < 3; ++part)
+    launch_pdl(kb_residual, bgrid(nslab), dim3(ROW_THREADS), 0, s, 1, bm, pre, nm, part);
+}
+void launch_b_fin(cudaStream_t s, int mode, const BatchMember *bm, int nm, bool tile_partials) {
+  launch_pdl(kb_fin, dim3((unsigned)nm), dim3(1024), 0, s, 1, bm, nm, mode, tile_partials ? 1 : 0);
+}
+void launch_b_fin5(cudaStream_t s, const BatchMember *bm, int nm) {
+  launch_pdl(kb_fin5, dim3((unsigned)nm), dim3(1024), 0, s, 1, bm, nm);
+}
+void launch_b_commit(cudaStream_t s, const BatchMember *bm, int nm) {
+  launch_pdl(kb_commit, bmem(nm), dim3(256), 0, s, 1, bm, nm);
+}
+#define BSL(kern) launch_pdl(kern, bgrid(nslab), dim3(ROW_THREADS), 0, s, 1, bm, pre, nm)
+void launch_b_start_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_start_f); }
+void launch_b_dot_r0f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_dot_r0f); }
+void launch_b_copy2_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_copy2_f); }
+void launch_b_axpyf(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_axpyf); }
+void launch_b_upd3f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_upd3f); }
+void launch_b_add_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_add_f); }
+void launch_b_x0(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab) { BSL(kb_x0); }
+#undef BSL
 
 }  // namespace cadmas

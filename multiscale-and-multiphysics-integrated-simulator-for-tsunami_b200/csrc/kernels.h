@@ -191,6 +191,40 @@ __host__ __device__ inline bool sweep_copy(const SkewGeo &q, int mode, int b, in
   return true;
 }
 
+// ---- batched solves of several grids (cadmas_batch_*) ----------------
+// One launch of a solver kernel covers the members of a batch: its blocks
+// are the members' blocks one after another (tiles for the sweeps and the
+// factorisation, slab blocks for the vector kernels, blocks of 256 layout
+// entries for the conversions), a block finding its member in the
+// prefix table and running the member's kernel body with its block index
+// inside the member.  BatchMember is a member's part of the solve.
+enum BatchVecF { BF_B = 0, BF_X, BF_R0, BF_RR, BF_PV, BF_AP, BF_AE, BF_Y2, BF_N };
+enum BatchVecD { BD_B = 0, BD_X, BD_Y2, BD_N };
+enum BatchRange { BR_TILE = 0, BR_SLAB = 1, BR_ELEM = 2, BR_N = 3 };
+constexpr int BATCH_ELEM = 256;  // layout entries per block of the conversions
+struct BatchMember {
+  Geo g;
+  SkewGeo q;
+  SkewSys S;       // FP64 system, INDC (skewed)
+  SkewSysF Sf;     // FP32 system
+  SysPtr a;        // the step's Poisson system (standard layout)
+  const int *indc; // INDC (standard layout)
+  double *pt;      // PT (standard layout): the initial guess in, the solution out
+  float *vf[BF_N];
+  double *vd[BD_N];
+  double *rb0, *rb1, *rb5, *dres;
+  SolveState *st;
+  int *pivot_bad;
+  long long nrb;   // slab blocks of the member (partials of its slab sums)
+  double epsa2, div2, tol2;
+  double scale, rn, eps2;  // the refinement pass: 1/|r|, |r|, inner tolerance squared
+  double U;                // MILU relaxation (CGPARA when ICGTYP != 0)
+  int icgmax, warm, active, pad;
+};
+// gathered per member after a kernel sequence: done, timeout, iter,
+// pivot_bad, the two stored sums (dres[6], dres[7])
+constexpr int BATCH_GATHER = 6;
+
 enum FinMode { FIN_BNORM = 0, FIN_START = 1, FIN_STORE = 2, FIN_RELRES = 3,
                FIN_ALPHA = 10, FIN_OMEGA = 11, FIN_CONV = 12 };
 
@@ -256,6 +290,29 @@ void launch_bwd(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSys &S
 void launch_fwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, const float *y,
                   const float *spmv_x, SolveState *st, float *ybuf);
 void launch_bwd_f(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysF &S, float *x, SolveState *st);
+// batched launches (k_poisson.cu); pre = the members' first blocks per
+// BatchRange, (nm + 1) entries each, on the device; nblk the total blocks
+void launch_b_to_skew(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nblk);
+void launch_b_sys_to_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nblk);
+bool launch_b_dcmp_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long ntiles, int T);
+// FP32 sweep of MODE over the members' tiles: vin, vout, vin2 select
+// float vectors (-1: none), rb5 selects rb5 for the sums (else rb0)
+bool launch_b_sweep(cudaStream_t s, int mode, const BatchMember *bm, const int *pre, int nm, long long ntiles,
+                    const SkewGeo &qref, int vin, int vout, int vin2, bool rb5, int nsm, int occ);
+bool b_sweeps_supported(const SkewGeo &qref, int nsm, int occ, long long ntiles);
+void launch_b_clear(cudaStream_t s, const BatchMember *bm, int nm);
+void launch_b_gather(cudaStream_t s, const BatchMember *bm, int nm, double *out);
+void launch_b_residual(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_fin(cudaStream_t s, int mode, const BatchMember *bm, int nm, bool tile_partials);
+void launch_b_fin5(cudaStream_t s, const BatchMember *bm, int nm);
+void launch_b_commit(cudaStream_t s, const BatchMember *bm, int nm);
+void launch_b_start_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_dot_r0f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_copy2_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_axpyf(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_upd3f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_add_f(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
+void launch_b_x0(cudaStream_t s, const BatchMember *bm, const int *pre, int nm, long long nslab);
 // the FP32 backward sweep with the inner products after it summed on the
 // way, one partial per tile (rb + c*nb); false when not available for the
 // layout (nothing launched)

@@ -20,3 +20,21 @@ def test_picks_the_fastest_and_caches(pkg, tmp_path):
     assert at.pick_tiles(c, cache=at.TileCache(tmp_path / "tiles.json"), measure=fake) == (16, 8)
     assert len(calls) == n
     assert cache.data[at.grid_key(c)]["s_per_step"]["16x8"] == 2.0
+
+
+def test_batch_shape_is_timed_on_the_whole_batch(pkg):
+    """The batch tuner times every candidate on all the grids together (one
+    call per shape with every case) and keeps the fastest; refused shapes
+    are skipped."""
+    at = importlib.import_module("cadmas_b200.autotune")
+    cases = [pkg.cases.random_tank(s) for s in range(3)]
+    seen = []
+
+    def fake(cs, ti, tj, **kw):
+        seen.append((len(cs), ti, tj))
+        return None if (ti, tj) == (32, 8) else {(16, 16): 1.5, (16, 8): 1.2, (8, 16): 1.4}[(ti, tj)]
+
+    tiles, timings = at.pick_batch_tiles(cases, measure=fake)
+    assert tiles == (16, 8)
+    assert all(n == 3 for n, _, _ in seen) and len(seen) == len(at.BATCH_CANDIDATES)
+    assert set(timings) == {"16x16", "16x8", "8x16"}

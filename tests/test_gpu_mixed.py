@@ -100,3 +100,41 @@ def test_inner_products_in_the_sweeps(gpu_lib, pkg, over):
     err = _errors(res[0][1], res[1][1])
     for k, v in err.items():
         assert v <= TOL[k], (k, v)
+
+
+def test_batch_matches_each_grid_alone(gpu_lib, pkg):
+    """A batch of grids of different sizes whose mixed pressure solves run
+    together (cadmas_batch_step: one launch per solver kernel over all the
+    grids, iterations in lockstep, converged grids skipped) gives each grid
+    bit for bit what it gives stepped alone, with the same iterations;
+    with the previous-step guess, over 8 steps."""
+    mk = lambda: [pkg.cases.porous_flume(nx=96 + 48 * i, ny=16 + 8 * (i % 2), nz=48 + 8 * i, depth=0.3,
+                                         block=(1.0, 1.3, 0.4), sponge_width=0.4) for i in range(4)]
+    kw = dict(solver=1, warm_start=1, precond_ti=16, precond_tj=8)
+    together = [pkg.Tank(c, **kw) for c in mk()]
+    alone = [pkg.Tank(c, **kw) for c in mk()]
+    for t in together + alone:
+        t.init_state(True)
+    batch = pkg.Batch(together)
+    for _ in range(8):
+        assert batch.step() == [0] * len(together)
+        for t in alone:
+            t.step()
+        for a, b in zip(together, alone):
+            assert a.stats()["icgitr"] == b.stats()["icgitr"]
+    batch.close()
+    for a, b in zip(together, alone):
+        sa, sb = a.get_state(), b.get_state()
+        for k in ("uu", "vv", "ww", "pp", "ff", "nf"):
+            assert sa[k].tobytes() == sb[k].tobytes(), k
+        assert a.stats()["fallbacks"] == b.stats()["fallbacks"] == 0
+
+
+def test_batch_rejects_mismatched_handles(gpu_lib, pkg):
+    c = pkg.cases.porous_flume(nx=64, ny=16, nz=40, depth=0.3, block=(0.6, 0.8, 0.4), sponge_width=0.3)
+    a = pkg.Tank(c, solver=1, precond_ti=16, precond_tj=8)
+    b = pkg.Tank(c, solver=1, precond_ti=8, precond_tj=8)
+    p = pkg.Tank(c, solver=0, precond_ti=16, precond_tj=8)
+    for bad in ([a, b], [a, p], [a, a]):
+        with pytest.raises(pkg.CadmasError):
+            pkg.Batch(bad)
