@@ -447,7 +447,10 @@ def run_ours(args, rank, world, local_rank):
 
 # Algorithmic bytes per interior cell of the FP32 sweeps of the mixed
 # solver (the same arrays as the FP64 ones, 4 B each).
-STAGE_BYTES_F32 = {"fwd": 10 * 4, "bwd": 6 * 4}
+# the mixed solver's FP32 sweeps: the fused forward sweep; the backward
+# sweeps with their sums (R0 read by the one after AP, R0 and RR by the one
+# after AE: 7 and 8 arrays, 7.5 on average)
+STAGE_BYTES_F32 = {"fwd": 10 * 4, "bwd": 7.5 * 4}
 
 
 def roofline_of(stages, cells, peak, peak_kind, bytes_table, traffic_per_cell=None):
@@ -467,11 +470,15 @@ def roofline_of(stages, cells, peak, peak_kind, bytes_table, traffic_per_cell=No
             "share_of_step": ms_dom / total_ms if total_ms else None}
 
 
-# DRAM bytes per interior cell of one launch of the dominant sweeps on the
-# beach (1024x128x128, 16x16 tiles), from ncu captures of a smaller beach
-# of the same tile shape (traffic per launch scales with the cells).
-NCU_TRAFFIC_BEACH = {"fwd": None, "bwd": None}
-NCU_TRAFFIC_BEACH_F32 = {"fwd": None, "bwd": None}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior
+# cell of one launch of the dominant sweeps on the beach (1024x128x128,
+# 16x16 tiles), from an ncu capture of a 1024x80x128 beach: the same
+# layers, tile shape and sweep variants (320 tiles, two blocks per SM for
+# the backward and FP32 sweeps), so the traffic per launch scales with the
+# cells.  FP32 backward: the mean of the sweeps after AP (33.6) and after
+# AE (38.8).
+NCU_TRAFFIC_BEACH = {"fwd": 99.8, "bwd": 57.9}
+NCU_TRAFFIC_BEACH_F32 = {"fwd": 49.9, "bwd": 36.2}
 
 
 def field_errors(a, b, case):
