@@ -957,8 +957,9 @@ def main():
     ap.add_argument("--acc-steps", type=int, default=200,
                     help="--case beach: steps after which the mixed run's fields are compared with the "
                          "plain run's")
-    ap.add_argument("--eps-inner", type=float, default=1.0e-3,
-                    help="floor of the FP32 inner tolerance of the mixed solver")
+    ap.add_argument("--eps-inner", type=float, default=1.0e-2,
+                    help="floor of the FP32 inner tolerance of the mixed solver (1e-2 measured best on the "
+                         "beach: fewer inner iterations in all than with tighter floors)")
     ap.add_argument("--occ", type=int, choices=[0, 1, 2], default=0,
                     help="thread blocks of the MILU sweeps per SM (0: the library's default)")
     ap.add_argument("--dot-passes", type=int, choices=[0, 1], default=0,
