@@ -62,10 +62,11 @@ STAGE_BYTES = {
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior
-# cell of one launch of each stage's dominant kernel, from an ncu capture of
-# the 256x32x96 flume with 16x16 tiles; the bench size has the same tile
-# shape, so the traffic per launch scales with the cells.
-NCU_TRAFFIC_PER_CELL = {"fwd": 97.4, "bwd": 52.6}
+# cell of one launch of each stage's dominant kernel, from ncu captures of
+# the 256x32x96 flume with 16x16 and 8x16 blocks (the same sweep variants
+# as the bench's 512x32x96, one block per SM), so the traffic per launch
+# scales with the cells.
+NCU_TRAFFIC_PER_CELL = {(16, 16): {"fwd": 97.4, "bwd": 52.6}, (8, 16): {"fwd": 91.0, "bwd": 50.3}}
 
 
 def _load_pkg():
@@ -405,8 +406,8 @@ def run_ours(args, rank, world, local_rank):
     total_ms = sum(v[0] for v in stages.values())
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": (NCU_TRAFFIC_PER_CELL[dom] * case.interior_cells
-                            if dom in NCU_TRAFFIC_PER_CELL and (args.ti, args.tj) == (16, 16) else None),
+                "traffic": (NCU_TRAFFIC_PER_CELL[(args.ti, args.tj)][dom] * case.interior_cells
+                            if dom in NCU_TRAFFIC_PER_CELL.get((args.ti, args.tj), {}) else None),
                 "algorithmic_bytes_per_launch": bytes_launch, "launches": n_dom,
                 "avg_launch_ms": ms_dom / n_dom if n_dom else None,
                 "share_of_step": ms_dom / total_ms if total_ms else None}
@@ -979,11 +980,19 @@ def main():
     ap.add_argument("--nx", type=int, default=512)
     ap.add_argument("--ny", type=int, default=32)
     ap.add_argument("--nz", type=int, default=96)
-    ap.add_argument("--ti", type=int, default=16)
-    ap.add_argument("--tj", type=int, default=16)
+    ap.add_argument("--ti", type=int, default=None,
+                    help="preconditioner block columns along x (default: 8 for --case flume, 16 otherwise)")
+    ap.add_argument("--tj", type=int, default=None,
+                    help="preconditioner block columns along y (default: 16)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    # block shapes measured best per workload: the flume's 512x32 columns
+    # make 128 blocks of 8x16 for the 148 SMs against 64 of 16x16
+    if args.ti is None:
+        args.ti = 8 if args.case == "flume" else 16
+    if args.tj is None:
+        args.tj = 16
     if args.guess is None:
         args.guess = "previous" if args.case == "beach" else "zero"
     world = int(os.environ.get("WORLD_SIZE", "1"))
