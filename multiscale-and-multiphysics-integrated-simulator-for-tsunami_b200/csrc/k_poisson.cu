@@ -511,11 +511,20 @@ __device__ __forceinline__ void cluster_barrier() {
 // and their evaluation order are those of the reference loops, so the
 // results do not change.  The step loop is unrolled by the ring length so
 // slot addresses and mbarrier phases are constants.
-template <int D, int MODE, typename V, int CS>
-__device__ __forceinline__ void sweep_body(const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *vin,
+// CT, CTIP: the layout tile's T and TIp at compile time (0: from q), so
+// that the slot offsets of a common tile shape are immediates and take no
+// registers.
+template <int D, int MODE, typename V, int CS, int CT = 0, int CTIP = 0>
+__device__ __forceinline__ void sweep_body(const Geo &g, const SkewGeo &q_, const SkewSysT<V> &S, const V *vin,
                                            V *vout, SolveState *st, const V *vin2, double *rb, int bx, int by) {
   constexpr bool BWD = MODE >= SWEEP_BWD;
   constexpr int NDOT = sweep_ndot(MODE);
+  SkewGeo q = q_;
+  if (CT > 0) {
+    q.T = CT;
+    q.TIp = CTIP;
+    q.TJ = CT / CTIP;
+  }
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
   // preconditioner block; every block of a cluster runs through the two
   // cluster barriers below, so none returns early.
@@ -809,11 +818,11 @@ __device__ __forceinline__ void sweep_body(const Geo &g, const SkewGeo &q, const
   }
   if (CS == 2) cluster_barrier();  // the partner may still write into this block's shared memory
 }
-template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1>
+template <int D, int MODE, int MAXT, typename V, int CS, int MINB = 1, int CT = 0, int CTIP = 0>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_sweep(Geo g, SkewGeo q, SkewSysT<V> S, const V *vin, V *vout, SolveState *st, const V *vin2, double *rb) {
   pdl_enter();
-  sweep_body<D, MODE, V, CS>(g, q, S, vin, vout, st, vin2, rb, (int)blockIdx.x, (int)blockIdx.y);
+  sweep_body<D, MODE, V, CS, CT, CTIP>(g, q, S, vin, vout, st, vin2, rb, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 // ------------------------------------------------------------ slab kernels
@@ -1447,7 +1456,10 @@ static int sweep_depth(const SkewGeo &q, int mode, int es) {
 constexpr int SWEEP2_THREADS = 288;
 static int sweep_depth2(const SkewGeo &q, int mode, int es) {
   if (q.split != 1 || sweep_threads(q.T) > SWEEP2_THREADS) return 0;
-  const int dmax = (mode == SWEEP_FWD_AX || mode == SWEEP_BWD5) ? 3 : 4;
+  // 16x16 tiles run the instances with the tile's constants compiled in,
+  // which leave room for depth 4 everywhere
+  const bool t256 = q.T == 256 && q.TIp == 16;
+  const int dmax = (!t256 && (mode == SWEEP_FWD_AX || mode == SWEEP_BWD5)) ? 3 : 4;
   for (int d : {4, 3, 2})
     if (d <= dmax && sweep_bytes(q, mode, d, es) <= 113 * 1024) return d;
   return 0;
@@ -1458,6 +1470,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   constexpr int ES = (int)sizeof(V);
   const V *vnull = nullptr;
   double *rnull = nullptr;
+  const bool t256 = q.T == 256 && q.TIp == 16;  // 16x16 tiles: the shape's constants compiled in
   const int d = sweep_depth(q, MODE, ES);
   const size_t bytes = sweep_bytes(q, MODE, d, ES);
   const int nty = q.nb / q.ntx;
@@ -1495,8 +1508,15 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
       switch (d2) {
 #define SWEEP_CASE_OCC2(DD)                                                                            \
   case DD:                                                                                             \
-    set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, bytes2);                                      \
-    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, grid, block, bytes2, s, 1, g, q, S, vin, vout, st, vnull, rnull); \
+    if (t256) {                                                                                        \
+      set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2, 256, 16>, bytes2);                           \
+      launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2, 256, 16>, grid, block, bytes2, s, 1, g, q, S, vin, vout, \
+                 st, vnull, rnull);                                                                    \
+    } else {                                                                                           \
+      set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, bytes2);                                    \
+      launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, V, 1, 2>, grid, block, bytes2, s, 1, g, q, S, vin, vout, st, vnull, \
+                 rnull);                                                                               \
+    }                                                                                                  \
     return;
         SWEEP_CASE_OCC2(4) SWEEP_CASE_OCC2(3) SWEEP_CASE_OCC2(2)
 #undef SWEEP_CASE_OCC2
@@ -1507,8 +1527,15 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   switch (d * 4096 + mt) {
 #define SWEEP_CASE(DD, MT)                                                              \
   case DD * 4096 + MT:                                                                  \
-    set_smem(k_sweep<DD, MODE, MT, V, 1>, bytes);                                       \
-    launch_pdl(k_sweep<DD, MODE, MT, V, 1>, grid, block, bytes, s, 1, g, q, S, vin, vout, st, vnull, rnull); \
+    if (MT == 512 && t256) {                                                            \
+      constexpr int CT_ = MT == 512 ? 256 : 0, CI_ = MT == 512 ? 16 : 0;                \
+      set_smem(k_sweep<DD, MODE, MT, V, 1, 1, CT_, CI_>, bytes);                        \
+      launch_pdl(k_sweep<DD, MODE, MT, V, 1, 1, CT_, CI_>, grid, block, bytes, s, 1, g, q, S, vin, vout, st, vnull, \
+                 rnull);                                                                \
+    } else {                                                                            \
+      set_smem(k_sweep<DD, MODE, MT, V, 1>, bytes);                                     \
+      launch_pdl(k_sweep<DD, MODE, MT, V, 1>, grid, block, bytes, s, 1, g, q, S, vin, vout, st, vnull, rnull); \
+    }                                                                                   \
     break;
     SWEEP_CASE(8, 256) SWEEP_CASE(6, 256) SWEEP_CASE(4, 256) SWEEP_CASE(3, 256) SWEEP_CASE(2, 256)
     SWEEP_CASE(8, 512) SWEEP_CASE(6, 512) SWEEP_CASE(4, 512) SWEEP_CASE(3, 512) SWEEP_CASE(2, 512)
@@ -1563,6 +1590,7 @@ static bool launch_bwd_dots(cudaStream_t s, const Geo &g, const SkewGeo &q, cons
                             const float *rr, float *x, double *rb, SolveState *st) {
   constexpr int ES = 4;
   if (q.split != 1) return false;
+  const bool t256 = q.T == 256 && q.TIp == 16;
   const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
   const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm);
   if (two) {
@@ -1571,8 +1599,14 @@ static bool launch_bwd_dots(cudaStream_t s, const Geo &g, const SkewGeo &q, cons
     switch (d2) {
 #define DOTS_OCC2(DD)                                                                                              \
   case DD:                                                                                                         \
-    set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, bytes2);                                              \
-    launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, grid, block, bytes2, s, 1, g, q, S, r0, x, st, rr, rb); \
+    if (t256) {                                                                                                    \
+      set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2, 256, 16>, bytes2);                                   \
+      launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2, 256, 16>, grid, block, bytes2, s, 1, g, q, S, r0, x, \
+                 st, rr, rb);                                                                                      \
+    } else {                                                                                                       \
+      set_smem(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, bytes2);                                            \
+      launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, grid, block, bytes2, s, 1, g, q, S, r0, x, st, rr, rb); \
+    }                                                                                                              \
     return true;
       DOTS_OCC2(4) DOTS_OCC2(3) DOTS_OCC2(2)
 #undef DOTS_OCC2
@@ -1586,8 +1620,14 @@ static bool launch_bwd_dots(cudaStream_t s, const Geo &g, const SkewGeo &q, cons
   switch (d * 4096 + mt) {
 #define DOTS_CASE(DD, MT)                                                                            \
   case DD * 4096 + MT:                                                                               \
-    set_smem(k_sweep<DD, MODE, MT, float, 1>, bytes);                                                \
-    launch_pdl(k_sweep<DD, MODE, MT, float, 1>, grid, block, bytes, s, 1, g, q, S, r0, x, st, rr, rb); \
+    if (MT == 512 && t256) {                                                                         \
+      constexpr int CT_ = MT == 512 ? 256 : 0, CI_ = MT == 512 ? 16 : 0;                             \
+      set_smem(k_sweep<DD, MODE, MT, float, 1, 1, CT_, CI_>, bytes);                                 \
+      launch_pdl(k_sweep<DD, MODE, MT, float, 1, 1, CT_, CI_>, grid, block, bytes, s, 1, g, q, S, r0, x, st, rr, rb); \
+    } else {                                                                                         \
+      set_smem(k_sweep<DD, MODE, MT, float, 1>, bytes);                                              \
+      launch_pdl(k_sweep<DD, MODE, MT, float, 1>, grid, block, bytes, s, 1, g, q, S, r0, x, st, rr, rb); \
+    }                                                                                                \
     return true;
     DOTS_CASE(4, 256) DOTS_CASE(3, 256) DOTS_CASE(2, 256) DOTS_CASE(4, 512) DOTS_CASE(3, 512) DOTS_CASE(2, 512)
 #undef DOTS_CASE
@@ -1750,12 +1790,12 @@ __global__ void kb_dcmp_f(const BatchMember *bm, const int *pre, int nm) {
   if (!M.active) return;
   dcmp_body<D, float>(M.g, M.q, (float)M.U, M.Sf, M.pivot_bad, (int)(lb_ % M.q.ntx), (int)(lb_ / M.q.ntx));
 }
-template <int D, int MODE, int MAXT, int MINB>
+template <int D, int MODE, int MAXT, int MINB, int CT = 0, int CTIP = 0>
 __global__ void __launch_bounds__(MAXT, MINB) kb_sweep(const BatchMember *bm, const int *pre, int nm, int vin,
                                                        int vout, int vin2, int rb5) {
   pdl_enter();
   BATCH_BLOCK(BR_TILE)
-  sweep_body<D, MODE, float, 1>(M.g, M.q, M.Sf, vin >= 0 ? M.vf[vin] : nullptr, vout >= 0 ? M.vf[vout] : nullptr,
+  sweep_body<D, MODE, float, 1, CT, CTIP>(M.g, M.q, M.Sf, vin >= 0 ? M.vf[vin] : nullptr, vout >= 0 ? M.vf[vout] : nullptr,
                                 M.st, vin2 >= 0 ? M.vf[vin2] : nullptr, rb5 ? M.rb5 : M.rb0,
                                 (int)(lb_ % M.q.ntx), (int)(lb_ / M.q.ntx));
 }
@@ -1897,13 +1937,20 @@ static bool launch_b_sweep_t(cudaStream_t s, const BatchMember *bm, const int *p
   const bool two = b_two(q, nsm, occ, ntiles) && sweep_threads(q.T) <= SWEEP2_THREADS;
   const int d = b_sweep_depth(q, MODE, two);
   if (d < 2) return false;
+  const bool t256 = q.T == 256 && q.TIp == 16;
   const size_t bytes = sweep_bytes(q, MODE, d, 4);
   const dim3 block((unsigned)sweep_threads(q.T));
   switch (d * 2 + (two ? 1 : 0)) {
 #define BSWEEP(DD, TWO, MT, MB)                                                                        \
   case DD * 2 + TWO:                                                                                   \
-    set_smem(kb_sweep<DD, MODE, MT, MB>, bytes);                                                       \
-    launch_pdl(kb_sweep<DD, MODE, MT, MB>, bgrid(ntiles), block, bytes, s, 1, bm, pre, nm, vin, vout, vin2, rb5); \
+    if (t256) {                                                                                        \
+      set_smem(kb_sweep<DD, MODE, MT, MB, 256, 16>, bytes);                                            \
+      launch_pdl(kb_sweep<DD, MODE, MT, MB, 256, 16>, bgrid(ntiles), block, bytes, s, 1, bm, pre, nm, vin, vout, \
+                 vin2, rb5);                                                                           \
+    } else {                                                                                           \
+      set_smem(kb_sweep<DD, MODE, MT, MB>, bytes);                                                     \
+      launch_pdl(kb_sweep<DD, MODE, MT, MB>, bgrid(ntiles), block, bytes, s, 1, bm, pre, nm, vin, vout, vin2, rb5); \
+    }                                                                                                  \
     return true;
     BSWEEP(2, 1, SWEEP2_THREADS, 2) BSWEEP(3, 1, SWEEP2_THREADS, 2) BSWEEP(4, 1, SWEEP2_THREADS, 2)
     BSWEEP(2, 0, 512, 1) BSWEEP(3, 0, 512, 1) BSWEEP(4, 0, 512, 1)
