@@ -1457,10 +1457,11 @@ constexpr int SWEEP2_THREADS = 288;
 static int sweep_depth2(const SkewGeo &q, int mode, int es) {
   if (q.split != 1 || sweep_threads(q.T) > SWEEP2_THREADS) return 0;
   // 16x16 tiles run the instances with the tile's constants compiled in,
-  // which leave room for depth 4 everywhere
+  // which leave room for depth 6 everywhere (8 measured no faster for the
+  // forward sweeps and slower for the backward ones)
   const bool t256 = q.T == 256 && q.TIp == 16;
-  const int dmax = (!t256 && (mode == SWEEP_FWD_AX || mode == SWEEP_BWD5)) ? 3 : 4;
-  for (int d : {4, 3, 2})
+  const int dmax = t256 ? 6 : ((mode == SWEEP_FWD_AX || mode == SWEEP_BWD5) ? 3 : 4);
+  for (int d : {6, 4, 3, 2})
     if (d <= dmax && sweep_bytes(q, mode, d, es) <= 113 * 1024) return d;
   return 0;
 }
@@ -1518,7 +1519,7 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
                  rnull);                                                                               \
     }                                                                                                  \
     return;
-        SWEEP_CASE_OCC2(4) SWEEP_CASE_OCC2(3) SWEEP_CASE_OCC2(2)
+        SWEEP_CASE_OCC2(6) SWEEP_CASE_OCC2(4) SWEEP_CASE_OCC2(3) SWEEP_CASE_OCC2(2)
 #undef SWEEP_CASE_OCC2
         default: break;
       }
@@ -1608,7 +1609,7 @@ static bool launch_bwd_dots(cudaStream_t s, const Geo &g, const SkewGeo &q, cons
       launch_pdl(k_sweep<DD, MODE, SWEEP2_THREADS, float, 1, 2>, grid, block, bytes2, s, 1, g, q, S, r0, x, st, rr, rb); \
     }                                                                                                              \
     return true;
-      DOTS_OCC2(4) DOTS_OCC2(3) DOTS_OCC2(2)
+      DOTS_OCC2(6) DOTS_OCC2(4) DOTS_OCC2(3) DOTS_OCC2(2)
 #undef DOTS_OCC2
       default: break;
     }
@@ -1953,6 +1954,7 @@ static bool launch_b_sweep_t(cudaStream_t s, const BatchMember *bm, const int *p
     }                                                                                                  \
     return true;
     BSWEEP(2, 1, SWEEP2_THREADS, 2) BSWEEP(3, 1, SWEEP2_THREADS, 2) BSWEEP(4, 1, SWEEP2_THREADS, 2)
+    BSWEEP(6, 1, SWEEP2_THREADS, 2)
     BSWEEP(2, 0, 512, 1) BSWEEP(3, 0, 512, 1) BSWEEP(4, 0, 512, 1)
 #undef BSWEEP
     default: return false;
