@@ -523,7 +523,7 @@ __device__ __forceinline__ void sweep_body(const Geo &g, const SkewGeo &q_, cons
   if (CT > 0) {
     q.T = CT;
     q.TIp = CTIP;
-    q.TJ = CT / CTIP;
+    q.TJ = CT / (CTIP > 0 ? CTIP : 1);
   }
   // CS = 2: the thread blocks of a cluster are the two layout tiles of one
   // preconditioner block; every block of a cluster runs through the two
