@@ -113,9 +113,18 @@ struct DropSums {
 // others hold the cleared values already (k_drop_start cleared every
 // non-droplet cell, and a droplet cell that runs dry is cleared in the
 // step that empties it).  Returns whether any F changed.
-template <int AX, class FGet, class FSet, class NGet>
+// next(s) gives the first position at or after s in walk order (s itself
+// when stepping through every cell) that may hold a droplet, or DROP_END:
+// the walk visits only those.  Skipping a stretch of cells that hold no
+// droplet changes nothing: such a cell only finishes its predecessor and
+// becomes the next cell's predecessor with no sums and unchanged F, which
+// the walk sets up again at the next droplet (F of a cell is changed only
+// by the walk's visits to it and to the cell after it, so a cell not yet
+// visited still holds its starting value).
+constexpr int DROP_END = -(1 << 30);
+template <int AX, class FGet, class FSet, class NGet, class Next>
 __device__ __forceinline__ bool drop_walk(const Geo &g, const Fld &f, const Prm &p, const DropArrays &d, int L, int I,
-                                          int J, int K, FGet F, FSet setF, NGet NFat) {
+                                          int J, int K, FGet F, FSet setF, NGet NFat, Next next) {
   const int NA = AX == 0 ? g.NI : (AX == 1 ? g.NJ : g.NK);
   const int lo = 2, hi = NA - 1, dl = (L == 1) ? -1 : 1;
   const int s0 = (L == 1) ? hi : lo, s1 = (L == 1) ? lo : hi;
@@ -152,7 +161,11 @@ __device__ __forceinline__ bool drop_walk(const Geo &g, const Fld &f, const Prm 
     }
     d.uu[c] = du; d.vv[c] = dv; d.ww[c] = dw;
   };
-  for (int s = s0;; s += dl) {
+  for (int s = next(s0); s != DROP_END; s = (s == s1) ? DROP_END : next(s + dl)) {
+    if (s - dl != q) {  // cells skipped since q: q is complete, s-dl is s's predecessor
+      finish(q, Fq, Nq, dq, Wq);
+      q = s - dl; Fq = F(q); Nq = NFat(q); dq = false; Wq = DropSums{0, 0, 0, 0, 0, 0, 0};
+    }
     const long long c = at(s);
     double Fs = F(s);
     const int Ns = NFat(s);
@@ -210,7 +223,6 @@ __device__ __forceinline__ bool drop_walk(const Geo &g, const Fld &f, const Prm 
     // the cell before is complete now
     finish(q, Fq, Nq, dq, Wq);
     q = s; Fq = Fs; Nq = Ns; dq = ds; Wq = W;
-    if (s == s1) break;
   }
   finish(q, Fq, Nq, dq, Wq);
   return any;
@@ -228,42 +240,90 @@ __global__ void k_drop_line(Geo g, Fld f, Prm p, DropArrays d, int L) {
   const int *NF = f.nf;
   auto at = [&](int s) -> long long { return AX == 1 ? cid(g, I, s, K) : cid(g, I, J, s); };
   drop_walk<AX>(g, f, p, d, L, I, J, K, [&](int s) { return FF[at(s)]; },
-                [&](int s, double v) { FF[at(s)] = v; }, [&](int s) { return NF[at(s)]; });
+                [&](int s, double v) { FF[at(s)] = v; }, [&](int s) { return NF[at(s)]; },
+                [](int s) { return s; });
 }
 
 // x lines: one warp per line (J,K); the warp stages the line's F and NF
-// (I = 1..NI) in shared memory, lane 0 walks it, the warp writes F back.
+// (I = 1..NI) in shared memory with a mask of its droplet cells (bit I-1),
+// and leaves the line at once when it holds none.  Lane 0 walks from
+// droplet to droplet; the warp writes F back if it changed.
 __global__ void k_drop_line_x(Geo g, Fld f, Prm p, DropArrays d, int L) {
   extern __shared__ __align__(16) double dsm[];
   const int NI = g.NI, lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int nw = (NI + 31) >> 5;
   const long long line = (long long)blockIdx.x * wpb + wib;
   const int nj = g.NJ - 2;
   if (line >= (long long)nj * (g.NK - 2)) return;
   const int J = 2 + (int)(line % nj), K = 2 + (int)(line / nj);
   double *Fs = dsm + (size_t)wib * NI;  // F(1..NI) at Fs[0..NI-1]
   int *Ns = reinterpret_cast<int *>(dsm + (size_t)wpb * NI) + (size_t)wib * NI;
+  unsigned *Ds = reinterpret_cast<unsigned *>(reinterpret_cast<int *>(dsm + (size_t)wpb * NI) + (size_t)wpb * NI) +
+                 (size_t)wib * nw;
   const long long row = cid(g, 1, J, K);
-  for (int i = lane; i < NI; i += 32) { Fs[i] = f.ff[row + i]; Ns[i] = f.nf[row + i]; }
+  const double FL = p.flower;
+  unsigned anyd = 0;
+  for (int base = 0; base < NI; base += 32) {
+    const int i = base + lane;
+    bool dr = false;
+    if (i < NI) {
+      const double fv = f.ff[row + i];
+      const int nv = f.nf[row + i];
+      Fs[i] = fv; Ns[i] = nv;
+      dr = i >= 1 && i <= NI - 2 && fv > FL && nv == 8;  // interior I = 2..NI-1
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, dr);
+    if (lane == 0) Ds[base >> 5] = m;
+    anyd |= m;
+  }
+  if (anyd == 0) return;  // the same for every lane of the warp
   __syncwarp();
   bool any = false;
-  if (lane == 0)
-    any = drop_walk<0>(g, f, p, d, L, 0, J, K, [&](int s) { return Fs[s - 1]; },
-                       [&](int s, double v) { Fs[s - 1] = v; }, [&](int s) { return Ns[s - 1]; });
+  if (lane == 0) {
+    // first droplet at or after position s in walk order (s = I)
+    auto next_up = [&](int s) -> int {  // L = 2: increasing I
+      if (s > NI - 1) return DROP_END;
+      int x = s - 1, w = x >> 5;
+      unsigned bits = Ds[w] & (0xffffffffu << (x & 31));
+      while (bits == 0) {
+        if (++w >= nw) return DROP_END;
+        bits = Ds[w];
+      }
+      return (w << 5) + __ffs(bits);  // (w*32 + bit) + 1
+    };
+    auto next_down = [&](int s) -> int {  // L = 1: decreasing I
+      if (s < 2) return DROP_END;
+      int x = s - 1, w = x >> 5;
+      unsigned bits = Ds[w] & (0xffffffffu >> (31 - (x & 31)));
+      while (bits == 0) {
+        if (--w < 0) return DROP_END;
+        bits = Ds[w];
+      }
+      return (w << 5) + (31 - __clz(bits)) + 1;
+    };
+    auto F = [&](int s) { return Fs[s - 1]; };
+    auto setF = [&](int s, double v) { Fs[s - 1] = v; };
+    auto NFat = [&](int s) { return Ns[s - 1]; };
+    any = (L == 1) ? drop_walk<0>(g, f, p, d, L, 0, J, K, F, setF, NFat, next_down)
+                   : drop_walk<0>(g, f, p, d, L, 0, J, K, F, setF, NFat, next_up);
+  }
   any = __shfl_sync(0xffffffffu, any, 0);
   __syncwarp();
   if (any)
     for (int i = lane; i < NI; i += 32) f.ff[row + i] = Fs[i];
 }
 
-// Warps per block of k_drop_line_x and its shared memory (F and NF of a
-// whole x line per warp).
+// Shared memory of one warp of k_drop_line_x: F and NF of a whole x line
+// and its droplet mask.
+static size_t drop_x_bytes(const Geo &g) { return (size_t)g.NI * 12 + (size_t)((g.NI + 31) / 32) * 4; }
+// Warps per block of k_drop_line_x.
 static int drop_x_warps(const Geo &g) {
-  const size_t per = (size_t)g.NI * 12;
+  const size_t per = drop_x_bytes(g);
   for (int w : {4, 2, 1})
     if (per * w <= 96 * 1024) return w;
   return 0;
 }
-bool drop_supported(const Geo &g) { return (size_t)g.NI * 12 <= 200 * 1024; }
+bool drop_supported(const Geo &g) { return drop_x_bytes(g) <= 200 * 1024; }
 
 void launch_fdropf(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, const DropArrays &d) {
   const long long ncell = (long long)(g.NI - 2) * (g.NJ - 2) * (g.NK - 2);
@@ -271,7 +331,7 @@ void launch_fdropf(cudaStream_t s, const Geo &g, const Fld &f, const Prm &p, con
   count_launch();
   int wpb = drop_x_warps(g);
   if (wpb == 0) wpb = 1;
-  const size_t xsm = (size_t)g.NI * 12 * wpb;
+  const size_t xsm = drop_x_bytes(g) * wpb;
   // the limit only rises (handles of other grids may be stepped from other
   // host threads at the same time)
   raise_dynamic_smem((const void *)k_drop_line_x, xsm);
