@@ -46,166 +46,187 @@ struct TanCtx {
   int S0;
 };
 
-__global__ void k_bsuwt(Geo g, Fld f, Prm p) {
+// The three face rules between surface and non-fluid cells, apart from
+// the common cases (gas on both sides: 0; fluid on a side: unchanged),
+// which the kernel handles inline with all its loads issued together.
+__device__ __noinline__ double bsuwt_x(const Geo &g, const int *NF, const double *UU, int S0, int I, int J, int K,
+                                       int NL, int NR) {
+  const int NI = g.NI, NJ = g.NJ, NK = g.NK;
+  (void)NI;
+  const int I1 = I - 1;
+  double DL = 0, VL = 0, DR = 0, VR = 0, V0;
+  if (NL == 3 || NR == 3) {
+    V0 = A(UU, I, J - 1, K);
+    if (S0) { int L1 = J - 1, L2 = J - 2;
+      if (L2 >= 1 && A(NF, I1, L1, K) != -1 && A(NF, I, L1, K) != -1)
+        if (A(NF, I1, L2, K) != -1 && A(NF, I, L2, K) != -1)
+          if (A(NF, I1, L2, K) == 0 || A(NF, I, L2, K) == 0)
+            V0 = V0 + (V0 - A(UU, I, L2, K)) * YY_(3, J) / YY_(3, L1); }
+    if (NL == 3) { DL = YY_(3, J); VL = V0; }
+    if (NR == 3) { DR = YY_(3, J); VR = V0; }
+  }
+  if (NL == 4 || NR == 4) {
+    V0 = A(UU, I, J + 1, K);
+    if (S0) { int L1 = J + 1, L2 = J + 2;
+      if (L2 <= NJ && A(NF, I1, L1, K) != -1 && A(NF, I, L1, K) != -1)
+        if (A(NF, I1, L2, K) != -1 && A(NF, I, L2, K) != -1)
+          if (A(NF, I1, L2, K) == 0 || A(NF, I, L2, K) == 0)
+            V0 = V0 + (V0 - A(UU, I, L2, K)) * YY_(3, L1) / YY_(3, L2); }
+    if (NL == 4) { DL = YY_(3, J + 1); VL = V0; }
+    if (NR == 4) { DR = YY_(3, J + 1); VR = V0; }
+  }
+  if (NL == 5 || NR == 5) {
+    V0 = A(UU, I, J, K - 1);
+    if (S0) { int L1 = K - 1, L2 = K - 2;
+      if (L2 >= 1 && A(NF, I1, J, L1) != -1 && A(NF, I, J, L1) != -1)
+        if (A(NF, I1, J, L2) != -1 && A(NF, I, J, L2) != -1)
+          if (A(NF, I1, J, L2) == 0 || A(NF, I, J, L2) == 0)
+            V0 = V0 + (V0 - A(UU, I, J, L2)) * ZZ_(3, K) / ZZ_(3, L1); }
+    if (NL == 5) { DL = ZZ_(3, K); VL = V0; }
+    if (NR == 5) { DR = ZZ_(3, K); VR = V0; }
+  }
+  if (NL == 6 || NR == 6) {
+    V0 = A(UU, I, J, K + 1);
+    if (S0) { int L1 = K + 1, L2 = K + 2;
+      if (L2 <= NK && A(NF, I1, J, L1) != -1 && A(NF, I, J, L1) != -1)
+        if (A(NF, I1, J, L2) != -1 && A(NF, I, J, L2) != -1)
+          if (A(NF, I1, J, L2) == 0 || A(NF, I, J, L2) == 0)
+            V0 = V0 + (V0 - A(UU, I, J, L2)) * ZZ_(3, L1) / ZZ_(3, L2); }
+    if (NL == 6) { DL = ZZ_(3, K + 1); VL = V0; }
+    if (NR == 6) { DR = ZZ_(3, K + 1); VR = V0; }
+  }
+  if (NL == 8) return VR;
+  if (NR == 8) return VL;
+  return (DR * VL + DL * VR) / (DR + DL);
+}
+__device__ __noinline__ double bsuwt_y(const Geo &g, const int *NF, const double *VV, int S0, int I, int J, int K,
+                                       int NL, int NR) {
+  const int NI = g.NI, NJ = g.NJ, NK = g.NK;
+  (void)NJ;
+  const int J1 = J - 1;
+  double DL = 0, VL = 0, DR = 0, VR = 0, V0;
+  if (NL == 1 || NR == 1) {
+    V0 = A(VV, I - 1, J, K);
+    if (S0) { int L1 = I - 1, L2 = I - 2;
+      if (L2 >= 1 && A(NF, L1, J1, K) != -1 && A(NF, L1, J, K) != -1)
+        if (A(NF, L2, J1, K) != -1 && A(NF, L2, J, K) != -1)
+          if (A(NF, L2, J1, K) == 0 || A(NF, L2, J, K) == 0)
+            V0 = V0 + (V0 - A(VV, L2, J, K)) * XX_(3, I) / XX_(3, L1); }
+    if (NL == 1) { DL = XX_(3, I); VL = V0; }
+    if (NR == 1) { DR = XX_(3, I); VR = V0; }
+  }
+  if (NL == 2 || NR == 2) {
+    V0 = A(VV, I + 1, J, K);
+    if (S0) { int L1 = I + 1, L2 = I + 2;
+      if (L2 <= NI && A(NF, L1, J1, K) != -1 && A(NF, L1, J, K) != -1)
+        if (A(NF, L2, J1, K) != -1 && A(NF, L2, J, K) != -1)
+          if (A(NF, L2, J1, K) == 0 || A(NF, L2, J, K) == 0)
+            V0 = V0 + (V0 - A(VV, L2, J, K)) * XX_(3, L1) / XX_(3, L2); }
+    if (NL == 2) { DL = XX_(3, I + 1); VL = V0; }
+    if (NR == 2) { DR = XX_(3, I + 1); VR = V0; }
+  }
+  if (NL == 5 || NR == 5) {
+    V0 = A(VV, I, J, K - 1);
+    if (S0) { int L1 = K - 1, L2 = K - 2;
+      if (L2 >= 1 && A(NF, I, J1, L1) != -1 && A(NF, I, J, L1) != -1)
+        if (A(NF, I, J1, L2) != -1 && A(NF, I, J, L2) != -1)
+          if (A(NF, I, J1, L2) == 0 || A(NF, I, J, L2) == 0)
+            V0 = V0 + (V0 - A(VV, I, J, L2)) * ZZ_(3, K) / ZZ_(3, L1); }
+    if (NL == 5) { DL = ZZ_(3, K); VL = V0; }
+    if (NR == 5) { DR = ZZ_(3, K); VR = V0; }
+  }
+  if (NL == 6 || NR == 6) {
+    V0 = A(VV, I, J, K + 1);
+    if (S0) { int L1 = K + 1, L2 = K + 2;
+      if (L2 <= NK && A(NF, I, J1, L1) != -1 && A(NF, I, J, L1) != -1)
+        if (A(NF, I, J1, L2) != -1 && A(NF, I, J, L2) != -1)
+          if (A(NF, I, J1, L2) == 0 || A(NF, I, J, L2) == 0)
+            V0 = V0 + (V0 - A(VV, I, J, L2)) * ZZ_(3, L1) / ZZ_(3, L2); }
+    if (NL == 6) { DL = ZZ_(3, K + 1); VL = V0; }
+    if (NR == 6) { DR = ZZ_(3, K + 1); VR = V0; }
+  }
+  if (NL == 8) return VR;
+  if (NR == 8) return VL;
+  return (DR * VL + DL * VR) / (DR + DL);
+}
+__device__ __noinline__ double bsuwt_z(const Geo &g, const int *NF, const double *WW, int S0, int I, int J, int K,
+                                       int NL, int NR) {
+  const int NI = g.NI, NJ = g.NJ, NK = g.NK;
+  (void)NK;
+  const int K1 = K - 1;
+  double DL = 0, VL = 0, DR = 0, VR = 0, V0;
+  if (NL == 1 || NR == 1) {
+    V0 = A(WW, I - 1, J, K);
+    if (S0) { int L1 = I - 1, L2 = I - 2;
+      if (L2 >= 1 && A(NF, L1, J, K1) != -1 && A(NF, L1, J, K) != -1)
+        if (A(NF, L2, J, K1) != -1 && A(NF, L2, J, K) != -1)
+          if (A(NF, L2, J, K1) == 0 || A(NF, L2, J, K) == 0)
+            V0 = V0 + (V0 - A(WW, L2, J, K)) * XX_(3, I) / XX_(3, L1); }
+    if (NL == 1) { DL = XX_(3, I); VL = V0; }
+    if (NR == 1) { DR = XX_(3, I); VR = V0; }
+  }
+  if (NL == 2 || NR == 2) {
+    V0 = A(WW, I + 1, J, K);
+    if (S0) { int L1 = I + 1, L2 = I + 2;
+      if (L2 <= NI && A(NF, L1, J, K1) != -1 && A(NF, L1, J, K) != -1)
+        if (A(NF, L2, J, K1) != -1 && A(NF, L2, J, K) != -1)
+          if (A(NF, L2, J, K1) == 0 || A(NF, L2, J, K) == 0)
+            V0 = V0 + (V0 - A(WW, L2, J, K)) * XX_(3, L1) / XX_(3, L2); }
+    if (NL == 2) { DL = XX_(3, I + 1); VL = V0; }
+    if (NR == 2) { DR = XX_(3, I + 1); VR = V0; }
+  }
+  if (NL == 3 || NR == 3) {
+    V0 = A(WW, I, J - 1, K);
+    if (S0) { int L1 = J - 1, L2 = J - 2;
+      if (L2 >= 1 && A(NF, I, L1, K1) != -1 && A(NF, I, L1, K) != -1)
+        if (A(NF, I, L2, K1) != -1 && A(NF, I, L2, K) != -1)
+          if (A(NF, I, L2, K1) == 0 || A(NF, I, L2, K) == 0)
+            V0 = V0 + (V0 - A(WW, I, L2, K)) * YY_(3, J) / YY_(3, L1); }
+    if (NL == 3) { DL = YY_(3, J); VL = V0; }
+    if (NR == 3) { DR = YY_(3, J); VR = V0; }
+  }
+  if (NL == 4 || NR == 4) {
+    V0 = A(WW, I, J + 1, K);
+    if (S0) { int L1 = J + 1, L2 = J + 2;
+      if (L2 <= NJ && A(NF, I, L1, K1) != -1 && A(NF, I, L1, K) != -1)
+        if (A(NF, I, L2, K1) != -1 && A(NF, I, L2, K) != -1)
+          if (A(NF, I, L2, K1) == 0 || A(NF, I, L2, K) == 0)
+            V0 = V0 + (V0 - A(WW, I, L2, K)) * YY_(3, L1) / YY_(3, L2); }
+    if (NL == 4) { DL = YY_(3, J + 1); VL = V0; }
+    if (NR == 4) { DR = YY_(3, J + 1); VR = V0; }
+  }
+  if (NL == 8) return VR;
+  if (NR == 8) return VL;
+  return (DR * VL + DL * VR) / (DR + DL);
+}
+
+__global__ void __launch_bounds__(ROW_THREADS, 4) k_bsuwt(Geo g, Fld f, Prm p) {
   const int S0 = (p.ibsuw0 == 0);
   const int *NF = f.nf;
   ROW_LOOP_BEGIN(g)
   const long long c = cid(g, I, J, K);
   const int NI = g.NI, NJ = g.NJ, NK = g.NK;
-  // ------------------------------ x faces  K=2..NK-1, J=2..NJ-1, I=3..NI-1
-  if (K >= 2 && K <= NK - 1 && J >= 2 && J <= NJ - 1 && I >= 3 && I <= NI - 1 && f.indx[c] == 0) {
-    double *UU = f.uu;
-    const int I1 = I - 1, NL = A(NF, I1, J, K), NR = NF[c];
-    if (NL == 8 && NR == 8) UU[c] = 0.0;
-    else if (NL != 0 && NR != 0) {
-      double DL = 0, VL = 0, DR = 0, VR = 0, V0;
-      if (NL == 3 || NR == 3) {
-        V0 = A(UU, I, J - 1, K);
-        if (S0) { int L1 = J - 1, L2 = J - 2;
-          if (L2 >= 1 && A(NF, I1, L1, K) != -1 && A(NF, I, L1, K) != -1)
-            if (A(NF, I1, L2, K) != -1 && A(NF, I, L2, K) != -1)
-              if (A(NF, I1, L2, K) == 0 || A(NF, I, L2, K) == 0)
-                V0 = V0 + (V0 - A(UU, I, L2, K)) * YY_(3, J) / YY_(3, L1); }
-        if (NL == 3) { DL = YY_(3, J); VL = V0; }
-        if (NR == 3) { DR = YY_(3, J); VR = V0; }
-      }
-      if (NL == 4 || NR == 4) {
-        V0 = A(UU, I, J + 1, K);
-        if (S0) { int L1 = J + 1, L2 = J + 2;
-          if (L2 <= NJ && A(NF, I1, L1, K) != -1 && A(NF, I, L1, K) != -1)
-            if (A(NF, I1, L2, K) != -1 && A(NF, I, L2, K) != -1)
-              if (A(NF, I1, L2, K) == 0 || A(NF, I, L2, K) == 0)
-                V0 = V0 + (V0 - A(UU, I, L2, K)) * YY_(3, L1) / YY_(3, L2); }
-        if (NL == 4) { DL = YY_(3, J + 1); VL = V0; }
-        if (NR == 4) { DR = YY_(3, J + 1); VR = V0; }
-      }
-      if (NL == 5 || NR == 5) {
-        V0 = A(UU, I, J, K - 1);
-        if (S0) { int L1 = K - 1, L2 = K - 2;
-          if (L2 >= 1 && A(NF, I1, J, L1) != -1 && A(NF, I, J, L1) != -1)
-            if (A(NF, I1, J, L2) != -1 && A(NF, I, J, L2) != -1)
-              if (A(NF, I1, J, L2) == 0 || A(NF, I, J, L2) == 0)
-                V0 = V0 + (V0 - A(UU, I, J, L2)) * ZZ_(3, K) / ZZ_(3, L1); }
-        if (NL == 5) { DL = ZZ_(3, K); VL = V0; }
-        if (NR == 5) { DR = ZZ_(3, K); VR = V0; }
-      }
-      if (NL == 6 || NR == 6) {
-        V0 = A(UU, I, J, K + 1);
-        if (S0) { int L1 = K + 1, L2 = K + 2;
-          if (L2 <= NK && A(NF, I1, J, L1) != -1 && A(NF, I, J, L1) != -1)
-            if (A(NF, I1, J, L2) != -1 && A(NF, I, J, L2) != -1)
-              if (A(NF, I1, J, L2) == 0 || A(NF, I, J, L2) == 0)
-                V0 = V0 + (V0 - A(UU, I, J, L2)) * ZZ_(3, L1) / ZZ_(3, L2); }
-        if (NL == 6) { DL = ZZ_(3, K + 1); VL = V0; }
-        if (NR == 6) { DR = ZZ_(3, K + 1); VR = V0; }
-      }
-      if (NL == 8) UU[c] = VR;
-      else if (NR == 8) UU[c] = VL;
-      else UU[c] = (DR * VL + DL * VR) / (DR + DL);
+  // x faces K=2..NK-1, J=2..NJ-1, I=3..NI-1; y faces K=2..NK-1, J=3..NJ-1,
+  // I=2..NI-1; z faces K=3..NK-1, J=2..NJ-1, I=2..NI-1
+  const bool bx = K >= 2 && K <= NK - 1 && J >= 2 && J <= NJ - 1 && I >= 3 && I <= NI - 1;
+  const bool by = K >= 2 && K <= NK - 1 && J >= 3 && J <= NJ - 1 && I >= 2 && I <= NI - 1;
+  const bool bz = K >= 3 && K <= NK - 1 && J >= 2 && J <= NJ - 1 && I >= 2 && I <= NI - 1;
+  if (bx || by || bz) {
+    const int ix = bx ? f.indx[c] : 1, iy = by ? f.indy[c] : 1, iz = bz ? f.indz[c] : 1;
+    const int NR = NF[c];
+    const int NLx = bx ? A(NF, I - 1, J, K) : 0, NLy = by ? A(NF, I, J - 1, K) : 0,
+              NLz = bz ? A(NF, I, J, K - 1) : 0;
+    if (ix == 0) {
+      if (NLx == 8 && NR == 8) f.uu[c] = 0.0;
+      else if (NLx != 0 && NR != 0) f.uu[c] = bsuwt_x(g, NF, f.uu, S0, I, J, K, NLx, NR);
     }
-  }
-  // ------------------------------ y faces  K=2..NK-1, J=3..NJ-1, I=2..NI-1
-  if (K >= 2 && K <= NK - 1 && J >= 3 && J <= NJ - 1 && I >= 2 && I <= NI - 1 && f.indy[c] == 0) {
-    double *VV = f.vv;
-    const int J1 = J - 1, NL = A(NF, I, J1, K), NR = NF[c];
-    if (NL == 8 && NR == 8) VV[c] = 0.0;
-    else if (NL != 0 && NR != 0) {
-      double DL = 0, VL = 0, DR = 0, VR = 0, V0;
-      if (NL == 1 || NR == 1) {
-        V0 = A(VV, I - 1, J, K);
-        if (S0) { int L1 = I - 1, L2 = I - 2;
-          if (L2 >= 1 && A(NF, L1, J1, K) != -1 && A(NF, L1, J, K) != -1)
-            if (A(NF, L2, J1, K) != -1 && A(NF, L2, J, K) != -1)
-              if (A(NF, L2, J1, K) == 0 || A(NF, L2, J, K) == 0)
-                V0 = V0 + (V0 - A(VV, L2, J, K)) * XX_(3, I) / XX_(3, L1); }
-        if (NL == 1) { DL = XX_(3, I); VL = V0; }
-        if (NR == 1) { DR = XX_(3, I); VR = V0; }
-      }
-      if (NL == 2 || NR == 2) {
-        V0 = A(VV, I + 1, J, K);
-        if (S0) { int L1 = I + 1, L2 = I + 2;
-          if (L2 <= NI && A(NF, L1, J1, K) != -1 && A(NF, L1, J, K) != -1)
-            if (A(NF, L2, J1, K) != -1 && A(NF, L2, J, K) != -1)
-              if (A(NF, L2, J1, K) == 0 || A(NF, L2, J, K) == 0)
-                V0 = V0 + (V0 - A(VV, L2, J, K)) * XX_(3, L1) / XX_(3, L2); }
-        if (NL == 2) { DL = XX_(3, I + 1); VL = V0; }
-        if (NR == 2) { DR = XX_(3, I + 1); VR = V0; }
-      }
-      if (NL == 5 || NR == 5) {
-        V0 = A(VV, I, J, K - 1);
-        if (S0) { int L1 = K - 1, L2 = K - 2;
-          if (L2 >= 1 && A(NF, I, J1, L1) != -1 && A(NF, I, J, L1) != -1)
-            if (A(NF, I, J1, L2) != -1 && A(NF, I, J, L2) != -1)
-              if (A(NF, I, J1, L2) == 0 || A(NF, I, J, L2) == 0)
-                V0 = V0 + (V0 - A(VV, I, J, L2)) * ZZ_(3, K) / ZZ_(3, L1); }
-        if (NL == 5) { DL = ZZ_(3, K); VL = V0; }
-        if (NR == 5) { DR = ZZ_(3, K); VR = V0; }
-      }
-      if (NL == 6 || NR == 6) {
-        V0 = A(VV, I, J, K + 1);
-        if (S0) { int L1 = K + 1, L2 = K + 2;
-          if (L2 <= NK && A(NF, I, J1, L1) != -1 && A(NF, I, J, L1) != -1)
-            if (A(NF, I, J1, L2) != -1 && A(NF, I, J, L2) != -1)
-              if (A(NF, I, J1, L2) == 0 || A(NF, I, J, L2) == 0)
-                V0 = V0 + (V0 - A(VV, I, J, L2)) * ZZ_(3, L1) / ZZ_(3, L2); }
-        if (NL == 6) { DL = ZZ_(3, K + 1); VL = V0; }
-        if (NR == 6) { DR = ZZ_(3, K + 1); VR = V0; }
-      }
-      if (NL == 8) VV[c] = VR;
-      else if (NR == 8) VV[c] = VL;
-      else VV[c] = (DR * VL + DL * VR) / (DR + DL);
+    if (iy == 0) {
+      if (NLy == 8 && NR == 8) f.vv[c] = 0.0;
+      else if (NLy != 0 && NR != 0) f.vv[c] = bsuwt_y(g, NF, f.vv, S0, I, J, K, NLy, NR);
     }
-  }
-  // ------------------------------ z faces  K=3..NK-1, J=2..NJ-1, I=2..NI-1
-  if (K >= 3 && K <= NK - 1 && J >= 2 && J <= NJ - 1 && I >= 2 && I <= NI - 1 && f.indz[c] == 0) {
-    double *WW = f.ww;
-    const int K1 = K - 1, NL = A(NF, I, J, K1), NR = NF[c];
-    if (NL == 8 && NR == 8) WW[c] = 0.0;
-    else if (NL != 0 && NR != 0) {
-      double DL = 0, VL = 0, DR = 0, VR = 0, V0;
-      if (NL == 1 || NR == 1) {
-        V0 = A(WW, I - 1, J, K);
-        if (S0) { int L1 = I - 1, L2 = I - 2;
-          if (L2 >= 1 && A(NF, L1, J, K1) != -1 && A(NF, L1, J, K) != -1)
-            if (A(NF, L2, J, K1) != -1 && A(NF, L2, J, K) != -1)
-              if (A(NF, L2, J, K1) == 0 || A(NF, L2, J, K) == 0)
-                V0 = V0 + (V0 - A(WW, L2, J, K)) * XX_(3, I) / XX_(3, L1); }
-        if (NL == 1) { DL = XX_(3, I); VL = V0; }
-        if (NR == 1) { DR = XX_(3, I); VR = V0; }
-      }
-      if (NL == 2 || NR == 2) {
-        V0 = A(WW, I + 1, J, K);
-        if (S0) { int L1 = I + 1, L2 = I + 2;
-          if (L2 <= NI && A(NF, L1, J, K1) != -1 && A(NF, L1, J, K) != -1)
-            if (A(NF, L2, J, K1) != -1 && A(NF, L2, J, K) != -1)
-              if (A(NF, L2, J, K1) == 0 || A(NF, L2, J, K) == 0)
-                V0 = V0 + (V0 - A(WW, L2, J, K)) * XX_(3, L1) / XX_(3, L2); }
-        if (NL == 2) { DL = XX_(3, I + 1); VL = V0; }
-        if (NR == 2) { DR = XX_(3, I + 1); VR = V0; }
-      }
-      if (NL == 3 || NR == 3) {
-        V0 = A(WW, I, J - 1, K);
-        if (S0) { int L1 = J - 1, L2 = J - 2;
-          if (L2 >= 1 && A(NF, I, L1, K1) != -1 && A(NF, I, L1, K) != -1)
-            if (A(NF, I, L2, K1) != -1 && A(NF, I, L2, K) != -1)
-              if (A(NF, I, L2, K1) == 0 || A(NF, I, L2, K) == 0)
-                V0 = V0 + (V0 - A(WW, I, L2, K)) * YY_(3, J) / YY_(3, L1); }
-        if (NL == 3) { DL = YY_(3, J); VL = V0; }
-        if (NR == 3) { DR = YY_(3, J); VR = V0; }
-      }
-      if (NL == 4 || NR == 4) {
-        V0 = A(WW, I, J + 1, K);
-        if (S0) { int L1 = J + 1, L2 = J + 2;
-          if (L2 <= NJ && A(NF, I, L1, K1) != -1 && A(NF, I, L1, K) != -1)
-            if (A(NF, I, L2, K1) != -1 && A(NF, I, L2, K) != -1)
-              if (A(NF, I, L2, K1) == 0 || A(NF, I, L2, K) == 0)
-                V0 = V0 + (V0 - A(WW, I, L2, K)) * YY_(3, L1) / YY_(3, L2); }
-        if (NL == 4) { DL = YY_(3, J + 1); VL = V0; }
-        if (NR == 4) { DR = YY_(3, J + 1); VR = V0; }
-      }
-      if (NL == 8) WW[c] = VR;
-      else if (NR == 8) WW[c] = VL;
-      else WW[c] = (DR * VL + DL * VR) / (DR + DL);
+    if (iz == 0) {
+      if (NLz == 8 && NR == 8) f.ww[c] = 0.0;
+      else if (NLz != 0 && NR != 0) f.ww[c] = bsuwt_z(g, NF, f.ww, S0, I, J, K, NLz, NR);
     }
   }
   ROW_LOOP_END
@@ -288,7 +309,7 @@ __device__ __forceinline__ void lat(const Geo &g, const int *NF, long long a, lo
     if (NF[a] != -1 && NF[b] != -1) { is = 1; d = dv; v = vv; }
 }
 
-__global__ void k_bsuwn3(Geo g, Fld f, Prm p) {
+__global__ void __launch_bounds__(ROW_THREADS, 3) k_bsuwn3(Geo g, Fld f, Prm p) {
   const int S0 = (p.ibsuw0 == 0);
   const int *NF = f.nf;
   double *UU = f.uu, *VV = f.vv, *WW = f.ww;

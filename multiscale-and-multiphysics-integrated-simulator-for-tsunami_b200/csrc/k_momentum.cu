@@ -27,7 +27,7 @@ __device__ __forceinline__ double bnd_tan(const Fld &f, int IS, int nsFirst, dou
   return bc[IS - 1];
 }
 
-__global__ void k_flux(Geo g, Fld f, Prm p, double *FLUU, double *FLUV, double *FLUW,
+__global__ void __launch_bounds__(ROW_THREADS, 3) k_flux(Geo g, Fld f, Prm p, double *FLUU, double *FLUV, double *FLUW,
                        double *FLVU, double *FLVV, double *FLVW, double *FLWU, double *FLWV,
                        double *FLWW) {
   const double SU = p.scmvp, SC = 1.0 - p.scmvp;
@@ -412,7 +412,7 @@ __device__ __forceinline__ double sponge_dmax(const Prm &p, double X, double Y, 
   return DMAX;
 }
 
-__global__ void k_predict(Geo g, Fld f, Prm p, const double *FLUU, const double *FLUV,
+__global__ void __launch_bounds__(ROW_THREADS, 3) k_predict(Geo g, Fld f, Prm p, const double *FLUU, const double *FLUV,
                           const double *FLUW, const double *FLVU, const double *FLVV,
                           const double *FLVW, const double *FLWU, const double *FLWV,
                           const double *FLWW, double *UN, double *VN, double *WN) {

@@ -33,7 +33,7 @@ namespace cadmas {
 #define ZZ_(m, k) gz(g, m, k)
 
 // ------------------------------------------------------------- VF_VPCOEF
-__global__ void k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
+__global__ void __launch_bounds__(ROW_THREADS, 3) k_vpcoef(Geo g, Fld f, Prm p, SysPtr A_, int *err) {
   const double DTI = 1.0 / p.dtnow, TR = p.dtnow / p.rho0, PPS = 0.0;
   const double *GGV = f.ggv, *GLV = f.glv, *FF = f.ff, *PP = f.pp;
   ROW_LOOP_BEGIN(g)
@@ -260,6 +260,67 @@ __global__ void k_to_skew(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys 
   const long long n = (long long)q.nb * q.W * q.T;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
     to_skew_elem(g, q, A_, INDC, S, X0, bsl, xsl, warm, e);
+}
+
+// The same conversion, one block per row tj of a layout tile b: the row's
+// interior cells of all layers, (NK-2) x TI values of one array at a time,
+// are staged in shared memory with coalesced loads and then written slab
+// by slab (TIp consecutive entries of a slab per row).  Same values as
+// to_skew_elem; used when a panel fits in shared memory.
+__global__ void k_to_skew_rows(Geo g, SkewGeo q, SysPtr A_, const int *INDC, SkewSys S, const double *X0,
+                               double *bsl, double *xsl, int warm) {
+  extern __shared__ __align__(16) double pan[];  // [(NK-2) * TI]
+  pdl_enter();
+  const int b = blockIdx.x / q.TJ, tj = blockIdx.x % q.TJ;
+  const int TI = q.TI, TIp = q.TIp, T = q.T, W = q.W, nk = g.NK - 2;
+  const int is = 2 + (b % q.ntx) * TI, J = 2 + (b / q.ntx) * q.TJ + tj;
+  const int wi = (J <= g.NJ - 1) ? min(TI, g.NI - is) : 0;  // columns of the row inside the interior
+  const int npan = nk * TI, nent = W * TIp;
+  const long long slab0 = (long long)b * W;
+  int *ipan = reinterpret_cast<int *>(pan);
+  // INDC, then DD = T = 0, INDC and the warm guess
+#pragma unroll 4
+  for (int x = threadIdx.x; x < npan; x += blockDim.x) {
+    const int k = 2 + x / TI, ti = x % TI;
+    ipan[x] = ti < wi ? INDC[cid(g, is + ti, J, k)] : -1;
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < nent; x += blockDim.x) {
+    const int w = x / TIp, ti = x % TIp, k = 2 + w - ti - tj, t = ti + TIp * tj;
+    const int ic = (ti < TI && k >= 2 && k <= g.NK - 1) ? ipan[(k - 2) * TI + ti] : -1;
+    const long long e = (slab0 + w) * T + t;
+    S.indc[e] = ic;
+    S.sys[sys_at(slab0 + w, SYS_DD, T, t)] = 0.0;
+    S.sys[sys_at(slab0 + w, SYS_T, T, t)] = 0.0;
+    if (warm) xsl[e] = ic != -1 ? xsl[e] : 0.0;
+  }
+  // AD, ALI, ALJ, ALK, AUI, AUJ, AUK, BB and (not warm) X0
+  const double *src[9] = {A_.ad, A_.ali, A_.alj, A_.alk, A_.aui, A_.auj, A_.auk, A_.bb, X0};
+  constexpr int cs[7] = {SYS_AD, SYS_ALI, SYS_ALJ, SYS_ALK, SYS_AUI, SYS_AUJ, SYS_AUK};
+  const int na = warm ? 8 : 9;
+#pragma unroll 1
+  for (int a = 0; a < na; ++a) {
+    __syncthreads();
+    const double *sa = src[a];
+#pragma unroll 4
+    for (int x = threadIdx.x; x < npan; x += blockDim.x) {
+      const int k = 2 + x / TI, ti = x % TI;
+      pan[x] = ti < wi ? sa[cid(g, is + ti, J, k)] : 0.0;
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < nent; x += blockDim.x) {
+      const int w = x / TIp, ti = x % TIp, k = 2 + w - ti - tj, t = ti + TIp * tj;
+      const double v = (ti < TI && k >= 2 && k <= g.NK - 1) ? pan[(k - 2) * TI + ti] : 0.0;
+      if (a < 7) S.sys[sys_at(slab0 + w, cs[a], T, t)] = v;
+      else if (a == 7) bsl[(slab0 + w) * T + t] = v;
+      else xsl[(slab0 + w) * T + t] = v;
+    }
+  }
+}
+// Shared memory of k_to_skew_rows (0: the panel does not fit, k_to_skew).
+static size_t to_skew_rows_bytes(const Geo &g, const SkewGeo &q) {
+  const size_t b = (size_t)(g.NK - 2) * q.TI * sizeof(double);
+  return b <= 64 * 1024 ? b : 0;
 }
 
 // Value of a skewed vector at the cell (ti,tj,k) of tile (bx,by), where ti
@@ -1401,6 +1462,13 @@ static inline dim3 skew_grid(const SkewGeo &q) { return dim3((unsigned)q.ntx, (u
 
 void launch_to_skew(cudaStream_t s, const Geo &g, const SkewGeo &q, const SysPtr &a, const int *indc,
                     const SkewSys &S, const double *x0, double *bsl, double *xsl, int warm) {
+  const size_t rb = to_skew_rows_bytes(g, q);
+  if (rb > 0) {
+    raise_dynamic_smem((const void *)k_to_skew_rows, rb);
+    launch_pdl(k_to_skew_rows, dim3((unsigned)(q.nb * q.TJ)), dim3(128), rb, s, 1, g, q, a, indc, S, x0, bsl, xsl,
+               warm);
+    return;
+  }
   const long long n = (long long)q.nb * q.W * q.T;
   const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
   launch_pdl(k_to_skew, dim3(blocks), dim3(256), 0, s, 1, g, q, a, indc, S, x0, bsl, xsl, warm);

@@ -382,7 +382,7 @@ __global__ void k_fbubup(Geo g, Fld f, Prm p, const unsigned char *active) {
 // ----------------------------------------------------------- VF_FNFPRV
 __device__ __forceinline__ double bcf_or(const Fld &f, int ind, double v) { return ind >= 1 ? f.bcf[ind - 1] : v; }
 
-__global__ void k_fnfprv(Geo g, Fld f, int *err) {
+__global__ void __launch_bounds__(ROW_THREADS, 3) k_fnfprv(Geo g, Fld f, int *err) {
   const double *FF = f.ff;
   int *NF = f.nf;
   ROW_LOOP_BEGIN(g)
