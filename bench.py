@@ -961,7 +961,7 @@ def main():
     ap.add_argument("--eps-inner", type=float, default=1.0e-2,
                     help="floor of the FP32 inner tolerance of the mixed solver (1e-2 measured best on the "
                          "beach: fewer inner iterations in all than with tighter floors)")
-    ap.add_argument("--occ", type=int, choices=[0, 1, 2], default=0,
+    ap.add_argument("--occ", type=int, choices=[0, 1, 2, 4], default=0,
                     help="thread blocks of the MILU sweeps per SM (0: the library's default)")
     ap.add_argument("--dot-passes", type=int, choices=[0, 1], default=0,
                     help="mixed solver: 0 inner products summed by the backward sweeps, 1 separate passes")

@@ -163,8 +163,11 @@ typedef struct cadmas_params {
      wavefronts of two tiles interleave on each SM; it needs blocks of at
      most 256 columns and applies where the ring fits.  0 = the default:
      two blocks for the backward sweeps and the FP32 sweeps when the grid
-     has at least two preconditioner blocks per SM, one otherwise.  The
-     results do not depend on it.                                         */
+     has at least two preconditioner blocks per SM, one otherwise; four
+     for the FP32 backward sweeps (the mixed solver's) of 16x16 blocks
+     (ring depth 4, at most 56 registers) when it has more than two per
+     SM.  4 = four blocks for those sweeps at any size, the default for
+     the others.  The results do not depend on it.                        */
   int    sweep_occupancy;
   /* Inner products of the mixed solver's FP32 iteration (solver 1; no
      counterpart in the reference): 0 = summed by the backward MILU sweeps

@@ -1125,7 +1125,7 @@ int cadmas_create(const cadmas_dims *d, const cadmas_params *p, cadmas_handle **
   h->q.W = (d->numk - 2) + (TI - 1) + (TJl - 1);
   h->q.ntx = (d->numi - 2 + TI - 1) / TI;
   h->q.nb = h->q.ntx * ((d->numj - 2 + TJl - 1) / TJl);
-  h->q.occ = (p->sweep_occupancy == 1 || p->sweep_occupancy == 2) ? p->sweep_occupancy : 0;
+  h->q.occ = (p->sweep_occupancy == 1 || p->sweep_occupancy == 2 || p->sweep_occupancy == 4) ? p->sweep_occupancy : 0;
   h->q.nsm = 148;
   {
     int nsm = 0;

@@ -229,6 +229,9 @@ __device__ __forceinline__ bool drop_walk(const Geo &g, const Fld &f, const Prm 
 }
 
 // y and z lines: one thread per line; consecutive threads take consecutive I.
+// The thread finds the droplet cells of its line 32 walk positions at a
+// time (the loads of a group issued together, its droplet mask kept) and
+// walks from droplet to droplet.
 template <int AX>
 __global__ void k_drop_line(Geo g, Fld f, Prm p, DropArrays d, int L) {
   const int ni = g.NI - 2, nb = AX == 1 ? g.NK - 2 : g.NJ - 2;
@@ -239,9 +242,37 @@ __global__ void k_drop_line(Geo g, Fld f, Prm p, DropArrays d, int L) {
   double *FF = f.ff;
   const int *NF = f.nf;
   auto at = [&](int s) -> long long { return AX == 1 ? cid(g, I, s, K) : cid(g, I, J, s); };
+  const int NA = AX == 1 ? g.NJ : g.NK, dl = (L == 1) ? -1 : 1, s0 = (L == 1) ? NA - 1 : 2, n = NA - 2;
+  const double FL = p.flower;
+  int cc = -1;      // group of walk positions whose mask is held
+  unsigned cm = 0;  // its droplet cells (bit j: walk position 32*cc + j)
+  auto next = [&](int s) -> int {
+    int u = (s - s0) * dl;
+    while (u < n) {
+      const int cu = u >> 5;
+      if (cu != cc) {
+        unsigned m = 0;
+#pragma unroll 8
+        for (int j = 0; j < 32; ++j) {
+          const int uu = (cu << 5) + j;
+          if (uu < n) {
+            const long long a = at(s0 + uu * dl);
+            const double fv = FF[a];
+            const int nv = NF[a];
+            if (fv > FL && nv == 8) m |= 1u << j;
+          }
+        }
+        cc = cu;
+        cm = m;
+      }
+      const unsigned bits = cm & (0xffffffffu << (u & 31));
+      if (bits) return s0 + ((cu << 5) + __ffs(bits) - 1) * dl;
+      u = (cu + 1) << 5;
+    }
+    return DROP_END;
+  };
   drop_walk<AX>(g, f, p, d, L, I, J, K, [&](int s) { return FF[at(s)]; },
-                [&](int s, double v) { FF[at(s)] = v; }, [&](int s) { return NF[at(s)]; },
-                [](int s) { return s; });
+                [&](int s, double v) { FF[at(s)] = v; }, [&](int s) { return NF[at(s)]; }, next);
 }
 
 // x lines: one warp per line (J,K); the warp stages the line's F and NF

@@ -1533,6 +1533,18 @@ static int sweep_depth2(const SkewGeo &q, int mode, int es) {
     if (d <= dmax && sweep_bytes(q, mode, d, es) <= 113 * 1024) return d;
   return 0;
 }
+// Four thread blocks per SM: the FP32 backward sweeps of 16x16 tiles, ring
+// depth 4 and at most 56 registers, so that up to four tiles per SM run in
+// one wave.  By default where the tiles fill more than two blocks per SM
+// (on 512 tiles: 19.6 against 23.0 ms of backward sweeps per step of the
+// mixed solver), or always with q.occ == 4; the other sweeps follow the
+// default's rule then.
+static bool sweep_four(const SkewGeo &q, int mode) {
+  return (q.occ == 4 || (q.occ == 0 && q.nb > 2 * q.nsm)) && q.split == 1 && mode >= SWEEP_BWD && q.T == 256 &&
+         q.TIp == 16 && sweep_bytes(q, mode, 4, 4) <= 55 * 1024;
+}
+// The default's rule for q.occ 0 and 4.
+static int sweep_occ(const SkewGeo &q) { return q.occ == 4 ? 0 : q.occ; }
 template <int MODE, typename V>
 static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const SkewSysT<V> &S, const V *vin,
                          V *vout, SolveState *st) {
@@ -1569,7 +1581,17 @@ static void launch_sweep(cudaStream_t s, const Geo &g, const SkewGeo &q, const S
   // the sweeps' per-step latency, not the bandwidth, sets the time and a
   // second tile's wavefront fills it.  The fused FP64 forward sweep keeps
   // one block: its ring of 8 arrays needs the depth and registers.
-  const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm && (ES == 4 || MODE >= SWEEP_BWD));
+  if constexpr (ES == 4 && MODE >= SWEEP_BWD) {
+    if (sweep_four(q, MODE)) {
+      const size_t b4 = sweep_bytes(q, MODE, 4, ES);
+      set_smem(k_sweep<4, MODE, SWEEP2_THREADS, V, 1, 4, 256, 16>, b4);
+      launch_pdl(k_sweep<4, MODE, SWEEP2_THREADS, V, 1, 4, 256, 16>, grid, block, b4, s, 1, g, q, S, vin, vout, st,
+                 vnull, rnull);
+      return;
+    }
+  }
+  const int oc = sweep_occ(q);
+  const bool two = oc == 2 || (oc == 0 && q.nb >= 2 * q.nsm && (ES == 4 || MODE >= SWEEP_BWD));
   if (two) {
     const int d2 = sweep_depth2(q, MODE, ES);
     if (d2 > 0) {
@@ -1661,7 +1683,15 @@ static bool launch_bwd_dots(cudaStream_t s, const Geo &g, const SkewGeo &q, cons
   if (q.split != 1) return false;
   const bool t256 = q.T == 256 && q.TIp == 16;
   const dim3 grid = skew_grid(q), block((unsigned)sweep_threads(q.T));
-  const bool two = q.occ == 2 || (q.occ == 0 && q.nb >= 2 * q.nsm);
+  if (sweep_four(q, MODE)) {
+    const size_t b4 = sweep_bytes(q, MODE, 4, ES);
+    set_smem(k_sweep<4, MODE, SWEEP2_THREADS, float, 1, 4, 256, 16>, b4);
+    launch_pdl(k_sweep<4, MODE, SWEEP2_THREADS, float, 1, 4, 256, 16>, grid, block, b4, s, 1, g, q, S, r0, x, st, rr,
+               rb);
+    return true;
+  }
+  const int oc = sweep_occ(q);
+  const bool two = oc == 2 || (oc == 0 && q.nb >= 2 * q.nsm);
   if (two) {
     const int d2 = sweep_depth2(q, MODE, ES);
     const size_t bytes2 = sweep_bytes(q, MODE, d2, ES);
@@ -1991,7 +2021,7 @@ static int b_sweep_depth(const SkewGeo &q, int mode, bool two) {
   return two ? sweep_depth2(q, mode, 4) : std::min(sweep_depth(q, mode, 4), 4);
 }
 static bool b_two(const SkewGeo &q, int nsm, int occ, long long ntiles) {
-  return occ == 2 || (occ == 0 && ntiles >= 2LL * nsm);
+  return occ == 2 || ((occ == 0 || occ == 4) && ntiles >= 2LL * nsm);
 }
 bool b_sweeps_supported(const SkewGeo &q, int nsm, int occ, long long ntiles) {
   if (q.split != 1 || sweep_threads(q.T) > 512) return false;

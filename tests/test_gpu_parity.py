@@ -85,19 +85,20 @@ def test_block_jacobi_preconditioner_bitwise(gpu_lib, pkg, orc):
     run_pair(pkg, orc, c, 10, check_every=5, precond_ti=16, precond_tj=4)
 
 
-@pytest.mark.parametrize("solver", [0, 1])
-def test_two_sweep_blocks_per_sm_bitwise(gpu_lib, pkg, orc, solver):
+@pytest.mark.parametrize("solver,occ", [(0, 2), (1, 2), (1, 4)])
+def test_two_sweep_blocks_per_sm_bitwise(gpu_lib, pkg, orc, solver, occ):
     """Two thread blocks of the MILU sweeps per SM (sweep_occupancy 2, a
-    shallower ring under a register cap) change the schedule only: the
-    FP64 run equals the oracle bit for bit, and the mixed solver's run
-    equals the same run with one block per SM bit for bit."""
+    shallower ring under a register cap), or four for the FP32 backward
+    sweeps (sweep_occupancy 4), change the schedule only: the FP64 run
+    equals the oracle bit for bit, and the mixed solver's run equals the
+    same run with one block per SM bit for bit."""
     c = pkg.cases.porous_flume(nx=96, ny=32, nz=30, dx=0.05, dz=0.025, depth=0.4,
                                block=(1.2, 1.8, 0.5), sponge_width=0.6, dt=2e-3)
     over = dict(precond_ti=16, precond_tj=16, cgepsr=1e-10)
     if solver == 0:
         run_pair(pkg, orc, c, 6, check_every=3, sweep_occupancy=2, **over)
         return
-    a = pkg.Tank(c, solver=1, sweep_occupancy=2, **over)
+    a = pkg.Tank(c, solver=1, sweep_occupancy=occ, **over)
     b = pkg.Tank(c, solver=1, sweep_occupancy=1, **over)
     for t in (a, b):
         t.init_state(True)
