@@ -477,7 +477,8 @@ def roofline_of(stages, cells, peak, peak_kind, bytes_table, traffic_per_cell=No
 # layers, tile shape and sweep variants (320 tiles, two blocks per SM for
 # the backward and FP32 sweeps), so the traffic per launch scales with the
 # cells.  FP32 backward: the mean of the sweeps after AP (33.6) and after
-# AE (38.8).
+# AE (38.8); the four-blocks-per-SM instances that now run them on both
+# beaches issue the same bulk copies per step.
 NCU_TRAFFIC_BEACH = {"fwd": 99.8, "bwd": 57.9}
 NCU_TRAFFIC_BEACH_F32 = {"fwd": 49.9, "bwd": 36.2}
 
