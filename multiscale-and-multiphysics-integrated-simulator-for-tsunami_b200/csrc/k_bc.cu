@@ -35,17 +35,6 @@ __device__ __forceinline__ bool inb(const Geo &g, int I, int J, int K) {
 }
 
 // ------------------------------------------------------------ VF_BSUWT
-// One rule of a tangential face: surface cell on side 'side' of the face
-// oriented along axis 'ax' (0 x,1 y,2 z) with fluid toward 'dir' (-1/+1).
-// a: the velocity array of the face; (I,J,K) the face; (I1,J1,K1) the
-// other cell of the face.  Returns V0 and D (XX/YY/ZZ(3,.) spacing).
-struct TanCtx {
-  const Geo *g;
-  const int *NF;
-  const double *a;
-  int S0;
-};
-
 // The three face rules between surface and non-fluid cells, apart from
 // the common cases (gas on both sides: 0; fluid on a side: unchanged),
 // which the kernel handles inline with all its loads issued together.
